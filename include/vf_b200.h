@@ -1,0 +1,154 @@
+/*
+ * vf_b200.h -- C ABI of virtualfluids_b200, a B200 (sm_100a) implementation of
+ * VirtualFluids' single-GPU lattice-Boltzmann time step.
+ *
+ * Every entry point takes plain pointers and sizes, launches on the given CUDA
+ * stream (NULL = legacy default stream) and returns a status code; nothing
+ * calls exit().  The device arrays follow the layout the reference's
+ * LBMSimulationParameter uses (src/gpu/core/Parameter/Parameter.h:67-254):
+ *
+ *   distributions  27 * numberOfLBnodes elements, direction-major
+ *                  (f[d * numberOfLBnodes + k], CudaMemoryManager.cpp:169),
+ *                  holding the shifted populations f_d - w_d;
+ *   neighborX/Y/Z  numberOfLBnodes uint32, the sparse index of the next node in
+ *                  the positive axis direction, node 0 a dummy
+ *                  (GridImp.cpp:2146-2185);
+ *   fluid node list uint32 sparse indices (GridImp.cpp:965-986).
+ *
+ * The storage argument selects the element type of the distributions:
+ * VFB_FP32 (float), VFB_FP64 (double), VFB_FP16 and VFB_BF16 (the precision
+ * form: 16-bit storage, FP32 arithmetic).  Arrays documented as "compute
+ * precision" are double for VFB_FP64 and float otherwise.
+ */
+#ifndef VF_B200_H
+#define VF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VFB_OK 0
+#define VFB_ERR_INVALID_ARGUMENT (-1)
+#define VFB_ERR_CUDA (-2)
+#define VFB_ERR_UNSUPPORTED (-3)
+#define VFB_ERR_NOT_FINITE (-4)
+#define VFB_ERR_OUT_OF_RANGE (-5)
+#define VFB_ERR_CONFIGURATION (-6)
+
+/* storage formats */
+#define VFB_FP32 0
+#define VFB_FP64 1
+#define VFB_FP16 2
+#define VFB_BF16 3
+
+/* CollisionTemplate (src/gpu/core/Calculation/Calculation.h:55-68) */
+#define VFB_TEMPLATE_DEFAULT 0
+#define VFB_TEMPLATE_WRITE_MACRO_VARS 1
+#define VFB_TEMPLATE_APPLY_BODY_FORCE 2
+#define VFB_TEMPLATE_ALL_FEATURES 3
+
+/* GEO types of typeOfGridNode (Calculation.h:38-48) */
+#define VFB_GEO_SOLID 15
+#define VFB_GEO_VOID 16
+#define VFB_GEO_FLUID 19
+
+/* library version (major * 10000 + minor * 100 + patch) */
+int vfb_version(void);
+/* message of the last failing call on this host thread ("" if none) */
+const char* vfb_last_error(void);
+/* bytes of one stored population for a storage format, 0 if unknown */
+int vfb_storage_bytes(int storage);
+
+/*
+ * Collision arguments.  Mirrors vf::gpu::GPUCollisionParameter
+ * (src/gpu/core/Utilities/RunCollision.cuh:49-72); the three global forces and
+ * the quadric limiters are passed by value instead of as device pointers.
+ */
+typedef struct vfb_collision_args {
+    void* distributions;
+    unsigned long long numberOfLBnodes;
+    const uint32_t* neighborX;
+    const uint32_t* neighborY;
+    const uint32_t* neighborZ;
+    const uint32_t* fluidNodeIndices;
+    uint32_t numberOfFluidNodes;
+    double omega;
+    double forces[3];          /* global acceleration (Parameter::getForcesDev) */
+    double forceFactor;        /* 2^-level (KernelUtilities.h:56-64) */
+    double quadricLimiters[3]; /* P, M, D (Parameter.cpp:69) */
+    int isEvenTimestep;
+    int collisionTemplate;     /* VFB_TEMPLATE_* */
+    void* rho;                 /* compute precision, numberOfLBnodes; templates 1 and 3 */
+    void* vx;
+    void* vy;
+    void* vz;
+    void* bodyForceX;          /* compute precision, numberOfLBnodes; templates 2 and 3 */
+    void* bodyForceY;
+    void* bodyForceZ;
+} vfb_collision_args;
+
+/*
+ * K17 compressible cumulant collision fused with esoteric-twist streaming over
+ * a fluid-node list.  Replaces K17CompressibleNavierStokes<None>::runOnIndices
+ * (src/gpu/core/Kernel/Compressible/NavierStokes/K17/K17CompressibleNavierStokes.cu:103-145),
+ * i.e. vf::gpu::runCollision<K17> (src/gpu/core/Utilities/RunCollision.cuh:74-143).
+ */
+int vfb_k17_collision(int storage, const vfb_collision_args* args, void* stream);
+
+/*
+ * BGK compressible collision fused with esoteric-twist streaming.  Replaces
+ * B92CompressibleNavierStokes::run
+ * (src/gpu/core/Kernel/Compressible/NavierStokes/B92/B92CompressibleNavierStokes.cu:43-57),
+ * which visits every node whose typeOfGridNode is neither GEO_SOLID nor
+ * GEO_VOID; pass the fluid-node list of those nodes (the reference's fluid-node
+ * list is exactly that set).  Only omega, the arrays, the node list and
+ * isEvenTimestep of args are used.
+ */
+int vfb_bgk_collision(int storage, const vfb_collision_args* args, void* stream);
+
+/*
+ * Equilibrium initialisation of one parity view from drho and velocity
+ * (compute precision arrays of numberOfLBnodes).  Replaces
+ * InitNavierStokesCompressible_Device
+ * (src/gpu/core/PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cu:44-212);
+ * nodes whose geo is GEO_SOLID or GEO_VOID are skipped.  PreProcessorImp::init
+ * (PreProcessorImp.cpp:50-58) calls it for the odd then the even view.
+ */
+int vfb_init_equilibrium(int storage, void* distributions, unsigned long long numberOfLBnodes, const uint32_t* geo,
+                         const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                         const void* rho, const void* vx, const void* vy, const void* vz, int isEvenTimestep,
+                         void* stream);
+
+/*
+ * drho and velocity of every node from the populations of the given parity
+ * (pyramid sums, src/lbm/MacroscopicQuantities.h:117-127); nodes with geo
+ * GEO_SOLID or GEO_VOID get zeros.  Outputs are compute-precision arrays of
+ * numberOfLBnodes.  The counterpart of calculateMacroscopicQuantitiesCompressible
+ * (src/gpu/core/PostProcessor/MacroscopicQuantities.cu).
+ */
+int vfb_macroscopic(int storage, const void* distributions, unsigned long long numberOfLBnodes, const uint32_t* geo,
+                    const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                    int isEvenTimestep, void* rho, void* vx, void* vy, void* vz, void* stream);
+
+/*
+ * Global sums in FP64 over a node list: out[0] = sum of drho, out[1] = sum of
+ * (drho + 1) * |u|^2 / 2, out[2] = number of non-finite nodes.  out is a HOST
+ * array of 3 doubles; the call synchronises the stream.  The kinetic-energy
+ * definition is that of KineticEnergyAnalyzer::run
+ * (src/gpu/core/PostProcessor/KineticEnergyAnalyzer.cu:66-108) with FP64
+ * accumulation instead of the reference's working-precision reduction.
+ */
+int vfb_mass_and_energy(int storage, const void* distributions, unsigned long long numberOfLBnodes,
+                        const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                        const uint32_t* nodeIndices, uint32_t numberOfIndices, int isEvenTimestep, double* out,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VF_B200_H */

@@ -1,0 +1,239 @@
+"""Python binding of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads the CPU restatement (oracle/liboracle_{f32,f64}.so, built from
+vf_oracle.c) and, when present, the reference's own sources compiled on the
+host (oracle/_ref/libvfref_{f32,f64}.so).  Only tests/, the smoke check and
+bench.py's CPU-baseline leg use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+
+_c = ctypes
+_vp = _c.c_void_p
+
+
+def build(with_ref: bool = False) -> None:
+    """Build the oracle (and the reference libraries when the tree exists)."""
+    subprocess.run(["make", "-C", str(HERE), "ref" if with_ref else "all", "-j8"], check=True,
+                   capture_output=True, text=True)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+class _Lib:
+    def __init__(self, path: Path, suffix: str, real):
+        self.path = path
+        self.L = _c.CDLL(str(path))
+        self.sfx = suffix
+        self.real = real
+
+    def fn(self, name):
+        return getattr(self.L, name + self.sfx)
+
+
+class Oracle(_Lib):
+    """The CPU restatement (vf_oracle.c) for one precision."""
+
+    def __init__(self, precision: str = "f64"):
+        real = np.float64 if precision == "f64" else np.float32
+        super().__init__(HERE / f"liboracle_{precision}.so", "_" + precision, real)
+        R = _c.c_double if precision == "f64" else _c.c_float
+        self.R = R
+        self.fn("vfo_k17_collide").argtypes = [_vp, R, _vp, R, R, R, _vp, _vp, _vp, _vp]
+        self.fn("vfo_collision_k17").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _c.c_uint32, R, _vp, R, _vp,
+                                                 _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        self.fn("vfo_bgk_collide").argtypes = [_vp, R]
+        self.fn("vfo_collision_bgk").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, R, _c.c_int]
+        self.fn("vfo_init_eq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_int]
+        self.fn("vfo_bc_post").argtypes = [_c.c_int, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _c.c_uint32, R, _vp,
+                                           _vp, _vp, _c.c_int]
+        self.fn("vfo_bc_pressure_noneq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
+                                                     _c.c_int, _c.c_int]
+        self.fn("vfo_macroscopic").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _c.c_int, _vp, _vp, _vp, _vp]
+
+    # -- single node ----------------------------------------------------------
+    def k17_node(self, f, omega, limiter=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0)):
+        f = np.ascontiguousarray(f, dtype=self.real).copy()
+        lim = np.asarray(limiter, dtype=self.real)
+        out = [self.R() for _ in range(4)]
+        self.fn("vfo_k17_collide")(_ptr(f), omega, _ptr(lim), force[0], force[1], force[2],
+                                   *[_c.byref(o) for o in out])
+        return f, np.array([o.value for o in out], dtype=self.real)
+
+    def bgk_node(self, f, omega):
+        f = np.ascontiguousarray(f, dtype=self.real).copy()
+        self.fn("vfo_bgk_collide")(_ptr(f), omega)
+        return f
+
+    # -- whole-lattice passes (arrays modified in place) ----------------------
+    def collision_k17(self, dist, N, nx, ny, nz, fluid, omega, forces=(0, 0, 0), force_factor=1.0,
+                      limiters=(0.01, 0.01, 0.01), is_even=True, flags=0, macro=None, body=None):
+        forces = np.asarray(forces, dtype=self.real)
+        lim = np.asarray(limiters, dtype=self.real)
+        rho, vx, vy, vz = macro if macro is not None else (None,) * 4
+        bx, by, bz = body if body is not None else (None,) * 3
+        self.fn("vfo_collision_k17")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(fluid), len(fluid), omega,
+                                     _ptr(forces), force_factor, _ptr(lim), int(is_even), flags, _ptr(rho), _ptr(vx),
+                                     _ptr(vy), _ptr(vz), _ptr(bx), _ptr(by), _ptr(bz))
+
+    def collision_bgk(self, dist, N, geo, nx, ny, nz, omega, is_even=True):
+        self.fn("vfo_collision_bgk")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), omega, int(is_even))
+
+    def init_eq(self, dist, N, geo, nx, ny, nz, rho, ux, uy, uz, is_even):
+        self.fn("vfo_init_eq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(rho), _ptr(ux),
+                               _ptr(uy), _ptr(uz), int(is_even))
+
+    def bc_post(self, kind, dist, N, nx, ny, nz, k, q, omega, vx=None, vy=None, vz=None, is_even=True):
+        self.fn("vfo_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,
+                               _ptr(vx), _ptr(vy), _ptr(vz), int(is_even))
+
+    def bc_pressure(self, dist, N, nx, ny, nz, k, kN, rho, direction, is_even=True):
+        self.fn("vfo_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN), _ptr(rho),
+                                         len(k), direction, int(is_even))
+
+    def macroscopic(self, dist, N, geo, nx, ny, nz, is_even):
+        out = [np.zeros(N, self.real) for _ in range(4)]
+        self.fn("vfo_macroscopic")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), int(is_even),
+                                   *[_ptr(o) for o in out])
+        return out
+
+
+def ref_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"libvfref_{precision}.so").exists()
+
+
+class Reference(_Lib):
+    """The reference's own sources compiled on the host (oracle/_ref)."""
+
+    def __init__(self, precision: str = "f64"):
+        real = np.float64 if precision == "f64" else np.float32
+        super().__init__(REF_DIR / f"libvfref_{precision}.so", "_" + precision, real)
+        R = _c.c_double if precision == "f64" else _c.c_float
+        self.R = R
+        self.fn("vfref_k17_node").argtypes = [_vp, R, _vp, R, R, R, _vp]
+        self.fn("vfref_collision_k17").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _c.c_uint, R, _vp, R, _vp,
+                                                   _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        self.fn("vfref_collision_bgk").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, R, _c.c_int]
+        self.fn("vfref_init_eq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_int]
+        self.fn("vfref_bc_post").argtypes = [_c.c_int, _vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _c.c_uint, R, _vp,
+                                             _vp, _vp, _c.c_int]
+        self.fn("vfref_bc_pressure_noneq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint,
+                                                       _c.c_int, _c.c_int]
+        self.fn("vfref_grid_build").restype = _vp
+        self.fn("vfref_grid_build").argtypes = [_vp]
+        self.fn("vfref_grid_levels").argtypes = [_vp]
+        self.fn("vfref_grid_count").restype = _c.c_longlong
+        self.fn("vfref_grid_count").argtypes = [_vp, _c.c_int, _c.c_char_p]
+        self.fn("vfref_grid_elem_size").argtypes = [_vp, _c.c_int, _c.c_char_p]
+        self.fn("vfref_grid_copy").argtypes = [_vp, _c.c_int, _c.c_char_p, _vp]
+        self.fn("vfref_grid_free").argtypes = [_vp]
+        self.fn("vfref_cpu_block_create").restype = _vp
+        self.fn("vfref_cpu_block_create").argtypes = [_c.c_int, _c.c_int, _c.c_int]
+        self.fn("vfref_cpu_block_free").argtypes = [_vp]
+        self.fn("vfref_cpu_block_run").restype = _c.c_double
+        self.fn("vfref_cpu_block_run").argtypes = [_vp, _c.c_int, R]
+
+    def k17_node(self, f, omega, limiter=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0)):
+        f = np.ascontiguousarray(f, dtype=self.real).copy()
+        lim = np.asarray(limiter, dtype=self.real)
+        out = np.zeros(4, self.real)
+        self.fn("vfref_k17_node")(_ptr(f), omega, _ptr(lim), force[0], force[1], force[2], _ptr(out))
+        return f, out
+
+    def collision_k17(self, dist, N, nx, ny, nz, fluid, omega, forces=(0, 0, 0), force_factor=1.0,
+                      limiters=(0.01, 0.01, 0.01), is_even=True, flags=0, macro=None, body=None):
+        forces = np.asarray(forces, dtype=self.real)
+        lim = np.asarray(limiters, dtype=self.real)
+        rho, vx, vy, vz = macro if macro is not None else (None,) * 4
+        bx, by, bz = body if body is not None else (None,) * 3
+        self.fn("vfref_collision_k17")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(fluid), len(fluid), omega,
+                                       _ptr(forces), force_factor, _ptr(lim), int(is_even), flags, _ptr(rho),
+                                       _ptr(vx), _ptr(vy), _ptr(vz), _ptr(bx), _ptr(by), _ptr(bz))
+
+    def collision_bgk(self, dist, N, geo, nx, ny, nz, omega, is_even=True):
+        self.fn("vfref_collision_bgk")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), omega, int(is_even))
+
+    def init_eq(self, dist, N, geo, nx, ny, nz, rho, ux, uy, uz, is_even):
+        self.fn("vfref_init_eq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(rho), _ptr(ux),
+                                 _ptr(uy), _ptr(uz), int(is_even))
+
+    def bc_post(self, kind, dist, N, nx, ny, nz, k, q, omega, vx=None, vy=None, vz=None, is_even=True):
+        self.fn("vfref_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,
+                                 _ptr(vx), _ptr(vy), _ptr(vz), int(is_even))
+
+    def bc_pressure(self, dist, N, nx, ny, nz, k, kN, rho, direction, is_even=True):
+        self.fn("vfref_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN),
+                                           _ptr(rho), len(k), direction, int(is_even))
+
+    def grid(self, spec):
+        """Build a grid with the reference builder; returns {level: {name: array}}."""
+        s = np.zeros(64)
+        s[:len(spec)] = spec
+        h = self.fn("vfref_grid_build")(_ptr(s))
+        try:
+            out = {}
+            for level in range(self.fn("vfref_grid_levels")(h)):
+                out[level] = _export_all(self, h, level, "vfref_grid")
+            return out
+        finally:
+            self.fn("vfref_grid_free")(h)
+
+    def cpu_block_mlups(self, n: int, steps: int, omega: float = 1.9) -> tuple[float, float]:
+        """Run the reference CPU K17 loop on an n^3 block; returns (seconds, MLUPS)."""
+        h = self.fn("vfref_cpu_block_create")(n, n, n)
+        try:
+            sec = self.fn("vfref_cpu_block_run")(h, steps, omega)
+        finally:
+            self.fn("vfref_cpu_block_free")(h)
+        return sec, steps * n ** 3 / sec / 1e6
+
+
+_NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims", "fluid",
+          "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k", "slip.nx", "slip.ny",
+          "slip.nz", "slip.q", "geometry.k", "geometry.q", "pressure.count", "cf.coarse", "cf.fine", "fc.coarse",
+          "fc.fine", "cf.offX", "cf.offY", "cf.offZ", "fc.offX", "fc.offY", "fc.offZ"]
+_INT_NAMES = {"velocity.k", "slip.k", "geometry.k", "pressure.count", "dims"}
+
+
+def _dtype_for(name: str, size: int):
+    base = name.split(".")[-1]
+    if name in _INT_NAMES or base in ("k", "kN", "dir", "count"):
+        return np.int32
+    if name in ("neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "fluid", "cf.coarse", "cf.fine",
+                "fc.coarse", "fc.fine"):
+        return np.uint32
+    return np.float64 if size == 8 else np.float32
+
+
+def _export_all(obj, h, level, prefix):
+    count = obj.fn(prefix + "_count") if hasattr(obj, "fn") else getattr(obj, prefix + "_count")
+    esize = obj.fn(prefix + "_elem_size")
+    copy = obj.fn(prefix + "_copy")
+    names = list(_NAMES)
+    npc = count(h, level, b"pressure.count")
+    if npc >= 0:
+        tmp = np.zeros(1, np.int32)
+        copy(h, level, b"pressure.count", _ptr(tmp))
+        for i in range(int(tmp[0])):
+            names += [f"pressure{i}.{s}" for s in ("k", "kN", "rho", "q", "dir")]
+    out = {}
+    for name in names:
+        n = count(h, level, name.encode())
+        if n < 0:
+            continue
+        es = esize(h, level, name.encode())
+        a = np.zeros(n, _dtype_for(name, es))
+        assert a.itemsize == es, (name, a.itemsize, es)
+        copy(h, level, name.encode(), _ptr(a))
+        out[name] = a
+    return out

@@ -1,0 +1,124 @@
+"""ctypes binding of the C ABI declared in include/vf_b200.h.
+
+The library is loaded from this package directory (libvfb200.so, built by
+``python -m virtualfluids_b200.build``).  There is no fallback: if the shared
+library is missing or fails to load, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libvfb200.so"
+
+VFB_OK = 0
+VFB_ERR_INVALID_ARGUMENT = -1
+VFB_ERR_CUDA = -2
+VFB_ERR_UNSUPPORTED = -3
+VFB_ERR_NOT_FINITE = -4
+VFB_ERR_OUT_OF_RANGE = -5
+VFB_ERR_CONFIGURATION = -6
+
+FP32, FP64, FP16, BF16 = 0, 1, 2, 3
+STORAGE_NAMES = {"fp32": FP32, "fp64": FP64, "fp16": FP16, "bf16": BF16}
+
+TEMPLATE_DEFAULT, TEMPLATE_WRITE_MACRO_VARS, TEMPLATE_APPLY_BODY_FORCE, TEMPLATE_ALL_FEATURES = 0, 1, 2, 3
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+class CollisionArgs(ctypes.Structure):
+    """vfb_collision_args (include/vf_b200.h)."""
+
+    _fields_ = [
+        ("distributions", ctypes.c_void_p),
+        ("numberOfLBnodes", ctypes.c_ulonglong),
+        ("neighborX", ctypes.c_void_p),
+        ("neighborY", ctypes.c_void_p),
+        ("neighborZ", ctypes.c_void_p),
+        ("fluidNodeIndices", ctypes.c_void_p),
+        ("numberOfFluidNodes", ctypes.c_uint32),
+        ("omega", ctypes.c_double),
+        ("forces", ctypes.c_double * 3),
+        ("forceFactor", ctypes.c_double),
+        ("quadricLimiters", ctypes.c_double * 3),
+        ("isEvenTimestep", ctypes.c_int),
+        ("collisionTemplate", ctypes.c_int),
+        ("rho", ctypes.c_void_p),
+        ("vx", ctypes.c_void_p),
+        ("vy", ctypes.c_void_p),
+        ("vz", ctypes.c_void_p),
+        ("bodyForceX", ctypes.c_void_p),
+        ("bodyForceY", ctypes.c_void_p),
+        ("bodyForceZ", ctypes.c_void_p),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point
+_SIGNATURES = [
+    ("vfb_version", ctypes.c_int, []),
+    ("vfb_last_error", ctypes.c_char_p, []),
+    ("vfb_storage_bytes", ctypes.c_int, [ctypes.c_int]),
+    ("vfb_k17_collision", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
+    ("vfb_bgk_collision", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
+    ("vfb_init_equilibrium", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+      ctypes.c_void_p]),
+    ("vfb_macroscopic", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ("vfb_mass_and_energy", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+    ("vfb_grid_levels", ctypes.c_int, [ctypes.c_void_p]),
+    ("vfb_grid_count", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),
+    ("vfb_grid_elem_size", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),
+    ("vfb_grid_copy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]),
+    ("vfb_grid_free", None, [ctypes.c_void_p]),
+]
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded native library; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m virtualfluids_b200.build` "
+                    "(there is no CPU fallback)")
+            L = ctypes.CDLL(str(LIB_PATH))
+            for name, res, args in _SIGNATURES:
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+        return _lib
+
+
+def exported_symbols() -> list[str]:
+    return [s[0] for s in _SIGNATURES]
+
+
+class VfbError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"vfb error {code}: {message}")
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != VFB_OK:
+        msg = lib().vfb_last_error()
+        raise VfbError(rc, msg.decode() if msg else "")
+
+
+def last_error() -> str:
+    m = lib().vfb_last_error()
+    return m.decode() if m else ""

@@ -1,0 +1,495 @@
+// collision.cu -- fused collide + esoteric-twist stream kernels (K17, BGK),
+// equilibrium initialisation, macroscopic output and FP64 reductions.
+//
+// One thread updates one fluid node: it follows the reference's index chain
+// (ListIndices, src/gpu/core/Utilities/KernelUtilities.h:221-245) to the
+// eight locations of the node, gathers the 27 pre-collision populations of the
+// current parity (KernelUtilities.h:252-281), collides in registers and
+// scatters the post-collision populations into the inverse slots
+// (KernelUtilities.h:350-379).  Every location is read and written by exactly
+// one thread, so the update is in place and race free.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "capi_common.cuh"
+#include "collision_math.cuh"
+#include "d3q27.cuh"
+#include "storage.cuh"
+
+namespace vfb
+{
+
+template <class S>
+struct CollisionKernelArgs {
+    using R = typename Storage<S>::R;
+    S* dist;
+    unsigned long long N;
+    const uint32_t* __restrict__ nX;
+    const uint32_t* __restrict__ nY;
+    const uint32_t* __restrict__ nZ;
+    const uint32_t* __restrict__ fluid;
+    uint32_t nFluid;
+    K17Rates<R> rates;
+    R fx, fy, fz;         // forces * 1/2 * forceFactor
+    R gfx, gfy, gfz;      // raw global forces (body-force template)
+    R forceFactor;
+    R* rho;
+    R* vx;
+    R* vy;
+    R* vz;
+    R* bfx;
+    R* bfy;
+    R* bfz;
+};
+
+template <class S, bool EVEN>
+__device__ __forceinline__ void gatherPre(typename Storage<S>::R* f, const S* __restrict__ dist, unsigned long long N,
+                                          const Locs& L)
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+}
+
+template <class S, bool EVEN>
+__device__ __forceinline__ void scatterPost(const typename Storage<S>::R* f, S* __restrict__ dist, unsigned long long N,
+                                            const Locs& L)
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[inv(d)]);
+}
+
+template <class S, bool EVEN>
+__device__ __forceinline__ void scatterPre(const typename Storage<S>::R* f, S* __restrict__ dist, unsigned long long N,
+                                           const Locs& L)
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d]);
+}
+
+constexpr int kCollisionThreads = 128;
+
+template <class S, bool EVEN, bool WRITE_MACRO, bool BODY_FORCE>
+__global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKernelArgs<S> a)
+{
+    using R = typename Storage<S>::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nFluid)
+        return;
+    const uint32_t k = __ldg(a.fluid + i);
+
+    R fx = a.fx, fy = a.fy, fz = a.fz;
+    if (BODY_FORCE) {
+        fx = (a.gfx + a.bfx[k]) * R(0.5) * a.forceFactor;
+        fy = (a.gfy + a.bfy[k]) * R(0.5) * a.forceFactor;
+        fz = (a.gfz + a.bfz[k]) * R(0.5) * a.forceFactor;
+        a.bfx[k] = R(0);
+        a.bfy[k] = R(0);
+        a.bfz[k] = R(0);
+    }
+
+    const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
+    R f[27];
+    gatherPre<S, EVEN>(f, a.dist, a.N, L);
+    R drho, ux, uy, uz;
+    k17Collide<R>(f, a.rates, fx, fy, fz, drho, ux, uy, uz);
+    if (WRITE_MACRO) {
+        a.vx[k] = ux;
+        a.vy[k] = uy;
+        a.vz[k] = uz;
+        a.rho[k] = drho;
+    }
+    scatterPost<S, EVEN>(f, a.dist, a.N, L);
+}
+
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(kCollisionThreads) bgkKernel(const CollisionKernelArgs<S> a)
+{
+    using R = typename Storage<S>::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nFluid)
+        return;
+    const uint32_t k = __ldg(a.fluid + i);
+    const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
+    R f[27];
+    gatherPre<S, EVEN>(f, a.dist, a.N, L);
+    bgkCollide<R>(f, a.rates.omega);
+    scatterPost<S, EVEN>(f, a.dist, a.N, L);
+}
+
+// InitNavierStokesCompressible_Device.cu:173-200
+template <class S, bool EVEN>
+__global__ void initEqKernel(S* dist, unsigned long long N, const uint32_t* __restrict__ geo,
+                             const uint32_t* __restrict__ nX, const uint32_t* __restrict__ nY,
+                             const uint32_t* __restrict__ nZ, const typename Storage<S>::R* rho,
+                             const typename Storage<S>::R* ux, const typename Storage<S>::R* uy,
+                             const typename Storage<S>::R* uz)
+{
+    using R = typename Storage<S>::R;
+    const unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N)
+        return;
+    const uint32_t g = geo[k];
+    if (g == 15u || g == 16u)
+        return;
+    const R drho = rho[k], vx1 = ux[k], vx2 = uy[k], vx3 = uz[k];
+    const R cu_sq = R(1.5) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+    R f[27];
+    f[d000] = weight<R>(d000) * (drho - cu_sq * (R(1) + drho));
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const R cu = cdot<R>(d, vx1, vx2, vx3);
+        f[d] = weight<R>(d) * (drho + (R(1) + drho) * (R(3) * cu + R(4.5) * cu * cu - cu_sq));
+    }
+    const Locs L = listIndices((uint32_t)k, nX, nY, nZ);
+    scatterPre<S, EVEN>(f, dist, N, L);
+}
+
+template <class S, bool EVEN>
+__global__ void macroscopicKernel(const S* dist, unsigned long long N, const uint32_t* __restrict__ geo,
+                                  const uint32_t* __restrict__ nX, const uint32_t* __restrict__ nY,
+                                  const uint32_t* __restrict__ nZ, typename Storage<S>::R* rho,
+                                  typename Storage<S>::R* vx, typename Storage<S>::R* vy, typename Storage<S>::R* vz)
+{
+    using R = typename Storage<S>::R;
+    const unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N)
+        return;
+    const uint32_t g = geo[k];
+    if (g == 15u || g == 16u) {
+        rho[k] = R(0);
+        vx[k] = R(0);
+        vy[k] = R(0);
+        vz[k] = R(0);
+        return;
+    }
+    const Locs L = listIndices((uint32_t)k, nX, nY, nZ);
+    R f[27];
+    gatherPre<S, EVEN>(f, dist, N, L);
+    const R drho = pyramidDensity(f);
+    const R oneOverRho = R(1) / (drho + R(1));
+    rho[k] = drho;
+    vx[k] = pyramidJx(f) * oneOverRho;
+    vy[k] = pyramidJy(f) * oneOverRho;
+    vz[k] = pyramidJz(f) * oneOverRho;
+}
+
+// FP64 block partial sums of mass, kinetic energy and non-finite count
+constexpr int kReduceThreads = 256;
+
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(kReduceThreads) massEnergyKernel(const S* dist, unsigned long long N,
+                                                                   const uint32_t* __restrict__ nX,
+                                                                   const uint32_t* __restrict__ nY,
+                                                                   const uint32_t* __restrict__ nZ,
+                                                                   const uint32_t* __restrict__ idx, uint32_t n,
+                                                                   double* __restrict__ partial)
+{
+    using R = typename Storage<S>::R;
+    double m = 0.0, e = 0.0, bad = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = __ldg(idx + i);
+        const Locs L = listIndices(k, nX, nY, nZ);
+        R f[27];
+        gatherPre<S, EVEN>(f, dist, N, L);
+        const R drho = pyramidDensity(f);
+        const R oneOverRho = R(1) / (drho + R(1));
+        const double ux = (double)(pyramidJx(f) * oneOverRho);
+        const double uy = (double)(pyramidJy(f) * oneOverRho);
+        const double uz = (double)(pyramidJz(f) * oneOverRho);
+        const double ke = 0.5 * (ux * ux + uy * uy + uz * uz) * ((double)drho + 1.0);
+        if (isfinite(ke) && isfinite((double)drho)) {
+            m += (double)drho;
+            e += ke;
+        } else {
+            bad += 1.0;
+        }
+    }
+    // warp then block reduction
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, o);
+        e += __shfl_down_sync(0xffffffffu, e, o);
+        bad += __shfl_down_sync(0xffffffffu, bad, o);
+    }
+    __shared__ double sm[3][kReduceThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sm[0][warp] = m;
+        sm[1][warp] = e;
+        sm[2][warp] = bad;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        m = lane < kReduceThreads / 32 ? sm[0][lane] : 0.0;
+        e = lane < kReduceThreads / 32 ? sm[1][lane] : 0.0;
+        bad = lane < kReduceThreads / 32 ? sm[2][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m += __shfl_down_sync(0xffffffffu, m, o);
+            e += __shfl_down_sync(0xffffffffu, e, o);
+            bad += __shfl_down_sync(0xffffffffu, bad, o);
+        }
+        if (lane == 0) {
+            partial[3 * blockIdx.x + 0] = m;
+            partial[3 * blockIdx.x + 1] = e;
+            partial[3 * blockIdx.x + 2] = bad;
+        }
+    }
+}
+
+// ------------------------------------------------------------- launchers --
+template <class S>
+static int launchCollision(bool bgk, const vfb_collision_args* a, cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    CollisionKernelArgs<S> k;
+    k.dist = static_cast<S*>(a->distributions);
+    k.N = a->numberOfLBnodes;
+    k.nX = a->neighborX;
+    k.nY = a->neighborY;
+    k.nZ = a->neighborZ;
+    k.fluid = a->fluidNodeIndices;
+    k.nFluid = a->numberOfFluidNodes;
+    k.rates = makeK17Rates<R>((R)a->omega, (R)a->quadricLimiters[0], (R)a->quadricLimiters[1],
+                              (R)a->quadricLimiters[2]);
+    k.forceFactor = (R)a->forceFactor;
+    k.gfx = (R)a->forces[0];
+    k.gfy = (R)a->forces[1];
+    k.gfz = (R)a->forces[2];
+    k.fx = k.gfx * R(0.5) * k.forceFactor;
+    k.fy = k.gfy * R(0.5) * k.forceFactor;
+    k.fz = k.gfz * R(0.5) * k.forceFactor;
+    k.rho = static_cast<R*>(a->rho);
+    k.vx = static_cast<R*>(a->vx);
+    k.vy = static_cast<R*>(a->vy);
+    k.vz = static_cast<R*>(a->vz);
+    k.bfx = static_cast<R*>(a->bodyForceX);
+    k.bfy = static_cast<R*>(a->bodyForceY);
+    k.bfz = static_cast<R*>(a->bodyForceZ);
+    if (a->numberOfFluidNodes == 0)
+        return VFB_OK;
+    const unsigned blocks = (a->numberOfFluidNodes + kCollisionThreads - 1) / kCollisionThreads;
+    const bool even = a->isEvenTimestep != 0;
+    if (bgk) {
+        if (even)
+            bgkKernel<S, true><<<blocks, kCollisionThreads, 0, stream>>>(k);
+        else
+            bgkKernel<S, false><<<blocks, kCollisionThreads, 0, stream>>>(k);
+        return checkLaunch("bgk collision");
+    }
+    const int t = a->collisionTemplate;
+#define VFB_K17(E, W, B) k17Kernel<S, E, W, B><<<blocks, kCollisionThreads, 0, stream>>>(k)
+    switch (t) {
+    case VFB_TEMPLATE_DEFAULT: even ? VFB_K17(true, false, false) : VFB_K17(false, false, false); break;
+    case VFB_TEMPLATE_WRITE_MACRO_VARS: even ? VFB_K17(true, true, false) : VFB_K17(false, true, false); break;
+    case VFB_TEMPLATE_APPLY_BODY_FORCE: even ? VFB_K17(true, false, true) : VFB_K17(false, false, true); break;
+    case VFB_TEMPLATE_ALL_FEATURES: even ? VFB_K17(true, true, true) : VFB_K17(false, true, true); break;
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "invalid collisionTemplate %d", t);
+    }
+#undef VFB_K17
+    return checkLaunch("k17 collision");
+}
+
+static int checkCollisionArgs(int storage, const vfb_collision_args* a, bool bgk)
+{
+    if (!a)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "args is NULL");
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (a->numberOfFluidNodes == 0)
+        return VFB_OK;
+    if (!a->distributions || !a->neighborX || !a->neighborY || !a->neighborZ || !a->fluidNodeIndices)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL distributions, neighbor or fluid-node array");
+    if (a->numberOfLBnodes < 2 || a->numberOfLBnodes > 0xffffffffull)
+        return setError(VFB_ERR_OUT_OF_RANGE, "numberOfLBnodes %llu outside [2, 2^32)", a->numberOfLBnodes);
+    if (!(a->omega > 0.0 && a->omega < 2.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "omega %g outside (0, 2)", a->omega);
+    if (!bgk) {
+        const int t = a->collisionTemplate;
+        if ((t == VFB_TEMPLATE_WRITE_MACRO_VARS || t == VFB_TEMPLATE_ALL_FEATURES) &&
+            (!a->rho || !a->vx || !a->vy || !a->vz))
+            return setError(VFB_ERR_INVALID_ARGUMENT, "template %d needs rho/vx/vy/vz", t);
+        if ((t == VFB_TEMPLATE_APPLY_BODY_FORCE || t == VFB_TEMPLATE_ALL_FEATURES) &&
+            (!a->bodyForceX || !a->bodyForceY || !a->bodyForceZ))
+            return setError(VFB_ERR_INVALID_ARGUMENT, "template %d needs bodyForceX/Y/Z", t);
+    }
+    return VFB_OK;
+}
+
+template <class S>
+static int launchInit(void* dist, unsigned long long N, const uint32_t* geo, const uint32_t* nX, const uint32_t* nY,
+                      const uint32_t* nZ, const void* rho, const void* vx, const void* vy, const void* vz, int even,
+                      cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    const unsigned blocks = (unsigned)((N + 127) / 128);
+    if (even)
+        initEqKernel<S, true><<<blocks, 128, 0, stream>>>(static_cast<S*>(dist), N, geo, nX, nY, nZ,
+                                                          static_cast<const R*>(rho), static_cast<const R*>(vx),
+                                                          static_cast<const R*>(vy), static_cast<const R*>(vz));
+    else
+        initEqKernel<S, false><<<blocks, 128, 0, stream>>>(static_cast<S*>(dist), N, geo, nX, nY, nZ,
+                                                           static_cast<const R*>(rho), static_cast<const R*>(vx),
+                                                           static_cast<const R*>(vy), static_cast<const R*>(vz));
+    return checkLaunch("init equilibrium");
+}
+
+template <class S>
+static int launchMacro(const void* dist, unsigned long long N, const uint32_t* geo, const uint32_t* nX,
+                       const uint32_t* nY, const uint32_t* nZ, int even, void* rho, void* vx, void* vy, void* vz,
+                       cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    const unsigned blocks = (unsigned)((N + 127) / 128);
+    if (even)
+        macroscopicKernel<S, true><<<blocks, 128, 0, stream>>>(static_cast<const S*>(dist), N, geo, nX, nY, nZ,
+                                                               static_cast<R*>(rho), static_cast<R*>(vx),
+                                                               static_cast<R*>(vy), static_cast<R*>(vz));
+    else
+        macroscopicKernel<S, false><<<blocks, 128, 0, stream>>>(static_cast<const S*>(dist), N, geo, nX, nY, nZ,
+                                                                static_cast<R*>(rho), static_cast<R*>(vx),
+                                                                static_cast<R*>(vy), static_cast<R*>(vz));
+    return checkLaunch("macroscopic");
+}
+
+template <class S>
+static int launchMassEnergy(const void* dist, unsigned long long N, const uint32_t* nX, const uint32_t* nY,
+                            const uint32_t* nZ, const uint32_t* idx, uint32_t n, int even, double* partial,
+                            unsigned blocks, cudaStream_t stream)
+{
+    if (even)
+        massEnergyKernel<S, true><<<blocks, kReduceThreads, 0, stream>>>(static_cast<const S*>(dist), N, nX, nY, nZ,
+                                                                         idx, n, partial);
+    else
+        massEnergyKernel<S, false><<<blocks, kReduceThreads, 0, stream>>>(static_cast<const S*>(dist), N, nX, nY,
+                                                                          nZ, idx, n, partial);
+    return checkLaunch("mass and energy");
+}
+
+} // namespace vfb
+
+using namespace vfb;
+
+extern "C" int vfb_k17_collision(int storage, const vfb_collision_args* args, void* stream)
+{
+    clearError();
+    int rc = checkCollisionArgs(storage, args, false);
+    if (rc != VFB_OK || args->numberOfFluidNodes == 0)
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchCollision<float>(false, args, s);
+    case VFB_FP64: return launchCollision<double>(false, args, s);
+    case VFB_FP16: return launchCollision<__half>(false, args, s);
+    case VFB_BF16: return launchCollision<__nv_bfloat16>(false, args, s);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+
+extern "C" int vfb_bgk_collision(int storage, const vfb_collision_args* args, void* stream)
+{
+    clearError();
+    int rc = checkCollisionArgs(storage, args, true);
+    if (rc != VFB_OK || args->numberOfFluidNodes == 0)
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchCollision<float>(true, args, s);
+    case VFB_FP64: return launchCollision<double>(true, args, s);
+    case VFB_FP16: return launchCollision<__half>(true, args, s);
+    case VFB_BF16: return launchCollision<__nv_bfloat16>(true, args, s);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+
+extern "C" int vfb_init_equilibrium(int storage, void* distributions, unsigned long long N, const uint32_t* geo,
+                                    const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ, const void* rho,
+                                    const void* vx, const void* vy, const void* vz, int isEven, void* stream)
+{
+    clearError();
+    if (!distributions || !geo || !nX || !nY || !nZ || !rho || !vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (N < 2 || N > 0xffffffffull)
+        return setError(VFB_ERR_OUT_OF_RANGE, "numberOfLBnodes %llu outside [2, 2^32)", N);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchInit<float>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    case VFB_FP64: return launchInit<double>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    case VFB_FP16: return launchInit<__half>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    case VFB_BF16: return launchInit<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+
+extern "C" int vfb_macroscopic(int storage, const void* distributions, unsigned long long N, const uint32_t* geo,
+                               const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ, int isEven, void* rho,
+                               void* vx, void* vy, void* vz, void* stream)
+{
+    clearError();
+    if (!distributions || !geo || !nX || !nY || !nZ || !rho || !vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (N < 2 || N > 0xffffffffull)
+        return setError(VFB_ERR_OUT_OF_RANGE, "numberOfLBnodes %llu outside [2, 2^32)", N);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchMacro<float>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    case VFB_FP64: return launchMacro<double>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    case VFB_FP16: return launchMacro<__half>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    case VFB_BF16: return launchMacro<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+
+extern "C" int vfb_mass_and_energy(int storage, const void* distributions, unsigned long long N, const uint32_t* nX,
+                                   const uint32_t* nY, const uint32_t* nZ, const uint32_t* idx, uint32_t n,
+                                   int isEven, double* out, void* stream)
+{
+    clearError();
+    if (!out)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out is NULL");
+    out[0] = out[1] = out[2] = 0.0;
+    if (n == 0)
+        return VFB_OK;
+    if (!distributions || !nX || !nY || !nZ || !idx)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    unsigned blocks = (unsigned)sms * 4u;
+    const unsigned need = (n + kReduceThreads - 1) / kReduceThreads;
+    if (need < blocks)
+        blocks = need;
+    double* partial = nullptr;
+    if (cudaMallocAsync(&partial, sizeof(double) * 3 * blocks, s) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "cudaMallocAsync of %u partial sums failed", blocks);
+    int rc = VFB_OK;
+    switch (storage) {
+    case VFB_FP32: rc = launchMassEnergy<float>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    case VFB_FP64: rc = launchMassEnergy<double>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    case VFB_FP16: rc = launchMassEnergy<__half>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    default: rc = launchMassEnergy<__nv_bfloat16>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    }
+    if (rc == VFB_OK) {
+        std::vector<double> host(3 * (size_t)blocks);
+        if (cudaMemcpyAsync(host.data(), partial, sizeof(double) * 3 * blocks, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = setError(VFB_ERR_CUDA, "copy of partial sums failed: %s", cudaGetErrorString(cudaGetLastError()));
+        } else {
+            for (unsigned b = 0; b < blocks; ++b) {
+                out[0] += host[3 * b + 0];
+                out[1] += host[3 * b + 1];
+                out[2] += host[3 * b + 2];
+            }
+        }
+    }
+    cudaFreeAsync(partial, s);
+    return rc;
+}

@@ -1,0 +1,212 @@
+// grid_capi.cpp -- C ABI of the grid builder: build a multi-level sparse grid
+// from a flat description and export the arrays the GPU solver consumes.
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "capi_common.cuh"
+#include "grid_builder.hpp"
+
+namespace
+{
+using namespace vfb::grid;
+
+struct Exported {
+    std::map<std::string, std::vector<char>> data;
+    std::map<std::string, int> elem;
+    template <class T>
+    void put(const std::string& name, const std::vector<T>& v)
+    {
+        std::vector<char>& d = data[name];
+        d.resize(v.size() * sizeof(T));
+        if (!v.empty())
+            std::memcpy(d.data(), v.data(), d.size());
+        elem[name] = (int)sizeof(T);
+    }
+};
+
+struct GridHandle {
+    GridBuilder builder;
+    std::vector<Exported> levels;
+};
+
+SideType sideOf(int s)
+{
+    if (s < 0 || s > 5)
+        throw std::invalid_argument("side id must be 0..5");
+    return (SideType)s;
+}
+
+void applyBC(GridBuilder& b, int side, int type, double v0, double v1, double v2)
+{
+    switch (type) {
+    case 0: break;
+    case 1: b.setNoSlipBoundaryCondition(sideOf(side)); break;
+    case 2: b.setVelocityBoundaryCondition(sideOf(side), v0, v1, v2); break;
+    case 3: b.setPressureBoundaryCondition(sideOf(side), v0); break;
+    case 4: b.setSlipBoundaryCondition(sideOf(side), v0, v1, v2); break;
+    default: throw std::invalid_argument("unknown boundary-condition type");
+    }
+}
+
+void concatenate(const std::vector<BCList>& lists, Exported& E, const std::string& prefix, bool velocity, bool slip)
+{
+    std::vector<int32_t> k;
+    std::vector<double> vx, vy, vz, nx, ny, nz;
+    size_t n = 0;
+    for (const auto& l : lists)
+        n += l.size();
+    std::vector<double> q(27 * n, -1.0);
+    size_t at = 0;
+    for (const auto& l : lists) {
+        const size_t m = l.size();
+        for (size_t i = 0; i < m; ++i) {
+            k.push_back(l.k[i]);
+            if (velocity) {
+                vx.push_back(l.vx[i]);
+                vy.push_back(l.vy[i]);
+                vz.push_back(l.vz[i]);
+            }
+            if (slip) {
+                nx.push_back(l.normalX[i]);
+                ny.push_back(l.normalY[i]);
+                nz.push_back(l.normalZ[i]);
+            }
+            for (int d = 0; d < 27; ++d)
+                q[(size_t)d * n + at + i] = l.q[(size_t)d * m + i];
+        }
+        at += m;
+    }
+    E.put(prefix + ".k", k);
+    E.put(prefix + ".q", q);
+    if (velocity) {
+        E.put(prefix + ".vx", vx);
+        E.put(prefix + ".vy", vy);
+        E.put(prefix + ".vz", vz);
+    }
+    if (slip) {
+        E.put(prefix + ".nx", nx);
+        E.put(prefix + ".ny", ny);
+        E.put(prefix + ".nz", nz);
+    }
+}
+
+void exportAll(GridHandle& h)
+{
+    GridBuilder& b = h.builder;
+    h.levels.assign(b.numberOfLevels(), Exported());
+    for (int level = 0; level < b.numberOfLevels(); ++level) {
+        Exported& E = h.levels[level];
+        const LevelGrid& g = b.grid(level);
+        std::vector<double> cx, cy, cz;
+        std::vector<uint32_t> nbx, nby, nbz, nbn, geo;
+        g.nodeValues(cx, cy, cz, nbx, nby, nbz, nbn, geo);
+        E.put("coordX", cx);
+        E.put("coordY", cy);
+        E.put("coordZ", cz);
+        E.put("neighborX", nbx);
+        E.put("neighborY", nby);
+        E.put("neighborZ", nbz);
+        E.put("neighborNeg", nbn);
+        E.put("geo", geo);
+        E.put("dims", std::vector<int32_t> { (int32_t)g.nx, (int32_t)g.ny, (int32_t)g.nz });
+        E.put("fluid", g.fluidNodes);
+        concatenate(b.velocityBCs(level), E, "velocity", true, false);
+        concatenate(b.slipBCs(level), E, "slip", false, true);
+        E.put("geometry.k", std::vector<int32_t>());
+        E.put("geometry.q", std::vector<double>());
+        const auto& pres = b.pressureBCs(level);
+        E.put("pressure.count", std::vector<int32_t> { (int32_t)pres.size() });
+        for (size_t i = 0; i < pres.size(); ++i) {
+            const std::string p = "pressure" + std::to_string(i);
+            E.put(p + ".k", pres[i].k);
+            E.put(p + ".kN", pres[i].kN);
+            E.put(p + ".rho", pres[i].rho);
+            E.put(p + ".q", pres[i].q);
+            E.put(p + ".dir", std::vector<int32_t> { pres[i].d3q27Direction });
+        }
+    }
+}
+} // namespace
+
+extern "C" {
+
+/*
+ * spec: [0..6] coarse grid start x,y,z, end x,y,z, delta; [7..9] periodic;
+ * [10] refinement boxes (0 only in this build); [17..18] layers; [19] solid
+ * cuboid present (0 only); [30..59] six side BCs (side, type, v0, v1, v2) in
+ * the order they are set; [60] enableThinWalls.  Same layout as the grid
+ * oracle.  Returns NULL on error (see vfb_last_error).
+ */
+void* vfb_grid_build(const double* s, int n)
+{
+    vfb::clearError();
+    if (!s || n < 61) {
+        vfb::setError(VFB_ERR_INVALID_ARGUMENT, "grid spec needs 61 values");
+        return nullptr;
+    }
+    auto* h = new GridHandle;
+    try {
+        if (s[10] > 0 || s[19] > 0)
+            throw std::invalid_argument("refinement boxes and solid geometry are not supported by this call");
+        h->builder.addCoarseGrid(s[0], s[1], s[2], s[3], s[4], s[5], s[6]);
+        h->builder.setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);
+        h->builder.buildGrids(s[60] > 0);
+        for (int i = 0; i < 6; ++i) {
+            const double* b = s + 30 + 5 * i;
+            applyBC(h->builder, (int)b[0], (int)b[1], b[2], b[3], b[4]);
+        }
+        for (int level = 0; level < h->builder.numberOfLevels(); ++level)
+            h->builder.grid(level).findFluidNodes();
+        exportAll(*h);
+    } catch (const std::exception& e) {
+        vfb::setError(VFB_ERR_CONFIGURATION, "grid build failed: %s", e.what());
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+int vfb_grid_levels(void* h) { return h ? (int)static_cast<GridHandle*>(h)->levels.size() : 0; }
+
+long long vfb_grid_count(void* h, int level, const char* name)
+{
+    auto* H = static_cast<GridHandle*>(h);
+    if (!H || !name || level < 0 || level >= (int)H->levels.size())
+        return -1;
+    auto it = H->levels[level].data.find(name);
+    if (it == H->levels[level].data.end())
+        return -1;
+    return (long long)(it->second.size() / H->levels[level].elem[name]);
+}
+
+int vfb_grid_elem_size(void* h, int level, const char* name)
+{
+    auto* H = static_cast<GridHandle*>(h);
+    if (!H || !name || level < 0 || level >= (int)H->levels.size())
+        return -1;
+    auto it = H->levels[level].elem.find(name);
+    return it == H->levels[level].elem.end() ? -1 : it->second;
+}
+
+int vfb_grid_copy(void* h, int level, const char* name, void* out)
+{
+    auto* H = static_cast<GridHandle*>(h);
+    if (!H || !name || level < 0 || level >= (int)H->levels.size())
+        return VFB_ERR_INVALID_ARGUMENT;
+    auto it = H->levels[level].data.find(name);
+    if (it == H->levels[level].data.end())
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!it->second.empty()) {
+        if (!out)
+            return VFB_ERR_INVALID_ARGUMENT;
+        std::memcpy(out, it->second.data(), it->second.size());
+    }
+    return VFB_OK;
+}
+
+void vfb_grid_free(void* h) { delete static_cast<GridHandle*>(h); }
+
+} // extern "C"

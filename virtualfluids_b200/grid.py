@@ -1,0 +1,176 @@
+"""Grid construction API (mirrors VirtualFluids' MultipleGridBuilder /
+LevelGridBuilder, src/gpu/GridGenerator/grid/GridBuilder/).
+
+The grid is built by the native library (csrc/grid_builder.cpp) through the C
+ABI (vfb_grid_*).  The result is a list of levels, each a dict of numpy arrays
+in the GPU layout of VirtualFluids' LBMSimulationParameter:
+
+  neighborX/Y/Z, neighborNeg, geo   uint32, numberOfNodes (+1 dummy node 0)
+  coordX/Y/Z                        float64 node coordinates
+  fluid                             uint32 fluid-node list (+1 shifted)
+  velocity.k / .vx / .vy / .vz / .q compacted velocity BC list (q direction-major)
+  slip.k / .nx / .ny / .nz / .q     compacted slip BC list
+  pressure<i>.k / .kN / .rho / .q / .dir   one list per pressure side
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _lib
+
+
+class SideType(enum.IntEnum):
+    """grid/BoundaryConditions/Side.h:62-65"""
+
+    MX = 0
+    PX = 1
+    MY = 2
+    PY = 3
+    MZ = 4
+    PZ = 5
+    GEOMETRY = 6
+
+
+_BC_NONE, _BC_NOSLIP, _BC_VELOCITY, _BC_PRESSURE, _BC_SLIP = 0, 1, 2, 3, 4
+
+_REAL_NAMES_PREFIX = ("coord",)
+
+
+def _dtype(name: str, esize: int):
+    base = name.split(".")[-1]
+    if name in ("dims", "pressure.count") or base in ("k", "kN", "dir"):
+        return np.int32
+    if name in ("neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "fluid", "cf.coarse", "cf.fine",
+                "fc.coarse", "fc.fine"):
+        return np.uint32
+    return np.float64 if esize == 8 else np.float32
+
+
+GRID_ARRAY_NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims",
+                    "fluid", "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k",
+                    "slip.nx", "slip.ny", "slip.nz", "slip.q", "geometry.k", "geometry.q", "pressure.count",
+                    "cf.coarse", "cf.fine", "fc.coarse", "fc.fine", "cf.offX", "cf.offY", "cf.offZ", "fc.offX",
+                    "fc.offY", "fc.offZ"]
+
+
+class MultipleGridBuilder:
+    """Builder with the reference's call sequence: addCoarseGrid, (addGrid,
+    addGeometry), setPeriodicBoundaryCondition, buildGrids, then the side
+    boundary conditions."""
+
+    def __init__(self):
+        self.spec = np.zeros(64)
+        self._coarse = False
+        self._built = False
+        self._bcs: list[tuple[int, int, float, float, float]] = []
+
+    # --- grid ---------------------------------------------------------------
+    def addCoarseGrid(self, startX, startY, startZ, endX, endY, endZ, delta):
+        self.spec[0:7] = [startX, startY, startZ, endX, endY, endZ, delta]
+        self._coarse = True
+
+    def addGrid(self, box, level: int = 1):
+        """Refinement box (minX, minY, minZ, maxX, maxY, maxZ) on level 1."""
+        if level != 1:
+            raise ValueError("only one refinement level is supported")
+        self.spec[10] = 1
+        self.spec[11:17] = box
+
+    def setNumberOfLayers(self, fine: int, between: int):
+        self.spec[17:19] = [fine, between]
+
+    def addGeometry(self, cuboid):
+        """Solid cuboid (minX, minY, minZ, maxX, maxY, maxZ)."""
+        self.spec[19] = 1
+        self.spec[20:26] = cuboid
+
+    def setPeriodicBoundaryCondition(self, px: bool, py: bool, pz: bool):
+        self.spec[7:10] = [float(px), float(py), float(pz)]
+
+    def buildGrids(self, enableThinWalls: bool = False):
+        if not self._coarse:
+            raise RuntimeError("addCoarseGrid must be called first")
+        self.spec[60] = 1.0 if enableThinWalls else 0.0
+        self._built = True
+
+    # --- boundary conditions (LevelGridBuilder.cpp:81-266) --------------------
+    def _add(self, side, kind, v0=0.0, v1=0.0, v2=0.0):
+        if not self._built:
+            raise RuntimeError("buildGrids() has to be called before setting boundary conditions")
+        side = SideType(side)
+        if side == SideType.GEOMETRY:
+            self.spec[26:30] = [kind, v0, v1, v2]
+            return
+        if len(self._bcs) >= 6:
+            raise RuntimeError("at most six side boundary conditions")
+        self._bcs.append((int(side), kind, v0, v1, v2))
+
+    def setNoSlipBoundaryCondition(self, side):
+        self._add(side, _BC_NOSLIP)
+
+    def setVelocityBoundaryCondition(self, side, vx, vy, vz):
+        self._add(side, _BC_VELOCITY, vx, vy, vz)
+
+    def setPressureBoundaryCondition(self, side, rho):
+        self._add(side, _BC_PRESSURE, rho)
+
+    def setSlipBoundaryCondition(self, side, normalX, normalY, normalZ):
+        self._add(side, _BC_SLIP, normalX, normalY, normalZ)
+
+    # --- result ---------------------------------------------------------------
+    def full_spec(self) -> np.ndarray:
+        s = self.spec.copy()
+        for i, b in enumerate(self._bcs):
+            s[30 + 5 * i: 35 + 5 * i] = b
+        return s
+
+    def arrays(self) -> list[dict[str, np.ndarray]]:
+        """Run the native builder and return the arrays of every level."""
+        L = _lib.lib()
+        s = self.full_spec()
+        h = L.vfb_grid_build(s.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(s))
+        if not h:
+            raise _lib.VfbError(_lib.VFB_ERR_CONFIGURATION, _lib.last_error())
+        try:
+            return [export_level(L, h, lvl, "vfb_grid") for lvl in range(L.vfb_grid_levels(h))]
+        finally:
+            L.vfb_grid_free(h)
+
+
+def export_level(L, h, level: int, prefix: str) -> dict[str, np.ndarray]:
+    count = getattr(L, prefix + "_count")
+    esize = getattr(L, prefix + "_elem_size")
+    copy = getattr(L, prefix + "_copy")
+    names = list(GRID_ARRAY_NAMES)
+    if count(h, level, b"pressure.count") > 0:
+        tmp = np.zeros(1, np.int32)
+        copy(h, level, b"pressure.count", tmp.ctypes.data_as(ctypes.c_void_p))
+        for i in range(int(tmp[0])):
+            names += [f"pressure{i}.{s}" for s in ("k", "kN", "rho", "q", "dir")]
+    out: dict[str, np.ndarray] = {}
+    for name in names:
+        n = count(h, level, name.encode())
+        if n < 0:
+            continue
+        es = esize(h, level, name.encode())
+        a = np.zeros(n, _dtype(name, es))
+        if a.itemsize != es:
+            raise RuntimeError(f"element size mismatch for {name}")
+        copy(h, level, name.encode(), a.ctypes.data_as(ctypes.c_void_p))
+        out[name] = a
+    return out
+
+
+def taylor_green_grid(n: int) -> dict[str, np.ndarray]:
+    """Periodic cube of n^3 fluid nodes on [-pi, pi]^3 with spacing 2 pi / n,
+    built as apps/gpu/TaylorGreenVortex/TaylorGreenVortex.cpp:107-114 does."""
+    import math
+    b = MultipleGridBuilder()
+    d = 2.0 * math.pi / n
+    b.addCoarseGrid(-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d)
+    b.setPeriodicBoundaryCondition(True, True, True)
+    b.buildGrids(True)
+    return b.arrays()[0]
