@@ -1,0 +1,346 @@
+"""Benchmark of the LBM time step: D3Q27 K17 cumulant MLUPS on the periodic
+Taylor-Green vortex, and its fraction of the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 512]
+                    [--storage fp32|fp64|fp16|bf16] [--impl reference]
+
+One step is one fused collide + stream launch over all n^3 fluid nodes (the
+reference's K17CompressibleNavierStokes::runOnIndices on one level).  Inputs
+(14.7 GB of FP32 populations at n = 512) are far larger than the 126 MB L2,
+so no flush is needed between timed steps.  Multi-GPU runs are independent
+replicas (the single-GPU step has no halo exchange); value is the sum of all
+ranks' node updates over the slowest rank's time.
+
+Rank 0 prints one JSON line.  ``--impl reference`` times the reference's own
+CPU K17 path (oracle/_ref, OpenMP on all host cores) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "D3Q27 cumulant MLUPS & % HBM roofline; FP16-store vs FP32 at stated L2 err"
+STORAGE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def algorithmic_bytes_per_node(storage: str) -> int:
+    """27 population reads + 27 writes, plus the node's fluid-index entry and
+    its three neighbour-array entries (the four neighbour-of-neighbour
+    lookups are cache hits)."""
+    return 54 * STORAGE_BYTES[storage] + 16
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def init_distributed():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- #
+# reference arm: the reference's CPU K17 path on the host cores
+# --------------------------------------------------------------------------- #
+def cpu_reference_mlups(n_block: int, steps: int):
+    from oracle.pyoracle import Reference, ref_available
+    if not ref_available("f32"):
+        return None
+    R = Reference("f32")
+    sec, mlups = R.cpu_block_mlups(n_block, steps)
+    return {"value": mlups, "seconds": sec, "cores": os.cpu_count(), "block": n_block, "steps": steps}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import platform
+    n_block = 96
+    rows = []
+    for _ in range(args.warmup):
+        cpu_reference_mlups(n_block, 1)
+    for _ in range(args.steps):
+        r = cpu_reference_mlups(n_block, 2)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent)"}))
+            return 0
+        rows.append(r)
+    value = statistics.median([r["value"] for r in rows])
+    sample = (f"{n_block}^3 block of the reference CPU K17 loop (EsoSplit storage, FP32), 2 passes per step, "
+              f"OpenMP over x3 on {os.cpu_count()} threads ({platform.processor() or platform.machine()})")
+    line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median([r["seconds"] for r in rows]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"taylor-green {args.n}^3 K17 (sampled on a {n_block}^3 block)",
+                       "storage": "fp32"},
+            "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline(seconds_target: float = 12.0):
+    """The reference CPU K17 path timed on the host cores for about
+    `seconds_target` seconds (rank 0, one GPU only)."""
+    try:
+        first = cpu_reference_mlups(96, 1)
+    except Exception as e:  # the baseline must not sink the GPU result
+        return {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {e}"}
+    if first is None:
+        return {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "oracle/_ref not built"}
+    steps = int(max(1, min(200, seconds_target / max(first["seconds"], 1e-3))))
+    r = cpu_reference_mlups(96, steps)
+    return {"value": r["value"], "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"reference CPU K17 loop (EsoSplit, FP32) on a 96^3 block, {steps} passes, "
+                      f"{r['seconds']:.1f} s, OpenMP on {os.cpu_count()} threads"}
+
+
+def run_gpu(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200 import kernels as K
+    from virtualfluids_b200.workloads import taylor_green
+
+    dtype = {"fp32": torch.float32, "fp64": torch.float64, "fp16": torch.float16, "bf16": torch.bfloat16}[
+        args.storage]
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    t_setup = time.time()
+    w = taylor_green(args.n)
+    g = w.grid
+    lat = K.DeviceLattice.from_arrays(g, device)
+    n_fluid = lat.numberOfFluidNodes
+    cd = K.compute_dtype(dtype)
+    # host copies of the initial fields in pinned memory (the user's input)
+    host_fields = [torch.from_numpy(a.astype(np.float64 if cd == torch.float64 else np.float32)).pin_memory()
+                   for a in (w.rho, w.vx, w.vy, w.vz)]
+    del w
+    dist = K.new_distributions(lat, dtype, device)
+    dev_fields = [h.to(device, non_blocking=True) for h in host_fields]
+    stream = torch.cuda.current_stream(device)
+    for ev in (False, True):
+        K.init_equilibrium(dist, lat, *dev_fields, ev)
+    del dev_fields
+    torch.cuda.synchronize(device)
+    setup_s = time.time() - t_setup
+
+    omega = 1.0 / (3.0 * (args.u0 * (args.n / (2 * math.pi)) / 1600.0) + 0.5)
+    even = True
+    for _ in range(args.warmup):
+        K.collision("K17", dist, lat, omega, even, stream=stream)
+        even = not even
+    torch.cuda.synchronize(device)
+
+    # --- device-resident timing (value) ---------------------------------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            K.collision("K17", dist, lat, omega, even, stream=stream)
+            stops[i].record(stream)
+            even = not even
+        t1.record(stream)
+        torch.cuda.synchronize(device)
+    barrier(world)
+    total_ms = max_over_ranks(world, t0.elapsed_time(t1))
+    launch_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    avg_launch_ms = sum(launch_ms) / len(launch_ms)
+    clk = clocks.summary()
+
+    # --- end to end through the public API with host buffers -------------------
+    # the whole job per call: pinned H2D of the initial fields, initialisation
+    # of both parities, K steps, D2H of the resulting fields; per-step bytes
+    # are the totals divided by K
+    out_host = [torch.empty(lat.N, dtype=cd).pin_memory() for _ in range(4)]
+    barrier(world)
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dev_fields = [h.to(device, non_blocking=True) for h in host_fields]
+    for ev in (False, True):
+        K.init_equilibrium(dist, lat, *dev_fields, ev, stream=stream)
+    even = True
+    for _ in range(args.steps):
+        K.collision("K17", dist, lat, omega, even, stream=stream)
+        even = not even
+    res = K.macroscopic(dist, lat, even, stream=stream)
+    for h, d in zip(out_host, res):
+        h.copy_(d, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    h2d = sum(h.numel() * h.element_size() for h in host_fields)
+    d2h = sum(h.numel() * h.element_size() for h in out_host)
+    finite = bool(np.isfinite(out_host[1].numpy()[g["fluid"][:1000]]).all())
+    del dev_fields, res
+
+    if rank != 0:
+        return 0
+    updates = n_fluid * args.steps * world
+    value = updates / (total_ms * 1e-3) / 1e6
+    e2e_value = updates / (e2e_ms * 1e-3) / 1e6
+    bpn = algorithmic_bytes_per_node(args.storage)
+    achieved = bpn * n_fluid / (avg_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    traffic = None
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get(f"k17_{args.storage}_{args.n}")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f16-store/f32", "bf16": "bf16-store/f32"}[
+            args.storage],
+        "data": "synthetic",
+        "config": {"workload": f"taylor-green {args.n}^3 periodic, K17 cumulant, {args.storage} storage",
+                   "fluid_nodes_per_gpu": n_fluid, "stored_nodes_per_gpu": lat.N, "omega": omega,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)",
+                   "setup_s": round(setup_s, 1), "finite": finite},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "bytes_per_node": bpn, "peak_kind": f"of {peak_kind}",
+                     "avg_launch_ms": avg_launch_ms},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": args.steps,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--u0", type=float, default=0.05)
+    ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE_BYTES))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world, rank, local = init_distributed()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

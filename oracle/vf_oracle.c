@@ -818,3 +818,36 @@ void FN(vfo_macroscopic)(const real *dist, uint64_t N, const uint32_t *geo, cons
         vz[k] = pyramid_jz(f) * oneOverRho;
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* exported primitives for the known-answer tests of the reference's unit     */
+/* tests (tests/unit-tests/lbm/ChimeraTests.cpp, MacroscopicQuantitiesTests.cpp, */
+/* tests/unit-tests/gpu/core/Utilities/KernelUtilitiesTests.cpp)            */
+/* ------------------------------------------------------------------------ */
+void FN(vfo_chimera)(int which, real *abc, real vv, real v2, real kinv, real k)
+{
+    switch (which) {
+    case 0: fwd_k(&abc[0], &abc[1], &abc[2], vv, v2, kinv, k); break;
+    case 1: bwd_k(&abc[0], &abc[1], &abc[2], vv, v2, kinv, k); break;
+    case 2: fwd_0(&abc[0], &abc[1], &abc[2], vv, v2); break;
+    default: bwd_0(&abc[0], &abc[1], &abc[2], vv, v2); break;
+    }
+}
+
+/* out: density, jx, jy, jz (incompressible sums), then the compressible
+ * drho, vx, vy, vz of getCompressibleMacroscopicValues */
+void FN(vfo_macros)(const real *f, real *out)
+{
+    out[0] = pyramid_density(f);
+    out[1] = pyramid_jx(f);
+    out[2] = pyramid_jy(f);
+    out[3] = pyramid_jz(f);
+    const real oneOverRho = (real)1 / (out[0] + (real)1);
+    out[4] = out[0];
+    out[5] = out[1] * oneOverRho;
+    out[6] = out[2] * oneOverRho;
+    out[7] = out[3] * oneOverRho;
+}
+
+/* array slot read for direction d in the given parity view */
+int FN(vfo_slot)(int d, int isEven) { return slot_of(d, isEven); }

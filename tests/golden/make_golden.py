@@ -1,0 +1,69 @@
+"""Generate the golden fixtures of tests/golden from the reference itself.
+
+Runs the reference's own sources compiled on the host (oracle/_ref, built by
+``make -C oracle ref`` from the reference tree) and stores small inputs and
+outputs as .npz files.  The parity tests compare the oracle and the
+repository's grid builder against these files, so the pin also holds on a
+machine without the reference tree.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle.pyoracle import Reference  # noqa: E402
+from tests.golden.scenarios import GRID_SCENARIOS, grid_spec, lattice_sequence  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def k17_nodes(precision: str) -> None:
+    R = Reference(precision)
+    rng = np.random.default_rng(20241203)
+    n = 64
+    fin = rng.uniform(-0.02, 0.02, (n, 27))
+    omega = rng.uniform(0.5, 1.99, n)
+    lim = np.where(rng.uniform(size=(n, 1)) < 0.5, 0.01, 1e6) * np.ones((n, 3))
+    lim[::7] = [0.02, 0.005, 0.1]
+    force = rng.uniform(-1e-4, 1e-4, (n, 3))
+    fout = np.zeros_like(fin)
+    macro = np.zeros((n, 4))
+    for i in range(n):
+        f, m = R.k17_node(fin[i], omega[i], tuple(lim[i]), tuple(force[i]))
+        fout[i], macro[i] = f, m
+    real = np.float64 if precision == "f64" else np.float32
+    np.savez_compressed(OUT / f"k17_nodes_{precision}.npz", fin=fin.astype(real), omega=omega.astype(real),
+                        lim=lim.astype(real), force=force.astype(real), fout=fout.astype(real),
+                        macro=macro.astype(real))
+
+
+def grids() -> None:
+    R = Reference("f64")
+    for name in GRID_SCENARIOS:
+        levels = R.grid(grid_spec(name))
+        arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
+        np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
+
+
+def lattice(precision: str) -> None:
+    R = Reference(precision)
+    levels = R.grid(grid_spec("channel"))
+    dist = lattice_sequence(R, levels[0], precision)
+    np.savez_compressed(OUT / f"lattice_channel_{precision}.npz", dist=dist)
+
+
+if __name__ == "__main__":
+    for p in ("f64", "f32"):
+        k17_nodes(p)
+        lattice(p)
+    grids()
+    for f in sorted(OUT.glob("*.npz")):
+        print(f.name, f.stat().st_size)

@@ -1,0 +1,77 @@
+"""Shared definitions of the golden scenarios (grid specs and the lattice
+update sequence), used both to generate the fixtures from the reference and
+to replay them in the tests."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+MX, PX, MY, PY, MZ, PZ = range(6)
+NONE, NOSLIP, VELOCITY, PRESSURE, SLIP = range(5)
+
+
+def _spec(coarse, periodic=(0, 0, 0), sides=(), thin_walls=False):
+    s = np.zeros(64)
+    s[0:7] = coarse
+    s[7:10] = periodic
+    for i, b in enumerate(sides):
+        s[30 + 5 * i: 35 + 5 * i] = b
+    s[60] = 1.0 if thin_walls else 0.0
+    return s
+
+
+def grid_spec(name: str) -> np.ndarray:
+    if name.startswith("tgv"):
+        n = int(name[3:])
+        d = 2 * math.pi / n
+        return _spec([-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d], (1, 1, 1), thin_walls=True)
+    if name == "cavity8":
+        sides = [(s, NOSLIP, 0, 0, 0) for s in (MX, PX, MY, PY, MZ)] + [(PZ, VELOCITY, 0.05, 0, 0)]
+        return _spec([0, 0, 0, 7, 7, 7, 1.0], sides=sides)
+    if name == "cavity8_lidfirst":
+        sides = [(PZ, VELOCITY, 0.05, 0, 0)] + [(s, NOSLIP, 0, 0, 0) for s in (MX, PX, MY, PY, MZ)]
+        return _spec([0, 0, 0, 7, 7, 7, 1.0], sides=sides)
+    if name == "channel":
+        sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        return _spec([0, 0, 0, 11, 7, 7, 1.0], (0, 1, 0), sides=sides)
+    raise KeyError(name)
+
+
+GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel"]
+
+
+def lattice_sequence(impl, g: dict, precision: str, steps: int = 4) -> np.ndarray:
+    """Init both parities, then per step: K17 with a force, the five
+    post-collision BC kernels, the pressure BC, and a BGK pass of the other
+    parity.  ``impl`` is the oracle or the reference binding."""
+    real = np.float64 if precision == "f64" else np.float32
+    N = len(g["geo"])
+    nx, ny, nz, geo, fl = g["neighborX"], g["neighborY"], g["neighborZ"], g["geo"], g["fluid"]
+    rng = np.random.default_rng(7)
+    rho = rng.uniform(-1e-3, 1e-3, N).astype(real)
+    ux = (0.04 + rng.uniform(-1e-3, 1e-3, N)).astype(real)
+    uy = rng.uniform(-1e-3, 1e-3, N).astype(real)
+    uz = rng.uniform(-1e-3, 1e-3, N).astype(real)
+    d = np.zeros(27 * N, real)
+    for ev in (0, 1):
+        impl.init_eq(d, N, geo, nx, ny, nz, rho, ux, uy, uz, ev)
+    vk = g["velocity.k"]
+    vq = g["velocity.q"].astype(real)
+    vvx, vvy, vvz = (g["velocity.vx"].astype(real), g["velocity.vy"].astype(real), g["velocity.vz"].astype(real))
+    sk, sq = g["slip.k"], g["slip.q"].astype(real)
+    pk, pkn = g["pressure0.k"], g["pressure0.kN"]
+    prho, pdir = g["pressure0.rho"].astype(real), int(g["pressure0.dir"][0])
+    even, om = True, 1.8
+    for _ in range(steps):
+        impl.collision_k17(d, N, nx, ny, nz, fl, om, forces=(1e-5, 0, 0), force_factor=1.0,
+                           limiters=(0.01, 0.01, 0.01), is_even=even)
+        impl.bc_post(2, d, N, nx, ny, nz, vk, vq, om, vvx, vvy, vvz, is_even=even)
+        impl.bc_post(0, d, N, nx, ny, nz, vk, vq, om, is_even=even)
+        impl.bc_post(4, d, N, nx, ny, nz, sk, sq, om, is_even=even)
+        impl.bc_post(1, d, N, nx, ny, nz, vk, vq, om, is_even=even)
+        impl.bc_post(3, d, N, nx, ny, nz, vk, vq, om, vvx, vvy, vvz, is_even=even)
+        impl.bc_pressure(d, N, nx, ny, nz, pk, pkn, prho, pdir, is_even=not even)
+        impl.collision_bgk(d, N, geo, nx, ny, nz, om, is_even=not even)
+        even = not even
+    return d

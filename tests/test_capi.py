@@ -1,0 +1,87 @@
+"""The C ABI library loads, exports every entry point include/vf_b200.h
+declares, and rejects invalid arguments without touching a GPU."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from virtualfluids_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "vf_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vfb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    assert "vfb_k17_collision" in declared_symbols()
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (vfb_[a-z0-9_]+)", out))
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    assert set(declared_symbols()) <= set(_lib.exported_symbols())
+
+
+def test_version_and_storage_sizes():
+    L = _lib.lib()
+    assert L.vfb_version() >= 100
+    assert [L.vfb_storage_bytes(s) for s in (0, 1, 2, 3, 9)] == [4, 8, 2, 2, 0]
+
+
+def test_null_args_rejected():
+    L = _lib.lib()
+    assert L.vfb_k17_collision(0, None, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert "NULL" in _lib.last_error()
+
+
+def test_invalid_omega_rejected():
+    a = _lib.CollisionArgs()
+    a.distributions = 1
+    a.neighborX = a.neighborY = a.neighborZ = a.fluidNodeIndices = 1
+    a.numberOfLBnodes = 10
+    a.numberOfFluidNodes = 5
+    a.omega = 2.5
+    rc = _lib.lib().vfb_k17_collision(0, ctypes.byref(a), None)
+    assert rc == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert "omega" in _lib.last_error()
+
+
+def test_unknown_storage_rejected():
+    a = _lib.CollisionArgs()
+    rc = _lib.lib().vfb_k17_collision(7, ctypes.byref(a), None)
+    assert rc == _lib.VFB_ERR_INVALID_ARGUMENT
+
+
+def test_template_needs_macro_arrays():
+    a = _lib.CollisionArgs()
+    a.distributions = 1
+    a.neighborX = a.neighborY = a.neighborZ = a.fluidNodeIndices = 1
+    a.numberOfLBnodes = 10
+    a.numberOfFluidNodes = 5
+    a.omega = 1.5
+    a.collisionTemplate = _lib.TEMPLATE_WRITE_MACRO_VARS
+    assert _lib.lib().vfb_k17_collision(0, ctypes.byref(a), None) == _lib.VFB_ERR_INVALID_ARGUMENT
+
+
+def test_empty_fluid_list_is_a_no_op():
+    a = _lib.CollisionArgs()
+    a.numberOfFluidNodes = 0
+    assert _lib.lib().vfb_k17_collision(0, ctypes.byref(a), None) == _lib.VFB_OK
+
+
+def test_grid_build_rejects_short_spec():
+    s = (ctypes.c_double * 10)()
+    assert not _lib.lib().vfb_grid_build(s, 10)
+    assert "61" in _lib.last_error()

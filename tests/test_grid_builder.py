@@ -1,0 +1,88 @@
+"""The grid builder (csrc/grid_builder.cpp, through the C ABI) against the
+reference's GridGenerator: neighbour arrays, geo, fluid-node list and the
+compacted BC lists must be identical element for element.  Golden fixtures
+always; the live reference build when present (more sizes and orders)."""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Reference, ref_available
+from tests.golden.scenarios import GRID_SCENARIOS, grid_spec
+from virtualfluids_b200 import grid as vgrid
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def build_mine(spec):
+    b = vgrid.MultipleGridBuilder()
+    b.spec[:] = 0
+    b.spec[:len(spec)] = spec
+    b._coarse = True
+    b._built = True
+    return b.arrays()
+
+
+def compare(mine, ref):
+    assert len(mine) == len(ref)
+    for lvl in range(len(ref)):
+        for name, v in ref[lvl].items():
+            if name.startswith("coord"):
+                np.testing.assert_allclose(mine[lvl][name], v, rtol=0, atol=1e-9 * max(1.0, np.abs(v).max()))
+                continue
+            m = mine[lvl].get(name)
+            if m is None:
+                assert len(v) == 0, name
+                continue
+            assert m.shape == v.shape, name
+            assert np.array_equal(m.astype(v.dtype) if m.dtype != v.dtype else m, v), name
+
+
+@pytest.mark.parametrize("name", GRID_SCENARIOS)
+def test_grid_matches_golden(name):
+    z = np.load(GOLDEN / f"grid_{name}.npz")
+    levels = sorted({int(k.split(":")[0][1:]) for k in z.files})
+    ref = [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith(f"L{lvl}:")} for lvl in levels]
+    compare(build_mine(grid_spec(name)), ref)
+
+
+def test_taylor_green_layout():
+    g = vgrid.taylor_green_grid(8)
+    assert list(g["dims"]) == [10, 10, 10]
+    assert len(g["geo"]) == 10 ** 3 + 1
+    assert len(g["fluid"]) == 8 ** 3
+    # periodic: the last fluid node of a row wraps to the first
+    nx = g["neighborX"]
+    first = g["fluid"][0]
+    assert nx[first + 7] == first
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("n", [3, 5, 12, 16])
+def test_periodic_cube_matches_reference(n):
+    spec = np.zeros(64)
+    d = 2 * math.pi / n
+    spec[0:7] = [-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d]
+    spec[7:10] = 1
+    spec[60] = 1
+    compare(build_mine(spec), Reference("f64").grid(spec))
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("order", [[0, 1, 2, 3, 4, 5], [5, 4, 3, 2, 1, 0], [2, 5, 0, 4, 1, 3]])
+@pytest.mark.parametrize("periodic", [(0, 0, 0), (1, 0, 0), (0, 1, 1)])
+def test_box_sides_match_reference(order, periodic):
+    spec = np.zeros(64)
+    spec[0:7] = [0, 0, 0, 9, 6, 7, 1.0]
+    spec[7:10] = periodic
+    kinds = {0: (2, 0.04, 0, 0), 1: (3, 0.0, 0, 0), 2: (1, 0, 0, 0), 3: (4, 0, 1, 0), 4: (1, 0, 0, 0),
+             5: (2, 0.05, 0.01, 0)}
+    i = 0
+    for side in order:
+        axis = side // 2
+        if periodic[axis]:
+            continue
+        spec[30 + 5 * i: 35 + 5 * i] = (side, *kinds[side])
+        i += 1
+    compare(build_mine(spec), Reference("f64").grid(spec))

@@ -1,0 +1,62 @@
+"""The oracle pinned to the reference.
+
+Against the committed golden fixtures (tests/golden, generated by
+tests/golden/make_golden.py from the reference's own sources) always, and
+against the live reference build (oracle/_ref) when it is present.  The bar
+is bit-exact equality: the oracle performs the reference's operations in the
+reference's order.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle, Reference, ref_available
+from tests.golden.scenarios import grid_spec, lattice_sequence
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_k17_node_matches_golden(precision):
+    g = np.load(GOLDEN / f"k17_nodes_{precision}.npz")
+    O = Oracle(precision)
+    for i in range(len(g["omega"])):
+        f, m = O.k17_node(g["fin"][i], g["omega"][i], tuple(g["lim"][i]), tuple(g["force"][i]))
+        assert np.array_equal(f, g["fout"][i]), i
+        assert np.array_equal(m, g["macro"][i]), i
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_lattice_sequence_matches_golden(precision):
+    from virtualfluids_b200.grid import MultipleGridBuilder  # noqa: F401  (builder checked separately)
+    grid = dict(np.load(GOLDEN / "grid_channel.npz"))
+    g = {k.split(":", 1)[1]: v for k, v in grid.items() if k.startswith("L0:")}
+    d = lattice_sequence(Oracle(precision), g, precision)
+    ref = np.load(GOLDEN / f"lattice_channel_{precision}.npz")["dist"]
+    assert np.array_equal(d, ref)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_k17_node_matches_live_reference(precision):
+    O, R = Oracle(precision), Reference(precision)
+    rng = np.random.default_rng(99)
+    for t in range(100):
+        f = rng.uniform(-0.03, 0.03, 27)
+        om = rng.uniform(0.2, 1.999)
+        lim = (0.01, 0.01, 0.01) if t % 3 else (1e6, 1e6, 1e6)
+        force = tuple(rng.uniform(-1e-4, 1e-4, 3))
+        a, ma = O.k17_node(f, om, lim, force)
+        b, mb = R.k17_node(f, om, lim, force)
+        assert np.array_equal(a, b) and np.array_equal(ma, mb)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_lattice_sequence_matches_live_reference(precision):
+    R = Reference(precision)
+    g = R.grid(grid_spec("channel"))[0]
+    a = lattice_sequence(Oracle(precision), g, precision, steps=6)
+    b = lattice_sequence(R, g, precision, steps=6)
+    assert np.array_equal(a, b)

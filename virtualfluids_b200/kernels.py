@@ -1,0 +1,126 @@
+"""Thin Python access to the kernel entry points of the C ABI, on torch CUDA
+tensors (torch provides device memory and the stream; the arithmetic is in
+libvfb200.so).
+
+This is the level of VirtualFluids' kernel launchers: one call is one launch of
+a collision, init or macroscopic kernel on one level.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the environment
+    torch = None
+
+STORAGE_OF_DTYPE = {}
+if torch is not None:
+    STORAGE_OF_DTYPE = {torch.float32: _lib.FP32, torch.float64: _lib.FP64, torch.float16: _lib.FP16,
+                        torch.bfloat16: _lib.BF16}
+
+
+def compute_dtype(storage_dtype):
+    return torch.float64 if storage_dtype == torch.float64 else torch.float32
+
+
+def _p(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+@dataclass
+class DeviceLattice:
+    """Index arrays of one grid level on the device (LBMSimulationParameter fields)."""
+
+    N: int
+    neighborX: "torch.Tensor"
+    neighborY: "torch.Tensor"
+    neighborZ: "torch.Tensor"
+    geo: "torch.Tensor"
+    fluid: "torch.Tensor"
+
+    @staticmethod
+    def from_arrays(g: dict[str, np.ndarray], device="cuda") -> "DeviceLattice":
+        def u32(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(device)
+        return DeviceLattice(len(g["geo"]), u32(g["neighborX"]), u32(g["neighborY"]), u32(g["neighborZ"]),
+                             u32(g["geo"]), u32(g["fluid"]))
+
+    @property
+    def numberOfFluidNodes(self) -> int:
+        return int(self.fluid.numel())
+
+
+def new_distributions(lat: DeviceLattice, dtype, device="cuda"):
+    return torch.zeros(27 * lat.N, dtype=dtype, device=device)
+
+
+def collision(kernel: str, dist, lat: DeviceLattice, omega: float, is_even: bool, *, forces=(0.0, 0.0, 0.0),
+              force_factor: float = 1.0, limiters=(0.01, 0.01, 0.01), template: int = 0, macro=None, body=None,
+              fluid=None, stream=None) -> None:
+    """One fused collide + stream pass (``kernel`` is "K17" or "BGK")."""
+    storage = STORAGE_OF_DTYPE[dist.dtype]
+    nodes = lat.fluid if fluid is None else fluid
+    a = _lib.CollisionArgs()
+    a.distributions = dist.data_ptr()
+    a.numberOfLBnodes = lat.N
+    a.neighborX = lat.neighborX.data_ptr()
+    a.neighborY = lat.neighborY.data_ptr()
+    a.neighborZ = lat.neighborZ.data_ptr()
+    a.fluidNodeIndices = nodes.data_ptr()
+    a.numberOfFluidNodes = int(nodes.numel())
+    a.omega = float(omega)
+    a.forces[:] = [float(x) for x in forces]
+    a.forceFactor = float(force_factor)
+    a.quadricLimiters[:] = [float(x) for x in limiters]
+    a.isEvenTimestep = int(bool(is_even))
+    a.collisionTemplate = int(template)
+    if macro is not None:
+        a.rho, a.vx, a.vy, a.vz = [_p(t) for t in macro]
+    if body is not None:
+        a.bodyForceX, a.bodyForceY, a.bodyForceZ = [_p(t) for t in body]
+    L = _lib.lib()
+    fn = L.vfb_k17_collision if kernel.upper() == "K17" else L.vfb_bgk_collision
+    _lib.check(fn(storage, ctypes.byref(a), _stream(stream)))
+
+
+def init_equilibrium(dist, lat: DeviceLattice, rho, vx, vy, vz, is_even: bool, stream=None) -> None:
+    storage = STORAGE_OF_DTYPE[dist.dtype]
+    _lib.check(_lib.lib().vfb_init_equilibrium(storage, dist.data_ptr(), lat.N, lat.geo.data_ptr(),
+                                               lat.neighborX.data_ptr(), lat.neighborY.data_ptr(),
+                                               lat.neighborZ.data_ptr(), rho.data_ptr(), vx.data_ptr(),
+                                               vy.data_ptr(), vz.data_ptr(), int(bool(is_even)), _stream(stream)))
+
+
+def macroscopic(dist, lat: DeviceLattice, is_even: bool, stream=None):
+    """(drho, vx, vy, vz) of every node from the populations of one parity."""
+    storage = STORAGE_OF_DTYPE[dist.dtype]
+    cd = compute_dtype(dist.dtype)
+    out = [torch.empty(lat.N, dtype=cd, device=dist.device) for _ in range(4)]
+    _lib.check(_lib.lib().vfb_macroscopic(storage, dist.data_ptr(), lat.N, lat.geo.data_ptr(),
+                                          lat.neighborX.data_ptr(), lat.neighborY.data_ptr(),
+                                          lat.neighborZ.data_ptr(), int(bool(is_even)), *[o.data_ptr() for o in out],
+                                          _stream(stream)))
+    return out
+
+
+def mass_and_energy(dist, lat: DeviceLattice, is_even: bool, nodes=None, stream=None) -> tuple[float, float, int]:
+    """FP64 sums over a node list: total drho, kinetic energy, non-finite count."""
+    storage = STORAGE_OF_DTYPE[dist.dtype]
+    idx = lat.fluid if nodes is None else nodes
+    out = (ctypes.c_double * 3)()
+    _lib.check(_lib.lib().vfb_mass_and_energy(storage, dist.data_ptr(), lat.N, lat.neighborX.data_ptr(),
+                                              lat.neighborY.data_ptr(), lat.neighborZ.data_ptr(), idx.data_ptr(),
+                                              int(idx.numel()), int(bool(is_even)), out, _stream(stream)))
+    return out[0], out[1], int(out[2])

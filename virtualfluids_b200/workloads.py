@@ -1,0 +1,58 @@
+"""Synthetic workloads of the benchmark and parity tests.
+
+No dataset is involved; every input is generated from seeded formulas.
+
+Taylor-Green vortex (periodic cube of n^3 fluid nodes on [-pi, pi]^3, the
+set-up of apps/gpu/TaylorGreenVortex/TaylorGreenVortex.cpp:107-148):
+    u  = u0 (sin x cos y cos z, -cos x sin y cos z, 0)
+    drho = 3 (u0^2 / 16) (cos 2x + cos 2y) (cos 2z + 2)
+with u0 = 0.05, uniform noise of +-1e-3 u0 on each velocity component
+(seeded), viscosity for Re = 1600 on the length n / (2 pi).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .grid import taylor_green_grid
+
+
+@dataclass
+class TaylorGreen:
+    n: int
+    u0: float
+    nu: float
+    omega: float
+    grid: dict
+    rho: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+
+
+def taylor_green_viscosity(n: int, u0: float = 0.05, reynolds: float = 1600.0) -> float:
+    return u0 * (n / (2.0 * math.pi)) / reynolds
+
+
+def taylor_green(n: int, u0: float = 0.05, reynolds: float = 1600.0, noise: float = 1e-3,
+                 seed: int = 1234) -> TaylorGreen:
+    g = taylor_green_grid(n)
+    x, y, z = g["coordX"], g["coordY"], g["coordZ"]
+    rho = 3.0 * ((u0 * u0) / 16.0 * (np.cos(2.0 * x) + np.cos(2.0 * y)) * (np.cos(2.0 * z) + 2.0))
+    vx = u0 * np.sin(x) * np.cos(y) * np.cos(z)
+    vy = -u0 * np.cos(x) * np.sin(y) * np.cos(z)
+    vz = np.zeros_like(x)
+    if noise > 0:
+        rng = np.random.default_rng(seed)
+        amp = noise * u0
+        vx = vx + rng.uniform(-amp, amp, x.shape)
+        vy = vy + rng.uniform(-amp, amp, x.shape)
+        vz = vz + rng.uniform(-amp, amp, x.shape)
+    solid = g["geo"] != 19
+    for a in (rho, vx, vy, vz):
+        a[solid] = 0.0
+    nu = taylor_green_viscosity(n, u0, reynolds)
+    omega = 1.0 / (3.0 * nu + 0.5)
+    return TaylorGreen(n, u0, nu, omega, g, rho, vx, vy, vz)
