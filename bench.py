@@ -68,7 +68,7 @@ class ClockSampler:
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -184,7 +184,7 @@ def cpu_baseline(seconds_target: float = 12.0):
     if first is None:
         return {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
                 "sample": "oracle/_ref not built"}
-    steps = int(max(1, min(200, seconds_target / max(first["seconds"], 1e-3))))
+    steps = int(max(1, min(5000, seconds_target / max(first["seconds"], 1e-3))))
     r = cpu_reference_mlups(96, steps)
     return {"value": r["value"], "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
             "sample": f"reference CPU K17 loop (EsoSplit, FP32) on a 96^3 block, {steps} passes, "
@@ -222,9 +222,26 @@ def run_gpu(args, world, rank, local):
     setup_s = time.time() - t_setup
 
     omega = 1.0 / (3.0 * (args.u0 * (args.n / (2 * math.pi)) / 1600.0) + 0.5)
+    plan = K.CollisionPlan(dtype, lat, stream=stream) if args.path == "planned" else None
+    plan_stats = plan.stats() if plan is not None else None
     even = True
+    # the generic (index-chain) kernel, for comparison only
+    generic_ms = None
+    if plan is not None:
+        for _ in range(2):
+            K.collision("K17", dist, lat, omega, even, stream=stream)
+            even = not even
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(4):
+            K.collision("K17", dist, lat, omega, even, stream=stream)
+            even = not even
+        g1.record(stream)
+        torch.cuda.synchronize(device)
+        generic_ms = g0.elapsed_time(g1) / 4
     for _ in range(args.warmup):
-        K.collision("K17", dist, lat, omega, even, stream=stream)
+        K.collision("K17", dist, lat, omega, even, stream=stream, plan=plan)
         even = not even
     torch.cuda.synchronize(device)
 
@@ -239,7 +256,7 @@ def run_gpu(args, world, rank, local):
         t0.record(stream)
         for i in range(args.steps):
             starts[i].record(stream)
-            K.collision("K17", dist, lat, omega, even, stream=stream)
+            K.collision("K17", dist, lat, omega, even, stream=stream, plan=plan)
             stops[i].record(stream)
             even = not even
         t1.record(stream)
@@ -265,7 +282,7 @@ def run_gpu(args, world, rank, local):
         K.init_equilibrium(dist, lat, *dev_fields, ev, stream=stream)
     even = True
     for _ in range(args.steps):
-        K.collision("K17", dist, lat, omega, even, stream=stream)
+        K.collision("K17", dist, lat, omega, even, stream=stream, plan=plan)
         even = not even
     res = K.macroscopic(dist, lat, even, stream=stream)
     for h, d in zip(out_host, res):
@@ -277,6 +294,8 @@ def run_gpu(args, world, rank, local):
     h2d = sum(h.numel() * h.element_size() for h in host_fields)
     d2h = sum(h.numel() * h.element_size() for h in out_host)
     finite = bool(np.isfinite(out_host[1].numpy()[g["fluid"][:1000]]).all())
+    if plan is not None:
+        plan.check(stream)
     del dev_fields, res
 
     if rank != 0:
@@ -303,7 +322,8 @@ def run_gpu(args, world, rank, local):
         "config": {"workload": f"taylor-green {args.n}^3 periodic, K17 cumulant, {args.storage} storage",
                    "fluid_nodes_per_gpu": n_fluid, "stored_nodes_per_gpu": lat.N, "omega": omega,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)",
-                   "setup_s": round(setup_s, 1), "finite": finite},
+                   "setup_s": round(setup_s, 1), "finite": finite, "path": args.path, "plan": plan_stats,
+                   "generic_kernel_mlups": (n_fluid / (generic_ms * 1e-3) / 1e6) if generic_ms else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "bytes_per_node": bpn, "peak_kind": f"of {peak_kind}",
                      "avg_launch_ms": avg_launch_ms},
@@ -321,11 +341,12 @@ def run_gpu(args, world, rank, local):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--u0", type=float, default=0.05)
     ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE_BYTES))
+    ap.add_argument("--path", default="planned", choices=["planned", "generic"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)

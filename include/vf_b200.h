@@ -111,6 +111,30 @@ int vfb_k17_collision(int storage, const vfb_collision_args* args, void* stream)
 int vfb_bgk_collision(int storage, const vfb_collision_args* args, void* stream);
 
 /*
+ * Collision plan: a one-off analysis of a level's fluid-node list and
+ * neighbour arrays that lets the planned kernels fetch runs of regular nodes
+ * with bulk copies (cp.async.bulk) one warp tile ahead and skip the index
+ * chain for them (virtualfluids_b200/csrc/collision_tiled.cu).  Building a
+ * plan copies the index arrays to the host once.  The planned kernels compute
+ * exactly what vfb_k17_collision / vfb_bgk_collision compute; they require a
+ * 16-byte aligned distributions array and the same index arrays (pointers,
+ * sizes) the plan was built for.  No counterpart in the reference, whose
+ * kernels always follow the index chain (KernelUtilities.h:221-245).
+ */
+typedef struct vfb_collision_plan vfb_collision_plan;
+int vfb_collision_plan_create(int storage, const vfb_collision_args* args, vfb_collision_plan** plan, void* stream);
+int vfb_collision_plan_destroy(vfb_collision_plan* plan);
+/* out6: tiles, bulk tiles, lane-by-lane tiles, bulk-fed nodes, exception
+ * nodes inside bulk tiles, nodes in lane-by-lane tiles */
+int vfb_collision_plan_stats(const vfb_collision_plan* plan, unsigned long long* out6);
+/* VFB_OK, or VFB_ERR_CUDA if a bounded wait of a planned kernel ran out
+ * (synchronises the stream) */
+int vfb_collision_plan_check(const vfb_collision_plan* plan, void* stream);
+/* planned K17CompressibleNavierStokes::runOnIndices / B92 run */
+int vfb_k17_collision_planned(const vfb_collision_plan* plan, const vfb_collision_args* args, void* stream);
+int vfb_bgk_collision_planned(const vfb_collision_plan* plan, const vfb_collision_args* args, void* stream);
+
+/*
  * Equilibrium initialisation of one parity view from drho and velocity
  * (compute precision arrays of numberOfLBnodes).  Replaces
  * InitNavierStokesCompressible_Device

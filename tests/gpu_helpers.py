@@ -47,9 +47,10 @@ def oracle_run(w, precision: str, steps: int, kernel="K17", limiters=(0.01, 0.01
     return d, macro, even
 
 
-def gpu_run(w, dtype, steps: int, kernel="K17", limiters=(0.01, 0.01, 0.01), forces=(0, 0, 0)):
+def gpu_run(w, dtype, steps: int, kernel="K17", limiters=(0.01, 0.01, 0.01), forces=(0, 0, 0), planned=False):
     import torch
     lat = K.DeviceLattice.from_arrays(w.grid)
+    plan = K.CollisionPlan(dtype, lat) if planned else None
     cd = K.compute_dtype(dtype)
     dist = K.new_distributions(lat, dtype)
     fields = [torch.from_numpy(a).to("cuda", cd) for a in (w.rho, w.vx, w.vy, w.vz)]
@@ -57,8 +58,10 @@ def gpu_run(w, dtype, steps: int, kernel="K17", limiters=(0.01, 0.01, 0.01), for
         K.init_equilibrium(dist, lat, *fields, ev)
     even = True
     for _ in range(steps):
-        K.collision(kernel, dist, lat, w.omega, even, limiters=limiters, forces=forces)
+        K.collision(kernel, dist, lat, w.omega, even, limiters=limiters, forces=forces, plan=plan)
         even = not even
     macro = [m.cpu().numpy() for m in K.macroscopic(dist, lat, even)]
     torch.cuda.synchronize()
+    if plan is not None:
+        plan.check()
     return dist, lat, macro, even

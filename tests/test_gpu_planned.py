@@ -1,0 +1,111 @@
+"""The planned (bulk-copy, warp-tiled) collision path against the oracle and
+against the generic kernel, on periodic and walled grids."""
+import numpy as np
+import pytest
+
+from tests.gpu_helpers import gpu_run, oracle_run, rel_l2, rel_max, tgv_state
+from virtualfluids_b200 import _lib
+from virtualfluids_b200 import kernels as K
+from virtualfluids_b200.grid import MultipleGridBuilder, SideType
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.mark.parametrize("n", [16, 10, 33])
+@pytest.mark.parametrize("kernel", ["K17", "BGK"])
+def test_planned_fp64_matches_oracle(cuda, n, kernel):
+    w = tgv_state(n)
+    steps = 12
+    _, ref, _ = oracle_run(w, "f64", steps, kernel)
+    _, _, got, _ = gpu_run(w, torch.float64, steps, kernel, planned=True)
+    fl = w.grid["fluid"]
+    for a, b in zip(got, ref):
+        assert rel_max(a[fl], b[fl]) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float16", "bfloat16"])
+def test_planned_matches_generic(cuda, dtype):
+    w = tgv_state(24)
+    dt = getattr(torch, dtype)
+    d1, _, m1, _ = gpu_run(w, dt, 10, planned=True)
+    d2, _, m2, _ = gpu_run(w, dt, 10, planned=False)
+    fl = w.grid["fluid"]
+    tol = 1e-6 if dtype == "float32" else 2e-3
+    for a, b in zip(m1, m2):
+        assert rel_l2(a[fl], b[fl]) < tol
+
+
+def test_plan_statistics_for_periodic_cube(cuda):
+    w = tgv_state(64)
+    lat = K.DeviceLattice.from_arrays(w.grid)
+    plan = K.CollisionPlan(torch.float32, lat)
+    st = plan.stats()
+    assert st["bulk_nodes"] + st["exception_nodes"] + st["lane_nodes"] == 64 ** 3
+    # only the periodic wraps break the strides
+    assert st["bulk_nodes"] >= 0.9 * 64 ** 3
+    assert st["exception_nodes"] > 0
+
+
+def _walled_grid(periodic_y=False):
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, 20, 13, 11, 1.0)
+    b.setPeriodicBoundaryCondition(False, periodic_y, False)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(SideType.MX, 0.03, 0, 0)
+    b.setNoSlipBoundaryCondition(SideType.MZ)
+    return b.arrays()[0]
+
+
+@pytest.mark.parametrize("periodic_y", [False, True])
+def test_planned_on_walled_grid_matches_generic(cuda, periodic_y):
+    g = _walled_grid(periodic_y)
+    lat = K.DeviceLattice.from_arrays(g)
+    rng = np.random.default_rng(5)
+    N = lat.N
+    fields = [torch.from_numpy(rng.uniform(-1e-3, 1e-3, N)).cuda() for _ in range(4)]
+    outs = []
+    for planned in (True, False):
+        dist = K.new_distributions(lat, torch.float64)
+        for ev in (False, True):
+            K.init_equilibrium(dist, lat, *fields, ev)
+        plan = K.CollisionPlan(torch.float64, lat) if planned else None
+        even = True
+        for _ in range(8):
+            K.collision("K17", dist, lat, 1.7, even, plan=plan, forces=(1e-5, 0, 0))
+            even = not even
+        outs.append(dist.cpu().numpy())
+    assert rel_max(outs[0], outs[1]) < 1e-13
+
+
+@pytest.mark.parametrize("template", [1, 2, 3])
+def test_planned_templates_match_generic(cuda, template):
+    w = tgv_state(12)
+    lat = K.DeviceLattice.from_arrays(w.grid)
+    N = lat.N
+    rng = np.random.default_rng(11)
+    body0 = [rng.uniform(-1e-5, 1e-5, N) for _ in range(3)]
+    res = []
+    for planned in (True, False):
+        dist = K.new_distributions(lat, torch.float64)
+        fields = [torch.from_numpy(a).cuda() for a in (w.rho, w.vx, w.vy, w.vz)]
+        for ev in (False, True):
+            K.init_equilibrium(dist, lat, *fields, ev)
+        macro = [torch.zeros(N, dtype=torch.float64, device="cuda") for _ in range(4)]
+        body = [torch.from_numpy(b.copy()).cuda() for b in body0]
+        plan = K.CollisionPlan(torch.float64, lat) if planned else None
+        K.collision("K17", dist, lat, w.omega, True, plan=plan, template=template, macro=macro, body=body,
+                    forces=(2e-6, 0, -1e-6), force_factor=0.5)
+        res.append([dist.cpu().numpy()] + [m.cpu().numpy() for m in macro] + [b.cpu().numpy() for b in body])
+    for a, b in zip(*res):
+        assert rel_max(a, b) < 1e-13 if np.abs(b).max() > 0 else np.array_equal(a, b)
+
+
+def test_plan_rejects_other_arrays(cuda):
+    w = tgv_state(8)
+    lat = K.DeviceLattice.from_arrays(w.grid)
+    plan = K.CollisionPlan(torch.float32, lat)
+    dist = K.new_distributions(lat, torch.float32)
+    other = lat.fluid.clone()
+    with pytest.raises(_lib.VfbError):
+        K.collision("K17", dist, lat, w.omega, True, plan=plan, fluid=other)

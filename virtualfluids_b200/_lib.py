@@ -73,6 +73,13 @@ _SIGNATURES = [
     ("vfb_mass_and_energy", ctypes.c_int,
      [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_collision_plan_create", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("vfb_collision_plan_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("vfb_collision_plan_check", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("vfb_k17_collision_planned", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
+    ("vfb_bgk_collision_planned", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
     ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     ("vfb_grid_levels", ctypes.c_int, [ctypes.c_void_p]),
     ("vfb_grid_count", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),

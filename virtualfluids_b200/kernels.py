@@ -66,14 +66,12 @@ def new_distributions(lat: DeviceLattice, dtype, device="cuda"):
     return torch.zeros(27 * lat.N, dtype=dtype, device=device)
 
 
-def collision(kernel: str, dist, lat: DeviceLattice, omega: float, is_even: bool, *, forces=(0.0, 0.0, 0.0),
-              force_factor: float = 1.0, limiters=(0.01, 0.01, 0.01), template: int = 0, macro=None, body=None,
-              fluid=None, stream=None) -> None:
-    """One fused collide + stream pass (``kernel`` is "K17" or "BGK")."""
-    storage = STORAGE_OF_DTYPE[dist.dtype]
+def collision_args(dist, lat: DeviceLattice, omega: float, is_even: bool, *, forces=(0.0, 0.0, 0.0),
+                   force_factor: float = 1.0, limiters=(0.01, 0.01, 0.01), template: int = 0, macro=None, body=None,
+                   fluid=None) -> _lib.CollisionArgs:
     nodes = lat.fluid if fluid is None else fluid
     a = _lib.CollisionArgs()
-    a.distributions = dist.data_ptr()
+    a.distributions = dist.data_ptr() if dist is not None else None
     a.numberOfLBnodes = lat.N
     a.neighborX = lat.neighborX.data_ptr()
     a.neighborY = lat.neighborY.data_ptr()
@@ -90,9 +88,58 @@ def collision(kernel: str, dist, lat: DeviceLattice, omega: float, is_even: bool
         a.rho, a.vx, a.vy, a.vz = [_p(t) for t in macro]
     if body is not None:
         a.bodyForceX, a.bodyForceY, a.bodyForceZ = [_p(t) for t in body]
+    return a
+
+
+def collision(kernel: str, dist, lat: DeviceLattice, omega: float, is_even: bool, *, plan=None, stream=None,
+              **kw) -> None:
+    """One fused collide + stream pass (``kernel`` is "K17" or "BGK"); with a
+    CollisionPlan the planned (bulk-copy) kernel is used."""
+    a = collision_args(dist, lat, omega, is_even, **kw)
     L = _lib.lib()
+    if plan is not None:
+        if plan.dtype != dist.dtype:
+            raise ValueError("plan was built for another storage type")
+        fn = L.vfb_k17_collision_planned if kernel.upper() == "K17" else L.vfb_bgk_collision_planned
+        _lib.check(fn(plan.handle, ctypes.byref(a), _stream(stream)))
+        return
+    storage = STORAGE_OF_DTYPE[dist.dtype]
     fn = L.vfb_k17_collision if kernel.upper() == "K17" else L.vfb_bgk_collision
     _lib.check(fn(storage, ctypes.byref(a), _stream(stream)))
+
+
+class CollisionPlan:
+    """vfb_collision_plan for one level (fluid list and neighbour arrays)."""
+
+    def __init__(self, dtype, lat: DeviceLattice, fluid=None, stream=None):
+        self.dtype = dtype
+        self.lat = lat
+        self.fluid = lat.fluid if fluid is None else fluid
+        a = collision_args(None, lat, 1.0, True, fluid=self.fluid)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().vfb_collision_plan_create(STORAGE_OF_DTYPE[dtype], ctypes.byref(a), ctypes.byref(h),
+                                                        _stream(stream)))
+        self.handle = h
+
+    def stats(self) -> dict[str, int]:
+        out = (ctypes.c_ulonglong * 6)()
+        _lib.check(_lib.lib().vfb_collision_plan_stats(self.handle, out))
+        keys = ("tiles", "bulk_tiles", "lane_tiles", "bulk_nodes", "exception_nodes", "lane_nodes")
+        return dict(zip(keys, [int(x) for x in out]))
+
+    def check(self, stream=None) -> None:
+        _lib.check(_lib.lib().vfb_collision_plan_check(self.handle, _stream(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            _lib.lib().vfb_collision_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def init_equilibrium(dist, lat: DeviceLattice, rho, vx, vy, vz, is_even: bool, stream=None) -> None:
