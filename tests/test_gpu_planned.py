@@ -41,10 +41,10 @@ def test_plan_statistics_for_periodic_cube(cuda):
     lat = K.DeviceLattice.from_arrays(w.grid)
     plan = K.CollisionPlan(torch.float32, lat)
     st = plan.stats()
-    assert st["bulk_nodes"] + st["exception_nodes"] + st["lane_nodes"] == 64 ** 3
+    assert st["bulk_nodes"] + st["lane_nodes"] == 64 ** 3
     # only the periodic wraps break the strides
     assert st["bulk_nodes"] >= 0.9 * 64 ** 3
-    assert st["exception_nodes"] > 0
+    assert 0 < st["exception_nodes"] <= st["lane_nodes"]
 
 
 def _walled_grid(periodic_y=False):

@@ -1,23 +1,27 @@
 // collision_tiled.cu -- the planned collide + stream path.
 //
 // A collision plan (built once per level from the fluid-node list and the
-// neighbour arrays) cuts the fluid-node list into warp tiles of up to 32
-// consecutive entries.  A tile whose nodes are consecutive sparse indices
-// k0 .. k0+count-1 and whose neighbours follow the lattice strides
-// (neighborX = k+1, neighborY = k+sy, neighborZ = k+sz, also for the
-// neighbours' neighbours) is "regular": for each of the 27 directions its
-// populations form one contiguous run of memory, so the tile is fetched with
-// 27 bulk copies (cp.async.bulk) into shared memory one tile ahead of its
-// collision, and no index array is read for it.  Lanes whose node breaks the
-// strides (a periodic wrap, a node next to a removed node) are exception
-// lanes: they follow the neighbour chain and read global memory directly,
-// exactly as the generic kernel does.  Tiles whose entries are not
-// consecutive, or whose bulk range would leave the array, are processed
-// lane by lane like the generic kernel.
+// neighbour arrays) sorts the level's fluid nodes into two kinds of tiles.
+// A node is regular when its neighbours follow the lattice strides
+// (neighborX = k+1, neighborY = k+sy, neighborZ = k+sz, and likewise for the
+// neighbours' neighbours).  Regular nodes are grouped into tiles covering a
+// range of T consecutive sparse indices [k0, k0+T) (T = 256, or 128 for FP64);
+// for each of the 27 directions the populations of such a range are one
+// contiguous run of memory, so the whole tile is fetched with 27 bulk copies
+// (cp.async.bulk, about 1 KB each) into shared memory while the block
+// collides the previous tile, and no index array is read for it.  A bit mask
+// marks which indices of the range are members of the fluid-node list (the
+// others -- stoppers, removed or differently tagged nodes -- are skipped).
+// Irregular nodes (periodic wraps, nodes next to removed ones) and sparse
+// ranges go to lane tiles, processed one node per thread through the index
+// chain exactly as the generic kernel does.
 //
-// Each warp owns two shared-memory stages and an mbarrier per stage; warps of
-// a persistent grid stride over the tiles.  The arithmetic is the same
-// k17Collide / bgkCollide as the generic kernel, so results are identical.
+// Each block owns two shared-memory stages and an mbarrier per stage; blocks
+// of a persistent grid stride over the tiles.  The arithmetic is the same
+// k17Collide / bgkCollide as the generic kernel.  Every population location
+// is read and written by exactly one node, and a thread uses only the values
+// at its own node's locations, so values a bulk copy fetches for positions no
+// thread uses may be stale without harm.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,22 +38,22 @@
 namespace vfb
 {
 
-// tile descriptor: x = first fluid-list entry, y = first node k0,
-// z = count | (bulk << 16), w = exception-lane mask
-using TileDesc = int4;
+// Tile descriptor: x = k0 (first sparse index of the range), y = index of the
+// tile's active-lane mask words
+using TileDesc = int2;
 
-constexpr int kTiledWarps = 4;
-constexpr int kTiledThreads = 32 * kTiledWarps;
 constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
 
+// tile width (nodes per block iteration) by storage size
 template <class S>
-struct Seg {
+struct TileShape {
+    static constexpr int T = sizeof(S) == 8 ? 128 : 256;          // threads per block = nodes per tile
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
-    static constexpr int CAP = ((E - 1 + 32 + E - 1) / E) * E;     // elements per direction segment
-    static constexpr int STAGE_ELEMS = 27 * CAP;
-    static constexpr int STAGE_BYTES = STAGE_ELEMS * (int)sizeof(S);
-    static constexpr int WARP_BYTES = 2 * STAGE_BYTES + 16;        // two stages + two mbarriers
-    static constexpr int BLOCK_BYTES = kTiledWarps * WARP_BYTES;
+    static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
+    static constexpr int STAGE_BYTES = 27 * CAP * (int)sizeof(S);
+    static constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 16;        // two stages + two mbarriers
+    static constexpr int MASK_WORDS = T / 32;
+    static constexpr int MIN_BLOCKS = sizeof(S) == 8 ? 2 : 3;       // resident blocks per SM the registers are sized for
 };
 
 enum class Op { K17, BGK };
@@ -62,8 +66,8 @@ struct TiledArgs {
     const uint32_t* __restrict__ nX;
     const uint32_t* __restrict__ nY;
     const uint32_t* __restrict__ nZ;
-    const uint32_t* __restrict__ fluid;
     const TileDesc* __restrict__ tiles;
+    const uint32_t* __restrict__ masks;
     uint32_t nTiles;
     uint32_t sy, sz;
     K17Rates<R> rates;
@@ -80,30 +84,31 @@ struct TiledArgs {
 
 // offset of location loc (bit 0 x, bit 1 y, bit 2 z) from the node for the
 // regular lattice strides
-__device__ __forceinline__ uint32_t locShift(int l, uint32_t sy, uint32_t sz)
+__host__ __device__ __forceinline__ uint32_t locShift(int l, uint32_t sy, uint32_t sz)
 {
     return (uint32_t)(l & 1) + ((l & 2) ? sy : 0u) + ((l & 4) ? sz : 0u);
 }
 
+// thread 0 arms the stage barrier and issues the 27 bulk copies of a tile
 template <class S, bool EVEN>
-__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, const TileDesc& t, S* stage, uint64_t* bar, int lane)
+__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t k0, S* stage, uint64_t* bar)
 {
-    using G = Seg<S>;
-    const uint32_t count = (uint32_t)t.z & 0xffffu;
-    uint32_t bytes = 0;
-    unsigned long long base = 0;
-    uint32_t lead = 0;
-    if (lane < 27) {
-        base = (unsigned long long)slot<EVEN>(lane) * a.N + (uint32_t)t.y + locShift(loc(lane), a.sy, a.sz);
-        lead = (uint32_t)(base % G::E);
-        bytes = ((lead + count + G::E - 1) / G::E) * G::E * (uint32_t)sizeof(S);
+    using G = TileShape<S>;
+    uint32_t total = 0;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const unsigned long long base = (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
+        const uint32_t lead = (uint32_t)(base % G::E);
+        total += ((lead + G::T + G::E - 1) / G::E) * G::E * (uint32_t)sizeof(S);
     }
-    const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
-    if (lane == 0)
-        tma::mbarArriveExpectTx(bar, total);
-    __syncwarp();
-    if (lane < 27)
-        tma::bulkLoad(stage + lane * G::CAP, a.dist + (base - lead), bytes, bar);
+    tma::mbarArriveExpectTx(bar, total);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const unsigned long long base = (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
+        const uint32_t lead = (uint32_t)(base % G::E);
+        const uint32_t bytes = ((lead + G::T + G::E - 1) / G::E) * G::E * (uint32_t)sizeof(S);
+        tma::bulkLoad(stage + d * G::CAP, a.dist + (base - lead), bytes, bar);
+    }
 }
 
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
@@ -134,99 +139,85 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
 }
 
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
-__global__ void __launch_bounds__(kTiledThreads) tiledKernel(const TiledArgs<S> a)
+__global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) tiledKernel(const TiledArgs<S> a)
 {
     using R = typename Storage<S>::R;
-    using G = Seg<S>;
+    using G = TileShape<S>;
     extern __shared__ __align__(128) unsigned char smemRaw[];
-    const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
-    unsigned char* mine = smemRaw + warp * G::WARP_BYTES;
-    S* stages[2] = { reinterpret_cast<S*>(mine), reinterpret_cast<S*>(mine + G::STAGE_BYTES) };
-    uint64_t* bars = reinterpret_cast<uint64_t*>(mine + 2 * G::STAGE_BYTES);
-    if (lane == 0) {
+    S* stages[2] = { reinterpret_cast<S*>(smemRaw), reinterpret_cast<S*>(smemRaw + G::STAGE_BYTES) };
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smemRaw + 2 * G::STAGE_BYTES);
+    __shared__ int abort;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        abort = 0;
         tma::mbarInit(&bars[0], 1);
         tma::mbarInit(&bars[1], 1);
         tma::fenceBarrierInit();
     }
-    __syncwarp();
+    __syncthreads();
 
-    const uint32_t totalWarps = gridDim.x * kTiledWarps;
-    uint32_t tIdx = blockIdx.x * kTiledWarps + warp;
-    if (tIdx >= a.nTiles)
+    uint32_t t = blockIdx.x;
+    if (t >= a.nTiles)
         return;
     uint32_t uses[2] = { 0, 0 };
     int s = 0;
-    TileDesc cur = a.tiles[tIdx];
-    if ((cur.z >> 16) & 1)
-        issueTile<S, EVEN>(a, cur, stages[s], &bars[s], lane);
+    TileDesc cur = a.tiles[t];
+    uint32_t curMask = a.masks[(size_t)cur.y * G::MASK_WORDS + warp];
+    if (tid == 0)
+        issueTile<S, EVEN>(a, (uint32_t)cur.x, stages[0], &bars[0]);
 
     while (true) {
-        const uint32_t nIdx = tIdx + totalWarps;
-        TileDesc nxt = make_int4(0, 0, 0, 0);
-        if (nIdx < a.nTiles) {
-            nxt = a.tiles[nIdx];
-            if ((nxt.z >> 16) & 1) {
+        const uint32_t tn = t + gridDim.x;
+        TileDesc nxt = make_int2(0, 0);
+        uint32_t nxtMask = 0;
+        if (tn < a.nTiles) {
+            nxt = a.tiles[tn];
+            nxtMask = a.masks[(size_t)nxt.y * G::MASK_WORDS + warp];
+            if (tid == 0) {
                 tma::fenceProxyAsync();
-                issueTile<S, EVEN>(a, nxt, stages[s ^ 1], &bars[s ^ 1], lane);
+                issueTile<S, EVEN>(a, (uint32_t)nxt.x, stages[s ^ 1], &bars[s ^ 1]);
             }
         }
 
-        const uint32_t count = (uint32_t)cur.z & 0xffffu;
-        const bool bulk = (cur.z >> 16) & 1;
-        const uint32_t exceptions = bulk ? (uint32_t)cur.w : 0xffffffffu;
-        if (bulk) {
-            const bool ok = __all_sync(0xffffffffu, tma::mbarWait(&bars[s], uses[s] & 1u, kWaitLimit));
+        {
+            // node k0 + tid, active if its mask bit is set
+            const bool ok = tma::mbarWait(&bars[s], uses[s] & 1u, kWaitLimit);
             uses[s]++;
-            if (!ok) {
-                if (lane == 0)
-                    atomicExch(a.errorFlag, 1);
-                return;
-            }
-        }
-        if ((uint32_t)lane < count) {
-            R f[27];
-            const bool exc = (exceptions >> lane) & 1u;
-            uint32_t k;
-            Locs L;
-            if (!exc) {
-                k = (uint32_t)cur.y + lane;
+            if (!ok)
+                abort = 1;
+            if (ok && ((curMask >> lane) & 1u)) {
+                const uint32_t k0 = (uint32_t)cur.x;
+                const uint32_t k = k0 + tid;
                 const S* st = stages[s];
+                R f[27];
 #pragma unroll
                 for (int d = 0; d < 27; ++d) {
                     const unsigned long long base =
-                        (unsigned long long)slot<EVEN>(d) * a.N + (uint32_t)cur.y + locShift(loc(d), a.sy, a.sz);
-                    f[d] = Storage<S>::load(st + d * G::CAP + (uint32_t)(base % G::E) + lane);
+                        (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
+                    f[d] = Storage<S>::load(st + d * G::CAP + (uint32_t)(base % G::E) + tid);
                 }
-            } else {
-                k = __ldg(a.fluid + cur.x + lane);
-                L = listIndices(k, a.nX, a.nY, a.nZ);
+                collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
                 for (int d = 0; d < 27; ++d)
-                    f[d] = Storage<S>::load(a.dist + (unsigned long long)slot<EVEN>(d) * a.N + L.k[loc(d)]);
-            }
-            collideNode<S, EVEN, OP, WM, BF>(a, f, k);
-            if (!exc) {
-#pragma unroll
-                for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.dist + (unsigned long long)slot<EVEN>(d) * a.N + k +
-                                          locShift(loc(d), a.sy, a.sz),
+                    Storage<S>::store(a.dist + (unsigned long long)slot<EVEN>(d) * a.N + k + locShift(loc(d), a.sy, a.sz),
                                       f[inv(d)]);
-            } else {
-#pragma unroll
-                for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.dist + (unsigned long long)slot<EVEN>(d) * a.N + L.k[loc(d)], f[inv(d)]);
             }
         }
-        __syncwarp();
-        if (nIdx >= a.nTiles)
+        __syncthreads();
+        if (abort) {
+            if (tid == 0)
+                atomicExch(a.errorFlag, 1);
+            return;
+        }
+        if (tn >= a.nTiles)
             break;
-        tIdx = nIdx;
+        t = tn;
         cur = nxt;
+        curMask = nxtMask;
         s ^= 1;
     }
 }
-
 
 // ------------------------------------------------------------------ plan --
 struct vfb_collision_plan_impl {
@@ -239,8 +230,12 @@ struct vfb_collision_plan_impl {
     uint32_t nFluid = 0;
     uint32_t sy = 0, sz = 0;
     TileDesc* tiles = nullptr;
+    uint32_t* masks = nullptr;
+    uint32_t* laneList = nullptr;
     uint32_t nTiles = 0;
-    unsigned long long stats[6] = { 0, 0, 0, 0, 0, 0 }; // tiles, bulk tiles, generic tiles, bulk nodes, exception lanes, generic nodes
+    uint32_t nLane = 0;
+    // tiles, bulk tiles, lane blocks, bulk-fed nodes, irregular nodes, nodes collided lane by lane
+    unsigned long long stats[6] = { 0, 0, 0, 0, 0, 0 };
     int* error = nullptr;
 };
 
@@ -264,6 +259,15 @@ uint32_t modeStride(const std::vector<uint32_t>& fluid, const std::vector<uint32
         }
     return (uint32_t)best;
 }
+
+template <class T>
+cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
+{
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * std::max<size_t>(1, v.size()));
+    if (e == cudaSuccess && !v.empty())
+        e = cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, stream);
+    return e;
+}
 } // namespace
 
 static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collision_args* a, cudaStream_t stream)
@@ -276,14 +280,20 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
         e = cudaMemcpyAsync(ny.data(), a->neighborY, N * 4, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(nz.data(), a->neighborZ, N * 4, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && nF)
         e = cudaMemcpyAsync(fl.data(), a->fluidNodeIndices, (size_t)nF * 4, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess)
         return setError(VFB_ERR_CUDA, "plan: copying index arrays failed: %s", cudaGetErrorString(e));
+    for (uint32_t i = 0; i < nF; ++i)
+        if (fl[i] >= N)
+            return setError(VFB_ERR_OUT_OF_RANGE, "fluid node %u of the list is outside the lattice", fl[i]);
 
-    const uint32_t sy = modeStride(fl, ny), sz = modeStride(fl, nz);
+    const int esize = vfb_storage_bytes(storage);
+    const uint64_t T = esize == 8 ? 128 : 256;
+    const uint64_t E = 16 / (uint64_t)esize;
+    const uint32_t sy = nF ? modeStride(fl, ny) : 1, sz = nF ? modeStride(fl, nz) : 1;
     auto regular = [&](uint64_t k) -> bool {
         const uint64_t far = k + 1 + (uint64_t)sy + sz;
         if (far >= N)
@@ -291,66 +301,72 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
         return nx[k] == k + 1 && ny[k] == k + sy && nz[k] == k + sz && ny[k + 1] == k + 1 + sy &&
                nz[k + 1] == k + 1 + sz && nz[k + sy] == k + sy + sz && nz[k + 1 + sy] == k + 1 + sy + sz;
     };
-    const int esize = vfb_storage_bytes(storage);
-    const uint64_t E = 16 / (uint64_t)esize;
     const uint64_t limit = 27ull * N;
-    auto bulkInBounds = [&](uint64_t k0, uint32_t count) -> bool {
+    auto bulkInBounds = [&](uint64_t k0) -> bool {
         for (int even = 0; even < 2; ++even)
             for (int d = 0; d < 27; ++d) {
-                const int sl = even ? d : inv(d);
-                const int l = loc(d);
-                const uint64_t base = (uint64_t)sl * N + k0 + (l & 1) + ((l & 2) ? sy : 0) + ((l & 4) ? sz : 0);
+                const uint64_t base = (uint64_t)(even ? d : inv(d)) * N + k0 + locShift(loc(d), sy, sz);
                 const uint64_t lead = base % E;
-                const uint64_t end = base - lead + ((lead + count + E - 1) / E) * E;
-                if (end > limit)
+                if (base - lead + ((lead + T + E - 1) / E) * E > limit)
                     return false;
             }
         return true;
     };
-    auto runLength = [&](uint32_t i) -> uint32_t {
-        uint32_t j = i + 1;
-        while (j < nF && j - i < 32 && fl[j] == fl[j - 1] + 1)
-            ++j;
-        return j - i;
-    };
 
-    std::vector<TileDesc> tiles;
-    tiles.reserve(nF / 32 + 16);
-    uint32_t i = 0;
-    while (i < nF) {
-        const uint32_t run = runLength(i);
-        if (run >= 8) {
-            uint32_t mask = 0, regularLanes = 0;
-            for (uint32_t t = 0; t < run; ++t) {
-                if (regular(fl[i + t]))
-                    ++regularLanes;
-                else
-                    mask |= 1u << t;
-            }
-            const bool bulk = regularLanes > 0 && bulkInBounds(fl[i], run);
-            if (!bulk)
-                mask = 0xffffffffu;
-            tiles.push_back(make_int4((int)i, (int)fl[i], (int)(run | (bulk ? 1u << 16 : 0u)), (int)mask));
-            if (bulk) {
-                p.stats[1]++;
-                p.stats[3] += regularLanes;
-                p.stats[4] += run - regularLanes;
-            } else {
-                p.stats[2]++;
-                p.stats[5] += run;
-            }
-            i += run;
-        } else {
-            uint32_t j = i;
-            while (j < nF && j - i < 32 && (j == i || runLength(j) < 8))
-                ++j;
-            tiles.push_back(make_int4((int)i, (int)fl[i], (int)(j - i), (int)0xffffffffu));
-            p.stats[2]++;
-            p.stats[5] += j - i;
-            i = j;
-        }
+    // regular list members, ascending; everything else goes lane by lane
+    std::vector<uint32_t> cand, lane;
+    cand.reserve(nF);
+    for (uint32_t i = 0; i < nF; ++i) {
+        if (regular(fl[i]))
+            cand.push_back(fl[i]);
+        else
+            lane.push_back(fl[i]);
     }
+    p.stats[4] = lane.size();
+    std::sort(cand.begin(), cand.end());
+    if (std::adjacent_find(cand.begin(), cand.end()) != cand.end())
+        return setError(VFB_ERR_INVALID_ARGUMENT, "the fluid-node list holds a node twice");
+
+    struct Entry {
+        uint32_t key;
+        TileDesc d;
+    };
+    std::vector<Entry> order;
+    std::vector<uint32_t> masks;
+    const uint64_t words = T / 32;
+    const uint64_t minActive = T / 4;
+    size_t i = 0;
+    while (i < cand.size()) {
+        const uint64_t k0 = cand[i];
+        size_t j = i;
+        while (j < cand.size() && cand[j] < k0 + T)
+            ++j;
+        const uint64_t active = j - i;
+        if (active >= minActive && bulkInBounds(k0)) {
+            const uint32_t maskIndex = (uint32_t)(masks.size() / words);
+            masks.resize(masks.size() + words, 0u);
+            for (size_t q = i; q < j; ++q) {
+                const uint64_t off = cand[q] - k0;
+                masks[(size_t)maskIndex * words + off / 32] |= 1u << (off % 32);
+            }
+            order.push_back({ (uint32_t)k0, make_int2((int)k0, (int)maskIndex) });
+            p.stats[1]++;
+            p.stats[3] += active;
+        } else {
+            for (size_t q = i; q < j; ++q)
+                lane.push_back(cand[q]);
+        }
+        i = j;
+    }
+    // the nodes left over are collided one per thread by the generic kernel
+    std::sort(lane.begin(), lane.end());
+    p.stats[2] = (lane.size() + T - 1) / T;
+    p.stats[5] = lane.size();
+    std::vector<TileDesc> tiles(order.size());
+    for (size_t q = 0; q < order.size(); ++q)
+        tiles[q] = order[q].d;
     p.stats[0] = tiles.size();
+
     p.storage = storage;
     p.N = N;
     p.nX = a->neighborX;
@@ -361,11 +377,14 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     p.sy = sy;
     p.sz = sz;
     p.nTiles = (uint32_t)tiles.size();
-    e = cudaMalloc(&p.tiles, sizeof(TileDesc) * std::max<size_t>(1, tiles.size()));
+    p.nLane = (uint32_t)lane.size();
+    e = upload(&p.tiles, tiles, stream);
+    if (e == cudaSuccess)
+        e = upload(&p.masks, masks, stream);
+    if (e == cudaSuccess)
+        e = upload(&p.laneList, lane, stream);
     if (e == cudaSuccess)
         e = cudaMalloc(&p.error, sizeof(int));
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(p.tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(p.error, 0, sizeof(int), stream);
     if (e == cudaSuccess)
@@ -378,23 +397,21 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
-    using G = Seg<S>;
+    using G = TileShape<S>;
     static int blocks = 0;
     if (blocks == 0) {
         cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, EVEN, OP, WM, BF>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::BLOCK_BYTES);
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
         if (e != cudaSuccess)
             return setError(VFB_ERR_CUDA, "tiled kernel shared memory attribute: %s", cudaGetErrorString(e));
         int perSM = 0, device = 0, sms = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, EVEN, OP, WM, BF>, kTiledThreads,
-                                                      G::BLOCK_BYTES);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, EVEN, OP, WM, BF>, G::T, G::SMEM_BYTES);
         blocks = std::max(1, perSM) * sms;
     }
-    const unsigned grid = (unsigned)std::min<unsigned long long>(
-        (unsigned long long)blocks, (a.nTiles + kTiledWarps - 1) / (unsigned long long)kTiledWarps);
-    tiledKernel<S, EVEN, OP, WM, BF><<<std::max(1u, grid), kTiledThreads, G::BLOCK_BYTES, stream>>>(a);
+    const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
+    tiledKernel<S, EVEN, OP, WM, BF><<<std::max(1u, grid), G::T, G::SMEM_BYTES, stream>>>(a);
     return checkLaunch("tiled collision");
 }
 
@@ -408,8 +425,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.nX = p.nX;
     a.nY = p.nY;
     a.nZ = p.nZ;
-    a.fluid = p.fluid;
     a.tiles = p.tiles;
+    a.masks = p.masks;
     a.nTiles = p.nTiles;
     a.sy = p.sy;
     a.sz = p.sz;
@@ -476,6 +493,15 @@ static int runPlanned(Op op, const vfb_collision_plan* plan, const vfb_collision
             return setError(VFB_ERR_INVALID_ARGUMENT, "template %d needs bodyForceX/Y/Z", t);
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (p.nLane) {
+        // the irregular nodes, one per thread through the index chain
+        vfb_collision_args lane = *c;
+        lane.fluidNodeIndices = p.laneList;
+        lane.numberOfFluidNodes = p.nLane;
+        const int rc = op == Op::K17 ? vfb_k17_collision(p.storage, &lane, stream) : vfb_bgk_collision(p.storage, &lane, stream);
+        if (rc != VFB_OK)
+            return rc;
+    }
     switch (p.storage) {
     case VFB_FP32: return launchTiled<float>(op, p, c, s);
     case VFB_FP64: return launchTiled<double>(op, p, c, s);
@@ -505,6 +531,8 @@ extern "C" int vfb_collision_plan_create(int storage, const vfb_collision_args* 
     const int rc = buildPlan(*p, storage, args, static_cast<cudaStream_t>(stream));
     if (rc != VFB_OK) {
         cudaFree(p->tiles);
+        cudaFree(p->masks);
+        cudaFree(p->laneList);
         cudaFree(p->error);
         delete p;
         return rc;
@@ -520,6 +548,8 @@ extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
         return VFB_OK;
     auto* p = reinterpret_cast<vfb_collision_plan_impl*>(plan);
     cudaFree(p->tiles);
+    cudaFree(p->masks);
+    cudaFree(p->laneList);
     cudaFree(p->error);
     delete p;
     return VFB_OK;
