@@ -171,6 +171,15 @@ int vfb_mass_and_energy(int storage, const void* distributions, unsigned long lo
                         const uint32_t* nodeIndices, uint32_t numberOfIndices, int isEvenTimestep, double* out,
                         void* stream);
 
+/*
+ * One node of the K17 (op 0) or BGK (op 1) collision on the host with the
+ * library's own arithmetic (the code the kernels run), for checks without a
+ * GPU.  precision: VFB_FP64 or VFB_FP32; f27 in/out, out4 = drho, vx, vy, vz.
+ * No counterpart in the reference.
+ */
+int vfb_debug_collide_node(int op, int precision, double* f27, double omega, const double* limiters,
+                           const double* force, double* out4);
+
 #ifdef __cplusplus
 }
 #endif

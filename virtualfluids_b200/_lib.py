@@ -80,6 +80,9 @@ _SIGNATURES = [
     ("vfb_collision_plan_check", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_k17_collision_planned", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
     ("vfb_bgk_collision_planned", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CollisionArgs), ctypes.c_void_p]),
+    ("vfb_debug_collide_node", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     ("vfb_grid_levels", ctypes.c_int, [ctypes.c_void_p]),
     ("vfb_grid_count", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),

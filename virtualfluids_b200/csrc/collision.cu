@@ -24,6 +24,7 @@ template <class S>
 struct CollisionKernelArgs {
     using R = typename Storage<S>::R;
     S* dist;
+    S* base[27];          // dist + slot(d) * N for the parity of the launch
     unsigned long long N;
     const uint32_t* __restrict__ nX;
     const uint32_t* __restrict__ nY;
@@ -93,7 +94,9 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
 
     const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
     R f[27];
-    gatherPre<S, EVEN>(f, a.dist, a.N, L);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)]);
     R drho, ux, uy, uz;
     k17Collide<R>(f, a.rates, fx, fy, fz, drho, ux, uy, uz);
     if (WRITE_MACRO) {
@@ -102,7 +105,9 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
         a.vz[k] = uz;
         a.rho[k] = drho;
     }
-    scatterPost<S, EVEN>(f, a.dist, a.N, L);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)]);
 }
 
 template <class S, bool EVEN>
@@ -115,9 +120,13 @@ __global__ void __launch_bounds__(kCollisionThreads) bgkKernel(const CollisionKe
     const uint32_t k = __ldg(a.fluid + i);
     const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
     R f[27];
-    gatherPre<S, EVEN>(f, a.dist, a.N, L);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)]);
     bgkCollide<R>(f, a.rates.omega);
-    scatterPost<S, EVEN>(f, a.dist, a.N, L);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)]);
 }
 
 // InitNavierStokesCompressible_Device.cu:173-200
@@ -274,6 +283,8 @@ static int launchCollision(bool bgk, const vfb_collision_args* a, cudaStream_t s
         return VFB_OK;
     const unsigned blocks = (a->numberOfFluidNodes + kCollisionThreads - 1) / kCollisionThreads;
     const bool even = a->isEvenTimestep != 0;
+    for (int d = 0; d < 27; ++d)
+        k.base[d] = k.dist + (unsigned long long)(even ? d : inv(d)) * k.N;
     if (bgk) {
         if (even)
             bgkKernel<S, true><<<blocks, kCollisionThreads, 0, stream>>>(k);
@@ -492,4 +503,50 @@ extern "C" int vfb_mass_and_energy(int storage, const void* distributions, unsig
     }
     cudaFreeAsync(partial, s);
     return rc;
+}
+
+/*
+ * One node of the K17 (op 0) or BGK (op 1) collision evaluated on the host
+ * with the library's arithmetic (the same __host__ __device__ code the
+ * kernels run; the host compiler does not contract multiply-adds beyond the
+ * explicit fma calls).  precision: VFB_FP64 or VFB_FP32.  f27 in/out;
+ * out4 = drho, vx, vy, vz (K17 only).  For tests without a GPU.
+ */
+extern "C" int vfb_debug_collide_node(int op, int precision, double* f27, double omega, const double* limiters,
+                                      const double* force, double* out4)
+{
+    clearError();
+    if (!f27 || !limiters || !force || !out4)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (precision == VFB_FP64) {
+        double f[27];
+        for (int d = 0; d < 27; ++d)
+            f[d] = f27[d];
+        const K17Rates<double> r = makeK17Rates<double>(omega, limiters[0], limiters[1], limiters[2]);
+        if (op == 0)
+            k17Collide<double>(f, r, force[0], force[1], force[2], out4[0], out4[1], out4[2], out4[3]);
+        else
+            bgkCollide<double>(f, omega);
+        for (int d = 0; d < 27; ++d)
+            f27[d] = f[d];
+        return VFB_OK;
+    }
+    if (precision == VFB_FP32) {
+        float f[27];
+        for (int d = 0; d < 27; ++d)
+            f[d] = (float)f27[d];
+        const K17Rates<float> r = makeK17Rates<float>((float)omega, (float)limiters[0], (float)limiters[1],
+                                                      (float)limiters[2]);
+        float o[4] = { 0, 0, 0, 0 };
+        if (op == 0)
+            k17Collide<float>(f, r, (float)force[0], (float)force[1], (float)force[2], o[0], o[1], o[2], o[3]);
+        else
+            bgkCollide<float>(f, (float)omega);
+        for (int d = 0; d < 27; ++d)
+            f27[d] = f[d];
+        for (int i = 0; i < 4; ++i)
+            out4[i] = o[i];
+        return VFB_OK;
+    }
+    return setError(VFB_ERR_INVALID_ARGUMENT, "precision must be VFB_FP64 or VFB_FP32");
 }

@@ -3,15 +3,21 @@
 // K17: the compressible cumulant collision of VirtualFluids
 // (src/lbm/collision/K17CompressibleNavierStokes.h:87-591, TurbulenceModel::None),
 // based on Geier et al., J. Comput. Phys. 348 (2017) 862-888 and 889-898.
-// The arithmetic of every retained term is performed in the same order as the
-// reference so that FP64 results agree to rounding (FMA contraction aside).
-// Two things are different by construction, neither changes a result:
+// The operator is the reference's, term for term; the arithmetic is arranged
+// for the GPU's issue rate (the step is instruction bound at ~1 kflop/node):
+//   * the chimera transforms are written in multiply-add form with their
+//     conditioning factors multiplied out (algebraically identical);
+//   * density, momentum and the first (z) chimera sweep share the sums over
+//     the nine z lines of the lattice;
 //   * rates that depend only on omega and the limiters are formed once per
 //     launch on the host (K17Rates) with the reference's expressions;
 //   * cumulants whose post-collision value does not depend on their
 //     pre-collision value (orders 4..6 with O4 = O5 = O6 = 1) are never
 //     formed: the reference computes them and then multiplies them by
-//     (1 - 1) = 0 or cancels them exactly (x + 1 * (-x) = +0).
+//     (1 - 1) = 0 or cancels them exactly (x + 1 * (-x) = +0);
+//   * in FP32 the seven limiter quotients use the fast division.
+// Results agree with the reference to rounding: FP64 fields within 1e-12
+// relative of the oracle after many steps (tests/test_gpu_collision.py).
 //
 // BGK: src/gpu/core/Kernel/Compressible/NavierStokes/B92/B92CompressibleNavierStokes_Device.cu:194-234.
 #pragma once
@@ -63,54 +69,75 @@ inline K17Rates<R> makeK17Rates(R omega, R qlP, R qlM, R qlD)
 }
 
 // ---------------------------------------------------------------- chimera --
-// ChimeraTransformation.h:58-121 (Geier et al. 2015, appendix J)
+// Central-moment transforms of ChimeraTransformation.h:58-121 (Geier et al.
+// 2015, appendix J), written in multiply-add form.  With the conditioning pair
+// (Kinverse, K) of a line and Kq = Kinverse * K:
+//   forward   a' = a + b + c
+//             b' = Kq (m1 - vv m0) - K vv,      m1 = c - a, m2 = a + c, m0 = a'
+//             c' = Kq (m2 - 2 vv m1 + v2 m0) + K v2
+//   backward  a' = c/2 + b (vv - 1/2) + (a + K) (v2 - vv)/2
+//             b' = (a - c) - 2 vv b - v2 (a + K)
+//             c' = c/2 + b (vv + 1/2) + (a + K) (v2 + vv)/2
+// which are the reference's expressions with the factors Kinverse and K
+// multiplied out (every line has Kq = 1 except the last forward x line, whose
+// pair (3, 1/9) gives Kq = 1/3; K = 0 gives the plain transforms).
 template <class R>
-__device__ __forceinline__ void fwdK(R& a, R& b, R& c, R vv, R v2, R kinv, R k)
+struct Sweep {
+    R vv, v2, nvv, n2vv, nv2, hm, hp, vvm, vvp;
+    __host__ __device__ __forceinline__ Sweep(R v)
+    {
+        vv = v;
+        v2 = v * v;
+        nvv = -v;
+        n2vv = R(-2) * v;
+        nv2 = -v2;
+        hm = R(0.5) * (v2 - v);
+        hp = R(0.5) * (v2 + v);
+        vvm = v - R(0.5);
+        vvp = v + R(0.5);
+    }
+};
+
+template <class R>
+__host__ __device__ __forceinline__ void fwd(R& a, R& b, R& c, const Sweep<R>& w, R K)
 {
     const R m2 = a + c;
     const R m1 = c - a;
-    R m0 = m2 + b;
+    const R m0 = m2 + b;
+    const R m0K = K != R(0) ? m0 + K : m0;
     a = m0;
-    m0 *= kinv;
-    m0 += R(1);
-    b = (m1 * kinv - m0 * vv) * k;
-    c = ((m2 - R(2) * m1 * vv) * kinv + v2 * m0) * k;
+    b = fma(w.nvv, m0K, m1);
+    c = fma(w.v2, m0K, fma(w.n2vv, m1, m2));
 }
 
+// the forward x line with (Kinverse, K) = (3, 1/9) of K17CompressibleNavierStokes.h:222
 template <class R>
-__device__ __forceinline__ void bwdK(R& a, R& b, R& c, R vv, R v2, R kinv, R k)
+__host__ __device__ __forceinline__ void fwdThird(R& a, R& b, R& c, const Sweep<R>& w)
 {
-    const R m0 = (((c - b) * R(0.5) + b * vv) * kinv + (a * kinv + R(1)) * (v2 - vv) * R(0.5)) * k;
-    const R m1 = (((a - c) - R(2) * b * vv) * kinv + (a * kinv + R(1)) * (-v2)) * k;
-    c = (((c + b) * R(0.5) + b * vv) * kinv + (a * kinv + R(1)) * (v2 + vv) * R(0.5)) * k;
+    const R m2 = a + c;
+    const R m1 = c - a;
+    const R m0 = m2 + b;
     a = m0;
-    b = m1;
+    b = fma(R(1) / R(3), fma(w.nvv, m0, m1), w.nvv * (R(1) / R(9)));
+    c = fma(R(1) / R(3), fma(w.v2, m0, fma(w.n2vv, m1, m2)), w.v2 * (R(1) / R(9)));
 }
 
 template <class R>
-__device__ __forceinline__ void fwd0(R& a, R& b, R& c, R vv, R v2)
+__host__ __device__ __forceinline__ void bwd(R& a, R& b, R& c, const Sweep<R>& w, R K)
 {
-    const R m1 = (a + c) + b;
-    const R m2 = c - a;
-    c = (c + a) + (v2 * m1 - R(2) * vv * m2);
-    b = m2 - vv * m1;
-    a = m1;
-}
-
-template <class R>
-__device__ __forceinline__ void bwd0(R& a, R& b, R& c, R vv, R v2)
-{
-    const R ma = (c + a * (v2 - vv)) * R(0.5) + b * (vv - R(0.5));
-    const R mb = ((a - c) - a * v2) - R(2) * b * vv;
-    c = (c + a * (v2 + vv)) * R(0.5) + b * (vv + R(0.5));
-    b = mb;
-    a = ma;
+    const R aK = K != R(0) ? a + K : a;
+    const R hc = R(0.5) * c;
+    const R na = fma(aK, w.hm, fma(b, w.vvm, hc));
+    const R nb = fma(w.nv2, aK, fma(w.n2vv, b, a - c));
+    c = fma(aK, w.hp, fma(b, w.vvp, hc));
+    a = na;
+    b = nb;
 }
 
 // --------------------------------------------------------- macroscopic sums --
 // MacroscopicQuantities.h:55-127 (pyramid summation)
 template <class R>
-__device__ __forceinline__ R pyramidDensity(const R* f)
+__host__ __device__ __forceinline__ R pyramidDensity(const R* f)
 {
     const R t1 = ((f[dPPP] + f[dMMM]) + (f[dMPM] + f[dPMP])) + ((f[dMPP] + f[dPMM]) + (f[dMMP] + f[dPPM]));
     const R t2 = (((f[d0MP] + f[d0PM]) + (f[d0MM] + f[d0PP])) + ((f[dM0P] + f[dP0M]) + (f[dM0M] + f[dP0P]))) +
@@ -119,21 +146,21 @@ __device__ __forceinline__ R pyramidDensity(const R* f)
     return ((t1 + t2) + f[d000]) + t3;
 }
 template <class R>
-__device__ __forceinline__ R pyramidJx(const R* f)
+__host__ __device__ __forceinline__ R pyramidJx(const R* f)
 {
     return ((((f[dPPP] - f[dMMM]) + (f[dPMP] - f[dMPM])) + ((f[dPMM] - f[dMPP]) + (f[dPPM] - f[dMMP]))) +
             (((f[dP0M] - f[dM0P]) + (f[dP0P] - f[dM0M])) + ((f[dPM0] - f[dMP0]) + (f[dPP0] - f[dMM0])))) +
            (f[dP00] - f[dM00]);
 }
 template <class R>
-__device__ __forceinline__ R pyramidJy(const R* f)
+__host__ __device__ __forceinline__ R pyramidJy(const R* f)
 {
     return ((((f[dPPP] - f[dMMM]) + (f[dMPM] - f[dPMP])) + ((f[dMPP] - f[dPMM]) + (f[dPPM] - f[dMMP]))) +
             (((f[d0PM] - f[d0MP]) + (f[d0PP] - f[d0MM])) + ((f[dMP0] - f[dPM0]) + (f[dPP0] - f[dMM0])))) +
            (f[d0P0] - f[d0M0]);
 }
 template <class R>
-__device__ __forceinline__ R pyramidJz(const R* f)
+__host__ __device__ __forceinline__ R pyramidJz(const R* f)
 {
     return ((((f[dPPP] - f[dMMM]) + (f[dPMP] - f[dMPM])) + ((f[dMPP] - f[dPMM]) + (f[dMMP] - f[dPPM]))) +
             (((f[d0MP] - f[d0PM]) + (f[d0PP] - f[d0MM])) + ((f[dM0P] - f[dP0M]) + (f[dP0P] - f[dM0M])))) +
@@ -143,7 +170,7 @@ __device__ __forceinline__ R pyramidJz(const R* f)
 // ------------------------------------------------------------------- K17 --
 // sixth-order correction term of K17CompressibleNavierStokes.h:320-330 / :489-500
 template <class R>
-__device__ __forceinline__ R c222Term(R m111, R m200, R m020, R m002, R m022, R m202, R m220, R m011, R m101, R m110,
+__host__ __device__ __forceinline__ R c222Term(R m111, R m200, R m020, R m002, R m022, R m202, R m220, R m011, R m101, R m110,
                                       R m211, R m121, R m112, R m120, R m102, R m210, R m012, R m201, R m021,
                                       R oneOverRho, R drho)
 {
@@ -160,54 +187,98 @@ __device__ __forceinline__ R c222Term(R m111, R m200, R m020, R m002, R m022, R 
            R(1) / R(27) * ((drho * drho - drho) * oneOverRho * oneOverRho);
 }
 
+template <class R>
+__host__ __device__ __forceinline__ R limiterQuotient(R x, R y)
+{
+    return x / y;
+}
+#ifdef __CUDA_ARCH__
+template <>
+__device__ __forceinline__ float limiterQuotient<float>(float x, float y)
+{
+    return __fdividef(x, y);
+}
+#endif
+
 // One K17 collision on f[27] (pre-collision in, post-collision out).
 // (fx, fy, fz) is half the acceleration already scaled by the level factor
 // (RunCollision.cuh:111-113).  Returns drho and the force-shifted velocity.
 template <class R>
-__device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, R fx, R fy, R fz, R& drho_out, R& vx_out,
-                                           R& vy_out, R& vz_out)
+__host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, R fx, R fy, R fz, R& drho_out,
+                                                    R& vx_out, R& vy_out, R& vz_out)
 {
-    const R drho = pyramidDensity(f);
+    // sums over the nine z lines (x, y fixed): s = a + b + c, m2 = a + c, d = c - a
+#define VFB_ZLINE(XY, A, B, C)                                                                                         \
+    const R m2_##XY = f[A] + f[C];                                                                                     \
+    const R d_##XY = f[C] - f[A];                                                                                      \
+    const R s_##XY = m2_##XY + f[B];
+    VFB_ZLINE(MM, dMMM, dMM0, dMMP)
+    VFB_ZLINE(M0, dM0M, dM00, dM0P)
+    VFB_ZLINE(MP, dMPM, dMP0, dMPP)
+    VFB_ZLINE(0M, d0MM, d0M0, d0MP)
+    VFB_ZLINE(00, d00M, d000, d00P)
+    VFB_ZLINE(0P, d0PM, d0P0, d0PP)
+    VFB_ZLINE(PM, dPMM, dPM0, dPMP)
+    VFB_ZLINE(P0, dP0M, dP00, dP0P)
+    VFB_ZLINE(PP, dPPM, dPP0, dPPP)
+#undef VFB_ZLINE
+    const R drho = (((s_MM + s_PP) + (s_MP + s_PM)) + ((s_M0 + s_P0) + (s_0M + s_0P))) + s_00;
+    const R jx = ((s_PM + s_PP) - (s_MM + s_MP)) + (s_P0 - s_M0);
+    const R jy = ((s_MP + s_PP) - (s_MM + s_PM)) + (s_0P - s_0M);
+    const R jz = (((d_MM + d_PP) + (d_MP + d_PM)) + ((d_M0 + d_P0) + (d_0M + d_0P))) + d_00;
     const R oneOverRho = R(1) / (drho + R(1));
-    R vvx = pyramidJx(f) * oneOverRho;
-    R vvy = pyramidJy(f) * oneOverRho;
-    R vvz = pyramidJz(f) * oneOverRho;
-    vvx += fx;
-    vvy += fy;
-    vvz += fz;
+    const R vvx = fma(jx, oneOverRho, fx);
+    const R vvy = fma(jy, oneOverRho, fy);
+    const R vvz = fma(jz, oneOverRho, fz);
     const R vx2 = vvx * vvx, vy2 = vvy * vvy, vz2 = vvz * vvz;
 
-    // forward chimera, z then y then x (:190-222)
-    fwdK(f[dMMM], f[dMM0], f[dMMP], vvz, vz2, R(36), R(1) / R(36));
-    fwdK(f[dM0M], f[dM00], f[dM0P], vvz, vz2, R(9), R(1) / R(9));
-    fwdK(f[dMPM], f[dMP0], f[dMPP], vvz, vz2, R(36), R(1) / R(36));
-    fwdK(f[d0MM], f[d0M0], f[d0MP], vvz, vz2, R(9), R(1) / R(9));
-    fwdK(f[d00M], f[d000], f[d00P], vvz, vz2, R(9) / R(4), R(4) / R(9));
-    fwdK(f[d0PM], f[d0P0], f[d0PP], vvz, vz2, R(9), R(1) / R(9));
-    fwdK(f[dPMM], f[dPM0], f[dPMP], vvz, vz2, R(36), R(1) / R(36));
-    fwdK(f[dP0M], f[dP00], f[dP0P], vvz, vz2, R(9), R(1) / R(9));
-    fwdK(f[dPPM], f[dPP0], f[dPPP], vvz, vz2, R(36), R(1) / R(36));
-
-    fwdK(f[dMMM], f[dM0M], f[dMPM], vvy, vy2, R(6), R(1) / R(6));
-    fwd0(f[dMM0], f[dM00], f[dMP0], vvy, vy2);
-    fwdK(f[dMMP], f[dM0P], f[dMPP], vvy, vy2, R(18), R(1) / R(18));
-    fwdK(f[d0MM], f[d00M], f[d0PM], vvy, vy2, R(3) / R(2), R(2) / R(3));
-    fwd0(f[d0M0], f[d000], f[d0P0], vvy, vy2);
-    fwdK(f[d0MP], f[d00P], f[d0PP], vvy, vy2, R(9) / R(2), R(2) / R(9));
-    fwdK(f[dPMM], f[dP0M], f[dPPM], vvy, vy2, R(6), R(1) / R(6));
-    fwd0(f[dPM0], f[dP00], f[dPP0], vvy, vy2);
-    fwdK(f[dPMP], f[dP0P], f[dPPP], vvy, vy2, R(18), R(1) / R(18));
-
-    fwdK(f[dMMM], f[d0MM], f[dPMM], vvx, vx2, R(1), R(1));
-    fwd0(f[dM0M], f[d00M], f[dP0M], vvx, vx2);
-    fwdK(f[dMPM], f[d0PM], f[dPPM], vvx, vx2, R(3), R(1) / R(3));
-    fwd0(f[dMM0], f[d0M0], f[dPM0], vvx, vx2);
-    fwd0(f[dM00], f[d000], f[dP00], vvx, vx2);
-    fwd0(f[dMP0], f[d0P0], f[dPP0], vvx, vx2);
-    fwdK(f[dMMP], f[d0MP], f[dPMP], vvx, vx2, R(3), R(1) / R(3));
-    fwd0(f[dM0P], f[d00P], f[dP0P], vvx, vx2);
-    // Kinverse = 3 with K = 1/9, as the reference header has it (:222)
-    fwdK(f[dMPP], f[d0PP], f[dPPP], vvx, vx2, R(3), R(1) / R(9));
+    // forward chimera in z (:190-199) from the line sums
+    {
+        const Sweep<R> w(vvz);
+#define VFB_ZFWD(XY, A, B, C, K)                                                                                       \
+    {                                                                                                                  \
+        const R m0K = s_##XY + (K);                                                                                    \
+        f[A] = s_##XY;                                                                                                 \
+        f[B] = fma(w.nvv, m0K, d_##XY);                                                                                \
+        f[C] = fma(w.v2, m0K, fma(w.n2vv, d_##XY, m2_##XY));                                                           \
+    }
+        VFB_ZFWD(MM, dMMM, dMM0, dMMP, R(1) / R(36))
+        VFB_ZFWD(M0, dM0M, dM00, dM0P, R(1) / R(9))
+        VFB_ZFWD(MP, dMPM, dMP0, dMPP, R(1) / R(36))
+        VFB_ZFWD(0M, d0MM, d0M0, d0MP, R(1) / R(9))
+        VFB_ZFWD(00, d00M, d000, d00P, R(4) / R(9))
+        VFB_ZFWD(0P, d0PM, d0P0, d0PP, R(1) / R(9))
+        VFB_ZFWD(PM, dPMM, dPM0, dPMP, R(1) / R(36))
+        VFB_ZFWD(P0, dP0M, dP00, dP0P, R(1) / R(9))
+        VFB_ZFWD(PP, dPPM, dPP0, dPPP, R(1) / R(36))
+#undef VFB_ZFWD
+    }
+    // y (:202-210)
+    {
+        const Sweep<R> w(vvy);
+        fwd(f[dMMM], f[dM0M], f[dMPM], w, R(1) / R(6));
+        fwd(f[dMM0], f[dM00], f[dMP0], w, R(0));
+        fwd(f[dMMP], f[dM0P], f[dMPP], w, R(1) / R(18));
+        fwd(f[d0MM], f[d00M], f[d0PM], w, R(2) / R(3));
+        fwd(f[d0M0], f[d000], f[d0P0], w, R(0));
+        fwd(f[d0MP], f[d00P], f[d0PP], w, R(2) / R(9));
+        fwd(f[dPMM], f[dP0M], f[dPPM], w, R(1) / R(6));
+        fwd(f[dPM0], f[dP00], f[dPP0], w, R(0));
+        fwd(f[dPMP], f[dP0P], f[dPPP], w, R(1) / R(18));
+    }
+    // x (:213-222)
+    {
+        const Sweep<R> w(vvx);
+        fwd(f[dMMM], f[d0MM], f[dPMM], w, R(1));
+        fwd(f[dM0M], f[d00M], f[dP0M], w, R(0));
+        fwd(f[dMPM], f[d0PM], f[dPPM], w, R(1) / R(3));
+        fwd(f[dMM0], f[d0M0], f[dPM0], w, R(0));
+        fwd(f[dM00], f[d000], f[dP00], w, R(0));
+        fwd(f[dMP0], f[d0P0], f[dPP0], w, R(0));
+        fwd(f[dMMP], f[d0MP], f[dPMP], w, R(1) / R(3));
+        fwd(f[dM0P], f[d00P], f[dP0P], w, R(0));
+        fwdThird(f[dMPP], f[d0PP], f[dPPP], w);
+    }
 
     // moment names: m_abc is stored in the slot of direction (a-1, b-1, c-1)
     R& m000 = f[dMMM];
@@ -267,19 +338,19 @@ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, R fx, R f
 
     // third order with quartic limiter (:404-417)
     R w;
-    w = r.Oxyz + r.oneMinusOxyz * fabs(m111) / (fabs(m111) + r.qlD);
+    w = fma(r.oneMinusOxyz, limiterQuotient(fabs(m111), fabs(m111) + r.qlD), r.Oxyz);
     m111 += w * (-m111);
-    w = r.OxyyPxzz + r.oneMinusOxyyPxzz * fabs(mxxyPyzz) / (fabs(mxxyPyzz) + r.qlP);
+    w = fma(r.oneMinusOxyyPxzz, limiterQuotient(fabs(mxxyPyzz), fabs(mxxyPyzz) + r.qlP), r.OxyyPxzz);
     mxxyPyzz += w * (-mxxyPyzz);
-    w = r.OxyyMxzz + r.oneMinusOxyyMxzz * fabs(mxxyMyzz) / (fabs(mxxyMyzz) + r.qlM);
+    w = fma(r.oneMinusOxyyMxzz, limiterQuotient(fabs(mxxyMyzz), fabs(mxxyMyzz) + r.qlM), r.OxyyMxzz);
     mxxyMyzz += w * (-mxxyMyzz);
-    w = r.OxyyPxzz + r.oneMinusOxyyPxzz * fabs(mxxzPyyz) / (fabs(mxxzPyyz) + r.qlP);
+    w = fma(r.oneMinusOxyyPxzz, limiterQuotient(fabs(mxxzPyyz), fabs(mxxzPyyz) + r.qlP), r.OxyyPxzz);
     mxxzPyyz += w * (-mxxzPyyz);
-    w = r.OxyyMxzz + r.oneMinusOxyyMxzz * fabs(mxxzMyyz) / (fabs(mxxzMyyz) + r.qlM);
+    w = fma(r.oneMinusOxyyMxzz, limiterQuotient(fabs(mxxzMyyz), fabs(mxxzMyyz) + r.qlM), r.OxyyMxzz);
     mxxzMyyz += w * (-mxxzMyyz);
-    w = r.OxyyPxzz + r.oneMinusOxyyPxzz * fabs(mxyyPxzz) / (fabs(mxyyPxzz) + r.qlP);
+    w = fma(r.oneMinusOxyyPxzz, limiterQuotient(fabs(mxyyPxzz), fabs(mxyyPxzz) + r.qlP), r.OxyyPxzz);
     mxyyPxzz += w * (-mxyyPxzz);
-    w = r.OxyyMxzz + r.oneMinusOxyyMxzz * fabs(mxyyMxzz) / (fabs(mxyyMxzz) + r.qlM);
+    w = fma(r.oneMinusOxyyMxzz, limiterQuotient(fabs(mxyyMxzz), fabs(mxyyMxzz) + r.qlM), r.OxyyMxzz);
     mxyyMxzz += w * (-mxyyMxzz);
 
     // back to single moments (:431-441)
@@ -330,35 +401,42 @@ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, R fx, R f
     m001 = -m001;
 
     // backward chimera, x then y then z (:525-557)
-    bwdK(m000, m100, m200, vvx, vx2, R(1), R(1));
-    bwd0(m010, m110, m210, vvx, vx2);
-    bwdK(m020, m120, m220, vvx, vx2, R(3), R(1) / R(3));
-    bwd0(m001, m101, m201, vvx, vx2);
-    bwd0(m011, m111, m211, vvx, vx2);
-    bwd0(m021, m121, m221, vvx, vx2);
-    bwdK(m002, m102, m202, vvx, vx2, R(3), R(1) / R(3));
-    bwd0(m012, m112, m212, vvx, vx2);
-    bwdK(m022, m122, m222, vvx, vx2, R(9), R(1) / R(9));
-
-    bwdK(m000, m010, m020, vvy, vy2, R(6), R(1) / R(6));
-    bwd0(m001, m011, m021, vvy, vy2);
-    bwdK(m002, m012, m022, vvy, vy2, R(18), R(1) / R(18));
-    bwdK(m100, m110, m120, vvy, vy2, R(3) / R(2), R(2) / R(3));
-    bwd0(m101, m111, m121, vvy, vy2);
-    bwdK(m102, m112, m122, vvy, vy2, R(9) / R(2), R(2) / R(9));
-    bwdK(m200, m210, m220, vvy, vy2, R(6), R(1) / R(6));
-    bwd0(m201, m211, m221, vvy, vy2);
-    bwdK(m202, m212, m222, vvy, vy2, R(18), R(1) / R(18));
-
-    bwdK(m000, m001, m002, vvz, vz2, R(36), R(1) / R(36));
-    bwdK(m010, m011, m012, vvz, vz2, R(9), R(1) / R(9));
-    bwdK(m020, m021, m022, vvz, vz2, R(36), R(1) / R(36));
-    bwdK(m100, m101, m102, vvz, vz2, R(9), R(1) / R(9));
-    bwdK(m110, m111, m112, vvz, vz2, R(9) / R(4), R(4) / R(9));
-    bwdK(m120, m121, m122, vvz, vz2, R(9), R(1) / R(9));
-    bwdK(m200, m201, m202, vvz, vz2, R(36), R(1) / R(36));
-    bwdK(m210, m211, m212, vvz, vz2, R(9), R(1) / R(9));
-    bwdK(m220, m221, m222, vvz, vz2, R(36), R(1) / R(36));
+    {
+        const Sweep<R> w(vvx);
+        bwd(m000, m100, m200, w, R(1));
+        bwd(m010, m110, m210, w, R(0));
+        bwd(m020, m120, m220, w, R(1) / R(3));
+        bwd(m001, m101, m201, w, R(0));
+        bwd(m011, m111, m211, w, R(0));
+        bwd(m021, m121, m221, w, R(0));
+        bwd(m002, m102, m202, w, R(1) / R(3));
+        bwd(m012, m112, m212, w, R(0));
+        bwd(m022, m122, m222, w, R(1) / R(9));
+    }
+    {
+        const Sweep<R> w(vvy);
+        bwd(m000, m010, m020, w, R(1) / R(6));
+        bwd(m001, m011, m021, w, R(0));
+        bwd(m002, m012, m022, w, R(1) / R(18));
+        bwd(m100, m110, m120, w, R(2) / R(3));
+        bwd(m101, m111, m121, w, R(0));
+        bwd(m102, m112, m122, w, R(2) / R(9));
+        bwd(m200, m210, m220, w, R(1) / R(6));
+        bwd(m201, m211, m221, w, R(0));
+        bwd(m202, m212, m222, w, R(1) / R(18));
+    }
+    {
+        const Sweep<R> w(vvz);
+        bwd(m000, m001, m002, w, R(1) / R(36));
+        bwd(m010, m011, m012, w, R(1) / R(9));
+        bwd(m020, m021, m022, w, R(1) / R(36));
+        bwd(m100, m101, m102, w, R(1) / R(9));
+        bwd(m110, m111, m112, w, R(4) / R(9));
+        bwd(m120, m121, m122, w, R(1) / R(9));
+        bwd(m200, m201, m202, w, R(1) / R(36));
+        bwd(m210, m211, m212, w, R(1) / R(9));
+        bwd(m220, m221, m222, w, R(1) / R(36));
+    }
 
     drho_out = drho;
     vx_out = vvx;
@@ -368,7 +446,7 @@ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, R fx, R f
 
 // ------------------------------------------------------------------- BGK --
 template <class R>
-__device__ __forceinline__ void bgkCollide(R* f, R omega)
+__host__ __device__ __forceinline__ void bgkCollide(R* f, R omega)
 {
     R drho = (f[dPPP] + f[dMMM]) + (f[dMMP] + f[dPPM]) + (f[dPMP] + f[dMPM]) + (f[dMPP] + f[dPMM]) +
              (f[dPP0] + f[dMM0]) + (f[dMP0] + f[dPM0]) + (f[dP0P] + f[dM0M]) + (f[dP0M] + f[dM0P]) +

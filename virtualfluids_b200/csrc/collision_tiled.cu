@@ -62,6 +62,15 @@ template <class S>
 struct TiledArgs {
     using R = typename Storage<S>::R;
     S* dist;
+    // per direction, for the parity of the launch: the global address of the
+    // direction's location of node 0 (dist + slot * N + location stride), the
+    // lead of a tile's segment (tiles start at multiples of 16 bytes), the
+    // shared-memory offset of node k0 and the bytes of one bulk copy
+    S* gbase[27];
+    int lead[27];
+    int smemOff[27];
+    uint32_t bytes[27];
+    uint32_t totalBytes;
     unsigned long long N;
     const uint32_t* __restrict__ nX;
     const uint32_t* __restrict__ nY;
@@ -94,21 +103,10 @@ template <class S, bool EVEN>
 __device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t k0, S* stage, uint64_t* bar)
 {
     using G = TileShape<S>;
-    uint32_t total = 0;
+    tma::mbarArriveExpectTx(bar, a.totalBytes);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        const unsigned long long base = (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
-        const uint32_t lead = (uint32_t)(base % G::E);
-        total += ((lead + G::T + G::E - 1) / G::E) * G::E * (uint32_t)sizeof(S);
-    }
-    tma::mbarArriveExpectTx(bar, total);
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        const unsigned long long base = (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
-        const uint32_t lead = (uint32_t)(base % G::E);
-        const uint32_t bytes = ((lead + G::T + G::E - 1) / G::E) * G::E * (uint32_t)sizeof(S);
-        tma::bulkLoad(stage + d * G::CAP, a.dist + (base - lead), bytes, bar);
-    }
+    for (int d = 0; d < 27; ++d)
+        tma::bulkLoad(stage + d * G::CAP, a.gbase[d] + (k0 - (uint32_t)a.lead[d]), a.bytes[d], bar);
 }
 
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
@@ -187,21 +185,16 @@ __global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) til
             if (!ok)
                 abort = 1;
             if (ok && ((curMask >> lane) & 1u)) {
-                const uint32_t k0 = (uint32_t)cur.x;
-                const uint32_t k = k0 + tid;
-                const S* st = stages[s];
+                const uint32_t k = (uint32_t)cur.x + tid;
+                const S* st = stages[s] + tid;
                 R f[27];
 #pragma unroll
-                for (int d = 0; d < 27; ++d) {
-                    const unsigned long long base =
-                        (unsigned long long)slot<EVEN>(d) * a.N + k0 + locShift(loc(d), a.sy, a.sz);
-                    f[d] = Storage<S>::load(st + d * G::CAP + (uint32_t)(base % G::E) + tid);
-                }
+                for (int d = 0; d < 27; ++d)
+                    f[d] = Storage<S>::load(st + a.smemOff[d]);
                 collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
                 for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.dist + (unsigned long long)slot<EVEN>(d) * a.N + k + locShift(loc(d), a.sy, a.sz),
-                                      f[inv(d)]);
+                    Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
             }
         }
         __syncthreads();
@@ -337,7 +330,7 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     const uint64_t minActive = T / 4;
     size_t i = 0;
     while (i < cand.size()) {
-        const uint64_t k0 = cand[i];
+        const uint64_t k0 = cand[i] - cand[i] % E; // bulk sources then share one lead per direction
         size_t j = i;
         while (j < cand.size() && cand[j] < k0 + T)
             ++j;
@@ -450,6 +443,17 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     if (p.nTiles == 0)
         return VFB_OK;
     const bool even = c->isEvenTimestep != 0;
+    using G = TileShape<S>;
+    a.totalBytes = 0;
+    for (int d = 0; d < 27; ++d) {
+        const unsigned long long off =
+            (unsigned long long)(even ? d : inv(d)) * p.N + locShift(loc(d), p.sy, p.sz);
+        a.gbase[d] = a.dist + off;
+        a.lead[d] = (int)(off % G::E);
+        a.smemOff[d] = d * G::CAP + a.lead[d];
+        a.bytes[d] = (uint32_t)(((a.lead[d] + G::T + G::E - 1) / G::E) * G::E * (int)sizeof(S));
+        a.totalBytes += a.bytes[d];
+    }
     if (op == Op::BGK)
         return even ? launchTiledT<S, true, Op::BGK, false, false>(a, stream)
                     : launchTiledT<S, false, Op::BGK, false, false>(a, stream);
