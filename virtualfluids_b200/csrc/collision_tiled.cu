@@ -51,7 +51,7 @@ struct TileShape {
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
     static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
     static constexpr int STAGE_BYTES = 27 * CAP * (int)sizeof(S);
-    static constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 16;        // two stages + two mbarriers
+    static constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 32;        // two stages + full / empty mbarriers
     static constexpr int MASK_WORDS = T / 32;
     static constexpr int MIN_BLOCKS = sizeof(S) == 8 ? 2 : 3;       // resident blocks per SM the registers are sized for
 };
@@ -136,21 +136,27 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
     }
 }
 
+// Pipeline of one block: thread 0 is the producer; before refilling a stage
+// it waits on the stage's "empty" barrier, on which every warp arrives once it
+// has read the stage, then arms the "full" barrier with the tile's byte count
+// and issues the 27 bulk copies.  Every warp waits on "full", collides its 32
+// nodes and arrives on "empty".  Warps never wait for each other otherwise.
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
 __global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) tiledKernel(const TiledArgs<S> a)
 {
     using R = typename Storage<S>::R;
     using G = TileShape<S>;
+    constexpr int WARPS = G::T / 32;
     extern __shared__ __align__(128) unsigned char smemRaw[];
-    S* stages[2] = { reinterpret_cast<S*>(smemRaw), reinterpret_cast<S*>(smemRaw + G::STAGE_BYTES) };
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smemRaw + 2 * G::STAGE_BYTES);
-    __shared__ int abort;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smemRaw + 2 * G::STAGE_BYTES);
+    uint64_t* empty = full + 2;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
-        abort = 0;
-        tma::mbarInit(&bars[0], 1);
-        tma::mbarInit(&bars[1], 1);
+        tma::mbarInit(&full[0], 1);
+        tma::mbarInit(&full[1], 1);
+        tma::mbarInit(&empty[0], WARPS);
+        tma::mbarInit(&empty[1], WARPS);
         tma::fenceBarrierInit();
     }
     __syncthreads();
@@ -158,55 +164,76 @@ __global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) til
     uint32_t t = blockIdx.x;
     if (t >= a.nTiles)
         return;
-    uint32_t uses[2] = { 0, 0 };
-    int s = 0;
+    const uint32_t stride = gridDim.x;
+    // descriptors of tiles j and j+1, and this warp's active-lane masks
     TileDesc cur = a.tiles[t];
+    TileDesc nxt = t + stride < a.nTiles ? a.tiles[t + stride] : make_int2(0, 0);
     uint32_t curMask = a.masks[(size_t)cur.y * G::MASK_WORDS + warp];
-    if (tid == 0)
-        issueTile<S, EVEN>(a, (uint32_t)cur.x, stages[0], &bars[0]);
+    uint32_t fills[2] = { 0, 0 }, reads[2] = { 0, 0 };
+    if (tid == 0) {
+        tma::mbarArriveExpectTx(&full[0], a.totalBytes);
+        for (int d = 0; d < 27; ++d)
+            tma::bulkLoad(reinterpret_cast<S*>(smemRaw) + d * G::CAP, a.gbase[d] + ((uint32_t)cur.x - (uint32_t)a.lead[d]),
+                          a.bytes[d], &full[0]);
+    }
+    fills[0] = 1;
+    int s = 0;
+    bool failed = false;
 
     while (true) {
-        const uint32_t tn = t + gridDim.x;
-        TileDesc nxt = make_int2(0, 0);
+        const uint32_t tn = t + stride;
+        const bool more = tn < a.nTiles;
         uint32_t nxtMask = 0;
-        if (tn < a.nTiles) {
-            nxt = a.tiles[tn];
+        if (more) {
             nxtMask = a.masks[(size_t)nxt.y * G::MASK_WORDS + warp];
             if (tid == 0) {
-                tma::fenceProxyAsync();
-                issueTile<S, EVEN>(a, (uint32_t)nxt.x, stages[s ^ 1], &bars[s ^ 1]);
+                const int sn = s ^ 1;
+                // the stage was last read for the tile before this one
+                if (fills[sn] > 0 && !tma::mbarWait(&empty[sn], (fills[sn] - 1) & 1u, kWaitLimit))
+                    failed = true;
+                if (!failed) {
+                    tma::fenceProxyAsync();
+                    tma::mbarArriveExpectTx(&full[sn], a.totalBytes);
+                    S* dst = reinterpret_cast<S*>(smemRaw + sn * G::STAGE_BYTES);
+                    for (int d = 0; d < 27; ++d)
+                        tma::bulkLoad(dst + d * G::CAP, a.gbase[d] + ((uint32_t)nxt.x - (uint32_t)a.lead[d]), a.bytes[d],
+                                      &full[sn]);
+                }
             }
+            if (s == 0)
+                fills[1]++;
+            else
+                fills[0]++;
         }
+        const TileDesc after = tn + stride < a.nTiles ? a.tiles[tn + stride] : make_int2(0, 0);
 
-        {
-            // node k0 + tid, active if its mask bit is set
-            const bool ok = tma::mbarWait(&bars[s], uses[s] & 1u, kWaitLimit);
-            uses[s]++;
-            if (!ok)
-                abort = 1;
-            if (ok && ((curMask >> lane) & 1u)) {
-                const uint32_t k = (uint32_t)cur.x + tid;
-                const S* st = stages[s] + tid;
-                R f[27];
-#pragma unroll
-                for (int d = 0; d < 27; ++d)
-                    f[d] = Storage<S>::load(st + a.smemOff[d]);
-                collideNode<S, EVEN, OP, WM, BF>(a, f, k);
-#pragma unroll
-                for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
-            }
-        }
-        __syncthreads();
-        if (abort) {
-            if (tid == 0)
+        const bool ok = tma::mbarWait(&full[s], reads[s] & 1u, kWaitLimit);
+        reads[s]++;
+        if (!__all_sync(0xffffffffu, ok) || __any_sync(0xffffffffu, failed)) {
+            if (lane == 0)
                 atomicExch(a.errorFlag, 1);
             return;
         }
-        if (tn >= a.nTiles)
+        if ((curMask >> lane) & 1u) {
+            const uint32_t k = (uint32_t)cur.x + tid;
+            const S* st = reinterpret_cast<const S*>(smemRaw + s * G::STAGE_BYTES) + tid;
+            R f[27];
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                f[d] = Storage<S>::load(st + a.smemOff[d]);
+            collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+        }
+        __syncwarp();
+        if (lane == 0)
+            tma::mbarArrive(&empty[s]);
+        if (!more)
             break;
         t = tn;
         cur = nxt;
+        nxt = after;
         curMask = nxtMask;
         s ^= 1;
     }

@@ -43,6 +43,12 @@ __device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// plain arrival (no transaction count)
+__device__ __forceinline__ void mbarArrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t parity)
 {
     uint32_t done;
