@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -44,16 +45,19 @@ using TileDesc = int2;
 
 constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
 
-// tile width (nodes per block iteration) by storage size
-template <class S>
-struct TileShape {
-    static constexpr int T = sizeof(S) == 8 ? 128 : 256;          // threads per block = nodes per tile
+// Tile shape: T nodes (= threads) per tile, STAGES shared-memory stages (a
+// prefetch depth of STAGES - 1 tiles), MINB resident blocks the registers are
+// sized for.
+template <class S, int T_, int STAGES_, int MINB_>
+struct TileCfg {
+    static constexpr int T = T_;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int MINB = MINB_;
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
     static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
     static constexpr int STAGE_BYTES = 27 * CAP * (int)sizeof(S);
-    static constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 32;        // two stages + full / empty mbarriers
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 16 * STAGES; // stages + full / empty mbarriers
     static constexpr int MASK_WORDS = T / 32;
-    static constexpr int MIN_BLOCKS = sizeof(S) == 8 ? 2 : 3;       // resident blocks per SM the registers are sized for
 };
 
 enum class Op { K17, BGK };
@@ -72,13 +76,9 @@ struct TiledArgs {
     uint32_t bytes[27];
     uint32_t totalBytes;
     unsigned long long N;
-    const uint32_t* __restrict__ nX;
-    const uint32_t* __restrict__ nY;
-    const uint32_t* __restrict__ nZ;
     const TileDesc* __restrict__ tiles;
     const uint32_t* __restrict__ masks;
     uint32_t nTiles;
-    uint32_t sy, sz;
     K17Rates<R> rates;
     R fx, fy, fz, gfx, gfy, gfz, forceFactor;
     R* rho;
@@ -98,15 +98,16 @@ __host__ __device__ __forceinline__ uint32_t locShift(int l, uint32_t sy, uint32
     return (uint32_t)(l & 1) + ((l & 2) ? sy : 0u) + ((l & 4) ? sz : 0u);
 }
 
-// thread 0 arms the stage barrier and issues the 27 bulk copies of a tile
-template <class S, bool EVEN>
-__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t k0, S* stage, uint64_t* bar)
+// thread 0 arms a stage's "full" barrier and issues the tile's 27 bulk copies
+template <class S, class C>
+__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t k0, unsigned char* smem, int stage,
+                                          uint64_t* full)
 {
-    using G = TileShape<S>;
-    tma::mbarArriveExpectTx(bar, a.totalBytes);
+    S* dst = reinterpret_cast<S*>(smem + stage * C::STAGE_BYTES);
+    tma::mbarArriveExpectTx(&full[stage], a.totalBytes);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        tma::bulkLoad(stage + d * G::CAP, a.gbase[d] + (k0 - (uint32_t)a.lead[d]), a.bytes[d], bar);
+        tma::bulkLoad(dst + d * C::CAP, a.gbase[d] + (k0 - (uint32_t)a.lead[d]), a.bytes[d], &full[stage]);
 }
 
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
@@ -136,79 +137,77 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
     }
 }
 
-// Pipeline of one block: thread 0 is the producer; before refilling a stage
+// Pipeline of one block: thread 0 is the producer.  Before refilling a stage
 // it waits on the stage's "empty" barrier, on which every warp arrives once it
-// has read the stage, then arms the "full" barrier with the tile's byte count
-// and issues the 27 bulk copies.  Every warp waits on "full", collides its 32
-// nodes and arrives on "empty".  Warps never wait for each other otherwise.
-template <class S, bool EVEN, Op OP, bool WM, bool BF>
-__global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) tiledKernel(const TiledArgs<S> a)
+// has read the stage, then arms the stage's "full" barrier with the tile's
+// byte count and issues the 27 bulk copies, STAGES - 1 tiles ahead of the
+// consumers.  Every warp waits on "full", collides its 32 nodes, stores them
+// and arrives on "empty".  Warps never wait for each other otherwise.
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+__global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> a)
 {
     using R = typename Storage<S>::R;
-    using G = TileShape<S>;
-    constexpr int WARPS = G::T / 32;
+    constexpr int WARPS = C::T / 32;
+    constexpr int ST = C::STAGES;
     extern __shared__ __align__(128) unsigned char smemRaw[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smemRaw + 2 * G::STAGE_BYTES);
-    uint64_t* empty = full + 2;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smemRaw + ST * C::STAGE_BYTES);
+    uint64_t* empty = full + ST;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
-        tma::mbarInit(&full[0], 1);
-        tma::mbarInit(&full[1], 1);
-        tma::mbarInit(&empty[0], WARPS);
-        tma::mbarInit(&empty[1], WARPS);
+        for (int i = 0; i < ST; ++i) {
+            tma::mbarInit(&full[i], 1);
+            tma::mbarInit(&empty[i], WARPS);
+        }
         tma::fenceBarrierInit();
     }
     __syncthreads();
 
-    uint32_t t = blockIdx.x;
-    if (t >= a.nTiles)
+    const uint32_t t0 = blockIdx.x, stride = gridDim.x;
+    if (t0 >= a.nTiles)
         return;
-    const uint32_t stride = gridDim.x;
-    // descriptors of tiles j and j+1, and this warp's active-lane masks
-    TileDesc cur = a.tiles[t];
-    TileDesc nxt = t + stride < a.nTiles ? a.tiles[t + stride] : make_int2(0, 0);
-    uint32_t curMask = a.masks[(size_t)cur.y * G::MASK_WORDS + warp];
-    uint32_t fills[2] = { 0, 0 }, reads[2] = { 0, 0 };
+    const uint32_t mine = (a.nTiles - t0 + stride - 1) / stride; // tiles of this block
+    auto tileOf = [&](uint32_t j) { return a.tiles[t0 + j * stride]; };
+
+    // producer: first STAGES - 1 tiles
+    TileDesc pnext = make_int2(0, 0); // descriptor of the next tile to issue
     if (tid == 0) {
-        tma::mbarArriveExpectTx(&full[0], a.totalBytes);
-        for (int d = 0; d < 27; ++d)
-            tma::bulkLoad(reinterpret_cast<S*>(smemRaw) + d * G::CAP, a.gbase[d] + ((uint32_t)cur.x - (uint32_t)a.lead[d]),
-                          a.bytes[d], &full[0]);
+        const uint32_t pre = mine < (uint32_t)(ST - 1) ? mine : (uint32_t)(ST - 1);
+        for (uint32_t q = 0; q < pre; ++q)
+            issueTile<S, C>(a, (uint32_t)tileOf(q).x, smemRaw, (int)q, full);
+        if ((uint32_t)(ST - 1) < mine)
+            pnext = tileOf(ST - 1);
     }
-    fills[0] = 1;
-    int s = 0;
+    TileDesc cur = tileOf(0);
+    uint32_t curMask = a.masks[(size_t)cur.y * C::MASK_WORDS + warp];
     bool failed = false;
 
-    while (true) {
-        const uint32_t tn = t + stride;
-        const bool more = tn < a.nTiles;
-        uint32_t nxtMask = 0;
-        if (more) {
-            nxtMask = a.masks[(size_t)nxt.y * G::MASK_WORDS + warp];
-            if (tid == 0) {
-                const int sn = s ^ 1;
-                // the stage was last read for the tile before this one
-                if (fills[sn] > 0 && !tma::mbarWait(&empty[sn], (fills[sn] - 1) & 1u, kWaitLimit))
+    for (uint32_t j = 0; j < mine; ++j) {
+        const int s = (int)(j % ST);
+        // producer: tile j + ST - 1 into the stage tile j - 1 used
+        if (tid == 0) {
+            const uint32_t q = j + ST - 1;
+            if (q < mine) {
+                const int sq = (int)(q % ST);
+                if (q >= (uint32_t)ST && !tma::mbarWait(&empty[sq], ((q - ST) / ST) & 1u, kWaitLimit))
                     failed = true;
                 if (!failed) {
                     tma::fenceProxyAsync();
-                    tma::mbarArriveExpectTx(&full[sn], a.totalBytes);
-                    S* dst = reinterpret_cast<S*>(smemRaw + sn * G::STAGE_BYTES);
-                    for (int d = 0; d < 27; ++d)
-                        tma::bulkLoad(dst + d * G::CAP, a.gbase[d] + ((uint32_t)nxt.x - (uint32_t)a.lead[d]), a.bytes[d],
-                                      &full[sn]);
+                    issueTile<S, C>(a, (uint32_t)pnext.x, smemRaw, sq, full);
                 }
+                if (q + 1 < mine)
+                    pnext = tileOf(q + 1);
             }
-            if (s == 0)
-                fills[1]++;
-            else
-                fills[0]++;
         }
-        const TileDesc after = tn + stride < a.nTiles ? a.tiles[tn + stride] : make_int2(0, 0);
+        // descriptor and mask of the next tile, for the next iteration
+        TileDesc nxt = cur;
+        uint32_t nxtMask = 0;
+        if (j + 1 < mine) {
+            nxt = tileOf(j + 1);
+            nxtMask = a.masks[(size_t)nxt.y * C::MASK_WORDS + warp];
+        }
 
-        const bool ok = tma::mbarWait(&full[s], reads[s] & 1u, kWaitLimit);
-        reads[s]++;
+        const bool ok = tma::mbarWait(&full[s], (j / ST) & 1u, kWaitLimit);
         if (!__all_sync(0xffffffffu, ok) || __any_sync(0xffffffffu, failed)) {
             if (lane == 0)
                 atomicExch(a.errorFlag, 1);
@@ -216,7 +215,7 @@ __global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) til
         }
         if ((curMask >> lane) & 1u) {
             const uint32_t k = (uint32_t)cur.x + tid;
-            const S* st = reinterpret_cast<const S*>(smemRaw + s * G::STAGE_BYTES) + tid;
+            const S* st = reinterpret_cast<const S*>(smemRaw + s * C::STAGE_BYTES) + tid;
             R f[27];
 #pragma unroll
             for (int d = 0; d < 27; ++d)
@@ -229,19 +228,16 @@ __global__ void __launch_bounds__(TileShape<S>::T, TileShape<S>::MIN_BLOCKS) til
         __syncwarp();
         if (lane == 0)
             tma::mbarArrive(&empty[s]);
-        if (!more)
-            break;
-        t = tn;
         cur = nxt;
-        nxt = after;
         curMask = nxtMask;
-        s ^= 1;
     }
 }
 
 // ------------------------------------------------------------------ plan --
 struct vfb_collision_plan_impl {
     int storage = 0;
+    int config = 0;      // index into kTileConfigs
+    uint32_t tileWidth = 256;
     unsigned long long N = 0;
     const uint32_t* nX = nullptr;
     const uint32_t* nY = nullptr;
@@ -290,8 +286,36 @@ cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 }
 } // namespace
 
+// Tile configurations (tile width, stages, resident blocks) the library is
+// compiled for.  Entry 0 is the default for 2- and 4-byte storage, entry 1 for
+// FP64; VFB_TILE_CONFIG=<index> selects another one at plan creation (used to
+// tune the shape on new hardware).
+struct TileConfigInfo {
+    int T, stages, minBlocks;
+    bool fp64;
+};
+static const TileConfigInfo kTileConfigs[] = {
+    { 256, 2, 3, false }, { 128, 2, 2, true }, { 256, 3, 2, false }, { 192, 3, 3, false },
+    { 160, 3, 4, false }, { 128, 4, 3, false }, { 128, 3, 3, true },
+};
+static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
+
+static int chooseTileConfig(int storage)
+{
+    const bool fp64 = storage == VFB_FP64;
+    int def = fp64 ? 1 : 0;
+    if (const char* env = std::getenv("VFB_TILE_CONFIG")) {
+        const int c = std::atoi(env);
+        if (c >= 0 && c < kNumTileConfigs && kTileConfigs[c].fp64 == fp64)
+            def = c;
+    }
+    return def;
+}
+
 static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collision_args* a, cudaStream_t stream)
 {
+    p.config = chooseTileConfig(storage);
+    p.tileWidth = (uint32_t)kTileConfigs[p.config].T;
     const unsigned long long N = a->numberOfLBnodes;
     const uint32_t nF = a->numberOfFluidNodes;
     std::vector<uint32_t> nx(N), ny(N), nz(N), fl(nF);
@@ -311,7 +335,7 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
             return setError(VFB_ERR_OUT_OF_RANGE, "fluid node %u of the list is outside the lattice", fl[i]);
 
     const int esize = vfb_storage_bytes(storage);
-    const uint64_t T = esize == 8 ? 128 : 256;
+    const uint64_t T = p.tileWidth;
     const uint64_t E = 16 / (uint64_t)esize;
     const uint32_t sy = nF ? modeStride(fl, ny) : 1, sz = nF ? modeStride(fl, nz) : 1;
     auto regular = [&](uint64_t k) -> bool {
@@ -414,25 +438,80 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     return VFB_OK;
 }
 
-template <class S, bool EVEN, Op OP, bool WM, bool BF>
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
-    using G = TileShape<S>;
     static int blocks = 0;
     if (blocks == 0) {
-        cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, EVEN, OP, WM, BF>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+        cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, C, EVEN, OP, WM, BF>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES);
         if (e != cudaSuccess)
             return setError(VFB_ERR_CUDA, "tiled kernel shared memory attribute: %s", cudaGetErrorString(e));
         int perSM = 0, device = 0, sms = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, EVEN, OP, WM, BF>, G::T, G::SMEM_BYTES);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, C, EVEN, OP, WM, BF>, C::T,
+                                                      C::SMEM_BYTES);
         blocks = std::max(1, perSM) * sms;
     }
     const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
-    tiledKernel<S, EVEN, OP, WM, BF><<<std::max(1u, grid), G::T, G::SMEM_BYTES, stream>>>(a);
+    tiledKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, C::SMEM_BYTES, stream>>>(a);
     return checkLaunch("tiled collision");
+}
+
+template <class S, class C>
+static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, cudaStream_t stream)
+{
+    a.totalBytes = 0;
+    for (int d = 0; d < 27; ++d) {
+        const unsigned long long off = (unsigned long long)(even ? d : inv(d)) * a.N + locShift(loc(d), sy, sz);
+        a.gbase[d] = a.dist + off;
+        a.lead[d] = (int)(off % C::E);
+        a.smemOff[d] = d * C::CAP + a.lead[d];
+        a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
+        a.totalBytes += a.bytes[d];
+    }
+    if (op == Op::BGK)
+        return even ? launchTiledT<S, C, true, Op::BGK, false, false>(a, stream)
+                    : launchTiledT<S, C, false, Op::BGK, false, false>(a, stream);
+    switch (tmpl) {
+    case VFB_TEMPLATE_DEFAULT:
+        return even ? launchTiledT<S, C, true, Op::K17, false, false>(a, stream)
+                    : launchTiledT<S, C, false, Op::K17, false, false>(a, stream);
+    case VFB_TEMPLATE_WRITE_MACRO_VARS:
+        return even ? launchTiledT<S, C, true, Op::K17, true, false>(a, stream)
+                    : launchTiledT<S, C, false, Op::K17, true, false>(a, stream);
+    case VFB_TEMPLATE_APPLY_BODY_FORCE:
+        return even ? launchTiledT<S, C, true, Op::K17, false, true>(a, stream)
+                    : launchTiledT<S, C, false, Op::K17, false, true>(a, stream);
+    case VFB_TEMPLATE_ALL_FEATURES:
+        return even ? launchTiledT<S, C, true, Op::K17, true, true>(a, stream)
+                    : launchTiledT<S, C, false, Op::K17, true, true>(a, stream);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "invalid collisionTemplate %d", tmpl);
+    }
+}
+
+// the tuning configurations are compiled for the default K17 and BGK passes
+// only; the other templates always use the default shape
+template <class S, class C>
+static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, cudaStream_t stream)
+{
+    if (tmpl != VFB_TEMPLATE_DEFAULT && op == Op::K17)
+        return setError(VFB_ERR_UNSUPPORTED, "tile configuration supports the default template only");
+    a.totalBytes = 0;
+    for (int d = 0; d < 27; ++d) {
+        const unsigned long long off = (unsigned long long)(even ? d : inv(d)) * a.N + locShift(loc(d), sy, sz);
+        a.gbase[d] = a.dist + off;
+        a.lead[d] = (int)(off % C::E);
+        a.smemOff[d] = d * C::CAP + a.lead[d];
+        a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
+        a.totalBytes += a.bytes[d];
+    }
+    if (op == Op::BGK)
+        return even ? launchTiledT<S, C, true, Op::BGK, false, false>(a, stream)
+                    : launchTiledT<S, C, false, Op::BGK, false, false>(a, stream);
+    return even ? launchTiledT<S, C, true, Op::K17, false, false>(a, stream)
+                : launchTiledT<S, C, false, Op::K17, false, false>(a, stream);
 }
 
 template <class S>
@@ -442,14 +521,9 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     TiledArgs<S> a;
     a.dist = static_cast<S*>(c->distributions);
     a.N = p.N;
-    a.nX = p.nX;
-    a.nY = p.nY;
-    a.nZ = p.nZ;
     a.tiles = p.tiles;
     a.masks = p.masks;
     a.nTiles = p.nTiles;
-    a.sy = p.sy;
-    a.sz = p.sz;
     a.rates = makeK17Rates<R>((R)c->omega, (R)c->quadricLimiters[0], (R)c->quadricLimiters[1],
                               (R)c->quadricLimiters[2]);
     a.forceFactor = (R)c->forceFactor;
@@ -470,34 +544,20 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     if (p.nTiles == 0)
         return VFB_OK;
     const bool even = c->isEvenTimestep != 0;
-    using G = TileShape<S>;
-    a.totalBytes = 0;
-    for (int d = 0; d < 27; ++d) {
-        const unsigned long long off =
-            (unsigned long long)(even ? d : inv(d)) * p.N + locShift(loc(d), p.sy, p.sz);
-        a.gbase[d] = a.dist + off;
-        a.lead[d] = (int)(off % G::E);
-        a.smemOff[d] = d * G::CAP + a.lead[d];
-        a.bytes[d] = (uint32_t)(((a.lead[d] + G::T + G::E - 1) / G::E) * G::E * (int)sizeof(S));
-        a.totalBytes += a.bytes[d];
-    }
-    if (op == Op::BGK)
-        return even ? launchTiledT<S, true, Op::BGK, false, false>(a, stream)
-                    : launchTiledT<S, false, Op::BGK, false, false>(a, stream);
-    switch (c->collisionTemplate) {
-    case VFB_TEMPLATE_DEFAULT:
-        return even ? launchTiledT<S, true, Op::K17, false, false>(a, stream)
-                    : launchTiledT<S, false, Op::K17, false, false>(a, stream);
-    case VFB_TEMPLATE_WRITE_MACRO_VARS:
-        return even ? launchTiledT<S, true, Op::K17, true, false>(a, stream)
-                    : launchTiledT<S, false, Op::K17, true, false>(a, stream);
-    case VFB_TEMPLATE_APPLY_BODY_FORCE:
-        return even ? launchTiledT<S, true, Op::K17, false, true>(a, stream)
-                    : launchTiledT<S, false, Op::K17, false, true>(a, stream);
-    case VFB_TEMPLATE_ALL_FEATURES:
-        return even ? launchTiledT<S, true, Op::K17, true, true>(a, stream)
-                    : launchTiledT<S, false, Op::K17, true, true>(a, stream);
-    default: return setError(VFB_ERR_INVALID_ARGUMENT, "invalid collisionTemplate %d", c->collisionTemplate);
+    const int t = c->collisionTemplate;
+    if constexpr (sizeof(S) == 8) {
+        switch (p.config) {
+        case 6: return dispatchTuning<S, TileCfg<S, 128, 3, 3>>(op, even, t, a, p.sy, p.sz, stream);
+        default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, stream);
+        }
+    } else {
+        switch (p.config) {
+        case 2: return dispatchTuning<S, TileCfg<S, 256, 3, 2>>(op, even, t, a, p.sy, p.sz, stream);
+        case 3: return dispatchTuning<S, TileCfg<S, 192, 3, 3>>(op, even, t, a, p.sy, p.sz, stream);
+        case 4: return dispatchTuning<S, TileCfg<S, 160, 3, 4>>(op, even, t, a, p.sy, p.sz, stream);
+        case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, stream);
+        default: return dispatchTiled<S, TileCfg<S, 256, 2, 3>>(op, even, t, a, p.sy, p.sz, stream);
+        }
     }
 }
 
