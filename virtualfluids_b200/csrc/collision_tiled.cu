@@ -39,8 +39,9 @@
 namespace vfb
 {
 
-// Tile descriptor: x = k0 (first sparse index of the range), y = index of the
-// tile's active-lane mask words
+// Tile descriptor: x = k0 (first sparse index of the range), y = unused; the
+// tile's active-lane mask words are masks[tile * T/32 ...], addressed by the
+// tile index so that they load independently of the descriptor
 using TileDesc = int2;
 
 constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
             pnext = tileOf(ST - 1);
     }
     TileDesc cur = tileOf(0);
-    uint32_t curMask = a.masks[(size_t)cur.y * C::MASK_WORDS + warp];
+    uint32_t curMask = a.masks[(size_t)t0 * C::MASK_WORDS + warp];
     bool failed = false;
 
     for (uint32_t j = 0; j < mine; ++j) {
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
         uint32_t nxtMask = 0;
         if (j + 1 < mine) {
             nxt = tileOf(j + 1);
-            nxtMask = a.masks[(size_t)nxt.y * C::MASK_WORDS + warp];
+            nxtMask = a.masks[(size_t)(t0 + (j + 1) * stride) * C::MASK_WORDS + warp];
         }
 
         const bool ok = tma::mbarWait(&full[s], (j / ST) & 1u, kWaitLimit);
