@@ -39,10 +39,9 @@
 namespace vfb
 {
 
-// Tile descriptor: x = k0 (first sparse index of the range), y = unused; the
-// tile's active-lane mask words are masks[tile * T/32 ...], addressed by the
-// tile index so that they load independently of the descriptor
-using TileDesc = int2;
+// Tile metadata, META_WORDS uint32 per tile: word 0 = k0 (first sparse index
+// of the range), words 1..3 unused, words 4.. = one active-lane mask per warp.
+// The producer bulk-copies it into the stage with the tile's populations.
 
 constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
 
@@ -56,9 +55,11 @@ struct TileCfg {
     static constexpr int MINB = MINB_;
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
     static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
-    static constexpr int STAGE_BYTES = 27 * CAP * (int)sizeof(S);
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 16 * STAGES; // stages + full / empty mbarriers
     static constexpr int MASK_WORDS = T / 32;
+    static constexpr int META_WORDS = 4 + MASK_WORDS;                // multiple of 4: 16-byte copies
+    static constexpr int DATA_BYTES = 27 * CAP * (int)sizeof(S);
+    static constexpr int STAGE_BYTES = DATA_BYTES + META_WORDS * 4;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 16 * STAGES; // stages + full / empty mbarriers
 };
 
 enum class Op { K17, BGK };
@@ -77,8 +78,7 @@ struct TiledArgs {
     uint32_t bytes[27];
     uint32_t totalBytes;
     unsigned long long N;
-    const TileDesc* __restrict__ tiles;
-    const uint32_t* __restrict__ masks;
+    const uint32_t* __restrict__ meta;
     uint32_t nTiles;
     K17Rates<R> rates;
     R fx, fy, fz, gfx, gfy, gfz, forceFactor;
@@ -99,13 +99,16 @@ __host__ __device__ __forceinline__ uint32_t locShift(int l, uint32_t sy, uint32
     return (uint32_t)(l & 1) + ((l & 2) ? sy : 0u) + ((l & 4) ? sz : 0u);
 }
 
-// thread 0 arms a stage's "full" barrier and issues the tile's 27 bulk copies
+// thread 0 arms a stage's "full" barrier and issues the tile's 27 bulk
+// copies plus the copy of its metadata
 template <class S, class C>
-__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t k0, unsigned char* smem, int stage,
-                                          uint64_t* full)
+__device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t tile, uint32_t k0, unsigned char* smem,
+                                          int stage, uint64_t* full)
 {
-    S* dst = reinterpret_cast<S*>(smem + stage * C::STAGE_BYTES);
-    tma::mbarArriveExpectTx(&full[stage], a.totalBytes);
+    unsigned char* base = smem + stage * C::STAGE_BYTES;
+    S* dst = reinterpret_cast<S*>(base);
+    tma::mbarArriveExpectTx(&full[stage], a.totalBytes + C::META_WORDS * 4);
+    tma::bulkLoad(base + C::DATA_BYTES, a.meta + (size_t)tile * C::META_WORDS, C::META_WORDS * 4, &full[stage]);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
         tma::bulkLoad(dst + d * C::CAP, a.gbase[d] + (k0 - (uint32_t)a.lead[d]), a.bytes[d], &full[stage]);
@@ -168,19 +171,17 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
     if (t0 >= a.nTiles)
         return;
     const uint32_t mine = (a.nTiles - t0 + stride - 1) / stride; // tiles of this block
-    auto tileOf = [&](uint32_t j) { return a.tiles[t0 + j * stride]; };
+    auto k0Of = [&](uint32_t j) { return tma::ldgOrdered(a.meta + (size_t)(t0 + j * stride) * C::META_WORDS); };
 
-    // producer: first STAGES - 1 tiles
-    TileDesc pnext = make_int2(0, 0); // descriptor of the next tile to issue
+    // producer: first STAGES - 1 tiles; pk0 = k0 of the next tile to issue
+    uint32_t pk0 = 0;
     if (tid == 0) {
         const uint32_t pre = mine < (uint32_t)(ST - 1) ? mine : (uint32_t)(ST - 1);
         for (uint32_t q = 0; q < pre; ++q)
-            issueTile<S, C>(a, (uint32_t)tileOf(q).x, smemRaw, (int)q, full);
+            issueTile<S, C>(a, t0 + q * stride, k0Of(q), smemRaw, (int)q, full);
         if ((uint32_t)(ST - 1) < mine)
-            pnext = tileOf(ST - 1);
+            pk0 = k0Of(ST - 1);
     }
-    TileDesc cur = tileOf(0);
-    uint32_t curMask = a.masks[(size_t)t0 * C::MASK_WORDS + warp];
     bool failed = false;
 
     for (uint32_t j = 0; j < mine; ++j) {
@@ -194,18 +195,11 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                     failed = true;
                 if (!failed) {
                     tma::fenceProxyAsync();
-                    issueTile<S, C>(a, (uint32_t)pnext.x, smemRaw, sq, full);
+                    issueTile<S, C>(a, t0 + q * stride, pk0, smemRaw, sq, full);
                 }
                 if (q + 1 < mine)
-                    pnext = tileOf(q + 1);
+                    pk0 = k0Of(q + 1);
             }
-        }
-        // descriptor and mask of the next tile, for the next iteration
-        TileDesc nxt = cur;
-        uint32_t nxtMask = 0;
-        if (j + 1 < mine) {
-            nxt = tileOf(j + 1);
-            nxtMask = a.masks[(size_t)(t0 + (j + 1) * stride) * C::MASK_WORDS + warp];
         }
 
         const bool ok = tma::mbarWait(&full[s], (j / ST) & 1u, kWaitLimit);
@@ -214,9 +208,12 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                 atomicExch(a.errorFlag, 1);
             return;
         }
-        if ((curMask >> lane) & 1u) {
-            const uint32_t k = (uint32_t)cur.x + tid;
-            const S* st = reinterpret_cast<const S*>(smemRaw + s * C::STAGE_BYTES) + tid;
+        const unsigned char* stage = smemRaw + s * C::STAGE_BYTES;
+        const uint32_t* meta = reinterpret_cast<const uint32_t*>(stage + C::DATA_BYTES);
+        const uint32_t mask = meta[4 + warp];
+        if ((mask >> lane) & 1u) {
+            const uint32_t k = meta[0] + tid;
+            const S* st = reinterpret_cast<const S*>(stage) + tid;
             R f[27];
 #pragma unroll
             for (int d = 0; d < 27; ++d)
@@ -229,8 +226,6 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
         __syncwarp();
         if (lane == 0)
             tma::mbarArrive(&empty[s]);
-        cur = nxt;
-        curMask = nxtMask;
     }
 }
 
@@ -246,8 +241,7 @@ struct vfb_collision_plan_impl {
     const uint32_t* fluid = nullptr;
     uint32_t nFluid = 0;
     uint32_t sy = 0, sz = 0;
-    TileDesc* tiles = nullptr;
-    uint32_t* masks = nullptr;
+    uint32_t* meta = nullptr;
     uint32_t* laneList = nullptr;
     uint32_t nTiles = 0;
     uint32_t nLane = 0;
@@ -372,13 +366,9 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     if (std::adjacent_find(cand.begin(), cand.end()) != cand.end())
         return setError(VFB_ERR_INVALID_ARGUMENT, "the fluid-node list holds a node twice");
 
-    struct Entry {
-        uint32_t key;
-        TileDesc d;
-    };
-    std::vector<Entry> order;
-    std::vector<uint32_t> masks;
+    std::vector<uint32_t> meta;
     const uint64_t words = T / 32;
+    const uint64_t metaWords = 4 + words;
     const uint64_t minActive = T / 4;
     size_t i = 0;
     while (i < cand.size()) {
@@ -388,13 +378,13 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
             ++j;
         const uint64_t active = j - i;
         if (active >= minActive && bulkInBounds(k0)) {
-            const uint32_t maskIndex = (uint32_t)(masks.size() / words);
-            masks.resize(masks.size() + words, 0u);
+            const size_t at = meta.size();
+            meta.resize(at + metaWords, 0u);
+            meta[at] = (uint32_t)k0;
             for (size_t q = i; q < j; ++q) {
                 const uint64_t off = cand[q] - k0;
-                masks[(size_t)maskIndex * words + off / 32] |= 1u << (off % 32);
+                meta[at + 4 + off / 32] |= 1u << (off % 32);
             }
-            order.push_back({ (uint32_t)k0, make_int2((int)k0, (int)maskIndex) });
             p.stats[1]++;
             p.stats[3] += active;
         } else {
@@ -407,10 +397,7 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     std::sort(lane.begin(), lane.end());
     p.stats[2] = (lane.size() + T - 1) / T;
     p.stats[5] = lane.size();
-    std::vector<TileDesc> tiles(order.size());
-    for (size_t q = 0; q < order.size(); ++q)
-        tiles[q] = order[q].d;
-    p.stats[0] = tiles.size();
+    p.stats[0] = p.stats[1];
 
     p.storage = storage;
     p.N = N;
@@ -421,11 +408,9 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     p.nFluid = nF;
     p.sy = sy;
     p.sz = sz;
-    p.nTiles = (uint32_t)tiles.size();
+    p.nTiles = (uint32_t)p.stats[1];
     p.nLane = (uint32_t)lane.size();
-    e = upload(&p.tiles, tiles, stream);
-    if (e == cudaSuccess)
-        e = upload(&p.masks, masks, stream);
+    e = upload(&p.meta, meta, stream);
     if (e == cudaSuccess)
         e = upload(&p.laneList, lane, stream);
     if (e == cudaSuccess)
@@ -522,8 +507,7 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     TiledArgs<S> a;
     a.dist = static_cast<S*>(c->distributions);
     a.N = p.N;
-    a.tiles = p.tiles;
-    a.masks = p.masks;
+    a.meta = p.meta;
     a.nTiles = p.nTiles;
     a.rates = makeK17Rates<R>((R)c->omega, (R)c->quadricLimiters[0], (R)c->quadricLimiters[1],
                               (R)c->quadricLimiters[2]);
@@ -622,8 +606,7 @@ extern "C" int vfb_collision_plan_create(int storage, const vfb_collision_args* 
     auto* p = new vfb_collision_plan_impl;
     const int rc = buildPlan(*p, storage, args, static_cast<cudaStream_t>(stream));
     if (rc != VFB_OK) {
-        cudaFree(p->tiles);
-        cudaFree(p->masks);
+        cudaFree(p->meta);
         cudaFree(p->laneList);
         cudaFree(p->error);
         delete p;
@@ -639,8 +622,7 @@ extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
     if (!plan)
         return VFB_OK;
     auto* p = reinterpret_cast<vfb_collision_plan_impl*>(plan);
-    cudaFree(p->tiles);
-    cudaFree(p->masks);
+    cudaFree(p->meta);
     cudaFree(p->laneList);
     cudaFree(p->error);
     delete p;

@@ -43,6 +43,15 @@ __device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// 32-bit global load kept in program order with the other asm statements
+// (the producer issues it one tile ahead of its use)
+__device__ __forceinline__ uint32_t ldgOrdered(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // plain arrival (no transaction count)
 __device__ __forceinline__ void mbarArrive(uint64_t* bar)
 {
