@@ -56,10 +56,16 @@ struct TileCfg {
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
     static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
     static constexpr int MASK_WORDS = T / 32;
-    static constexpr int META_WORDS = 4 + MASK_WORDS;                // multiple of 4: 16-byte copies
+    static constexpr int META_WORDS = ((4 + MASK_WORDS + 3) / 4) * 4; // multiple of 4: 16-byte copies
     static constexpr int DATA_BYTES = 27 * CAP * (int)sizeof(S);
     static constexpr int STAGE_BYTES = DATA_BYTES + META_WORDS * 4;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 16 * STAGES; // stages + full / empty mbarriers
+    // every bulk copy needs 16-byte aligned addresses and sizes
+    static_assert((CAP * (int)sizeof(S)) % 16 == 0, "direction segments must be 16-byte multiples");
+    static_assert(DATA_BYTES % 16 == 0, "metadata must start on a 16-byte boundary");
+    static_assert((META_WORDS * 4) % 16 == 0, "metadata copy must be a 16-byte multiple");
+    static_assert(STAGE_BYTES % 16 == 0, "stages must start on 16-byte boundaries");
+    static_assert(T % 32 == 0, "tiles are whole warps");
 };
 
 enum class Op { K17, BGK };
@@ -234,6 +240,7 @@ struct vfb_collision_plan_impl {
     int storage = 0;
     int config = 0;      // index into kTileConfigs
     uint32_t tileWidth = 256;
+    uint32_t metaWords = 12;
     unsigned long long N = 0;
     const uint32_t* nX = nullptr;
     const uint32_t* nY = nullptr;
@@ -368,7 +375,7 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
 
     std::vector<uint32_t> meta;
     const uint64_t words = T / 32;
-    const uint64_t metaWords = 4 + words;
+    const uint64_t metaWords = ((4 + words + 3) / 4) * 4; // TileCfg::META_WORDS
     const uint64_t minActive = T / 4;
     size_t i = 0;
     while (i < cand.size()) {
@@ -409,6 +416,7 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     p.sy = sy;
     p.sz = sz;
     p.nTiles = (uint32_t)p.stats[1];
+    p.metaWords = (uint32_t)metaWords;
     p.nLane = (uint32_t)lane.size();
     e = upload(&p.meta, meta, stream);
     if (e == cudaSuccess)
@@ -446,8 +454,11 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 }
 
 template <class S, class C>
-static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, cudaStream_t stream)
+static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, uint32_t metaWords,
+                  cudaStream_t stream)
 {
+    if (metaWords != (uint32_t)C::META_WORDS)
+        return setError(VFB_ERR_CONFIGURATION, "plan metadata layout does not match the kernel configuration");
     a.totalBytes = 0;
     for (int d = 0; d < 27; ++d) {
         const unsigned long long off = (unsigned long long)(even ? d : inv(d)) * a.N + locShift(loc(d), sy, sz);
@@ -480,8 +491,11 @@ static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t s
 // the tuning configurations are compiled for the default K17 and BGK passes
 // only; the other templates always use the default shape
 template <class S, class C>
-static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, cudaStream_t stream)
+static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t sy, uint32_t sz, uint32_t metaWords,
+                  cudaStream_t stream)
 {
+    if (metaWords != (uint32_t)C::META_WORDS)
+        return setError(VFB_ERR_CONFIGURATION, "plan metadata layout does not match the kernel configuration");
     if (tmpl != VFB_TEMPLATE_DEFAULT && op == Op::K17)
         return setError(VFB_ERR_UNSUPPORTED, "tile configuration supports the default template only");
     a.totalBytes = 0;
@@ -532,16 +546,16 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     const int t = c->collisionTemplate;
     if constexpr (sizeof(S) == 8) {
         switch (p.config) {
-        case 6: return dispatchTuning<S, TileCfg<S, 128, 3, 3>>(op, even, t, a, p.sy, p.sz, stream);
-        default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, stream);
+        case 6: return dispatchTuning<S, TileCfg<S, 128, 3, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     } else {
         switch (p.config) {
-        case 2: return dispatchTuning<S, TileCfg<S, 256, 3, 2>>(op, even, t, a, p.sy, p.sz, stream);
-        case 3: return dispatchTuning<S, TileCfg<S, 192, 3, 3>>(op, even, t, a, p.sy, p.sz, stream);
-        case 4: return dispatchTuning<S, TileCfg<S, 160, 3, 4>>(op, even, t, a, p.sy, p.sz, stream);
-        case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, stream);
-        default: return dispatchTiled<S, TileCfg<S, 256, 2, 3>>(op, even, t, a, p.sy, p.sz, stream);
+        case 2: return dispatchTuning<S, TileCfg<S, 256, 3, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 3: return dispatchTuning<S, TileCfg<S, 192, 3, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 4: return dispatchTuning<S, TileCfg<S, 160, 3, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        default: return dispatchTiled<S, TileCfg<S, 256, 2, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     }
 }
