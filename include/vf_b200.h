@@ -172,6 +172,25 @@ int vfb_mass_and_energy(int storage, const void* distributions, unsigned long lo
                         void* stream);
 
 /*
+ * vfb_mass_and_energy without any allocation: same arguments, same sums in
+ * the same order.  No counterpart in the reference.  It is for callers that
+ * cannot allocate device memory where they want the sums (a host whose pool
+ * allocator owns all of HBM, or a monitor inside a solver loop whose memory
+ * footprint must stay fixed).  Its scratch is a fixed 24 KiB device array in
+ * the library (partial sums of at most 1024 blocks), held by every GPU that
+ * loads the library until exit; a launch that would need more blocks is
+ * rejected with VFB_ERR_OUT_OF_RANGE.  The first call on each device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  All calls on a device share the array, so calls that overlap on
+ * the GPU (other streams, other host threads) race; the call synchronises its
+ * stream before it returns.
+ */
+int vfb_mass_and_energy_static(int storage, const void* distributions, unsigned long long numberOfLBnodes,
+                               const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                               const uint32_t* nodeIndices, uint32_t numberOfIndices, int isEvenTimestep,
+                               double* out, void* stream);
+
+/*
  * One node of the K17 (op 0) or BGK (op 1) collision on the host with the
  * library's own arithmetic (the code the kernels run), for checks without a
  * GPU.  precision: VFB_FP64 or VFB_FP32; f27 in/out, out4 = drho, vx, vy, vz.

@@ -73,6 +73,9 @@ _SIGNATURES = [
     ("vfb_mass_and_energy", ctypes.c_int,
      [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_mass_and_energy_static", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_collision_plan_create", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),
