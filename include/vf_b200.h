@@ -124,8 +124,8 @@ int vfb_bgk_collision(int storage, const vfb_collision_args* args, void* stream)
 typedef struct vfb_collision_plan vfb_collision_plan;
 int vfb_collision_plan_create(int storage, const vfb_collision_args* args, vfb_collision_plan** plan, void* stream);
 int vfb_collision_plan_destroy(vfb_collision_plan* plan);
-/* out6: tiles, bulk tiles, lane-by-lane tiles, bulk-fed nodes, exception
- * nodes inside bulk tiles, nodes in lane-by-lane tiles */
+/* out6: tiles, bulk tiles, lane-by-lane tiles, bulk-fed nodes, periodic
+ * wrap nodes served inside bulk tiles, nodes collided lane by lane */
 int vfb_collision_plan_stats(const vfb_collision_plan* plan, unsigned long long* out6);
 /* VFB_OK, or VFB_ERR_CUDA if a bounded wait of a planned kernel ran out
  * (synchronises the stream) */

@@ -12,12 +12,18 @@
 // collides the previous tile, and no index array is read for it.  A bit mask
 // marks which indices of the range are members of the fluid-node list (the
 // others -- stoppers, removed or differently tagged nodes -- are skipped).
-// Irregular nodes (periodic wraps, nodes next to removed ones) and sparse
-// ranges go to lane tiles, processed one node per thread through the index
-// chain exactly as the generic kernel does.
+// Nodes on a periodic wrap stay in the tiles (their wrapped locations are
+// read and written in global memory by their own lane).  Irregular nodes
+// (next to removed ones, at refinement borders) and sparse ranges go to a
+// lane list, collided one node per thread through the index chain by the
+// generic kernel.
 //
-// Each block owns two shared-memory stages and an mbarrier per stage; blocks
-// of a persistent grid stride over the tiles.  The arithmetic is the same
+// Two kernels consume the plan.  In the staged kernel (the FP32 / FP64
+// default) each block owns shared-memory stages with an mbarrier pair each;
+// blocks of a persistent grid stride over the tiles.  In the direct kernel
+// (the FP16 / BF16 default, where the collision arithmetic and not the memory
+// bounds the step) each block takes one tile and its warps load their values
+// from global memory straight into registers.  The arithmetic is the same
 // k17Collide / bgkCollide as the generic kernel.  Every population location
 // is read and written by exactly one node, and a thread uses only the values
 // at its own node's locations, so values a bulk copy fetches for positions no
@@ -39,9 +45,18 @@
 namespace vfb
 {
 
-// Tile metadata, META_WORDS uint32 per tile: word 0 = k0 (first sparse index
-// of the range), words 1..3 unused, words 4.. = one active-lane mask per warp.
-// The producer bulk-copies it into the stage with the tile's populations.
+// Tile metadata, META_WORDS uint32 per tile (W = warps per tile): word 0 = k0
+// (first sparse index of the range), word 1 = bit w set when warp w holds a
+// node that wraps around a periodic boundary, words 2..3 unused, words
+// 4..4+W = one active-lane mask per warp, then W x-wrap, W y-wrap and W z-wrap
+// lane masks.  The producer bulk-copies it into the stage with the tile's
+// populations.
+//
+// A wrap node (the last node of a periodic x line, y column or z pillar) has
+// the lattice strides on every axis except the wrapped ones, whose neighbour
+// sits a fixed distance back (the wrap offset of that axis).  Its populations
+// at the locations on a wrapped axis are not in the tile's bulk copies; its
+// lane reads and writes them in global memory directly.
 
 constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
 
@@ -56,7 +71,7 @@ struct TileCfg {
     static constexpr int E = 16 / (int)sizeof(S);                  // elements per 16 bytes
     static constexpr int CAP = ((E - 1 + T + E - 1) / E) * E;      // elements per direction segment
     static constexpr int MASK_WORDS = T / 32;
-    static constexpr int META_WORDS = ((4 + MASK_WORDS + 3) / 4) * 4; // multiple of 4: 16-byte copies
+    static constexpr int META_WORDS = ((4 + 4 * MASK_WORDS + 3) / 4) * 4; // multiple of 4: 16-byte copies
     static constexpr int DATA_BYTES = 27 * CAP * (int)sizeof(S);
     static constexpr int STAGE_BYTES = DATA_BYTES + META_WORDS * 4;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 16 * STAGES; // stages + full / empty mbarriers
@@ -79,6 +94,10 @@ struct TiledArgs {
     // lead of a tile's segment (tiles start at multiples of 16 bytes), the
     // shared-memory offset of node k0 and the bytes of one bulk copy
     S* gbase[27];
+    // the last 16-byte aligned start at which a copy of bytes[d] stays inside
+    // the population array; a copy that would run past the end starts there
+    // instead (the plan guarantees that no lane of such a tile uses it)
+    const S* lastSrc[27];
     int lead[27];
     int smemOff[27];
     uint32_t bytes[27];
@@ -86,6 +105,9 @@ struct TiledArgs {
     unsigned long long N;
     const uint32_t* __restrict__ meta;
     uint32_t nTiles;
+    // wrap offset minus lattice stride per axis (added to a location on a
+    // wrapped axis)
+    long long wrapDelta[3];
     K17Rates<R> rates;
     R fx, fy, fz, gfx, gfy, gfz, forceFactor;
     R* rho;
@@ -117,7 +139,10 @@ __device__ __forceinline__ void issueTile(const TiledArgs<S>& a, uint32_t tile, 
     tma::bulkLoad(base + C::DATA_BYTES, a.meta + (size_t)tile * C::META_WORDS, C::META_WORDS * 4, &full[stage]);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        tma::bulkLoad(dst + d * C::CAP, a.gbase[d] + (k0 - (uint32_t)a.lead[d]), a.bytes[d], &full[stage]);
+    {
+        const S* src = a.gbase[d] + (k0 - (uint32_t)a.lead[d]);
+        tma::bulkLoad(dst + d * C::CAP, src < a.lastSrc[d] ? src : a.lastSrc[d], a.bytes[d], &full[stage]);
+    }
 }
 
 template <class S, bool EVEN, Op OP, bool WM, bool BF>
@@ -151,8 +176,9 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
 // it waits on the stage's "empty" barrier, on which every warp arrives once it
 // has read the stage, then arms the stage's "full" barrier with the tile's
 // byte count and issues the 27 bulk copies, STAGES - 1 tiles ahead of the
-// consumers.  Every warp waits on "full", collides its 32 nodes, stores them
-// and arrives on "empty".  Warps never wait for each other otherwise.
+// consumers.  Every warp waits on "full", moves its 32 nodes' values into
+// registers, arrives on "empty", then collides and stores.  Warps never wait
+// for each other otherwise.
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> a)
 {
@@ -216,22 +242,106 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
         }
         const unsigned char* stage = smemRaw + s * C::STAGE_BYTES;
         const uint32_t* meta = reinterpret_cast<const uint32_t*>(stage + C::DATA_BYTES);
-        const uint32_t mask = meta[4 + warp];
-        if ((mask >> lane) & 1u) {
-            const uint32_t k = meta[0] + tid;
-            const S* st = reinterpret_cast<const S*>(stage) + tid;
-            R f[27];
+        const bool active = (meta[4 + warp] >> lane) & 1u;
+        const uint32_t k = meta[0] + tid;
+        const bool wrapWarp = (meta[1] >> warp) & 1u; // the same for the whole warp
+        // wrap bits of this lane: bit 0 x, bit 1 y, bit 2 z
+        const int wb = wrapWarp ? (int)((meta[4 + WARPS + warp] >> lane) & 1u) |
+                                      (int)(((meta[4 + 2 * WARPS + warp] >> lane) & 1u) << 1) |
+                                      (int)(((meta[4 + 3 * WARPS + warp] >> lane) & 1u) << 2)
+                                : 0;
+        const S* st = reinterpret_cast<const S*>(stage) + tid;
+        R f[27];
+        if (active) {
+            if (!wrapWarp) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d)
-                f[d] = Storage<S>::load(st + a.smemOff[d]);
-            collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+                for (int d = 0; d < 27; ++d)
+                    f[d] = Storage<S>::load(st + a.smemOff[d]);
+            } else {
+                const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
+                const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
+                const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
 #pragma unroll
-            for (int d = 0; d < 27; ++d)
-                Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+                for (int d = 0; d < 27; ++d) {
+                    const int l = loc(d);
+                    const long long delta = ((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll);
+                    f[d] = (l & wb) ? Storage<S>::load(a.gbase[d] + k + delta) : Storage<S>::load(st + a.smemOff[d]);
+                }
+            }
         }
+        // the stage is free once the warp holds its values: release it before
+        // colliding, so the producer refills it while the warp computes (and a
+        // wrap lane waiting for its global loads does not hold it)
         __syncwarp();
         if (lane == 0)
             tma::mbarArrive(&empty[s]);
+        if (active) {
+            collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+            if (!wrapWarp) {
+#pragma unroll
+                for (int d = 0; d < 27; ++d)
+                    Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+            } else {
+                const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
+                const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
+                const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+#pragma unroll
+                for (int d = 0; d < 27; ++d) {
+                    const int l = loc(d);
+                    const long long delta = ((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll);
+                    Storage<S>::store(a.gbase[d] + k + delta, f[inv(d)]);
+                }
+            }
+        }
+    }
+}
+
+// Direct form of the planned kernel (a tile configuration with 0 stages): one
+// block per tile, every warp loads its nodes' 27 values straight from global
+// memory into registers (coalesced: consecutive lanes read consecutive
+// addresses of each direction's run), collides and stores.  No producer, no
+// shared memory; latency is hidden by the warps resident on the SM.
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+__global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S> a)
+{
+    using R = typename Storage<S>::R;
+    constexpr int WARPS = C::T / 32;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const uint32_t* meta = a.meta + (size_t)blockIdx.x * C::META_WORDS;
+    const bool active = (__ldg(meta + 4 + warp) >> lane) & 1u;
+    if (!active)
+        return;
+    const uint32_t k = __ldg(meta) + tid;
+    const bool wrapWarp = (__ldg(meta + 1) >> warp) & 1u;
+    R f[27];
+    if (!wrapWarp) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = Storage<S>::load(a.gbase[d] + k);
+        collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+    } else {
+        const int wb = (int)((__ldg(meta + 4 + WARPS + warp) >> lane) & 1u) |
+                       (int)(((__ldg(meta + 4 + 2 * WARPS + warp) >> lane) & 1u) << 1) |
+                       (int)(((__ldg(meta + 4 + 3 * WARPS + warp) >> lane) & 1u) << 2);
+        const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
+        const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
+        const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const int l = loc(d);
+            f[d] = Storage<S>::load(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll)));
+        }
+        collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const int l = loc(d);
+            Storage<S>::store(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll)),
+                              f[inv(d)]);
+        }
     }
 }
 
@@ -248,11 +358,12 @@ struct vfb_collision_plan_impl {
     const uint32_t* fluid = nullptr;
     uint32_t nFluid = 0;
     uint32_t sy = 0, sz = 0;
+    long long wrapDelta[3] = { 0, 0, 0 };
     uint32_t* meta = nullptr;
     uint32_t* laneList = nullptr;
     uint32_t nTiles = 0;
     uint32_t nLane = 0;
-    // tiles, bulk tiles, lane blocks, bulk-fed nodes, irregular nodes, nodes collided lane by lane
+    // tiles, bulk tiles, lane blocks, bulk-fed nodes, wrap nodes served in bulk tiles, nodes collided lane by lane
     unsigned long long stats[6] = { 0, 0, 0, 0, 0, 0 };
     int* error = nullptr;
 };
@@ -278,6 +389,26 @@ uint32_t modeStride(const std::vector<uint32_t>& fluid, const std::vector<uint32
     return (uint32_t)best;
 }
 
+// the most frequent value of nb[k] - k other than the stride over all fluid
+// nodes (the wrap offset of a periodic axis), 0 if there is none
+long long modeWrap(const std::vector<uint32_t>& fluid, const std::vector<uint32_t>& nb, long long stride)
+{
+    std::map<long long, size_t> h;
+    for (const uint32_t k : fluid) {
+        const long long v = (long long)nb[k] - (long long)k;
+        if (v != stride)
+            h[v]++;
+    }
+    long long best = 0;
+    size_t n = 0;
+    for (auto& kv : h)
+        if (kv.second > n && kv.first != 0) {
+            n = kv.second;
+            best = kv.first;
+        }
+    return best;
+}
+
 template <class T>
 cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 {
@@ -289,9 +420,10 @@ cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 } // namespace
 
 // Tile configurations (tile width, stages, resident blocks) the library is
-// compiled for.  Entry 0 is the default for 2- and 4-byte storage, entry 1 for
-// FP64; VFB_TILE_CONFIG=<index> selects another one at plan creation (used to
-// tune the shape on new hardware).
+// compiled for; 0 stages selects the direct-load kernel.  Entry 0 is the
+// default for FP32, entry 9 for FP16 / BF16 and entry 1 for FP64;
+// VFB_TILE_CONFIG=<index> selects another one at plan creation (used to tune
+// the shape on new hardware).
 struct TileConfigInfo {
     int T, stages, minBlocks;
     bool fp64;
@@ -299,13 +431,15 @@ struct TileConfigInfo {
 static const TileConfigInfo kTileConfigs[] = {
     { 256, 2, 3, false }, { 128, 2, 2, true }, { 256, 3, 2, false }, { 192, 3, 3, false },
     { 160, 3, 4, false }, { 128, 4, 3, false }, { 128, 3, 3, true },
+    // direct loads (0 stages)
+    { 128, 0, 4, false }, { 256, 0, 3, false }, { 128, 0, 6, false }, { 128, 0, 2, true }, { 128, 0, 3, true },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
 static int chooseTileConfig(int storage)
 {
     const bool fp64 = storage == VFB_FP64;
-    int def = fp64 ? 1 : 0;
+    int def = fp64 ? 1 : (vfb_storage_bytes(storage) == 2 ? 9 : 0);
     if (const char* env = std::getenv("VFB_TILE_CONFIG")) {
         const int c = std::atoi(env);
         if (c >= 0 && c < kNumTileConfigs && kTileConfigs[c].fp64 == fp64)
@@ -340,63 +474,109 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     const uint64_t T = p.tileWidth;
     const uint64_t E = 16 / (uint64_t)esize;
     const uint32_t sy = nF ? modeStride(fl, ny) : 1, sz = nF ? modeStride(fl, nz) : 1;
-    auto regular = [&](uint64_t k) -> bool {
-        const uint64_t far = k + 1 + (uint64_t)sy + sz;
-        if (far >= N)
-            return false;
-        return nx[k] == k + 1 && ny[k] == k + sy && nz[k] == k + sz && ny[k + 1] == k + 1 + sy &&
-               nz[k + 1] == k + 1 + sz && nz[k + sy] == k + sy + sz && nz[k + 1 + sy] == k + 1 + sy + sz;
+    // periodic wrap offsets (0: the axis does not wrap)
+    const long long wx = modeWrap(fl, nx, 1), wy = modeWrap(fl, ny, sy), wz = modeWrap(fl, nz, sz);
+    auto at = [&](const std::vector<uint32_t>& nb, long long k, long long expect) {
+        return k >= 0 && k < (long long)N && (long long)nb[k] == expect;
+    };
+    // wrap bits of node k (bit 0 x, bit 1 y, bit 2 z), or -1 when its
+    // neighbours follow neither the strides nor the wrap offsets
+    auto classify = [&](uint64_t k) -> int {
+        const long long kk = (long long)k;
+        int bits = 0;
+        long long o[3];
+        const std::vector<uint32_t>* nb[3] = { &nx, &ny, &nz };
+        const long long stride[3] = { 1, sy, sz }, wrap[3] = { wx, wy, wz };
+        for (int ax = 0; ax < 3; ++ax) {
+            const long long v = (long long)(*nb[ax])[k] - kk;
+            if (v == stride[ax])
+                o[ax] = stride[ax];
+            else if (wrap[ax] != 0 && v == wrap[ax]) {
+                o[ax] = wrap[ax];
+                bits |= 1 << ax;
+            } else
+                return -1;
+        }
+        const long long k1 = kk + o[0], k2 = kk + o[1], k3 = k1 + o[1];
+        if (!at(ny, k1, k3) || !at(nz, k1, k1 + o[2]) || !at(nz, k2, k2 + o[2]) || !at(nz, k3, k3 + o[2]))
+            return -1;
+        // all eight locations inside the lattice (the wrap lanes address them directly)
+        for (int l = 0; l < 8; ++l) {
+            const long long kl = kk + ((l & 1) ? o[0] : 0) + ((l & 2) ? o[1] : 0) + ((l & 4) ? o[2] : 0);
+            if (kl < 0 || kl >= (long long)N)
+                return -1;
+        }
+        return bits;
     };
     const uint64_t limit = 27ull * N;
-    auto bulkInBounds = [&](uint64_t k0) -> bool {
+    // a copy that would run past the end of the array is moved back inside it
+    // by the kernel, so the tile may only hold lanes that do not read it (lanes
+    // that wrap on an axis of the copy's location)
+    auto bulkUsable = [&](uint64_t k0, const uint64_t* first, const uint64_t* last) -> bool {
+        if (N * 27ull < T + 2 * E)
+            return false;
         for (int even = 0; even < 2; ++even)
             for (int d = 0; d < 27; ++d) {
                 const uint64_t base = (uint64_t)(even ? d : inv(d)) * N + k0 + locShift(loc(d), sy, sz);
                 const uint64_t lead = base % E;
-                if (base - lead + ((lead + T + E - 1) / E) * E > limit)
-                    return false;
+                if (base - lead + ((lead + T + E - 1) / E) * E <= limit)
+                    continue;
+                for (const uint64_t* q = first; q != last; ++q)
+                    if ((loc(d) & (int)(*q & 7u)) == 0)
+                        return false;
             }
         return true;
     };
 
-    // regular list members, ascending; everything else goes lane by lane
-    std::vector<uint32_t> cand, lane;
+    // classified list members as (k << 3 | wrap bits), ascending; the others go lane by lane
+    std::vector<uint64_t> cand;
+    std::vector<uint32_t> lane;
     cand.reserve(nF);
     for (uint32_t i = 0; i < nF; ++i) {
-        if (regular(fl[i]))
-            cand.push_back(fl[i]);
+        const int bits = classify(fl[i]);
+        if (bits >= 0)
+            cand.push_back(((uint64_t)fl[i] << 3) | (uint64_t)bits);
         else
             lane.push_back(fl[i]);
     }
-    p.stats[4] = lane.size();
     std::sort(cand.begin(), cand.end());
-    if (std::adjacent_find(cand.begin(), cand.end()) != cand.end())
-        return setError(VFB_ERR_INVALID_ARGUMENT, "the fluid-node list holds a node twice");
+    for (size_t i = 1; i < cand.size(); ++i)
+        if ((cand[i] >> 3) == (cand[i - 1] >> 3))
+            return setError(VFB_ERR_INVALID_ARGUMENT, "the fluid-node list holds a node twice");
 
     std::vector<uint32_t> meta;
     const uint64_t words = T / 32;
-    const uint64_t metaWords = ((4 + words + 3) / 4) * 4; // TileCfg::META_WORDS
+    const uint64_t metaWords = ((4 + 4 * words + 3) / 4) * 4; // TileCfg::META_WORDS
     const uint64_t minActive = T / 4;
     size_t i = 0;
     while (i < cand.size()) {
-        const uint64_t k0 = cand[i] - cand[i] % E; // bulk sources then share one lead per direction
+        const uint64_t first = cand[i] >> 3;
+        const uint64_t k0 = first - first % E; // bulk sources then share one lead per direction
         size_t j = i;
-        while (j < cand.size() && cand[j] < k0 + T)
+        while (j < cand.size() && (cand[j] >> 3) < k0 + T)
             ++j;
         const uint64_t active = j - i;
-        if (active >= minActive && bulkInBounds(k0)) {
-            const size_t at = meta.size();
-            meta.resize(at + metaWords, 0u);
-            meta[at] = (uint32_t)k0;
+        if (active >= minActive && bulkUsable(k0, cand.data() + i, cand.data() + j)) {
+            const size_t base = meta.size();
+            meta.resize(base + metaWords, 0u);
+            meta[base] = (uint32_t)k0;
             for (size_t q = i; q < j; ++q) {
-                const uint64_t off = cand[q] - k0;
-                meta[at + 4 + off / 32] |= 1u << (off % 32);
+                const uint64_t off = (cand[q] >> 3) - k0;
+                const uint32_t bits = (uint32_t)(cand[q] & 7u), w = (uint32_t)(off / 32), b = 1u << (off % 32);
+                meta[base + 4 + w] |= b;
+                for (int ax = 0; ax < 3; ++ax)
+                    if (bits & (1u << ax))
+                        meta[base + 4 + (1 + ax) * words + w] |= b;
+                if (bits) {
+                    meta[base + 1] |= 1u << w;
+                    p.stats[4]++;
+                }
             }
             p.stats[1]++;
             p.stats[3] += active;
         } else {
             for (size_t q = i; q < j; ++q)
-                lane.push_back(cand[q]);
+                lane.push_back((uint32_t)(cand[q] >> 3));
         }
         i = j;
     }
@@ -415,6 +595,9 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     p.nFluid = nF;
     p.sy = sy;
     p.sz = sz;
+    p.wrapDelta[0] = wx ? wx - 1 : 0;
+    p.wrapDelta[1] = wy ? wy - (long long)sy : 0;
+    p.wrapDelta[2] = wz ? wz - (long long)sz : 0;
     p.nTiles = (uint32_t)p.stats[1];
     p.metaWords = (uint32_t)metaWords;
     p.nLane = (uint32_t)lane.size();
@@ -435,6 +618,10 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
+    if constexpr (C::STAGES == 0) {
+        directKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T, 0, stream>>>(a);
+        return checkLaunch("direct planned collision");
+    } else {
     static int blocks = 0;
     if (blocks == 0) {
         cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, C, EVEN, OP, WM, BF>,
@@ -451,6 +638,7 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
     const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
     tiledKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, C::SMEM_BYTES, stream>>>(a);
     return checkLaunch("tiled collision");
+    }
 }
 
 template <class S, class C>
@@ -466,6 +654,7 @@ static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t s
         a.lead[d] = (int)(off % C::E);
         a.smemOff[d] = d * C::CAP + a.lead[d];
         a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
+        a.lastSrc[d] = a.dist + ((27ull * a.N - a.bytes[d] / sizeof(S)) / C::E) * C::E;
         a.totalBytes += a.bytes[d];
     }
     if (op == Op::BGK)
@@ -505,6 +694,7 @@ static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t 
         a.lead[d] = (int)(off % C::E);
         a.smemOff[d] = d * C::CAP + a.lead[d];
         a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
+        a.lastSrc[d] = a.dist + ((27ull * a.N - a.bytes[d] / sizeof(S)) / C::E) * C::E;
         a.totalBytes += a.bytes[d];
     }
     if (op == Op::BGK)
@@ -523,6 +713,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.N = p.N;
     a.meta = p.meta;
     a.nTiles = p.nTiles;
+    for (int ax = 0; ax < 3; ++ax)
+        a.wrapDelta[ax] = p.wrapDelta[ax];
     a.rates = makeK17Rates<R>((R)c->omega, (R)c->quadricLimiters[0], (R)c->quadricLimiters[1],
                               (R)c->quadricLimiters[2]);
     a.forceFactor = (R)c->forceFactor;
@@ -547,6 +739,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     if constexpr (sizeof(S) == 8) {
         switch (p.config) {
         case 6: return dispatchTuning<S, TileCfg<S, 128, 3, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 10: return dispatchTuning<S, TileCfg<S, 128, 0, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 11: return dispatchTuning<S, TileCfg<S, 128, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     } else {
@@ -555,6 +749,14 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 3: return dispatchTuning<S, TileCfg<S, 192, 3, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 4: return dispatchTuning<S, TileCfg<S, 160, 3, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 7: return dispatchTuning<S, TileCfg<S, 128, 0, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 9:
+            // the default for 16-bit storage (compute bound: direct loads keep more warps colliding)
+            if constexpr (sizeof(S) == 2)
+                return dispatchTiled<S, TileCfg<S, 128, 0, 6>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+            else
+                return dispatchTuning<S, TileCfg<S, 128, 0, 6>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         default: return dispatchTiled<S, TileCfg<S, 256, 2, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     }

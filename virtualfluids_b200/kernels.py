@@ -124,7 +124,7 @@ class CollisionPlan:
     def stats(self) -> dict[str, int]:
         out = (ctypes.c_ulonglong * 6)()
         _lib.check(_lib.lib().vfb_collision_plan_stats(self.handle, out))
-        keys = ("tiles", "bulk_tiles", "lane_tiles", "bulk_nodes", "exception_nodes", "lane_nodes")
+        keys = ("tiles", "bulk_tiles", "lane_tiles", "bulk_nodes", "wrap_nodes", "lane_nodes")
         return dict(zip(keys, [int(x) for x in out]))
 
     def check(self, stream=None) -> None:
