@@ -135,6 +135,91 @@ int vfb_k17_collision_planned(const vfb_collision_plan* plan, const vfb_collisio
 int vfb_bgk_collision_planned(const vfb_collision_plan* plan, const vfb_collision_args* args, void* stream);
 
 /*
+ * Boundary conditions.  The lattice a BC kernel runs on, and one compacted BC
+ * list: QforBoundaryConditions (src/gpu/core/Calculation/Calculation.h:105-117)
+ * with k the BC node indices, q the subgrid distances direction-major
+ * (q[d * numberOfBCnodes + i], src/gpu/core/Utilities/KernelUtilities.h:140-169;
+ * a direction is active when 0 <= q <= 1) and Vx/Vy/Vz the per-node wall
+ * velocity of a velocity BC.  q and the velocities are compute-precision arrays.
+ */
+typedef struct vfb_bc_lattice {
+    void* distributions;
+    unsigned long long numberOfLBnodes;
+    const uint32_t* neighborX;
+    const uint32_t* neighborY;
+    const uint32_t* neighborZ;
+    double omega;
+    int isEvenTimestep; /* the parity the reference passes at this call */
+} vfb_bc_lattice;
+
+typedef struct vfb_bc_list {
+    const int32_t* k;
+    const void* q;
+    const void* Vx;
+    const void* Vy;
+    const void* Vz;
+    uint32_t numberOfBCnodes;
+} vfb_bc_list;
+
+/* post-collision BC kinds (BoundaryConditionFactory.h:75-94) */
+#define VFB_BC_NOSLIP_INTERPOLATED 0   /* NoSlipInterpolatedCompressible_Device, NoSlip/NoSlipInterpolatedCompressible.cu:44-378 */
+#define VFB_BC_NOSLIP_BOUNCE_BACK 1    /* NoSlipBounceBack_Device, NoSlip/NoSlipBounceBack.cu */
+#define VFB_BC_VELOCITY_INTERPOLATED 2 /* VelocityInterpolatedCompressible_Device, Velocity/VelocityInterpolatedCompressible.cu:44-418 */
+#define VFB_BC_VELOCITY_BOUNCE_BACK 3  /* VelocityBounceBack_Device, Velocity/VelocityBounceBack.cu */
+#define VFB_BC_SLIP 4                  /* SlipCompressible_Device, Slip/SlipCompressible.cu:45-550 */
+
+/*
+ * One post-collision BC kernel over a list (one thread per BC node).  Replaces
+ * the host launchers NoSlipInterpolatedCompressible / NoSlipBounceBack
+ * (src/gpu/core/BoundaryConditions/NoSlip/NoSlip.cu:81-98),
+ * VelocityInterpolatedCompressible / VelocityBounceBack (Velocity/Velocity.cu)
+ * and SlipCompressible (Slip/Slip.cu), called by
+ * BoundaryConditionKernelManager::runVelocityBCKernelPost / runNoSlipBCKernelPost
+ * / runSlipBCKernelPost (BoundaryConditionKernelManager.cpp:257-344) in the
+ * order velocity, no-slip, slip.  The velocity arrays are read by the velocity
+ * kinds only.
+ */
+int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice, const vfb_bc_list* list, void* stream);
+
+/*
+ * The pre-collision non-equilibrium pressure BC of one directional list
+ * (QforDirectionalBoundaryCondition, Calculation.h:119-127).  Replaces
+ * PressureNonEquilibriumCompressible (src/gpu/core/BoundaryConditions/Pressure/Pressure.cu),
+ * i.e. PressureNonEquilibriumCompressible_Device
+ * (Pressure/PressureNonEquilibriumCompressible.cu:45-311): k the BC nodes, kN
+ * their inner neighbours, rhoBC the prescribed drho (compute precision),
+ * direction the D3Q27 id of the outward normal (1..6: P00, M00, 0P0, 0M0, 00P,
+ * 00M).  lattice->omega is not used.
+ */
+int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,
+                          const void* rhoBC, uint32_t numberOfBCnodes, int direction, void* stream);
+
+/*
+ * Grid builder (host only).  Builds the sparse grid of a box and exports the
+ * arrays the kernels consume, bit for bit those of the reference's
+ * MultipleGridBuilder / LevelGridBuilder (src/gpu/GridGenerator/grid/GridBuilder/
+ * MultipleGridBuilder.cpp, LevelGridBuilder.cpp:395-944, GridImp.cpp:914-1121,
+ * Side.cpp:64-215).  spec (at least 61 values): [0..6] coarse grid start x, y,
+ * z, end x, y, z, delta (MultipleGridBuilder::addCoarseGrid); [7..9] periodic
+ * x, y, z (setPeriodicBoundaryCondition); [10] number of refinement boxes (0);
+ * [17..18] layers; [19] solid cuboid present (0); [30..59] up to six side BCs
+ * as (side 0..5 = MX PX MY PY MZ PZ, type 1 no-slip / 2 velocity / 3 pressure /
+ * 4 slip, three values) applied in order (setNoSlip / setVelocity / setPressure
+ * / setSlipBoundaryCondition); [60] enableThinWalls.  Returns a handle, NULL on
+ * error.  Array names per level: "geo", "neighborX/Y/Z", "neighborNeg",
+ * "coordX/Y/Z", "fluid", "dims", "velocity.k/.q/.vx/.vy/.vz", "slip.k/.q/.nx/
+ * .ny/.nz", "geometry.k/.q", "pressure.count" and "pressure<i>.k/.kN/.rho/.q/.dir".
+ */
+void* vfb_grid_build(const double* spec, int n);
+int vfb_grid_levels(void* grid);
+/* number of elements of an array (-1 if unknown) and their size in bytes */
+long long vfb_grid_count(void* grid, int level, const char* name);
+int vfb_grid_elem_size(void* grid, int level, const char* name);
+/* copies the array into out (count * elem_size bytes) */
+int vfb_grid_copy(void* grid, int level, const char* name, void* out);
+void vfb_grid_free(void* grid);
+
+/*
  * Equilibrium initialisation of one parity view from drho and velocity
  * (compute precision arrays of numberOfLBnodes).  Replaces
  * InitNavierStokesCompressible_Device

@@ -55,6 +55,35 @@ class CollisionArgs(ctypes.Structure):
     ]
 
 
+class BcLattice(ctypes.Structure):
+    """vfb_bc_lattice (include/vf_b200.h)."""
+
+    _fields_ = [
+        ("distributions", ctypes.c_void_p),
+        ("numberOfLBnodes", ctypes.c_ulonglong),
+        ("neighborX", ctypes.c_void_p),
+        ("neighborY", ctypes.c_void_p),
+        ("neighborZ", ctypes.c_void_p),
+        ("omega", ctypes.c_double),
+        ("isEvenTimestep", ctypes.c_int),
+    ]
+
+
+class BcList(ctypes.Structure):
+    """vfb_bc_list (include/vf_b200.h)."""
+
+    _fields_ = [
+        ("k", ctypes.c_void_p),
+        ("q", ctypes.c_void_p),
+        ("Vx", ctypes.c_void_p),
+        ("Vy", ctypes.c_void_p),
+        ("Vz", ctypes.c_void_p),
+        ("numberOfBCnodes", ctypes.c_uint32),
+    ]
+
+
+BC_NOSLIP_INTERPOLATED, BC_NOSLIP_BOUNCE_BACK, BC_VELOCITY_INTERPOLATED, BC_VELOCITY_BOUNCE_BACK, BC_SLIP = range(5)
+
 # (name, restype, argtypes) of every exported entry point
 _SIGNATURES = [
     ("vfb_version", ctypes.c_int, []),
@@ -76,6 +105,11 @@ _SIGNATURES = [
     ("vfb_mass_and_energy_static", ctypes.c_int,
      [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_bc_post", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.POINTER(BcList), ctypes.c_void_p]),
+    ("vfb_bc_pressure_noneq", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+      ctypes.c_int, ctypes.c_void_p]),
     ("vfb_collision_plan_create", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),

@@ -1,0 +1,364 @@
+// bc.cu -- boundary-condition kernels over compacted BC lists.
+//
+// One thread per BC node, as in the reference: the lists are small (a few
+// planes of a level), so these kernels are bound by launch latency and the
+// gather of the node's 27 populations, not by bandwidth.  The q array is
+// direction-major, so the 26 q reads of a warp are coalesced.
+//
+// Post-collision kinds (run after the collision of the same parity, reading
+// the post-collision values through the isEven view and writing the
+// bounced-back values into the !isEven view, NoSlipInterpolatedCompressible.cu:71,165):
+//   no-slip interpolated  NoSlipInterpolatedCompressible.cu:44-378
+//   no-slip bounce-back   NoSlipBounceBack.cu
+//   velocity interpolated VelocityInterpolatedCompressible.cu:44-418
+//   velocity bounce-back  VelocityBounceBack.cu
+//   slip                  SlipCompressible.cu:45-550
+// Pre-collision kind (after the parity swap):
+//   pressure non-equilibrium PressureNonEquilibriumCompressible.cu:45-311
+//
+// Every node writes only its own locations, and no node reads a location
+// another node of the same list writes (for a fixed location bit the map
+// node -> location index is one to one), so the kernels are race free.
+#include <cuda_runtime.h>
+
+#include "capi_common.cuh"
+#include "collision_math.cuh"
+#include "d3q27.cuh"
+#include "storage.cuh"
+
+namespace vfb
+{
+
+// directions in the order the reference's BC kernels visit them
+__host__ __device__ constexpr int qOrder(int j)
+{
+    constexpr int t[26] = { dP00, dM00, d0P0, d0M0, d00P, d00M, dPP0, dMM0, dPM0, dMP0, dP0P, dM0M, dP0M,
+                            dM0P, d0PP, d0MM, d0PM, d0MP, dPPP, dMMM, dPPM, dMMP, dPMP, dMPM, dPMM, dMPP };
+    return t[j];
+}
+
+template <class R>
+struct BcLattice {
+    unsigned long long N;
+    const uint32_t* __restrict__ nX;
+    const uint32_t* __restrict__ nY;
+    const uint32_t* __restrict__ nZ;
+    R omega;
+};
+
+// drho and velocity from post-collision populations with the plain sums of
+// NoSlipInterpolatedCompressible.cu:144-160 (g[d] moves in direction d)
+template <class R>
+__device__ __forceinline__ void bcMacros(const R* g, R& drho, R& vx1, R& vx2, R& vx3)
+{
+    R s = g[dPMP];
+    s = s + g[dMPP];
+    s = s + g[dPPP];
+    s = s + g[dMMP];
+    s = s + g[dPMM];
+    s = s + g[dMPM];
+    s = s + g[dPPM];
+    s = s + g[dMMM];
+    s = s + g[d0PM];
+    s = s + g[d0MP];
+    s = s + g[d0PP];
+    s = s + g[d0MM];
+    s = s + g[dP0M];
+    s = s + g[dM0P];
+    s = s + g[dP0P];
+    s = s + g[dM0M];
+    s = s + g[dPM0];
+    s = s + g[dMP0];
+    s = s + g[dPP0];
+    s = s + g[dMM0];
+    s = s + g[d00P];
+    s = s + g[d00M];
+    s = s + g[d0P0];
+    s = s + g[d0M0];
+    s = s + g[dP00];
+    s = s + g[dM00];
+    s = s + g[d000];
+    drho = s;
+    const R r1 = R(1) + s;
+    vx1 = (((g[dPMP] - g[dMPM]) - (g[dMPP] - g[dPMM])) + ((g[dPPP] - g[dMMM]) - (g[dMMP] - g[dPPM])) +
+           ((g[dP0M] - g[dM0P]) + (g[dP0P] - g[dM0M])) + ((g[dPM0] - g[dMP0]) + (g[dPP0] - g[dMM0])) +
+           (g[dP00] - g[dM00])) /
+          r1;
+    vx2 = ((-(g[dPMP] - g[dMPM]) + (g[dMPP] - g[dPMM])) + ((g[dPPP] - g[dMMM]) - (g[dMMP] - g[dPPM])) +
+           ((g[d0PM] - g[d0MP]) + (g[d0PP] - g[d0MM])) + (-(g[dPM0] - g[dMP0]) + (g[dPP0] - g[dMM0])) +
+           (g[d0P0] - g[d0M0])) /
+          r1;
+    vx3 = (((g[dPMP] - g[dMPM]) + (g[dMPP] - g[dPMM])) + ((g[dPPP] - g[dMMM]) + (g[dMMP] - g[dPPM])) +
+           (-(g[d0PM] - g[d0MP]) + (g[d0PP] - g[d0MM])) + ((g[dP0P] - g[dM0M]) - (g[dP0M] - g[dM0P])) +
+           (g[d00P] - g[d00M])) /
+          r1;
+}
+
+// KernelUtilities.h:171-174
+template <class R>
+__device__ __forceinline__ R feqBC(R drho, R vel, R cuSq, R w)
+{
+    return w * (drho + R(9) / R(2) * vel * vel * (R(1) + drho) - cuSq);
+}
+
+// KernelUtilities.h:189-195
+template <class R>
+__device__ __forceinline__ R interpNoSlip(R q, R f, R finv, R feq, R omega)
+{
+    return (R(1) - q) / (R(1) + q) * (f - finv + (f + finv - R(2) * feq * omega) / (R(1) - omega)) * (R(1) / R(2)) +
+           (q * (f + finv)) / (R(1) + q);
+}
+
+// KernelUtilities.h:176-182
+template <class R>
+__device__ __forceinline__ R interpVelocity(R q, R f, R finv, R feq, R omega, R vel, R w)
+{
+    return (R(1) - q) / (R(1) + q) * (f - finv + (f + finv - R(2) * feq * omega) / (R(1) - omega)) * (R(1) / R(2)) +
+           (q * (f + finv) - R(6) * w * vel) / (R(1) + q);
+}
+
+template <class S, int KIND, bool EVEN>
+__global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
+                                                     const int32_t* __restrict__ bcK,
+                                                     const typename Storage<S>::R* __restrict__ q, uint32_t nBC,
+                                                     const typename Storage<S>::R* __restrict__ Vx,
+                                                     const typename Storage<S>::R* __restrict__ Vy,
+                                                     const typename Storage<S>::R* __restrict__ Vz)
+{
+    using R = typename Storage<S>::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nBC)
+        return;
+    const unsigned long long N = lat.N;
+    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    // post-collision population moving in direction d: slot of inv(d), location of inv(d)
+    R g[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        g[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(inv(d)) * N + L.k[loc(inv(d))]);
+
+    R drho = R(0), vx1 = R(0), vx2 = R(0), vx3 = R(0), cuSq = R(0);
+    if (KIND == VFB_BC_NOSLIP_INTERPOLATED || KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_SLIP) {
+        bcMacros(g, drho, vx1, vx2, vx3);
+        cuSq = R(3) / R(2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3) * (R(1) + drho);
+    }
+    R UX = R(0), UY = R(0), UZ = R(0);
+    if (KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_VELOCITY_BOUNCE_BACK) {
+        UX = __ldg(Vx + i);
+        UY = __ldg(Vy + i);
+        UZ = __ldg(Vz + i);
+    }
+    // slip: normal components are removed for each axis with an active axis direction
+    bool flagX = false, flagY = false, flagZ = false;
+#pragma unroll
+    for (int j = 0; j < 26; ++j) {
+        const int d = qOrder(j);
+        const R qd = __ldg(q + (unsigned long long)d * nBC + i);
+        if (!(qd >= R(0) && qd <= R(1)))
+            continue;
+        const int e = inv(d);
+        S* target = dist + (unsigned long long)slot<!EVEN>(e) * N + L.k[loc(e)];
+        const R w = weight<R>(d);
+        R value;
+        if (KIND == VFB_BC_NOSLIP_BOUNCE_BACK) {
+            value = g[d];
+        } else if (KIND == VFB_BC_VELOCITY_BOUNCE_BACK) {
+            // 6 w (-c_d . U) with 6 w = 4/9, 1/9, 1/36 for face, edge, corner directions
+            const R k6 = order(d) == 1 ? R(4) / R(9) : order(d) == 2 ? R(1) / R(9) : R(1) / R(36);
+            value = g[d] + k6 * cdot<R>(e, UX, UY, UZ);
+        } else if (KIND == VFB_BC_NOSLIP_INTERPOLATED) {
+            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
+            value = interpNoSlip(qd, g[d], g[e], feq, lat.omega);
+        } else if (KIND == VFB_BC_VELOCITY_INTERPOLATED) {
+            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
+            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, UX, UY, UZ), w);
+        } else {
+            if (order(d) == 1) {
+                if (cx(d) != 0)
+                    flagX = true;
+                else if (cy(d) != 0)
+                    flagY = true;
+                else
+                    flagZ = true;
+            }
+            const R sx = flagX ? R(0) : vx1, sy = flagY ? R(0) : vx2, sz = flagZ ? R(0) : vx3;
+            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
+            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, sx, sy, sz), w);
+        }
+        Storage<S>::store(target, value);
+    }
+}
+
+// PressureNonEquilibriumCompressible.cu:75-309: the neighbour's
+// pre-collision populations with their equilibrium part moved from the
+// neighbour's density to the prescribed one, written into the BC node's
+// directions whose component along the normal axis differs from the normal's
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
+                                                         const int32_t* __restrict__ bcK,
+                                                         const int32_t* __restrict__ bcKN,
+                                                         const typename Storage<S>::R* __restrict__ rhoBC, uint32_t nBC,
+                                                         int axis, int sgn)
+{
+    using R = typename Storage<S>::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nBC)
+        return;
+    const unsigned long long N = lat.N;
+    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    const Locs LN = listIndices((uint32_t)__ldg(bcKN + i), lat.nX, lat.nY, lat.nZ);
+    R f[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)]);
+    R drho1 = pyramidDensity(f);
+    const R oneOverRho = R(1) / (drho1 + R(1));
+    const R vx1 = pyramidJx(f) * oneOverRho;
+    const R vx2 = pyramidJy(f) * oneOverRho;
+    const R vx3 = pyramidJz(f) * oneOverRho;
+    const R cusq = R(3) / R(2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == d000) {
+            f[d] -= R(8) / R(27) * (drho1 - (drho1 + R(1)) * cusq);
+        } else {
+            const R cu = cdot<R>(d, vx1, vx2, vx3);
+            f[d] -= weight<R>(d) * (drho1 + (drho1 + R(1)) * (R(3) * cu + R(9) / R(2) * cu * cu - cusq));
+        }
+    }
+    drho1 = __ldg(rhoBC + i);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == d000) {
+            f[d] += R(8) / R(27) * (drho1 - (drho1 + R(1)) * cusq);
+        } else {
+            const R cu = cdot<R>(d, vx1, vx2, vx3);
+            f[d] += weight<R>(d) * (drho1 + (drho1 + R(1)) * (R(3) * cu + R(9) / R(2) * cu * cu - cusq));
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const int c = axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d);
+        if (c == sgn)
+            continue;
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d]);
+    }
+}
+
+template <class S, int KIND>
+static void launchPostKind(bool even, unsigned blocks, cudaStream_t stream, S* dist, const BcLattice<typename Storage<S>::R>& lat,
+                           const vfb_bc_list* l)
+{
+    using R = typename Storage<S>::R;
+    const R* q = static_cast<const R*>(l->q);
+    const R* vx = static_cast<const R*>(l->Vx);
+    const R* vy = static_cast<const R*>(l->Vy);
+    const R* vz = static_cast<const R*>(l->Vz);
+    if (even)
+        bcPostKernel<S, KIND, true><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz);
+    else
+        bcPostKernel<S, KIND, false><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz);
+}
+
+template <class S>
+static int launchPost(int kind, const vfb_bc_lattice* t, const vfb_bc_list* l, cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    BcLattice<R> lat { t->numberOfLBnodes, t->neighborX, t->neighborY, t->neighborZ, (R)t->omega };
+    S* dist = static_cast<S*>(t->distributions);
+    const unsigned blocks = (l->numberOfBCnodes + 127) / 128;
+    const bool even = t->isEvenTimestep != 0;
+    switch (kind) {
+    case VFB_BC_NOSLIP_INTERPOLATED: launchPostKind<S, VFB_BC_NOSLIP_INTERPOLATED>(even, blocks, stream, dist, lat, l); break;
+    case VFB_BC_NOSLIP_BOUNCE_BACK: launchPostKind<S, VFB_BC_NOSLIP_BOUNCE_BACK>(even, blocks, stream, dist, lat, l); break;
+    case VFB_BC_VELOCITY_INTERPOLATED: launchPostKind<S, VFB_BC_VELOCITY_INTERPOLATED>(even, blocks, stream, dist, lat, l); break;
+    case VFB_BC_VELOCITY_BOUNCE_BACK: launchPostKind<S, VFB_BC_VELOCITY_BOUNCE_BACK>(even, blocks, stream, dist, lat, l); break;
+    default: launchPostKind<S, VFB_BC_SLIP>(even, blocks, stream, dist, lat, l); break;
+    }
+    return checkLaunch("post-collision boundary condition");
+}
+
+template <class S>
+static int launchPressure(const vfb_bc_lattice* t, const int32_t* k, const int32_t* kN, const void* rhoBC, uint32_t n,
+                          int axis, int sgn, cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    BcLattice<R> lat { t->numberOfLBnodes, t->neighborX, t->neighborY, t->neighborZ, (R)t->omega };
+    S* dist = static_cast<S*>(t->distributions);
+    const unsigned blocks = (n + 127) / 128;
+    const R* rho = static_cast<const R*>(rhoBC);
+    if (t->isEvenTimestep)
+        bcPressureKernel<S, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, rho, n, axis, sgn);
+    else
+        bcPressureKernel<S, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, rho, n, axis, sgn);
+    return checkLaunch("pressure boundary condition");
+}
+
+static int checkLattice(const vfb_bc_lattice* t)
+{
+    if (!t || !t->distributions || !t->neighborX || !t->neighborY || !t->neighborZ)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL lattice or lattice array");
+    if (t->numberOfLBnodes < 2)
+        return setError(VFB_ERR_OUT_OF_RANGE, "numberOfLBnodes %llu < 2", t->numberOfLBnodes);
+    return VFB_OK;
+}
+
+} // namespace vfb
+
+using namespace vfb;
+
+extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice, const vfb_bc_list* list, void* stream)
+{
+    clearError();
+    if (kind < VFB_BC_NOSLIP_INTERPOLATED || kind > VFB_BC_SLIP)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown BC kind %d", kind);
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (!list)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "list is NULL");
+    if (list->numberOfBCnodes == 0)
+        return VFB_OK;
+    if (const int rc = checkLattice(lattice))
+        return rc;
+    if (!list->k || !list->q)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL k or q of the BC list");
+    if ((kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_VELOCITY_BOUNCE_BACK) &&
+        (!list->Vx || !list->Vy || !list->Vz))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "velocity BC needs Vx, Vy, Vz");
+    if ((kind == VFB_BC_NOSLIP_INTERPOLATED || kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_SLIP) &&
+        !(lattice->omega > 0.0 && lattice->omega < 2.0 && lattice->omega != 1.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "omega %g outside (0, 2) or equal to 1 (the interpolation divides by 1 - omega)",
+                        lattice->omega);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchPost<float>(kind, lattice, list, s);
+    case VFB_FP64: return launchPost<double>(kind, lattice, list, s);
+    case VFB_FP16: return launchPost<__half>(kind, lattice, list, s);
+    default: return launchPost<__nv_bfloat16>(kind, lattice, list, s);
+    }
+}
+
+extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,
+                                     const void* rhoBC, uint32_t numberOfBCnodes, int direction, void* stream)
+{
+    clearError();
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (numberOfBCnodes == 0)
+        return VFB_OK;
+    if (const int rc = checkLattice(lattice))
+        return rc;
+    if (!k || !kN || !rhoBC)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL k, kN or rhoBC");
+    if (direction < dP00 || direction > d00M)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "direction %d is not an axis direction (1..6)", direction);
+    const int axis = cx(direction) != 0 ? 0 : cy(direction) != 0 ? 1 : 2;
+    const int sgn = axis == 0 ? cx(direction) : axis == 1 ? cy(direction) : cz(direction);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchPressure<float>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    case VFB_FP64: return launchPressure<double>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    case VFB_FP16: return launchPressure<__half>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    }
+}

@@ -25,6 +25,16 @@ if torch is not None:
                         torch.bfloat16: _lib.BF16}
 
 
+# FP16 storage holds the shifted populations times this power of two (so that
+# deviations of order 1e-6 stay normal numbers); the kernels undo it on load
+HALF_STORAGE_SCALE = 4096.0
+
+
+def storage_scale(storage_dtype) -> float:
+    """Factor between a stored population and its value (1 except FP16)."""
+    return HALF_STORAGE_SCALE if storage_dtype == torch.float16 else 1.0
+
+
 def compute_dtype(storage_dtype):
     return torch.float64 if storage_dtype == torch.float64 else torch.float32
 
@@ -171,3 +181,38 @@ def mass_and_energy(dist, lat: DeviceLattice, is_even: bool, nodes=None, stream=
                                               lat.neighborY.data_ptr(), lat.neighborZ.data_ptr(), idx.data_ptr(),
                                               int(idx.numel()), int(bool(is_even)), out, _stream(stream)))
     return out[0], out[1], int(out[2])
+
+
+def _bc_lattice(dist, lat: DeviceLattice, omega: float, is_even: bool) -> _lib.BcLattice:
+    t = _lib.BcLattice()
+    t.distributions = dist.data_ptr()
+    t.numberOfLBnodes = lat.N
+    t.neighborX = lat.neighborX.data_ptr()
+    t.neighborY = lat.neighborY.data_ptr()
+    t.neighborZ = lat.neighborZ.data_ptr()
+    t.omega = float(omega)
+    t.isEvenTimestep = int(bool(is_even))
+    return t
+
+
+def bc_post(kind: int, dist, lat: DeviceLattice, k, q, omega: float, is_even: bool, vx=None, vy=None, vz=None,
+            stream=None) -> None:
+    """One post-collision BC kernel (``kind`` one of _lib.BC_*) over a list:
+    ``k`` int32 node indices, ``q`` compute-precision array of 27 * len(k)
+    (direction-major), ``vx``/``vy``/``vz`` per-node wall velocity."""
+    lst = _lib.BcList()
+    lst.k = k.data_ptr()
+    lst.q = q.data_ptr()
+    lst.Vx, lst.Vy, lst.Vz = _p(vx), _p(vy), _p(vz)
+    lst.numberOfBCnodes = int(k.numel())
+    t = _bc_lattice(dist, lat, omega, is_even)
+    _lib.check(_lib.lib().vfb_bc_post(int(kind), STORAGE_OF_DTYPE[dist.dtype], ctypes.byref(t), ctypes.byref(lst),
+                                      _stream(stream)))
+
+
+def bc_pressure(dist, lat: DeviceLattice, k, kN, rho, direction: int, is_even: bool, stream=None) -> None:
+    """The pre-collision non-equilibrium pressure BC of one directional list."""
+    t = _bc_lattice(dist, lat, 1.0, is_even)
+    _lib.check(_lib.lib().vfb_bc_pressure_noneq(STORAGE_OF_DTYPE[dist.dtype], ctypes.byref(t), k.data_ptr(),
+                                                kN.data_ptr(), rho.data_ptr(), int(k.numel()), int(direction),
+                                                _stream(stream)))
