@@ -220,6 +220,53 @@ int vfb_grid_copy(void* grid, int level, const char* name, void* out);
 void vfb_grid_free(void* grid);
 
 /*
+ * Simulation: the host side of the time step.  Mirrors Simulation /
+ * UpdateGrid27 of the reference (src/gpu/core/Calculation/Simulation.cpp:117-441,
+ * UpdateGrid27.cpp:54-96,228-308): it owns every level's device arrays
+ * (uploaded from a vfb_grid handle), selects the collision and BC kernels like
+ * KernelFactory / BoundaryConditionFactory, and runs the recursive per-level
+ * substep schedule
+ *   updateGrid(level): if level is not the finest, updateGrid(level + 1) twice;
+ *                      collision; post-collision BCs (velocity, no-slip, slip,
+ *                      geometry); parity swap; pre-collision BCs (pressure);
+ *                      if not the finest, fine-to-coarse then coarse-to-fine.
+ * Level l uses nu_l = nu * 2^l, omega_l = 1 / (3 nu_l + 1/2) and force factor
+ * 2^-l (Parameter.cpp:395-420).
+ */
+typedef struct vfb_sim_params {
+    int storage;               /* VFB_FP32 / FP64 / FP16 / BF16 */
+    int collisionKernel;       /* 0 "K17CompressibleNavierStokes", 1 "BGKCompSP27" (KernelTypes.h:36-38) */
+    int velocityBC;            /* VFB_BC_VELOCITY_INTERPOLATED or VFB_BC_VELOCITY_BOUNCE_BACK */
+    int noSlipBC;              /* VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK, -1 NoSlipDelayBounceBack (no kernel) */
+    int geometryBC;            /* as noSlipBC, for the geometry list */
+    int slipBC;                /* VFB_BC_SLIP or -1 */
+    int pressureBC;            /* 0 PressureNonEquilibriumCompressible, -1 none */
+    double viscosity;          /* coarse-level kinematic viscosity, lattice units */
+    double forces[3];          /* global acceleration */
+    double quadricLimiters[3]; /* default 0.01 each (Parameter.cpp:69) */
+    int usePlan;               /* 1: the planned (bulk-copy) collision kernels */
+} vfb_sim_params;
+
+typedef struct vfb_simulation vfb_simulation;
+/* uploads every level of grid (a vfb_grid_build handle; it may be freed afterwards) */
+int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simulation** sim, void* stream);
+int vfb_sim_destroy(vfb_simulation* sim);
+int vfb_sim_levels(const vfb_simulation* sim);
+/* equilibrium from host arrays (compute precision, numberOfLBnodes of the
+ * level) into both parity views, odd then even (PreProcessorImp.cpp:50-58) */
+int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rho, const void* vx, const void* vy, const void* vz,
+                       void* stream);
+/* coarse time steps (each runs 2^l substeps of level l) */
+int vfb_sim_run(vfb_simulation* sim, unsigned int steps, void* stream);
+/* macroscopic fields of a level into host arrays (compute precision); synchronises */
+int vfb_sim_macroscopic(vfb_simulation* sim, int level, void* rho, void* vx, void* vy, void* vz, void* stream);
+/* FP64 sums over the level's fluid nodes (see vfb_mass_and_energy) */
+int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* out3, void* stream);
+/* the level's device population array and its parity, for inspection */
+int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,
+                        int* isEvenTimestep, double* omega);
+
+/*
  * Equilibrium initialisation of one parity view from drho and velocity
  * (compute precision arrays of numberOfLBnodes).  Replaces
  * InitNavierStokesCompressible_Device

@@ -1,0 +1,152 @@
+"""The C++ time-step schedule (vfb_sim_*, driven through the pyfluids-style
+Simulation) against the oracle running the reference's UpdateGrid27 order
+(collision, post-collision BCs velocity / slip, parity swap, pressure BC) on
+walled grids."""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from tests.gpu_helpers import rel_l2, rel_max
+from virtualfluids_b200 import _lib
+from virtualfluids_b200.grid import MultipleGridBuilder, SideType
+from virtualfluids_b200.simulation import (BoundaryConditionFactory, Parameter, PressureBC, SlipBC, Simulation,
+                                           VelocityBC)
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def cavity(n):
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, n - 1, n - 1, n - 1, 1.0)
+    b.buildGrids()
+    for s in (SideType.MX, SideType.PX, SideType.MY, SideType.PY, SideType.MZ):
+        b.setNoSlipBoundaryCondition(s)
+    b.setVelocityBoundaryCondition(SideType.PZ, 0.05, 0.0, 0.0)
+    return b
+
+
+def channel():
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, 15, 7, 7, 1.0)
+    b.setPeriodicBoundaryCondition(False, True, False)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(SideType.MX, 0.04, 0.0, 0.0)
+    b.setPressureBoundaryCondition(SideType.PX, 0.0)
+    b.setNoSlipBoundaryCondition(SideType.MZ)
+    b.setSlipBoundaryCondition(SideType.PZ, 0.0, 0.0, 1.0)
+    return b
+
+
+def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, velocity_kind=2):
+    """UpdateGrid27::updateGrid for one level, on the oracle."""
+    O = Oracle(precision)
+    real = O.real
+    N = len(g["geo"])
+    nx, ny, nz, geo, fl = g["neighborX"], g["neighborY"], g["neighborZ"], g["geo"], g["fluid"]
+    d = np.zeros(27 * N, real)
+    for ev in (0, 1):
+        O.init_eq(d, N, geo, nx, ny, nz, *[a.astype(real) for a in init], ev)
+    om = 1.0 / (3.0 * nu + 0.5)
+    vel = [g[f"velocity.{c}"].astype(real) for c in ("vx", "vy", "vz")]
+    even = True
+    for _ in range(steps):
+        O.collision_k17(d, N, nx, ny, nz, fl, om, forces=(0, 0, 0), force_factor=1.0, limiters=(0.01, 0.01, 0.01),
+                        is_even=even)
+        O.bc_post(velocity_kind, d, N, nx, ny, nz, g["velocity.k"], g["velocity.q"].astype(real), om, *vel,
+                  is_even=even)
+        if slip:
+            O.bc_post(4, d, N, nx, ny, nz, g["slip.k"], g["slip.q"].astype(real), om, is_even=even)
+        even = not even
+        if pressure:
+            O.bc_pressure(d, N, nx, ny, nz, g["pressure0.k"], g["pressure0.kN"], g["pressure0.rho"].astype(real),
+                          int(g["pressure0.dir"][0]), is_even=even)
+    return O.macroscopic(d, N, geo, nx, ny, nz, even)
+
+
+def _init(g, seed=2):
+    rng = np.random.default_rng(seed)
+    N = len(g["geo"])
+    f = [rng.uniform(-1e-3, 1e-3, N) for _ in range(4)]
+    for a in f:
+        a[g["geo"] != 19] = 0.0
+    return f
+
+
+@pytest.mark.parametrize("storage", ["fp64", "fp32"])
+@pytest.mark.parametrize("use_plan", [True, False])
+def test_cavity_schedule_matches_oracle(cuda, storage, use_plan):
+    b = cavity(12)
+    p = Parameter()
+    p.set_storage(storage)
+    p.set_viscosity_LB(0.0032)
+    p.use_plan = use_plan
+    sim = Simulation(p, b, BoundaryConditionFactory())
+    g = sim.levels[0]
+    init = _init(g)
+    sim.init_level(0, *init)
+    steps = 30
+    sim.run(steps)
+    got = sim.macroscopic(0)
+    ref = oracle_schedule(g, "f64" if storage == "fp64" else "f32", 0.0032, steps, init)
+    fl = g["fluid"]
+    for a, r in zip(got, ref):
+        if storage == "fp64":
+            assert rel_max(a[fl], r[fl]) < 1e-12
+        else:
+            assert rel_l2(a[fl], r[fl]) < 1e-5
+    _, _, bad = sim.mass_and_energy(0)
+    assert bad == 0
+
+
+def test_channel_schedule_with_slip_and_pressure(cuda):
+    b = channel()
+    p = Parameter()
+    p.set_viscosity_LB(0.01)
+    bc = BoundaryConditionFactory()
+    bc.set_velocity_boundary_condition(VelocityBC.VelocityInterpolatedCompressible)
+    bc.set_slip_boundary_condition(SlipBC.SlipCompressible)
+    bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+    sim = Simulation(p, b, bc)
+    g = sim.levels[0]
+    init = _init(g, 5)
+    sim.init_level(0, *init)
+    sim.run(20)
+    got = sim.macroscopic(0)
+    ref = oracle_schedule(g, "f64", 0.01, 20, init, slip=True, pressure=True)
+    fl = g["fluid"]
+    for a, r in zip(got, ref):
+        assert rel_max(a[fl], r[fl]) < 1e-12
+
+
+def test_velocity_bounce_back_selection(cuda):
+    b = cavity(8)
+    p = Parameter()
+    p.set_viscosity_LB(0.01)
+    bc = BoundaryConditionFactory()
+    bc.set_velocity_boundary_condition(VelocityBC.VelocityBounceBack)
+    sim = Simulation(p, b, bc)
+    g = sim.levels[0]
+    init = _init(g, 9)
+    sim.init_level(0, *init)
+    sim.run(10)
+    got = sim.macroscopic(0)
+    ref = oracle_schedule(g, "f64", 0.01, 10, init, velocity_kind=_lib.BC_VELOCITY_BOUNCE_BACK)
+    fl = g["fluid"]
+    for a, r in zip(got, ref):
+        assert rel_max(a[fl], r[fl]) < 1e-12
+
+
+def test_initial_condition_function_and_parity(cuda):
+    b = cavity(8)
+    p = Parameter()
+    p.set_viscosity_LB(0.01)
+    p.set_initial_condition(lambda x, y, z: (0.0 * x, 0.01 * np.sin(z), 0.0 * x, 0.0 * x))
+    sim = Simulation(p, b, BoundaryConditionFactory())
+    rho, vx, vy, vz = sim.macroscopic(0)
+    g = sim.levels[0]
+    fl = g["fluid"]
+    assert np.abs(vx[fl] - 0.01 * np.sin(g["coordZ"][fl])).max() < 1e-12
+    assert sim.level_state(0)[2] is True
+    sim.run(3)
+    assert sim.level_state(0)[2] is False

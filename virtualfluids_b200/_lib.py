@@ -110,6 +110,21 @@ _SIGNATURES = [
     ("vfb_bc_pressure_noneq", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
       ctypes.c_int, ctypes.c_void_p]),
+    ("vfb_sim_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    ("vfb_sim_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("vfb_sim_levels", ctypes.c_int, [ctypes.c_void_p]),
+    ("vfb_sim_init_level", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ("vfb_sim_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]),
+    ("vfb_sim_macroscopic", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ("vfb_sim_mass_and_energy", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_sim_level_state", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong),
+      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     ("vfb_collision_plan_create", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),

@@ -1,0 +1,529 @@
+// simulation.cpp -- the host side of the time step: level data, kernel
+// selection and the recursive per-level substep schedule of the reference's
+// UpdateGrid27 (src/gpu/core/Calculation/UpdateGrid27.cpp:54-96,228-308),
+// calling the kernels through the library's own C ABI.
+//
+// Everything here is stream ordered on the caller's stream; the host never
+// waits except where a call returns data to the host.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "capi_common.cuh"
+
+namespace vfb
+{
+namespace
+{
+
+int elementBytes(int storage) { return vfb_storage_bytes(storage); }
+bool computeIsDouble(int storage) { return storage == VFB_FP64; }
+
+// a device array owned by the simulation
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t allocate(size_t n)
+    {
+        bytes = n;
+        return cudaMalloc(&ptr, n ? n : 1);
+    }
+    ~DeviceBuffer()
+    {
+        if (ptr)
+            cudaFree(ptr);
+    }
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+};
+
+struct BcListDevice {
+    DeviceBuffer k, q, vx, vy, vz;
+    uint32_t n = 0;
+};
+
+struct PressureListDevice {
+    DeviceBuffer k, kN, rho;
+    uint32_t n = 0;
+    int direction = 0;
+};
+
+struct Level {
+    unsigned long long N = 0;
+    uint32_t nFluid = 0;
+    DeviceBuffer dist, nX, nY, nZ, geo, fluid;
+    BcListDevice velocity, noSlip, slip, geometry;
+    std::vector<PressureListDevice*> pressure;
+    double omega = 1.0;
+    double forceFactor = 1.0;
+    bool isEven = true;
+    vfb_collision_plan* plan = nullptr;
+    ~Level()
+    {
+        for (auto* p : pressure)
+            delete p;
+        if (plan)
+            vfb_collision_plan_destroy(plan);
+    }
+};
+
+} // namespace
+} // namespace vfb
+
+struct vfb_simulation {
+    vfb_sim_params params;
+    std::vector<vfb::Level*> levels;
+    ~vfb_simulation()
+    {
+        for (auto* l : levels)
+            delete l;
+    }
+};
+
+namespace vfb
+{
+namespace
+{
+
+// copies a grid array of `name` (count elements of elemSize bytes) to the host
+bool gridArray(void* grid, int level, const char* name, std::vector<char>& out, long long& count, int& elemSize)
+{
+    count = vfb_grid_count(grid, level, name);
+    elemSize = vfb_grid_elem_size(grid, level, name);
+    if (count < 0 || elemSize <= 0)
+        return false;
+    out.resize((size_t)count * elemSize);
+    return vfb_grid_copy(grid, level, name, out.empty() ? nullptr : out.data()) == VFB_OK;
+}
+
+cudaError_t uploadRaw(DeviceBuffer& b, const void* host, size_t bytes, cudaStream_t s)
+{
+    cudaError_t e = b.allocate(bytes);
+    if (e == cudaSuccess && bytes)
+        e = cudaMemcpyAsync(b.ptr, host, bytes, cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+// uploads a double array as the compute precision of the storage
+cudaError_t uploadReal(DeviceBuffer& b, const std::vector<char>& raw, int storage, cudaStream_t s,
+                       std::vector<std::vector<char>>& keep)
+{
+    const size_t n = raw.size() / sizeof(double);
+    const double* src = reinterpret_cast<const double*>(raw.data());
+    keep.emplace_back();
+    std::vector<char>& host = keep.back();
+    if (computeIsDouble(storage)) {
+        host = raw;
+    } else {
+        host.resize(n * sizeof(float));
+        float* dst = reinterpret_cast<float*>(host.data());
+        for (size_t i = 0; i < n; ++i)
+            dst[i] = (float)src[i];
+    }
+    return uploadRaw(b, host.data(), host.size(), s);
+}
+
+int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, std::vector<std::vector<char>>& keep)
+{
+    std::vector<char> raw;
+    long long count = 0;
+    int es = 0;
+    auto fail = [&](const char* what) { return setError(VFB_ERR_CONFIGURATION, "grid level %d: array %s", level, what); };
+    auto need = [&](const char* name, int elem) -> bool {
+        return gridArray(grid, level, name, raw, count, es) && es == elem;
+    };
+    cudaError_t e = cudaSuccess;
+    if (!need("geo", 4))
+        return fail("geo");
+    L.N = (unsigned long long)count;
+    keep.push_back(raw);
+    e = uploadRaw(L.geo, keep.back().data(), raw.size(), s);
+    const char* nb[3] = { "neighborX", "neighborY", "neighborZ" };
+    DeviceBuffer* nbuf[3] = { &L.nX, &L.nY, &L.nZ };
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+        if (!need(nb[i], 4) || (unsigned long long)count != L.N)
+            return fail(nb[i]);
+        keep.push_back(raw);
+        e = uploadRaw(*nbuf[i], keep.back().data(), raw.size(), s);
+    }
+    if (e == cudaSuccess) {
+        if (!need("fluid", 4))
+            return fail("fluid");
+        L.nFluid = (uint32_t)count;
+        keep.push_back(raw);
+        e = uploadRaw(L.fluid, keep.back().data(), raw.size(), s);
+    }
+    // compacted BC lists: k (int32), q (27 * n doubles), velocities
+    auto list = [&](const std::string& prefix, BcListDevice& B, bool velocity) -> int {
+        if (!need((prefix + ".k").c_str(), 4))
+            return fail((prefix + ".k").c_str());
+        B.n = (uint32_t)count;
+        keep.push_back(raw);
+        e = uploadRaw(B.k, keep.back().data(), raw.size(), s);
+        if (e != cudaSuccess)
+            return VFB_OK;
+        if (!need((prefix + ".q").c_str(), 8) || (unsigned long long)count != 27ull * B.n)
+            return fail((prefix + ".q").c_str());
+        e = uploadReal(B.q, raw, storage, s, keep);
+        if (velocity) {
+            const char* v[3] = { ".vx", ".vy", ".vz" };
+            DeviceBuffer* vb[3] = { &B.vx, &B.vy, &B.vz };
+            for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+                if (!need((prefix + v[i]).c_str(), 8) || (uint32_t)count != B.n)
+                    return fail((prefix + v[i]).c_str());
+                e = uploadReal(*vb[i], raw, storage, s, keep);
+            }
+        }
+        return VFB_OK;
+    };
+    if (e == cudaSuccess)
+        if (const int rc = list("velocity", L.velocity, true))
+            return rc;
+    if (e == cudaSuccess)
+        if (const int rc = list("slip", L.slip, false))
+            return rc;
+    if (e == cudaSuccess)
+        if (const int rc = list("geometry", L.geometry, false))
+            return rc;
+    if (e == cudaSuccess && need("pressure.count", 4) && count == 1) {
+        const int np = *reinterpret_cast<const int32_t*>(raw.data());
+        for (int i = 0; i < np && e == cudaSuccess; ++i) {
+            auto* P = new PressureListDevice;
+            L.pressure.push_back(P);
+            const std::string p = "pressure" + std::to_string(i);
+            if (!need((p + ".k").c_str(), 4))
+                return fail((p + ".k").c_str());
+            P->n = (uint32_t)count;
+            keep.push_back(raw);
+            e = uploadRaw(P->k, keep.back().data(), raw.size(), s);
+            if (e == cudaSuccess) {
+                if (!need((p + ".kN").c_str(), 4) || (uint32_t)count != P->n)
+                    return fail((p + ".kN").c_str());
+                keep.push_back(raw);
+                e = uploadRaw(P->kN, keep.back().data(), raw.size(), s);
+            }
+            if (e == cudaSuccess) {
+                if (!need((p + ".rho").c_str(), 8) || (uint32_t)count != P->n)
+                    return fail((p + ".rho").c_str());
+                e = uploadReal(P->rho, raw, storage, s, keep);
+            }
+            if (e == cudaSuccess) {
+                if (!need((p + ".dir").c_str(), 4) || count != 1)
+                    return fail((p + ".dir").c_str());
+                P->direction = *reinterpret_cast<const int32_t*>(raw.data());
+            }
+        }
+    }
+    if (e == cudaSuccess)
+        e = L.dist.allocate(27ull * L.N * (size_t)elementBytes(storage));
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(L.dist.ptr, 0, L.dist.bytes, s);
+    if (e != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "grid level %d: device upload failed: %s", level, cudaGetErrorString(e));
+    return VFB_OK;
+}
+
+} // namespace
+} // namespace vfb
+
+namespace vfb
+{
+namespace
+{
+
+vfb_collision_args collisionArgs(const vfb_simulation& S, const Level& L)
+{
+    vfb_collision_args a;
+    std::memset(&a, 0, sizeof(a));
+    a.distributions = L.dist.ptr;
+    a.numberOfLBnodes = L.N;
+    a.neighborX = static_cast<const uint32_t*>(L.nX.ptr);
+    a.neighborY = static_cast<const uint32_t*>(L.nY.ptr);
+    a.neighborZ = static_cast<const uint32_t*>(L.nZ.ptr);
+    a.fluidNodeIndices = static_cast<const uint32_t*>(L.fluid.ptr);
+    a.numberOfFluidNodes = L.nFluid;
+    a.omega = L.omega;
+    for (int i = 0; i < 3; ++i) {
+        a.forces[i] = S.params.forces[i];
+        a.quadricLimiters[i] = S.params.quadricLimiters[i];
+    }
+    a.forceFactor = L.forceFactor;
+    a.isEvenTimestep = L.isEven ? 1 : 0;
+    a.collisionTemplate = VFB_TEMPLATE_DEFAULT;
+    return a;
+}
+
+vfb_bc_lattice bcLattice(const Level& L)
+{
+    vfb_bc_lattice t;
+    t.distributions = L.dist.ptr;
+    t.numberOfLBnodes = L.N;
+    t.neighborX = static_cast<const uint32_t*>(L.nX.ptr);
+    t.neighborY = static_cast<const uint32_t*>(L.nY.ptr);
+    t.neighborZ = static_cast<const uint32_t*>(L.nZ.ptr);
+    t.omega = L.omega;
+    t.isEvenTimestep = L.isEven ? 1 : 0;
+    return t;
+}
+
+vfb_bc_list bcList(const BcListDevice& B)
+{
+    vfb_bc_list l;
+    l.k = static_cast<const int32_t*>(B.k.ptr);
+    l.q = B.q.ptr;
+    l.Vx = B.vx.ptr;
+    l.Vy = B.vy.ptr;
+    l.Vz = B.vz.ptr;
+    l.numberOfBCnodes = B.n;
+    return l;
+}
+
+// CollisionStrategy (CollisisionStrategy.cpp:67-98): the fluid-node list of the level
+int collision(vfb_simulation& S, Level& L, void* stream)
+{
+    vfb_collision_args a = collisionArgs(S, L);
+    const bool k17 = S.params.collisionKernel == 0;
+    if (L.plan)
+        return k17 ? vfb_k17_collision_planned(L.plan, &a, stream) : vfb_bgk_collision_planned(L.plan, &a, stream);
+    return k17 ? vfb_k17_collision(S.params.storage, &a, stream) : vfb_bgk_collision(S.params.storage, &a, stream);
+}
+
+// UpdateGrid27::postCollisionBC (UpdateGrid27.cpp:228-263): velocity, no-slip,
+// slip, (stress: not built), geometry; every kernel only when its list is not empty
+int postCollisionBC(vfb_simulation& S, Level& L, void* stream)
+{
+    const vfb_bc_lattice t = bcLattice(L);
+    const int storage = S.params.storage;
+    struct Item {
+        const BcListDevice* list;
+        int kind;
+    } items[4] = { { &L.velocity, S.params.velocityBC },
+                   { &L.noSlip, S.params.noSlipBC },
+                   { &L.slip, S.params.slipBC },
+                   { &L.geometry, S.params.geometryBC } };
+    for (const Item& it : items) {
+        if (it.list->n == 0 || it.kind < 0)
+            continue;
+        const vfb_bc_list l = bcList(*it.list);
+        if (const int rc = vfb_bc_post(it.kind, storage, &t, &l, stream))
+            return rc;
+    }
+    return VFB_OK;
+}
+
+// UpdateGrid27::preCollisionBC (UpdateGrid27.cpp:289-308): the pressure lists
+int preCollisionBC(vfb_simulation& S, Level& L, void* stream)
+{
+    if (S.params.pressureBC < 0)
+        return VFB_OK;
+    const vfb_bc_lattice t = bcLattice(L);
+    for (const PressureListDevice* P : L.pressure) {
+        if (P->n == 0)
+            continue;
+        if (const int rc = vfb_bc_pressure_noneq(S.params.storage, &t, static_cast<const int32_t*>(P->k.ptr),
+                                                 static_cast<const int32_t*>(P->kN.ptr), P->rho.ptr, P->n,
+                                                 P->direction, stream))
+            return rc;
+    }
+    return VFB_OK;
+}
+
+// UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-96)
+int updateGrid(vfb_simulation& S, int level, void* stream)
+{
+    const int finest = (int)S.levels.size() - 1;
+    if (level != finest) {
+        if (const int rc = updateGrid(S, level + 1, stream))
+            return rc;
+        if (const int rc = updateGrid(S, level + 1, stream))
+            return rc;
+    }
+    Level& L = *S.levels[level];
+    if (const int rc = collision(S, L, stream))
+        return rc;
+    if (const int rc = postCollisionBC(S, L, stream))
+        return rc;
+    L.isEven = !L.isEven; // swapBetweenEvenAndOddTimestep (:265-269)
+    if (const int rc = preCollisionBC(S, L, stream))
+        return rc;
+    if (level != finest)
+        return setError(VFB_ERR_UNSUPPORTED, "grid refinement (fine-to-coarse / coarse-to-fine) is not built");
+    return VFB_OK;
+}
+
+bool validKind(int k, int lo, int hi) { return k < 0 || (k >= lo && k <= hi); }
+
+} // namespace
+} // namespace vfb
+
+using namespace vfb;
+
+extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simulation** sim, void* stream)
+{
+    clearError();
+    if (!params || !grid || !sim)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *sim = nullptr;
+    const vfb_sim_params& P = *params;
+    if (elementBytes(P.storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", P.storage);
+    if (P.collisionKernel != 0 && P.collisionKernel != 1)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown collision kernel %d", P.collisionKernel);
+    if (P.velocityBC != VFB_BC_VELOCITY_INTERPOLATED && P.velocityBC != VFB_BC_VELOCITY_BOUNCE_BACK)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "velocityBC must be a velocity kind");
+    if (!validKind(P.noSlipBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
+        !validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
+        !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC < 0 || P.pressureBC == 0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "invalid boundary-condition selection");
+    if (!(P.viscosity > 0.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "viscosity %g must be positive", P.viscosity);
+    const int nLevels = vfb_grid_levels(grid);
+    if (nLevels < 1)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "grid has no level");
+    auto* S = new vfb_simulation;
+    S->params = P;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::vector<std::vector<char>> keep;
+    int rc = VFB_OK;
+    for (int l = 0; l < nLevels && rc == VFB_OK; ++l) {
+        auto* L = new Level;
+        S->levels.push_back(L);
+        rc = uploadLevel(*L, grid, l, P.storage, s, keep);
+        // Parameter::initLBMSimulationParameter (Parameter.cpp:395-420)
+        const double nu = P.viscosity * std::pow(2.0, l);
+        L->omega = 1.0 / (3.0 * nu + 0.5);
+        L->forceFactor = 1.0 / std::pow(2.0, l);
+    }
+    if (rc == VFB_OK && cudaStreamSynchronize(s) != cudaSuccess)
+        rc = setError(VFB_ERR_CUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+    for (size_t l = 0; l < S->levels.size() && rc == VFB_OK && P.usePlan; ++l) {
+        Level& L = *S->levels[l];
+        vfb_collision_args a = collisionArgs(*S, L);
+        rc = vfb_collision_plan_create(P.storage, &a, &L.plan, stream);
+    }
+    if (rc != VFB_OK) {
+        delete S;
+        return rc;
+    }
+    *sim = S;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_destroy(vfb_simulation* sim)
+{
+    clearError();
+    delete sim;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_levels(const vfb_simulation* sim) { return sim ? (int)sim->levels.size() : 0; }
+
+static Level* levelOf(vfb_simulation* sim, int level)
+{
+    if (!sim || level < 0 || level >= (int)sim->levels.size()) {
+        setError(VFB_ERR_INVALID_ARGUMENT, "no level %d", level);
+        return nullptr;
+    }
+    return sim->levels[level];
+}
+
+extern "C" int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rho, const void* vx, const void* vy,
+                                  const void* vz, void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!rho || !vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL field");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t bytes = L->N * (computeIsDouble(sim->params.storage) ? sizeof(double) : sizeof(float));
+    DeviceBuffer f[4];
+    const void* host[4] = { rho, vx, vy, vz };
+    for (int i = 0; i < 4; ++i)
+        if (uploadRaw(f[i], host[i], bytes, s) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "field upload failed");
+    int rc = VFB_OK;
+    for (int even = 0; even < 2 && rc == VFB_OK; ++even)
+        rc = vfb_init_equilibrium(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->geo.ptr),
+                                  static_cast<const uint32_t*>(L->nX.ptr), static_cast<const uint32_t*>(L->nY.ptr),
+                                  static_cast<const uint32_t*>(L->nZ.ptr), f[0].ptr, f[1].ptr, f[2].ptr, f[3].ptr, even,
+                                  stream);
+    L->isEven = true;
+    // the temporary fields are freed on return: wait for the init kernels
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == VFB_OK)
+        rc = setError(VFB_ERR_CUDA, "init failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return rc;
+}
+
+extern "C" int vfb_sim_run(vfb_simulation* sim, unsigned int steps, void* stream)
+{
+    clearError();
+    if (!sim)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "sim is NULL");
+    for (unsigned int t = 0; t < steps; ++t)
+        if (const int rc = updateGrid(*sim, 0, stream))
+            return rc;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_macroscopic(vfb_simulation* sim, int level, void* rho, void* vx, void* vy, void* vz,
+                                   void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!rho || !vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL output");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t bytes = L->N * (computeIsDouble(sim->params.storage) ? sizeof(double) : sizeof(float));
+    DeviceBuffer f[4];
+    for (int i = 0; i < 4; ++i)
+        if (f[i].allocate(bytes) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "allocation failed");
+    int rc = vfb_macroscopic(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->geo.ptr),
+                             static_cast<const uint32_t*>(L->nX.ptr), static_cast<const uint32_t*>(L->nY.ptr),
+                             static_cast<const uint32_t*>(L->nZ.ptr), L->isEven ? 1 : 0, f[0].ptr, f[1].ptr, f[2].ptr,
+                             f[3].ptr, stream);
+    void* out[4] = { rho, vx, vy, vz };
+    for (int i = 0; i < 4 && rc == VFB_OK; ++i)
+        if (cudaMemcpyAsync(out[i], f[i].ptr, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            rc = setError(VFB_ERR_CUDA, "copy failed");
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == VFB_OK)
+        rc = setError(VFB_ERR_CUDA, "macroscopic failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return rc;
+}
+
+extern "C" int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* out3, void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    return vfb_mass_and_energy(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->nX.ptr),
+                               static_cast<const uint32_t*>(L->nY.ptr), static_cast<const uint32_t*>(L->nZ.ptr),
+                               static_cast<const uint32_t*>(L->fluid.ptr), L->nFluid, L->isEven ? 1 : 0, out3, stream);
+}
+
+extern "C" int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions,
+                                   unsigned long long* numberOfLBnodes, int* isEvenTimestep, double* omega)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (distributions)
+        *distributions = L->dist.ptr;
+    if (numberOfLBnodes)
+        *numberOfLBnodes = L->N;
+    if (isEvenTimestep)
+        *isEvenTimestep = L->isEven ? 1 : 0;
+    if (omega)
+        *omega = L->omega;
+    return VFB_OK;
+}

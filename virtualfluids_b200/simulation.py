@@ -1,0 +1,211 @@
+"""pyfluids-style host API over the simulation C ABI.
+
+Mirrors the names of the reference's Python bindings
+(pythonbindings/src/gpu/submodules/simulation.cpp:52-79, parameter.cpp:60-143,
+boundary_conditions.cpp:42-82): a ``Parameter``, a ``BoundaryConditionFactory``
+and a ``Simulation(parameter, gridBuilder, bcFactory, gridScalingFactory)``
+whose ``run`` crosses into the library once and runs the whole time loop in
+C++ (the recursive per-level schedule of UpdateGrid27).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _lib
+from .grid import MultipleGridBuilder
+
+
+class VfbSimParams(ctypes.Structure):
+    """vfb_sim_params (include/vf_b200.h)."""
+
+    _fields_ = [
+        ("storage", ctypes.c_int),
+        ("collisionKernel", ctypes.c_int),
+        ("velocityBC", ctypes.c_int),
+        ("noSlipBC", ctypes.c_int),
+        ("geometryBC", ctypes.c_int),
+        ("slipBC", ctypes.c_int),
+        ("pressureBC", ctypes.c_int),
+        ("viscosity", ctypes.c_double),
+        ("forces", ctypes.c_double * 3),
+        ("quadricLimiters", ctypes.c_double * 3),
+        ("usePlan", ctypes.c_int),
+    ]
+
+
+class VelocityBC(enum.IntEnum):
+    VelocityInterpolatedCompressible = _lib.BC_VELOCITY_INTERPOLATED
+    VelocityBounceBack = _lib.BC_VELOCITY_BOUNCE_BACK
+
+
+class NoSlipBC(enum.IntEnum):
+    NoSlipDelayBounceBack = -1  # no kernel: bounce-back through the stopper nodes
+    NoSlipInterpolatedCompressible = _lib.BC_NOSLIP_INTERPOLATED
+    NoSlipBounceBack = _lib.BC_NOSLIP_BOUNCE_BACK
+
+
+class SlipBC(enum.IntEnum):
+    NotSpecified = -1
+    SlipCompressible = _lib.BC_SLIP
+
+
+class PressureBC(enum.IntEnum):
+    NotSpecified = -1
+    PressureNonEquilibriumCompressible = 0
+
+
+KERNELS = {"K17CompressibleNavierStokes": 0, "BGKCompSP27": 1}
+
+
+class BoundaryConditionFactory:
+    """Selection of the BC kernels (BoundaryConditionFactory.h:75-162)."""
+
+    def __init__(self):
+        self.velocity = VelocityBC.VelocityInterpolatedCompressible
+        self.no_slip = NoSlipBC.NoSlipDelayBounceBack
+        self.geometry = NoSlipBC.NoSlipDelayBounceBack
+        self.slip = SlipBC.NotSpecified
+        self.pressure = PressureBC.NotSpecified
+
+    def set_velocity_boundary_condition(self, boundary_condition_type: VelocityBC):
+        self.velocity = VelocityBC(boundary_condition_type)
+
+    def set_no_slip_boundary_condition(self, boundary_condition_type: NoSlipBC):
+        self.no_slip = NoSlipBC(boundary_condition_type)
+
+    def set_geometry_boundary_condition(self, boundary_condition_type: NoSlipBC):
+        self.geometry = NoSlipBC(boundary_condition_type)
+
+    def set_slip_boundary_condition(self, boundary_condition_type: SlipBC):
+        self.slip = SlipBC(boundary_condition_type)
+
+    def set_pressure_boundary_condition(self, boundary_condition_type: PressureBC):
+        self.pressure = PressureBC(boundary_condition_type)
+
+
+class Parameter:
+    """The subset of Parameter the time step reads (Parameter.cpp:69,395-420)."""
+
+    def __init__(self):
+        self.viscosity = 0.001
+        self.forcing = (0.0, 0.0, 0.0)
+        self.quadric_limiters = (0.01, 0.01, 0.01)
+        self.main_kernel = "K17CompressibleNavierStokes"
+        self.storage = "fp64"
+        self.use_plan = True
+        self.initial_condition = None
+
+    def set_viscosity_LB(self, viscosity: float):
+        self.viscosity = float(viscosity)
+
+    def set_forcing(self, forcing_x: float, forcing_y: float, forcing_z: float):
+        self.forcing = (float(forcing_x), float(forcing_y), float(forcing_z))
+
+    def set_quadric_limiters(self, quadric_limiter_p: float, quadric_limiter_m: float, quadric_limiter_d: float):
+        self.quadric_limiters = (float(quadric_limiter_p), float(quadric_limiter_m), float(quadric_limiter_d))
+
+    def configure_main_kernel(self, kernel: str):
+        if kernel not in KERNELS:
+            raise ValueError(f"unknown kernel {kernel!r}; known: {sorted(KERNELS)}")
+        self.main_kernel = kernel
+
+    def set_storage(self, storage: str):
+        """Population storage: "fp64", "fp32", or the 16-bit forms "fp16" / "bf16"."""
+        if storage not in _lib.STORAGE_NAMES:
+            raise ValueError(f"unknown storage {storage!r}")
+        self.storage = storage
+
+    def set_initial_condition(self, init_func):
+        """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
+        self.initial_condition = init_func
+
+
+class Simulation:
+    """Simulation(parameter, gridBuilder, bcFactory[, gridScalingFactory])."""
+
+    def __init__(self, parameter: Parameter, gridBuilder: MultipleGridBuilder, bcFactory: BoundaryConditionFactory,
+                 gridScalingFactory=None, stream=None):
+        self.parameter = parameter
+        self.stream = 0 if stream is None else int(stream)
+        L = _lib.lib()
+        p = VfbSimParams()
+        p.storage = _lib.STORAGE_NAMES[parameter.storage]
+        p.collisionKernel = KERNELS[parameter.main_kernel]
+        p.velocityBC = int(bcFactory.velocity)
+        p.noSlipBC = int(bcFactory.no_slip)
+        p.geometryBC = int(bcFactory.geometry)
+        p.slipBC = int(bcFactory.slip)
+        p.pressureBC = int(bcFactory.pressure)
+        p.viscosity = parameter.viscosity
+        p.forces[:] = parameter.forcing
+        p.quadricLimiters[:] = parameter.quadric_limiters
+        p.usePlan = int(bool(parameter.use_plan))
+        self._double = p.storage == _lib.FP64
+        spec = gridBuilder.full_spec()
+        grid = L.vfb_grid_build(spec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(spec))
+        if not grid:
+            raise _lib.VfbError(_lib.VFB_ERR_CONFIGURATION, _lib.last_error())
+        try:
+            self.levels = gridBuilder.arrays()
+            h = ctypes.c_void_p()
+            _lib.check(L.vfb_sim_create(ctypes.byref(p), grid, ctypes.byref(h), self.stream))
+            self._h = h
+        finally:
+            L.vfb_grid_free(grid)
+        if parameter.initial_condition is not None:
+            for lvl, g in enumerate(self.levels):
+                fields = parameter.initial_condition(g["coordX"], g["coordY"], g["coordZ"])
+                solid = g["geo"] != 19
+                arrays = []
+                for f in fields:
+                    a = np.array(np.broadcast_to(f, g["coordX"].shape), dtype=np.float64)
+                    a[solid] = 0.0
+                    arrays.append(a)
+                self.init_level(lvl, *arrays)
+
+    @property
+    def real(self):
+        return np.float64 if self._double else np.float32
+
+    def init_level(self, level: int, drho, vx, vy, vz):
+        a = [np.ascontiguousarray(x, dtype=self.real) for x in (drho, vx, vy, vz)]
+        _lib.check(_lib.lib().vfb_sim_init_level(self._h, level, *[x.ctypes.data for x in a], self.stream))
+
+    def run(self, steps: int = 1):
+        _lib.check(_lib.lib().vfb_sim_run(self._h, int(steps), self.stream))
+
+    def macroscopic(self, level: int = 0):
+        """(drho, vx, vy, vz) host arrays of a level."""
+        N = len(self.levels[level]["geo"])
+        out = [np.zeros(N, self.real) for _ in range(4)]
+        _lib.check(_lib.lib().vfb_sim_macroscopic(self._h, level, *[o.ctypes.data for o in out], self.stream))
+        return out
+
+    def mass_and_energy(self, level: int = 0):
+        out = (ctypes.c_double * 3)()
+        _lib.check(_lib.lib().vfb_sim_mass_and_energy(self._h, level, out, self.stream))
+        return out[0], out[1], int(out[2])
+
+    def level_state(self, level: int = 0):
+        """(device pointer of the populations, N, isEvenTimestep, omega)."""
+        ptr = ctypes.c_void_p()
+        n = ctypes.c_ulonglong()
+        ev = ctypes.c_int()
+        om = ctypes.c_double()
+        _lib.check(_lib.lib().vfb_sim_level_state(self._h, level, ctypes.byref(ptr), ctypes.byref(n), ctypes.byref(ev),
+                                                  ctypes.byref(om)))
+        return ptr.value, n.value, bool(ev.value), om.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().vfb_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
