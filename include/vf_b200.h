@@ -195,6 +195,52 @@ int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice, const int3
                           const void* rhoBC, uint32_t numberOfBCnodes, int direction, void* stream);
 
 /*
+ * Grid scaling between a level and the next finer one.  Mirrors the
+ * gridScaling function type (src/gpu/core/GridScaling/GridScalingFactory.h:46)
+ * with the interface cells of InterpolationCells / ICellNeigh
+ * (src/gpu/core/Calculation/Calculation.h:72-89): cell i is given by the base
+ * (most negative) coarse node coarseCells[i] and the base fine node
+ * fineCells[i] of its 2x2x2 source block (coarse-to-fine), or by the coarse
+ * node at its centre coarseCells[i] and the base fine node fineCells[i]
+ * (fine-to-coarse); offsetX/Y/Z (compute precision) shift the interpolation
+ * point for refinement into a wall.  isEvenTimestep is the coarse level's
+ * parity; the fine level is always read / written in the even view, as in the
+ * reference.  Replace scaleCoarseToFineCompressible<false> and
+ * scaleFineToCoarseCompressible<false> (GridScaling/Scaling.cuh:44-58;
+ * kernels scaleCoarseToFineCompressible.cu:305-528, scaleFineToCoarseCompressible.cu:76-124),
+ * called by GridScalingKernelManager::runCoarseToFineKernelLB /
+ * runFineToCoarseKernelLB (GridScalingKernelManager.cpp:64-74).
+ */
+typedef struct vfb_scaling_args {
+    void* distributionsCoarse;
+    void* distributionsFine;
+    const uint32_t* neighborXcoarse;
+    const uint32_t* neighborYcoarse;
+    const uint32_t* neighborZcoarse;
+    const uint32_t* neighborXfine;
+    const uint32_t* neighborYfine;
+    const uint32_t* neighborZfine;
+    unsigned long long numberOfLBnodesCoarse;
+    unsigned long long numberOfLBnodesFine;
+    int isEvenTimestep;
+    const uint32_t* coarseCells;
+    const uint32_t* fineCells;
+    uint32_t numberOfCells;
+    double omegaCoarse;
+    double omegaFine;
+    const void* offsetX;
+    const void* offsetY;
+    const void* offsetZ;
+} vfb_scaling_args;
+
+int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream);
+int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* stream);
+/* the same interpolation on the host (host arrays, VFB_FP32 or VFB_FP64),
+ * with the library's own arithmetic; for checks without a GPU.  No
+ * counterpart in the reference. */
+int vfb_debug_scale_host(int coarseToFine, int precision, const vfb_scaling_args* args);
+
+/*
  * Grid builder (host only).  Builds the sparse grid of a box and exports the
  * arrays the kernels consume, bit for bit those of the reference's
  * MultipleGridBuilder / LevelGridBuilder (src/gpu/GridGenerator/grid/GridBuilder/

@@ -142,6 +142,19 @@ class Reference(_Lib):
         self.fn("vfref_cpu_block_free").argtypes = [_vp]
         self.fn("vfref_cpu_block_run").restype = _c.c_double
         self.fn("vfref_cpu_block_run").argtypes = [_vp, _c.c_int, R]
+        for name in ("vfref_scale_cf", "vfref_scale_fc"):
+            self.fn(name).argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_ulonglong, _c.c_ulonglong, _c.c_int,
+                                      _vp, _vp, _c.c_uint, R, R, _vp, _vp, _vp]
+
+    def scale(self, coarse_to_fine, distC, distF, coarse, fine, is_even, cells_c, cells_f, omega_c, omega_f,
+              off_x, off_y, off_z):
+        """scaleCoarseToFineCompressible_Device<false> / scaleFineToCoarseCompressible_Device<false>
+        over all cells; coarse / fine are dicts with neighborX/Y/Z."""
+        name = "vfref_scale_cf" if coarse_to_fine else "vfref_scale_fc"
+        self.fn(name)(_ptr(distC), _ptr(distF), _ptr(coarse["neighborX"]), _ptr(coarse["neighborY"]),
+                      _ptr(coarse["neighborZ"]), _ptr(fine["neighborX"]), _ptr(fine["neighborY"]),
+                      _ptr(fine["neighborZ"]), len(coarse["geo"]), len(fine["geo"]), int(is_even), _ptr(cells_c),
+                      _ptr(cells_f), len(cells_c), omega_c, omega_f, _ptr(off_x), _ptr(off_y), _ptr(off_z))
 
     def k17_node(self, f, omega, limiter=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0)):
         f = np.ascontiguousarray(f, dtype=self.real).copy()

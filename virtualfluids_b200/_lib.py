@@ -82,6 +82,32 @@ class BcList(ctypes.Structure):
     ]
 
 
+class ScalingArgs(ctypes.Structure):
+    """vfb_scaling_args (include/vf_b200.h)."""
+
+    _fields_ = [
+        ("distributionsCoarse", ctypes.c_void_p),
+        ("distributionsFine", ctypes.c_void_p),
+        ("neighborXcoarse", ctypes.c_void_p),
+        ("neighborYcoarse", ctypes.c_void_p),
+        ("neighborZcoarse", ctypes.c_void_p),
+        ("neighborXfine", ctypes.c_void_p),
+        ("neighborYfine", ctypes.c_void_p),
+        ("neighborZfine", ctypes.c_void_p),
+        ("numberOfLBnodesCoarse", ctypes.c_ulonglong),
+        ("numberOfLBnodesFine", ctypes.c_ulonglong),
+        ("isEvenTimestep", ctypes.c_int),
+        ("coarseCells", ctypes.c_void_p),
+        ("fineCells", ctypes.c_void_p),
+        ("numberOfCells", ctypes.c_uint32),
+        ("omegaCoarse", ctypes.c_double),
+        ("omegaFine", ctypes.c_double),
+        ("offsetX", ctypes.c_void_p),
+        ("offsetY", ctypes.c_void_p),
+        ("offsetZ", ctypes.c_void_p),
+    ]
+
+
 BC_NOSLIP_INTERPOLATED, BC_NOSLIP_BOUNCE_BACK, BC_VELOCITY_INTERPOLATED, BC_VELOCITY_BOUNCE_BACK, BC_SLIP = range(5)
 
 # (name, restype, argtypes) of every exported entry point
@@ -125,6 +151,9 @@ _SIGNATURES = [
     ("vfb_sim_level_state", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong),
       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    ("vfb_scale_coarse_to_fine", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
+    ("vfb_scale_fine_to_coarse", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
+    ("vfb_debug_scale_host", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ScalingArgs)]),
     ("vfb_collision_plan_create", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),

@@ -200,6 +200,51 @@ __device__ __forceinline__ float limiterQuotient<float>(float x, float y)
 }
 #endif
 
+// Central moments (in the slots of k17Collide's naming: m_abc in the slot of
+// direction (a-1, b-1, c-1)) to populations: the backward chimera transform
+// in x, then y, then z (K17CompressibleNavierStokes.h:525-557; the same
+// sequence closes the interface interpolation, InterpolationCF.h:250-285).
+template <class R>
+__host__ __device__ __forceinline__ void centralMomentsToPopulations(R* f, R vvx, R vvy, R vvz)
+{
+    {
+        const Sweep<R> w(vvx);
+        bwd(f[dMMM], f[d0MM], f[dPMM], w, R(1));
+        bwd(f[dM0M], f[d00M], f[dP0M], w, R(0));
+        bwd(f[dMPM], f[d0PM], f[dPPM], w, R(1) / R(3));
+        bwd(f[dMM0], f[d0M0], f[dPM0], w, R(0));
+        bwd(f[dM00], f[d000], f[dP00], w, R(0));
+        bwd(f[dMP0], f[d0P0], f[dPP0], w, R(0));
+        bwd(f[dMMP], f[d0MP], f[dPMP], w, R(1) / R(3));
+        bwd(f[dM0P], f[d00P], f[dP0P], w, R(0));
+        bwd(f[dMPP], f[d0PP], f[dPPP], w, R(1) / R(9));
+    }
+    {
+        const Sweep<R> w(vvy);
+        bwd(f[dMMM], f[dM0M], f[dMPM], w, R(1) / R(6));
+        bwd(f[dMM0], f[dM00], f[dMP0], w, R(0));
+        bwd(f[dMMP], f[dM0P], f[dMPP], w, R(1) / R(18));
+        bwd(f[d0MM], f[d00M], f[d0PM], w, R(2) / R(3));
+        bwd(f[d0M0], f[d000], f[d0P0], w, R(0));
+        bwd(f[d0MP], f[d00P], f[d0PP], w, R(2) / R(9));
+        bwd(f[dPMM], f[dP0M], f[dPPM], w, R(1) / R(6));
+        bwd(f[dPM0], f[dP00], f[dPP0], w, R(0));
+        bwd(f[dPMP], f[dP0P], f[dPPP], w, R(1) / R(18));
+    }
+    {
+        const Sweep<R> w(vvz);
+        bwd(f[dMMM], f[dMM0], f[dMMP], w, R(1) / R(36));
+        bwd(f[dM0M], f[dM00], f[dM0P], w, R(1) / R(9));
+        bwd(f[dMPM], f[dMP0], f[dMPP], w, R(1) / R(36));
+        bwd(f[d0MM], f[d0M0], f[d0MP], w, R(1) / R(9));
+        bwd(f[d00M], f[d000], f[d00P], w, R(4) / R(9));
+        bwd(f[d0PM], f[d0P0], f[d0PP], w, R(1) / R(9));
+        bwd(f[dPMM], f[dPM0], f[dPMP], w, R(1) / R(36));
+        bwd(f[dP0M], f[dP00], f[dP0P], w, R(1) / R(9));
+        bwd(f[dPPM], f[dPP0], f[dPPP], w, R(1) / R(36));
+    }
+}
+
 // One K17 collision on f[27] (pre-collision in, post-collision out).
 // (fx, fy, fz) is half the acceleration already scaled by the level factor
 // (RunCollision.cuh:111-113).  Returns drho and the force-shifted velocity.
@@ -401,42 +446,7 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
     m001 = -m001;
 
     // backward chimera, x then y then z (:525-557)
-    {
-        const Sweep<R> w(vvx);
-        bwd(m000, m100, m200, w, R(1));
-        bwd(m010, m110, m210, w, R(0));
-        bwd(m020, m120, m220, w, R(1) / R(3));
-        bwd(m001, m101, m201, w, R(0));
-        bwd(m011, m111, m211, w, R(0));
-        bwd(m021, m121, m221, w, R(0));
-        bwd(m002, m102, m202, w, R(1) / R(3));
-        bwd(m012, m112, m212, w, R(0));
-        bwd(m022, m122, m222, w, R(1) / R(9));
-    }
-    {
-        const Sweep<R> w(vvy);
-        bwd(m000, m010, m020, w, R(1) / R(6));
-        bwd(m001, m011, m021, w, R(0));
-        bwd(m002, m012, m022, w, R(1) / R(18));
-        bwd(m100, m110, m120, w, R(2) / R(3));
-        bwd(m101, m111, m121, w, R(0));
-        bwd(m102, m112, m122, w, R(2) / R(9));
-        bwd(m200, m210, m220, w, R(1) / R(6));
-        bwd(m201, m211, m221, w, R(0));
-        bwd(m202, m212, m222, w, R(1) / R(18));
-    }
-    {
-        const Sweep<R> w(vvz);
-        bwd(m000, m001, m002, w, R(1) / R(36));
-        bwd(m010, m011, m012, w, R(1) / R(9));
-        bwd(m020, m021, m022, w, R(1) / R(36));
-        bwd(m100, m101, m102, w, R(1) / R(9));
-        bwd(m110, m111, m112, w, R(4) / R(9));
-        bwd(m120, m121, m122, w, R(1) / R(9));
-        bwd(m200, m201, m202, w, R(1) / R(36));
-        bwd(m210, m211, m212, w, R(1) / R(9));
-        bwd(m220, m221, m222, w, R(1) / R(36));
-    }
+    centralMomentsToPopulations(f, vvx, vvy, vvz);
 
     drho_out = drho;
     vx_out = vvx;

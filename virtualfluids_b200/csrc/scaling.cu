@@ -1,0 +1,300 @@
+// scaling.cu -- refinement-interface kernels: coarse-to-fine and
+// fine-to-coarse interpolation (scaleCoarseToFineCompressible_Device,
+// src/gpu/core/GridScaling/scaleCoarseToFineCompressible.cu:46-528;
+// scaleFineToCoarseCompressible_Device, scaleFineToCoarseCompressible.cu:43-124;
+// source moments gathered as in src/gpu/core/Utilities/ScalingUtilities.h:53-241).
+//
+// One thread per interface cell.  A cell is a 2x2x2 block of source nodes
+// given by its base (most negative) node; the 27 nodes of the 3x3x3 block
+// starting there hold the eight locations of each of the cell's nodes.  The
+// block is walked through the neighbour arrays along the same paths as the
+// reference (which matters only next to stoppers, where paths differ).
+//   coarse to fine: moments of the 8 coarse nodes (pre-collision view of the
+//     coarse parity) -> polynomial -> the 8 fine nodes at +-1/4 coarse
+//     spacing, written into the fine pre-collision view of parity "even"
+//     (the reference hard-wires the fine parity, scaleCoarseToFineCompressible.cu:59);
+//   fine to coarse: moments of the 8 fine nodes (view "even",
+//     scaleFineToCoarseCompressible.cu:105) -> polynomial -> the one coarse
+//     node at the cell centre, written into the coarse pre-collision view.
+// Cells are disjoint, so the kernels are race free.
+#include <cuda_runtime.h>
+
+#include "capi_common.cuh"
+#include "d3q27.cuh"
+#include "interpolation.cuh"
+#include "storage.cuh"
+
+namespace vfb
+{
+
+// the 3x3x3 block of sparse indices above a base node, B[x + 3 y + 9 z],
+// along the reference's neighbour paths
+__host__ __device__ __forceinline__ void blockWalk(uint32_t b, const uint32_t* nX, const uint32_t* nY,
+                                                   const uint32_t* nZ, uint32_t* B)
+{
+#define VFB_B(x, y, z) B[(x) + 3 * (y) + 9 * (z)]
+    VFB_B(0, 0, 0) = b;
+    VFB_B(1, 0, 0) = nX[VFB_B(0, 0, 0)];
+    VFB_B(0, 1, 0) = nY[VFB_B(0, 0, 0)];
+    VFB_B(0, 0, 1) = nZ[VFB_B(0, 0, 0)];
+    VFB_B(1, 1, 0) = nY[VFB_B(1, 0, 0)];
+    VFB_B(1, 0, 1) = nZ[VFB_B(1, 0, 0)];
+    VFB_B(0, 1, 1) = nZ[VFB_B(0, 1, 0)];
+    VFB_B(1, 1, 1) = nZ[VFB_B(1, 1, 0)];
+    VFB_B(0, 0, 2) = nZ[VFB_B(0, 0, 1)];
+    VFB_B(1, 0, 2) = nZ[VFB_B(1, 0, 1)];
+    VFB_B(0, 1, 2) = nZ[VFB_B(0, 1, 1)];
+    VFB_B(1, 1, 2) = nZ[VFB_B(1, 1, 1)];
+    VFB_B(2, 0, 1) = nX[VFB_B(1, 0, 1)];
+    VFB_B(2, 1, 1) = nX[VFB_B(1, 1, 1)];
+    VFB_B(2, 0, 2) = nX[VFB_B(1, 0, 2)];
+    VFB_B(2, 1, 2) = nX[VFB_B(1, 1, 2)];
+    VFB_B(2, 0, 0) = nX[VFB_B(1, 0, 0)];
+    VFB_B(2, 1, 0) = nX[VFB_B(1, 1, 0)];
+    VFB_B(0, 2, 0) = nY[VFB_B(0, 1, 0)];
+    VFB_B(1, 2, 0) = nY[VFB_B(1, 1, 0)];
+    VFB_B(0, 2, 1) = nY[VFB_B(0, 1, 1)];
+    VFB_B(1, 2, 1) = nY[VFB_B(1, 1, 1)];
+    VFB_B(0, 2, 2) = nZ[VFB_B(0, 2, 1)];
+    VFB_B(1, 2, 2) = nZ[VFB_B(1, 2, 1)];
+    VFB_B(2, 2, 1) = nX[VFB_B(1, 2, 1)];
+    VFB_B(2, 2, 2) = nX[VFB_B(1, 2, 2)];
+    VFB_B(2, 2, 0) = nX[VFB_B(1, 2, 0)];
+#undef VFB_B
+}
+
+// location l (bit 0 x, 1 y, 2 z) of the cell node at corner c (same bits)
+__host__ __device__ __forceinline__ uint32_t cornerLocation(const uint32_t* B, int c, int l)
+{
+    const int x = (c & 1) + (l & 1), y = ((c >> 1) & 1) + ((l >> 1) & 1), z = ((c >> 2) & 1) + ((l >> 2) & 1);
+    return B[x + 3 * y + 9 * z];
+}
+
+// memory access of the cell functions: device storage (any format) or host FP32 / FP64
+template <class S>
+struct DeviceAccess {
+    using R = typename Storage<S>::R;
+    __device__ __forceinline__ static R load(const S* p) { return Storage<S>::load(p); }
+    __device__ __forceinline__ static void store(S* p, R v) { Storage<S>::store(p, v); }
+};
+template <class S>
+struct HostAccess {
+    using R = S;
+    static R load(const S* p) { return *p; }
+    static void store(S* p, R v) { *p = v; }
+};
+
+template <class S, class R>
+struct ScalingView {
+    S* distC;
+    S* distF;
+    const uint32_t* nXc;
+    const uint32_t* nYc;
+    const uint32_t* nZc;
+    const uint32_t* nXf;
+    const uint32_t* nYf;
+    const uint32_t* nZf;
+    unsigned long long NC, NF;
+    const uint32_t* coarseCells;
+    const uint32_t* fineCells;
+    uint32_t nCells;
+    R omegaC, omegaF;
+    const R* offX;
+    const R* offY;
+    const R* offZ;
+};
+
+// the moments of the 8 source nodes of a cell (pre-collision view of parity EVEN)
+template <class A, bool EVEN, class S, class R>
+__host__ __device__ __forceinline__ void cellSourceMoments(const S* dist, unsigned long long N, const uint32_t* B,
+                                                           R omega, SourceMoments<R>* src)
+{
+    for (int c = 0; c < 8; ++c) {
+        R f[27];
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = A::load(dist + (unsigned long long)slot<EVEN>(d) * N + cornerLocation(B, c, loc(d)));
+        src[c] = sourceMoments(f, omega);
+    }
+}
+
+template <class A, bool EVEN_C, class S, class R>
+__host__ __device__ __forceinline__ void coarseToFineCell(const ScalingView<S, R>& v, uint32_t i)
+{
+    uint32_t B[27];
+    blockWalk(v.coarseCells[i], v.nXc, v.nYc, v.nZc, B);
+    SourceMoments<R> src[8];
+    cellSourceMoments<A, EVEN_C>(v.distC, v.NC, B, v.omegaC, src);
+    const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[i], v.offY[i], v.offZ[i]);
+    blockWalk(v.fineCells[i], v.nXf, v.nYf, v.nZf, B);
+    for (int c = 0; c < 8; ++c) {
+        const R x = (c & 1) ? R(1) / R(4) : -R(1) / R(4);
+        const R y = (c & 2) ? R(1) / R(4) : -R(1) / R(4);
+        const R z = (c & 4) ? R(1) / R(4) : -R(1) / R(4);
+        R f[27];
+        interpolateCoarseToFine(f, k, v.omegaF, x, y, z);
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            A::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + cornerLocation(B, c, loc(d)), f[d]);
+    }
+}
+
+template <class A, bool EVEN_C, class S, class R>
+__host__ __device__ __forceinline__ void fineToCoarseCell(const ScalingView<S, R>& v, uint32_t i)
+{
+    uint32_t B[27];
+    blockWalk(v.fineCells[i], v.nXf, v.nYf, v.nZf, B);
+    SourceMoments<R> src[8];
+    cellSourceMoments<A, true>(v.distF, v.NF, B, v.omegaF, src);
+    const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[i], v.offY[i], v.offZ[i]);
+    R f[27];
+    interpolateFineToCoarse(f, k, v.omegaC);
+    // the coarse node's own eight locations
+    const uint32_t kc = v.coarseCells[i];
+    uint32_t L[8];
+    L[0] = kc;
+    L[1] = v.nXc[kc];
+    L[2] = v.nYc[kc];
+    L[4] = v.nZc[kc];
+    L[3] = v.nYc[L[1]];
+    L[5] = v.nZc[L[1]];
+    L[6] = v.nZc[L[2]];
+    L[7] = v.nZc[L[3]];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        A::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d]);
+}
+
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(64) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < v.nCells)
+        coarseToFineCell<DeviceAccess<S>, EVEN_C>(v, i);
+}
+
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(64) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < v.nCells)
+        fineToCoarseCell<DeviceAccess<S>, EVEN_C>(v, i);
+}
+
+template <class S, class R>
+static ScalingView<S, R> viewOf(const vfb_scaling_args* a)
+{
+    ScalingView<S, R> v;
+    v.distC = static_cast<S*>(a->distributionsCoarse);
+    v.distF = static_cast<S*>(a->distributionsFine);
+    v.nXc = a->neighborXcoarse;
+    v.nYc = a->neighborYcoarse;
+    v.nZc = a->neighborZcoarse;
+    v.nXf = a->neighborXfine;
+    v.nYf = a->neighborYfine;
+    v.nZf = a->neighborZfine;
+    v.NC = a->numberOfLBnodesCoarse;
+    v.NF = a->numberOfLBnodesFine;
+    v.coarseCells = a->coarseCells;
+    v.fineCells = a->fineCells;
+    v.nCells = a->numberOfCells;
+    v.omegaC = (R)a->omegaCoarse;
+    v.omegaF = (R)a->omegaFine;
+    v.offX = static_cast<const R*>(a->offsetX);
+    v.offY = static_cast<const R*>(a->offsetY);
+    v.offZ = static_cast<const R*>(a->offsetZ);
+    return v;
+}
+
+template <class S>
+static int launchScaling(bool cf, const vfb_scaling_args* a, cudaStream_t s)
+{
+    using R = typename Storage<S>::R;
+    const ScalingView<S, R> v = viewOf<S, R>(a);
+    const unsigned blocks = (a->numberOfCells + 63) / 64;
+    if (cf) {
+        if (a->isEvenTimestep)
+            coarseToFineKernel<S, true><<<blocks, 64, 0, s>>>(v);
+        else
+            coarseToFineKernel<S, false><<<blocks, 64, 0, s>>>(v);
+    } else {
+        if (a->isEvenTimestep)
+            fineToCoarseKernel<S, true><<<blocks, 64, 0, s>>>(v);
+        else
+            fineToCoarseKernel<S, false><<<blocks, 64, 0, s>>>(v);
+    }
+    return checkLaunch(cf ? "coarse-to-fine interpolation" : "fine-to-coarse interpolation");
+}
+
+static int checkScalingArgs(int storage, const vfb_scaling_args* a)
+{
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (!a)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "args is NULL");
+    if (a->numberOfCells == 0)
+        return VFB_OK;
+    if (!a->distributionsCoarse || !a->distributionsFine || !a->neighborXcoarse || !a->neighborYcoarse ||
+        !a->neighborZcoarse || !a->neighborXfine || !a->neighborYfine || !a->neighborZfine || !a->coarseCells ||
+        !a->fineCells || !a->offsetX || !a->offsetY || !a->offsetZ)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL array in scaling args");
+    if (!(a->omegaCoarse > 0.0 && a->omegaCoarse < 2.0 && a->omegaFine > 0.0 && a->omegaFine < 2.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "omega outside (0, 2)");
+    return VFB_OK;
+}
+
+static int runScaling(bool cf, int storage, const vfb_scaling_args* a, void* stream)
+{
+    clearError();
+    if (const int rc = checkScalingArgs(storage, a))
+        return rc;
+    if (a->numberOfCells == 0)
+        return VFB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchScaling<float>(cf, a, s);
+    case VFB_FP64: return launchScaling<double>(cf, a, s);
+    case VFB_FP16: return launchScaling<__half>(cf, a, s);
+    default: return launchScaling<__nv_bfloat16>(cf, a, s);
+    }
+}
+
+template <class S>
+static void hostScaling(bool cf, const vfb_scaling_args* a)
+{
+    const ScalingView<S, S> v = viewOf<S, S>(a);
+    for (uint32_t i = 0; i < v.nCells; ++i) {
+        if (cf)
+            a->isEvenTimestep ? coarseToFineCell<HostAccess<S>, true>(v, i) : coarseToFineCell<HostAccess<S>, false>(v, i);
+        else
+            a->isEvenTimestep ? fineToCoarseCell<HostAccess<S>, true>(v, i) : fineToCoarseCell<HostAccess<S>, false>(v, i);
+    }
+}
+
+} // namespace vfb
+
+using namespace vfb;
+
+extern "C" int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream)
+{
+    return runScaling(true, storage, args, stream);
+}
+
+extern "C" int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* stream)
+{
+    return runScaling(false, storage, args, stream);
+}
+
+extern "C" int vfb_debug_scale_host(int coarseToFine, int precision, const vfb_scaling_args* args)
+{
+    clearError();
+    if (precision != VFB_FP32 && precision != VFB_FP64)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "precision must be VFB_FP32 or VFB_FP64");
+    if (const int rc = checkScalingArgs(precision, args))
+        return rc;
+    if (precision == VFB_FP64)
+        hostScaling<double>(coarseToFine != 0, args);
+    else
+        hostScaling<float>(coarseToFine != 0, args);
+    return VFB_OK;
+}
