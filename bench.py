@@ -267,36 +267,52 @@ def run_gpu(args, world, rank, local):
     avg_launch_ms = sum(launch_ms) / len(launch_ms)
     clk = clocks.summary()
 
+    if plan is not None:
+        plan.check(stream)
+        lane_nodes = plan_stats["lane_nodes"]
+        plan.close()
+    else:
+        lane_nodes = 0
+    del dist, plan
+    torch.cuda.empty_cache()
+
     # --- end to end through the public API with host buffers -------------------
-    # the whole job per call: pinned H2D of the initial fields, initialisation
-    # of both parities, K steps, D2H of the resulting fields; per-step bytes
-    # are the totals divided by K
-    out_host = [torch.empty(lat.N, dtype=cd).pin_memory() for _ in range(4)]
+    # Simulation (the C++ schedule behind vfb_sim_*): the timed region holds
+    # the H2D of the initial fields from host arrays, the initialisation of
+    # both parities, K time steps and the D2H of the resulting fields; the
+    # per-step bytes are the totals divided by K
+    from virtualfluids_b200.grid import MultipleGridBuilder
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, Simulation
+    b = MultipleGridBuilder()
+    d = 2.0 * math.pi / args.n
+    b.addCoarseGrid(-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d)
+    b.setPeriodicBoundaryCondition(True, True, True)
+    b.buildGrids(True)
+    p = Parameter()
+    p.set_storage(args.storage)
+    p.set_viscosity_LB(args.u0 * (args.n / (2 * math.pi)) / 1600.0)
+    sim = Simulation(p, b, BoundaryConditionFactory(), stream=stream.cuda_stream)
+    real = np.float64 if cd == torch.float64 else np.float32
+    # the user's host buffers are pinned (page-locked), as for any fast copy
+    fields_np = [h.numpy().astype(real, copy=False) for h in host_fields]
+    out_pinned = [torch.empty(lat.N, dtype=cd).pin_memory() for _ in range(4)]
+    out_np = [t.numpy() for t in out_pinned]
     barrier(world)
     torch.cuda.synchronize(device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    dev_fields = [h.to(device, non_blocking=True) for h in host_fields]
-    for ev in (False, True):
-        K.init_equilibrium(dist, lat, *dev_fields, ev, stream=stream)
-    even = True
-    for _ in range(args.steps):
-        K.collision("K17", dist, lat, omega, even, stream=stream, plan=plan)
-        even = not even
-    res = K.macroscopic(dist, lat, even, stream=stream)
-    for h, d in zip(out_host, res):
-        h.copy_(d, non_blocking=True)
+    sim.init_level(0, *fields_np)
+    sim.run(args.steps)
+    out_host = sim.macroscopic(0, out=out_np)
     e1.record(stream)
     torch.cuda.synchronize(device)
     barrier(world)
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
-    h2d = sum(h.numel() * h.element_size() for h in host_fields)
-    d2h = sum(h.numel() * h.element_size() for h in out_host)
-    finite = bool(np.isfinite(out_host[1].numpy()[g["fluid"][:1000]]).all())
-    if plan is not None:
-        plan.check(stream)
-    del dev_fields, res
+    h2d = sum(a.nbytes for a in fields_np)
+    d2h = sum(a.nbytes for a in out_host)
+    finite = bool(np.isfinite(out_host[1][g["fluid"][:1000]]).all())
+    sim.close()
 
     if rank != 0:
         return 0
@@ -330,11 +346,70 @@ def run_gpu(args, world, rank, local):
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (2 if lane_nodes else 1),
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def precision_report(args):
+    """The precision form: the Taylor-Green case run for --steps steps with
+    every storage format through the same public API; L2 velocity error and
+    kinetic-energy error of FP32 / FP16 / BF16 against the FP64 run (itself
+    checked against the FP64 oracle at small sizes by the GPU tests), and the
+    MLUPS of each.  One JSON line."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200.grid import MultipleGridBuilder
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, Simulation
+    from virtualfluids_b200.workloads import taylor_green
+
+    w = taylor_green(args.n)
+    fl = w.grid["fluid"]
+    nu = args.u0 * (args.n / (2 * math.pi)) / 1600.0
+    b = MultipleGridBuilder()
+    d = 2.0 * math.pi / args.n
+    b.addCoarseGrid(-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d)
+    b.setPeriodicBoundaryCondition(True, True, True)
+    b.buildGrids(True)
+    rows, ref = {}, None
+    for storage in ("fp64", "fp32", "fp16", "bf16"):
+        p = Parameter()
+        p.set_storage(storage)
+        p.set_viscosity_LB(nu)
+        sim = Simulation(p, b, BoundaryConditionFactory())
+        sim.init_level(0, w.rho, w.vx, w.vy, w.vz)
+        ke0 = sim.mass_and_energy(0)[1]
+        sim.run(3)
+        sim.init_level(0, w.rho, w.vx, w.vy, w.vz)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        sim.run(args.steps)
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        mass, ke, bad = sim.mass_and_energy(0)
+        _, vx, vy, vz = [a[fl].astype(np.float64) for a in sim.macroscopic(0)]
+        sim.close()
+        row = {"mlups": len(fl) * args.steps / (ms * 1e-3) / 1e6, "bytes_per_node": algorithmic_bytes_per_node(storage),
+               "kinetic_energy": ke, "kinetic_energy_initial": ke0, "nonfinite": bad}
+        if ref is None:
+            ref = (vx, vy, vz, ke, ke0)
+        else:
+            num = np.sqrt(np.sum((vx - ref[0]) ** 2 + (vy - ref[1]) ** 2 + (vz - ref[2]) ** 2))
+            den = np.sqrt(np.sum(ref[0] ** 2 + ref[1] ** 2 + ref[2] ** 2))
+            row["l2_velocity_error_vs_fp64"] = float(num / den)
+            row["kinetic_energy_error_vs_fp64"] = abs(ke - ref[3]) / ref[3]
+            row["kinetic_energy_decay_error_vs_fp64"] = abs((ref[4] - ref[3]) - (ke0 - ke)) / max(ref[4] - ref[3], 1e-300)
+        rows[storage] = row
+    rows["fp16_over_fp32_mlups"] = rows["fp16"]["mlups"] / rows["fp32"]["mlups"]
+    rows["bf16_over_fp32_mlups"] = rows["bf16"]["mlups"] / rows["fp32"]["mlups"]
+    print(json.dumps({"report": "precision form", "workload": f"taylor-green {args.n}^3 periodic, K17",
+                      "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
 
 
@@ -349,9 +424,13 @@ def main(argv=None):
     ap.add_argument("--path", default="planned", choices=["planned", "generic"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    if args.precision_report:
+        return precision_report(args)
     world, rank, local = init_distributed()
     try:
         if args.impl == "reference":

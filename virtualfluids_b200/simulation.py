@@ -15,7 +15,7 @@ import enum
 import numpy as np
 
 from . import _lib
-from .grid import MultipleGridBuilder
+from .grid import MultipleGridBuilder, export_level
 
 
 class VfbSimParams(ctypes.Structure):
@@ -149,7 +149,7 @@ class Simulation:
         if not grid:
             raise _lib.VfbError(_lib.VFB_ERR_CONFIGURATION, _lib.last_error())
         try:
-            self.levels = gridBuilder.arrays()
+            self.levels = [export_level(L, grid, lvl, "vfb_grid") for lvl in range(L.vfb_grid_levels(grid))]
             h = ctypes.c_void_p()
             _lib.check(L.vfb_sim_create(ctypes.byref(p), grid, ctypes.byref(h), self.stream))
             self._h = h
@@ -177,10 +177,15 @@ class Simulation:
     def run(self, steps: int = 1):
         _lib.check(_lib.lib().vfb_sim_run(self._h, int(steps), self.stream))
 
-    def macroscopic(self, level: int = 0):
-        """(drho, vx, vy, vz) host arrays of a level."""
+    def macroscopic(self, level: int = 0, out=None):
+        """(drho, vx, vy, vz) host arrays of a level, into `out` (four
+        contiguous arrays of the compute precision, e.g. views of pinned
+        buffers for fast copies) when given."""
         N = len(self.levels[level]["geo"])
-        out = [np.zeros(N, self.real) for _ in range(4)]
+        if out is None:
+            out = [np.zeros(N, self.real) for _ in range(4)]
+        elif len(out) != 4 or any(o.dtype != self.real or o.size != N or not o.flags.c_contiguous for o in out):
+            raise ValueError(f"out must be four contiguous {np.dtype(self.real).name} arrays of {N} elements")
         _lib.check(_lib.lib().vfb_sim_macroscopic(self._h, level, *[o.ctypes.data for o in out], self.stream))
         return out
 
