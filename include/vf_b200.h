@@ -231,6 +231,14 @@ typedef struct vfb_scaling_args {
     const void* offsetX;
     const void* offsetY;
     const void* offsetZ;
+    /* coarse to fine only: bit c of fineWriteMask[27 i + d] set = cell i
+     * writes direction d of its fine node at corner c (bit 0 x, 1 y, 2 z);
+     * NULL = every cell writes everything.  Cells of a real grid write some
+     * memory cells more than once (cells repeated across periodic seams, edge
+     * stoppers whose locations alias other nodes'); the reference kernel
+     * races there.  vfb_scaling_write_mask gives the mask under which the
+     * result is that of the cells applied one by one in list order. */
+    const uint8_t* fineWriteMask;
 } vfb_scaling_args;
 
 int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream);
@@ -239,6 +247,13 @@ int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* st
  * with the library's own arithmetic; for checks without a GPU.  No
  * counterpart in the reference. */
 int vfb_debug_scale_host(int coarseToFine, int precision, const vfb_scaling_args* args);
+/* Host arrays: for numberOfCells coarse-to-fine cells with base fine nodes
+ * fineCells, the write mask (27 bytes per cell) under which every memory cell
+ * is written only by its last writer in the order cells, then corners as the
+ * reference visits them.  No counterpart in the reference. */
+int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t numberOfCells, const uint32_t* neighborXfine,
+                           const uint32_t* neighborYfine, const uint32_t* neighborZfine,
+                           unsigned long long numberOfLBnodesFine, uint8_t* mask);
 
 /*
  * Grid builder (host only).  Builds the sparse grid of a box and exports the
@@ -264,6 +279,16 @@ int vfb_grid_elem_size(void* grid, int level, const char* name);
 /* copies the array into out (count * elem_size bytes) */
 int vfb_grid_copy(void* grid, int level, const char* name, void* out);
 void vfb_grid_free(void* grid);
+/* An empty grid container to be filled array by array by another grid
+ * provider (e.g. grids made by the reference's own builder or read from
+ * files), with the names and element types vfb_grid_build exports; levels
+ * above 0 may add the interface cells of the level and the next finer one:
+ * "cf.coarse", "cf.fine", "fc.coarse", "fc.fine" (uint32) and "cf.offX/Y/Z",
+ * "fc.offX/Y/Z" (double), the arrays of LevelGridBuilder::getGridInterfaceIndices /
+ * getOffsetCF / getOffsetFC (LevelGridBuilder.cpp:395-944).  The role of the
+ * reference's GridProvider (GridGenerator.cpp:91-1035). */
+void* vfb_grid_create(int levels);
+int vfb_grid_put(void* grid, int level, const char* name, int elemSize, long long count, const void* data);
 
 /*
  * Simulation: the host side of the time step.  Mirrors Simulation /

@@ -20,7 +20,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle.pyoracle import Reference  # noqa: E402
-from tests.golden.scenarios import GRID_SCENARIOS, grid_spec, lattice_sequence  # noqa: E402
+from tests.golden.scenarios import (GRID_SCENARIOS, REFINED_SCENARIOS, grid_spec, lattice_sequence,  # noqa: E402
+                                    refined_spec)
 
 OUT = Path(__file__).resolve().parent
 
@@ -53,6 +54,15 @@ def grids() -> None:
         np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
 
 
+def refined_grids() -> None:
+    """Two-level grids with their interface cells, from the reference builder."""
+    R = Reference("f64")
+    for name in REFINED_SCENARIOS:
+        levels = R.grid(refined_spec(name))
+        arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
+        np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
+
+
 def lattice(precision: str) -> None:
     R = Reference(precision)
     levels = R.grid(grid_spec("channel"))
@@ -65,5 +75,6 @@ if __name__ == "__main__":
         k17_nodes(p)
         lattice(p)
     grids()
+    refined_grids()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

@@ -40,6 +40,21 @@ def grid_spec(name: str) -> np.ndarray:
 
 GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel"]
 
+# two-level grids made by the reference's builder (the repository's builder
+# does not build refinement levels): a channel 24 x 16 x 16 with a refined box
+# and the reference's default layer counts, inlet velocity and outlet pressure
+REFINED_SCENARIOS = ["refined_channel"]
+
+
+def refined_spec(name: str) -> np.ndarray:
+    if name == "refined_channel":
+        sides = [(MX, VELOCITY, 0.02, 0, 0), (PX, PRESSURE, 0.0, 0, 0)]
+        s = _spec([0, 0, 0, 23, 15, 15, 1.0], (0, 1, 1), sides=sides)
+        s[10] = 1.0
+        s[11:17] = [8, 5, 5, 15, 10, 10]
+        return s
+    raise KeyError(name)
+
 
 def lattice_sequence(impl, g: dict, precision: str, steps: int = 4) -> np.ndarray:
     """Init both parities, then per step: K17 with a force, the five

@@ -1,0 +1,129 @@
+"""The recursive two-level schedule (UpdateGrid27::updateGrid with fine-to-coarse
+and coarse-to-fine interpolation) on a grid made by the reference's own
+builder, against the same schedule run on the host: the oracle for collision
+and boundary conditions, and the library's host interpolation (pinned to the
+reference's scaling kernels by tests/test_scaling_host.py)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from tests.gpu_helpers import rel_max
+from tests.scaling_cases import scaling_args
+from virtualfluids_b200 import _lib
+from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, PressureBC, Simulation
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+NU = 0.02
+
+
+def levels():
+    with np.load(GOLDEN / "grid_refined_channel.npz") as z:
+        out = {}
+        for key in z.files:
+            lvl, name = key.split(":", 1)
+            out.setdefault(int(lvl[1:]), {})[name] = z[key]
+    return [out[i] for i in sorted(out)]
+
+
+def initial(g, seed):
+    rng = np.random.default_rng(seed)
+    N = len(g["geo"])
+    f = [rng.uniform(-1e-4, 1e-4, N), 0.02 + rng.uniform(-1e-3, 1e-3, N), rng.uniform(-1e-3, 1e-3, N),
+         rng.uniform(-1e-3, 1e-3, N)]
+    for a in f:
+        a[g["geo"] != 19] = 0.0
+    return f
+
+
+class HostSchedule:
+    """UpdateGrid27::updateGrid for all levels on the host."""
+
+    def __init__(self, lv, inits):
+        self.O = Oracle("f64")
+        self.lv = lv
+        self.d = []
+        for g, init in zip(lv, inits):
+            N = len(g["geo"])
+            d = np.zeros(27 * N)
+            for ev in (0, 1):
+                self.O.init_eq(d, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], *init, ev)
+            self.d.append(d)
+        self.even = [True] * len(lv)
+        self.omega = [1.0 / (3.0 * NU * 2 ** l + 0.5) for l in range(len(lv))]
+
+    def update(self, level):
+        O, g, d = self.O, self.lv[level], self.d[level]
+        finest = len(self.lv) - 1
+        if level != finest:
+            self.update(level + 1)
+            self.update(level + 1)
+        N = len(g["geo"])
+        nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+        om, ev = self.omega[level], self.even[level]
+        O.collision_k17(d, N, *nb, g["fluid"], om, forces=(0, 0, 0), force_factor=1.0 / 2 ** level,
+                        limiters=(0.01, 0.01, 0.01), is_even=ev)
+        if len(g["velocity.k"]):
+            vel = [g[f"velocity.{c}"] for c in ("vx", "vy", "vz")]
+            O.bc_post(2, d, N, *nb, g["velocity.k"], g["velocity.q"], om, *vel, is_even=ev)
+        self.even[level] = not ev
+        if "pressure0.k" in g and len(g["pressure0.k"]):
+            O.bc_pressure(d, N, *nb, g["pressure0.k"], g["pressure0.kN"], g["pressure0.rho"],
+                          int(g["pressure0.dir"][0]), is_even=self.even[level])
+        if level != finest:
+            self.scale(level, False)
+            self.scale(level, True)
+
+    def scale(self, level, coarse_to_fine):
+        tag = "cf" if coarse_to_fine else "fc"
+        gc, gf = self.lv[level], self.lv[level + 1]
+        if len(gc[f"{tag}.coarse"]) == 0:
+            return
+        c = {"gc": gc, "gf": gf, f"coarse_{tag}": gc[f"{tag}.coarse"], f"fine_{tag}": gc[f"{tag}.fine"],
+             "omegaC": self.omega[level], "omegaF": self.omega[level + 1]}
+        offs = [np.ascontiguousarray(gc[f"{tag}.off{a}"]) for a in "XYZ"]
+        arrays = {f"{k}.neighbor{a}": c[k][f"neighbor{a}"].ctypes.data for k in ("gc", "gf") for a in "XYZ"}
+        arrays[f"coarse_{tag}"] = c[f"coarse_{tag}"].ctypes.data
+        arrays[f"fine_{tag}"] = c[f"fine_{tag}"].ctypes.data
+        arrays.update({f"off{a}": o.ctypes.data for a, o in zip("XYZ", offs)})
+        a = scaling_args(c, coarse_to_fine, self.even[level], self.d[level].ctypes.data,
+                         self.d[level + 1].ctypes.data, arrays)
+        _lib.check(_lib.lib().vfb_debug_scale_host(int(coarse_to_fine), _lib.FP64, a))
+
+    def macroscopic(self, level):
+        g = self.lv[level]
+        return self.O.macroscopic(self.d[level], len(g["geo"]), g["geo"], g["neighborX"], g["neighborY"],
+                                  g["neighborZ"], self.even[level])
+
+
+@pytest.mark.parametrize("use_plan", [True, False])
+def test_two_level_schedule_matches_host(cuda, use_plan):
+    lv = levels()
+    assert len(lv) == 2 and len(lv[0]["cf.coarse"]) > 0 and len(lv[0]["fc.coarse"]) > 0
+    inits = [initial(g, 10 + i) for i, g in enumerate(lv)]
+    p = Parameter()
+    p.set_viscosity_LB(NU)
+    p.use_plan = use_plan
+    bc = BoundaryConditionFactory()
+    bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+    sim = Simulation(p, lv, bc)
+    for lvl, init in enumerate(inits):
+        sim.init_level(lvl, *init)
+    host = HostSchedule(lv, inits)
+    steps = 4
+    sim.run(steps)
+    for _ in range(steps):
+        host.update(0)
+    for lvl, g in enumerate(lv):
+        got = sim.macroscopic(lvl)
+        ref = host.macroscopic(lvl)
+        fl = g["fluid"]
+        for a, r in zip(got, ref):
+            assert rel_max(a[fl], r[fl]) < 1e-12, lvl
+    # the fine level ran two substeps per coarse step: parity back to the start
+    assert sim.level_state(1)[2] is True
+    assert sim.level_state(0)[2] is (steps % 2 == 0)

@@ -105,6 +105,7 @@ class ScalingArgs(ctypes.Structure):
         ("offsetX", ctypes.c_void_p),
         ("offsetY", ctypes.c_void_p),
         ("offsetZ", ctypes.c_void_p),
+        ("fineWriteMask", ctypes.c_void_p),
     ]
 
 
@@ -154,6 +155,9 @@ _SIGNATURES = [
     ("vfb_scale_coarse_to_fine", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
     ("vfb_scale_fine_to_coarse", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
     ("vfb_debug_scale_host", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ScalingArgs)]),
+    ("vfb_scaling_write_mask", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong,
+      ctypes.c_void_p]),
     ("vfb_collision_plan_create", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(CollisionArgs), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_collision_plan_destroy", ctypes.c_int, [ctypes.c_void_p]),
@@ -170,6 +174,9 @@ _SIGNATURES = [
     ("vfb_grid_elem_size", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),
     ("vfb_grid_copy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]),
     ("vfb_grid_free", None, [ctypes.c_void_p]),
+    ("vfb_grid_create", ctypes.c_void_p, [ctypes.c_int]),
+    ("vfb_grid_put", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]),
 ]
 
 _lock = threading.Lock()

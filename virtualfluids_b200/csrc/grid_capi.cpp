@@ -209,4 +209,32 @@ int vfb_grid_copy(void* h, int level, const char* name, void* out)
 
 void vfb_grid_free(void* h) { delete static_cast<GridHandle*>(h); }
 
+void* vfb_grid_create(int levels)
+{
+    vfb::clearError();
+    if (levels < 1 || levels > 32) {
+        vfb::setError(VFB_ERR_INVALID_ARGUMENT, "levels %d outside [1, 32]", levels);
+        return nullptr;
+    }
+    auto* h = new GridHandle;
+    h->levels.assign((size_t)levels, Exported());
+    return h;
+}
+
+int vfb_grid_put(void* h, int level, const char* name, int elemSize, long long count, const void* data)
+{
+    vfb::clearError();
+    auto* H = static_cast<GridHandle*>(h);
+    if (!H || !name || level < 0 || level >= (int)H->levels.size())
+        return vfb::setError(VFB_ERR_INVALID_ARGUMENT, "no grid level %d", level);
+    if (!(elemSize == 1 || elemSize == 2 || elemSize == 4 || elemSize == 8) || count < 0 || (count > 0 && !data))
+        return vfb::setError(VFB_ERR_INVALID_ARGUMENT, "array %s: element size %d, count %lld", name, elemSize, count);
+    std::vector<char>& d = H->levels[level].data[name];
+    d.resize((size_t)count * (size_t)elemSize);
+    if (count > 0)
+        std::memcpy(d.data(), data, d.size());
+    H->levels[level].elem[name] = elemSize;
+    return VFB_OK;
+}
+
 } // extern "C"

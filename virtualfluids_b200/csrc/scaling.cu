@@ -16,8 +16,17 @@
 //   fine to coarse: moments of the 8 fine nodes (view "even",
 //     scaleFineToCoarseCompressible.cu:105) -> polynomial -> the one coarse
 //     node at the cell centre, written into the coarse pre-collision view.
-// Cells are disjoint, so the kernels are race free.
+// Coarse-to-fine cells of a real grid may write the same memory: cells repeat
+// across periodic seams, and cells at the edge of the fine grid write stopper
+// nodes whose locations alias those of other nodes.  The reference's kernel
+// races there; its result applied cell by cell (cells in list order, corners
+// in its visiting order) is made exact here by a write mask per cell and
+// direction (vfb_scaling_write_mask) that leaves each memory cell to its last
+// writer.  The fine-to-coarse cells of a grid write distinct coarse nodes.
 #include <cuda_runtime.h>
+
+#include <unordered_map>
+#include <vector>
 
 #include "capi_common.cuh"
 #include "d3q27.cuh"
@@ -63,6 +72,14 @@ __host__ __device__ __forceinline__ void blockWalk(uint32_t b, const uint32_t* n
 #undef VFB_B
 }
 
+// the order in which the reference's coarse-to-fine kernel visits the fine
+// corners (MMM, MMP, PMP, PMM, MPM, MPP, PPP, PPM; corner bits x | y << 1 | z << 2)
+__host__ __device__ constexpr int cfCornerOrder(int j)
+{
+    constexpr int t[8] = { 0, 4, 5, 1, 2, 6, 7, 3 };
+    return t[j];
+}
+
 // location l (bit 0 x, 1 y, 2 z) of the cell node at corner c (same bits)
 __host__ __device__ __forceinline__ uint32_t cornerLocation(const uint32_t* B, int c, int l)
 {
@@ -102,6 +119,7 @@ struct ScalingView {
     const R* offX;
     const R* offY;
     const R* offZ;
+    const uint8_t* mask; // coarse to fine: mask[27 i + d] bit c = corner c writes direction d (NULL: all)
 };
 
 // the moments of the 8 source nodes of a cell (pre-collision view of parity EVEN)
@@ -127,7 +145,9 @@ __host__ __device__ __forceinline__ void coarseToFineCell(const ScalingView<S, R
     cellSourceMoments<A, EVEN_C>(v.distC, v.NC, B, v.omegaC, src);
     const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[i], v.offY[i], v.offZ[i]);
     blockWalk(v.fineCells[i], v.nXf, v.nYf, v.nZf, B);
-    for (int c = 0; c < 8; ++c) {
+    const uint8_t* writes = v.mask ? v.mask + 27 * (size_t)i : nullptr;
+    for (int j = 0; j < 8; ++j) {
+        const int c = cfCornerOrder(j);
         const R x = (c & 1) ? R(1) / R(4) : -R(1) / R(4);
         const R y = (c & 2) ? R(1) / R(4) : -R(1) / R(4);
         const R z = (c & 4) ? R(1) / R(4) : -R(1) / R(4);
@@ -135,7 +155,8 @@ __host__ __device__ __forceinline__ void coarseToFineCell(const ScalingView<S, R
         interpolateCoarseToFine(f, k, v.omegaF, x, y, z);
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            A::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + cornerLocation(B, c, loc(d)), f[d]);
+            if (!writes || ((writes[d] >> c) & 1))
+                A::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + cornerLocation(B, c, loc(d)), f[d]);
     }
 }
 
@@ -203,6 +224,7 @@ static ScalingView<S, R> viewOf(const vfb_scaling_args* a)
     v.offX = static_cast<const R*>(a->offsetX);
     v.offY = static_cast<const R*>(a->offsetY);
     v.offZ = static_cast<const R*>(a->offsetZ);
+    v.mask = a->fineWriteMask;
     return v;
 }
 
@@ -274,6 +296,50 @@ static void hostScaling(bool cf, const vfb_scaling_args* a)
 } // namespace vfb
 
 using namespace vfb;
+
+extern "C" int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t n, const uint32_t* nXf, const uint32_t* nYf,
+                                      const uint32_t* nZf, unsigned long long NF, uint8_t* mask)
+{
+    clearError();
+    if (n == 0)
+        return VFB_OK;
+    if (!fineCells || !nXf || !nYf || !nZf || !mask || NF == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    // the last write (cell order, then the reference's corner order) to each
+    // memory cell (slot d of the even view, location index)
+    std::unordered_map<unsigned long long, uint32_t> last;
+    last.reserve((size_t)n * 216);
+    std::vector<unsigned long long> target((size_t)n * 216);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (fineCells[i] >= NF)
+            return setError(VFB_ERR_OUT_OF_RANGE, "fine cell %u: base node %u outside the level", i, fineCells[i]);
+        uint32_t B[27];
+        blockWalk(fineCells[i], nXf, nYf, nZf, B);
+        for (int b = 0; b < 27; ++b)
+            if (B[b] >= NF)
+                return setError(VFB_ERR_OUT_OF_RANGE, "fine cell %u: node %u outside the level", i, B[b]);
+        for (int j = 0; j < 8; ++j) {
+            const int c = cfCornerOrder(j);
+            for (int d = 0; d < 27; ++d) {
+                const unsigned long long cell = (unsigned long long)slot<true>(d) * NF + cornerLocation(B, c, loc(d));
+                const size_t w = (size_t)i * 216 + (size_t)c * 27 + (size_t)d;
+                target[w] = cell;
+                last[cell] = (uint32_t)w;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        for (int d = 0; d < 27; ++d) {
+            uint8_t m = 0;
+            for (int c = 0; c < 8; ++c) {
+                const size_t w = (size_t)i * 216 + (size_t)c * 27 + (size_t)d;
+                if (last[target[w]] == (uint32_t)w)
+                    m |= (uint8_t)(1u << c);
+            }
+            mask[27 * (size_t)i + d] = m;
+        }
+    return VFB_OK;
+}
 
 extern "C" int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream)
 {

@@ -46,6 +46,13 @@ struct BcListDevice {
     uint32_t n = 0;
 };
 
+// interface cells between this level and the next finer one (InterpolationCells
+// + ICellNeigh, Calculation.h:72-89)
+struct InterfaceDevice {
+    DeviceBuffer coarse, fine, offX, offY, offZ, mask;
+    uint32_t n = 0;
+};
+
 struct PressureListDevice {
     DeviceBuffer k, kN, rho;
     uint32_t n = 0;
@@ -58,6 +65,7 @@ struct Level {
     DeviceBuffer dist, nX, nY, nZ, geo, fluid;
     BcListDevice velocity, noSlip, slip, geometry;
     std::vector<PressureListDevice*> pressure;
+    InterfaceDevice coarseToFine, fineToCoarse;
     double omega = 1.0;
     double forceFactor = 1.0;
     bool isEven = true;
@@ -218,6 +226,35 @@ int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, st
             }
         }
     }
+    // interface cells to the next finer level, when the grid has them
+    auto interface = [&](const char* tag, InterfaceDevice& I) -> int {
+        const std::string t = tag;
+        if (!need((t + ".coarse").c_str(), 4))
+            return VFB_OK;
+        I.n = (uint32_t)count;
+        keep.push_back(raw);
+        e = uploadRaw(I.coarse, keep.back().data(), raw.size(), s);
+        if (e == cudaSuccess) {
+            if (!need((t + ".fine").c_str(), 4) || (uint32_t)count != I.n)
+                return fail((t + ".fine").c_str());
+            keep.push_back(raw);
+            e = uploadRaw(I.fine, keep.back().data(), raw.size(), s);
+        }
+        const char* off[3] = { ".offX", ".offY", ".offZ" };
+        DeviceBuffer* ob[3] = { &I.offX, &I.offY, &I.offZ };
+        for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+            if (!need((t + off[i]).c_str(), 8) || (uint32_t)count != I.n)
+                return fail((t + off[i]).c_str());
+            e = uploadReal(*ob[i], raw, storage, s, keep);
+        }
+        return VFB_OK;
+    };
+    if (e == cudaSuccess)
+        if (const int rc = interface("cf", L.coarseToFine))
+            return rc;
+    if (e == cudaSuccess)
+        if (const int rc = interface("fc", L.fineToCoarse))
+            return rc;
     if (e == cudaSuccess)
         e = L.dist.allocate(27ull * L.N * (size_t)elementBytes(storage));
     if (e == cudaSuccess)
@@ -332,6 +369,46 @@ int preCollisionBC(vfb_simulation& S, Level& L, void* stream)
     return VFB_OK;
 }
 
+// GridScalingKernelManager::runFineToCoarseKernelLB / runCoarseToFineKernelLB
+// (GridScalingKernelManager.cpp:64-74), in the order of Refinement_noExchange
+// (RefinementStrategy.cpp:169-178): fine to coarse, then coarse to fine
+int refinement(vfb_simulation& S, Level& C, Level& F, void* stream)
+{
+    vfb_scaling_args a;
+    std::memset(&a, 0, sizeof(a));
+    a.distributionsCoarse = C.dist.ptr;
+    a.distributionsFine = F.dist.ptr;
+    a.neighborXcoarse = static_cast<const uint32_t*>(C.nX.ptr);
+    a.neighborYcoarse = static_cast<const uint32_t*>(C.nY.ptr);
+    a.neighborZcoarse = static_cast<const uint32_t*>(C.nZ.ptr);
+    a.neighborXfine = static_cast<const uint32_t*>(F.nX.ptr);
+    a.neighborYfine = static_cast<const uint32_t*>(F.nY.ptr);
+    a.neighborZfine = static_cast<const uint32_t*>(F.nZ.ptr);
+    a.numberOfLBnodesCoarse = C.N;
+    a.numberOfLBnodesFine = F.N;
+    a.isEvenTimestep = C.isEven ? 1 : 0;
+    a.omegaCoarse = C.omega;
+    a.omegaFine = F.omega;
+    const InterfaceDevice* order[2] = { &C.fineToCoarse, &C.coarseToFine };
+    for (int i = 0; i < 2; ++i) {
+        const InterfaceDevice& I = *order[i];
+        if (I.n == 0)
+            continue;
+        a.coarseCells = static_cast<const uint32_t*>(I.coarse.ptr);
+        a.fineCells = static_cast<const uint32_t*>(I.fine.ptr);
+        a.numberOfCells = I.n;
+        a.offsetX = I.offX.ptr;
+        a.offsetY = I.offY.ptr;
+        a.offsetZ = I.offZ.ptr;
+        a.fineWriteMask = static_cast<const uint8_t*>(I.mask.ptr);
+        const int rc = i == 0 ? vfb_scale_fine_to_coarse(S.params.storage, &a, stream)
+                              : vfb_scale_coarse_to_fine(S.params.storage, &a, stream);
+        if (rc)
+            return rc;
+    }
+    return VFB_OK;
+}
+
 // UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-96)
 int updateGrid(vfb_simulation& S, int level, void* stream)
 {
@@ -351,7 +428,7 @@ int updateGrid(vfb_simulation& S, int level, void* stream)
     if (const int rc = preCollisionBC(S, L, stream))
         return rc;
     if (level != finest)
-        return setError(VFB_ERR_UNSUPPORTED, "grid refinement (fine-to-coarse / coarse-to-fine) is not built");
+        return refinement(S, L, *S.levels[level + 1], stream);
     return VFB_OK;
 }
 
@@ -397,6 +474,29 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         const double nu = P.viscosity * std::pow(2.0, l);
         L->omega = 1.0 / (3.0 * nu + 0.5);
         L->forceFactor = 1.0 / std::pow(2.0, l);
+    }
+    // coarse-to-fine cells that share fine nodes: one writer per node (the last in list order)
+    for (int l = 0; l + 1 < nLevels && rc == VFB_OK; ++l) {
+        Level& C = *S->levels[l];
+        if (C.coarseToFine.n == 0)
+            continue;
+        std::vector<char> cells, nx, ny, nz;
+        long long count = 0;
+        int es = 0;
+        if (!gridArray(grid, l, "cf.fine", cells, count, es) || !gridArray(grid, l + 1, "neighborX", nx, count, es) ||
+            !gridArray(grid, l + 1, "neighborY", ny, count, es) || !gridArray(grid, l + 1, "neighborZ", nz, count, es)) {
+            rc = setError(VFB_ERR_CONFIGURATION, "grid level %d: interface arrays", l);
+            break;
+        }
+        keep.emplace_back(27 * (size_t)C.coarseToFine.n);
+        std::vector<char>& mask = keep.back();
+        rc = vfb_scaling_write_mask(reinterpret_cast<const uint32_t*>(cells.data()), C.coarseToFine.n,
+                                    reinterpret_cast<const uint32_t*>(nx.data()),
+                                    reinterpret_cast<const uint32_t*>(ny.data()),
+                                    reinterpret_cast<const uint32_t*>(nz.data()), S->levels[l + 1]->N,
+                                    reinterpret_cast<uint8_t*>(mask.data()));
+        if (rc == VFB_OK && uploadRaw(C.coarseToFine.mask, mask.data(), mask.size(), s) != cudaSuccess)
+            rc = setError(VFB_ERR_CUDA, "interface mask upload failed");
     }
     if (rc == VFB_OK && cudaStreamSynchronize(s) != cudaSuccess)
         rc = setError(VFB_ERR_CUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -123,8 +123,30 @@ class Parameter:
         self.initial_condition = init_func
 
 
+def grid_from_arrays(levels) -> int:
+    """A vfb_grid container holding the given levels (a list of dicts of named
+    arrays, as MultipleGridBuilder.arrays() or another grid provider returns
+    them, interface cells included).  The caller frees it with vfb_grid_free."""
+    L = _lib.lib()
+    h = L.vfb_grid_create(len(levels))
+    if not h:
+        raise _lib.VfbError(_lib.VFB_ERR_INVALID_ARGUMENT, _lib.last_error())
+    try:
+        for lvl, arrays in enumerate(levels):
+            for name, a in arrays.items():
+                a = np.ascontiguousarray(a)
+                _lib.check(L.vfb_grid_put(h, lvl, name.encode(), a.itemsize, a.size, a.ctypes.data))
+    except Exception:
+        L.vfb_grid_free(h)
+        raise
+    return h
+
+
 class Simulation:
-    """Simulation(parameter, gridBuilder, bcFactory[, gridScalingFactory])."""
+    """Simulation(parameter, gridBuilder, bcFactory[, gridScalingFactory]).
+
+    gridBuilder is a MultipleGridBuilder, or the list of per-level array dicts
+    of another grid provider (e.g. a grid made by the reference's builder)."""
 
     def __init__(self, parameter: Parameter, gridBuilder: MultipleGridBuilder, bcFactory: BoundaryConditionFactory,
                  gridScalingFactory=None, stream=None):
@@ -144,8 +166,11 @@ class Simulation:
         p.quadricLimiters[:] = parameter.quadric_limiters
         p.usePlan = int(bool(parameter.use_plan))
         self._double = p.storage == _lib.FP64
-        spec = gridBuilder.full_spec()
-        grid = L.vfb_grid_build(spec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(spec))
+        if isinstance(gridBuilder, MultipleGridBuilder):
+            spec = gridBuilder.full_spec()
+            grid = L.vfb_grid_build(spec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(spec))
+        else:
+            grid = grid_from_arrays(gridBuilder)
         if not grid:
             raise _lib.VfbError(_lib.VFB_ERR_CONFIGURATION, _lib.last_error())
         try:
