@@ -27,6 +27,20 @@
 namespace vfb
 {
 
+// The scalar type behind an arithmetic type R (R itself for float / double;
+// a paired type maps to its element type), and the rational constants of the
+// operator as compile-time scalars converted to R.
+template <class R>
+struct ScalarOf {
+    using type = R;
+};
+template <class R>
+__host__ __device__ __forceinline__ R cst(int n, int m)
+{
+    using S = typename ScalarOf<R>::type;
+    return R(S(n) / S(m));
+}
+
 // Per-launch constants of the K17 collision (K17CompressibleNavierStokes.h:245-273,
 // limiter inputs :176-178, force factor RunCollision.cuh:111-113).
 template <class R>
@@ -57,11 +71,11 @@ inline K17Rates<R> makeK17Rates(R omega, R qlP, R qlM, R qlD)
     r.oneMinusOxyz = R(1) - r.Oxyz;
     r.factorA = (R(4) + R(2) * omega - R(3) * omega * omega) / (R(2) - R(7) * omega + R(5) * omega * omega);
     r.factorB = (R(4) + R(28) * omega - R(14) * omega * omega) / (R(6) - R(21) * omega + R(15) * omega * omega);
-    r.minusTau = -R(1) * (R(1) / omega - R(1) / R(2));
-    r.halfMinusOmega = R(1) / R(2) * (-omega);
-    r.omegaThreeHalves = omega * (R(3) / R(2));
+    r.minusTau = -R(1) * (R(1) / omega - cst<R>(1, 2));
+    r.halfMinusOmega = cst<R>(1, 2) * (-omega);
+    r.omegaThreeHalves = omega * (cst<R>(3, 2));
     r.minusThreeOmega = -R(3) * omega;
-    r.secondOrderCorrection = R(3) * (R(1) + R(1) / R(2) * (-omega));
+    r.secondOrderCorrection = R(3) * (R(1) + cst<R>(1, 2) * (-omega));
     r.qlP = qlP;
     r.qlM = qlM;
     r.qlD = qlD;
@@ -99,12 +113,12 @@ struct Sweep {
 };
 
 template <class R>
-__host__ __device__ __forceinline__ void fwd(R& a, R& b, R& c, const Sweep<R>& w, R K)
+__host__ __device__ __forceinline__ void fwd(R& a, R& b, R& c, const Sweep<R>& w, typename ScalarOf<R>::type K)
 {
     const R m2 = a + c;
     const R m1 = c - a;
     const R m0 = m2 + b;
-    const R m0K = K != R(0) ? m0 + K : m0;
+    const R m0K = K != 0 ? m0 + R(K) : m0;
     a = m0;
     b = fma(w.nvv, m0K, m1);
     c = fma(w.v2, m0K, fma(w.n2vv, m1, m2));
@@ -118,14 +132,14 @@ __host__ __device__ __forceinline__ void fwdThird(R& a, R& b, R& c, const Sweep<
     const R m1 = c - a;
     const R m0 = m2 + b;
     a = m0;
-    b = fma(R(1) / R(3), fma(w.nvv, m0, m1), w.nvv * (R(1) / R(9)));
-    c = fma(R(1) / R(3), fma(w.v2, m0, fma(w.n2vv, m1, m2)), w.v2 * (R(1) / R(9)));
+    b = fma(cst<R>(1, 3), fma(w.nvv, m0, m1), w.nvv * (cst<R>(1, 9)));
+    c = fma(cst<R>(1, 3), fma(w.v2, m0, fma(w.n2vv, m1, m2)), w.v2 * (cst<R>(1, 9)));
 }
 
 template <class R>
-__host__ __device__ __forceinline__ void bwd(R& a, R& b, R& c, const Sweep<R>& w, R K)
+__host__ __device__ __forceinline__ void bwd(R& a, R& b, R& c, const Sweep<R>& w, typename ScalarOf<R>::type K)
 {
-    const R aK = K != R(0) ? a + K : a;
+    const R aK = K != 0 ? a + R(K) : a;
     const R hc = R(0.5) * c;
     const R na = fma(aK, w.hm, fma(b, w.vvm, hc));
     const R nb = fma(w.nv2, aK, fma(w.n2vv, b, a - c));
@@ -180,11 +194,11 @@ __host__ __device__ __forceinline__ R c222Term(R m111, R m200, R m020, R m002, R
            (R(4) * (m101 * m101 * m020 + m011 * m011 * m200 + m110 * m110 * m002) + R(2) * (m200 * m020 * m002) +
             R(16) * m110 * m101 * m011) *
                oneOverRho * oneOverRho -
-           R(1) / R(3) * (m022 + m202 + m220) * oneOverRho - R(1) / R(9) * (m200 + m020 + m002) * oneOverRho +
+           cst<R>(1, 3) * (m022 + m202 + m220) * oneOverRho - cst<R>(1, 9) * (m200 + m020 + m002) * oneOverRho +
            (R(2) * (m101 * m101 + m011 * m011 + m110 * m110) + (m002 * m020 + m002 * m200 + m020 * m200) +
-            R(1) / R(3) * (m002 + m020 + m200)) *
-               oneOverRho * oneOverRho * (R(2) / R(3)) +
-           R(1) / R(27) * ((drho * drho - drho) * oneOverRho * oneOverRho);
+            cst<R>(1, 3) * (m002 + m020 + m200)) *
+               oneOverRho * oneOverRho * (cst<R>(2, 3)) +
+           cst<R>(1, 27) * ((drho * drho - drho) * oneOverRho * oneOverRho);
 }
 
 template <class R>
@@ -209,39 +223,39 @@ __host__ __device__ __forceinline__ void centralMomentsToPopulations(R* f, R vvx
 {
     {
         const Sweep<R> w(vvx);
-        bwd(f[dMMM], f[d0MM], f[dPMM], w, R(1));
-        bwd(f[dM0M], f[d00M], f[dP0M], w, R(0));
-        bwd(f[dMPM], f[d0PM], f[dPPM], w, R(1) / R(3));
-        bwd(f[dMM0], f[d0M0], f[dPM0], w, R(0));
-        bwd(f[dM00], f[d000], f[dP00], w, R(0));
-        bwd(f[dMP0], f[d0P0], f[dPP0], w, R(0));
-        bwd(f[dMMP], f[d0MP], f[dPMP], w, R(1) / R(3));
-        bwd(f[dM0P], f[d00P], f[dP0P], w, R(0));
-        bwd(f[dMPP], f[d0PP], f[dPPP], w, R(1) / R(9));
+        bwd(f[dMMM], f[d0MM], f[dPMM], w, typename ScalarOf<R>::type(1));
+        bwd(f[dM0M], f[d00M], f[dP0M], w, typename ScalarOf<R>::type(0));
+        bwd(f[dMPM], f[d0PM], f[dPPM], w, cst<typename ScalarOf<R>::type>(1, 3));
+        bwd(f[dMM0], f[d0M0], f[dPM0], w, typename ScalarOf<R>::type(0));
+        bwd(f[dM00], f[d000], f[dP00], w, typename ScalarOf<R>::type(0));
+        bwd(f[dMP0], f[d0P0], f[dPP0], w, typename ScalarOf<R>::type(0));
+        bwd(f[dMMP], f[d0MP], f[dPMP], w, cst<typename ScalarOf<R>::type>(1, 3));
+        bwd(f[dM0P], f[d00P], f[dP0P], w, typename ScalarOf<R>::type(0));
+        bwd(f[dMPP], f[d0PP], f[dPPP], w, cst<typename ScalarOf<R>::type>(1, 9));
     }
     {
         const Sweep<R> w(vvy);
-        bwd(f[dMMM], f[dM0M], f[dMPM], w, R(1) / R(6));
-        bwd(f[dMM0], f[dM00], f[dMP0], w, R(0));
-        bwd(f[dMMP], f[dM0P], f[dMPP], w, R(1) / R(18));
-        bwd(f[d0MM], f[d00M], f[d0PM], w, R(2) / R(3));
-        bwd(f[d0M0], f[d000], f[d0P0], w, R(0));
-        bwd(f[d0MP], f[d00P], f[d0PP], w, R(2) / R(9));
-        bwd(f[dPMM], f[dP0M], f[dPPM], w, R(1) / R(6));
-        bwd(f[dPM0], f[dP00], f[dPP0], w, R(0));
-        bwd(f[dPMP], f[dP0P], f[dPPP], w, R(1) / R(18));
+        bwd(f[dMMM], f[dM0M], f[dMPM], w, cst<typename ScalarOf<R>::type>(1, 6));
+        bwd(f[dMM0], f[dM00], f[dMP0], w, typename ScalarOf<R>::type(0));
+        bwd(f[dMMP], f[dM0P], f[dMPP], w, cst<typename ScalarOf<R>::type>(1, 18));
+        bwd(f[d0MM], f[d00M], f[d0PM], w, cst<typename ScalarOf<R>::type>(2, 3));
+        bwd(f[d0M0], f[d000], f[d0P0], w, typename ScalarOf<R>::type(0));
+        bwd(f[d0MP], f[d00P], f[d0PP], w, cst<typename ScalarOf<R>::type>(2, 9));
+        bwd(f[dPMM], f[dP0M], f[dPPM], w, cst<typename ScalarOf<R>::type>(1, 6));
+        bwd(f[dPM0], f[dP00], f[dPP0], w, typename ScalarOf<R>::type(0));
+        bwd(f[dPMP], f[dP0P], f[dPPP], w, cst<typename ScalarOf<R>::type>(1, 18));
     }
     {
         const Sweep<R> w(vvz);
-        bwd(f[dMMM], f[dMM0], f[dMMP], w, R(1) / R(36));
-        bwd(f[dM0M], f[dM00], f[dM0P], w, R(1) / R(9));
-        bwd(f[dMPM], f[dMP0], f[dMPP], w, R(1) / R(36));
-        bwd(f[d0MM], f[d0M0], f[d0MP], w, R(1) / R(9));
-        bwd(f[d00M], f[d000], f[d00P], w, R(4) / R(9));
-        bwd(f[d0PM], f[d0P0], f[d0PP], w, R(1) / R(9));
-        bwd(f[dPMM], f[dPM0], f[dPMP], w, R(1) / R(36));
-        bwd(f[dP0M], f[dP00], f[dP0P], w, R(1) / R(9));
-        bwd(f[dPPM], f[dPP0], f[dPPP], w, R(1) / R(36));
+        bwd(f[dMMM], f[dMM0], f[dMMP], w, cst<typename ScalarOf<R>::type>(1, 36));
+        bwd(f[dM0M], f[dM00], f[dM0P], w, cst<typename ScalarOf<R>::type>(1, 9));
+        bwd(f[dMPM], f[dMP0], f[dMPP], w, cst<typename ScalarOf<R>::type>(1, 36));
+        bwd(f[d0MM], f[d0M0], f[d0MP], w, cst<typename ScalarOf<R>::type>(1, 9));
+        bwd(f[d00M], f[d000], f[d00P], w, cst<typename ScalarOf<R>::type>(4, 9));
+        bwd(f[d0PM], f[d0P0], f[d0PP], w, cst<typename ScalarOf<R>::type>(1, 9));
+        bwd(f[dPMM], f[dPM0], f[dPMP], w, cst<typename ScalarOf<R>::type>(1, 36));
+        bwd(f[dP0M], f[dP00], f[dP0P], w, cst<typename ScalarOf<R>::type>(1, 9));
+        bwd(f[dPPM], f[dPP0], f[dPPP], w, cst<typename ScalarOf<R>::type>(1, 36));
     }
 }
 
@@ -287,41 +301,41 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
         f[B] = fma(w.nvv, m0K, d_##XY);                                                                                \
         f[C] = fma(w.v2, m0K, fma(w.n2vv, d_##XY, m2_##XY));                                                           \
     }
-        VFB_ZFWD(MM, dMMM, dMM0, dMMP, R(1) / R(36))
-        VFB_ZFWD(M0, dM0M, dM00, dM0P, R(1) / R(9))
-        VFB_ZFWD(MP, dMPM, dMP0, dMPP, R(1) / R(36))
-        VFB_ZFWD(0M, d0MM, d0M0, d0MP, R(1) / R(9))
-        VFB_ZFWD(00, d00M, d000, d00P, R(4) / R(9))
-        VFB_ZFWD(0P, d0PM, d0P0, d0PP, R(1) / R(9))
-        VFB_ZFWD(PM, dPMM, dPM0, dPMP, R(1) / R(36))
-        VFB_ZFWD(P0, dP0M, dP00, dP0P, R(1) / R(9))
-        VFB_ZFWD(PP, dPPM, dPP0, dPPP, R(1) / R(36))
+        VFB_ZFWD(MM, dMMM, dMM0, dMMP, cst<R>(1, 36))
+        VFB_ZFWD(M0, dM0M, dM00, dM0P, cst<R>(1, 9))
+        VFB_ZFWD(MP, dMPM, dMP0, dMPP, cst<R>(1, 36))
+        VFB_ZFWD(0M, d0MM, d0M0, d0MP, cst<R>(1, 9))
+        VFB_ZFWD(00, d00M, d000, d00P, cst<R>(4, 9))
+        VFB_ZFWD(0P, d0PM, d0P0, d0PP, cst<R>(1, 9))
+        VFB_ZFWD(PM, dPMM, dPM0, dPMP, cst<R>(1, 36))
+        VFB_ZFWD(P0, dP0M, dP00, dP0P, cst<R>(1, 9))
+        VFB_ZFWD(PP, dPPM, dPP0, dPPP, cst<R>(1, 36))
 #undef VFB_ZFWD
     }
     // y (:202-210)
     {
         const Sweep<R> w(vvy);
-        fwd(f[dMMM], f[dM0M], f[dMPM], w, R(1) / R(6));
-        fwd(f[dMM0], f[dM00], f[dMP0], w, R(0));
-        fwd(f[dMMP], f[dM0P], f[dMPP], w, R(1) / R(18));
-        fwd(f[d0MM], f[d00M], f[d0PM], w, R(2) / R(3));
-        fwd(f[d0M0], f[d000], f[d0P0], w, R(0));
-        fwd(f[d0MP], f[d00P], f[d0PP], w, R(2) / R(9));
-        fwd(f[dPMM], f[dP0M], f[dPPM], w, R(1) / R(6));
-        fwd(f[dPM0], f[dP00], f[dPP0], w, R(0));
-        fwd(f[dPMP], f[dP0P], f[dPPP], w, R(1) / R(18));
+        fwd(f[dMMM], f[dM0M], f[dMPM], w, cst<typename ScalarOf<R>::type>(1, 6));
+        fwd(f[dMM0], f[dM00], f[dMP0], w, typename ScalarOf<R>::type(0));
+        fwd(f[dMMP], f[dM0P], f[dMPP], w, cst<typename ScalarOf<R>::type>(1, 18));
+        fwd(f[d0MM], f[d00M], f[d0PM], w, cst<typename ScalarOf<R>::type>(2, 3));
+        fwd(f[d0M0], f[d000], f[d0P0], w, typename ScalarOf<R>::type(0));
+        fwd(f[d0MP], f[d00P], f[d0PP], w, cst<typename ScalarOf<R>::type>(2, 9));
+        fwd(f[dPMM], f[dP0M], f[dPPM], w, cst<typename ScalarOf<R>::type>(1, 6));
+        fwd(f[dPM0], f[dP00], f[dPP0], w, typename ScalarOf<R>::type(0));
+        fwd(f[dPMP], f[dP0P], f[dPPP], w, cst<typename ScalarOf<R>::type>(1, 18));
     }
     // x (:213-222)
     {
         const Sweep<R> w(vvx);
-        fwd(f[dMMM], f[d0MM], f[dPMM], w, R(1));
-        fwd(f[dM0M], f[d00M], f[dP0M], w, R(0));
-        fwd(f[dMPM], f[d0PM], f[dPPM], w, R(1) / R(3));
-        fwd(f[dMM0], f[d0M0], f[dPM0], w, R(0));
-        fwd(f[dM00], f[d000], f[dP00], w, R(0));
-        fwd(f[dMP0], f[d0P0], f[dPP0], w, R(0));
-        fwd(f[dMMP], f[d0MP], f[dPMP], w, R(1) / R(3));
-        fwd(f[dM0P], f[d00P], f[dP0P], w, R(0));
+        fwd(f[dMMM], f[d0MM], f[dPMM], w, typename ScalarOf<R>::type(1));
+        fwd(f[dM0M], f[d00M], f[dP0M], w, typename ScalarOf<R>::type(0));
+        fwd(f[dMPM], f[d0PM], f[dPPM], w, cst<typename ScalarOf<R>::type>(1, 3));
+        fwd(f[dMM0], f[d0M0], f[dPM0], w, typename ScalarOf<R>::type(0));
+        fwd(f[dM00], f[d000], f[dP00], w, typename ScalarOf<R>::type(0));
+        fwd(f[dMP0], f[d0P0], f[dPP0], w, typename ScalarOf<R>::type(0));
+        fwd(f[dMMP], f[d0MP], f[dPMP], w, cst<typename ScalarOf<R>::type>(1, 3));
+        fwd(f[dM0P], f[d00P], f[dP0P], w, typename ScalarOf<R>::type(0));
         fwdThird(f[dMPP], f[d0PP], f[dPPP], w);
     }
 
@@ -399,9 +413,9 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
     mxyyMxzz += w * (-mxyyMxzz);
 
     // back to single moments (:431-441)
-    m200 = R(1) / R(3) * (mxxMyy + mxxMzz + mxxPyyPzz);
-    m020 = R(1) / R(3) * (-R(2) * mxxMyy + mxxMzz + mxxPyyPzz);
-    m002 = R(1) / R(3) * (mxxMyy - R(2) * mxxMzz + mxxPyyPzz);
+    m200 = cst<R>(1, 3) * (mxxMyy + mxxMzz + mxxPyyPzz);
+    m020 = cst<R>(1, 3) * (-R(2) * mxxMyy + mxxMzz + mxxPyyPzz);
+    m002 = cst<R>(1, 3) * (mxxMyy - R(2) * mxxMzz + mxxPyyPzz);
     m210 = (mxxyMyzz + mxxyPyzz) * R(0.5);
     m012 = (-mxxyMyzz + mxxyPyzz) * R(0.5);
     m201 = (mxxzMyyz + mxxzPyyz) * R(0.5);
@@ -411,30 +425,30 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
 
     // fourth order to the modified equilibrium (:452-457); orders 5 and 6
     // relax to zero (:463-471)
-    const R cm022 = r.minusTau * (dyuy + dzuz) * (R(2) / R(3)) * r.factorA;
-    const R cm202 = r.minusTau * (dxux + dzuz) * (R(2) / R(3)) * r.factorA;
-    const R cm220 = r.minusTau * (dyuy + dxux) * (R(2) / R(3)) * r.factorA;
-    const R cm112 = r.minusTau * Dxy * (R(1) / R(3)) * r.factorB;
-    const R cm121 = r.minusTau * Dxz * (R(1) / R(3)) * r.factorB;
-    const R cm211 = r.minusTau * Dyz * (R(1) / R(3)) * r.factorB;
+    const R cm022 = r.minusTau * (dyuy + dzuz) * (cst<R>(2, 3)) * r.factorA;
+    const R cm202 = r.minusTau * (dxux + dzuz) * (cst<R>(2, 3)) * r.factorA;
+    const R cm220 = r.minusTau * (dyuy + dxux) * (cst<R>(2, 3)) * r.factorA;
+    const R cm112 = r.minusTau * Dxy * (cst<R>(1, 3)) * r.factorB;
+    const R cm121 = r.minusTau * Dxz * (cst<R>(1, 3)) * r.factorB;
+    const R cm211 = r.minusTau * Dyz * (cst<R>(1, 3)) * r.factorB;
 
     // cumulants back to central moments (:478-505)
-    m211 = cm211 + R(1) / R(3) * ((R(3) * m200 + R(1)) * m011 + R(6) * m110 * m101) * oneOverRho;
-    m121 = cm121 + R(1) / R(3) * ((R(3) * m020 + R(1)) * m101 + R(6) * m110 * m011) * oneOverRho;
-    m112 = cm112 + R(1) / R(3) * ((R(3) * m002 + R(1)) * m110 + R(6) * m101 * m011) * oneOverRho;
+    m211 = cm211 + cst<R>(1, 3) * ((R(3) * m200 + R(1)) * m011 + R(6) * m110 * m101) * oneOverRho;
+    m121 = cm121 + cst<R>(1, 3) * ((R(3) * m020 + R(1)) * m101 + R(6) * m110 * m011) * oneOverRho;
+    m112 = cm112 + cst<R>(1, 3) * ((R(3) * m002 + R(1)) * m110 + R(6) * m101 * m011) * oneOverRho;
     m220 = cm220 + (((m200 * m020 + R(2) * m110 * m110) * R(9) + R(3) * (m200 + m020)) * oneOverRho - (drho * oneOverRho)) *
-                       (R(1) / R(9));
+                       (cst<R>(1, 9));
     m202 = cm202 + (((m200 * m002 + R(2) * m101 * m101) * R(9) + R(3) * (m200 + m002)) * oneOverRho - (drho * oneOverRho)) *
-                       (R(1) / R(9));
+                       (cst<R>(1, 9));
     m022 = cm022 + (((m002 * m020 + R(2) * m011 * m011) * R(9) + R(3) * (m002 + m020)) * oneOverRho - (drho * oneOverRho)) *
-                       (R(1) / R(9));
-    m122 = R(1) / R(3) *
+                       (cst<R>(1, 9));
+    m122 = cst<R>(1, 3) *
            (R(3) * (m002 * m120 + m020 * m102 + R(4) * m011 * m111 + R(2) * (m101 * m021 + m110 * m012)) + (m120 + m102)) *
            oneOverRho;
-    m212 = R(1) / R(3) *
+    m212 = cst<R>(1, 3) *
            (R(3) * (m002 * m210 + m200 * m012 + R(4) * m101 * m111 + R(2) * (m011 * m201 + m110 * m102)) + (m210 + m012)) *
            oneOverRho;
-    m221 = R(1) / R(3) *
+    m221 = cst<R>(1, 3) *
            (R(3) * (m200 * m021 + m020 * m201 + R(4) * m110 * m111 + R(2) * (m101 * m120 + m011 * m210)) + (m021 + m201)) *
            oneOverRho;
     m222 = -c222Term(m111, m200, m020, m002, m022, m202, m220, m011, m101, m110, m211, m121, m112, m120, m102, m210,

@@ -40,6 +40,7 @@
 #include "collision_math.cuh"
 #include "d3q27.cuh"
 #include "storage.cuh"
+#include "pair32.cuh"
 #include "tma.cuh"
 
 namespace vfb
@@ -110,6 +111,9 @@ struct TiledArgs {
     long long wrapDelta[3];
     K17Rates<R> rates;
     R fx, fy, fz, gfx, gfy, gfz, forceFactor;
+    // the same rates and forces duplicated into register pairs (paired kernel)
+    K17Rates<F2> rates2;
+    F2 fx2, fy2, fz2;
     R* rho;
     R* vx;
     R* vy;
@@ -345,6 +349,98 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
     }
 }
 
+// Paired direct form (a tile configuration with 1 stage): blocks of T / 2
+// threads take one tile each; thread t collides nodes k0 + t and
+// k0 + T / 2 + t together in paired FP32 arithmetic (both loads of every
+// direction coalesced across the warp).  FP32 arithmetic only (FP32, FP16,
+// BF16 storage); the K17 collision.
+template <class S>
+__device__ __forceinline__ long long wrapLocDelta(const TiledArgs<S>& a, int wb, int l)
+{
+    const int m = l & wb;
+    return ((m & 1) ? a.wrapDelta[0] : 0ll) + ((m & 2) ? a.wrapDelta[1] : 0ll) + ((m & 4) ? a.wrapDelta[2] : 0ll);
+}
+
+template <class S, class C, bool EVEN, bool WM, bool BF>
+__global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<S> a)
+{
+    constexpr int HALF = C::T / 2;
+    constexpr int W2 = HALF / 32; // warps of a block = mask words of one half
+    constexpr int WARPS = C::T / 32;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const uint32_t* meta = a.meta + (size_t)blockIdx.x * C::META_WORDS;
+    const bool actA = (__ldg(meta + 4 + warp) >> lane) & 1u;
+    const bool actB = (__ldg(meta + 4 + W2 + warp) >> lane) & 1u;
+    if (!(actA || actB))
+        return;
+    const uint32_t k0 = __ldg(meta);
+    const uint32_t kA = k0 + tid, kB = k0 + HALF + tid;
+    const uint32_t wf = __ldg(meta + 1);
+    const bool wrap = (((wf >> warp) | (wf >> (W2 + warp))) & 1u) != 0;
+    int wbA = 0, wbB = 0;
+    if (wrap) {
+        auto bitsOf = [&](int word) {
+            return (int)((__ldg(meta + 4 + WARPS + word) >> lane) & 1u) |
+                   (int)(((__ldg(meta + 4 + 2 * WARPS + word) >> lane) & 1u) << 1) |
+                   (int)(((__ldg(meta + 4 + 3 * WARPS + word) >> lane) & 1u) << 2);
+        };
+        wbA = bitsOf(warp);
+        wbB = bitsOf(W2 + warp);
+    }
+    F2 f[27];
+    if (!wrap) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const float x = actA ? Storage<S>::load(a.gbase[d] + kA) : 0.0f;
+            const float y = actB ? Storage<S>::load(a.gbase[d] + kB) : 0.0f;
+            f[d] = F2(x, y);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const float x = actA ? Storage<S>::load(a.gbase[d] + kA + wrapLocDelta(a, wbA, loc(d))) : 0.0f;
+            const float y = actB ? Storage<S>::load(a.gbase[d] + kB + wrapLocDelta(a, wbB, loc(d))) : 0.0f;
+            f[d] = F2(x, y);
+        }
+    }
+    F2 fx = a.fx2, fy = a.fy2, fz = a.fz2;
+    if (BF) {
+        const float h = 0.5f * a.forceFactor;
+        fx = F2(actA ? (a.gfx + a.bfx[kA]) * h : 0.0f, actB ? (a.gfx + a.bfx[kB]) * h : 0.0f);
+        fy = F2(actA ? (a.gfy + a.bfy[kA]) * h : 0.0f, actB ? (a.gfy + a.bfy[kB]) * h : 0.0f);
+        fz = F2(actA ? (a.gfz + a.bfz[kA]) * h : 0.0f, actB ? (a.gfz + a.bfz[kB]) * h : 0.0f);
+        if (actA)
+            a.bfx[kA] = a.bfy[kA] = a.bfz[kA] = 0.0f;
+        if (actB)
+            a.bfx[kB] = a.bfy[kB] = a.bfz[kB] = 0.0f;
+    }
+    F2 drho, ux, uy, uz;
+    k17Collide<F2>(f, a.rates2, fx, fy, fz, drho, ux, uy, uz);
+    if (WM) {
+        if (actA) {
+            a.rho[kA] = drho.v.x;
+            a.vx[kA] = ux.v.x;
+            a.vy[kA] = uy.v.x;
+            a.vz[kA] = uz.v.x;
+        }
+        if (actB) {
+            a.rho[kB] = drho.v.y;
+            a.vx[kB] = ux.v.y;
+            a.vy[kB] = uy.v.y;
+            a.vz[kB] = uz.v.y;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const F2 v = f[inv(d)];
+        if (actA)
+            Storage<S>::store(a.gbase[d] + kA + (wrap ? wrapLocDelta(a, wbA, loc(d)) : 0ll), v.v.x);
+        if (actB)
+            Storage<S>::store(a.gbase[d] + kB + (wrap ? wrapLocDelta(a, wbB, loc(d)) : 0ll), v.v.y);
+    }
+}
+
 // ------------------------------------------------------------------ plan --
 struct vfb_collision_plan_impl {
     int storage = 0;
@@ -420,8 +516,9 @@ cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 } // namespace
 
 // Tile configurations (tile width, stages, resident blocks) the library is
-// compiled for; 0 stages selects the direct-load kernel.  Entry 0 is the
-// default for FP32, entry 9 for FP16 / BF16 and entry 1 for FP64;
+// compiled for; 0 stages selects the direct-load kernel, 1 stage the paired
+// direct-load kernel.  Entry 12 is the default for FP32, entry 9 for FP16 /
+// BF16 and entry 1 for FP64 (the fastest at Taylor-Green 512^3 on B200);
 // VFB_TILE_CONFIG=<index> selects another one at plan creation (used to tune
 // the shape on new hardware).
 struct TileConfigInfo {
@@ -433,13 +530,15 @@ static const TileConfigInfo kTileConfigs[] = {
     { 160, 3, 4, false }, { 128, 4, 3, false }, { 128, 3, 3, true },
     // direct loads (0 stages)
     { 128, 0, 4, false }, { 256, 0, 3, false }, { 128, 0, 6, false }, { 128, 0, 2, true }, { 128, 0, 3, true },
+    // paired direct loads (1 stage: T / 2 threads, two nodes each)
+    { 256, 1, 4, false }, { 256, 1, 3, false }, { 256, 1, 2, false },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
 static int chooseTileConfig(int storage)
 {
     const bool fp64 = storage == VFB_FP64;
-    int def = fp64 ? 1 : (vfb_storage_bytes(storage) == 2 ? 9 : 0);
+    int def = fp64 ? 1 : (vfb_storage_bytes(storage) == 2 ? 9 : 12);
     if (const char* env = std::getenv("VFB_TILE_CONFIG")) {
         const int c = std::atoi(env);
         if (c >= 0 && c < kNumTileConfigs && kTileConfigs[c].fp64 == fp64)
@@ -618,7 +717,10 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
-    if constexpr (C::STAGES == 0) {
+    if constexpr (C::STAGES == 1 && OP == Op::K17 && sizeof(S) <= 4) {
+        pairKernel<S, C, EVEN, WM, BF><<<a.nTiles, C::T / 2, 0, stream>>>(a);
+        return checkLaunch("paired planned collision");
+    } else if constexpr (C::STAGES <= 1) {
         directKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T, 0, stream>>>(a);
         return checkLaunch("direct planned collision");
     } else {
@@ -724,6 +826,12 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.fx = a.gfx * R(0.5) * a.forceFactor;
     a.fy = a.gfy * R(0.5) * a.forceFactor;
     a.fz = a.gfz * R(0.5) * a.forceFactor;
+    if constexpr (sizeof(R) == 4) {
+        a.rates2 = pairRates(a.rates);
+        a.fx2 = F2(a.fx);
+        a.fy2 = F2(a.fy);
+        a.fz2 = F2(a.fz);
+    }
     a.rho = static_cast<R*>(c->rho);
     a.vx = static_cast<R*>(c->vx);
     a.vy = static_cast<R*>(c->vy);
@@ -750,6 +858,9 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 4: return dispatchTuning<S, TileCfg<S, 160, 3, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 7: return dispatchTuning<S, TileCfg<S, 128, 0, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 12: return dispatchTiled<S, TileCfg<S, 256, 1, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 13: return dispatchTiled<S, TileCfg<S, 256, 1, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 14: return dispatchTiled<S, TileCfg<S, 256, 1, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 9:
             // the default for 16-bit storage (compute bound: direct loads keep more warps colliding)
