@@ -64,8 +64,9 @@ constexpr uint32_t kWaitLimit = 1u << 24; // bounded mbarrier waits
 // Tile shape: T nodes (= threads) per tile, STAGES shared-memory stages (a
 // prefetch depth of STAGES - 1 tiles), MINB resident blocks the registers are
 // sized for.
-template <class S, int T_, int STAGES_, int MINB_>
+template <class S, int T_, int STAGES_, int MINB_, int KIND_ = 0>
 struct TileCfg {
+    static constexpr int KIND = KIND_; // 1: per-warp asynchronous-copy pipeline
     static constexpr int T = T_;
     static constexpr int STAGES = STAGES_;
     static constexpr int MINB = MINB_;
@@ -441,6 +442,94 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
     }
 }
 
+// Per-thread pipelined form (KIND 1, 4- and 8-byte storage): a persistent
+// grid; every thread owns one lane of every tile its block visits and
+// prefetches the 27 values of its node of the next tile with cp.async into
+// its own shared-memory slots while it collides the current node.  A thread
+// reads only what it copied itself, so no barrier of any kind is needed; the
+// copies complete through cp.async.wait_group of the same thread.
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+__global__ void __launch_bounds__(C::T, C::MINB) asyncKernel(const TiledArgs<S> a)
+{
+    using R = typename Storage<S>::R;
+    constexpr int WARPS = C::T / 32;
+    extern __shared__ __align__(16) unsigned char smemAsync[];
+    S* buf = reinterpret_cast<S*>(smemAsync); // [2][27][T]
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const uint32_t stride = gridDim.x;
+    uint32_t tile = blockIdx.x;
+    if (tile >= a.nTiles)
+        return;
+    // head of a tile for this lane: k0, active bit, wrap bits (bit 0 x, 1 y, 2 z)
+    auto head = [&](uint32_t t, uint32_t& k0, bool& act, int& wb) {
+        const uint32_t* m = a.meta + (size_t)t * C::META_WORDS;
+        k0 = __ldg(m);
+        act = (__ldg(m + 4 + warp) >> lane) & 1u;
+        wb = 0;
+        if ((__ldg(m + 1) >> warp) & 1u)
+            wb = (int)((__ldg(m + 4 + WARPS + warp) >> lane) & 1u) |
+                 (int)(((__ldg(m + 4 + 2 * WARPS + warp) >> lane) & 1u) << 1) |
+                 (int)(((__ldg(m + 4 + 3 * WARPS + warp) >> lane) & 1u) << 2);
+    };
+    // copies of the lane's regular locations only: a wrapped location is read
+    // from global memory when the node is collided (its regular address may lie
+    // outside the array)
+    auto prefetch = [&](int stage, uint32_t k0, bool act, int wb) {
+        if (act) {
+            S* dst = buf + (size_t)stage * 27 * C::T + tid;
+            const uint32_t k = k0 + tid;
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                if (!(loc(d) & wb))
+                    tma::cpAsync<(int)sizeof(S)>(dst + d * C::T, a.gbase[d] + k);
+        }
+        tma::cpAsyncCommit();
+    };
+    uint32_t k0, nk0 = 0;
+    bool act, nact = false;
+    int wb, nwb = 0;
+    head(tile, k0, act, wb);
+    prefetch(0, k0, act, wb);
+    for (int stage = 0; tile < a.nTiles; tile += stride, stage ^= 1) {
+        const uint32_t next = tile + stride;
+        if (next < a.nTiles)
+            head(next, nk0, nact, nwb);
+        else
+            nact = false;
+        prefetch(stage ^ 1, nk0, nact, nwb); // an empty group at the end keeps the count uniform
+        tma::cpAsyncWait<1>();               // this thread's copies of the current tile are done
+        if (act) {
+            const uint32_t k = k0 + tid;
+            const S* src = buf + (size_t)stage * 27 * C::T + tid;
+            R f[27];
+            const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
+            const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
+            const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+#pragma unroll
+            for (int d = 0; d < 27; ++d) {
+                const int l = loc(d);
+                if (l & wb)
+                    f[d] = Storage<S>::load(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) +
+                                                             ((l & 4) ? dz : 0ll)));
+                else
+                    f[d] = Storage<S>::load(src + d * C::T);
+            }
+            collideNode<S, EVEN, OP, WM, BF>(a, f, k);
+#pragma unroll
+            for (int d = 0; d < 27; ++d) {
+                const int l = loc(d);
+                const long long delta = ((l & wb & 1) ? dx : 0ll) + ((l & wb & 2) ? dy : 0ll) + ((l & wb & 4) ? dz : 0ll);
+                Storage<S>::store(a.gbase[d] + k + delta, f[inv(d)]);
+            }
+        }
+        k0 = nk0;
+        act = nact;
+        wb = nwb;
+    }
+    tma::cpAsyncWait<0>();
+}
+
 // ------------------------------------------------------------------ plan --
 struct vfb_collision_plan_impl {
     int storage = 0;
@@ -532,6 +621,8 @@ static const TileConfigInfo kTileConfigs[] = {
     { 128, 0, 4, false }, { 256, 0, 3, false }, { 128, 0, 6, false }, { 128, 0, 2, true }, { 128, 0, 3, true },
     // paired direct loads (1 stage: T / 2 threads, two nodes each)
     { 256, 1, 4, false }, { 256, 1, 3, false }, { 256, 1, 2, false },
+    // per-thread cp.async pipeline (2 shared-memory stages per thread)
+    { 256, 2, 3, false }, { 128, 2, 6, false }, { 128, 2, 3, true }, { 128, 2, 2, true },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
@@ -717,7 +808,24 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
-    if constexpr (C::STAGES == 1 && OP == Op::K17 && sizeof(S) <= 4) {
+    if constexpr (C::KIND == 1) {
+        static int blocks = 0;
+        constexpr int smem = 2 * 27 * C::T * (int)sizeof(S);
+        if (blocks == 0) {
+            cudaError_t e = cudaFuncSetAttribute(asyncKernel<S, C, EVEN, OP, WM, BF>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess)
+                return setError(VFB_ERR_CUDA, "pipelined kernel shared memory attribute: %s", cudaGetErrorString(e));
+            int perSM = 0, device = 0, sms = 0;
+            cudaGetDevice(&device);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, asyncKernel<S, C, EVEN, OP, WM, BF>, C::T, smem);
+            blocks = std::max(1, perSM) * sms;
+        }
+        const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
+        asyncKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, smem, stream>>>(a);
+        return checkLaunch("pipelined planned collision");
+    } else if constexpr (C::STAGES == 1 && OP == Op::K17 && sizeof(S) <= 4) {
         pairKernel<S, C, EVEN, WM, BF><<<a.nTiles, C::T / 2, 0, stream>>>(a);
         return checkLaunch("paired planned collision");
     } else if constexpr (C::STAGES <= 1) {
@@ -849,6 +957,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 6: return dispatchTuning<S, TileCfg<S, 128, 3, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 10: return dispatchTuning<S, TileCfg<S, 128, 0, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 11: return dispatchTuning<S, TileCfg<S, 128, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 17: return dispatchTuning<S, TileCfg<S, 128, 2, 3, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 18: return dispatchTuning<S, TileCfg<S, 128, 2, 2, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     } else {
@@ -859,6 +969,16 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 5: return dispatchTuning<S, TileCfg<S, 128, 4, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 7: return dispatchTuning<S, TileCfg<S, 128, 0, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 12: return dispatchTiled<S, TileCfg<S, 256, 1, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 15:
+            if constexpr (sizeof(S) == 4)
+                return dispatchTuning<S, TileCfg<S, 256, 2, 3, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+            else
+                return setError(VFB_ERR_UNSUPPORTED, "the pipelined kernel needs 4- or 8-byte storage");
+        case 16:
+            if constexpr (sizeof(S) == 4)
+                return dispatchTuning<S, TileCfg<S, 128, 2, 6, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+            else
+                return setError(VFB_ERR_UNSUPPORTED, "the pipelined kernel needs 4- or 8-byte storage");
         case 13: return dispatchTiled<S, TileCfg<S, 256, 1, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 14: return dispatchTiled<S, TileCfg<S, 256, 1, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);

@@ -52,6 +52,22 @@ __device__ __forceinline__ uint32_t ldgOrdered(const uint32_t* p)
     return v;
 }
 
+// per-thread asynchronous copy of 4 or 8 bytes global -> shared (cp.async,
+// completed by cp.async.wait_group of the same thread)
+template <int BYTES>
+__device__ __forceinline__ void cpAsync(void* dst, const void* src)
+{
+    static_assert(BYTES == 4 || BYTES == 8, "cp.async.ca copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smemAddr(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// waits until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cpAsyncWait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // plain arrival (no transaction count)
 __device__ __forceinline__ void mbarArrive(uint64_t* bar)
 {
