@@ -31,7 +31,10 @@ def test_planned_matches_generic(cuda, dtype):
     d1, _, m1, _ = gpu_run(w, dt, 10, planned=True)
     d2, _, m2, _ = gpu_run(w, dt, 10, planned=False)
     fl = w.grid["fluid"]
-    tol = 1e-6 if dtype == "float32" else 2e-3
+    # FP32: the planned default multiplies and adds two nodes at once in paired
+    # FP32 arithmetic, which rounds some products the scalar kernel fuses, so the
+    # bound is the FP32 contract (1e-5 L2, the tolerance against the FP64 oracle)
+    tol = 1e-5 if dtype == "float32" else 2e-3
     for a, b in zip(m1, m2):
         assert rel_l2(a[fl], b[fl]) < tol
 
@@ -110,3 +113,13 @@ def test_plan_rejects_other_arrays(cuda):
     other = lat.fluid.clone()
     with pytest.raises(_lib.VfbError):
         K.collision("K17", dist, lat, w.omega, True, plan=plan, fluid=other)
+
+
+@pytest.mark.parametrize("n", [16, 13])
+def test_planned_fp32_matches_fp64_oracle(cuda, n):
+    w = tgv_state(n)
+    _, ref, _ = oracle_run(w, "f64", 12)
+    _, _, got, _ = gpu_run(w, torch.float32, 12, planned=True)
+    fl = w.grid["fluid"]
+    for a, b in zip(got, ref):
+        assert rel_l2(a[fl], b[fl]) < 1e-5
