@@ -316,6 +316,7 @@ typedef struct vfb_sim_params {
     double forces[3];          /* global acceleration */
     double quadricLimiters[3]; /* default 0.01 each (Parameter.cpp:69) */
     int usePlan;               /* 1: the planned (bulk-copy) collision kernels */
+    int useGraphs;             /* 1: replay two coarse steps at a time from a captured CUDA graph */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;
@@ -327,7 +328,12 @@ int vfb_sim_levels(const vfb_simulation* sim);
  * level) into both parity views, odd then even (PreProcessorImp.cpp:50-58) */
 int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rho, const void* vx, const void* vy, const void* vz,
                        void* stream);
-/* coarse time steps (each runs 2^l substeps of level l) */
+/* coarse time steps (each runs 2^l substeps of level l).  With useGraphs,
+ * the launches of two coarse steps (after which every level's parity is back
+ * where it started) are captured once into a CUDA graph on an internal
+ * stream, after two ordinary warm-up steps, and replayed into the given
+ * stream; an odd remainder runs ordinarily.  No counterpart in the reference,
+ * which launches every kernel from the host every substep. */
 int vfb_sim_run(vfb_simulation* sim, unsigned int steps, void* stream);
 /* macroscopic fields of a level into host arrays (compute precision); synchronises */
 int vfb_sim_macroscopic(vfb_simulation* sim, int level, void* rho, void* vx, void* vy, void* vz, void* stream);

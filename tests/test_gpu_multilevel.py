@@ -127,3 +127,23 @@ def test_two_level_schedule_matches_host(cuda, use_plan):
     # the fine level ran two substeps per coarse step: parity back to the start
     assert sim.level_state(1)[2] is True
     assert sim.level_state(0)[2] is (steps % 2 == 0)
+
+
+def test_two_level_graph_replay_equals_direct_launches(cuda):
+    lv = levels()
+    inits = [initial(g, 20 + i) for i, g in enumerate(lv)]
+    outs = []
+    for graphs in (False, True):
+        p = Parameter()
+        p.set_viscosity_LB(NU)
+        p.use_graphs = graphs
+        bc = BoundaryConditionFactory()
+        bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+        sim = Simulation(p, lv, bc)
+        for lvl, init in enumerate(inits):
+            sim.init_level(lvl, *init)
+        sim.run(9)
+        outs.append([sim.macroscopic(l) for l in range(2)])
+    for la, lb in zip(*outs):
+        for a, b in zip(la, lb):
+            assert np.array_equal(a, b)

@@ -150,3 +150,26 @@ def test_initial_condition_function_and_parity(cuda):
     assert sim.level_state(0)[2] is True
     sim.run(3)
     assert sim.level_state(0)[2] is False
+
+
+@pytest.mark.parametrize("steps", [7, 10])
+def test_graph_replay_equals_direct_launches(cuda, steps):
+    """Two coarse steps captured into a CUDA graph and replayed give the same
+    populations as launching every kernel from the host."""
+    outs = []
+    for graphs in (False, True):
+        b = channel()
+        p = Parameter()
+        p.set_viscosity_LB(0.01)
+        p.use_graphs = graphs
+        bc = BoundaryConditionFactory()
+        bc.set_slip_boundary_condition(SlipBC.SlipCompressible)
+        bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+        sim = Simulation(p, b, bc)
+        sim.init_level(0, *_init(sim.levels[0], 4))
+        sim.run(3)
+        sim.run(steps)
+        outs.append((sim.macroscopic(0), sim.level_state(0)[2]))
+    for a, b in zip(outs[0][0], outs[1][0]):
+        assert np.array_equal(a, b)
+    assert outs[0][1] == outs[1][1]

@@ -9,6 +9,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -85,8 +86,16 @@ struct Level {
 struct vfb_simulation {
     vfb_sim_params params;
     std::vector<vfb::Level*> levels;
+    // captured two-coarse-step graphs, keyed by the parity pattern they start from
+    cudaStream_t captureStream = nullptr;
+    std::map<unsigned long long, cudaGraphExec_t> graphs;
+    unsigned long long stepsRun = 0;
     ~vfb_simulation()
     {
+        for (auto& g : graphs)
+            cudaGraphExecDestroy(g.second);
+        if (captureStream)
+            cudaStreamDestroy(captureStream);
         for (auto* l : levels)
             delete l;
     }
@@ -560,12 +569,71 @@ extern "C" int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rh
     return rc;
 }
 
+namespace
+{
+unsigned long long parityPattern(const vfb_simulation& S)
+{
+    unsigned long long key = 0;
+    for (size_t l = 0; l < S.levels.size(); ++l)
+        key |= (unsigned long long)(S.levels[l]->isEven ? 1 : 0) << l;
+    return key;
+}
+
+// the graph of two coarse steps from the current parity pattern (captured on first use)
+int graphForPattern(vfb_simulation& S, cudaGraphExec_t& exec)
+{
+    const unsigned long long key = parityPattern(S);
+    auto it = S.graphs.find(key);
+    if (it != S.graphs.end()) {
+        exec = it->second;
+        return VFB_OK;
+    }
+    if (!S.captureStream && cudaStreamCreateWithFlags(&S.captureStream, cudaStreamNonBlocking) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "capture stream: %s", cudaGetErrorString(cudaGetLastError()));
+    if (cudaStreamBeginCapture(S.captureStream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "begin capture: %s", cudaGetErrorString(cudaGetLastError()));
+    int rc = VFB_OK;
+    for (int t = 0; t < 2 && rc == VFB_OK; ++t)
+        rc = updateGrid(S, 0, S.captureStream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(S.captureStream, &graph);
+    // nothing ran: the parities are back to the pattern the capture started from
+    // (two coarse steps flip every level an even number of times)
+    if (rc == VFB_OK && (e != cudaSuccess || !graph))
+        rc = setError(VFB_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    if (rc == VFB_OK && parityPattern(S) != key)
+        rc = setError(VFB_ERR_CONFIGURATION, "the parities did not return after two coarse steps");
+    if (rc == VFB_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        rc = setError(VFB_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(cudaGetLastError()));
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (rc == VFB_OK)
+        S.graphs[key] = exec;
+    return rc;
+}
+} // namespace
+
 extern "C" int vfb_sim_run(vfb_simulation* sim, unsigned int steps, void* stream)
 {
     clearError();
     if (!sim)
         return setError(VFB_ERR_INVALID_ARGUMENT, "sim is NULL");
-    for (unsigned int t = 0; t < steps; ++t)
+    unsigned int t = 0;
+    if (sim->params.useGraphs) {
+        // two ordinary steps first: every kernel path has run once before a capture
+        for (; t < steps && sim->stepsRun < 2; ++t, ++sim->stepsRun)
+            if (const int rc = updateGrid(*sim, 0, stream))
+                return rc;
+        for (; t + 2 <= steps; t += 2) {
+            cudaGraphExec_t exec = nullptr;
+            if (const int rc = graphForPattern(*sim, exec))
+                return rc;
+            if (cudaGraphLaunch(exec, static_cast<cudaStream_t>(stream)) != cudaSuccess)
+                return setError(VFB_ERR_CUDA, "graph launch: %s", cudaGetErrorString(cudaGetLastError()));
+            sim->stepsRun += 2;
+        }
+    }
+    for (; t < steps; ++t, ++sim->stepsRun)
         if (const int rc = updateGrid(*sim, 0, stream))
             return rc;
     return VFB_OK;

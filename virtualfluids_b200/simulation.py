@@ -33,6 +33,7 @@ class VfbSimParams(ctypes.Structure):
         ("forces", ctypes.c_double * 3),
         ("quadricLimiters", ctypes.c_double * 3),
         ("usePlan", ctypes.c_int),
+        ("useGraphs", ctypes.c_int),
     ]
 
 
@@ -96,6 +97,7 @@ class Parameter:
         self.main_kernel = "K17CompressibleNavierStokes"
         self.storage = "fp64"
         self.use_plan = True
+        self.use_graphs = True
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -165,6 +167,7 @@ class Simulation:
         p.forces[:] = parameter.forcing
         p.quadricLimiters[:] = parameter.quadric_limiters
         p.usePlan = int(bool(parameter.use_plan))
+        p.useGraphs = int(bool(parameter.use_graphs))
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
