@@ -413,6 +413,88 @@ def precision_report(args):
     return 0
 
 
+def cavity_report(args):
+    """The lid-driven cavity (64^3, FP64, lid u = 0.05 on +z, q = 1/2 walls,
+    nu = 0.0032, 2000 steps): the C++ schedule with and without CUDA-graph
+    replay, and parity with the FP64 oracle running the same schedule over the
+    first `check` steps.  One JSON line."""
+    import numpy as np
+    import torch
+
+    from oracle.pyoracle import Oracle
+    from virtualfluids_b200.grid import MultipleGridBuilder, SideType
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, Simulation
+
+    n, nu, steps, check = 64, 0.0032, 2000, 200
+
+    def builder():
+        b = MultipleGridBuilder()
+        b.addCoarseGrid(0, 0, 0, n - 1, n - 1, n - 1, 1.0)
+        b.buildGrids()
+        for side in (SideType.MX, SideType.PX, SideType.MY, SideType.PY, SideType.MZ):
+            b.setNoSlipBoundaryCondition(side)
+        b.setVelocityBoundaryCondition(SideType.PZ, 0.05, 0.0, 0.0)
+        return b
+
+    result = {"report": "lid-driven cavity", "workload": f"cavity {n}^3, K17, fp64, lid 0.05, nu {nu}",
+              "steps": steps}
+    for graphs in (False, True):
+        p = Parameter()
+        p.set_storage("fp64")
+        p.set_viscosity_LB(nu)
+        p.use_graphs = graphs
+        sim = Simulation(p, builder(), BoundaryConditionFactory())
+        g = sim.levels[0]
+        zero = np.zeros(len(g["geo"]))
+        sim.init_level(0, zero, zero, zero, zero)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        sim.run(steps)
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        key = "graphs" if graphs else "direct_launches"
+        result[key] = {"mlups": len(g["fluid"]) * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps}
+        if graphs:
+            _, vx, vy, vz = sim.macroscopic(0)
+            fl = g["fluid"]
+            result["max_speed_after_steps"] = float(np.sqrt(vx[fl] ** 2 + vy[fl] ** 2 + vz[fl] ** 2).max())
+        sim.close()
+    # parity over the first steps: the same schedule on the FP64 oracle
+    p = Parameter()
+    p.set_storage("fp64")
+    p.set_viscosity_LB(nu)
+    sim = Simulation(p, builder(), BoundaryConditionFactory())
+    g = sim.levels[0]
+    zero = np.zeros(len(g["geo"]))
+    sim.init_level(0, zero, zero, zero, zero)
+    sim.run(check)
+    got = sim.macroscopic(0)
+    O = Oracle("f64")
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    d = np.zeros(27 * N)
+    for ev in (0, 1):
+        O.init_eq(d, N, g["geo"], *nb, zero, zero, zero, zero, ev)
+    om = 1.0 / (3.0 * nu + 0.5)
+    vel = [g[f"velocity.{c}"] for c in ("vx", "vy", "vz")]
+    even = True
+    for _ in range(check):
+        O.collision_k17(d, N, *nb, g["fluid"], om, forces=(0, 0, 0), force_factor=1.0, limiters=(0.01, 0.01, 0.01),
+                        is_even=even)
+        O.bc_post(2, d, N, *nb, g["velocity.k"], g["velocity.q"], om, *vel, is_even=even)
+        even = not even
+    ref = O.macroscopic(d, N, g["geo"], *nb, even)
+    fl = g["fluid"]
+    result["parity_steps"] = check
+    result["max_rel_diff_vs_fp64_oracle"] = max(
+        float(np.abs(a[fl] - r[fl]).max() / max(np.abs(r[fl]).max(), 1e-300)) for a, r in zip(got, ref))
+    result["graph_speedup"] = result["graphs"]["mlups"] / result["direct_launches"]["mlups"]
+    print(json.dumps(result), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -424,6 +506,8 @@ def main(argv=None):
     ap.add_argument("--path", default="planned", choices=["planned", "generic"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cavity-report", action="store_true",
+                    help="lid-driven cavity 64^3 FP64: graph vs direct launches and oracle parity (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",
                     help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
     args = ap.parse_args(argv)
@@ -431,6 +515,8 @@ def main(argv=None):
         ap.error("--warmup must be at least 3")
     if args.precision_report:
         return precision_report(args)
+    if args.cavity_report:
+        return cavity_report(args)
     world, rank, local = init_distributed()
     try:
         if args.impl == "reference":
