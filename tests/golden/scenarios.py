@@ -43,7 +43,7 @@ GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel"]
 # two-level grids made by the reference's builder (the repository's builder
 # does not build refinement levels): a channel 24 x 16 x 16 with a refined box
 # and the reference's default layer counts, inlet velocity and outlet pressure
-REFINED_SCENARIOS = ["refined_channel"]
+REFINED_SCENARIOS = ["refined_channel", "cube_channel"]
 
 
 def refined_spec(name: str) -> np.ndarray:
@@ -52,6 +52,19 @@ def refined_spec(name: str) -> np.ndarray:
         s = _spec([0, 0, 0, 23, 15, 15, 1.0], (0, 1, 1), sides=sides)
         s[10] = 1.0
         s[11:17] = [8, 5, 5, 15, 10, 10]
+        return s
+    if name == "cube_channel":
+        # the wall-mounted cube of the two-level benchmark, scaled down: a
+        # channel 48 x 16 x 16 (periodic span), inlet velocity, outlet pressure,
+        # no-slip floor, slip top, a solid cube of side 4 on the floor inside a
+        # refined box, no-slip (interpolated) on the cube faces
+        sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 47, 15, 15, 1.0], (0, 1, 0), sides=sides)
+        s[10] = 1.0
+        s[11:17] = [12, 4, 0, 28, 12, 8]
+        s[19] = 1.0
+        s[20:26] = [16, 6, 0, 20, 10, 4]
+        s[26] = 1.0
         return s
     raise KeyError(name)
 

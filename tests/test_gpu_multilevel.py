@@ -12,7 +12,8 @@ from oracle.pyoracle import Oracle
 from tests.gpu_helpers import rel_max
 from tests.scaling_cases import scaling_args
 from virtualfluids_b200 import _lib
-from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, PressureBC, Simulation
+from virtualfluids_b200.simulation import (BoundaryConditionFactory, NoSlipBC, Parameter, PressureBC, Simulation,
+                                           SlipBC)
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -21,8 +22,8 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 NU = 0.02
 
 
-def levels():
-    with np.load(GOLDEN / "grid_refined_channel.npz") as z:
+def levels(name="refined_channel"):
+    with np.load(GOLDEN / f"grid_{name}.npz") as z:
         out = {}
         for key in z.files:
             lvl, name = key.split(":", 1)
@@ -43,7 +44,8 @@ def initial(g, seed):
 class HostSchedule:
     """UpdateGrid27::updateGrid for all levels on the host."""
 
-    def __init__(self, lv, inits):
+    def __init__(self, lv, inits, slip=False, geometry=False):
+        self.slip, self.geometry = slip, geometry
         self.O = Oracle("f64")
         self.lv = lv
         self.d = []
@@ -67,9 +69,14 @@ class HostSchedule:
         om, ev = self.omega[level], self.even[level]
         O.collision_k17(d, N, *nb, g["fluid"], om, forces=(0, 0, 0), force_factor=1.0 / 2 ** level,
                         limiters=(0.01, 0.01, 0.01), is_even=ev)
+        # post-collision BCs in the reference's order: velocity, (no-slip), slip, geometry
         if len(g["velocity.k"]):
             vel = [g[f"velocity.{c}"] for c in ("vx", "vy", "vz")]
             O.bc_post(2, d, N, *nb, g["velocity.k"], g["velocity.q"], om, *vel, is_even=ev)
+        if self.slip and len(g["slip.k"]):
+            O.bc_post(4, d, N, *nb, g["slip.k"], g["slip.q"], om, is_even=ev)
+        if self.geometry and len(g["geometry.k"]):
+            O.bc_post(0, d, N, *nb, g["geometry.k"], g["geometry.q"], om, is_even=ev)
         self.even[level] = not ev
         if "pressure0.k" in g and len(g["pressure0.k"]):
             O.bc_pressure(d, N, *nb, g["pressure0.k"], g["pressure0.kN"], g["pressure0.rho"],
@@ -147,3 +154,32 @@ def test_two_level_graph_replay_equals_direct_launches(cuda):
     for la, lb in zip(*outs):
         for a, b in zip(la, lb):
             assert np.array_equal(a, b)
+
+
+def test_cube_channel_two_levels_matches_host(cuda):
+    """The wall-mounted cube benchmark scaled down (two levels, solid cube with
+    interpolated no-slip faces on the fine level, velocity inlet, pressure
+    outlet, slip top, periodic span), grid made by the reference's builder."""
+    lv = levels("cube_channel")
+    assert len(lv) == 2 and len(lv[1]["geometry.k"]) > 0 and len(lv[0]["slip.k"]) > 0
+    inits = [initial(g, 30 + i) for i, g in enumerate(lv)]
+    p = Parameter()
+    p.set_viscosity_LB(NU)
+    bc = BoundaryConditionFactory()
+    bc.set_slip_boundary_condition(SlipBC.SlipCompressible)
+    bc.set_geometry_boundary_condition(NoSlipBC.NoSlipInterpolatedCompressible)
+    bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+    sim = Simulation(p, lv, bc)
+    for lvl, init in enumerate(inits):
+        sim.init_level(lvl, *init)
+    host = HostSchedule(lv, inits, slip=True, geometry=True)
+    steps = 4
+    sim.run(steps)
+    for _ in range(steps):
+        host.update(0)
+    for lvl, g in enumerate(lv):
+        got = sim.macroscopic(lvl)
+        ref = host.macroscopic(lvl)
+        fl = g["fluid"]
+        for a, r in zip(got, ref):
+            assert rel_max(a[fl], r[fl]) < 1e-12, lvl
