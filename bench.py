@@ -416,16 +416,15 @@ def precision_report(args):
 def cavity_report(args):
     """The lid-driven cavity (64^3, FP64, lid u = 0.05 on +z, q = 1/2 walls,
     nu = 0.0032, 2000 steps): the C++ schedule with and without CUDA-graph
-    replay, and parity with the FP64 oracle running the same schedule over the
-    first `check` steps.  One JSON line."""
+    replay (its parity with the FP64 oracle is checked by
+    tests/test_gpu_cavity.py).  One JSON line."""
     import numpy as np
     import torch
 
-    from oracle.pyoracle import Oracle
     from virtualfluids_b200.grid import MultipleGridBuilder, SideType
     from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, Simulation
 
-    n, nu, steps, check = 64, 0.0032, 2000, 200
+    n, nu, steps = 64, 0.0032, 2000
 
     def builder():
         b = MultipleGridBuilder()
@@ -461,37 +460,160 @@ def cavity_report(args):
             fl = g["fluid"]
             result["max_speed_after_steps"] = float(np.sqrt(vx[fl] ** 2 + vy[fl] ** 2 + vz[fl] ** 2).max())
         sim.close()
-    # parity over the first steps: the same schedule on the FP64 oracle
-    p = Parameter()
-    p.set_storage("fp64")
-    p.set_viscosity_LB(nu)
-    sim = Simulation(p, builder(), BoundaryConditionFactory())
-    g = sim.levels[0]
-    zero = np.zeros(len(g["geo"]))
-    sim.init_level(0, zero, zero, zero, zero)
-    sim.run(check)
-    got = sim.macroscopic(0)
-    O = Oracle("f64")
-    N = len(g["geo"])
-    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
-    d = np.zeros(27 * N)
-    for ev in (0, 1):
-        O.init_eq(d, N, g["geo"], *nb, zero, zero, zero, zero, ev)
-    om = 1.0 / (3.0 * nu + 0.5)
-    vel = [g[f"velocity.{c}"] for c in ("vx", "vy", "vz")]
-    even = True
-    for _ in range(check):
-        O.collision_k17(d, N, *nb, g["fluid"], om, forces=(0, 0, 0), force_factor=1.0, limiters=(0.01, 0.01, 0.01),
-                        is_even=even)
-        O.bc_post(2, d, N, *nb, g["velocity.k"], g["velocity.q"], om, *vel, is_even=even)
-        even = not even
-    ref = O.macroscopic(d, N, g["geo"], *nb, even)
-    fl = g["fluid"]
-    result["parity_steps"] = check
-    result["max_rel_diff_vs_fp64_oracle"] = max(
-        float(np.abs(a[fl] - r[fl]).max() / max(np.abs(r[fl]).max(), 1e-300)) for a, r in zip(got, ref))
     result["graph_speedup"] = result["graphs"]["mlups"] / result["direct_launches"]["mlups"]
     print(json.dumps(result), flush=True)
+    return 0
+
+
+def kernel_report(args):
+    """Achieved bandwidth of the other kernels of the step, event-timed, with
+    their algorithmic bytes per unit (s = bytes per stored population):
+      BGK (planned, TGV n^3):            27 s read + 27 s write + 16 B per node
+      velocity BC (interpolated):        27 s read + 27 q (4 B) + 4 B k + 12 B u + active q writes per BC node
+      pressure BC (non-equilibrium):     27 s read at the neighbour + 18 s write + 8 B k/kN + 4 B rho per BC node
+      coarse to fine / fine to coarse:   8 * 27 s read + 8 * 27 s (CF) or 27 s (FC) write + 20 B per cell
+    One JSON line."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200 import _lib
+    from virtualfluids_b200 import kernels as K
+    from virtualfluids_b200.grid import MultipleGridBuilder, SideType
+    from virtualfluids_b200.workloads import taylor_green
+
+    peak, peak_kind = hbm_peak()
+    out = {"report": "kernels", "peak_gbs": peak, "peak_kind": peak_kind, "storage": "fp32", "kernels": {}}
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def record(name, units, bytes_per_unit, ms, unit_name):
+        gbs = units * bytes_per_unit / (ms * 1e-3) / 1e9
+        out["kernels"][name] = {unit_name: int(units), "bytes_per_unit": bytes_per_unit, "ms": ms, "gbs": gbs,
+                                "frac_of_peak": gbs / peak}
+
+    # BGK, planned, TGV
+    w = taylor_green(args.n)
+    lat = K.DeviceLattice.from_arrays(w.grid)
+    dist = K.new_distributions(lat, torch.float32)
+    fields = [torch.from_numpy(a).to("cuda", torch.float32) for a in (w.rho, w.vx, w.vy, w.vz)]
+    for ev in (False, True):
+        K.init_equilibrium(dist, lat, *fields, ev)
+    del fields
+    plan = K.CollisionPlan(torch.float32, lat)
+    state = {"even": True}
+
+    def bgk():
+        K.collision("BGK", dist, lat, w.omega, state["even"], plan=plan)
+        state["even"] = not state["even"]
+    record("bgk_planned_tgv", lat.numberOfFluidNodes, 54 * 4 + 16, timed(bgk), "nodes")
+    plan.close()
+    del dist, plan, lat, w
+    torch.cuda.empty_cache()
+
+    # BC kernels on a cavity (velocity list on all six walls) and a channel (pressure outlet)
+    def grid_of(builder):
+        return builder.arrays()[0]
+    nb = 256
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, nb - 1, nb - 1, nb - 1, 1.0)
+    b.buildGrids()
+    for side in (SideType.MX, SideType.PX, SideType.MY, SideType.PY, SideType.MZ):
+        b.setNoSlipBoundaryCondition(side)
+    b.setVelocityBoundaryCondition(SideType.PZ, 0.05, 0.0, 0.0)
+    g = grid_of(b)
+    lat = K.DeviceLattice.from_arrays(g)
+    dist = K.new_distributions(lat, torch.float32)
+    dist.uniform_(-1e-3, 1e-3)
+    k = torch.from_numpy(g["velocity.k"]).cuda()
+    q = torch.from_numpy(g["velocity.q"].astype(np.float32)).cuda()
+    v = [torch.from_numpy(g[f"velocity.{c}"].astype(np.float32)).cuda() for c in ("vx", "vy", "vz")]
+    active = int((g["velocity.q"].reshape(27, -1) >= 0).sum())
+    n_bc = len(g["velocity.k"])
+    ms = timed(lambda: K.bc_post(_lib.BC_VELOCITY_INTERPOLATED, dist, lat, k, q, 1.9, True, *v))
+    record(f"velocity_bc_cavity{nb}", n_bc, (27 * 4 + 27 * 4 + 4 + 12) + active * 4 / n_bc, ms, "bc_nodes")
+    del dist, lat
+    torch.cuda.empty_cache()
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, 255, 127, 127, 1.0)
+    b.setPeriodicBoundaryCondition(False, True, True)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(SideType.MX, 0.04, 0.0, 0.0)
+    b.setPressureBoundaryCondition(SideType.PX, 0.0)
+    g = grid_of(b)
+    lat = K.DeviceLattice.from_arrays(g)
+    dist = K.new_distributions(lat, torch.float32)
+    dist.uniform_(-1e-3, 1e-3)
+    pk, pkn = (torch.from_numpy(g[f"pressure0.{x}"]).cuda() for x in ("k", "kN"))
+    prho = torch.from_numpy(g["pressure0.rho"].astype(np.float32)).cuda()
+    ms = timed(lambda: K.bc_pressure(dist, lat, pk, pkn, prho, int(g["pressure0.dir"][0]), True))
+    record("pressure_bc_channel256x128x128", len(g["pressure0.k"]), 27 * 4 + 18 * 4 + 12, ms, "bc_nodes")
+    del dist, lat
+    torch.cuda.empty_cache()
+
+    # interface interpolation: two periodic boxes (coarse 128^3, fine 256^3) with
+    # structured interfaces: coarse-to-fine cells on two coarse z planes, each
+    # writing the fine 2x2x2 block at twice its coordinates; fine-to-coarse
+    # cells on a third plane reading the fine block below
+    from virtualfluids_b200.grid import taylor_green_grid
+    ncg, nfg = 128, 256
+    gc, gf = taylor_green_grid(ncg), taylor_green_grid(nfg)
+    flc, flf = gc["fluid"], gf["fluid"]
+
+    def coarse_at(i, j, kk):
+        return flc[i + ncg * (j + ncg * kk)]
+
+    def fine_at(i, j, kk):
+        return flf[i + nfg * (j + nfg * kk)]
+    ii, jj = np.meshgrid(np.arange(ncg), np.arange(ncg), indexing="ij")
+    ii, jj = ii.ravel(), jj.ravel()
+    cells = {}
+    for tag, planes in (("cf", (40, 41)), ("fc", (80,))):
+        cc, ff = [], []
+        for kk in planes:
+            cc.append(coarse_at(ii, jj, kk))
+            ff.append(fine_at(2 * ii, 2 * jj, 2 * kk))
+        cells[tag] = (np.concatenate(cc).astype(np.uint32), np.concatenate(ff).astype(np.uint32))
+    latc, latf = K.DeviceLattice.from_arrays(gc), K.DeviceLattice.from_arrays(gf)
+    dc, df = K.new_distributions(latc, torch.float32), K.new_distributions(latf, torch.float32)
+    dc.uniform_(-1e-3, 1e-3)
+    df.uniform_(-1e-3, 1e-3)
+    keep = []
+
+    def dev(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        keep.append(t)
+        return t.data_ptr()
+    for tag, fn, write in (("cf", _lib.lib().vfb_scale_coarse_to_fine, 8 * 27 * 4),
+                           ("fc", _lib.lib().vfb_scale_fine_to_coarse, 27 * 4)):
+        coarse, fine = cells[tag]
+        n = len(coarse)
+        zeros = np.zeros(n, np.float32)
+        a = _lib.ScalingArgs()
+        a.distributionsCoarse, a.distributionsFine = dc.data_ptr(), df.data_ptr()
+        a.neighborXcoarse, a.neighborYcoarse, a.neighborZcoarse = (latc.neighborX.data_ptr(), latc.neighborY.data_ptr(),
+                                                                   latc.neighborZ.data_ptr())
+        a.neighborXfine, a.neighborYfine, a.neighborZfine = (latf.neighborX.data_ptr(), latf.neighborY.data_ptr(),
+                                                             latf.neighborZ.data_ptr())
+        a.numberOfLBnodesCoarse, a.numberOfLBnodesFine = latc.N, latf.N
+        a.isEvenTimestep = 1
+        a.coarseCells, a.fineCells = dev(coarse.view(np.int32)), dev(fine.view(np.int32))
+        a.numberOfCells = n
+        a.omegaCoarse, a.omegaFine = 1.9, 1.85
+        a.offsetX = a.offsetY = a.offsetZ = dev(zeros)
+        ms = timed(lambda: _lib.check(fn(_lib.FP32, a, None)))
+        record("coarse_to_fine_cells" if tag == "cf" else "fine_to_coarse_cells", n, 8 * 27 * 4 + write + 20, ms,
+               "cells")
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -506,8 +628,10 @@ def main(argv=None):
     ap.add_argument("--path", default="planned", choices=["planned", "generic"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-report", action="store_true",
+                    help="bandwidth of the BGK, BC and interface kernels (not a bench line)")
     ap.add_argument("--cavity-report", action="store_true",
-                    help="lid-driven cavity 64^3 FP64: graph vs direct launches and oracle parity (not a bench line)")
+                    help="lid-driven cavity 64^3 FP64: graph replay vs direct launches (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",
                     help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
     args = ap.parse_args(argv)
@@ -517,6 +641,8 @@ def main(argv=None):
         return precision_report(args)
     if args.cavity_report:
         return cavity_report(args)
+    if args.kernel_report:
+        return kernel_report(args)
     world, rank, local = init_distributed()
     try:
         if args.impl == "reference":

@@ -123,3 +123,15 @@ def test_planned_fp32_matches_fp64_oracle(cuda, n):
     fl = w.grid["fluid"]
     for a, b in zip(got, ref):
         assert rel_l2(a[fl], b[fl]) < 1e-5
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float16"])
+def test_planned_bgk_matches_generic(cuda, dtype):
+    w = tgv_state(20)
+    dt = getattr(torch, dtype)
+    _, _, m1, _ = gpu_run(w, dt, 8, "BGK", planned=True)
+    _, _, m2, _ = gpu_run(w, dt, 8, "BGK", planned=False)
+    fl = w.grid["fluid"]
+    tol = 1e-6 if dtype == "float32" else 2e-3
+    for a, b in zip(m1, m2):
+        assert rel_l2(a[fl], b[fl]) < tol

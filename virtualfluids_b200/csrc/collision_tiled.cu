@@ -828,7 +828,11 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
     } else if constexpr (C::STAGES == 1 && OP == Op::K17 && sizeof(S) <= 4) {
         pairKernel<S, C, EVEN, WM, BF><<<a.nTiles, C::T / 2, 0, stream>>>(a);
         return checkLaunch("paired planned collision");
-    } else if constexpr (C::STAGES <= 1) {
+    } else if constexpr (C::STAGES == 1) {
+        // the paired form is K17 only: other operators use the staged kernel of
+        // the same tile width (same metadata layout and copy geometry)
+        return launchTiledT<S, TileCfg<S, C::T, 2, 3>, EVEN, OP, WM, BF>(a, stream);
+    } else if constexpr (C::STAGES == 0) {
         directKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T, 0, stream>>>(a);
         return checkLaunch("direct planned collision");
     } else {
