@@ -101,7 +101,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def init_distributed():
+def init_distributed(backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL
+    carries only the barriers and the max-over-ranks timing (the replicas
+    exchange no data).  The short timeout makes a rank that never arrives end
+    the others with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -110,8 +114,9 @@ def init_distributed():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -126,9 +131,16 @@ def max_over_ranks(world, value: float) -> float:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, world: int, slowest_ms: float) -> float:
+    """Updates per second of all replicas together, over the slowest rank's time
+    (weak scaling: every rank processes the same number of units)."""
+    return units_per_rank * world / (slowest_ms * 1e-3)
 
 
 # --------------------------------------------------------------------------- #
@@ -316,9 +328,8 @@ def run_gpu(args, world, rank, local):
 
     if rank != 0:
         return 0
-    updates = n_fluid * args.steps * world
-    value = updates / (total_ms * 1e-3) / 1e6
-    e2e_value = updates / (e2e_ms * 1e-3) / 1e6
+    value = whole_job_rate(n_fluid * args.steps, world, total_ms) / 1e6
+    e2e_value = whole_job_rate(n_fluid * args.steps, world, e2e_ms) / 1e6
     bpn = algorithmic_bytes_per_node(args.storage)
     achieved = bpn * n_fluid / (avg_launch_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
