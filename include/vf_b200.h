@@ -339,6 +339,13 @@ int vfb_sim_run(vfb_simulation* sim, unsigned int steps, void* stream);
 int vfb_sim_macroscopic(vfb_simulation* sim, int level, void* rho, void* vx, void* vy, void* vz, void* stream);
 /* FP64 sums over the level's fluid nodes (see vfb_mass_and_energy) */
 int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* out3, void* stream);
+/* KineticEnergyAnalyzer::run (src/gpu/core/PostProcessor/KineticEnergyAnalyzer.cu:66-108,137-154):
+ * out2[0] = sum of (drho + 1) |u|^2 / 2 over the level's nodes whose type is
+ * fluid and whose six axis neighbours (reached as the reference reaches them,
+ * through neighborX/Y/Z and the inverse neighbour) are fluid, divided by their
+ * number; out2[1] = that number.  The sum is FP64 (the reference reduces in
+ * the working precision).  Synchronises the stream. */
+int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* stream);
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,
                         int* isEvenTimestep, double* omega);

@@ -173,3 +173,28 @@ def test_graph_replay_equals_direct_launches(cuda, steps):
     for a, b in zip(outs[0][0], outs[1][0]):
         assert np.array_equal(a, b)
     assert outs[0][1] == outs[1][1]
+
+
+def test_kinetic_energy_analyzer_definition(cuda):
+    """vfb_sim_kinetic_energy: the mean of (1 + drho) |u|^2 / 2 over the fluid
+    nodes whose six axis neighbours are fluid, as KineticEnergyAnalyzer selects
+    them (the walls of a channel exclude the nodes next to them)."""
+    b = channel()
+    p = Parameter()
+    p.set_viscosity_LB(0.01)
+    sim = Simulation(p, b, BoundaryConditionFactory())
+    g = sim.levels[0]
+    sim.init_level(0, *_init(g, 8))
+    sim.run(5)
+    ke, count = sim.kinetic_energy(0)
+    geo, nx, ny, nz, nn = (g[k].astype(np.int64) for k in ("geo", "neighborX", "neighborY", "neighborZ",
+                                                           "neighborNeg"))
+    fluid = geo == 19
+    k = np.nonzero(fluid)[0]
+    w = nn[k]
+    sel = fluid[nx[k]] & fluid[ny[k]] & fluid[nz[k]] & fluid[w] & fluid[nz[ny[w]]] & fluid[nz[nx[w]]] & fluid[ny[nx[w]]]
+    nodes = k[sel]
+    assert 0 < count == len(nodes) < len(k)
+    drho, vx, vy, vz = sim.macroscopic(0)
+    want = np.sum(0.5 * (vx[nodes] ** 2 + vy[nodes] ** 2 + vz[nodes] ** 2) * (drho[nodes] + 1.0)) / len(nodes)
+    assert abs(ke - want) <= 1e-12 * abs(want)

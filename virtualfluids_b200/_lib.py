@@ -149,6 +149,8 @@ _SIGNATURES = [
       ctypes.c_void_p]),
     ("vfb_sim_mass_and_energy", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_sim_kinetic_energy", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_sim_level_state", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong),
       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),

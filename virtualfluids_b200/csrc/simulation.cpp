@@ -67,6 +67,8 @@ struct Level {
     BcListDevice velocity, noSlip, slip, geometry;
     std::vector<PressureListDevice*> pressure;
     InterfaceDevice coarseToFine, fineToCoarse;
+    DeviceBuffer energyNodes; // the kinetic-energy analyzer's node set
+    uint32_t nEnergy = 0;
     double omega = 1.0;
     double forceFactor = 1.0;
     bool isEven = true;
@@ -484,6 +486,41 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         L->omega = 1.0 / (3.0 * nu + 0.5);
         L->forceFactor = 1.0 / std::pow(2.0, l);
     }
+    // the kinetic-energy analyzer's node set of every level (KineticEnergyAnalyzer.cu:137-154)
+    for (int l = 0; l < nLevels && rc == VFB_OK; ++l) {
+        std::vector<char> geo, nx, ny, nz, nn;
+        long long count = 0;
+        int es = 0;
+        if (!gridArray(grid, l, "geo", geo, count, es) || !gridArray(grid, l, "neighborX", nx, count, es) ||
+            !gridArray(grid, l, "neighborY", ny, count, es) || !gridArray(grid, l, "neighborZ", nz, count, es))
+            continue;
+        const bool haveInverse = gridArray(grid, l, "neighborNeg", nn, count, es) && es == 4;
+        if (!haveInverse)
+            continue;
+        const uint32_t* G = reinterpret_cast<const uint32_t*>(geo.data());
+        const uint32_t* X = reinterpret_cast<const uint32_t*>(nx.data());
+        const uint32_t* Y = reinterpret_cast<const uint32_t*>(ny.data());
+        const uint32_t* Z = reinterpret_cast<const uint32_t*>(nz.data());
+        const uint32_t* W = reinterpret_cast<const uint32_t*>(nn.data());
+        const uint64_t N = S->levels[l]->N;
+        auto fluid = [&](uint32_t k) { return k < N && G[k] == VFB_GEO_FLUID; };
+        keep.emplace_back();
+        std::vector<char>& list = keep.back();
+        for (uint64_t k = 0; k < N; ++k) {
+            if (!fluid((uint32_t)k))
+                continue;
+            const uint32_t w = W[k];
+            if (!fluid(X[k]) || !fluid(Y[k]) || !fluid(Z[k]) || !fluid(w))
+                continue;
+            if (!fluid(Z[Y[w]]) || !fluid(Z[X[w]]) || !fluid(Y[X[w]]))
+                continue;
+            const uint32_t v = (uint32_t)k;
+            list.insert(list.end(), reinterpret_cast<const char*>(&v), reinterpret_cast<const char*>(&v) + 4);
+        }
+        S->levels[l]->nEnergy = (uint32_t)(list.size() / 4);
+        if (uploadRaw(S->levels[l]->energyNodes, list.data(), list.size(), s) != cudaSuccess)
+            rc = setError(VFB_ERR_CUDA, "energy node upload failed");
+    }
     // coarse-to-fine cells that share fine nodes: one writer per node (the last in list order)
     for (int l = 0; l + 1 < nLevels && rc == VFB_OK; ++l) {
         Level& C = *S->levels[l];
@@ -676,6 +713,29 @@ extern "C" int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* o
     return vfb_mass_and_energy(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->nX.ptr),
                                static_cast<const uint32_t*>(L->nY.ptr), static_cast<const uint32_t*>(L->nZ.ptr),
                                static_cast<const uint32_t*>(L->fluid.ptr), L->nFluid, L->isEven ? 1 : 0, out3, stream);
+}
+
+extern "C" int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!out2)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out2 is NULL");
+    out2[0] = out2[1] = 0.0;
+    if (L->nEnergy == 0)
+        return VFB_OK;
+    double sums[3];
+    const int rc = vfb_mass_and_energy(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->nX.ptr),
+                                       static_cast<const uint32_t*>(L->nY.ptr), static_cast<const uint32_t*>(L->nZ.ptr),
+                                       static_cast<const uint32_t*>(L->energyNodes.ptr), L->nEnergy,
+                                       L->isEven ? 1 : 0, sums, stream);
+    if (rc)
+        return rc;
+    out2[0] = sums[1] / (double)L->nEnergy;
+    out2[1] = (double)L->nEnergy;
+    return VFB_OK;
 }
 
 extern "C" int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions,

@@ -222,6 +222,13 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_mass_and_energy(self._h, level, out, self.stream))
         return out[0], out[1], int(out[2])
 
+    def kinetic_energy(self, level: int = 0):
+        """KineticEnergyAnalyzer's value: mean (1 + drho) |u|^2 / 2 over the
+        fluid nodes whose six axis neighbours are fluid (FP64 sum), and their number."""
+        out = (ctypes.c_double * 2)()
+        _lib.check(_lib.lib().vfb_sim_kinetic_energy(self._h, level, out, self.stream))
+        return out[0], int(out[1])
+
     def level_state(self, level: int = 0):
         """(device pointer of the populations, N, isEvenTimestep, omega)."""
         ptr = ctypes.c_void_p()
