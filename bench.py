@@ -490,7 +490,7 @@ def kernel_report(args):
     from virtualfluids_b200 import _lib
     from virtualfluids_b200 import kernels as K
     from virtualfluids_b200.grid import MultipleGridBuilder, SideType
-    from virtualfluids_b200.workloads import taylor_green
+    from virtualfluids_b200.workloads import cavity_grid, interface_planes, taylor_green
 
     peak, peak_kind = hbm_peak()
     out = {"report": "kernels", "peak_gbs": peak, "peak_kind": peak_kind, "storage": "fp32", "kernels": {}}
@@ -535,13 +535,7 @@ def kernel_report(args):
     def grid_of(builder):
         return builder.arrays()[0]
     nb = 256
-    b = MultipleGridBuilder()
-    b.addCoarseGrid(0, 0, 0, nb - 1, nb - 1, nb - 1, 1.0)
-    b.buildGrids()
-    for side in (SideType.MX, SideType.PX, SideType.MY, SideType.PY, SideType.MZ):
-        b.setNoSlipBoundaryCondition(side)
-    b.setVelocityBoundaryCondition(SideType.PZ, 0.05, 0.0, 0.0)
-    g = grid_of(b)
+    g = cavity_grid(nb)
     lat = K.DeviceLattice.from_arrays(g)
     dist = K.new_distributions(lat, torch.float32)
     dist.uniform_(-1e-3, 1e-3)
@@ -571,29 +565,9 @@ def kernel_report(args):
     del dist, lat
     torch.cuda.empty_cache()
 
-    # interface interpolation: two periodic boxes (coarse 128^3, fine 256^3) with
-    # structured interfaces: coarse-to-fine cells on two coarse z planes, each
-    # writing the fine 2x2x2 block at twice its coordinates; fine-to-coarse
-    # cells on a third plane reading the fine block below
-    from virtualfluids_b200.grid import taylor_green_grid
-    ncg, nfg = 128, 256
-    gc, gf = taylor_green_grid(ncg), taylor_green_grid(nfg)
-    flc, flf = gc["fluid"], gf["fluid"]
-
-    def coarse_at(i, j, kk):
-        return flc[i + ncg * (j + ncg * kk)]
-
-    def fine_at(i, j, kk):
-        return flf[i + nfg * (j + nfg * kk)]
-    ii, jj = np.meshgrid(np.arange(ncg), np.arange(ncg), indexing="ij")
-    ii, jj = ii.ravel(), jj.ravel()
-    cells = {}
-    for tag, planes in (("cf", (40, 41)), ("fc", (80,))):
-        cc, ff = [], []
-        for kk in planes:
-            cc.append(coarse_at(ii, jj, kk))
-            ff.append(fine_at(2 * ii, 2 * jj, 2 * kk))
-        cells[tag] = (np.concatenate(cc).astype(np.uint32), np.concatenate(ff).astype(np.uint32))
+    # interface interpolation: structured coarse-to-fine / fine-to-coarse planes
+    # between a coarse 128^3 and a fine 256^3 periodic box
+    gc, gf, cells = interface_planes(128, 256)
     latc, latf = K.DeviceLattice.from_arrays(gc), K.DeviceLattice.from_arrays(gf)
     dc, df = K.new_distributions(latc, torch.float32), K.new_distributions(latf, torch.float32)
     dc.uniform_(-1e-3, 1e-3)

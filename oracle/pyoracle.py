@@ -211,6 +211,68 @@ class Reference(_Lib):
         return sec, steps * n ** 3 / sec / 1e6
 
 
+def ref_gpu_available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"libvfref_gpu_{precision}.so").exists()
+
+
+def _dptr(t):
+    """Device address of a tensor (or None)."""
+    return None if t is None else _vp(t.data_ptr())
+
+
+class ReferenceGpu(_Lib):
+    """The reference's GPU kernel sources compiled unmodified by nvcc for
+    sm_100a (oracle/_ref/libvfref_gpu_{f32,f64}.so, launchers in
+    oracle/ref/ref_gpu_device.cu).  Arguments are CUDA tensors; every call is
+    asynchronous on `stream` (a cudaStream_t address, 0 = legacy stream)."""
+
+    def __init__(self, precision: str = "f64"):
+        real = np.float64 if precision == "f64" else np.float32
+        super().__init__(REF_DIR / f"libvfref_gpu_{precision}.so", "_" + precision, real)
+        R = _c.c_double if precision == "f64" else _c.c_float
+        self.R = R
+        self.fn("vfref_gpu_collision_k17").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _c.c_uint, R, _vp, R,
+                                                       _vp, _c.c_int, _vp]
+        self.fn("vfref_gpu_collision_bgk").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, R, _c.c_int, _vp]
+        self.fn("vfref_gpu_bc_post").argtypes = [_c.c_int, _vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _c.c_uint, R,
+                                                 _vp, _vp, _vp, _c.c_int, _vp]
+        for name in ("vfref_gpu_scale_cf", "vfref_gpu_scale_fc"):
+            self.fn(name).argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_ulonglong, _c.c_ulonglong, _c.c_int,
+                                      _vp, _vp, _c.c_uint, R, R, _vp, _vp, _vp, _vp]
+
+    @staticmethod
+    def _check(rc: int, what: str) -> None:
+        if rc != 0:
+            raise RuntimeError(f"{what}: CUDA error {rc}")
+
+    def collision_k17(self, dist, lat, omega, is_even, forces, limiters, force_factor=1.0, stream=0):
+        """forces / limiters: device tensors of three values of the library's real type."""
+        self._check(self.fn("vfref_gpu_collision_k17")(
+            _dptr(dist), lat.N, _dptr(lat.neighborX), _dptr(lat.neighborY), _dptr(lat.neighborZ), _dptr(lat.fluid),
+            lat.fluid.numel(), omega, _dptr(forces), force_factor, _dptr(limiters), int(is_even), _vp(stream)),
+            "runCollision<K17>")
+
+    def collision_bgk(self, dist, lat, omega, is_even, stream=0):
+        self._check(self.fn("vfref_gpu_collision_bgk")(
+            _dptr(dist), lat.N, _dptr(lat.geo), _dptr(lat.neighborX), _dptr(lat.neighborY), _dptr(lat.neighborZ),
+            omega, int(is_even), _vp(stream)), "B92CompressibleNavierStokes_Device")
+
+    def bc_post(self, kind, dist, lat, k, q, omega, is_even, vx=None, vy=None, vz=None, stream=0):
+        rc = self.fn("vfref_gpu_bc_post")(
+            kind, _dptr(dist), lat.N, _dptr(lat.neighborX), _dptr(lat.neighborY), _dptr(lat.neighborZ), _dptr(k),
+            _dptr(q), k.numel(), omega, _dptr(vx), _dptr(vy), _dptr(vz), int(is_even), _vp(stream))
+        self._check(rc, f"BC kernel kind {kind}")
+
+    def scale(self, coarse_to_fine, distC, distF, latC, latF, is_even, cells_c, cells_f, omega_c, omega_f,
+              off_x, off_y, off_z, stream=0):
+        name = "vfref_gpu_scale_cf" if coarse_to_fine else "vfref_gpu_scale_fc"
+        rc = self.fn(name)(_dptr(distC), _dptr(distF), _dptr(latC.neighborX), _dptr(latC.neighborY),
+                           _dptr(latC.neighborZ), _dptr(latF.neighborX), _dptr(latF.neighborY), _dptr(latF.neighborZ),
+                           latC.N, latF.N, int(is_even), _dptr(cells_c), _dptr(cells_f), cells_c.numel(), omega_c,
+                           omega_f, _dptr(off_x), _dptr(off_y), _dptr(off_z), _vp(stream))
+        self._check(rc, name)
+
+
 _NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims", "fluid",
           "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k", "slip.nx", "slip.ny",
           "slip.nz", "slip.q", "geometry.k", "geometry.q", "pressure.count", "cf.coarse", "cf.fine", "fc.coarse",

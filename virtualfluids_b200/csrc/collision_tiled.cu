@@ -107,9 +107,13 @@ struct TiledArgs {
     unsigned long long N;
     const uint32_t* __restrict__ meta;
     uint32_t nTiles;
-    // wrap offset minus lattice stride per axis (added to a location on a
-    // wrapped axis)
-    long long wrapDelta[3];
+    // per direction: the start of the direction's slot (dist + slot * N); a
+    // location's element index within the slot is always in [0, N)
+    S* sbase[27];
+    // per axis (x, y, z): the location offset of a node, {lattice stride,
+    // offset of the periodic image for a node that wraps on that axis}, both
+    // modulo 2^32 (node index + offset is the location's index in [0, N))
+    uint32_t axisOff[3][2];
     K17Rates<R> rates;
     R fx, fy, fz, gfx, gfy, gfz, forceFactor;
     // the same rates and forces duplicated into register pairs (paired kernel)
@@ -130,6 +134,27 @@ struct TiledArgs {
 __host__ __device__ __forceinline__ uint32_t locShift(int l, uint32_t sy, uint32_t sz)
 {
     return (uint32_t)(l & 1) + ((l & 2) ? sy : 0u) + ((l & 4) ? sz : 0u);
+}
+
+// location offsets of one lane along x, y and z: the lattice stride, or the
+// offset of the periodic image on an axis where the lane's node wraps (wrap
+// bits wb: bit 0 x, bit 1 y, bit 2 z)
+struct LaneOffsets {
+    uint32_t x, y, z;
+};
+
+template <class S>
+__device__ __forceinline__ LaneOffsets laneOffsets(const TiledArgs<S>& a, int wb)
+{
+    return { (wb & 1) ? a.axisOff[0][1] : a.axisOff[0][0], (wb & 2) ? a.axisOff[1][1] : a.axisOff[1][0],
+             (wb & 4) ? a.axisOff[2][1] : a.axisOff[2][0] };
+}
+
+// element index, within its slot, of location l of node k.  The true index is
+// in [0, N), so the 32-bit sum with wrap-around is exact.
+__device__ __forceinline__ uint32_t locIndex(uint32_t k, LaneOffsets o, int l)
+{
+    return k + ((l & 1) ? o.x : 0u) + ((l & 2) ? o.y : 0u) + ((l & 4) ? o.z : 0u);
 }
 
 // thread 0 arms a stage's "full" barrier and issues the tile's 27 bulk
@@ -263,14 +288,12 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                 for (int d = 0; d < 27; ++d)
                     f[d] = Storage<S>::load(st + a.smemOff[d]);
             } else {
-                const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
-                const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
-                const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+                const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
                 for (int d = 0; d < 27; ++d) {
                     const int l = loc(d);
-                    const long long delta = ((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll);
-                    f[d] = (l & wb) ? Storage<S>::load(a.gbase[d] + k + delta) : Storage<S>::load(st + a.smemOff[d]);
+                    f[d] = (l & wb) ? Storage<S>::load(a.sbase[d] + locIndex(k, o, l))
+                                    : Storage<S>::load(st + a.smemOff[d]);
                 }
             }
         }
@@ -287,15 +310,10 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                 for (int d = 0; d < 27; ++d)
                     Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
             } else {
-                const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
-                const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
-                const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+                const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
-                for (int d = 0; d < 27; ++d) {
-                    const int l = loc(d);
-                    const long long delta = ((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll);
-                    Storage<S>::store(a.gbase[d] + k + delta, f[inv(d)]);
-                }
+                for (int d = 0; d < 27; ++d)
+                    Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
             }
         }
     }
@@ -332,21 +350,14 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
         const int wb = (int)((__ldg(meta + 4 + WARPS + warp) >> lane) & 1u) |
                        (int)(((__ldg(meta + 4 + 2 * WARPS + warp) >> lane) & 1u) << 1) |
                        (int)(((__ldg(meta + 4 + 3 * WARPS + warp) >> lane) & 1u) << 2);
-        const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
-        const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
-        const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+        const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            const int l = loc(d);
-            f[d] = Storage<S>::load(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll)));
-        }
+        for (int d = 0; d < 27; ++d)
+            f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, loc(d)));
         collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            const int l = loc(d);
-            Storage<S>::store(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) + ((l & 4) ? dz : 0ll)),
-                              f[inv(d)]);
-        }
+        for (int d = 0; d < 27; ++d)
+            Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
     }
 }
 
@@ -355,13 +366,11 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
 // k0 + T / 2 + t together in paired FP32 arithmetic (both loads of every
 // direction coalesced across the warp).  FP32 arithmetic only (FP32, FP16,
 // BF16 storage); the K17 collision.
-template <class S>
-__device__ __forceinline__ long long wrapLocDelta(const TiledArgs<S>& a, int wb, int l)
-{
-    const int m = l & wb;
-    return ((m & 1) ? a.wrapDelta[0] : 0ll) + ((m & 2) ? a.wrapDelta[1] : 0ll) + ((m & 4) ? a.wrapDelta[2] : 0ll);
-}
-
+//
+// A warp whose 64 nodes are all active and none wraps (the common case)
+// loads and stores without predicates, the second node's address an
+// immediate offset from the first's.  Other warps take the general path:
+// per-lane predicates and the lanes' location offsets.
 template <class S, class C, bool EVEN, bool WM, bool BF>
 __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<S> a)
 {
@@ -371,37 +380,40 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const uint32_t* meta = a.meta + (size_t)blockIdx.x * C::META_WORDS;
-    const bool actA = (__ldg(meta + 4 + warp) >> lane) & 1u;
-    const bool actB = (__ldg(meta + 4 + W2 + warp) >> lane) & 1u;
+    const uint32_t maskA = __ldg(meta + 4 + warp), maskB = __ldg(meta + 4 + W2 + warp);
+    const bool actA = (maskA >> lane) & 1u;
+    const bool actB = (maskB >> lane) & 1u;
     if (!(actA || actB))
         return;
     const uint32_t k0 = __ldg(meta);
     const uint32_t kA = k0 + tid, kB = k0 + HALF + tid;
     const uint32_t wf = __ldg(meta + 1);
     const bool wrap = (((wf >> warp) | (wf >> (W2 + warp))) & 1u) != 0;
-    int wbA = 0, wbB = 0;
+    // the same for every lane of the warp
+    const bool full = !wrap && (maskA & maskB) == 0xffffffffu;
+    LaneOffsets oA = laneOffsets(a, 0), oB = oA;
     if (wrap) {
         auto bitsOf = [&](int word) {
             return (int)((__ldg(meta + 4 + WARPS + word) >> lane) & 1u) |
                    (int)(((__ldg(meta + 4 + 2 * WARPS + word) >> lane) & 1u) << 1) |
                    (int)(((__ldg(meta + 4 + 3 * WARPS + word) >> lane) & 1u) << 2);
         };
-        wbA = bitsOf(warp);
-        wbB = bitsOf(W2 + warp);
+        oA = laneOffsets(a, bitsOf(warp));
+        oB = laneOffsets(a, bitsOf(W2 + warp));
     }
     F2 f[27];
-    if (!wrap) {
+    if (full) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
-            const float x = actA ? Storage<S>::load(a.gbase[d] + kA) : 0.0f;
-            const float y = actB ? Storage<S>::load(a.gbase[d] + kB) : 0.0f;
-            f[d] = F2(x, y);
+            const S* p = a.gbase[d] + kA;
+            f[d] = F2(Storage<S>::load(p), Storage<S>::load(p + HALF));
         }
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
-            const float x = actA ? Storage<S>::load(a.gbase[d] + kA + wrapLocDelta(a, wbA, loc(d))) : 0.0f;
-            const float y = actB ? Storage<S>::load(a.gbase[d] + kB + wrapLocDelta(a, wbB, loc(d))) : 0.0f;
+            const int l = loc(d);
+            const float x = actA ? Storage<S>::load(a.sbase[d] + locIndex(kA, oA, l)) : 0.0f;
+            const float y = actB ? Storage<S>::load(a.sbase[d] + locIndex(kB, oB, l)) : 0.0f;
             f[d] = F2(x, y);
         }
     }
@@ -432,13 +444,24 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
             a.vz[kB] = uz.v.y;
         }
     }
+    if (full) {
 #pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        const F2 v = f[inv(d)];
-        if (actA)
-            Storage<S>::store(a.gbase[d] + kA + (wrap ? wrapLocDelta(a, wbA, loc(d)) : 0ll), v.v.x);
-        if (actB)
-            Storage<S>::store(a.gbase[d] + kB + (wrap ? wrapLocDelta(a, wbB, loc(d)) : 0ll), v.v.y);
+        for (int d = 0; d < 27; ++d) {
+            S* p = a.gbase[d] + kA;
+            const F2 v = f[inv(d)];
+            Storage<S>::store(p, v.v.x);
+            Storage<S>::store(p + HALF, v.v.y);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const int l = loc(d);
+            const F2 v = f[inv(d)];
+            if (actA)
+                Storage<S>::store(a.sbase[d] + locIndex(kA, oA, l), v.v.x);
+            if (actB)
+                Storage<S>::store(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
+        }
     }
 }
 
@@ -503,25 +526,19 @@ __global__ void __launch_bounds__(C::T, C::MINB) asyncKernel(const TiledArgs<S> 
             const uint32_t k = k0 + tid;
             const S* src = buf + (size_t)stage * 27 * C::T + tid;
             R f[27];
-            const long long dx = (wb & 1) ? a.wrapDelta[0] : 0ll;
-            const long long dy = (wb & 2) ? a.wrapDelta[1] : 0ll;
-            const long long dz = (wb & 4) ? a.wrapDelta[2] : 0ll;
+            const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const int l = loc(d);
                 if (l & wb)
-                    f[d] = Storage<S>::load(a.gbase[d] + k + (((l & 1) ? dx : 0ll) + ((l & 2) ? dy : 0ll) +
-                                                             ((l & 4) ? dz : 0ll)));
+                    f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, l));
                 else
                     f[d] = Storage<S>::load(src + d * C::T);
             }
             collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
-            for (int d = 0; d < 27; ++d) {
-                const int l = loc(d);
-                const long long delta = ((l & wb & 1) ? dx : 0ll) + ((l & wb & 2) ? dy : 0ll) + ((l & wb & 4) ? dz : 0ll);
-                Storage<S>::store(a.gbase[d] + k + delta, f[inv(d)]);
-            }
+            for (int d = 0; d < 27; ++d)
+                Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
         }
         k0 = nk0;
         act = nact;
@@ -865,6 +882,7 @@ static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t s
     for (int d = 0; d < 27; ++d) {
         const unsigned long long off = (unsigned long long)(even ? d : inv(d)) * a.N + locShift(loc(d), sy, sz);
         a.gbase[d] = a.dist + off;
+        a.sbase[d] = a.dist + (unsigned long long)(even ? d : inv(d)) * a.N;
         a.lead[d] = (int)(off % C::E);
         a.smemOff[d] = d * C::CAP + a.lead[d];
         a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
@@ -905,6 +923,7 @@ static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t 
     for (int d = 0; d < 27; ++d) {
         const unsigned long long off = (unsigned long long)(even ? d : inv(d)) * a.N + locShift(loc(d), sy, sz);
         a.gbase[d] = a.dist + off;
+        a.sbase[d] = a.dist + (unsigned long long)(even ? d : inv(d)) * a.N;
         a.lead[d] = (int)(off % C::E);
         a.smemOff[d] = d * C::CAP + a.lead[d];
         a.bytes[d] = (uint32_t)(((a.lead[d] + C::T + C::E - 1) / C::E) * C::E * (int)sizeof(S));
@@ -927,8 +946,11 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.N = p.N;
     a.meta = p.meta;
     a.nTiles = p.nTiles;
-    for (int ax = 0; ax < 3; ++ax)
-        a.wrapDelta[ax] = p.wrapDelta[ax];
+    const uint32_t strides[3] = { 1u, p.sy, p.sz };
+    for (int ax = 0; ax < 3; ++ax) {
+        a.axisOff[ax][0] = strides[ax];
+        a.axisOff[ax][1] = (uint32_t)(p.wrapDelta[ax] + (long long)strides[ax]);
+    }
     a.rates = makeK17Rates<R>((R)c->omega, (R)c->quadricLimiters[0], (R)c->quadricLimiters[1],
                               (R)c->quadricLimiters[2]);
     a.forceFactor = (R)c->forceFactor;

@@ -56,3 +56,36 @@ def taylor_green(n: int, u0: float = 0.05, reynolds: float = 1600.0, noise: floa
     nu = taylor_green_viscosity(n, u0, reynolds)
     omega = 1.0 / (3.0 * nu + 0.5)
     return TaylorGreen(n, u0, nu, omega, g, rho, vx, vy, vz)
+
+
+def cavity_grid(n: int, lid: float = 0.05) -> dict:
+    """Level 0 of the lid-driven cavity: n^3 nodes, interpolated no-slip
+    (q = 1/2) on five faces and the lid velocity (lid, 0, 0) on +z, built by
+    the library's grid builder."""
+    from .grid import MultipleGridBuilder, SideType
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, n - 1, n - 1, n - 1, 1.0)
+    b.buildGrids()
+    for side in (SideType.MX, SideType.PX, SideType.MY, SideType.PY, SideType.MZ):
+        b.setNoSlipBoundaryCondition(side)
+    b.setVelocityBoundaryCondition(SideType.PZ, lid, 0.0, 0.0)
+    return b.arrays()[0]
+
+
+def interface_planes(ncg: int = 128, nfg: int = 256, cf_planes=(40, 41), fc_planes=(80,)):
+    """Two periodic boxes (coarse ncg^3, fine nfg^3) with structured interface
+    cells: coarse-to-fine cells on the coarse z planes `cf_planes`, each
+    writing the fine 2x2x2 block at twice its coordinates, and fine-to-coarse
+    cells on `fc_planes` reading the fine block there.  No two cells write the
+    same node.  Returns (coarse grid, fine grid, {"cf": (coarse, fine),
+    "fc": (coarse, fine)}) with uint32 cell index arrays."""
+    gc, gf = taylor_green_grid(ncg), taylor_green_grid(nfg)
+    flc, flf = gc["fluid"], gf["fluid"]
+    ii, jj = np.meshgrid(np.arange(ncg), np.arange(ncg), indexing="ij")
+    ii, jj = ii.ravel(), jj.ravel()
+    cells = {}
+    for tag, planes in (("cf", cf_planes), ("fc", fc_planes)):
+        cc = [flc[ii + ncg * (jj + ncg * kk)] for kk in planes]
+        ff = [flf[2 * ii + nfg * (2 * jj + nfg * 2 * kk)] for kk in planes]
+        cells[tag] = (np.concatenate(cc).astype(np.uint32), np.concatenate(ff).astype(np.uint32))
+    return gc, gf, cells
