@@ -401,21 +401,28 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
         oA = laneOffsets(a, bitsOf(warp));
         oB = laneOffsets(a, bitsOf(W2 + warp));
     }
+    // FP16's storage scale is applied to both nodes in one paired multiply
+    using St = Storage<S>;
     F2 f[27];
     if (full) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const S* p = a.gbase[d] + kA;
-            f[d] = F2(Storage<S>::load(p), Storage<S>::load(p + HALF));
+            f[d] = F2(St::loadRaw(p), St::loadRaw(p + HALF));
         }
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int l = loc(d);
-            const float x = actA ? Storage<S>::load(a.sbase[d] + locIndex(kA, oA, l)) : 0.0f;
-            const float y = actB ? Storage<S>::load(a.sbase[d] + locIndex(kB, oB, l)) : 0.0f;
+            const float x = actA ? St::loadRaw(a.sbase[d] + locIndex(kA, oA, l)) : 0.0f;
+            const float y = actB ? St::loadRaw(a.sbase[d] + locIndex(kB, oB, l)) : 0.0f;
             f[d] = F2(x, y);
         }
+    }
+    if (St::scaled) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = f[d] * F2(kHalfInvScale);
     }
     F2 fx = a.fx2, fy = a.fy2, fz = a.fz2;
     if (BF) {
@@ -444,13 +451,18 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
             a.vz[kB] = uz.v.y;
         }
     }
+    if (St::scaled) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = f[d] * F2(kHalfScale);
+    }
     if (full) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             S* p = a.gbase[d] + kA;
             const F2 v = f[inv(d)];
-            Storage<S>::store(p, v.v.x);
-            Storage<S>::store(p + HALF, v.v.y);
+            St::storeRaw(p, v.v.x);
+            St::storeRaw(p + HALF, v.v.y);
         }
     } else {
 #pragma unroll
@@ -458,9 +470,9 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
             const int l = loc(d);
             const F2 v = f[inv(d)];
             if (actA)
-                Storage<S>::store(a.sbase[d] + locIndex(kA, oA, l), v.v.x);
+                St::storeRaw(a.sbase[d] + locIndex(kA, oA, l), v.v.x);
             if (actB)
-                Storage<S>::store(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
+                St::storeRaw(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
         }
     }
 }
@@ -623,8 +635,8 @@ cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 
 // Tile configurations (tile width, stages, resident blocks) the library is
 // compiled for; 0 stages selects the direct-load kernel, 1 stage the paired
-// direct-load kernel.  Entry 12 is the default for FP32, entry 9 for FP16 /
-// BF16 and entry 1 for FP64 (the fastest at Taylor-Green 512^3 on B200);
+// direct-load kernel.  Entry 12 (paired) is the default for FP32, FP16 and
+// BF16, entry 1 for FP64 (the fastest at Taylor-Green 512^3 on B200);
 // VFB_TILE_CONFIG=<index> selects another one at plan creation (used to tune
 // the shape on new hardware).
 struct TileConfigInfo {
@@ -640,13 +652,15 @@ static const TileConfigInfo kTileConfigs[] = {
     { 256, 1, 4, false }, { 256, 1, 3, false }, { 256, 1, 2, false },
     // per-thread cp.async pipeline (2 shared-memory stages per thread)
     { 256, 2, 3, false }, { 128, 2, 6, false }, { 128, 2, 3, true }, { 128, 2, 2, true },
+    // paired, five resident blocks (96 registers, small spills)
+    { 256, 1, 5, false },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
 static int chooseTileConfig(int storage)
 {
     const bool fp64 = storage == VFB_FP64;
-    int def = fp64 ? 1 : (vfb_storage_bytes(storage) == 2 ? 9 : 12);
+    int def = fp64 ? 1 : 12;
     if (const char* env = std::getenv("VFB_TILE_CONFIG")) {
         const int c = std::atoi(env);
         if (c >= 0 && c < kNumTileConfigs && kTileConfigs[c].fp64 == fp64)
@@ -1007,9 +1021,10 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
                 return setError(VFB_ERR_UNSUPPORTED, "the pipelined kernel needs 4- or 8-byte storage");
         case 13: return dispatchTiled<S, TileCfg<S, 256, 1, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 14: return dispatchTiled<S, TileCfg<S, 256, 1, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 19: return dispatchTiled<S, TileCfg<S, 256, 1, 5>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 9:
-            // the default for 16-bit storage (compute bound: direct loads keep more warps colliding)
+            // direct loads, six resident blocks (16-bit storage: all templates)
             if constexpr (sizeof(S) == 2)
                 return dispatchTiled<S, TileCfg<S, 128, 0, 6>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
             else

@@ -22,14 +22,18 @@ template <>
 struct Storage<float> {
     using R = float;
     static constexpr int id = 0;
+    static constexpr bool scaled = false;
     __device__ __forceinline__ static R load(const float* p) { return *p; }
     __device__ __forceinline__ static void store(float* p, R v) { *p = v; }
+    __device__ __forceinline__ static R loadRaw(const float* p) { return *p; }
+    __device__ __forceinline__ static void storeRaw(float* p, R v) { *p = v; }
 };
 
 template <>
 struct Storage<double> {
     using R = double;
     static constexpr int id = 1;
+    static constexpr bool scaled = false;
     __device__ __forceinline__ static R load(const double* p) { return *p; }
     __device__ __forceinline__ static void store(double* p, R v) { *p = v; }
 };
@@ -42,15 +46,23 @@ template <>
 struct Storage<__half> {
     using R = float;
     static constexpr int id = 2;
+    static constexpr bool scaled = true;
     __device__ __forceinline__ static R load(const __half* p) { return __half2float(*p) * kHalfInvScale; }
     __device__ __forceinline__ static void store(__half* p, R v) { *p = __float2half_rn(v * kHalfScale); }
+    // the stored number without the scale (a caller applies kHalfInvScale /
+    // kHalfScale itself, e.g. to two values in one paired multiply)
+    __device__ __forceinline__ static R loadRaw(const __half* p) { return __half2float(*p); }
+    __device__ __forceinline__ static void storeRaw(__half* p, R v) { *p = __float2half_rn(v); }
 };
 
 template <>
 struct Storage<__nv_bfloat16> {
     using R = float;
     static constexpr int id = 3;
+    static constexpr bool scaled = false;
     __device__ __forceinline__ static R load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn(v); }
+    __device__ __forceinline__ static R loadRaw(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ __forceinline__ static void storeRaw(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn(v); }
 };
 } // namespace vfb
