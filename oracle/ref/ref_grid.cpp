@@ -94,6 +94,7 @@ extern "C" {
 //  [30..59] six side BCs in the order they are set: side id (0..5 = MX..PZ),
 //           type (0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip), 3 values
 //  [60]     enableThinWalls argument of buildGrids
+//  [61]     finest level of the refinement box (0 = level 1)
 void* REF(vfref_grid_build)(const double* s)
 {
     auto builder = std::make_shared<MultipleGridBuilder>();
@@ -101,7 +102,8 @@ void* REF(vfref_grid_build)(const double* s)
     if (s[17] > 0)
         builder->setNumberOfLayers((uint)s[17], (uint)s[18]);
     if (s[10] > 0)
-        builder->addGrid(std::make_shared<Cuboid>(s[11], s[12], s[13], s[14], s[15], s[16]), 1);
+        builder->addGrid(std::make_shared<Cuboid>(s[11], s[12], s[13], s[14], s[15], s[16]),
+                         s[61] > 0 ? (uint)s[61] : 1u);
     if (s[19] > 0)
         builder->addGeometry(std::make_shared<Cuboid>(s[20], s[21], s[22], s[23], s[24], s[25]));
     builder->setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);

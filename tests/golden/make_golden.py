@@ -14,6 +14,8 @@ import math
 import sys
 from pathlib import Path
 
+import subprocess
+
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
@@ -54,13 +56,19 @@ def grids() -> None:
         np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
 
 
+def refined_grid(name: str) -> None:
+    """One multi-level grid with its interface cells, from the reference builder."""
+    levels = Reference("f64").grid(refined_spec(name))
+    arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
+    np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
+
+
 def refined_grids() -> None:
-    """Two-level grids with their interface cells, from the reference builder."""
-    R = Reference("f64")
+    """Every multi-level scenario, each built in a fresh process: the
+    reference's builder is not reliable across several multi-level builds in
+    one process (it has crashed there)."""
     for name in REFINED_SCENARIOS:
-        levels = R.grid(refined_spec(name))
-        arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
-        np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
+        subprocess.run([sys.executable, __file__, "--refined", name], check=True)
 
 
 def lattice(precision: str) -> None:
@@ -71,6 +79,9 @@ def lattice(precision: str) -> None:
 
 
 if __name__ == "__main__":
+    if len(sys.argv) == 3 and sys.argv[1] == "--refined":
+        refined_grid(sys.argv[2])
+        sys.exit(0)
     for p in ("f64", "f32"):
         k17_nodes(p)
         lattice(p)

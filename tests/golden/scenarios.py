@@ -40,10 +40,14 @@ def grid_spec(name: str) -> np.ndarray:
 
 GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel"]
 
-# two-level grids made by the reference's builder (the repository's builder
-# does not build refinement levels): a channel 24 x 16 x 16 with a refined box
-# and the reference's default layer counts, inlet velocity and outlet pressure
-REFINED_SCENARIOS = ["refined_channel", "cube_channel"]
+# multi-level grids made by the reference's builder, which the repository's
+# builder reproduces: a channel 24 x 16 x 16 with a refined box and the
+# reference's default layer counts, inlet velocity and outlet pressure; the
+# cube channel (below); a box refined twice (three levels) with its own layer
+# counts (the reference's builder crashes for two layers between levels); a
+# box on the floor and the inlet wall (odd starts, refinement into
+# two walls) around a solid cuboid
+REFINED_SCENARIOS = ["refined_channel", "cube_channel", "two_level_box", "wall_box_solid"]
 
 
 def refined_spec(name: str) -> np.ndarray:
@@ -64,6 +68,24 @@ def refined_spec(name: str) -> np.ndarray:
         s[11:17] = [12, 4, 0, 28, 12, 8]
         s[19] = 1.0
         s[20:26] = [16, 6, 0, 20, 10, 4]
+        s[26] = 1.0
+        return s
+    if name == "two_level_box":
+        sides = [(MX, VELOCITY, 0.03, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 31, 23, 23, 1.0], (0, 1, 0), sides=sides)
+        s[10] = 1.0
+        s[11:17] = [12, 9, 9, 17, 14, 14]
+        s[17:19] = [6, 4]
+        s[61] = 2.0
+        return s
+    if name == "wall_box_solid":
+        sides = [(PX, PRESSURE, 0.0, 0, 0), (MX, VELOCITY, 0.04, 0.0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 23, 13, 11, 1.0], (0, 1, 0), sides=sides)
+        s[10] = 1.0
+        s[11:17] = [0, 3, 0, 10, 10, 6]
+        s[17:19] = [6, 3]
+        s[19] = 1.0
+        s[20:26] = [3, 5, 0, 6, 8, 3]
         s[26] = 1.0
         return s
     raise KeyError(name)

@@ -1,6 +1,7 @@
 // grid_builder.cpp -- see grid_builder.hpp.
 #include "grid_builder.hpp"
 
+#include <cfloat>
 #include <cmath>
 #include <stdexcept>
 
@@ -42,6 +43,40 @@ LevelGrid::LevelGrid(double sx, double sy, double sz, double ex, double ey, doub
     ny = (uint32_t)std::lround((endY - startY + delta) / delta);
     nz = (uint32_t)std::lround((endZ - startZ + delta) / delta);
     size = (uint64_t)nx * ny * nz;
+}
+
+namespace
+{
+// vf::Math::lessEqual / greaterEqual with the default tolerance
+// (utilities/math/Math.cpp:40-64, EPSILON = FLT_EPSILON)
+bool nearlyEqual(double a, double b)
+{
+    const double largest = std::fabs(b) > std::fabs(a) ? std::fabs(b) : std::fabs(a);
+    return std::fabs(a - b) <= largest * (double)FLT_EPSILON;
+}
+bool lessEqualTol(double a, double b) { return a < b || nearlyEqual(a, b); }
+bool greaterEqualTol(double a, double b) { return a > b || nearlyEqual(a, b); }
+} // namespace
+
+bool Box::containsPoint(double x, double y, double z) const
+{
+    const double lo[3] = { std::fmin(minX, maxX), std::fmin(minY, maxY), std::fmin(minZ, maxZ) };
+    const double hi[3] = { std::fmax(minX, maxX), std::fmax(minY, maxY), std::fmax(minZ, maxZ) };
+    const double p[3] = { x, y, z };
+    for (int a = 0; a < 3; ++a)
+        if (lessEqualTol(p[a], lo[a]) || greaterEqualTol(p[a], hi[a]))
+            return false;
+    return true;
+}
+
+int64_t LevelGrid::coordToIndex(double x, double y, double z) const
+{
+    const long ix = std::lround((x - startX) / delta);
+    const long iy = std::lround((y - startY) / delta);
+    const long iz = std::lround((z - startZ) / delta);
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= (long)nx || iy >= (long)ny || iz >= (long)nz)
+        return -1;
+    return (int64_t)ix + (int64_t)nx * ((int64_t)iy + (int64_t)ny * (int64_t)iz);
 }
 
 bool LevelGrid::isFluid(uint64_t i) const
@@ -89,30 +124,106 @@ bool LevelGrid::hasAllNeighbors(uint64_t idx) const
     return true;
 }
 
-// Coarse level: everything but the outermost layer is fluid
-// (GridImp::findInnerNode, GridImp.cpp:225-248), then odd cells are completed
-// (GridImp::fixOddCell, :466-472) and the outermost layer becomes the stopper
-// layer (GridImp::findEndOfGridStopperNode, :436-448).
-void LevelGrid::initialNodes()
+// The node types of one level (GridImp::inital, GridImp.cpp:122-194): the
+// inner region (the coarse level: everything but the outermost layer,
+// GridImp::findInnerNode :228-248; a refined level: the nodes whose odd cell
+// lies inside the refinement box; an intermediate level: the nodes with a
+// fluid child on the finer level, :311-336), the overlap layers (:338-366),
+// the completed odd cells (:465-472) and the end-of-grid stoppers (:436-448).
+void LevelGrid::initial(const LevelGrid* finer)
 {
     field.assign(size, INVALID_OUT_OF_GRID);
-    for (uint32_t z = 1; z + 1 < nz; ++z)
-        for (uint32_t y = 1; y + 1 < ny; ++y)
-            for (uint32_t x = 1; x + 1 < nx; ++x)
-                field[(uint64_t)index(x, y, z)] = FLUID;
+    if (innerFromFiner) {
+        if (!finer)
+            throw std::runtime_error("intermediate level without a finer level");
+        setInnerBasedOnFinerGrid(*finer);
+    } else {
+        findInnerNodes();
+    }
+    addOverlap();
     fixOddCells();
+    findStoppers();
 }
 
-// Odd cells are 2x2x2 blocks starting at odd indices (xOddStart == false).
-// A block lying completely inside the grid that holds a fluid node is made
-// entirely fluid.
-void LevelGrid::fixOddCells()
+// start index of the odd cell (2x2x2 block) holding index i along an axis
+// (GridImp::getOddCellFromIndex, GridImp.cpp:287-309)
+int64_t LevelGrid::oddCellStart(int64_t i, int axis) const
 {
-    auto cellStart = [](int64_t i) { return (i % 2 != 0) ? i : i - 1; };
+    const bool odd = (i % 2) != 0;
+    return oddStart[axis] ? (odd ? i - 1 : i) : (odd ? i : i - 1);
+}
+
+void LevelGrid::findInnerNodes()
+{
+    if (level == 0) {
+        for (uint32_t z = 1; z + 1 < nz; ++z)
+            for (uint32_t y = 1; y + 1 < ny; ++y)
+                for (uint32_t x = 1; x + 1 < nx; ++x)
+                    field[(uint64_t)index(x, y, z)] = FLUID;
+        return;
+    }
+    if (!hasShape)
+        throw std::runtime_error("refined level without a refinement box");
     for (uint64_t idx = 0; idx < size; ++idx) {
         int64_t ix, iy, iz;
         coords(idx, ix, iy, iz);
-        const int64_t x0 = cellStart(ix), y0 = cellStart(iy), z0 = cellStart(iz);
+        // the cell's corner coordinates as the reference forms them: the
+        // node's coordinate, or one spacing below it, plus 0 / 1 spacing
+        const double x = coordX(ix), y = coordY(iy), z = coordZ(iz);
+        const double xs = oddCellStart(ix, 0) == ix ? x : x - delta;
+        const double ys = oddCellStart(iy, 1) == iy ? y : y - delta;
+        const double zs = oddCellStart(iz, 2) == iz ? z : z - delta;
+        bool inside = true;
+        for (int c = 0; c < 8 && inside; ++c)
+            inside = shape.containsPoint((c & 1) ? xs + delta : xs, (c & 2) ? ys + delta : ys,
+                                         (c & 4) ? zs + delta : zs);
+        if (inside)
+            field[idx] = FLUID;
+    }
+}
+
+void LevelGrid::setInnerBasedOnFinerGrid(const LevelGrid& fine)
+{
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        const double x = coordX(ix), y = coordY(iy), z = coordZ(iz);
+        const double q = 0.25 * delta;
+        // children in the order of GridImp.cpp:318-325 (+ before -, z fastest)
+        for (int c = 0; c < 8; ++c) {
+            const double cxq = (c & 4) ? x - q : x + q;
+            const double cyq = (c & 2) ? y - q : y + q;
+            const double czq = (c & 1) ? z - q : z + q;
+            const int64_t child = fine.coordToIndex(cxq, cyq, czq);
+            if (child >= 0 && fine.field[(uint64_t)child] == FLUID) {
+                field[idx] = FLUID;
+                break;
+            }
+        }
+    }
+}
+
+void LevelGrid::addOverlap()
+{
+    for (uint32_t layer = 0; layer < numberOfLayers; ++layer) {
+        for (uint64_t idx = 0; idx < size; ++idx)
+            if (field[idx] == INVALID_OUT_OF_GRID && hasNeighborOfType(idx, FLUID))
+                field[idx] = OVERLAP_TMP;
+        for (uint64_t idx = 0; idx < size; ++idx)
+            if (field[idx] == OVERLAP_TMP)
+                field[idx] = FLUID;
+    }
+}
+
+// A 2x2x2 odd cell lying completely inside the grid that holds a fluid node
+// is made entirely fluid.  Odd cells tile the grid, so the result does not
+// depend on the visiting order.
+void LevelGrid::fixOddCells()
+{
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        const int64_t x0 = oddCellStart(ix, 0), y0 = oddCellStart(iy, 1), z0 = oddCellStart(iz, 2);
         if (x0 < 0 || y0 < 0 || z0 < 0 || x0 + 1 >= (int64_t)nx || y0 + 1 >= (int64_t)ny || z0 + 1 >= (int64_t)nz)
             continue;
         bool any = false;
@@ -249,6 +360,300 @@ void LevelGrid::findFluidNodes()
             fluidNodes.push_back((uint32_t)(sparseIndex[i] + 1));
 }
 
+// ------------------------------------------------------------------ solid --
+// GridImp::mesh for a geometric primitive (GridImp.cpp:1300-1320): nodes
+// strictly inside the cuboid become INVALID_SOLID (GridImp::discretize
+// :251-268), needle cells are closed (:1362-1401), INVALID_SOLID nodes next to
+// fluid become STOPPER_SOLID (:449-453) and fluid nodes next to those BC_SOLID,
+// numbered in matrix order (:455-463).
+void LevelGrid::meshSolid(const Box& solid)
+{
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (field[idx] == INVALID_SOLID)
+            continue;
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        if (solid.containsPoint(coordX(ix), coordY(iy), coordZ(iz)))
+            field[idx] = INVALID_SOLID;
+    }
+    auto isSolidAt = [&](int64_t jx, int64_t jy, int64_t jz) {
+        const int64_t m = index(jx, jy, jz);
+        return m >= 0 && field[(uint64_t)m] == INVALID_SOLID;
+    };
+    uint64_t closed;
+    do {
+        closed = 0;
+        for (uint64_t idx = 0; idx < size; ++idx) {
+            if (field[idx] != FLUID)
+                continue;
+            int64_t ix, iy, iz;
+            coords(idx, ix, iy, iz);
+            if ((isSolidAt(ix + 1, iy, iz) && isSolidAt(ix - 1, iy, iz)) ||
+                (isSolidAt(ix, iy + 1, iz) && isSolidAt(ix, iy - 1, iz)) ||
+                (isSolidAt(ix, iy, iz + 1) && isSolidAt(ix, iy, iz - 1))) {
+                field[idx] = INVALID_SOLID;
+                ++closed;
+            }
+        }
+    } while (closed > 0);
+    for (uint64_t idx = 0; idx < size; ++idx)
+        if (field[idx] == INVALID_SOLID && hasNeighborOfType(idx, FLUID))
+            field[idx] = STOPPER_SOLID;
+    solidBoundaryIndex.assign(size, -1);
+    numberOfSolidBoundaryNodes = 0;
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (field[idx] == FLUID && hasNeighborOfType(idx, STOPPER_SOLID)) {
+            field[idx] = BC_SOLID;
+            solidBoundaryIndex[idx] = numberOfSolidBoundaryNodes++;
+        }
+    }
+}
+
+// Geometry::addIndices (Side.cpp:270-307).  A cuboid has no ray
+// intersection (Object::getIntersection returns an error for primitives), so
+// GridImp::findQsPrimitive leaves every q at -1 and a link gets q = 1/2 when its
+// neighbour is a stopper node.
+void LevelGrid::geometryList(std::vector<int32_t>& k, std::vector<double>& q) const
+{
+    std::vector<int64_t> nodes;
+    for (uint64_t idx = 0; idx < size; ++idx)
+        if (field[idx] == BC_SOLID)
+            nodes.push_back((int64_t)idx);
+    const size_t n = nodes.size();
+    k.assign(n, 0);
+    q.assign(27 * n, -1.0);
+    for (size_t i = 0; i < n; ++i) {
+        const uint64_t idx = (uint64_t)nodes[i];
+        k[i] = (int32_t)(sparseIndex[idx] + 1);
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        for (int d = 0; d < 27; ++d) {
+            const int64_t m = index(ix + cx(d), iy + cy(d), iz + cz(d));
+            if (m < 0)
+                continue;
+            const uint8_t t = field[(uint64_t)m];
+            if (t == STOPPER_OUT_OF_GRID_BOUNDARY || t == STOPPER_OUT_OF_GRID || t == STOPPER_SOLID)
+                q[(size_t)d * n + i] = 0.5;
+        }
+    }
+}
+
+// -------------------------------------------------------------- interface --
+// (GridInterface.cpp).  Coordinates are mapped between the levels with the
+// reference's own arithmetic: a coarse node and the fine node a quarter coarse
+// spacing above / below it.
+int64_t LevelGrid::coarseToFineIndex(uint64_t idx, const LevelGrid& fine) const
+{
+    int64_t ix, iy, iz;
+    coords(idx, ix, iy, iz);
+    return fine.coordToIndex(coordX(ix) + fine.delta * 0.5, coordY(iy) + fine.delta * 0.5, coordZ(iz) + fine.delta * 0.5);
+}
+
+int64_t LevelGrid::fineToCoarseIndex(uint64_t idx, const LevelGrid& fine) const
+{
+    int64_t ix, iy, iz;
+    coords(idx, ix, iy, iz);
+    return fine.coordToIndex(coordX(ix) - fine.delta * 0.5, coordY(iy) - fine.delta * 0.5, coordZ(iz) - fine.delta * 0.5);
+}
+
+// GridInterface::isNeighborFineInvalid (:254-271)
+bool LevelGrid::isNeighborFineInvalid(int64_t jx, int64_t jy, int64_t jz, const LevelGrid& fine) const
+{
+    const int64_t nb = index(jx, jy, jz);
+    if (nb < 0)
+        return false;
+    const uint8_t t = field[(uint64_t)nb];
+    if (t == STOPPER_OUT_OF_GRID || t == STOPPER_OUT_OF_GRID_BOUNDARY)
+        return false;
+    const int64_t f = coarseToFineIndex((uint64_t)nb, fine);
+    if (f < 0)
+        return true;
+    const uint8_t ft = fine.field[(uint64_t)f];
+    return ft == INVALID_OUT_OF_GRID || ft == STOPPER_OUT_OF_GRID;
+}
+
+// the cell starting at (x0, y0, z0) lies in the grid and holds only types a / b
+bool LevelGrid::cellContainsOnly(int64_t x0, int64_t y0, int64_t z0, uint8_t a, uint8_t b) const
+{
+    for (int c = 0; c < 8; ++c) {
+        const int64_t m = index(x0 + (c & 1), y0 + ((c >> 1) & 1), z0 + ((c >> 2) & 1));
+        if (m < 0)
+            return false;
+        const uint8_t t = field[(uint64_t)m];
+        if (t != a && t != b)
+            return false;
+    }
+    return true;
+}
+
+// GridImp::setNonStopperOutOfGridCellTo (:708-724): the cell starting at the node
+void LevelGrid::setNonStopperOutOfGridCellTo(uint64_t idx, uint8_t type)
+{
+    int64_t ix, iy, iz;
+    coords(idx, ix, iy, iz);
+    for (int c = 0; c < 8; ++c) {
+        const int64_t m = index(ix + (c & 1), iy + ((c >> 1) & 1), iz + ((c >> 2) & 1));
+        if (m < 0)
+            continue;
+        const uint8_t t = field[(uint64_t)m];
+        if (t != STOPPER_OUT_OF_GRID && t != STOPPER_OUT_OF_GRID_BOUNDARY)
+            field[(uint64_t)m] = type;
+    }
+}
+
+// GridInterface::findOffsetCF (:372-399): the node's own cell if it holds
+// only fluid / coarse-to-fine nodes, else the first neighbour cell (in
+// direction order) that does; offset = that direction
+int64_t LevelGrid::offsetCellCF(uint64_t idx, int& offset) const
+{
+    int64_t ix, iy, iz;
+    coords(idx, ix, iy, iz);
+    offset = d000;
+    if (cellContainsOnly(ix, iy, iz, FLUID, FLUID_CFC))
+        return (int64_t)idx;
+    for (int d = 0; d < 27; ++d) {
+        if (cellContainsOnly(ix + cx(d), iy + cy(d), iz + cz(d), FLUID, FLUID_CFC)) {
+            offset = d;
+            return index(ix + cx(d), iy + cy(d), iz + cz(d));
+        }
+    }
+    return (int64_t)idx;
+}
+
+// GridInterface::findOffsetFC (:401-428), on the fine level.  The neighbour
+// cells are tested for fluid / coarse-to-fine types, as the reference does.
+int64_t LevelGrid::offsetCellFC(uint64_t idx, int& offset) const
+{
+    int64_t ix, iy, iz;
+    coords(idx, ix, iy, iz);
+    offset = d000;
+    if (cellContainsOnly(ix, iy, iz, FLUID, FLUID_FCF))
+        return (int64_t)idx;
+    for (int d = 0; d < 27; ++d) {
+        if (cellContainsOnly(ix + cx(d), iy + cy(d), iz + cz(d), FLUID, FLUID_CFC)) {
+            offset = d;
+            return index(ix + cx(d), iy + cy(d), iz + cz(d));
+        }
+    }
+    return (int64_t)idx;
+}
+
+// GridImp::findGridInterface (:1204-1232): coarse-to-fine cells (fluid and
+// boundary-stopper variants, GridInterface.cpp:60-122), then fine-to-coarse
+// cells (:125-158), then the coarse nodes under the fine level (:160-196),
+// each a pass over the coarse level in matrix order.
+void LevelGrid::findGridInterface(LevelGrid& fine)
+{
+    cf = InterfaceCells();
+    fc = InterfaceCells();
+    auto addCF = [&](uint64_t idx, int64_t f) {
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        for (int d = 0; d < 27; ++d) {
+            if (isNeighborFineInvalid(ix + cx(d), iy + cy(d), iz + cz(d), fine)) {
+                int offset;
+                const int64_t c = offsetCellCF(idx, offset);
+                cf.coarse.push_back(c);
+                cf.fine.push_back(f);
+                cf.offset.push_back(offset);
+                setNonStopperOutOfGridCellTo(idx, FLUID_CFC);
+                fine.setNonStopperOutOfGridCellTo((uint64_t)f, FLUID_CFF);
+                return;
+            }
+        }
+    };
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (isFluid(idx)) {
+            const int64_t f = coarseToFineIndex(idx, fine);
+            if (f >= 0 && fine.isFluid((uint64_t)f))
+                addCF(idx, f);
+        }
+        if (field[idx] == STOPPER_OUT_OF_GRID_BOUNDARY) {
+            const int64_t f = coarseToFineIndex(idx, fine);
+            if (f >= 0 && fine.field[(uint64_t)f] == STOPPER_OUT_OF_GRID_BOUNDARY)
+                addCF(idx, f);
+        }
+    }
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (!isFluid(idx) || field[idx] == FLUID_CFC)
+            continue;
+        const int64_t f = fineToCoarseIndex(idx, fine);
+        if (f < 0 || !fine.isFluid((uint64_t)f))
+            continue;
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        for (int d = 0; d < 27; ++d) {
+            const int64_t nb = index(ix + cx(d), iy + cy(d), iz + cz(d));
+            if (nb >= 0 && field[(uint64_t)nb] == FLUID_CFC) {
+                int offset;
+                const int64_t fcell = fine.offsetCellFC((uint64_t)f, offset);
+                fc.coarse.push_back((int64_t)idx);
+                fc.fine.push_back(fcell);
+                fc.offset.push_back(offset);
+                fine.setNonStopperOutOfGridCellTo((uint64_t)f, FLUID_FCF);
+                field[idx] = FLUID_FCC;
+                break;
+            }
+        }
+    }
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (!isFluid(idx) || field[idx] == FLUID_CFC || field[idx] == FLUID_FCC)
+            continue;
+        const int64_t f = fineToCoarseIndex(idx, fine);
+        if (f < 0)
+            continue;
+        if (hasNeighborOfType(idx, FLUID_FCC)) {
+            field[idx] = STOPPER_COARSE_UNDER_FINE;
+            continue;
+        }
+        const uint8_t ft = fine.field[(uint64_t)f];
+        if (ft == INVALID_SOLID || fine.isFluid((uint64_t)f) || ft == STOPPER_SOLID || ft == BC_SOLID)
+            field[idx] = INVALID_COARSE_UNDER_FINE;
+    }
+}
+
+// GridInterface::repairGridInterfaceOnMultiGPU (:298-361): keep the
+// coarse-to-fine cells whose coarse cell holds only coarse-to-fine nodes and
+// the fine-to-coarse cells whose fine cell holds only fine-to-coarse nodes
+void LevelGrid::repairGridInterface(const LevelGrid& fine)
+{
+    InterfaceCells keepCF, keepFC;
+    for (size_t i = 0; i < cf.size(); ++i) {
+        int64_t ix, iy, iz;
+        coords((uint64_t)cf.coarse[i], ix, iy, iz);
+        if (cellContainsOnly(ix, iy, iz, FLUID_CFC, FLUID_CFC)) {
+            keepCF.coarse.push_back(cf.coarse[i]);
+            keepCF.fine.push_back(cf.fine[i]);
+            keepCF.offset.push_back(cf.offset[i]);
+        }
+    }
+    for (size_t i = 0; i < fc.size(); ++i) {
+        int64_t ix, iy, iz;
+        fine.coords((uint64_t)fc.fine[i], ix, iy, iz);
+        if (fine.cellContainsOnly(ix, iy, iz, FLUID_FCF, FLUID_FCF)) {
+            keepFC.coarse.push_back(fc.coarse[i]);
+            keepFC.fine.push_back(fc.fine[i]);
+            keepFC.offset.push_back(fc.offset[i]);
+        }
+    }
+    cf = std::move(keepCF);
+    fc = std::move(keepFC);
+}
+
+// GridInterface::findSparseIndex (:363-369): matrix to sparse indices (both
+// levels' sparse indices must be current)
+void LevelGrid::renumberGridInterface(const LevelGrid& fine)
+{
+    for (size_t i = 0; i < cf.size(); ++i) {
+        cf.coarse[i] = sparseIndex[(uint64_t)cf.coarse[i]];
+        cf.fine[i] = fine.sparseIndex[(uint64_t)cf.fine[i]];
+    }
+    for (size_t i = 0; i < fc.size(); ++i) {
+        fc.coarse[i] = sparseIndex[(uint64_t)fc.coarse[i]];
+        fc.fine[i] = fine.sparseIndex[(uint64_t)fc.fine[i]];
+    }
+}
+
 void LevelGrid::nodeValues(std::vector<double>& cxs, std::vector<double>& cys, std::vector<double>& czs,
                            std::vector<uint32_t>& nbx, std::vector<uint32_t>& nby, std::vector<uint32_t>& nbz,
                            std::vector<uint32_t>& nbneg, std::vector<uint32_t>& geo) const
@@ -340,6 +745,106 @@ void GridBuilder::addCoarseGrid(double sx, double sy, double sz, double ex, doub
     pressure.emplace_back();
 }
 
+void GridBuilder::setNumberOfLayers(uint32_t fine, uint32_t betweenLevels)
+{
+    layersFine = fine;
+    layersBetweenLevels = betweenLevels;
+}
+
+// MultipleGridBuilder::getStaggeredCoordinates (MultipleGridBuilder.cpp:228-356),
+// step for step in the same floating-point operations: the box widened by
+// the overlap of this level, snapped to the parent's nodes, staggered by a
+// quarter parent spacing, grown by one parent spacing until it covers the
+// box, and pulled back inside the parent (odd start) where it sticks out.
+std::array<double, 6> GridBuilder::staggeredCoordinates(const Box& shape, int level, int levelFine, bool odd[3]) const
+{
+    const LevelGrid& parent = *grids[(size_t)level - 1];
+    const double deltaCoarse = parent.delta;
+    const double delta = 0.5 * deltaCoarse;
+    double lo[3] = { std::fmin(shape.minX, shape.maxX), std::fmin(shape.minY, shape.maxY),
+                     std::fmin(shape.minZ, shape.maxZ) };
+    double hi[3] = { std::fmax(shape.minX, shape.maxX), std::fmax(shape.minY, shape.maxY),
+                     std::fmax(shape.minZ, shape.maxZ) };
+    if (levelFine >= level) {
+        double overlap = 0.0;
+        if (level != levelFine) {
+            overlap += (double)(layersBetweenLevels + 1) * delta;
+            overlap *= 2.0 * (1.0 - std::pow(0.5, (double)(unsigned)(levelFine - level)));
+        }
+        overlap += (double)layersFine * delta * std::pow(0.5, (double)(unsigned)(levelFine - level));
+        for (int a = 0; a < 3; ++a) {
+            lo[a] -= overlap;
+            hi[a] += overlap;
+        }
+    }
+    const double pStart[3] = { parent.startX, parent.startY, parent.startZ };
+    const double pEnd[3] = { parent.endX, parent.endY, parent.endZ };
+    std::array<double, 6> c { pStart[0], pStart[1], pStart[2], pEnd[0], pEnd[1], pEnd[2] };
+    for (int a = 0; a < 3; ++a)
+        while (c[a] < lo[a])
+            c[a] += deltaCoarse;
+    for (int a = 0; a < 3; ++a)
+        while (c[3 + a] > hi[a])
+            c[3 + a] -= deltaCoarse;
+    for (int a = 0; a < 3; ++a) {
+        c[a] -= 0.25 * deltaCoarse;
+        c[3 + a] += 0.25 * deltaCoarse;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (c[a] > lo[a])
+            c[a] -= deltaCoarse;
+    for (int a = 0; a < 3; ++a)
+        if (c[3 + a] < hi[a])
+            c[3 + a] += deltaCoarse;
+    for (int a = 0; a < 3; ++a)
+        odd[a] = c[a] < pStart[a];
+    for (int a = 0; a < 3; ++a)
+        while (c[a] < pStart[a])
+            c[a] += delta;
+    for (int a = 0; a < 3; ++a)
+        while (c[3 + a] > pEnd[a])
+            c[3 + a] -= delta;
+    return c;
+}
+
+void GridBuilder::addGrid(const Box& box, int levelFine)
+{
+    if (grids.empty())
+        throw std::runtime_error("addGrid: add the coarse grid first");
+    if (built)
+        throw std::runtime_error("addGrid after buildGrids");
+    if (levelFine < (int)grids.size())
+        throw std::runtime_error("addGrid: level already exists");
+    for (int level = (int)grids.size(); level <= levelFine; ++level) {
+        bool odd[3];
+        const std::array<double, 6> c = staggeredCoordinates(box, level, levelFine, odd);
+        double delta = grids[0]->delta; // MultipleGridBuilder::calculateDelta
+        for (int i = 0; i < level; ++i)
+            delta *= 0.5;
+        auto* g = new LevelGrid(c[0], c[1], c[2], c[3], c[4], c[5], delta, level);
+        for (int a = 0; a < 3; ++a) {
+            g->oddStart[a] = odd[a];
+            g->periodic[a] = false;
+        }
+        g->hasShape = true;
+        g->shape = box;
+        g->innerFromFiner = level != levelFine;
+        g->numberOfLayers = level != levelFine ? layersBetweenLevels : layersFine;
+        grids.emplace_back(g);
+        velocity.emplace_back();
+        slip.emplace_back();
+        pressure.emplace_back();
+    }
+}
+
+void GridBuilder::addGeometry(const Box& s)
+{
+    if (built)
+        throw std::runtime_error("addGeometry after buildGrids");
+    hasSolid = true;
+    solid = s;
+}
+
 void GridBuilder::setPeriodicBoundaryCondition(bool px, bool py, bool pz)
 {
     for (auto& g : grids) {
@@ -349,19 +854,41 @@ void GridBuilder::setPeriodicBoundaryCondition(bool px, bool py, bool pz)
     }
 }
 
-void GridBuilder::buildGrids(bool)
+// MultipleGridBuilder::buildGrids (MultipleGridBuilder.cpp:469-597): levels
+// initialised from the finest to the coarsest, the solid on the finest
+// level, the interfaces between neighbouring levels, their repair, then the
+// sparse renumbering (interface cells included).
+void GridBuilder::buildGrids(bool enableThinWalls)
 {
     if (grids.empty())
         throw std::runtime_error("buildGrids: no coarse grid");
-    for (int level = (int)grids.size() - 1; level >= 0; --level) {
-        grids[level]->initialNodes();
-        grids[level]->findStoppers();
-    }
-    for (auto& g : grids) {
-        g->findSparseIndices();
+    if (enableThinWalls && hasSolid)
+        throw std::runtime_error("thin-wall treatment of solids is not supported");
+    const int L = (int)grids.size();
+    for (int level = L - 1; level >= 0; --level)
+        grids[level]->initial(level + 1 < L ? grids[level + 1].get() : nullptr);
+    if (hasSolid)
+        grids[L - 1]->meshSolid(solid);
+    for (int level = 0; level + 1 < L; ++level)
+        grids[level]->findGridInterface(*grids[level + 1]);
+    for (int level = 0; level + 1 < L; ++level)
+        grids[level]->repairGridInterface(*grids[level + 1]);
+    for (int level = 0; level < L; ++level)
+        grids[level]->findSparseIndices();
+    for (int level = 0; level + 1 < L; ++level)
+        grids[level]->renumberGridInterface(*grids[level + 1]);
+    for (auto& g : grids)
         g->findFluidNodes();
-    }
     built = true;
+}
+
+void GridBuilder::setNoSlipGeometryBoundaryCondition()
+{
+    if (!built)
+        throw std::runtime_error("boundary conditions need buildGrids first");
+    if (!hasSolid)
+        throw std::runtime_error("no geometry was added");
+    geometryNoSlip = true;
 }
 
 static void addSide(std::vector<std::unique_ptr<LevelGrid>>& grids, std::vector<std::vector<BCList>>& lists,

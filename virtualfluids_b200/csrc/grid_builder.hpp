@@ -51,6 +51,18 @@ enum class BCKind { NoSlip = 1, Velocity = 2, Pressure = 3, Slip = 4 };
 
 struct Box {
     double minX, minY, minZ, maxX, maxY, maxZ;
+    // Cuboid::isPointInObject (Cuboid.cpp): strictly inside, with the
+    // reference's relative comparison tolerance (FLT_EPSILON)
+    bool containsPoint(double x, double y, double z) const;
+};
+
+// interface cells between a level and the next finer one
+// (GridInterface::cf / fc): matrix indices until the sparse renumbering,
+// sparse indices after it; offset = index of the D3Q27 direction
+struct InterfaceCells {
+    std::vector<int64_t> coarse, fine;
+    std::vector<int> offset;
+    size_t size() const { return coarse.size(); }
 };
 
 // One compacted boundary-condition list of one level, in the GPU layout of
@@ -76,10 +88,21 @@ public:
               int level);
 
     // --- construction (mirrors GridImp::inital / findSparseIndices) ------
-    void initialNodes();
-    void findStoppers();
+    // node types of the level: inner region (from the refinement box, or
+    // from the finer level for intermediate levels), overlap layers, odd
+    // cells completed, end-of-grid stoppers
+    void initial(const LevelGrid* finer);
     void findSparseIndices();
     void findFluidNodes();
+    // solid cuboid on this level (GridImp::mesh + findQsPrimitive for a
+    // geometric primitive): inside nodes removed, one stopper layer inside the
+    // solid, one BC_SOLID layer outside it
+    void meshSolid(const Box& solid);
+    // interface cells to the next finer level (GridImp::findGridInterface,
+    // repairGridInterfaceOnMultiGPU) and their sparse renumbering
+    void findGridInterface(LevelGrid& fine);
+    void repairGridInterface(const LevelGrid& fine);
+    void renumberGridInterface(const LevelGrid& fine);
 
     // --- accessors --------------------------------------------------------
     uint32_t nx, ny, nz;
@@ -87,6 +110,14 @@ public:
     double startX, startY, startZ, endX, endY, endZ, delta;
     int level;
     bool periodic[3] = { false, false, false };
+    bool oddStart[3] = { false, false, false };
+    uint32_t numberOfLayers = 0;    // overlap layers around the inner region
+    bool innerFromFiner = false;    // intermediate level: inner region from the finer level
+    bool hasShape = false;          // level > 0: the refinement box
+    Box shape {};
+    std::vector<int64_t> solidBoundaryIndex; // BC_SOLID nodes in matrix order, -1 elsewhere
+    uint32_t numberOfSolidBoundaryNodes = 0;
+    InterfaceCells cf, fc;          // to the next finer level
 
     std::vector<uint8_t> field;
     std::vector<int64_t> sparseIndex;       // -1 for removed nodes
@@ -112,6 +143,13 @@ public:
         iy = (int64_t)((idx / nx) % ny);
         iz = (int64_t)((idx / nx) / ny % nz);
     }
+    // coordinates of a matrix index and the matrix index of a coordinate
+    // (GridImp::transIndexToCoords / transCoordToIndex: rounded to the
+    // nearest node, -1 outside the grid)
+    double coordX(int64_t ix) const { return (double)ix * delta + startX; }
+    double coordY(int64_t iy) const { return (double)iy * delta + startY; }
+    double coordZ(int64_t iz) const { return (double)iz * delta + startZ; }
+    int64_t coordToIndex(double x, double y, double z) const;
     bool isFluid(uint64_t idx) const;
     bool isStopper(uint64_t idx) const;
     bool isStopperForBC(int64_t idx) const;
@@ -120,7 +158,23 @@ public:
     // q values of a node on a domain side (Side::setQs)
     void sideQs(SideType side, int64_t ix, int64_t iy, int64_t iz, double* qNode) const;
 
+    // geometry boundary list of this level (Geometry::addIndices): BC_SOLID
+    // nodes in matrix order, q = 1/2 towards stopper nodes, -1 otherwise
+    void geometryList(std::vector<int32_t>& k, std::vector<double>& q) const;
+
 private:
+    void findInnerNodes();
+    void setInnerBasedOnFinerGrid(const LevelGrid& fine);
+    void addOverlap();
+    void findStoppers();
+    int64_t oddCellStart(int64_t i, int axis) const;
+    bool cellContainsOnly(int64_t x0, int64_t y0, int64_t z0, uint8_t a, uint8_t b) const;
+    void setNonStopperOutOfGridCellTo(uint64_t idx, uint8_t type);
+    int64_t coarseToFineIndex(uint64_t idx, const LevelGrid& fine) const;
+    int64_t fineToCoarseIndex(uint64_t idx, const LevelGrid& fine) const;
+    bool isNeighborFineInvalid(int64_t ix, int64_t iy, int64_t iz, const LevelGrid& fine) const;
+    int64_t offsetCellCF(uint64_t idx, int& offset) const;
+    int64_t offsetCellFC(uint64_t idx, int& offset) const;
     int64_t neighborIndexPositive(int64_t ix, int64_t iy, int64_t iz, int axis) const;
     int64_t negativeNeighborIndex(int64_t ix, int64_t iy, int64_t iz) const;
     int64_t firstFluidAlong(int64_t ix, int64_t iy, int64_t iz, int axis) const;
@@ -134,6 +188,13 @@ class GridBuilder
 public:
     void addCoarseGrid(double startX, double startY, double startZ, double endX, double endY, double endZ,
                        double delta);
+    // refinement box up to level levelFine (MultipleGridBuilder::addGrid):
+    // one grid per missing level, staggered on its parent, with the overlap
+    // layers of setNumberOfLayers
+    void addGrid(const Box& box, int levelFine);
+    void setNumberOfLayers(uint32_t fine, uint32_t betweenLevels);
+    // solid cuboid, meshed on the finest level (MultipleGridBuilder::addGeometry)
+    void addGeometry(const Box& solid);
     void setPeriodicBoundaryCondition(bool px, bool py, bool pz);
     void buildGrids(bool enableThinWalls = false);
 
@@ -141,6 +202,8 @@ public:
     void setVelocityBoundaryCondition(SideType side, double vx, double vy, double vz);
     void setPressureBoundaryCondition(SideType side, double rho);
     void setSlipBoundaryCondition(SideType side, double normalX, double normalY, double normalZ);
+    // no-slip on the solid geometry's BC_SOLID nodes, every level
+    void setNoSlipGeometryBoundaryCondition();
 
     int numberOfLevels() const { return (int)grids.size(); }
     LevelGrid& grid(int level) { return *grids.at(level); }
@@ -151,10 +214,16 @@ public:
     const std::vector<BCList>& velocityBCs(int level) const { return velocity.at(level); }
     const std::vector<BCList>& slipBCs(int level) const { return slip.at(level); }
     const std::vector<BCList>& pressureBCs(int level) const { return pressure.at(level); }
+    bool hasGeometryBC() const { return geometryNoSlip; }
 
 private:
+    std::array<double, 6> staggeredCoordinates(const Box& shape, int level, int levelFine, bool odd[3]) const;
     std::vector<std::unique_ptr<LevelGrid>> grids;
     std::vector<std::vector<BCList>> velocity, slip, pressure;
+    uint32_t layersFine = 12, layersBetweenLevels = 8; // MultipleGridBuilder.cpp:53
+    bool hasSolid = false;
+    Box solid {};
+    bool geometryNoSlip = false;
     bool built = false;
 };
 

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "capi_common.cuh"
+#include "d3q27.cuh"
 #include "grid_builder.hpp"
 
 namespace
@@ -115,8 +116,12 @@ void exportAll(GridHandle& h)
         E.put("fluid", g.fluidNodes);
         concatenate(b.velocityBCs(level), E, "velocity", true, false);
         concatenate(b.slipBCs(level), E, "slip", false, true);
-        E.put("geometry.k", std::vector<int32_t>());
-        E.put("geometry.q", std::vector<double>());
+        std::vector<int32_t> gk;
+        std::vector<double> gq;
+        if (b.hasGeometryBC())
+            g.geometryList(gk, gq);
+        E.put("geometry.k", gk);
+        E.put("geometry.q", gq);
         const auto& pres = b.pressureBCs(level);
         E.put("pressure.count", std::vector<int32_t> { (int32_t)pres.size() });
         for (size_t i = 0; i < pres.size(); ++i) {
@@ -127,6 +132,29 @@ void exportAll(GridHandle& h)
             E.put(p + ".q", pres[i].q);
             E.put(p + ".dir", std::vector<int32_t> { pres[i].d3q27Direction });
         }
+        if (level + 1 < b.numberOfLevels()) {
+            // LevelGridBuilder::getGridInterfaceIndices (+1 shifted sparse
+            // indices) and getOffsetCF / getOffsetFC (the negated offset
+            // direction, LevelGridBuilder.cpp:400-422)
+            for (const char* tag : { "cf", "fc" }) {
+                const InterfaceCells& ic = tag[0] == 'c' ? g.cf : g.fc;
+                std::vector<uint32_t> c(ic.size()), f(ic.size());
+                std::vector<double> ox(ic.size()), oy(ic.size()), oz(ic.size());
+                for (size_t i = 0; i < ic.size(); ++i) {
+                    c[i] = (uint32_t)(ic.coarse[i] + 1);
+                    f[i] = (uint32_t)(ic.fine[i] + 1);
+                    ox[i] = -(double)vfb::cx(ic.offset[i]);
+                    oy[i] = -(double)vfb::cy(ic.offset[i]);
+                    oz[i] = -(double)vfb::cz(ic.offset[i]);
+                }
+                const std::string t(tag);
+                E.put(t + ".coarse", c);
+                E.put(t + ".fine", f);
+                E.put(t + ".offX", ox);
+                E.put(t + ".offY", oy);
+                E.put(t + ".offZ", oz);
+            }
+        }
     }
 }
 } // namespace
@@ -135,10 +163,13 @@ extern "C" {
 
 /*
  * spec: [0..6] coarse grid start x,y,z, end x,y,z, delta; [7..9] periodic;
- * [10] refinement boxes (0 only in this build); [17..18] layers; [19] solid
- * cuboid present (0 only); [30..59] six side BCs (side, type, v0, v1, v2) in
- * the order they are set; [60] enableThinWalls.  Same layout as the grid
- * oracle.  Returns NULL on error (see vfb_last_error).
+ * [10] refinement box present, [11..16] the box (min x,y,z, max x,y,z);
+ * [17..18] layers fine / between levels (used when [17] > 0); [19] solid
+ * cuboid present, [20..25] its extent; [26..29] geometry BC (type 1 =
+ * no-slip); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
+ * are set; [60] enableThinWalls; [61] finest level of the refinement box
+ * (0 = 1; n >= 62 values).  Same layout as the grid oracle.  Returns NULL on
+ * error (see vfb_last_error).
  */
 void* vfb_grid_build(const double* s, int n)
 {
@@ -149,14 +180,25 @@ void* vfb_grid_build(const double* s, int n)
     }
     auto* h = new GridHandle;
     try {
-        if (s[10] > 0 || s[19] > 0)
-            throw std::invalid_argument("refinement boxes and solid geometry are not supported by this call");
         h->builder.addCoarseGrid(s[0], s[1], s[2], s[3], s[4], s[5], s[6]);
+        if (s[17] > 0)
+            h->builder.setNumberOfLayers((uint32_t)s[17], (uint32_t)s[18]);
+        if (s[10] > 0) {
+            const int levelFine = (n > 61 && s[61] > 0) ? (int)s[61] : 1;
+            h->builder.addGrid(Box { s[11], s[12], s[13], s[14], s[15], s[16] }, levelFine);
+        }
+        if (s[19] > 0)
+            h->builder.addGeometry(Box { s[20], s[21], s[22], s[23], s[24], s[25] });
         h->builder.setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);
         h->builder.buildGrids(s[60] > 0);
         for (int i = 0; i < 6; ++i) {
             const double* b = s + 30 + 5 * i;
             applyBC(h->builder, (int)b[0], (int)b[1], b[2], b[3], b[4]);
+        }
+        if (s[19] > 0 && (int)s[26] != 0) {
+            if ((int)s[26] != 1)
+                throw std::invalid_argument("only a no-slip boundary condition is supported on the geometry");
+            h->builder.setNoSlipGeometryBoundaryCondition();
         }
         for (int level = 0; level < h->builder.numberOfLevels(); ++level)
             h->builder.grid(level).findFluidNodes();

@@ -73,11 +73,14 @@ class MultipleGridBuilder:
         self._coarse = True
 
     def addGrid(self, box, level: int = 1):
-        """Refinement box (minX, minY, minZ, maxX, maxY, maxZ) on level 1."""
-        if level != 1:
-            raise ValueError("only one refinement level is supported")
+        """Refinement box (minX, minY, minZ, maxX, maxY, maxZ) refined down to
+        `level` (MultipleGridBuilder::addGrid(gridShape, levelFine)): one grid
+        per level from the current finest + 1 to `level`."""
+        if level < 1:
+            raise ValueError("the refinement level must be at least 1")
         self.spec[10] = 1
         self.spec[11:17] = box
+        self.spec[61] = level
 
     def setNumberOfLayers(self, fine: int, between: int):
         self.spec[17:19] = [fine, between]
