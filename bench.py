@@ -476,6 +476,82 @@ def cavity_report(args):
     return 0
 
 
+def cube_report(args):
+    """The wall-mounted cube in a channel, two levels (coarse 256 x 96 x 96,
+    refined box x 48..128, y 24..72, z 0..40, cube of side 16 on the floor at
+    x = 64, inlet 0.04 with +-1% seeded noise, pressure outlet, slip top,
+    periodic span, nu = 0.04 * 16 / 2000 on the coarse level), grid built by
+    the library's builder, stepped by the C++ schedule with graph replay.
+    Per storage: NUPS as the reference counts them (steps x sum over levels
+    of nodes x 2^level / s, PerformanceMeasurement.cpp:43,63) and fluid-node
+    updates per second; for FP32 / FP16 / BF16 the L2 velocity error and the
+    kinetic-energy error against the FP64 run after --steps coarse steps
+    (both levels).  One JSON line."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200.simulation import (BoundaryConditionFactory, NoSlipBC, Parameter, PressureBC, SlipBC,
+                                               Simulation)
+    from virtualfluids_b200.workloads import wall_mounted_cube
+
+    t0 = time.time()
+    levels = wall_mounted_cube()
+    build_s = time.time() - t0
+    nu = 0.04 * 16 / 2000
+    nodes = [len(g["geo"]) for g in levels]
+    fluid = [len(g["fluid"]) for g in levels]
+    per_step_nodes = sum(n * 2 ** lvl for lvl, n in enumerate(nodes))
+    per_step_fluid = sum(n * 2 ** lvl for lvl, n in enumerate(fluid))
+    rows, ref = {}, None
+    for storage in ("fp64", "fp32", "fp16", "bf16"):
+        p = Parameter()
+        p.set_storage(storage)
+        p.set_viscosity_LB(nu)
+        bc = BoundaryConditionFactory()
+        bc.set_slip_boundary_condition(SlipBC.SlipCompressible)
+        bc.set_geometry_boundary_condition(NoSlipBC.NoSlipInterpolatedCompressible)
+        bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+        sim = Simulation(p, levels, bc)
+        for lvl, g in enumerate(levels):
+            zero = np.zeros(len(g["geo"]))
+            sim.init_level(lvl, zero, zero, zero, zero)
+        sim.run(4)  # warm-up: graph capture of the two-step pattern
+        for lvl, g in enumerate(levels):
+            zero = np.zeros(len(g["geo"]))
+            sim.init_level(lvl, zero, zero, zero, zero)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        sim.run(args.steps)
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        fields = []
+        for lvl, g in enumerate(levels):
+            fl = g["fluid"]
+            _, vx, vy, vz = [a[fl].astype(np.float64) for a in sim.macroscopic(lvl)]
+            fields.append((vx, vy, vz, sim.kinetic_energy(lvl)[0], int(sim.mass_and_energy(lvl)[2])))
+        sim.close()
+        row = {"nups": per_step_nodes * args.steps / (ms * 1e-3), "fluid_updates_per_s": per_step_fluid * args.steps /
+               (ms * 1e-3), "ms_per_coarse_step": ms / args.steps, "nonfinite": sum(f[4] for f in fields),
+               "kinetic_energy": [f[3] for f in fields]}
+        if ref is None:
+            ref = fields
+        else:
+            num = sum(np.sum((f[0] - r[0]) ** 2 + (f[1] - r[1]) ** 2 + (f[2] - r[2]) ** 2) for f, r in zip(fields, ref))
+            den = sum(np.sum(r[0] ** 2 + r[1] ** 2 + r[2] ** 2) for r in ref)
+            row["l2_velocity_error_vs_fp64"] = float(np.sqrt(num / den))
+            row["kinetic_energy_error_vs_fp64"] = [abs(f[3] - r[3]) / abs(r[3]) for f, r in zip(fields, ref)]
+        rows[storage] = row
+    for s16 in ("fp16", "bf16"):
+        rows[f"{s16}_over_fp32_nups"] = rows[s16]["nups"] / rows["fp32"]["nups"]
+    print(json.dumps({"report": "wall-mounted cube, two levels", "workload":
+                      "cube channel 256x96x96 + refined box 48..128 x 24..72 x 0..40, cube 16 at x=64, K17",
+                      "nodes_per_level": nodes, "fluid_nodes_per_level": fluid, "grid_build_s": build_s,
+                      "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
+    return 0
+
+
 def kernel_report(args):
     """Achieved bandwidth of the other kernels of the step, event-timed, with
     their algorithmic bytes per unit (s = bytes per stored population):
@@ -617,6 +693,8 @@ def main(argv=None):
                     help="bandwidth of the BGK, BC and interface kernels (not a bench line)")
     ap.add_argument("--cavity-report", action="store_true",
                     help="lid-driven cavity 64^3 FP64: graph replay vs direct launches (not a bench line)")
+    ap.add_argument("--cube-report", action="store_true",
+                    help="wall-mounted cube on two levels: NUPS per storage and errors against FP64 (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",
                     help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
     args = ap.parse_args(argv)
@@ -626,6 +704,8 @@ def main(argv=None):
         return precision_report(args)
     if args.cavity_report:
         return cavity_report(args)
+    if args.cube_report:
+        return cube_report(args)
     if args.kernel_report:
         return kernel_report(args)
     world, rank, local = init_distributed()

@@ -6,6 +6,7 @@ it), so every case gets a fresh process and a crash of the reference skips
 the case instead of ending the test run.
 
     python tests/grid_compare_case.py <seed>   ->  prints "ok", "diff ..." or "mine failed ..."
+    (seed -1: the full-size wall-mounted cube benchmark grid)
 """
 from __future__ import annotations
 
@@ -53,8 +54,26 @@ def random_spec(seed: int) -> np.ndarray:
     return s
 
 
+def cube_benchmark_spec() -> np.ndarray:
+    """The wall-mounted cube benchmark at full size: coarse 256 x 96 x 96,
+    refined box x 48..128, y 24..72, z 0..40, cube of side 16 on the floor at
+    x = 64 centred in y, inlet velocity, pressure outlet, no-slip floor, slip
+    top, periodic span, no-slip geometry."""
+    s = np.zeros(64)
+    s[0:7] = [0, 0, 0, 255, 95, 95, 1.0]
+    s[8] = 1
+    s[10] = 1
+    s[11:17] = [48, 24, 0, 128, 72, 40]
+    s[19] = 1
+    s[20:26] = [64, 40, 0, 80, 56, 16]
+    s[26] = 1
+    for i, b in enumerate([(0, 2, 0.04, 0, 0), (1, 3, 0.0, 0, 0), (4, 1, 0, 0, 0), (5, 4, 0, 0, 1)]):
+        s[30 + 5 * i: 35 + 5 * i] = b
+    return s
+
+
 def main(seed: int) -> int:
-    s = random_spec(seed)
+    s = cube_benchmark_spec() if seed < 0 else random_spec(seed)
     ref = Reference("f64").grid(s)
     ref = [ref[lvl] for lvl in sorted(ref)]
     try:

@@ -122,3 +122,15 @@ def test_random_multilevel_grids_match_reference():
         assert out.startswith("ok"), f"seed {seed}: {out}"
         compared += 1
     assert compared >= 7
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+def test_full_size_cube_benchmark_grid_matches_reference():
+    """The wall-mounted cube benchmark grid at full size (2.2 M + 2.0 M
+    nodes, 18,689 coarse-to-fine and 17,140 fine-to-coarse cells, 5,380 cube
+    BC nodes) is the reference builder's, array for array (child process)."""
+    r = subprocess.run([sys.executable, str(Path(__file__).parent / "grid_compare_case.py"), "-1"],
+                       capture_output=True, text=True, timeout=600)
+    if r.returncode < 0:
+        pytest.skip(f"the reference's builder crashed (signal {-r.returncode})")
+    assert r.stdout.strip().splitlines()[-1].startswith("ok"), r.stdout[-500:] + r.stderr[-500:]

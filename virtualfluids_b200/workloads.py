@@ -89,3 +89,36 @@ def interface_planes(ncg: int = 128, nfg: int = 256, cf_planes=(40, 41), fc_plan
         ff = [flf[2 * ii + nfg * (2 * jj + nfg * 2 * kk)] for kk in planes]
         cells[tag] = (np.concatenate(cc).astype(np.uint32), np.concatenate(ff).astype(np.uint32))
     return gc, gf, cells
+
+
+def wall_mounted_cube(seed: int = 1234, coarse=(256, 96, 96), box=(48, 24, 0, 128, 72, 40), cube_x: int = 64,
+                      cube_side: int = 16, inlet: float = 0.04, noise: float = 0.01) -> list[dict]:
+    """The wall-mounted cube in a channel on two levels, built by the
+    library's grid builder: coarse grid nx x ny x nz (spacing 1), a refined
+    box (level 1), a solid cube of side `cube_side` on the floor at x =
+    cube_x centred in y with interpolated no-slip faces, velocity inlet
+    `inlet` with seeded +-`noise` relative noise per node, non-equilibrium
+    pressure outlet (drho = 0), no-slip floor, slip top, periodic span.
+    Returns the per-level array dicts (the inlet noise applied), ready for
+    Simulation."""
+    from .grid import MultipleGridBuilder, SideType
+    nx, ny, nz = coarse
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, nx - 1, ny - 1, nz - 1, 1.0)
+    b.addGrid(box, 1)
+    y0 = ny / 2 - cube_side / 2
+    b.addGeometry((cube_x, y0, 0, cube_x + cube_side, y0 + cube_side, cube_side))
+    b.setPeriodicBoundaryCondition(False, True, False)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(SideType.MX, inlet, 0.0, 0.0)
+    b.setPressureBoundaryCondition(SideType.PX, 0.0)
+    b.setNoSlipBoundaryCondition(SideType.MZ)
+    b.setSlipBoundaryCondition(SideType.PZ, 0.0, 0.0, 1.0)
+    b.setNoSlipBoundaryCondition(SideType.GEOMETRY)
+    levels = b.arrays()
+    rng = np.random.default_rng(seed)
+    for g in levels:
+        vx = g["velocity.vx"]
+        inflow = vx != 0
+        vx[inflow] = vx[inflow] * (1.0 + rng.uniform(-noise, noise, int(inflow.sum())))
+    return levels
