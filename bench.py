@@ -541,7 +541,8 @@ def cube_report(args):
             num = sum(np.sum((f[0] - r[0]) ** 2 + (f[1] - r[1]) ** 2 + (f[2] - r[2]) ** 2) for f, r in zip(fields, ref))
             den = sum(np.sum(r[0] ** 2 + r[1] ** 2 + r[2] ** 2) for r in ref)
             row["l2_velocity_error_vs_fp64"] = float(np.sqrt(num / den))
-            row["kinetic_energy_error_vs_fp64"] = [abs(f[3] - r[3]) / abs(r[3]) for f, r in zip(fields, ref)]
+            row["kinetic_energy_error_vs_fp64"] = [abs(f[3] - r[3]) / abs(r[3]) if r[3] != 0 else None
+                                                   for f, r in zip(fields, ref)]
         rows[storage] = row
     for s16 in ("fp16", "bf16"):
         rows[f"{s16}_over_fp32_nups"] = rows[s16]["nups"] / rows["fp32"]["nups"]
