@@ -260,16 +260,25 @@ int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t numberOfCells, co
  * arrays the kernels consume, bit for bit those of the reference's
  * MultipleGridBuilder / LevelGridBuilder (src/gpu/GridGenerator/grid/GridBuilder/
  * MultipleGridBuilder.cpp, LevelGridBuilder.cpp:395-944, GridImp.cpp:914-1121,
- * Side.cpp:64-215).  spec (at least 61 values): [0..6] coarse grid start x, y,
- * z, end x, y, z, delta (MultipleGridBuilder::addCoarseGrid); [7..9] periodic
- * x, y, z (setPeriodicBoundaryCondition); [10] number of refinement boxes (0);
- * [17..18] layers; [19] solid cuboid present (0); [30..59] up to six side BCs
- * as (side 0..5 = MX PX MY PY MZ PZ, type 1 no-slip / 2 velocity / 3 pressure /
- * 4 slip, three values) applied in order (setNoSlip / setVelocity / setPressure
- * / setSlipBoundaryCondition); [60] enableThinWalls.  Returns a handle, NULL on
- * error.  Array names per level: "geo", "neighborX/Y/Z", "neighborNeg",
- * "coordX/Y/Z", "fluid", "dims", "velocity.k/.q/.vx/.vy/.vz", "slip.k/.q/.nx/
- * .ny/.nz", "geometry.k/.q", "pressure.count" and "pressure<i>.k/.kN/.rho/.q/.dir".
+ * Side.cpp:64-215, GridInterface.cpp:60-428).  spec (at least 61 values):
+ * [0..6] coarse grid start x, y, z, end x, y, z, delta
+ * (MultipleGridBuilder::addCoarseGrid); [7..9] periodic x, y, z
+ * (setPeriodicBoundaryCondition); [10] refinement box present, [11..16] the box
+ * (min x, y, z, max x, y, z; MultipleGridBuilder::addGrid with a Cuboid);
+ * [17..18] layers fine / between levels (setNumberOfLayers, used when [17] > 0);
+ * [19] solid cuboid present, [20..25] its extent (addGeometry, meshed on the
+ * finest level); [26] geometry BC (1 = no-slip, setNoSlipBoundaryCondition
+ * (GEOMETRY)); [30..59] up to six side BCs as (side 0..5 = MX PX MY PY MZ PZ,
+ * type 1 no-slip / 2 velocity / 3 pressure / 4 slip, three values) applied in
+ * order (setNoSlip / setVelocity / setPressure / setSlipBoundaryCondition);
+ * [60] enableThinWalls (not with a solid); [61] finest level of the box (0 =
+ * 1; needs n >= 62).  Returns a handle, NULL on error.  Array names per level:
+ * "geo", "neighborX/Y/Z", "neighborNeg", "coordX/Y/Z", "fluid", "dims",
+ * "velocity.k/.q/.vx/.vy/.vz", "slip.k/.q/.nx/.ny/.nz", "geometry.k/.q",
+ * "pressure.count", "pressure<i>.k/.kN/.rho/.q/.dir" and, on every level but the
+ * finest, the interface cells to the next level: "cf.coarse/.fine/.offX/.offY/
+ * .offZ" and "fc.coarse/.fine/.offX/.offY/.offZ" (getGridInterfaceIndices,
+ * getOffsetCF / getOffsetFC).
  */
 void* vfb_grid_build(const double* spec, int n);
 int vfb_grid_levels(void* grid);
