@@ -55,6 +55,9 @@ struct K17Rates {
     R minusThreeOmega;                // -3 * omega
     R secondOrderCorrection;          // 3 * (1 + 1/2 * (-omega))
     R qlP, qlM, qlD;                  // quartic limiters
+    // per-launch factors of the fourth-order terms (:452-457):
+    // minusTau * 2/3 * factorA, minusTau * (-3 omega) * 1/3 * factorB
+    R fourthA, fourthB;
 };
 
 template <class R>
@@ -79,6 +82,8 @@ inline K17Rates<R> makeK17Rates(R omega, R qlP, R qlM, R qlD)
     r.qlP = qlP;
     r.qlM = qlM;
     r.qlD = qlD;
+    r.fourthA = r.minusTau * cst<R>(2, 3) * r.factorA;
+    r.fourthB = r.minusTau * r.minusThreeOmega * cst<R>(1, 3) * r.factorB;
     return r;
 }
 
@@ -142,10 +147,11 @@ __host__ __device__ __forceinline__ void bwd(R& a, R& b, R& c, const Sweep<R>& w
     const R aK = K != 0 ? a + R(K) : a;
     const R hc = R(0.5) * c;
     const R na = fma(aK, w.hm, fma(b, w.vvm, hc));
-    const R nb = fma(w.nv2, aK, fma(w.n2vv, b, a - c));
-    c = fma(aK, w.hp, fma(b, w.vvp, hc));
+    // hp - hm = v and vvp - vvm = 1; the three populations sum to a
+    const R nc = na + fma(aK, w.vv, b);
+    b = (a - na) - nc;
     a = na;
-    b = nb;
+    c = nc;
 }
 
 // --------------------------------------------------------- macroscopic sums --
@@ -182,23 +188,33 @@ __host__ __device__ __forceinline__ R pyramidJz(const R* f)
 }
 
 // ------------------------------------------------------------------- K17 --
-// sixth-order correction term of K17CompressibleNavierStokes.h:320-330 / :489-500
+// sixth-order correction term of K17CompressibleNavierStokes.h:320-330 / :489-500,
+// regrouped as (A + B / rho) / rho: A collects the terms over rho, B those
+// over rho^2 (the same terms, fused multiply-adds)
 template <class R>
 __host__ __device__ __forceinline__ R c222Term(R m111, R m200, R m020, R m002, R m022, R m202, R m220, R m011, R m101, R m110,
                                       R m211, R m121, R m112, R m120, R m102, R m210, R m012, R m201, R m021,
                                       R oneOverRho, R drho)
 {
-    return (-R(4) * m111 * m111 - (m200 * m022 + m020 * m202 + m002 * m220) -
-            R(4) * (m011 * m211 + m101 * m121 + m110 * m112) - R(2) * (m120 * m102 + m210 * m012 + m201 * m021)) *
-               oneOverRho +
-           (R(4) * (m101 * m101 * m020 + m011 * m011 * m200 + m110 * m110 * m002) + R(2) * (m200 * m020 * m002) +
-            R(16) * m110 * m101 * m011) *
-               oneOverRho * oneOverRho -
-           cst<R>(1, 3) * (m022 + m202 + m220) * oneOverRho - cst<R>(1, 9) * (m200 + m020 + m002) * oneOverRho +
-           (R(2) * (m101 * m101 + m011 * m011 + m110 * m110) + (m002 * m020 + m002 * m200 + m020 * m200) +
-            cst<R>(1, 3) * (m002 + m020 + m200)) *
-               oneOverRho * oneOverRho * (cst<R>(2, 3)) +
-           cst<R>(1, 27) * ((drho * drho - drho) * oneOverRho * oneOverRho);
+    const R s2 = m200 + m020 + m002;
+    const R a1 = fma(m002, m220, fma(m020, m202, m200 * m022));
+    const R a2 = fma(m110, m112, fma(m101, m121, m011 * m211));
+    const R a3 = fma(m201, m021, fma(m210, m012, m120 * m102));
+    R A = fma(R(-4), m111 * m111, -a1);
+    A = fma(R(-4), a2, A);
+    A = fma(R(-2), a3, A);
+    A = fma(-cst<R>(1, 3), m022 + m202 + m220, A);
+    A = fma(-cst<R>(1, 9), s2, A);
+    const R q101 = m101 * m101, q011 = m011 * m011, q110 = m110 * m110;
+    const R m200m020 = m200 * m020;
+    const R b1 = fma(q110, m002, fma(q011, m200, q101 * m020));
+    const R pairs = fma(m002, m020, fma(m002, m200, m200m020));
+    const R inner = fma(cst<R>(1, 3), s2, fma(R(2), q101 + q011 + q110, pairs));
+    R B = fma(R(2), m200m020 * m002, R(4) * b1);
+    B = fma(R(16), (m110 * m101) * m011, B);
+    B = fma(cst<R>(2, 3), inner, B);
+    B = fma(cst<R>(1, 27), fma(drho, drho, -drho), B);
+    return fma(B, oneOverRho, A) * oneOverRho;
 }
 
 template <class R>
@@ -379,10 +395,12 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
     R mxyyPxzz = m120 + m102;
     R mxyyMxzz = m120 - m102;
 
-    // velocity gradients (:357-362), OxxPyyPzz = 1
-    const R Dxy = r.minusThreeOmega * m110;
-    const R Dxz = r.minusThreeOmega * m101;
-    const R Dyz = r.minusThreeOmega * m011;
+    // velocity gradients (:357-362), OxxPyyPzz = 1; the mixed ones (from the
+    // second-order moments before relaxation) enter only the fourth-order
+    // terms, through fourthB
+    const R cm112 = r.fourthB * m110;
+    const R cm121 = r.fourthB * m101;
+    const R cm211 = r.fourthB * m011;
     const R dxux = r.halfMinusOmega * (mxxMyy + mxxMzz) + R(0.5) * (m000 - mxxPyyPzz);
     const R dyuy = dxux + r.omegaThreeHalves * mxxMyy;
     const R dzuz = dxux + r.omegaThreeHalves * mxxMzz;
@@ -413,9 +431,10 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
     mxyyMxzz += w * (-mxyyMxzz);
 
     // back to single moments (:431-441)
+    // (1/3)(-2 a + b + c) = (1/3)(a + b + c) - a, likewise for m002
     m200 = cst<R>(1, 3) * (mxxMyy + mxxMzz + mxxPyyPzz);
-    m020 = cst<R>(1, 3) * (-R(2) * mxxMyy + mxxMzz + mxxPyyPzz);
-    m002 = cst<R>(1, 3) * (mxxMyy - R(2) * mxxMzz + mxxPyyPzz);
+    m020 = m200 - mxxMyy;
+    m002 = m200 - mxxMzz;
     m210 = (mxxyMyzz + mxxyPyzz) * R(0.5);
     m012 = (-mxxyMyzz + mxxyPyzz) * R(0.5);
     m201 = (mxxzMyyz + mxxzPyyz) * R(0.5);
@@ -425,32 +444,27 @@ __host__ __device__ __forceinline__ void k17Collide(R* f, const K17Rates<R>& r, 
 
     // fourth order to the modified equilibrium (:452-457); orders 5 and 6
     // relax to zero (:463-471)
-    const R cm022 = r.minusTau * (dyuy + dzuz) * (cst<R>(2, 3)) * r.factorA;
-    const R cm202 = r.minusTau * (dxux + dzuz) * (cst<R>(2, 3)) * r.factorA;
-    const R cm220 = r.minusTau * (dyuy + dxux) * (cst<R>(2, 3)) * r.factorA;
-    const R cm112 = r.minusTau * Dxy * (cst<R>(1, 3)) * r.factorB;
-    const R cm121 = r.minusTau * Dxz * (cst<R>(1, 3)) * r.factorB;
-    const R cm211 = r.minusTau * Dyz * (cst<R>(1, 3)) * r.factorB;
+    const R cm022 = r.fourthA * (dyuy + dzuz);
+    const R cm202 = r.fourthA * (dxux + dzuz);
+    const R cm220 = r.fourthA * (dyuy + dxux);
 
     // cumulants back to central moments (:478-505)
-    m211 = cm211 + cst<R>(1, 3) * ((R(3) * m200 + R(1)) * m011 + R(6) * m110 * m101) * oneOverRho;
-    m121 = cm121 + cst<R>(1, 3) * ((R(3) * m020 + R(1)) * m101 + R(6) * m110 * m011) * oneOverRho;
-    m112 = cm112 + cst<R>(1, 3) * ((R(3) * m002 + R(1)) * m110 + R(6) * m101 * m011) * oneOverRho;
-    m220 = cm220 + (((m200 * m020 + R(2) * m110 * m110) * R(9) + R(3) * (m200 + m020)) * oneOverRho - (drho * oneOverRho)) *
-                       (cst<R>(1, 9));
-    m202 = cm202 + (((m200 * m002 + R(2) * m101 * m101) * R(9) + R(3) * (m200 + m002)) * oneOverRho - (drho * oneOverRho)) *
-                       (cst<R>(1, 9));
-    m022 = cm022 + (((m002 * m020 + R(2) * m011 * m011) * R(9) + R(3) * (m002 + m020)) * oneOverRho - (drho * oneOverRho)) *
-                       (cst<R>(1, 9));
-    m122 = cst<R>(1, 3) *
-           (R(3) * (m002 * m120 + m020 * m102 + R(4) * m011 * m111 + R(2) * (m101 * m021 + m110 * m012)) + (m120 + m102)) *
-           oneOverRho;
-    m212 = cst<R>(1, 3) *
-           (R(3) * (m002 * m210 + m200 * m012 + R(4) * m101 * m111 + R(2) * (m011 * m201 + m110 * m102)) + (m210 + m012)) *
-           oneOverRho;
-    m221 = cst<R>(1, 3) *
-           (R(3) * (m200 * m021 + m020 * m201 + R(4) * m110 * m111 + R(2) * (m101 * m120 + m011 * m210)) + (m021 + m201)) *
-           oneOverRho;
+    // (the reference's (1/3) X / rho and (9 P + 3 S) / (9 rho) - drho / (9 rho)
+    // regrouped as X (1/(3 rho)) and P / rho + S / (3 rho) - drho / (9 rho))
+    const R oor3 = oneOverRho * cst<R>(1, 3);
+    const R dr9 = drho * oneOverRho * cst<R>(1, 9);
+    m211 = fma(fma(fma(R(3), m200, R(1)), m011, R(6) * (m110 * m101)), oor3, cm211);
+    m121 = fma(fma(fma(R(3), m020, R(1)), m101, R(6) * (m110 * m011)), oor3, cm121);
+    m112 = fma(fma(fma(R(3), m002, R(1)), m110, R(6) * (m101 * m011)), oor3, cm112);
+    m220 = fma(fma(m200, m020, R(2) * (m110 * m110)), oneOverRho, fma(m200 + m020, oor3, cm220 - dr9));
+    m202 = fma(fma(m200, m002, R(2) * (m101 * m101)), oneOverRho, fma(m200 + m002, oor3, cm202 - dr9));
+    m022 = fma(fma(m002, m020, R(2) * (m011 * m011)), oneOverRho, fma(m002 + m020, oor3, cm022 - dr9));
+    m122 = fma(fma(m002, m120, fma(m020, m102, fma(R(4) * m011, m111, R(2) * fma(m101, m021, m110 * m012)))),
+               oneOverRho, (m120 + m102) * oor3);
+    m212 = fma(fma(m002, m210, fma(m200, m012, fma(R(4) * m101, m111, R(2) * fma(m011, m201, m110 * m102)))),
+               oneOverRho, (m210 + m012) * oor3);
+    m221 = fma(fma(m200, m021, fma(m020, m201, fma(R(4) * m110, m111, R(2) * fma(m101, m120, m011 * m210)))),
+               oneOverRho, (m021 + m201) * oor3);
     m222 = -c222Term(m111, m200, m020, m002, m022, m202, m220, m011, m101, m110, m211, m121, m112, m120, m102, m210,
                      m012, m201, m021, oneOverRho, drho);
 

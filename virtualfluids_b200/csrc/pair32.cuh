@@ -84,6 +84,8 @@ inline K17Rates<F2> pairRates(const K17Rates<float>& r)
     p.qlP = F2(r.qlP);
     p.qlM = F2(r.qlM);
     p.qlD = F2(r.qlD);
+    p.fourthA = F2(r.fourthA);
+    p.fourthB = F2(r.fourthB);
     return p;
 }
 
