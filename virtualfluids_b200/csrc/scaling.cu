@@ -122,11 +122,14 @@ struct ScalingView {
     const uint8_t* mask; // coarse to fine: mask[27 i + d] bit c = corner c writes direction d (NULL: all)
 };
 
-// the moments of the 8 source nodes of a cell (pre-collision view of parity EVEN)
+// the moments of the 8 source nodes of a cell (pre-collision view of parity EVEN);
+// the corner loops here and in coarseToFineCell are unrolled so that the
+// cell's node indices and the corner moment sets stay in registers
 template <class A, bool EVEN, class S, class R>
 __host__ __device__ __forceinline__ void cellSourceMoments(const S* dist, unsigned long long N, const uint32_t* B,
                                                            R omega, SourceMoments<R>* src)
 {
+#pragma unroll
     for (int c = 0; c < 8; ++c) {
         R f[27];
 #pragma unroll
@@ -146,6 +149,7 @@ __host__ __device__ __forceinline__ void coarseToFineCell(const ScalingView<S, R
     const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[i], v.offY[i], v.offZ[i]);
     blockWalk(v.fineCells[i], v.nXf, v.nYf, v.nZf, B);
     const uint8_t* writes = v.mask ? v.mask + 27 * (size_t)i : nullptr;
+#pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int c = cfCornerOrder(j);
         const R x = (c & 1) ? R(1) / R(4) : -R(1) / R(4);
