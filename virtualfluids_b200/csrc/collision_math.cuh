@@ -147,11 +147,20 @@ __host__ __device__ __forceinline__ void bwd(R& a, R& b, R& c, const Sweep<R>& w
     const R aK = K != 0 ? a + R(K) : a;
     const R hc = R(0.5) * c;
     const R na = fma(aK, w.hm, fma(b, w.vvm, hc));
-    // hp - hm = v and vvp - vvm = 1; the three populations sum to a
-    const R nc = na + fma(aK, w.vv, b);
-    b = (a - na) - nc;
-    a = na;
-    c = nc;
+    if constexpr (sizeof(typename ScalarOf<R>::type) == 8) {
+        // FP64: three independent chains (measured faster in double precision)
+        const R nb = fma(w.nv2, aK, fma(w.n2vv, b, a - c));
+        c = fma(aK, w.hp, fma(b, w.vvp, hc));
+        a = na;
+        b = nb;
+    } else {
+        // FP32 (scalar or paired): two operations fewer; hp - hm = v and
+        // vvp - vvm = 1, and the three populations sum to a
+        const R nc = na + fma(aK, w.vv, b);
+        b = (a - na) - nc;
+        a = na;
+        c = nc;
+    }
 }
 
 // --------------------------------------------------------- macroscopic sums --
