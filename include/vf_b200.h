@@ -266,8 +266,9 @@ int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t numberOfCells, co
  * (setPeriodicBoundaryCondition); [10] refinement box present, [11..16] the box
  * (min x, y, z, max x, y, z; MultipleGridBuilder::addGrid with a Cuboid);
  * [17..18] layers fine / between levels (setNumberOfLayers, used when [17] > 0);
- * [19] solid cuboid present, [20..25] its extent (addGeometry, meshed on the
- * finest level); [26] geometry BC (1 = no-slip, setNoSlipBoundaryCondition
+ * [19] solid primitive (addGeometry, meshed on the finest level): 1 a Cuboid
+ * with [20..25] its extent, 2 a Sphere with [20..23] centre and radius (its
+ * links' q values from the ray intersection, GridImp::calculateQs); [26] geometry BC (1 = no-slip, setNoSlipBoundaryCondition
  * (GEOMETRY)); [30..59] up to six side BCs as (side 0..5 = MX PX MY PY MZ PZ,
  * type 1 no-slip / 2 velocity / 3 pressure / 4 slip, three values) applied in
  * order (setNoSlip / setVelocity / setPressure / setSlipBoundaryCondition);

@@ -35,10 +35,19 @@ def grid_spec(name: str) -> np.ndarray:
     if name == "channel":
         sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
         return _spec([0, 0, 0, 11, 7, 7, 1.0], (0, 1, 0), sides=sides)
+    if name == "sphere_channel":
+        # a solid sphere in a channel: the geometry list's q values come from
+        # the ray-sphere intersection (fractional q on most links)
+        sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 31, 15, 15, 1.0], (0, 1, 0), sides=sides)
+        s[19] = 2.0
+        s[20:24] = [12, 7.3, 7.6, 3.2]
+        s[26] = 1.0
+        return s
     raise KeyError(name)
 
 
-GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel"]
+GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel", "sphere_channel"]
 
 # multi-level grids made by the reference's builder, which the repository's
 # builder reproduces: a channel 24 x 16 x 16 with a refined box and the

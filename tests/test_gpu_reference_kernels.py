@@ -107,6 +107,23 @@ def test_bc_kernels_match_reference_gpu_kernels(cuda, kind, lst, is_even, grid):
     assert _close(ours, ref, "f64")
 
 
+@pytest.mark.parametrize("kind", [_lib.BC_NOSLIP_INTERPOLATED, _lib.BC_SLIP])
+def test_bc_kernels_on_fractional_q_match_reference_gpu_kernels(cuda, kind):
+    """The solid sphere's geometry list (q from the ray-sphere intersection)."""
+    g = _grid("sphere_channel")
+    _, d = _random_state(g, "f64")
+    lat = K.DeviceLattice.from_arrays(g)
+    ours = torch.from_numpy(d).cuda()
+    ref = ours.clone()
+    k = torch.from_numpy(g["geometry.k"].astype(np.int32)).cuda()
+    q = torch.from_numpy(g["geometry.q"].astype(np.float64)).cuda()
+    for ev in (True, False):
+        K.bc_post(kind, ours, lat, k, q, 1.7, ev, stream=0)
+        ReferenceGpu("f64").bc_post(kind, ref, lat, k, q, 1.7, ev)
+    torch.cuda.synchronize()
+    assert _close(ours, ref, "f64")
+
+
 @pytest.mark.parametrize("is_even", [True, False])
 @pytest.mark.parametrize("coarse_to_fine", [True, False])
 def test_interface_kernels_match_reference_gpu_kernels(cuda, coarse_to_fine, is_even):

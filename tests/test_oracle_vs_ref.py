@@ -60,3 +60,34 @@ def test_lattice_sequence_matches_live_reference(precision):
     a = lattice_sequence(Oracle(precision), g, precision, steps=6)
     b = lattice_sequence(R, g, precision, steps=6)
     assert np.array_equal(a, b)
+
+
+def _sphere_grid():
+    with np.load(GOLDEN / "grid_sphere_channel.npz") as z:
+        return {k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("kind", [0, 1, 4])
+@pytest.mark.parametrize("is_even", [True, False])
+def test_bc_on_fractional_q_matches_live_reference(kind, is_even):
+    """The solid sphere's geometry list, whose q come from the ray-sphere
+    intersection (fractional on most links): the oracle's no-slip
+    (interpolated, bounce-back) and slip BCs equal the reference's kernels
+    bit for bit."""
+    g = _sphere_grid()
+    k, q = g["geometry.k"], g["geometry.q"].astype(np.float64)
+    assert ((q > 0) & (q < 1) & (q != 0.5)).sum() > 1000
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    rng = np.random.default_rng(17)
+    fields = [rng.uniform(-1e-2, 1e-2, N) for _ in range(4)]
+    out = []
+    for impl in (Oracle("f64"), Reference("f64")):
+        d = np.zeros(27 * N)
+        for ev in (0, 1):
+            impl.init_eq(d, N, g["geo"], *nb, *fields, ev)
+        d += np.random.default_rng(3).uniform(-1e-3, 1e-3, d.shape) * (d != 0)
+        impl.bc_post(kind, d, N, *nb, k, q, 1.7, is_even=is_even)
+        out.append(d)
+    assert np.array_equal(out[0], out[1])

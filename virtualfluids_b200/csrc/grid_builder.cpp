@@ -69,6 +69,40 @@ bool Box::containsPoint(double x, double y, double z) const
     return true;
 }
 
+bool Solid::contains(double x, double y, double z) const
+{
+    if (kind == Kind::Cuboid)
+        return box.containsPoint(x, y, z);
+    // Sphere::isPointInObject with zero offsets (Sphere.cpp)
+    const double dx = x - cx, dy = y - cy, dz = z - cz;
+    return (dx * dx + dy * dy + dz * dz) < (r * r);
+}
+
+// Sphere::getIntersection (Sphere.cpp): the roots of |p + t d - c|^2 = r^2,
+// the smaller non-negative one
+bool Solid::intersect(double px, double py, double pz, double dx, double dy, double dz, double& t) const
+{
+    if (kind == Kind::Cuboid)
+        return false;
+    const double rx = px - cx, ry = py - cy, rz = pz - cz;
+    const double dd = dx * dx + dy * dy + dz * dz;
+    const double p = 2 * (rx * dx + ry * dy + rz * dz) / dd;
+    const double q = (rx * rx + ry * ry + rz * rz - r * r) / dd;
+    const double disc = 0.25 * p * p - q;
+    if (disc < 0.0)
+        return false;
+    double t1 = -0.5 * p + std::sqrt(disc);
+    double t2 = -0.5 * p - std::sqrt(disc);
+    if (t1 < 0.0 && t2 < 0.0)
+        return false;
+    if (t1 < 0.0)
+        t1 = (double)FLT_MAX;
+    if (t2 < 0.0)
+        t2 = (double)FLT_MAX;
+    t = t2 < t1 ? t2 : t1;
+    return true;
+}
+
 int64_t LevelGrid::coordToIndex(double x, double y, double z) const
 {
     const long ix = std::lround((x - startX) / delta);
@@ -366,14 +400,14 @@ void LevelGrid::findFluidNodes()
 // :251-268), needle cells are closed (:1362-1401), INVALID_SOLID nodes next to
 // fluid become STOPPER_SOLID (:449-453) and fluid nodes next to those BC_SOLID,
 // numbered in matrix order (:455-463).
-void LevelGrid::meshSolid(const Box& solid)
+void LevelGrid::meshSolid(const Solid& solid)
 {
     for (uint64_t idx = 0; idx < size; ++idx) {
         if (field[idx] == INVALID_SOLID)
             continue;
         int64_t ix, iy, iz;
         coords(idx, ix, iy, iz);
-        if (solid.containsPoint(coordX(ix), coordY(iy), coordZ(iz)))
+        if (solid.contains(coordX(ix), coordY(iy), coordZ(iz)))
             field[idx] = INVALID_SOLID;
     }
     auto isSolidAt = [&](int64_t jx, int64_t jy, int64_t jz) {
@@ -407,12 +441,37 @@ void LevelGrid::meshSolid(const Box& solid)
             solidBoundaryIndex[idx] = numberOfSolidBoundaryNodes++;
         }
     }
+    // GridImp::findQsPrimitive / calculateQs (GridImp.cpp:1522-1596): per
+    // BC_SOLID node and link to a node of the grid, the distance to the
+    // surface along the link in lattice spacings, kept when it lies in
+    // [0, 1] (with the reference's relative tolerance).  The rest direction
+    // has no length and never yields a value.
+    const uint32_t nS = numberOfSolidBoundaryNodes;
+    solidQ.assign(27 * (size_t)nS, -1.0);
+    for (uint64_t idx = 0; idx < size; ++idx) {
+        if (field[idx] != BC_SOLID)
+            continue;
+        int64_t ix, iy, iz;
+        coords(idx, ix, iy, iz);
+        const double x = coordX(ix), y = coordY(iy), z = coordZ(iz);
+        for (int d = 1; d < 27; ++d) {
+            const double dx = (double)vfb::cx(d), dy = (double)vfb::cy(d), dz = (double)vfb::cz(d);
+            if (coordToIndex(x + dx * delta, y + dy * delta, z + dz * delta) < 0)
+                continue;
+            double t;
+            if (!solid.intersect(x, y, z, dx, dy, dz, t))
+                continue;
+            const double sub = t / delta;
+            double& qv = solidQ[(size_t)d * nS + (size_t)solidBoundaryIndex[idx]];
+            if (lessEqualTol(sub, 1.0) && greaterEqualTol(sub, 0.0) && (-0.5 > qv || sub < qv))
+                qv = sub;
+        }
+    }
 }
 
-// Geometry::addIndices (Side.cpp:270-307).  A cuboid has no ray
-// intersection (Object::getIntersection returns an error for primitives), so
-// GridImp::findQsPrimitive leaves every q at -1 and a link gets q = 1/2 when its
-// neighbour is a stopper node.
+// Geometry::addIndices (Side.cpp:270-307): the links' q values (a cuboid has
+// no ray intersection, Object::getIntersection, so all its q stay -1), and a
+// link without one gets q = 1/2 when its neighbour is a stopper node.
 void LevelGrid::geometryList(std::vector<int32_t>& k, std::vector<double>& q) const
 {
     std::vector<int64_t> nodes;
@@ -428,12 +487,14 @@ void LevelGrid::geometryList(std::vector<int32_t>& k, std::vector<double>& q) co
         int64_t ix, iy, iz;
         coords(idx, ix, iy, iz);
         for (int d = 0; d < 27; ++d) {
+            double qd = solidQ[(size_t)d * numberOfSolidBoundaryNodes + (size_t)solidBoundaryIndex[idx]];
             const int64_t m = index(ix + cx(d), iy + cy(d), iz + cz(d));
-            if (m < 0)
-                continue;
-            const uint8_t t = field[(uint64_t)m];
-            if (t == STOPPER_OUT_OF_GRID_BOUNDARY || t == STOPPER_OUT_OF_GRID || t == STOPPER_SOLID)
-                q[(size_t)d * n + i] = 0.5;
+            if (qd < -0.5 && m >= 0) {
+                const uint8_t t = field[(uint64_t)m];
+                if (t == STOPPER_OUT_OF_GRID_BOUNDARY || t == STOPPER_OUT_OF_GRID || t == STOPPER_SOLID)
+                    qd = 0.5;
+            }
+            q[(size_t)d * n + i] = qd;
         }
     }
 }
@@ -837,7 +898,7 @@ void GridBuilder::addGrid(const Box& box, int levelFine)
     }
 }
 
-void GridBuilder::addGeometry(const Box& s)
+void GridBuilder::addGeometry(const Solid& s)
 {
     if (built)
         throw std::runtime_error("addGeometry after buildGrids");

@@ -56,6 +56,20 @@ struct Box {
     bool containsPoint(double x, double y, double z) const;
 };
 
+// A solid geometric primitive of the reference (geometries/Cuboid,
+// geometries/Sphere): which lattice points it holds and, for the sphere, where
+// a ray from a point along a lattice direction meets its surface.
+struct Solid {
+    enum class Kind { Cuboid, Sphere } kind = Kind::Cuboid;
+    Box box {};                           // cuboid
+    double cx = 0, cy = 0, cz = 0, r = 0; // sphere
+    bool contains(double x, double y, double z) const;
+    // Object::getIntersection: true with t (in units of the direction
+    // vector) when the ray point + t * direction meets the surface at t >= 0;
+    // a cuboid reports no intersection, as the reference's primitive does
+    bool intersect(double px, double py, double pz, double dx, double dy, double dz, double& t) const;
+};
+
 // interface cells between a level and the next finer one
 // (GridInterface::cf / fc): matrix indices until the sparse renumbering,
 // sparse indices after it; offset = index of the D3Q27 direction
@@ -94,10 +108,10 @@ public:
     void initial(const LevelGrid* finer);
     void findSparseIndices();
     void findFluidNodes();
-    // solid cuboid on this level (GridImp::mesh + findQsPrimitive for a
+    // solid primitive on this level (GridImp::mesh + findQsPrimitive for a
     // geometric primitive): inside nodes removed, one stopper layer inside the
-    // solid, one BC_SOLID layer outside it
-    void meshSolid(const Box& solid);
+    // solid, one BC_SOLID layer outside it, the links' q values
+    void meshSolid(const Solid& solid);
     // interface cells to the next finer level (GridImp::findGridInterface,
     // repairGridInterfaceOnMultiGPU) and their sparse renumbering
     void findGridInterface(LevelGrid& fine);
@@ -117,6 +131,7 @@ public:
     Box shape {};
     std::vector<int64_t> solidBoundaryIndex; // BC_SOLID nodes in matrix order, -1 elsewhere
     uint32_t numberOfSolidBoundaryNodes = 0;
+    std::vector<double> solidQ;             // q[d * numberOfSolidBoundaryNodes + BC_SOLID number], -1 none
     InterfaceCells cf, fc;          // to the next finer level
 
     std::vector<uint8_t> field;
@@ -193,8 +208,8 @@ public:
     // layers of setNumberOfLayers
     void addGrid(const Box& box, int levelFine);
     void setNumberOfLayers(uint32_t fine, uint32_t betweenLevels);
-    // solid cuboid, meshed on the finest level (MultipleGridBuilder::addGeometry)
-    void addGeometry(const Box& solid);
+    // solid primitive, meshed on the finest level (MultipleGridBuilder::addGeometry)
+    void addGeometry(const Solid& solid);
     void setPeriodicBoundaryCondition(bool px, bool py, bool pz);
     void buildGrids(bool enableThinWalls = false);
 
@@ -222,7 +237,7 @@ private:
     std::vector<std::vector<BCList>> velocity, slip, pressure;
     uint32_t layersFine = 12, layersBetweenLevels = 8; // MultipleGridBuilder.cpp:53
     bool hasSolid = false;
-    Box solid {};
+    Solid solid {};
     bool geometryNoSlip = false;
     bool built = false;
 };

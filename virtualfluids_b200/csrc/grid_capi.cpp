@@ -165,7 +165,8 @@ extern "C" {
  * spec: [0..6] coarse grid start x,y,z, end x,y,z, delta; [7..9] periodic;
  * [10] refinement box present, [11..16] the box (min x,y,z, max x,y,z);
  * [17..18] layers fine / between levels (used when [17] > 0); [19] solid
- * cuboid present, [20..25] its extent; [26..29] geometry BC (type 1 =
+ * primitive: 1 cuboid with [20..25] its extent, 2 sphere with [20..23]
+ * centre and radius; [26..29] geometry BC (type 1 =
  * no-slip); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
  * are set; [60] enableThinWalls; [61] finest level of the refinement box
  * (0 = 1; n >= 62 values).  Same layout as the grid oracle.  Returns NULL on
@@ -187,8 +188,19 @@ void* vfb_grid_build(const double* s, int n)
             const int levelFine = (n > 61 && s[61] > 0) ? (int)s[61] : 1;
             h->builder.addGrid(Box { s[11], s[12], s[13], s[14], s[15], s[16] }, levelFine);
         }
-        if (s[19] > 0)
-            h->builder.addGeometry(Box { s[20], s[21], s[22], s[23], s[24], s[25] });
+        if (s[19] > 0) {
+            Solid solid;
+            if (s[19] == 2) {
+                solid.kind = Solid::Kind::Sphere;
+                solid.cx = s[20];
+                solid.cy = s[21];
+                solid.cz = s[22];
+                solid.r = s[23];
+            } else {
+                solid.box = Box { s[20], s[21], s[22], s[23], s[24], s[25] };
+            }
+            h->builder.addGeometry(solid);
+        }
         h->builder.setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);
         h->builder.buildGrids(s[60] > 0);
         for (int i = 0; i < 6; ++i) {
