@@ -134,3 +134,19 @@ def test_full_size_cube_benchmark_grid_matches_reference():
     if r.returncode < 0:
         pytest.skip(f"the reference's builder crashed (signal {-r.returncode})")
     assert r.stdout.strip().splitlines()[-1].startswith("ok"), r.stdout[-500:] + r.stderr[-500:]
+
+
+def test_sphere_through_the_builder_api():
+    """addGeometry(Sphere(...)) gives the golden sphere grid."""
+    b = vgrid.MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, 31, 15, 15, 1.0)
+    b.addGeometry(vgrid.Sphere(12, 7.3, 7.6, 3.2))
+    b.setPeriodicBoundaryCondition(False, True, False)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(vgrid.SideType.MX, 0.04, 0, 0)
+    b.setPressureBoundaryCondition(vgrid.SideType.PX, 0.0)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.MZ)
+    b.setSlipBoundaryCondition(vgrid.SideType.PZ, 0, 0, 1)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.GEOMETRY)
+    z = np.load(GOLDEN / "grid_sphere_channel.npz")
+    compare(b.arrays(), [{k.split(":", 1)[1]: z[k] for k in z.files}])

@@ -56,6 +56,24 @@ GRID_ARRAY_NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "nei
                     "fc.offY", "fc.offZ"]
 
 
+class Cuboid:
+    """Axis-aligned box between two corners (geometries/Cuboid)."""
+
+    def __init__(self, minX, minY, minZ, maxX, maxY, maxZ):
+        self.corners = (minX, minY, minZ, maxX, maxY, maxZ)
+
+    def box(self):
+        return self.corners
+
+
+class Sphere:
+    """Sphere of a centre and a radius (geometries/Sphere); as a solid its
+    links' q values come from the ray-sphere intersection."""
+
+    def __init__(self, centerX, centerY, centerZ, radius):
+        self.centerX, self.centerY, self.centerZ, self.radius = centerX, centerY, centerZ, radius
+
+
 class MultipleGridBuilder:
     """Builder with the reference's call sequence: addCoarseGrid, (addGrid,
     addGeometry), setPeriodicBoundaryCondition, buildGrids, then the side
@@ -85,10 +103,16 @@ class MultipleGridBuilder:
     def setNumberOfLayers(self, fine: int, between: int):
         self.spec[17:19] = [fine, between]
 
-    def addGeometry(self, cuboid):
-        """Solid cuboid (minX, minY, minZ, maxX, maxY, maxZ)."""
-        self.spec[19] = 1
-        self.spec[20:26] = cuboid
+    def addGeometry(self, solid):
+        """Solid primitive, meshed on the finest level: a Sphere, a Cuboid, or
+        a plain (minX, minY, minZ, maxX, maxY, maxZ) cuboid."""
+        if isinstance(solid, Sphere):
+            self.spec[19] = 2
+            self.spec[20:26] = [solid.centerX, solid.centerY, solid.centerZ, solid.radius, 0, 0]
+        else:
+            c = solid.box() if isinstance(solid, Cuboid) else tuple(solid)
+            self.spec[19] = 1
+            self.spec[20:26] = c
 
     def setPeriodicBoundaryCondition(self, px: bool, py: bool, pz: bool):
         self.spec[7:10] = [float(px), float(py), float(pz)]
