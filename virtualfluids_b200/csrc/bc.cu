@@ -16,9 +16,15 @@
 // Pre-collision kind (after the parity swap):
 //   pressure non-equilibrium PressureNonEquilibriumCompressible.cu:45-311
 //
-// Every node writes only its own locations, and no node reads a location
-// another node of the same list writes (for a fixed location bit the map
-// node -> location index is one to one), so the kernels are race free.
+// Every node writes only its own locations, so no two nodes write one cell
+// (for a fixed location bit the map node -> location index is one to one).
+// Nodes of a list that are lattice neighbours of each other (around a solid
+// body, not along a flat wall) can read a cell another node writes: a node's
+// bounce-back value lands where a neighbouring BC node reads a post-collision
+// population.  Like the reference's kernels, these read all of a node's values
+// before writing, so a list resident in one wave sees the state before the
+// launch everywhere; across waves the outcome depends on the schedule, as it
+// does in the reference.
 #include <cuda_runtime.h>
 
 #include "capi_common.cuh"
