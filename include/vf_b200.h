@@ -416,6 +416,10 @@ int vfb_mass_and_energy_static(int storage, const void* distributions, unsigned 
                                const uint32_t* nodeIndices, uint32_t numberOfIndices, int isEvenTimestep,
                                double* out, void* stream);
 
+/* Check hook of the grid builder's side q rule: the q values of a node on
+ * side `side` (0..5 = MX PX MY PY MZ PZ) whose neighbours are all boundary
+ * stoppers, after the sides alreadySet[0..nSet) (Side::setQs, Side.cpp:149-215). */
+int vfb_debug_side_qs(int side, const int* alreadySet, int nSet, double* q27);
 /*
  * One node of the K17 (op 0) or BGK (op 1) collision on the host with the
  * library's own arithmetic (the code the kernels run), for checks without a

@@ -223,6 +223,30 @@ void* vfb_grid_build(const double* s, int n)
     return h;
 }
 
+/*
+ * The q values the builder gives a node on domain side `side` (0..5 = MX PX MY
+ * PY MZ PZ) when every node around it is a boundary stopper and the sides
+ * alreadySet[0..nSet) were set on it before (Side::setQs with its diagonal
+ * reset, Side.cpp:149-215): q27[d] = 1/2 for the links along the side's
+ * normal, -1 otherwise.  A check hook; the geometry side has no normal and
+ * is rejected, as the reference rejects it.
+ */
+int vfb_debug_side_qs(int side, const int* alreadySet, int nSet, double* q27)
+{
+    vfb::clearError();
+    if (side < 0 || side > 5 || !q27 || nSet < 0 || nSet > 6 || (nSet > 0 && !alreadySet))
+        return vfb::setError(VFB_ERR_INVALID_ARGUMENT, "side must be 0..5 with up to six sides set before");
+    LevelGrid g(0, 0, 0, 2, 2, 2, 1.0, 0);
+    g.field.assign(g.size, STOPPER_OUT_OF_GRID_BOUNDARY);
+    for (int i = 0; i < nSet; ++i) {
+        if (alreadySet[i] < 0 || alreadySet[i] > 5)
+            return vfb::setError(VFB_ERR_INVALID_ARGUMENT, "side %d set before has no normal", alreadySet[i]);
+        g.bcAlreadySet.push_back((SideType)alreadySet[i]);
+    }
+    g.sideQs((SideType)side, 1, 1, 1, q27);
+    return VFB_OK;
+}
+
 int vfb_grid_levels(void* h) { return h ? (int)static_cast<GridHandle*>(h)->levels.size() : 0; }
 
 long long vfb_grid_count(void* h, int level, const char* name)
