@@ -27,10 +27,7 @@ MX, PX, MY, PY, MZ, PZ = range(6)
 
 
 def side_qs(side, already=()):
-    L = _lib.lib()
-    f = L.vfb_debug_side_qs
-    f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    f.restype = ctypes.c_int
+    f = _lib.lib().vfb_debug_side_qs
     s = (ctypes.c_int * 6)(*already)
     q = (ctypes.c_double * 27)()
     _lib.check(f(side, s, len(already), q))
@@ -96,7 +93,6 @@ def test_side_qs_every_combination_of_earlier_sides(side):
 
 def test_geometry_side_is_rejected():
     f = _lib.lib().vfb_debug_side_qs
-    f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     q = (ctypes.c_double * 27)()
     assert f(PX, (ctypes.c_int * 1)(6), 1, q) == _lib.VFB_ERR_INVALID_ARGUMENT
 

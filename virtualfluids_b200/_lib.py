@@ -170,6 +170,8 @@ _SIGNATURES = [
     ("vfb_debug_collide_node", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.POINTER(ctypes.c_double),
       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("vfb_debug_side_qs", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     ("vfb_grid_levels", ctypes.c_int, [ctypes.c_void_p]),
     ("vfb_grid_count", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),
