@@ -23,8 +23,8 @@ from tests.test_grid_builder import build_mine  # noqa: E402
 
 def random_spec(seed: int) -> np.ndarray:
     """A box refined to level 1 or 2 inside a coarse channel, random
-    periodicity, layer counts, side BCs and (half the time) a solid cuboid
-    strictly inside the box."""
+    periodicity, layer counts, side BCs and (half the time) a solid cuboid or
+    sphere strictly inside the box."""
     rng = np.random.default_rng(seed)
     s = np.zeros(64)
     n = rng.integers(16, 36, 3)
@@ -43,6 +43,12 @@ def random_spec(seed: int) -> np.ndarray:
             s[19] = 1
             s[20:26] = [*c0, *c1]
             s[26] = 1
+            if rng.random() < 0.5:
+                # a sphere inside that cuboid instead (fractional q from the ray intersection)
+                centre = [(c0[a] + c1[a]) / 2 + rng.uniform(-0.2, 0.2) for a in range(3)]
+                radius = min(c1[a] - c0[a] for a in range(3)) / 2 * rng.uniform(0.6, 0.95)
+                s[19] = 2
+                s[20:26] = [*centre, radius, 0, 0]
     i = 0
     for side in rng.permutation(6):
         if s[7 + side // 2] > 0:
