@@ -109,7 +109,8 @@ void REF(vfref_init_eq)(real* dist, unsigned long long N, unsigned* geo, unsigne
 }
 
 // post-collision BC kernels; kind: 0 no-slip interpolated, 1 no-slip
-// bounce-back, 2 velocity interpolated, 3 velocity bounce-back, 4 slip
+// bounce-back, 2 velocity interpolated, 3 velocity bounce-back, 4 slip,
+// 5 velocity with pressure interpolated
 void REF(vfref_bc_post)(int kind, real* dist, unsigned long long N, unsigned* nx, unsigned* ny, unsigned* nz,
                         int* bcNodes, real* q, unsigned nBC, real omega, real* Vx, real* Vy, real* Vz, int isEven)
 {
@@ -123,6 +124,10 @@ void REF(vfref_bc_post)(int kind, real* dist, unsigned long long N, unsigned* nx
             break;
         case 3: VelocityBounceBack_Device(Vx, Vy, Vz, dist, bcNodes, q, nBC, nx, ny, nz, N, isEven != 0); break;
         case 4: SlipCompressible_Device(dist, bcNodes, q, nBC, omega, nx, ny, nz, N, isEven != 0); break;
+        case 5:
+            VelocityWithPressureInterpolatedCompressible_Device(Vx, Vy, Vz, dist, bcNodes, q, nBC, omega, nx, ny, nz, N,
+                                                                isEven != 0);
+            break;
         default: break;
         }
     }

@@ -101,7 +101,8 @@ int REF(vfref_gpu_collision_bgk)(real* dist, unsigned long long N, unsigned* geo
 
 // post-collision BC launchers (NoSlip.cu:81-98, Velocity.cu, Slip.cu); kind:
 // 0 no-slip interpolated, 1 no-slip bounce-back, 2 velocity interpolated,
-// 3 velocity bounce-back, 4 slip.  Returns -1 for another kind.
+// 3 velocity bounce-back, 4 slip, 5 velocity with pressure interpolated.
+// Returns -1 for another kind.
 int REF(vfref_gpu_bc_post)(int kind, real* dist, unsigned long long N, unsigned* nx, unsigned* ny, unsigned* nz,
                            int* bcNodes, real* q, unsigned nBC, real omega, real* Vx, real* Vy, real* Vz, int isEven,
                            void* stream)
@@ -118,6 +119,10 @@ int REF(vfref_gpu_bc_post)(int kind, real* dist, unsigned long long N, unsigned*
         break;
     case 3: VelocityBounceBack_Device<<<grid, kThreads, 0, s>>>(Vx, Vy, Vz, dist, bcNodes, q, nBC, nx, ny, nz, N, ev); break;
     case 4: SlipCompressible_Device<<<grid, kThreads, 0, s>>>(dist, bcNodes, q, nBC, omega, nx, ny, nz, N, ev); break;
+    case 5:
+        VelocityWithPressureInterpolatedCompressible_Device<<<grid, kThreads, 0, s>>>(Vx, Vy, Vz, dist, bcNodes, q, nBC,
+                                                                                       omega, nx, ny, nz, N, ev);
+        break;
     default: return -1;
     }
     return (int)cudaGetLastError();

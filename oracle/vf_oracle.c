@@ -669,6 +669,7 @@ static const int QORDER[26] = { dP00, dM00, d0P0, d0M0, d00P, d00M, dPP0, dMM0, 
 #define BC_VELOCITY_INTERP 2
 #define BC_VELOCITY_BB 3
 #define BC_SLIP 4
+#define BC_VELOCITY_PRESSURE 5
 
 /* post-collision BC over a compacted list (kind selects the formula):
  *   NoSlipInterpolatedCompressible.cu:44-378, NoSlipBounceBack.cu,
@@ -685,12 +686,12 @@ void FN(vfo_bc_post)(int kind, real *dist, uint64_t N, const uint32_t *nx, const
         for (int d = 0; d < 27; ++d)
             g[d] = post_value(dist, N, &L, isEven, d);
         real drho = 0, vx1 = 0, vx2 = 0, vx3 = 0, cu_sq = 0;
-        if (kind == BC_NOSLIP_INTERP || kind == BC_VELOCITY_INTERP || kind == BC_SLIP) {
+        if (kind == BC_NOSLIP_INTERP || kind == BC_VELOCITY_INTERP || kind == BC_SLIP || kind == BC_VELOCITY_PRESSURE) {
             bc_macros(g, &drho, &vx1, &vx2, &vx3);
             cu_sq = C(3, 2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3) * ((real)1 + drho);
         }
         real UX = 0, UY = 0, UZ = 0;
-        if (kind == BC_VELOCITY_INTERP || kind == BC_VELOCITY_BB) {
+        if (kind == BC_VELOCITY_INTERP || kind == BC_VELOCITY_BB || kind == BC_VELOCITY_PRESSURE) {
             UX = Vx[i];
             UY = Vy[i];
             UZ = Vz[i];
@@ -724,6 +725,13 @@ void FN(vfo_bc_post)(int kind, real *dist, uint64_t N, const uint32_t *nx, const
             case BC_VELOCITY_INTERP: {
                 const real feq = feq_bc(drho, cdot(d, vx1, vx2, vx3), cu_sq, w);
                 *target = interp_velo(qd, g[d], g[e], feq, omega, cdot(d, UX, UY, UZ), w);
+                break;
+            }
+            case BC_VELOCITY_PRESSURE: {
+                /* the velocity formula minus w drho (KernelUtilities.h:208-214,
+                 * VelocityWithPressureInterpolatedCompressible.cu) */
+                const real feq = feq_bc(drho, cdot(d, vx1, vx2, vx3), cu_sq, w);
+                *target = interp_velo(qd, g[d], g[e], feq, omega, cdot(d, UX, UY, UZ), w) - w * drho;
                 break;
             }
             case BC_SLIP: {

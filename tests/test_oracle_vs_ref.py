@@ -91,3 +91,38 @@ def test_bc_on_fractional_q_matches_live_reference(kind, is_even):
         impl.bc_post(kind, d, N, *nb, k, q, 1.7, is_even=is_even)
         out.append(d)
     assert np.array_equal(out[0], out[1])
+
+
+def _golden_level0(name):
+    with np.load(GOLDEN / f"grid_{name}.npz") as z:
+        return {k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("grid,lst", [("cavity8", "velocity"), ("channel", "velocity"), ("sphere_channel", "geometry")])
+@pytest.mark.parametrize("is_even", [True, False])
+def test_velocity_with_pressure_bc_matches_live_reference(precision, grid, lst, is_even):
+    """VelocityWithPressureInterpolatedCompressible (kind 5): the oracle equals
+    the reference's kernel source built for the host, bit for bit, on wall
+    lists (q = 1/2) and on the sphere's fractional q."""
+    g = _golden_level0(grid)
+    real = np.float64 if precision == "f64" else np.float32
+    k, q = g[f"{lst}.k"], g[f"{lst}.q"].astype(real)
+    n = len(k)
+    rng = np.random.default_rng(21)
+    vel = [rng.uniform(-0.03, 0.03, n).astype(real) for _ in range(3)]
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    fields = [rng.uniform(-1e-2, 1e-2, N).astype(real) for _ in range(4)]
+    out = []
+    for impl in (Oracle(precision), Reference(precision)):
+        d = np.zeros(27 * N, real)
+        for ev in (0, 1):
+            impl.init_eq(d, N, g["geo"], *nb, *fields, ev)
+        d += (np.random.default_rng(5).uniform(-1e-3, 1e-3, d.shape) * (d != 0)).astype(real)
+        before = d.copy()
+        impl.bc_post(5, d, N, *nb, k, q, real(1.7), *vel, is_even=is_even)
+        assert (d != before).sum() > n
+        out.append(d)
+    assert np.array_equal(out[0], out[1])
