@@ -167,6 +167,8 @@ typedef struct vfb_bc_list {
 #define VFB_BC_VELOCITY_INTERPOLATED 2 /* VelocityInterpolatedCompressible_Device, Velocity/VelocityInterpolatedCompressible.cu:44-418 */
 #define VFB_BC_VELOCITY_BOUNCE_BACK 3  /* VelocityBounceBack_Device, Velocity/VelocityBounceBack.cu */
 #define VFB_BC_SLIP 4                  /* SlipCompressible_Device, Slip/SlipCompressible.cu:45-550 */
+#define VFB_BC_VELOCITY_WITH_PRESSURE 5 /* VelocityWithPressureInterpolatedCompressible_Device,
+                                           Velocity/VelocityWithPressureInterpolatedCompressible.cu */
 
 /*
  * One post-collision BC kernel over a list (one thread per BC node).  Replaces
@@ -317,7 +319,7 @@ int vfb_grid_put(void* grid, int level, const char* name, int elemSize, long lon
 typedef struct vfb_sim_params {
     int storage;               /* VFB_FP32 / FP64 / FP16 / BF16 */
     int collisionKernel;       /* 0 "K17CompressibleNavierStokes", 1 "BGKCompSP27" (KernelTypes.h:36-38) */
-    int velocityBC;            /* VFB_BC_VELOCITY_INTERPOLATED or VFB_BC_VELOCITY_BOUNCE_BACK */
+    int velocityBC;            /* VFB_BC_VELOCITY_INTERPOLATED, VFB_BC_VELOCITY_BOUNCE_BACK or VFB_BC_VELOCITY_WITH_PRESSURE */
     int noSlipBC;              /* VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK, -1 NoSlipDelayBounceBack (no kernel) */
     int geometryBC;            /* as noSlipBC, for the geometry list */
     int slipBC;                /* VFB_BC_SLIP or -1 */

@@ -109,7 +109,8 @@ class ScalingArgs(ctypes.Structure):
     ]
 
 
-BC_NOSLIP_INTERPOLATED, BC_NOSLIP_BOUNCE_BACK, BC_VELOCITY_INTERPOLATED, BC_VELOCITY_BOUNCE_BACK, BC_SLIP = range(5)
+(BC_NOSLIP_INTERPOLATED, BC_NOSLIP_BOUNCE_BACK, BC_VELOCITY_INTERPOLATED, BC_VELOCITY_BOUNCE_BACK, BC_SLIP,
+ BC_VELOCITY_WITH_PRESSURE) = range(6)
 
 # (name, restype, argtypes) of every exported entry point
 _SIGNATURES = [

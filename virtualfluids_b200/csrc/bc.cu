@@ -13,6 +13,8 @@
 //   velocity interpolated VelocityInterpolatedCompressible.cu:44-418
 //   velocity bounce-back  VelocityBounceBack.cu
 //   slip                  SlipCompressible.cu:45-550
+//   velocity with pressure VelocityWithPressureInterpolatedCompressible.cu
+//                          (the velocity formula minus w drho, KernelUtilities.h:208-214)
 // Pre-collision kind (after the parity swap):
 //   pressure non-equilibrium PressureNonEquilibriumCompressible.cu:45-311
 //
@@ -144,12 +146,14 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
         g[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(inv(d)) * N + L.k[loc(inv(d))]);
 
     R drho = R(0), vx1 = R(0), vx2 = R(0), vx3 = R(0), cuSq = R(0);
-    if (KIND == VFB_BC_NOSLIP_INTERPOLATED || KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_SLIP) {
+    if (KIND == VFB_BC_NOSLIP_INTERPOLATED || KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_SLIP ||
+        KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
         bcMacros(g, drho, vx1, vx2, vx3);
         cuSq = R(3) / R(2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3) * (R(1) + drho);
     }
     R UX = R(0), UY = R(0), UZ = R(0);
-    if (KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_VELOCITY_BOUNCE_BACK) {
+    if (KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_VELOCITY_BOUNCE_BACK ||
+        KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
         UX = __ldg(Vx + i);
         UY = __ldg(Vy + i);
         UZ = __ldg(Vz + i);
@@ -178,6 +182,9 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
         } else if (KIND == VFB_BC_VELOCITY_INTERPOLATED) {
             const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
             value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, UX, UY, UZ), w);
+        } else if (KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
+            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
+            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, UX, UY, UZ), w) - w * drho;
         } else {
             if (order(d) == 1) {
                 if (cx(d) != 0)
@@ -279,6 +286,9 @@ static int launchPost(int kind, const vfb_bc_lattice* t, const vfb_bc_list* l, c
     case VFB_BC_NOSLIP_BOUNCE_BACK: launchPostKind<S, VFB_BC_NOSLIP_BOUNCE_BACK>(even, blocks, stream, dist, lat, l); break;
     case VFB_BC_VELOCITY_INTERPOLATED: launchPostKind<S, VFB_BC_VELOCITY_INTERPOLATED>(even, blocks, stream, dist, lat, l); break;
     case VFB_BC_VELOCITY_BOUNCE_BACK: launchPostKind<S, VFB_BC_VELOCITY_BOUNCE_BACK>(even, blocks, stream, dist, lat, l); break;
+    case VFB_BC_VELOCITY_WITH_PRESSURE:
+        launchPostKind<S, VFB_BC_VELOCITY_WITH_PRESSURE>(even, blocks, stream, dist, lat, l);
+        break;
     default: launchPostKind<S, VFB_BC_SLIP>(even, blocks, stream, dist, lat, l); break;
     }
     return checkLaunch("post-collision boundary condition");
@@ -316,7 +326,7 @@ using namespace vfb;
 extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice, const vfb_bc_list* list, void* stream)
 {
     clearError();
-    if (kind < VFB_BC_NOSLIP_INTERPOLATED || kind > VFB_BC_SLIP)
+    if (kind < VFB_BC_NOSLIP_INTERPOLATED || kind > VFB_BC_VELOCITY_WITH_PRESSURE)
         return setError(VFB_ERR_INVALID_ARGUMENT, "unknown BC kind %d", kind);
     if (vfb_storage_bytes(storage) == 0)
         return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
@@ -328,10 +338,12 @@ extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice,
         return rc;
     if (!list->k || !list->q)
         return setError(VFB_ERR_INVALID_ARGUMENT, "NULL k or q of the BC list");
-    if ((kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_VELOCITY_BOUNCE_BACK) &&
+    if ((kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_VELOCITY_BOUNCE_BACK ||
+         kind == VFB_BC_VELOCITY_WITH_PRESSURE) &&
         (!list->Vx || !list->Vy || !list->Vz))
         return setError(VFB_ERR_INVALID_ARGUMENT, "velocity BC needs Vx, Vy, Vz");
-    if ((kind == VFB_BC_NOSLIP_INTERPOLATED || kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_SLIP) &&
+    if ((kind == VFB_BC_NOSLIP_INTERPOLATED || kind == VFB_BC_VELOCITY_INTERPOLATED || kind == VFB_BC_SLIP ||
+         kind == VFB_BC_VELOCITY_WITH_PRESSURE) &&
         !(lattice->omega > 0.0 && lattice->omega < 2.0 && lattice->omega != 1.0))
         return setError(VFB_ERR_INVALID_ARGUMENT, "omega %g outside (0, 2) or equal to 1 (the interpolation divides by 1 - omega)",
                         lattice->omega);

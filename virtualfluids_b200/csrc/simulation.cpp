@@ -461,7 +461,8 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", P.storage);
     if (P.collisionKernel != 0 && P.collisionKernel != 1)
         return setError(VFB_ERR_INVALID_ARGUMENT, "unknown collision kernel %d", P.collisionKernel);
-    if (P.velocityBC != VFB_BC_VELOCITY_INTERPOLATED && P.velocityBC != VFB_BC_VELOCITY_BOUNCE_BACK)
+    if (P.velocityBC != VFB_BC_VELOCITY_INTERPOLATED && P.velocityBC != VFB_BC_VELOCITY_BOUNCE_BACK &&
+        P.velocityBC != VFB_BC_VELOCITY_WITH_PRESSURE)
         return setError(VFB_ERR_INVALID_ARGUMENT, "velocityBC must be a velocity kind");
     if (!validKind(P.noSlipBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
         !validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||

@@ -40,6 +40,7 @@ class VfbSimParams(ctypes.Structure):
 class VelocityBC(enum.IntEnum):
     VelocityInterpolatedCompressible = _lib.BC_VELOCITY_INTERPOLATED
     VelocityBounceBack = _lib.BC_VELOCITY_BOUNCE_BACK
+    VelocityWithPressureInterpolatedCompressible = _lib.BC_VELOCITY_WITH_PRESSURE
 
 
 class NoSlipBC(enum.IntEnum):
