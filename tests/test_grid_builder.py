@@ -150,3 +150,32 @@ def test_sphere_through_the_builder_api():
     b.setNoSlipBoundaryCondition(vgrid.SideType.GEOMETRY)
     z = np.load(GOLDEN / "grid_sphere_channel.npz")
     compare(b.arrays(), [{k.split(":", 1)[1]: z[k] for k in z.files}])
+
+
+def _spec_with(**kv):
+    s = np.zeros(64)
+    s[0:7] = [0, 0, 0, 15, 11, 9, 1.0]
+    for k, v in kv.items():
+        i = int(k[1:])
+        s[i:i + np.size(v)] = v
+    return s
+
+
+@pytest.mark.parametrize("bad", [
+    {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s60": 1},          # thin walls with a solid: not supported
+    {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s26": 2},          # velocity BC on the geometry: not supported
+    {"s30": [7, 1, 0, 0, 0]},                                 # side id outside 0..5
+    {"s30": [0, 9, 0, 0, 0]},                                 # unknown BC type
+])
+def test_builder_rejects_unsupported_specs(bad):
+    from virtualfluids_b200 import _lib
+    with pytest.raises(_lib.VfbError):
+        build_mine(_spec_with(**bad))
+
+
+def test_builder_rejects_short_spec():
+    import ctypes
+    from virtualfluids_b200 import _lib
+    s = np.zeros(40)
+    h = _lib.lib().vfb_grid_build(s.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(s))
+    assert not h
