@@ -329,6 +329,8 @@ typedef struct vfb_sim_params {
     double quadricLimiters[3]; /* default 0.01 each (Parameter.cpp:69) */
     int usePlan;               /* 1: the planned (bulk-copy) collision kernels */
     int useGraphs;             /* 1: replay two coarse steps at a time from a captured CUDA graph */
+    int useInitNeq;            /* 1: vfb_sim_init_level writes equilibrium plus the strain-rate part
+                                  (Parameter::setUseInitNeq); the grid must carry neighborNeg */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;
@@ -336,8 +338,9 @@ typedef struct vfb_simulation vfb_simulation;
 int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simulation** sim, void* stream);
 int vfb_sim_destroy(vfb_simulation* sim);
 int vfb_sim_levels(const vfb_simulation* sim);
-/* equilibrium from host arrays (compute precision, numberOfLBnodes of the
- * level) into both parity views, odd then even (PreProcessorImp.cpp:50-58) */
+/* equilibrium (or, with useInitNeq, non-equilibrium) populations from host
+ * arrays (compute precision, numberOfLBnodes of the level) into both parity
+ * views, odd then even (PreProcessorImp.cpp:50-58) */
 int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rho, const void* vx, const void* vy, const void* vz,
                        void* stream);
 /* coarse time steps (each runs 2^l substeps of level l).  With useGraphs,
@@ -374,6 +377,24 @@ int vfb_init_equilibrium(int storage, void* distributions, unsigned long long nu
                          const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
                          const void* rho, const void* vx, const void* vy, const void* vz, int isEvenTimestep,
                          void* stream);
+
+/*
+ * Non-equilibrium initialisation of one parity view: the equilibrium of
+ * (drho, u) plus the first-order strain-rate part built from the central
+ * differences of u over the six axis neighbours (the negative ones reached
+ * through neighborInverse, the -x-y-z neighbour, and two positive steps).
+ * Replaces InitNavierStokesCompressibleNonEquilibrium_Device
+ * (src/gpu/core/PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cu:216-500),
+ * which InitNavierStokesCompressible::init (InitNavierStokesCompressible.cu:63-83)
+ * launches when Parameter::getUseInitNeq() is set.  Nodes whose geo is
+ * GEO_SOLID or GEO_VOID get 96 in their rest population, as in the reference
+ * (FP16 storage: its largest finite value, 96 being out of its scaled range).
+ * omega in (0, 2).
+ */
+int vfb_init_nonequilibrium(int storage, void* distributions, unsigned long long numberOfLBnodes, const uint32_t* geo,
+                            const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                            const uint32_t* neighborInverse, const void* rho, const void* vx, const void* vy,
+                            const void* vz, double omega, int isEvenTimestep, void* stream);
 
 /*
  * drho and velocity of every node from the populations of the given parity
@@ -430,6 +451,14 @@ int vfb_debug_side_qs(int side, const int* alreadySet, int nSet, double* q27);
  */
 int vfb_debug_collide_node(int op, int precision, double* f27, double omega, const double* limiters,
                            const double* force, double* out4);
+/*
+ * One node of the non-equilibrium initialisation on the host with the code
+ * the kernel runs: drhoVelocity4 = drho, vx, vy, vz; gradient9[3a + b] =
+ * d u_a / d x_b; f27 out, direction order.  precision: VFB_FP64 or VFB_FP32.
+ * No counterpart in the reference.
+ */
+int vfb_debug_init_nonequilibrium_node(int precision, const double* drhoVelocity4, const double* gradient9,
+                                       double omega, double* f27);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,9 @@ class Oracle(_Lib):
         self.fn("vfo_bgk_collide").argtypes = [_vp, R]
         self.fn("vfo_collision_bgk").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, R, _c.c_int]
         self.fn("vfo_init_eq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_int]
+        self.fn("vfo_init_noneq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, R,
+                                              _c.c_int]
+        self.fn("vfo_noneq_node").argtypes = [R, R, R, R, _vp, R, _vp]
         self.fn("vfo_bc_post").argtypes = [_c.c_int, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _c.c_uint32, R, _vp,
                                            _vp, _vp, _c.c_int]
         self.fn("vfo_bc_pressure_noneq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
@@ -75,6 +78,15 @@ class Oracle(_Lib):
         self.fn("vfo_bgk_collide")(_ptr(f), omega)
         return f
 
+    def noneq_node(self, drho, vx, vy, vz, grad, omega):
+        """Equilibrium plus non-equilibrium populations of one node (27,
+        canonical direction order) from the velocity gradient grad[a][b] =
+        d u_a / d x_b."""
+        g = np.ascontiguousarray(grad, dtype=self.real).reshape(9)
+        f = np.zeros(27, self.real)
+        self.fn("vfo_noneq_node")(drho, vx, vy, vz, _ptr(g), omega, _ptr(f))
+        return f
+
     # -- whole-lattice passes (arrays modified in place) ----------------------
     def collision_k17(self, dist, N, nx, ny, nz, fluid, omega, forces=(0, 0, 0), force_factor=1.0,
                       limiters=(0.01, 0.01, 0.01), is_even=True, flags=0, macro=None, body=None):
@@ -92,6 +104,10 @@ class Oracle(_Lib):
     def init_eq(self, dist, N, geo, nx, ny, nz, rho, ux, uy, uz, is_even):
         self.fn("vfo_init_eq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(rho), _ptr(ux),
                                _ptr(uy), _ptr(uz), int(is_even))
+
+    def init_noneq(self, dist, N, geo, nx, ny, nz, nneg, rho, ux, uy, uz, omega, is_even):
+        self.fn("vfo_init_noneq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(nneg), _ptr(rho),
+                                  _ptr(ux), _ptr(uy), _ptr(uz), omega, int(is_even))
 
     def bc_post(self, kind, dist, N, nx, ny, nz, k, q, omega, vx=None, vy=None, vz=None, is_even=True):
         self.fn("vfo_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,
@@ -125,6 +141,8 @@ class Reference(_Lib):
                                                    _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         self.fn("vfref_collision_bgk").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, R, _c.c_int]
         self.fn("vfref_init_eq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_int]
+        self.fn("vfref_init_noneq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                R, _c.c_int]
         self.fn("vfref_bc_post").argtypes = [_c.c_int, _vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _c.c_uint, R, _vp,
                                              _vp, _vp, _c.c_int]
         self.fn("vfref_bc_pressure_noneq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint,
@@ -179,6 +197,10 @@ class Reference(_Lib):
     def init_eq(self, dist, N, geo, nx, ny, nz, rho, ux, uy, uz, is_even):
         self.fn("vfref_init_eq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(rho), _ptr(ux),
                                  _ptr(uy), _ptr(uz), int(is_even))
+
+    def init_noneq(self, dist, N, geo, nx, ny, nz, nneg, rho, ux, uy, uz, omega, is_even):
+        self.fn("vfref_init_noneq")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), _ptr(nneg), _ptr(rho),
+                                    _ptr(ux), _ptr(uy), _ptr(uz), omega, int(is_even))
 
     def bc_post(self, kind, dist, N, nx, ny, nz, k, q, omega, vx=None, vy=None, vz=None, is_even=True):
         self.fn("vfref_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,

@@ -108,6 +108,17 @@ void REF(vfref_init_eq)(real* dist, unsigned long long N, unsigned* geo, unsigne
     }
 }
 
+// InitNavierStokesCompressibleNonEquilibrium_Device for one parity
+void REF(vfref_init_noneq)(real* dist, unsigned long long N, unsigned* geo, unsigned* nx, unsigned* ny, unsigned* nz,
+                           unsigned* nneg, real* rho, real* ux, real* uy, real* uz, real omega, int isEven)
+{
+    for (unsigned long long t = 0; t < N; ++t) {
+        setThread(t);
+        InitNavierStokesCompressibleNonEquilibrium_Device(nx, ny, nz, nneg, geo, rho, ux, uy, uz, (unsigned)N, dist,
+                                                          omega, isEven != 0);
+    }
+}
+
 // post-collision BC kernels; kind: 0 no-slip interpolated, 1 no-slip
 // bounce-back, 2 velocity interpolated, 3 velocity bounce-back, 4 slip,
 // 5 velocity with pressure interpolated

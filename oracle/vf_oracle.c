@@ -19,6 +19,7 @@
  *                                B92CompressibleNavierStokes_Device.cu:41-274
  *   - equilibrium init           src/gpu/core/PreProcessor/PreProcessorStrategy/
  *                                InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cu:44-212
+ *   - non-equilibrium init       InitNavierStokesCompressible_Device.cu:216-500
  *   - BC formulas                KernelUtilities.h:171-214 and the BC kernels in
  *                                src/gpu/core/BoundaryConditions/{NoSlip,Velocity,Slip,Pressure}/
  *
@@ -612,6 +613,86 @@ void FN(vfo_init_eq)(real *dist, uint64_t N, const uint32_t *geo, const uint32_t
         real f[27];
         for (int d = 0; d < 27; ++d)
             f[d] = feq_full(d, drho, vx1, vx2, vx3, cu_sq);
+        scatter_pre(dist, N, &L, isEven, f);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* non-equilibrium init (InitNavierStokesCompressible_Device.cu:216-500)     */
+/* ------------------------------------------------------------------------ */
+/* Coefficient slot of each direction: opposite directions share one
+ * non-equilibrium value (:460-486).  Slots: 0 rest, 1-3 the x, y, z axes,
+ * 4 xy same sign, 5 xy opposite, 6 xz same, 7 xz opposite, 8 yz same,
+ * 9 yz opposite, 10 PPP/MMM, 11 PPM/MMP, 12 PMP/MPM, 13 PMM/MPP. */
+static const int NEQ_SLOT[27] = { 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 9, 9, 10, 13, 12, 11, 11, 12, 13, 10 };
+
+/* The fourteen non-equilibrium coefficients from the central-difference
+ * velocity gradient g[a][b] = d u_a / d x_b (:378-425, the strain part of the
+ * Chapman-Enskog expansion at first order).  The reference spells them with
+ * double literals, so every product with a literal is formed in double even
+ * when real is float, while sums of two gradients in parentheses stay in real;
+ * each coefficient is rounded to real once.  Its factors eps_new and op are 1
+ * and multiply exactly; they are left out. */
+static void noneq_coefficients(const real g[3][3], real omega, real c[14])
+{
+    const real ax = g[0][0], ay = g[0][1], az = g[0][2];
+    const real bx = g[1][0], by = g[1][1], bz = g[1][2];
+    const real cx = g[2][0], cy = g[2][1], cz = g[2][2];
+    const real o = omega;
+    c[1] = (real)((5. * ax * o + 5. * by * o + 5. * cz * o - 8. * ax + 4. * by + 4. * cz) / (54. * o));
+    c[2] = (real)(c[1] + (2. * (ax - by)) / (9. * o));
+    c[3] = (real)(c[1] + (2. * (ax - cz)) / (9. * o));
+    c[4] = (real)(-(5. * cz * o + 3. * (ay + bx) - 2. * cz + ax * (5. * o + 1.) + by * (5. * o + 1.)) / (54. * o));
+    c[5] = (real)(c[4] + (ay + bx) / (9. * o));
+    c[6] = (real)(-(5. * cz * o + by * (5. * o - 2.) + 3. * (az + cx) + cz + ax * (5. * o + 1.)) / (54. * o));
+    c[7] = (real)(c[6] + (az + cx) / (9. * o));
+    c[8] = (real)(-(5. * ax * o + 5. * by * o + 5. * cz * o - 2. * ax + by + 3. * bz + 3. * cy + cz) / (54. * o));
+    c[9] = (real)(c[8] + (bz + cy) / (9. * o));
+    c[0] = (real)((5. * (ax + by + cz)) / 9.);
+    c[10] = (real)(-(ay + az + bx + bz + cx + cy) / (72. * o));
+    c[11] = (real)(-c[10] - (ay + bx) / (36. * o));
+    c[12] = (real)(-c[10] - (az + cx) / (36. * o));
+    c[13] = (real)(-c[10] - (bz + cy) / (36. * o));
+}
+
+/* one node: equilibrium of (drho, u) plus (1 + drho) times the coefficient of
+ * each direction's slot (:428-486), in canonical direction order */
+void FN(vfo_noneq_node)(real drho, real vx1, real vx2, real vx3, const real *grad9, real omega, real *f)
+{
+    real g[3][3], c[14];
+    for (int a = 0; a < 9; ++a)
+        g[a / 3][a % 3] = grad9[a];
+    noneq_coefficients(g, omega, c);
+    const real cu_sq = C(3, 2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+    for (int d = 0; d < 27; ++d) {
+        const real eq = feq_full(d, drho, vx1, vx2, vx3, cu_sq);
+        f[d] = eq + ((real)1 + drho) * c[NEQ_SLOT[d]];
+    }
+}
+
+void FN(vfo_init_noneq)(real *dist, uint64_t N, const uint32_t *geo, const uint32_t *nx, const uint32_t *ny,
+                        const uint32_t *nz, const uint32_t *nneg, const real *rho, const real *ux, const real *uy,
+                        const real *uz, real omega, int isEven)
+{
+    const real *u[3] = { ux, uy, uz };
+    for (uint64_t kk = 0; kk < N; ++kk) {
+        const uint32_t k = (uint32_t)kk;
+        if (geo[k] == GEO_SOLID || geo[k] == GEO_VOID) {
+            dist[k] = (real)96; /* the rest population of a solid node is set to 96 (:490-499) */
+            continue;
+        }
+        /* axis neighbours; the negative ones through the inverse (-x-y-z)
+         * neighbour and two positive steps (:347-353) */
+        const uint32_t w = nneg[k];
+        const uint32_t plus[3] = { nx[k], ny[k], nz[k] };
+        const uint32_t minus[3] = { nz[ny[w]], nz[nx[w]], ny[nx[w]] };
+        real grad[9];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                grad[3 * a + b] = (u[a][plus[b]] - u[a][minus[b]]) / (real)2;
+        real f[27];
+        FN(vfo_noneq_node)(rho[k], ux[k], uy[k], uz[k], grad, omega, f);
+        locs8 L = list_indices(k, nx, ny, nz);
         scatter_pre(dist, N, &L, isEven, f);
     }
 }

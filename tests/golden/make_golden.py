@@ -6,7 +6,8 @@ outputs as .npz files.  The parity tests compare the oracle and the
 repository's grid builder against these files, so the pin also holds on a
 machine without the reference tree.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                 (all fixtures)
+    python tests/golden/make_golden.py --init-noneq    (the non-equilibrium init only)
 """
 from __future__ import annotations
 
@@ -78,13 +79,37 @@ def lattice(precision: str) -> None:
     np.savez_compressed(OUT / f"lattice_channel_{precision}.npz", dist=dist)
 
 
+def init_noneq(precision: str) -> None:
+    """InitNavierStokesCompressibleNonEquilibrium_Device over the channel
+    grid (walls, inflow and outflow planes) for both parity views, from
+    seeded fields."""
+    R = Reference(precision)
+    real = np.float64 if precision == "f64" else np.float32
+    g = R.grid(grid_spec("channel"))[0]
+    N = len(g["geo"])
+    rng = np.random.default_rng(20261203)
+    fields = [rng.uniform(-0.02, 0.02, N).astype(real) for _ in range(4)]
+    omega = real(1.6)
+    dist = np.zeros(27 * N, real)
+    for ev in (0, 1):
+        R.init_noneq(dist, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], g["neighborNeg"], *fields,
+                     omega, ev)
+    np.savez_compressed(OUT / f"init_noneq_channel_{precision}.npz", rho=fields[0], vx=fields[1], vy=fields[2],
+                        vz=fields[3], omega=np.array(omega), dist=dist)
+
+
 if __name__ == "__main__":
     if len(sys.argv) == 3 and sys.argv[1] == "--refined":
         refined_grid(sys.argv[2])
         sys.exit(0)
+    if len(sys.argv) == 2 and sys.argv[1] == "--init-noneq":
+        for p in ("f64", "f32"):
+            init_noneq(p)
+        sys.exit(0)
     for p in ("f64", "f32"):
         k17_nodes(p)
         lattice(p)
+        init_noneq(p)
     grids()
     refined_grids()
     for f in sorted(OUT.glob("*.npz")):

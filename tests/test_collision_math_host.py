@@ -62,3 +62,45 @@ def test_rest_state_is_a_fixed_point():
     got, m = lib_node(0, _lib.FP64, np.zeros(27), 1.9, (0.01,) * 3, (0, 0, 0))
     assert np.abs(got).max() < 1e-17
     assert np.abs(m).max() < 1e-17
+
+
+def lib_noneq_node(precision, drho_u, grad, omega):
+    dv = np.ascontiguousarray(drho_u, dtype=np.float64)
+    g = np.ascontiguousarray(grad, dtype=np.float64).reshape(9)
+    f = np.zeros(27)
+    rc = _lib.lib().vfb_debug_init_nonequilibrium_node(precision, dv.ctypes.data_as(D), g.ctypes.data_as(D), omega,
+                                                       f.ctypes.data_as(D))
+    assert rc == 0, _lib.last_error()
+    return f
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_noneq_init_node_matches_oracle_bit_for_bit(precision):
+    """The non-equilibrium init's node arithmetic (the kernel's own code, run
+    on the host) equals the oracle exactly: it performs the reference's
+    operations in the reference's order, double products included in FP32.
+    Mass and momentum of the non-equilibrium part vanish."""
+    O = Oracle(precision)
+    p = _lib.FP64 if precision == "f64" else _lib.FP32
+    rng = np.random.default_rng(31)
+    c = np.array([[0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1],
+                  [0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, -1],
+                  [0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, 1, 1, 1, -1, -1, -1, -1]])
+    for t in range(200):
+        drho_u = rng.uniform(-0.03, 0.03, 4).astype(O.real)
+        grad = rng.uniform(-1e-2, 1e-2, 9).astype(O.real)
+        omega = O.real(rng.uniform(0.3, 1.99))
+        ref = O.noneq_node(*drho_u, grad.reshape(3, 3), omega)
+        got = lib_noneq_node(p, drho_u, grad, float(omega))
+        assert np.array_equal(got.astype(O.real), ref), t
+        neq = ref.astype(np.float64) - O.noneq_node(*drho_u, np.zeros((3, 3)), omega).astype(np.float64)
+        scale = np.abs(neq).max()
+        assert abs(neq.sum()) <= 1e-5 * scale and np.abs(c @ neq).max() <= 1e-5 * scale, t
+
+
+def test_noneq_init_node_rejects_bad_arguments():
+    f = np.zeros(27)
+    assert _lib.lib().vfb_debug_init_nonequilibrium_node(_lib.FP16, f.ctypes.data_as(D), f.ctypes.data_as(D), 1.0,
+                                                         f.ctypes.data_as(D)) != 0
+    assert _lib.lib().vfb_debug_init_nonequilibrium_node(_lib.FP64, None, f.ctypes.data_as(D), 1.0,
+                                                         f.ctypes.data_as(D)) != 0

@@ -38,16 +38,20 @@ def channel():
     return b
 
 
-def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, velocity_kind=2):
-    """UpdateGrid27::updateGrid for one level, on the oracle."""
+def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, velocity_kind=2, init_neq=False):
+    """UpdateGrid27::updateGrid for one level, on the oracle (initialised by
+    the equilibrium, or with init_neq by the non-equilibrium init)."""
     O = Oracle(precision)
     real = O.real
     N = len(g["geo"])
     nx, ny, nz, geo, fl = g["neighborX"], g["neighborY"], g["neighborZ"], g["geo"], g["fluid"]
     d = np.zeros(27 * N, real)
-    for ev in (0, 1):
-        O.init_eq(d, N, geo, nx, ny, nz, *[a.astype(real) for a in init], ev)
     om = 1.0 / (3.0 * nu + 0.5)
+    for ev in (0, 1):
+        if init_neq:
+            O.init_noneq(d, N, geo, nx, ny, nz, g["neighborNeg"], *[a.astype(real) for a in init], real(om), ev)
+        else:
+            O.init_eq(d, N, geo, nx, ny, nz, *[a.astype(real) for a in init], ev)
     vel = [g[f"velocity.{c}"].astype(real) for c in ("vx", "vy", "vz")]
     even = True
     for _ in range(steps):

@@ -126,3 +126,49 @@ def test_velocity_with_pressure_bc_matches_live_reference(precision, grid, lst, 
         assert (d != before).sum() > n
         out.append(d)
     assert np.array_equal(out[0], out[1])
+
+
+def _channel_level0():
+    with np.load(GOLDEN / "grid_channel.npz") as z:
+        return {k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_init_noneq_matches_golden(precision):
+    """The non-equilibrium init (both parity views) on the channel grid
+    equals the fixture made by the reference's kernel built for the host."""
+    g = _channel_level0()
+    ref = np.load(GOLDEN / f"init_noneq_channel_{precision}.npz")
+    O = Oracle(precision)
+    N = len(g["geo"])
+    d = np.zeros(27 * N, O.real)
+    for ev in (0, 1):
+        O.init_noneq(d, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], g["neighborNeg"], ref["rho"],
+                     ref["vx"], ref["vy"], ref["vz"], ref["omega"][()], ev)
+    assert np.array_equal(d, ref["dist"])
+    # the rest population of every solid node carries the reference's marker
+    solid = (g["geo"] == 15) | (g["geo"] == 16)
+    assert solid.any() and np.all(d[:N][solid] == 96)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("grid", ["channel", "sphere_channel", "cavity8"])
+@pytest.mark.parametrize("omega", [1.6, 0.7])
+def test_init_noneq_matches_live_reference(precision, grid, omega):
+    """InitNavierStokesCompressibleNonEquilibrium_Device: the oracle equals
+    the reference's kernel built for the host, bit for bit, including the
+    double-literal products of the single-precision build."""
+    g = _golden_level0(grid)
+    O, R = Oracle(precision), Reference(precision)
+    N = len(g["geo"])
+    rng = np.random.default_rng(41)
+    fields = [rng.uniform(-0.02, 0.02, N).astype(O.real) for _ in range(4)]
+    out = []
+    for impl in (O, R):
+        d = np.zeros(27 * N, O.real)
+        for ev in (0, 1):
+            impl.init_noneq(d, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], g["neighborNeg"], *fields,
+                            O.real(omega), ev)
+        out.append(d)
+    assert np.array_equal(out[0], out[1])

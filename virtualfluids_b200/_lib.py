@@ -123,6 +123,10 @@ _SIGNATURES = [
      [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
       ctypes.c_void_p]),
+    ("vfb_init_nonequilibrium", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_double, ctypes.c_int, ctypes.c_void_p]),
     ("vfb_macroscopic", ctypes.c_int,
      [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -171,6 +175,9 @@ _SIGNATURES = [
     ("vfb_debug_collide_node", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.POINTER(ctypes.c_double),
       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("vfb_debug_init_nonequilibrium_node", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+      ctypes.POINTER(ctypes.c_double)]),
     ("vfb_debug_side_qs", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),

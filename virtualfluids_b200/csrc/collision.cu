@@ -1,5 +1,6 @@
 // collision.cu -- fused collide + esoteric-twist stream kernels (K17, BGK),
-// equilibrium initialisation, macroscopic output and FP64 reductions.
+// equilibrium and non-equilibrium initialisation, macroscopic output and FP64
+// reductions.
 //
 // One thread updates one fluid node: it follows the reference's index chain
 // (ListIndices, src/gpu/core/Utilities/KernelUtilities.h:221-245) to the
@@ -153,6 +154,114 @@ __global__ void initEqKernel(S* dist, unsigned long long N, const uint32_t* __re
         const R cu = cdot<R>(d, vx1, vx2, vx3);
         f[d] = weight<R>(d) * (drho + (R(1) + drho) * (R(3) * cu + R(4.5) * cu * cu - cu_sq));
     }
+    const Locs L = listIndices((uint32_t)k, nX, nY, nZ);
+    scatterPre<S, EVEN>(f, dist, N, L);
+}
+
+// Non-equilibrium initialisation, InitNavierStokesCompressible_Device.cu:216-500.
+// Opposite directions share one non-equilibrium coefficient (:460-486).
+// Slots: 0 rest, 1-3 the x, y, z axes, 4 / 5 xy same / opposite signs, 6 / 7
+// xz, 8 / 9 yz, 10 PPP/MMM, 11 PPM/MMP, 12 PMP/MPM, 13 PMM/MPP.
+__host__ __device__ constexpr int noneqSlot(int d)
+{
+    constexpr int t[27] = { 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 9, 9, 10, 13, 12, 11, 11, 12, 13, 10 };
+    return t[d];
+}
+
+// The fourteen first-order (strain-rate) non-equilibrium coefficients from the
+// central-difference velocity gradient g[a][b] = d u_a / d x_b (:378-425).
+// The reference writes them with double literals, so in its single-precision
+// build too every product with a literal is a double product, sums of two
+// gradients in parentheses stay in the working precision, and each
+// coefficient is rounded to the working precision once; the code below keeps
+// that, so FP32 follows that build.  The reference's factors eps_new and op
+// are 1 and multiply exactly; they are left out.
+template <class R>
+__host__ __device__ inline void noneqCoefficients(const R g[3][3], R omega, R c[14])
+{
+    const R ax = g[0][0], ay = g[0][1], az = g[0][2];
+    const R bx = g[1][0], by = g[1][1], bz = g[1][2];
+    const R cx = g[2][0], cy = g[2][1], cz = g[2][2];
+    const double o = (double)omega;
+    const double five = 5.0 * o;
+    c[1] = R((5.0 * ax * o + 5.0 * by * o + 5.0 * cz * o - 8.0 * ax + 4.0 * by + 4.0 * cz) / (54.0 * o));
+    c[2] = R(c[1] + (2.0 * (ax - by)) / (9.0 * o));
+    c[3] = R(c[1] + (2.0 * (ax - cz)) / (9.0 * o));
+    c[4] = R(-(5.0 * cz * o + 3.0 * (ay + bx) - 2.0 * cz + ax * (five + 1.0) + by * (five + 1.0)) / (54.0 * o));
+    c[5] = R(c[4] + (ay + bx) / (9.0 * o));
+    c[6] = R(-(5.0 * cz * o + by * (five - 2.0) + 3.0 * (az + cx) + cz + ax * (five + 1.0)) / (54.0 * o));
+    c[7] = R(c[6] + (az + cx) / (9.0 * o));
+    c[8] = R(-(5.0 * ax * o + 5.0 * by * o + 5.0 * cz * o - 2.0 * ax + by + 3.0 * bz + 3.0 * cy + cz) / (54.0 * o));
+    c[9] = R(c[8] + (bz + cy) / (9.0 * o));
+    c[0] = R((5.0 * (ax + by + cz)) / 9.0);
+    c[10] = R(-(ay + az + bx + bz + cx + cy) / (72.0 * o));
+    c[11] = R(-c[10] - (ay + bx) / (36.0 * o));
+    c[12] = R(-c[10] - (az + cx) / (36.0 * o));
+    c[13] = R(-c[10] - (bz + cy) / (36.0 * o));
+}
+
+// equilibrium of (drho, u) plus (1 + drho) times each direction's
+// non-equilibrium coefficient (:428-486), canonical direction order
+template <class R>
+__host__ __device__ inline void noneqNode(R drho, R vx1, R vx2, R vx3, const R g[3][3], R omega, R* f)
+{
+    R c[14];
+    noneqCoefficients<R>(g, omega, c);
+    const R cu_sq = R(1.5) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+    const R rho1 = R(1) + drho;
+    f[d000] = weight<R>(d000) * (drho - cu_sq * rho1) + rho1 * c[0];
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const R cu = cdot<R>(d, vx1, vx2, vx3);
+        const R eq = weight<R>(d) * (drho + rho1 * (R(3) * cu + R(4.5) * cu * cu - cu_sq));
+        f[d] = eq + rho1 * c[noneqSlot(d)];
+    }
+}
+
+// The reference sets the rest population of a solid or void node to 96
+// (:490-499).  Scaled FP16 cannot hold 96 (its range ends near 16), so it
+// stores the largest finite value instead.
+template <class S>
+__device__ __forceinline__ void storeSolidMarker(S* p)
+{
+    if constexpr (Storage<S>::scaled)
+        Storage<S>::storeRaw(p, 65504.0f);
+    else
+        Storage<S>::store(p, typename Storage<S>::R(96));
+}
+
+template <class S, bool EVEN>
+__global__ void initNoneqKernel(S* dist, unsigned long long N, const uint32_t* __restrict__ geo,
+                                const uint32_t* __restrict__ nX, const uint32_t* __restrict__ nY,
+                                const uint32_t* __restrict__ nZ, const uint32_t* __restrict__ nNeg,
+                                const typename Storage<S>::R* rho, const typename Storage<S>::R* ux,
+                                const typename Storage<S>::R* uy, const typename Storage<S>::R* uz,
+                                typename Storage<S>::R omega)
+{
+    using R = typename Storage<S>::R;
+    const unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N)
+        return;
+    const uint32_t type = geo[k];
+    if (type == 15u || type == 16u) {
+        storeSolidMarker<S>(dist + k);
+        return;
+    }
+    // axis neighbours; the negative ones through the inverse (-x-y-z)
+    // neighbour and two positive steps (:347-353)
+    const uint32_t w = __ldg(nNeg + k);
+    const uint32_t wx = __ldg(nX + w);
+    const uint32_t plus[3] = { __ldg(nX + k), __ldg(nY + k), __ldg(nZ + k) };
+    const uint32_t minus[3] = { __ldg(nZ + __ldg(nY + w)), __ldg(nZ + wx), __ldg(nY + wx) };
+    const R* u[3] = { ux, uy, uz };
+    R g[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            g[a][b] = (u[a][plus[b]] - u[a][minus[b]]) / R(2);
+    R f[27];
+    noneqNode<R>(rho[k], ux[k], uy[k], uz[k], g, omega, f);
     const Locs L = listIndices((uint32_t)k, nX, nY, nZ);
     scatterPre<S, EVEN>(f, dist, N, L);
 }
@@ -350,6 +459,25 @@ static int launchInit(void* dist, unsigned long long N, const uint32_t* geo, con
 }
 
 template <class S>
+static int launchInitNoneq(void* dist, unsigned long long N, const uint32_t* geo, const uint32_t* nX,
+                           const uint32_t* nY, const uint32_t* nZ, const uint32_t* nNeg, const void* rho,
+                           const void* vx, const void* vy, const void* vz, double omega, int even,
+                           cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    const unsigned blocks = (unsigned)((N + 127) / 128);
+    const R* f[4] = { static_cast<const R*>(rho), static_cast<const R*>(vx), static_cast<const R*>(vy),
+                      static_cast<const R*>(vz) };
+    if (even)
+        initNoneqKernel<S, true><<<blocks, 128, 0, stream>>>(static_cast<S*>(dist), N, geo, nX, nY, nZ, nNeg, f[0],
+                                                             f[1], f[2], f[3], (R)omega);
+    else
+        initNoneqKernel<S, false><<<blocks, 128, 0, stream>>>(static_cast<S*>(dist), N, geo, nX, nY, nZ, nNeg, f[0],
+                                                              f[1], f[2], f[3], (R)omega);
+    return checkLaunch("init non-equilibrium");
+}
+
+template <class S>
 static int launchMacro(const void* dist, unsigned long long N, const uint32_t* geo, const uint32_t* nX,
                        const uint32_t* nY, const uint32_t* nZ, int even, void* rho, void* vx, void* vy, void* vz,
                        cudaStream_t stream)
@@ -432,6 +560,30 @@ extern "C" int vfb_init_equilibrium(int storage, void* distributions, unsigned l
     case VFB_FP64: return launchInit<double>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_FP16: return launchInit<__half>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_BF16: return launchInit<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+
+extern "C" int vfb_init_nonequilibrium(int storage, void* distributions, unsigned long long N, const uint32_t* geo,
+                                       const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
+                                       const uint32_t* neighborInverse, const void* rho, const void* vx, const void* vy,
+                                       const void* vz, double omega, int isEven, void* stream)
+{
+    clearError();
+    if (!distributions || !geo || !nX || !nY || !nZ || !neighborInverse || !rho || !vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (N < 2 || N > 0xffffffffull)
+        return setError(VFB_ERR_OUT_OF_RANGE, "numberOfLBnodes %llu outside [2, 2^32)", N);
+    if (!(omega > 0.0 && omega < 2.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "omega %g outside (0, 2)", omega);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint32_t* w = neighborInverse;
+    switch (storage) {
+    case VFB_FP32: return launchInitNoneq<float>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
+    case VFB_FP64: return launchInitNoneq<double>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
+    case VFB_FP16: return launchInitNoneq<__half>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
+    case VFB_BF16:
+        return launchInitNoneq<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
 }
@@ -549,4 +701,39 @@ extern "C" int vfb_debug_collide_node(int op, int precision, double* f27, double
         return VFB_OK;
     }
     return setError(VFB_ERR_INVALID_ARGUMENT, "precision must be VFB_FP64 or VFB_FP32");
+}
+
+namespace
+{
+template <class R>
+void noneqNodeHost(const double* drhoVelocity4, const double* gradient9, double omega, double* f27)
+{
+    R g[3][3], f[27];
+    for (int i = 0; i < 9; ++i)
+        g[i / 3][i % 3] = (R)gradient9[i];
+    noneqNode<R>((R)drhoVelocity4[0], (R)drhoVelocity4[1], (R)drhoVelocity4[2], (R)drhoVelocity4[3], g, (R)omega, f);
+    for (int d = 0; d < 27; ++d)
+        f27[d] = f[d];
+}
+} // namespace
+
+/*
+ * One node of the non-equilibrium initialisation evaluated on the host with
+ * the code the kernel runs: drhoVelocity4 = drho, vx, vy, vz; gradient9[3a+b]
+ * = d u_a / d x_b; f27 = the 27 populations in direction order.  precision:
+ * VFB_FP64 or VFB_FP32 (inputs are rounded to it).  For tests without a GPU.
+ */
+extern "C" int vfb_debug_init_nonequilibrium_node(int precision, const double* drhoVelocity4, const double* gradient9,
+                                                  double omega, double* f27)
+{
+    clearError();
+    if (!drhoVelocity4 || !gradient9 || !f27)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (precision == VFB_FP64)
+        noneqNodeHost<double>(drhoVelocity4, gradient9, omega, f27);
+    else if (precision == VFB_FP32)
+        noneqNodeHost<float>(drhoVelocity4, gradient9, omega, f27);
+    else
+        return setError(VFB_ERR_INVALID_ARGUMENT, "precision must be VFB_FP64 or VFB_FP32");
+    return VFB_OK;
 }

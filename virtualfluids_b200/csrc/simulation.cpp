@@ -64,6 +64,7 @@ struct Level {
     unsigned long long N = 0;
     uint32_t nFluid = 0;
     DeviceBuffer dist, nX, nY, nZ, geo, fluid;
+    DeviceBuffer nNeg; // the -x-y-z neighbour, uploaded for the non-equilibrium init only
     BcListDevice velocity, noSlip, slip, geometry;
     std::vector<PressureListDevice*> pressure;
     InterfaceDevice coarseToFine, fineToCoarse;
@@ -482,6 +483,18 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         auto* L = new Level;
         S->levels.push_back(L);
         rc = uploadLevel(*L, grid, l, P.storage, s, keep);
+        if (rc == VFB_OK && P.useInitNeq) {
+            std::vector<char> nn;
+            long long count = 0;
+            int es = 0;
+            if (!gridArray(grid, l, "neighborNeg", nn, count, es) || es != 4 || (unsigned long long)count != L->N)
+                rc = setError(VFB_ERR_CONFIGURATION, "grid level %d: array neighborNeg (needed by useInitNeq)", l);
+            else {
+                keep.push_back(std::move(nn));
+                if (uploadRaw(L->nNeg, keep.back().data(), keep.back().size(), s) != cudaSuccess)
+                    rc = setError(VFB_ERR_CUDA, "neighborNeg upload failed");
+            }
+        }
         // Parameter::initLBMSimulationParameter (Parameter.cpp:395-420)
         const double nu = P.viscosity * std::pow(2.0, l);
         L->omega = 1.0 / (3.0 * nu + 0.5);
@@ -595,11 +608,20 @@ extern "C" int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rh
         if (uploadRaw(f[i], host[i], bytes, s) != cudaSuccess)
             return setError(VFB_ERR_CUDA, "field upload failed");
     int rc = VFB_OK;
-    for (int even = 0; even < 2 && rc == VFB_OK; ++even)
-        rc = vfb_init_equilibrium(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->geo.ptr),
-                                  static_cast<const uint32_t*>(L->nX.ptr), static_cast<const uint32_t*>(L->nY.ptr),
-                                  static_cast<const uint32_t*>(L->nZ.ptr), f[0].ptr, f[1].ptr, f[2].ptr, f[3].ptr, even,
-                                  stream);
+    const auto* geo = static_cast<const uint32_t*>(L->geo.ptr);
+    const auto* nX = static_cast<const uint32_t*>(L->nX.ptr);
+    const auto* nY = static_cast<const uint32_t*>(L->nY.ptr);
+    const auto* nZ = static_cast<const uint32_t*>(L->nZ.ptr);
+    // InitNavierStokesCompressible::init (InitNavierStokesCompressible.cu:46-83)
+    for (int even = 0; even < 2 && rc == VFB_OK; ++even) {
+        if (sim->params.useInitNeq)
+            rc = vfb_init_nonequilibrium(sim->params.storage, L->dist.ptr, L->N, geo, nX, nY, nZ,
+                                         static_cast<const uint32_t*>(L->nNeg.ptr), f[0].ptr, f[1].ptr, f[2].ptr,
+                                         f[3].ptr, L->omega, even, stream);
+        else
+            rc = vfb_init_equilibrium(sim->params.storage, L->dist.ptr, L->N, geo, nX, nY, nZ, f[0].ptr, f[1].ptr,
+                                      f[2].ptr, f[3].ptr, even, stream);
+    }
     L->isEven = true;
     // the temporary fields are freed on return: wait for the init kernels
     if (cudaStreamSynchronize(s) != cudaSuccess && rc == VFB_OK)

@@ -59,13 +59,17 @@ class DeviceLattice:
     neighborZ: "torch.Tensor"
     geo: "torch.Tensor"
     fluid: "torch.Tensor"
+    # the -x-y-z neighbour (neighborInverse / neighborWSB of the reference),
+    # needed only by the non-equilibrium initialisation
+    neighborInverse: "torch.Tensor | None" = None
 
     @staticmethod
     def from_arrays(g: dict[str, np.ndarray], device="cuda") -> "DeviceLattice":
         def u32(a):
             return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(device)
+        inverse = u32(g["neighborNeg"]) if "neighborNeg" in g else None
         return DeviceLattice(len(g["geo"]), u32(g["neighborX"]), u32(g["neighborY"]), u32(g["neighborZ"]),
-                             u32(g["geo"]), u32(g["fluid"]))
+                             u32(g["geo"]), u32(g["fluid"]), inverse)
 
     @property
     def numberOfFluidNodes(self) -> int:
@@ -158,6 +162,21 @@ def init_equilibrium(dist, lat: DeviceLattice, rho, vx, vy, vz, is_even: bool, s
                                                lat.neighborX.data_ptr(), lat.neighborY.data_ptr(),
                                                lat.neighborZ.data_ptr(), rho.data_ptr(), vx.data_ptr(),
                                                vy.data_ptr(), vz.data_ptr(), int(bool(is_even)), _stream(stream)))
+
+
+def init_nonequilibrium(dist, lat: DeviceLattice, rho, vx, vy, vz, omega: float, is_even: bool,
+                        stream=None) -> None:
+    """InitNavierStokesCompressibleNonEquilibrium_Device: equilibrium plus the
+    strain-rate part from central differences of (vx, vy, vz); the lattice
+    needs its inverse neighbour array."""
+    if lat.neighborInverse is None:
+        raise _lib.VfbError(_lib.VFB_ERR_INVALID_ARGUMENT, "lattice has no inverse neighbour array (neighborNeg)")
+    storage = STORAGE_OF_DTYPE[dist.dtype]
+    _lib.check(_lib.lib().vfb_init_nonequilibrium(storage, dist.data_ptr(), lat.N, lat.geo.data_ptr(),
+                                                  lat.neighborX.data_ptr(), lat.neighborY.data_ptr(),
+                                                  lat.neighborZ.data_ptr(), lat.neighborInverse.data_ptr(),
+                                                  rho.data_ptr(), vx.data_ptr(), vy.data_ptr(), vz.data_ptr(),
+                                                  float(omega), int(bool(is_even)), _stream(stream)))
 
 
 def macroscopic(dist, lat: DeviceLattice, is_even: bool, stream=None):

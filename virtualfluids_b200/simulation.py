@@ -34,6 +34,7 @@ class VfbSimParams(ctypes.Structure):
         ("quadricLimiters", ctypes.c_double * 3),
         ("usePlan", ctypes.c_int),
         ("useGraphs", ctypes.c_int),
+        ("useInitNeq", ctypes.c_int),
     ]
 
 
@@ -99,6 +100,7 @@ class Parameter:
         self.storage = "fp64"
         self.use_plan = True
         self.use_graphs = True
+        self.use_init_neq = False
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -120,6 +122,13 @@ class Parameter:
         if storage not in _lib.STORAGE_NAMES:
             raise ValueError(f"unknown storage {storage!r}")
         self.storage = storage
+
+    def set_use_init_neq(self, use_init_neq: bool):
+        """Initialise with the equilibrium plus the first-order strain-rate
+        part computed from the initial velocity field (Parameter::setUseInitNeq,
+        InitNavierStokesCompressibleNonEquilibrium_Device) instead of the
+        equilibrium alone."""
+        self.use_init_neq = bool(use_init_neq)
 
     def set_initial_condition(self, init_func):
         """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
@@ -169,6 +178,7 @@ class Simulation:
         p.quadricLimiters[:] = parameter.quadric_limiters
         p.usePlan = int(bool(parameter.use_plan))
         p.useGraphs = int(bool(parameter.use_graphs))
+        p.useInitNeq = int(bool(parameter.use_init_neq))
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
