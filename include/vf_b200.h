@@ -197,6 +197,22 @@ int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice, const int3
                           const void* rhoBC, uint32_t numberOfBCnodes, int direction, void* stream);
 
 /*
+ * The non-reflecting outflow of one directional list, in the pre-collision
+ * slot of the pressure BC.  Replaces OutflowNonReflecting and, with
+ * pressureCorrection != 0, OutflowNonReflectingPressureCorrection
+ * (src/gpu/core/BoundaryConditions/Outflow/Outflow.cu:44-84; kernels
+ * OutflowNonReflecting.cu:50-276 and OutflowNonReflectingPressureCorrection.cu:51-241),
+ * which BoundaryConditionFactory returns for PressureBC::OutflowNonReflective
+ * and ::OutflowNonReflectivePressureCorrection (BoundaryConditionFactory.cpp:162-166).
+ * k, kN, direction as for vfb_bc_pressure_noneq; correctionFactor is
+ * Parameter::outflowPressureCorrectionFactor (used with the correction only).
+ * lattice->omega is not used.
+ */
+int vfb_bc_outflow_nonreflecting(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,
+                                 uint32_t numberOfBCnodes, int direction, int pressureCorrection,
+                                 double correctionFactor, void* stream);
+
+/*
  * Grid scaling between a level and the next finer one.  Mirrors the
  * gridScaling function type (src/gpu/core/GridScaling/GridScalingFactory.h:46)
  * with the interface cells of InterpolationCells / ICellNeigh
@@ -323,7 +339,8 @@ typedef struct vfb_sim_params {
     int noSlipBC;              /* VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK, -1 NoSlipDelayBounceBack (no kernel) */
     int geometryBC;            /* as noSlipBC, for the geometry list */
     int slipBC;                /* VFB_BC_SLIP or -1 */
-    int pressureBC;            /* 0 PressureNonEquilibriumCompressible, -1 none */
+    int pressureBC;            /* 0 PressureNonEquilibriumCompressible, 1 OutflowNonReflective,
+                                  2 OutflowNonReflectivePressureCorrection, -1 none */
     double viscosity;          /* coarse-level kinematic viscosity, lattice units */
     double forces[3];          /* global acceleration */
     double quadricLimiters[3]; /* default 0.01 each (Parameter.cpp:69) */
@@ -331,6 +348,7 @@ typedef struct vfb_sim_params {
     int useGraphs;             /* 1: replay two coarse steps at a time from a captured CUDA graph */
     int useInitNeq;            /* 1: vfb_sim_init_level writes equilibrium plus the strain-rate part
                                   (Parameter::setUseInitNeq); the grid must carry neighborNeg */
+    double outflowPressureCorrectionFactor; /* pressureBC 2 (Parameter::setOutflowPressureCorrectionFactor) */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;

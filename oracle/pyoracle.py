@@ -62,6 +62,8 @@ class Oracle(_Lib):
                                            _vp, _vp, _c.c_int]
         self.fn("vfo_bc_pressure_noneq").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
                                                      _c.c_int, _c.c_int]
+        self.fn("vfo_bc_outflow").argtypes = [_c.c_int, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
+                                              _c.c_int, R, _c.c_int]
         self.fn("vfo_macroscopic").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _c.c_int, _vp, _vp, _vp, _vp]
 
     # -- single node ----------------------------------------------------------
@@ -117,6 +119,10 @@ class Oracle(_Lib):
         self.fn("vfo_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN), _ptr(rho),
                                          len(k), direction, int(is_even))
 
+    def bc_outflow(self, dist, N, nx, ny, nz, k, kN, direction, correction=False, factor=0.0, is_even=True):
+        self.fn("vfo_bc_outflow")(int(bool(correction)), _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN),
+                                  len(k), direction, factor, int(is_even))
+
     def macroscopic(self, dist, N, geo, nx, ny, nz, is_even):
         out = [np.zeros(N, self.real) for _ in range(4)]
         self.fn("vfo_macroscopic")(_ptr(dist), N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz), int(is_even),
@@ -147,6 +153,8 @@ class Reference(_Lib):
                                              _vp, _vp, _c.c_int]
         self.fn("vfref_bc_pressure_noneq").argtypes = [_vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_uint,
                                                        _c.c_int, _c.c_int]
+        self.fn("vfref_bc_outflow").argtypes = [_c.c_int, _vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _c.c_uint,
+                                                _c.c_int, R, _c.c_int]
         self.fn("vfref_grid_build").restype = _vp
         self.fn("vfref_grid_build").argtypes = [_vp]
         self.fn("vfref_grid_levels").argtypes = [_vp]
@@ -209,6 +217,10 @@ class Reference(_Lib):
     def bc_pressure(self, dist, N, nx, ny, nz, k, kN, rho, direction, is_even=True):
         self.fn("vfref_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN),
                                            _ptr(rho), len(k), direction, int(is_even))
+
+    def bc_outflow(self, dist, N, nx, ny, nz, k, kN, direction, correction=False, factor=0.0, is_even=True):
+        self.fn("vfref_bc_outflow")(int(bool(correction)), _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k),
+                                    _ptr(kN), len(k), direction, factor, int(is_even))
 
     def grid(self, spec):
         """Build a grid with the reference builder; returns {level: {name: array}}."""

@@ -24,6 +24,7 @@
 #include "BoundaryConditions/Velocity/Velocity_Device.cuh"
 #include "BoundaryConditions/Slip/Slip_Device.cuh"
 #include "BoundaryConditions/Pressure/Pressure_Device.cuh"
+#include "BoundaryConditions/Outflow/Outflow_Device.cuh"
 #include "Kernel/Compressible/NavierStokes/B92/B92CompressibleNavierStokes_Device.cuh"
 #include "PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cuh"
 
@@ -105,6 +106,22 @@ void REF(vfref_init_eq)(real* dist, unsigned long long N, unsigned* geo, unsigne
     for (unsigned long long t = 0; t < N; ++t) {
         setThread(t);
         InitNavierStokesCompressible_Device(nx, ny, nz, geo, rho, ux, uy, uz, (unsigned)N, dist, isEven != 0);
+    }
+}
+
+// OutflowNonReflecting_Device (correction 0) or
+// OutflowNonReflectingPressureCorrection_Device over one directional list
+void REF(vfref_bc_outflow)(int correction, real* dist, unsigned long long N, unsigned* nx, unsigned* ny, unsigned* nz,
+                           int* bcNodes, int* bcNeighbors, unsigned nBC, int direction, real factor, int isEven)
+{
+    for (unsigned t = 0; t < nBC; ++t) {
+        setThread(t);
+        if (correction)
+            OutflowNonReflectingPressureCorrection_Device(nullptr, dist, bcNodes, bcNeighbors, (int)nBC, (real)1, nx, ny,
+                                                          nz, N, isEven != 0, direction, factor);
+        else
+            OutflowNonReflecting_Device(nullptr, dist, bcNodes, bcNeighbors, (int)nBC, (real)1, nx, ny, nz, N,
+                                        isEven != 0, direction);
     }
 }
 

@@ -21,7 +21,7 @@
  *                                InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cu:44-212
  *   - non-equilibrium init       InitNavierStokesCompressible_Device.cu:216-500
  *   - BC formulas                KernelUtilities.h:171-214 and the BC kernels in
- *                                src/gpu/core/BoundaryConditions/{NoSlip,Velocity,Slip,Pressure}/
+ *                                src/gpu/core/BoundaryConditions/{NoSlip,Velocity,Slip,Pressure,Outflow}/
  *
  * Parity is pinned: tests/test_oracle_vs_ref.py compares every function here
  * bit for bit against the reference's own sources compiled on the host
@@ -876,6 +876,50 @@ void FN(vfo_bc_pressure_noneq)(real *dist, uint64_t N, const uint32_t *nx, const
             if (c == sgn)
                 continue;
             dist[(uint64_t)slot_of(d, isEven) * N + L.k[loc_of(d)]] = f[d];
+        }
+    }
+}
+
+/* Non-reflecting outflow, one directional list: OutflowNonReflecting_Device
+ * (OutflowNonReflecting.cu:50-276) when correction == 0,
+ * OutflowNonReflectingPressureCorrection_Device
+ * (OutflowNonReflectingPressureCorrection.cu:51-241) otherwise.  For the nine
+ * directions whose component along the normal's axis is opposite to the
+ * normal, the BC node gets cs f_neighbour + (1 - cs) f_node (minus
+ * w_d factor drho_node with the correction), cs = 1 / sqrtf(3) formed from a
+ * single-precision square root as in the reference.  Both read the current
+ * view and write the other view (:199 / :164).  The corrected form reads the
+ * neighbour's populations at the neighbour itself for the directions without
+ * a negative component, but at the BC node's shifted locations for the others
+ * (its kN_* indices are taken from the BC node, :89-96); that is reproduced. */
+void FN(vfo_bc_outflow)(int correction, real *dist, uint64_t N, const uint32_t *nx, const uint32_t *ny,
+                        const uint32_t *nz, const int32_t *bcNodes, const int32_t *bcNeighbors, uint32_t nBC,
+                        int direction, real factor, int isEven)
+{
+    const int axis = CX[direction] != 0 ? 0 : CY[direction] != 0 ? 1 : 2;
+    const int sgn = axis == 0 ? CX[direction] : axis == 1 ? CY[direction] : CZ[direction];
+    const real cs = (real)1 / (real)sqrtf(3.0f);
+    for (uint32_t i = 0; i < nBC; ++i) {
+        const locs8 L = list_indices((uint32_t)bcNodes[i], nx, ny, nz);
+        locs8 LN;
+        if (correction) {
+            LN = L;
+            LN.k[0] = (uint32_t)bcNeighbors[i];
+        } else {
+            LN = list_indices((uint32_t)bcNeighbors[i], nx, ny, nz);
+        }
+        real f[27], fN[27];
+        gather_pre(f, dist, N, &L, isEven);
+        gather_pre(fN, dist, N, &LN, isEven);
+        const real rhoCorrection = correction ? factor * pyramid_density(f) : (real)0;
+        for (int d = 1; d < 27; ++d) {
+            const int c = axis == 0 ? CX[d] : axis == 1 ? CY[d] : CZ[d];
+            if (c != -sgn)
+                continue;
+            real v = fN[d] * cs + ((real)1 - cs) * f[d];
+            if (correction)
+                v = v - weight_of(d) * rhoCorrection;
+            dist[(uint64_t)slot_of(d, !isEven) * N + L.k[loc_of(d)]] = v;
         }
     }
 }

@@ -8,6 +8,7 @@ machine without the reference tree.
 
     python tests/golden/make_golden.py                 (all fixtures)
     python tests/golden/make_golden.py --init-noneq    (the non-equilibrium init only)
+    python tests/golden/make_golden.py --outflow       (the non-reflecting outflow only)
 """
 from __future__ import annotations
 
@@ -98,6 +99,29 @@ def init_noneq(precision: str) -> None:
                         vz=fields[3], omega=np.array(omega), dist=dist)
 
 
+def outflow(precision: str) -> None:
+    """OutflowNonReflecting_Device and its pressure-corrected form over the
+    channel grid's outflow list (both parity views), from seeded populations;
+    the outputs are stored at the positions the kernels write."""
+    R = Reference(precision)
+    real = np.float64 if precision == "f64" else np.float32
+    g = R.grid(grid_spec("channel"))[0]
+    N = len(g["geo"])
+    rng = np.random.default_rng(20261204)
+    dist0 = rng.uniform(-0.02, 0.02, 27 * N).astype(real)
+    factor = real(0.3)
+    out = {"dist": dist0, "factor": np.array(factor)}
+    for correction in (0, 1):
+        for ev in (0, 1):
+            d = dist0.copy()
+            R.bc_outflow(d, N, g["neighborX"], g["neighborY"], g["neighborZ"], g["pressure0.k"], g["pressure0.kN"],
+                         int(g["pressure0.dir"][0]), bool(correction), factor, bool(ev))
+            idx = np.flatnonzero(d != dist0)
+            out[f"idx_c{correction}_e{ev}"] = idx
+            out[f"val_c{correction}_e{ev}"] = d[idx]
+    np.savez_compressed(OUT / f"outflow_channel_{precision}.npz", **out)
+
+
 if __name__ == "__main__":
     if len(sys.argv) == 3 and sys.argv[1] == "--refined":
         refined_grid(sys.argv[2])
@@ -105,6 +129,11 @@ if __name__ == "__main__":
     if len(sys.argv) == 2 and sys.argv[1] == "--init-noneq":
         for p in ("f64", "f32"):
             init_noneq(p)
+        outflow(p)
+        sys.exit(0)
+    if len(sys.argv) == 2 and sys.argv[1] == "--outflow":
+        for p in ("f64", "f32"):
+            outflow(p)
         sys.exit(0)
     for p in ("f64", "f32"):
         k17_nodes(p)

@@ -38,9 +38,12 @@ def channel():
     return b
 
 
-def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, velocity_kind=2, init_neq=False):
+def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, velocity_kind=2, init_neq=False,
+                    pressure_kind=0, correction_factor=0.0):
     """UpdateGrid27::updateGrid for one level, on the oracle (initialised by
-    the equilibrium, or with init_neq by the non-equilibrium init)."""
+    the equilibrium, or with init_neq by the non-equilibrium init; the
+    pressure list runs PressureNonEquilibriumCompressible for pressure_kind 0,
+    the non-reflecting outflow for 1 and its pressure-corrected form for 2)."""
     O = Oracle(precision)
     real = O.real
     N = len(g["geo"])
@@ -62,9 +65,12 @@ def oracle_schedule(g, precision, nu, steps, init, slip=False, pressure=False, v
         if slip:
             O.bc_post(4, d, N, nx, ny, nz, g["slip.k"], g["slip.q"].astype(real), om, is_even=even)
         even = not even
-        if pressure:
+        if pressure and pressure_kind == 0:
             O.bc_pressure(d, N, nx, ny, nz, g["pressure0.k"], g["pressure0.kN"], g["pressure0.rho"].astype(real),
                           int(g["pressure0.dir"][0]), is_even=even)
+        elif pressure:
+            O.bc_outflow(d, N, nx, ny, nz, g["pressure0.k"], g["pressure0.kN"], int(g["pressure0.dir"][0]),
+                         pressure_kind == 2, real(correction_factor), is_even=even)
     return O.macroscopic(d, N, geo, nx, ny, nz, even)
 
 

@@ -172,3 +172,52 @@ def test_init_noneq_matches_live_reference(precision, grid, omega):
                             O.real(omega), ev)
         out.append(d)
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("correction", [0, 1])
+@pytest.mark.parametrize("is_even", [0, 1])
+def test_outflow_matches_golden(precision, correction, is_even):
+    """OutflowNonReflecting (and its pressure-corrected form) on the channel
+    grid's outflow plane equals the fixture made by the reference's kernels
+    built for the host: the written positions and values, nothing else."""
+    g = _channel_level0()
+    ref = np.load(GOLDEN / f"outflow_channel_{precision}.npz")
+    O = Oracle(precision)
+    N = len(g["geo"])
+    d = ref["dist"].copy()
+    O.bc_outflow(d, N, g["neighborX"], g["neighborY"], g["neighborZ"], g["pressure0.k"], g["pressure0.kN"],
+                 int(g["pressure0.dir"][0]), bool(correction), ref["factor"][()], bool(is_even))
+    idx = np.flatnonzero(d != ref["dist"])
+    assert np.array_equal(idx, ref[f"idx_c{correction}_e{is_even}"])
+    assert np.array_equal(d[idx], ref[f"val_c{correction}_e{is_even}"])
+    assert len(idx) == 9 * len(g["pressure0.k"])
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("correction", [False, True])
+def test_outflow_matches_live_reference_every_direction(precision, correction):
+    """All six normals, both parities, on random node pairs of a periodic box
+    and on the outflow planes of the channel and cube grids."""
+    from virtualfluids_b200.workloads import taylor_green
+    O, R = Oracle(precision), Reference(precision)
+    g = taylor_green(9).grid
+    N = len(g["geo"])
+    rng = np.random.default_rng(2)
+    k = rng.choice(np.arange(1, N), 40, replace=False).astype(np.int32)
+    kN = rng.integers(1, N, 40).astype(np.int32)
+    cases = [(g, k, kN, direction) for direction in range(1, 7)]
+    for name in ("channel", "cube_channel"):
+        h = _golden_level0(name)
+        cases.append((h, h["pressure0.k"], h["pressure0.kN"], int(h["pressure0.dir"][0])))
+    for grid, kk, kkN, direction in cases:
+        M = len(grid["geo"])
+        for ev in (True, False):
+            out = []
+            for impl in (O, R):
+                d = np.random.default_rng(5).uniform(-0.02, 0.02, 27 * M).astype(O.real)
+                impl.bc_outflow(d, M, grid["neighborX"], grid["neighborY"], grid["neighborZ"], kk, kkN, direction,
+                                correction, O.real(0.7), ev)
+                out.append(d)
+            assert np.array_equal(out[0], out[1]), (direction, ev)

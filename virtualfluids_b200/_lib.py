@@ -142,6 +142,9 @@ _SIGNATURES = [
     ("vfb_bc_pressure_noneq", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
       ctypes.c_int, ctypes.c_void_p]),
+    ("vfb_bc_outflow_nonreflecting", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+      ctypes.c_int, ctypes.c_double, ctypes.c_void_p]),
     ("vfb_sim_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     ("vfb_sim_destroy", ctypes.c_int, [ctypes.c_void_p]),
     ("vfb_sim_levels", ctypes.c_int, [ctypes.c_void_p]),

@@ -15,8 +15,10 @@
 //   slip                  SlipCompressible.cu:45-550
 //   velocity with pressure VelocityWithPressureInterpolatedCompressible.cu
 //                          (the velocity formula minus w drho, KernelUtilities.h:208-214)
-// Pre-collision kind (after the parity swap):
+// Pre-collision kinds (after the parity swap):
 //   pressure non-equilibrium PressureNonEquilibriumCompressible.cu:45-311
+//   non-reflecting outflow   OutflowNonReflecting.cu:50-276, with pressure
+//                            correction OutflowNonReflectingPressureCorrection.cu:51-241
 //
 // Every node writes only its own locations, so no two nodes write one cell
 // (for a fixed location bit the map node -> location index is one to one).
@@ -28,6 +30,8 @@
 // launch everywhere; across waves the outcome depends on the schedule, as it
 // does in the reference.
 #include <cuda_runtime.h>
+
+#include <cmath>
 
 #include "capi_common.cuh"
 #include "collision_math.cuh"
@@ -258,6 +262,56 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
     }
 }
 
+// OutflowNonReflecting.cu:50-276 (CORRECTION false) and
+// OutflowNonReflectingPressureCorrection.cu:51-241 (true): for the nine
+// directions whose component along the normal's axis is opposite to the
+// normal, the BC node's population becomes cs f_neighbour + (1 - cs) f_node
+// (minus w_d factor drho_node with the correction), read from the current
+// view and written into the other one at the same location.  The corrected
+// form takes the neighbour's shifted locations from the BC node (:89-96), so
+// only its rest location is the neighbour's own; that is kept.  Reads (the
+// nine directions) and writes (their inverse slots) never share a slot, so
+// BC nodes of one list do not race.
+template <class S, bool EVEN, bool CORRECTION>
+__global__ void __launch_bounds__(128) bcOutflowKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
+                                                        const int32_t* __restrict__ bcK,
+                                                        const int32_t* __restrict__ bcKN, uint32_t nBC, int axis,
+                                                        int sgn, typename Storage<S>::R cs,
+                                                        typename Storage<S>::R factor)
+{
+    using R = typename Storage<S>::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nBC)
+        return;
+    const unsigned long long N = lat.N;
+    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    Locs LN = L;
+    if (CORRECTION)
+        LN.k[0] = (uint32_t)__ldg(bcKN + i);
+    else
+        LN = listIndices((uint32_t)__ldg(bcKN + i), lat.nX, lat.nY, lat.nZ);
+    R rhoCorrection = R(0);
+    if (CORRECTION) {
+        R f[27];
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+        rhoCorrection = factor * pyramidDensity(f);
+    }
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const int c = axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d);
+        if (c != -sgn)
+            continue;
+        const R fNode = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+        const R fNeighbour = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)]);
+        R v = fNeighbour * cs + (R(1) - cs) * fNode;
+        if (CORRECTION)
+            v = v - weight<R>(d) * rhoCorrection;
+        Storage<S>::store(dist + (unsigned long long)slot<!EVEN>(d) * N + L.k[loc(d)], v);
+    }
+}
+
 template <class S, int KIND>
 static void launchPostKind(bool even, unsigned blocks, cudaStream_t stream, S* dist, const BcLattice<typename Storage<S>::R>& lat,
                            const vfb_bc_list* l)
@@ -308,6 +362,32 @@ static int launchPressure(const vfb_bc_lattice* t, const int32_t* k, const int32
     else
         bcPressureKernel<S, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, rho, n, axis, sgn);
     return checkLaunch("pressure boundary condition");
+}
+
+template <class S>
+static int launchOutflow(const vfb_bc_lattice* t, const int32_t* k, const int32_t* kN, uint32_t n, int axis, int sgn,
+                         bool correction, double factor, cudaStream_t stream)
+{
+    using R = typename Storage<S>::R;
+    BcLattice<R> lat { t->numberOfLBnodes, t->neighborX, t->neighborY, t->neighborZ, (R)t->omega };
+    S* dist = static_cast<S*>(t->distributions);
+    const unsigned blocks = (n + 127) / 128;
+    // cs = 1 / sqrtf(3): the reference takes a single-precision root in both precisions
+    const R cs = R(1) / R(std::sqrt(3.0f));
+    const R fac = (R)factor;
+    const bool even = t->isEvenTimestep != 0;
+    if (correction) {
+        if (even)
+            bcOutflowKernel<S, true, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+        else
+            bcOutflowKernel<S, false, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+    } else {
+        if (even)
+            bcOutflowKernel<S, true, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+        else
+            bcOutflowKernel<S, false, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+    }
+    return checkLaunch("outflow boundary condition");
 }
 
 static int checkLattice(const vfb_bc_lattice* t)
@@ -378,5 +458,35 @@ extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice,
     case VFB_FP64: return launchPressure<double>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     case VFB_FP16: return launchPressure<__half>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    }
+}
+
+extern "C" int vfb_bc_outflow_nonreflecting(int storage, const vfb_bc_lattice* lattice, const int32_t* k,
+                                            const int32_t* kN, uint32_t numberOfBCnodes, int direction,
+                                            int pressureCorrection, double correctionFactor, void* stream)
+{
+    clearError();
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (numberOfBCnodes == 0)
+        return VFB_OK;
+    if (const int rc = checkLattice(lattice))
+        return rc;
+    if (!k || !kN)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL k or kN");
+    if (direction < dP00 || direction > d00M)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "direction %d is not an axis direction (1..6)", direction);
+    if (!std::isfinite(correctionFactor))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "correction factor is not finite");
+    const int axis = cx(direction) != 0 ? 0 : cy(direction) != 0 ? 1 : 2;
+    const int sgn = axis == 0 ? cx(direction) : axis == 1 ? cy(direction) : cz(direction);
+    const bool corr = pressureCorrection != 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchOutflow<float>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
+    case VFB_FP64: return launchOutflow<double>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
+    case VFB_FP16: return launchOutflow<__half>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
+    default:
+        return launchOutflow<__nv_bfloat16>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     }
 }

@@ -373,9 +373,15 @@ int preCollisionBC(vfb_simulation& S, Level& L, void* stream)
     for (const PressureListDevice* P : L.pressure) {
         if (P->n == 0)
             continue;
-        if (const int rc = vfb_bc_pressure_noneq(S.params.storage, &t, static_cast<const int32_t*>(P->k.ptr),
-                                                 static_cast<const int32_t*>(P->kN.ptr), P->rho.ptr, P->n,
-                                                 P->direction, stream))
+        const auto* k = static_cast<const int32_t*>(P->k.ptr);
+        const auto* kN = static_cast<const int32_t*>(P->kN.ptr);
+        // BoundaryConditionFactory::getPressureBoundaryConditionPre (BoundaryConditionFactory.cpp:151-168)
+        const int rc = S.params.pressureBC == 0
+                           ? vfb_bc_pressure_noneq(S.params.storage, &t, k, kN, P->rho.ptr, P->n, P->direction, stream)
+                           : vfb_bc_outflow_nonreflecting(S.params.storage, &t, k, kN, P->n, P->direction,
+                                                          S.params.pressureBC == 2,
+                                                          S.params.outflowPressureCorrectionFactor, stream);
+        if (rc)
             return rc;
     }
     return VFB_OK;
@@ -467,7 +473,7 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         return setError(VFB_ERR_INVALID_ARGUMENT, "velocityBC must be a velocity kind");
     if (!validKind(P.noSlipBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
         !validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
-        !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC < 0 || P.pressureBC == 0))
+        !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC >= -1 && P.pressureBC <= 2))
         return setError(VFB_ERR_INVALID_ARGUMENT, "invalid boundary-condition selection");
     if (!(P.viscosity > 0.0))
         return setError(VFB_ERR_INVALID_ARGUMENT, "viscosity %g must be positive", P.viscosity);

@@ -229,6 +229,18 @@ def bc_post(kind: int, dist, lat: DeviceLattice, k, q, omega: float, is_even: bo
                                       _stream(stream)))
 
 
+def bc_outflow(dist, lat: DeviceLattice, k, kN, direction: int, is_even: bool, pressure_correction: bool = False,
+               correction_factor: float = 0.0, stream=None) -> None:
+    """The non-reflecting outflow (OutflowNonReflecting, or with
+    pressure_correction OutflowNonReflectingPressureCorrection) of one
+    directional list."""
+    t = _bc_lattice(dist, lat, 1.0, is_even)
+    _lib.check(_lib.lib().vfb_bc_outflow_nonreflecting(STORAGE_OF_DTYPE[dist.dtype], ctypes.byref(t), k.data_ptr(),
+                                                       kN.data_ptr(), int(k.numel()), int(direction),
+                                                       int(bool(pressure_correction)), float(correction_factor),
+                                                       _stream(stream)))
+
+
 def bc_pressure(dist, lat: DeviceLattice, k, kN, rho, direction: int, is_even: bool, stream=None) -> None:
     """The pre-collision non-equilibrium pressure BC of one directional list."""
     t = _bc_lattice(dist, lat, 1.0, is_even)

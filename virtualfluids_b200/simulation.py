@@ -35,6 +35,7 @@ class VfbSimParams(ctypes.Structure):
         ("usePlan", ctypes.c_int),
         ("useGraphs", ctypes.c_int),
         ("useInitNeq", ctypes.c_int),
+        ("outflowPressureCorrectionFactor", ctypes.c_double),
     ]
 
 
@@ -58,6 +59,8 @@ class SlipBC(enum.IntEnum):
 class PressureBC(enum.IntEnum):
     NotSpecified = -1
     PressureNonEquilibriumCompressible = 0
+    OutflowNonReflective = 1
+    OutflowNonReflectivePressureCorrection = 2
 
 
 KERNELS = {"K17CompressibleNavierStokes": 0, "BGKCompSP27": 1}
@@ -101,6 +104,9 @@ class Parameter:
         self.use_plan = True
         self.use_graphs = True
         self.use_init_neq = False
+        # the reference leaves it unset; it matters only for
+        # PressureBC.OutflowNonReflectivePressureCorrection
+        self.outflow_pressure_correction_factor = 0.0
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -129,6 +135,11 @@ class Parameter:
         InitNavierStokesCompressibleNonEquilibrium_Device) instead of the
         equilibrium alone."""
         self.use_init_neq = bool(use_init_neq)
+
+    def set_outflow_pressure_correction_factor(self, correction_factor: float):
+        """Parameter::setOutflowPressureCorrectionFactor: the density
+        correction of OutflowNonReflectivePressureCorrection."""
+        self.outflow_pressure_correction_factor = float(correction_factor)
 
     def set_initial_condition(self, init_func):
         """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
@@ -179,6 +190,7 @@ class Simulation:
         p.usePlan = int(bool(parameter.use_plan))
         p.useGraphs = int(bool(parameter.use_graphs))
         p.useInitNeq = int(bool(parameter.use_init_neq))
+        p.outflowPressureCorrectionFactor = parameter.outflow_pressure_correction_factor
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
