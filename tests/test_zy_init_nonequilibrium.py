@@ -62,10 +62,11 @@ def test_init_noneq_matches_oracle(cuda, grid, dtype):
     assert np.all(got[solid] == marker)
 
 
-@pytest.mark.parametrize("dtype,tol", [("float64", 1e-12), ("float32", 1e-4)])
-def test_init_noneq_keeps_the_macroscopic_fields(cuda, dtype, tol):
+@pytest.mark.parametrize("dtype,atol", [("float64", 1e-13), ("float32", 1e-6)])
+def test_init_noneq_keeps_the_macroscopic_fields(cuda, dtype, atol):
     """The strain-rate part carries no mass and no momentum: the macroscopic
-    fields read back from the populations are the ones given, while the
+    fields read back from the populations are the ones given (to the rounding
+    of the 27-term sums, absolute: the velocity scale is 0.05), while the
     populations differ from the equilibrium init's."""
     w = tgv_state(48)
     lat = K.DeviceLattice.from_arrays(w.grid)
@@ -79,8 +80,11 @@ def test_init_noneq_keeps_the_macroscopic_fields(cuda, dtype, tol):
     macro = [m.cpu().numpy() for m in K.macroscopic(dist, lat, True)]
     fl = w.grid["fluid"]
     for m, a in zip(macro, (w.rho, w.vx, w.vy, w.vz)):
-        assert np.abs(m[fl] - a[fl]).max() <= tol * np.abs(a).max()
-    assert rel_l2(dist.cpu().numpy(), eq.cpu().numpy()) > 1e-4
+        assert np.abs(m[fl] - a[fl]).max() <= atol
+    geo = w.grid["geo"]
+    keep = np.ones(27 * lat.N, bool)
+    keep[np.flatnonzero((geo == 15) | (geo == 16))] = False  # rest populations of non-fluid nodes hold the marker
+    assert rel_l2(dist.cpu().numpy()[keep], eq.cpu().numpy()[keep]) > 1e-2
 
 
 def test_init_noneq_needs_the_inverse_neighbour(cuda):
