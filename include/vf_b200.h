@@ -379,6 +379,12 @@ int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* out3, void* 
  * number; out2[1] = that number.  The sum is FP64 (the reference reduces in
  * the working precision).  Synchronises the stream. */
 int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* stream);
+/* EnstrophyAnalyzer::run (src/gpu/core/PostProcessor/EnstrophyAnalyzer.cu:63-98)
+ * on a level: out2[0] = the mean of 1/2 (drho + 1) |curl u|^2 over the fluid
+ * nodes whose six axis neighbours are fluid (FP64 sum), out2[1] = their
+ * number.  Computes the macroscopic fields into temporary device arrays
+ * first; synchronises the stream. */
+int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream);
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,
                         int* isEvenTimestep, double* omega);
@@ -413,6 +419,21 @@ int vfb_init_nonequilibrium(int storage, void* distributions, unsigned long long
                             const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
                             const uint32_t* neighborInverse, const void* rho, const void* vx, const void* vy,
                             const void* vz, double omega, int isEvenTimestep, void* stream);
+
+/*
+ * The enstrophy analyzer over one level's macroscopic fields (device arrays
+ * of numberOfLBnodes in the compute precision: precision VFB_FP64 or
+ * VFB_FP32).  Per fluid node whose six axis neighbours are fluid:
+ * 1/2 (drho + 1) |curl u|^2, each axis with the widest central difference
+ * (order 8, 6, 4 or 2) whose stencil stays on fluid nodes
+ * (EnstrophyAnalyzer.cu:112-338, enstrophyKernel / enstrophyFunction).
+ * out2[0] = the mean over those nodes (FP64 sum; the reference sums in the
+ * working precision), out2[1] = their number.  Synchronises the stream.
+ */
+int vfb_enstrophy(int precision, const void* rho, const void* vx, const void* vy, const void* vz,
+                  unsigned long long numberOfLBnodes, const uint32_t* geo, const uint32_t* neighborX,
+                  const uint32_t* neighborY, const uint32_t* neighborZ, const uint32_t* neighborInverse,
+                  double* out2, void* stream);
 
 /*
  * drho and velocity of every node from the populations of the given parity
@@ -477,6 +498,15 @@ int vfb_debug_collide_node(int op, int precision, double* f27, double omega, con
  */
 int vfb_debug_init_nonequilibrium_node(int precision, const double* drhoVelocity4, const double* gradient9,
                                        double omega, double* f27);
+/*
+ * The enstrophy node values on the host with the code the kernel runs
+ * (host arrays of the compute precision): out[k] the value, counted[k] 1
+ * where the node enters the mean.  No counterpart in the reference.
+ */
+int vfb_debug_enstrophy_nodes(int precision, const void* rho, const void* vx, const void* vy, const void* vz,
+                              unsigned long long numberOfLBnodes, const uint32_t* geo, const uint32_t* neighborX,
+                              const uint32_t* neighborY, const uint32_t* neighborZ, const uint32_t* neighborInverse,
+                              double* out, int* counted);
 
 #ifdef __cplusplus
 }

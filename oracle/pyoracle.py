@@ -64,6 +64,8 @@ class Oracle(_Lib):
                                                      _c.c_int, _c.c_int]
         self.fn("vfo_bc_outflow").argtypes = [_c.c_int, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
                                               _c.c_int, R, _c.c_int]
+        self.fn("vfo_enstrophy_nodes").argtypes = [_vp, _vp, _vp, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                   _vp]
         self.fn("vfo_macroscopic").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _c.c_int, _vp, _vp, _vp, _vp]
 
     # -- single node ----------------------------------------------------------
@@ -122,6 +124,16 @@ class Oracle(_Lib):
     def bc_outflow(self, dist, N, nx, ny, nz, k, kN, direction, correction=False, factor=0.0, is_even=True):
         self.fn("vfo_bc_outflow")(int(bool(correction)), _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN),
                                   len(k), direction, factor, int(is_even))
+
+    def enstrophy_nodes(self, rho, vx, vy, vz, geo, nx, ny, nz, nneg):
+        """Per-node enstrophy values and the counted mask of EnstrophyAnalyzer."""
+        N = len(geo)
+        out = np.zeros(N, self.real)
+        counted = np.zeros(N, np.uint32)
+        args = [np.ascontiguousarray(a, dtype=self.real) for a in (rho, vx, vy, vz)]
+        self.fn("vfo_enstrophy_nodes")(*[_ptr(a) for a in args], N, _ptr(geo), _ptr(nx), _ptr(ny), _ptr(nz),
+                                       _ptr(nneg), _ptr(out), _ptr(counted))
+        return out, counted.astype(bool)
 
     def macroscopic(self, dist, N, geo, nx, ny, nz, is_even):
         out = [np.zeros(N, self.real) for _ in range(4)]

@@ -20,6 +20,7 @@
  *   - equilibrium init           src/gpu/core/PreProcessor/PreProcessorStrategy/
  *                                InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cu:44-212
  *   - non-equilibrium init       InitNavierStokesCompressible_Device.cu:216-500
+ *   - enstrophy per node         src/gpu/core/PostProcessor/EnstrophyAnalyzer.cu:112-338
  *   - BC formulas                KernelUtilities.h:171-214 and the BC kernels in
  *                                src/gpu/core/BoundaryConditions/{NoSlip,Velocity,Slip,Pressure,Outflow}/
  *
@@ -27,6 +28,10 @@
  * bit for bit against the reference's own sources compiled on the host
  * (oracle/Makefile, target ref), and tests/golden/ holds fixtures generated
  * from that build so the pin also runs where the reference tree is absent.
+ * One exception, parity unpinned: vfo_enstrophy_nodes restates
+ * EnstrophyAnalyzer.cu by reading, because that file (a kernel launch and
+ * thrust device vectors beside the node function) does not build for the
+ * host; tests/test_enstrophy_host.py checks it against analytic curls.
  *
  * Compiled twice by oracle/Makefile: -DVFO_REAL=double (suffix _f64) and
  * -DVFO_REAL=float (suffix _f32), always with -ffp-contract=off so that no
@@ -927,6 +932,80 @@ void FN(vfo_bc_outflow)(int correction, real *dist, uint64_t N, const uint32_t *
 /* ------------------------------------------------------------------------ */
 /* macroscopic output and reductions                                          */
 /* ------------------------------------------------------------------------ */
+/* enstrophy of one node (EnstrophyAnalyzer.cu:112-338): 1/2 (drho + 1) |curl u|^2
+ * with one-sided reach: the six axis neighbours must be fluid, and each axis
+ * uses the widest central difference (order 8, 6, 4 or 2) whose stencil
+ * stays on fluid nodes.  Negative steps go through the inverse (-x-y-z)
+ * neighbour and two positive steps, as everywhere in the reference. */
+#define GEO_FLUID_NODE 19
+
+static uint32_t step_plus(int axis, uint32_t k, const uint32_t *nx, const uint32_t *ny, const uint32_t *nz)
+{
+    return axis == 0 ? nx[k] : axis == 1 ? ny[k] : nz[k];
+}
+
+static uint32_t step_minus(int axis, uint32_t k, const uint32_t *nx, const uint32_t *ny, const uint32_t *nz,
+                           const uint32_t *nneg)
+{
+    const uint32_t w = nneg[k];
+    return axis == 0 ? nz[ny[w]] : axis == 1 ? nz[nx[w]] : ny[nx[w]];
+}
+
+/* d u / d x_axis with the central difference of the given order (:285-327) */
+static real central_difference(const real *u, const uint32_t P[4], const uint32_t M[4], int order)
+{
+    if (order == 2)
+        return (u[P[0]] - u[M[0]]) / (real)2;
+    if (order == 4)
+        return (((real)8 * u[P[0]] - (real)8 * u[M[0]]) - (u[P[1]] - u[M[1]])) / (real)12;
+    if (order == 6)
+        return (((real)5 * (real)9) * (u[P[0]] - u[M[0]]) - (real)9 * (u[P[1]] - u[M[1]]) + (u[P[2]] - u[M[2]])) /
+               ((real)6 * (real)10);
+    return (((real)28 * (real)8) * (u[P[0]] - u[M[0]]) - ((real)7 * (real)8) * (u[P[1]] - u[M[1]]) +
+            ((real)8 * (real)4 * C(1, 3)) * (u[P[2]] - u[M[2]]) - (u[P[3]] - u[M[3]])) /
+           ((real)7 * (real)10 * (real)4);
+}
+
+void FN(vfo_enstrophy_nodes)(const real *rho, const real *vx, const real *vy, const real *vz, uint64_t N,
+                             const uint32_t *geo, const uint32_t *nx, const uint32_t *ny, const uint32_t *nz,
+                             const uint32_t *nneg, real *out, uint32_t *isFluid)
+{
+    for (uint64_t kk = 0; kk < N; ++kk) {
+        const uint32_t k = (uint32_t)kk;
+        out[k] = 0;
+        isFluid[k] = 0;
+        if (geo[k] != GEO_FLUID_NODE)
+            continue;
+        uint32_t P[3][4], M[3][4];
+        int order[3] = { 8, 8, 8 }, reach = 1;
+        for (int a = 0; a < 3; ++a) {
+            P[a][0] = step_plus(a, k, nx, ny, nz);
+            M[a][0] = step_minus(a, k, nx, ny, nz, nneg);
+            if (geo[P[a][0]] != GEO_FLUID_NODE || geo[M[a][0]] != GEO_FLUID_NODE)
+                reach = 0;
+        }
+        if (!reach)
+            continue;
+        for (int a = 0; a < 3; ++a) {
+            for (int i = 1; i < 4; ++i) {
+                P[a][i] = step_plus(a, P[a][i - 1], nx, ny, nz);
+                M[a][i] = step_minus(a, M[a][i - 1], nx, ny, nz, nneg);
+                const int cap = 2 * i; /* a non-fluid node at distance i + 1 caps the order at 2 i */
+                if ((geo[P[a][i]] != GEO_FLUID_NODE || geo[M[a][i]] != GEO_FLUID_NODE) && order[a] > cap)
+                    order[a] = cap;
+            }
+        }
+        const real dxvy = central_difference(vy, P[0], M[0], order[0]);
+        const real dxvz = central_difference(vz, P[0], M[0], order[0]);
+        const real dyvx = central_difference(vx, P[1], M[1], order[1]);
+        const real dyvz = central_difference(vz, P[1], M[1], order[1]);
+        const real dzvx = central_difference(vx, P[2], M[2], order[2]);
+        const real dzvy = central_difference(vy, P[2], M[2], order[2]);
+        const real wx = dyvz - dzvy, wy = dzvx - dxvz, wz = dxvy - dyvx;
+        isFluid[k] = 1;
+        out[k] = C(1, 2) * (rho[k] + (real)1) * (wx * wx + wy * wy + wz * wz);
+    }
+}
 /* rho (drho) and velocity of every valid node from its pre-collision view,
  * with the pyramid sums of MacroscopicQuantities.h:117-127 */
 void FN(vfo_macroscopic)(const real *dist, uint64_t N, const uint32_t *geo, const uint32_t *nx, const uint32_t *ny,

@@ -181,6 +181,16 @@ _SIGNATURES = [
     ("vfb_debug_init_nonequilibrium_node", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_double,
       ctypes.POINTER(ctypes.c_double)]),
+    ("vfb_enstrophy", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_debug_enstrophy_nodes", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ("vfb_sim_enstrophy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.c_void_p]),
     ("vfb_debug_side_qs", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("vfb_grid_build", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_double), ctypes.c_int]),

@@ -64,7 +64,7 @@ struct Level {
     unsigned long long N = 0;
     uint32_t nFluid = 0;
     DeviceBuffer dist, nX, nY, nZ, geo, fluid;
-    DeviceBuffer nNeg; // the -x-y-z neighbour, uploaded for the non-equilibrium init only
+    DeviceBuffer nNeg; // the -x-y-z neighbour (non-equilibrium init, enstrophy)
     BcListDevice velocity, noSlip, slip, geometry;
     std::vector<PressureListDevice*> pressure;
     InterfaceDevice coarseToFine, fineToCoarse;
@@ -489,13 +489,15 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         auto* L = new Level;
         S->levels.push_back(L);
         rc = uploadLevel(*L, grid, l, P.storage, s, keep);
-        if (rc == VFB_OK && P.useInitNeq) {
+        if (rc == VFB_OK) {
+            // the inverse neighbour: required by useInitNeq, otherwise uploaded when the grid has it
             std::vector<char> nn;
             long long count = 0;
             int es = 0;
-            if (!gridArray(grid, l, "neighborNeg", nn, count, es) || es != 4 || (unsigned long long)count != L->N)
-                rc = setError(VFB_ERR_CONFIGURATION, "grid level %d: array neighborNeg (needed by useInitNeq)", l);
-            else {
+            if (!gridArray(grid, l, "neighborNeg", nn, count, es) || es != 4 || (unsigned long long)count != L->N) {
+                if (P.useInitNeq)
+                    rc = setError(VFB_ERR_CONFIGURATION, "grid level %d: array neighborNeg (needed by useInitNeq)", l);
+            } else {
                 keep.push_back(std::move(nn));
                 if (uploadRaw(L->nNeg, keep.back().data(), keep.back().size(), s) != cudaSuccess)
                     rc = setError(VFB_ERR_CUDA, "neighborNeg upload failed");
@@ -742,6 +744,34 @@ extern "C" int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* o
     return vfb_mass_and_energy(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->nX.ptr),
                                static_cast<const uint32_t*>(L->nY.ptr), static_cast<const uint32_t*>(L->nZ.ptr),
                                static_cast<const uint32_t*>(L->fluid.ptr), L->nFluid, L->isEven ? 1 : 0, out3, stream);
+}
+
+extern "C" int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!out2)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out2 is NULL");
+    if (!L->nNeg.ptr)
+        return setError(VFB_ERR_CONFIGURATION, "level %d has no inverse neighbour array", level);
+    const bool dbl = computeIsDouble(sim->params.storage);
+    const size_t bytes = L->N * (dbl ? sizeof(double) : sizeof(float));
+    DeviceBuffer m[4];
+    for (auto& b : m)
+        if (b.allocate(bytes) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "macroscopic buffers");
+    const auto* geo = static_cast<const uint32_t*>(L->geo.ptr);
+    const auto* nX = static_cast<const uint32_t*>(L->nX.ptr);
+    const auto* nY = static_cast<const uint32_t*>(L->nY.ptr);
+    const auto* nZ = static_cast<const uint32_t*>(L->nZ.ptr);
+    int rc = vfb_macroscopic(sim->params.storage, L->dist.ptr, L->N, geo, nX, nY, nZ, L->isEven ? 1 : 0, m[0].ptr,
+                             m[1].ptr, m[2].ptr, m[3].ptr, stream);
+    if (rc == VFB_OK)
+        rc = vfb_enstrophy(dbl ? VFB_FP64 : VFB_FP32, m[0].ptr, m[1].ptr, m[2].ptr, m[3].ptr, L->N, geo, nX, nY, nZ,
+                           static_cast<const uint32_t*>(L->nNeg.ptr), out2, stream);
+    return rc;
 }
 
 extern "C" int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* stream)

@@ -179,6 +179,21 @@ def init_nonequilibrium(dist, lat: DeviceLattice, rho, vx, vy, vz, omega: float,
                                                   float(omega), int(bool(is_even)), _stream(stream)))
 
 
+def enstrophy(lat: DeviceLattice, rho, vx, vy, vz, stream=None) -> tuple[float, int]:
+    """EnstrophyAnalyzer's value over one level's macroscopic fields (device
+    tensors of the compute precision): the mean of 1/2 (drho + 1) |curl u|^2
+    over the fluid nodes whose axis neighbours are fluid, and their number."""
+    if lat.neighborInverse is None:
+        raise _lib.VfbError(_lib.VFB_ERR_INVALID_ARGUMENT, "lattice has no inverse neighbour array (neighborNeg)")
+    precision = _lib.FP64 if rho.dtype == torch.float64 else _lib.FP32
+    out = (ctypes.c_double * 2)()
+    _lib.check(_lib.lib().vfb_enstrophy(precision, rho.data_ptr(), vx.data_ptr(), vy.data_ptr(), vz.data_ptr(), lat.N,
+                                        lat.geo.data_ptr(), lat.neighborX.data_ptr(), lat.neighborY.data_ptr(),
+                                        lat.neighborZ.data_ptr(), lat.neighborInverse.data_ptr(), out,
+                                        _stream(stream)))
+    return out[0], int(out[1])
+
+
 def macroscopic(dist, lat: DeviceLattice, is_even: bool, stream=None):
     """(drho, vx, vy, vz) of every node from the populations of one parity."""
     storage = STORAGE_OF_DTYPE[dist.dtype]

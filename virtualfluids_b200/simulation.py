@@ -252,6 +252,14 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_kinetic_energy(self._h, level, out, self.stream))
         return out[0], int(out[1])
 
+    def enstrophy(self, level: int = 0):
+        """EnstrophyAnalyzer's value: mean 1/2 (1 + drho) |curl u|^2 over the
+        fluid nodes whose six axis neighbours are fluid (FP64 sum), and their
+        number."""
+        out = (ctypes.c_double * 2)()
+        _lib.check(_lib.lib().vfb_sim_enstrophy(self._h, level, out, self.stream))
+        return out[0], int(out[1])
+
     def level_state(self, level: int = 0):
         """(device pointer of the populations, N, isEvenTimestep, omega)."""
         ptr = ctypes.c_void_p()
