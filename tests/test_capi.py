@@ -85,3 +85,51 @@ def test_grid_build_rejects_short_spec():
     s = (ctypes.c_double * 10)()
     assert not _lib.lib().vfb_grid_build(s, 10)
     assert "61" in _lib.last_error()
+
+
+def test_init_nonequilibrium_rejects_bad_arguments():
+    L = _lib.lib()
+    p = [1] * 9  # placeholders: the checks return before any device access
+    assert L.vfb_init_nonequilibrium(0, None, 10, *p[:9], 1.0, 1, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert L.vfb_init_nonequilibrium(0, 1, 10, *p[:9], 2.0, 1, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert "omega" in _lib.last_error()
+    assert L.vfb_init_nonequilibrium(0, 1, 1, *p[:9], 1.0, 1, None) == _lib.VFB_ERR_OUT_OF_RANGE
+    assert L.vfb_init_nonequilibrium(9, 1, 10, *p[:9], 1.0, 1, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+
+
+def test_outflow_rejects_bad_arguments():
+    L = _lib.lib()
+    t = _lib.BcLattice()
+    t.distributions = t.neighborX = t.neighborY = t.neighborZ = 1
+    t.numberOfLBnodes = 10
+    assert L.vfb_bc_outflow_nonreflecting(0, ctypes.byref(t), 1, 1, 0, 1, 0, 0.0, None) == _lib.VFB_OK  # empty list
+    assert L.vfb_bc_outflow_nonreflecting(0, ctypes.byref(t), 1, 1, 4, 7, 0, 0.0, None) == \
+        _lib.VFB_ERR_INVALID_ARGUMENT
+    assert "direction" in _lib.last_error()
+    assert L.vfb_bc_outflow_nonreflecting(0, ctypes.byref(t), None, 1, 4, 1, 0, 0.0, None) == \
+        _lib.VFB_ERR_INVALID_ARGUMENT
+    assert L.vfb_bc_outflow_nonreflecting(0, ctypes.byref(t), 1, 1, 4, 1, 1, float("nan"), None) == \
+        _lib.VFB_ERR_INVALID_ARGUMENT
+    assert L.vfb_bc_outflow_nonreflecting(8, ctypes.byref(t), 1, 1, 4, 1, 0, 0.0, None) == \
+        _lib.VFB_ERR_INVALID_ARGUMENT
+
+
+def test_enstrophy_rejects_bad_arguments():
+    L = _lib.lib()
+    out = (ctypes.c_double * 2)()
+    p = [1] * 9
+    assert L.vfb_enstrophy(1, *p[:4], 10, *p[:5], None, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert L.vfb_enstrophy(1, None, *p[:3], 10, *p[:5], out, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert L.vfb_enstrophy(2, *p[:4], 10, *p[:5], out, None) == _lib.VFB_ERR_INVALID_ARGUMENT
+    assert "precision" in _lib.last_error()
+    assert L.vfb_enstrophy(1, *p[:4], 1, *p[:5], out, None) == _lib.VFB_ERR_OUT_OF_RANGE
+
+
+def test_parameter_setters_of_the_new_options():
+    from virtualfluids_b200.simulation import Parameter, PressureBC
+    p = Parameter()
+    assert p.use_init_neq is False and p.outflow_pressure_correction_factor == 0.0
+    p.set_use_init_neq(True)
+    p.set_outflow_pressure_correction_factor(0.25)
+    assert p.use_init_neq is True and p.outflow_pressure_correction_factor == 0.25
+    assert int(PressureBC.OutflowNonReflective) == 1 and int(PressureBC.OutflowNonReflectivePressureCorrection) == 2
