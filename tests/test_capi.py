@@ -133,3 +133,20 @@ def test_parameter_setters_of_the_new_options():
     p.set_outflow_pressure_correction_factor(0.25)
     assert p.use_init_neq is True and p.outflow_pressure_correction_factor == 0.25
     assert int(PressureBC.OutflowNonReflective) == 1 and int(PressureBC.OutflowNonReflectivePressureCorrection) == 2
+
+
+def test_initial_condition_helpers():
+    import numpy as np
+    from virtualfluids_b200.simulation import Parameter
+    p = Parameter()
+    x = np.linspace(0.0, 10.0, 11)
+    p.set_initial_condition_uniform(0.01, -0.02, 0.0)
+    rho, vx, vy, vz = p.initial_condition(x, x, x)
+    assert np.all(rho == 0) and np.all(vx == 0.01) and np.all(vy == -0.02) and np.all(vz == 0)
+    p.set_initial_condition_log_law(0.3, 0.1, 10.0)
+    _, vx, vy, _ = p.initial_condition(x, x, x - 1.0)
+    assert vx[0] == 0.0 and vx[1] == 0.0  # z clipped at 0
+    assert abs(vx[-1] - 0.3 / 0.4 * np.log(9.0 / 0.1 + 1.0) / 10.0) < 1e-15 and np.all(vy == 0)
+    p.set_initial_condition_perturbed_log_law(0.3, 0.1, 100.0, 50.0, 20.0, 10.0)
+    _, vx, vy, vz = p.initial_condition(x, x, x)
+    assert np.all(np.isfinite(vx)) and np.all(np.isfinite(vz)) and np.abs(vy).max() > 0

@@ -145,6 +145,37 @@ class Parameter:
         """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
         self.initial_condition = init_func
 
+    # The pyfluids helpers (pythonbindings/src/gpu/submodules/parameter.cpp:98-133),
+    # evaluated in FP64 on the coordinate arrays.
+    def set_initial_condition_uniform(self, velocity_x: float, velocity_y: float, velocity_z: float):
+        """drho = 0 and a uniform velocity."""
+        v = (float(velocity_x), float(velocity_y), float(velocity_z))
+        self.initial_condition = lambda x, y, z: (0.0 * x, v[0] + 0.0 * x, v[1] + 0.0 * x, v[2] + 0.0 * x)
+
+    def set_initial_condition_log_law(self, u_star: float, z0: float, velocity_ratio: float):
+        """vx = u_star / 0.4 * log(max(z, 0) / z0 + 1) / velocity_ratio (von Karman constant 0.4)."""
+        def f(x, y, z):
+            zc = np.maximum(z, 0.0)
+            vx = u_star / 0.4 * np.log(zc / z0 + 1.0) / velocity_ratio
+            return 0.0 * x, vx, 0.0 * x, 0.0 * x
+        self.initial_condition = f
+
+    def set_initial_condition_perturbed_log_law(self, u_star: float, z0: float, length_x: float, length_z: float,
+                                                height: float, velocity_ratio: float):
+        """The log law plus the sinusoidal perturbations of the reference's
+        atmospheric boundary-layer set-up."""
+        def f(x, y, z):
+            zc = np.maximum(z, 0.0)
+            bump = 2.0 * np.sin(np.pi * 16.0 * x / length_x) * np.sin(np.pi * 8.0 * zc / height) / \
+                ((zc / height) ** 2 + 1.0)
+            vx = (u_star / 0.4 * np.log(zc / z0 + 1.0) + bump) / velocity_ratio
+            vy = bump / velocity_ratio
+            vz = 8.0 * u_star / 0.4 * (np.sin(np.pi * 8.0 * y / height) * np.sin(np.pi * 8.0 * zc / height) +
+                                       np.sin(np.pi * 8.0 * x / length_x)) / \
+                ((0.5 * length_z - zc) ** 2 + 1.0) / velocity_ratio
+            return 0.0 * x, vx, vy, vz
+        self.initial_condition = f
+
 
 def grid_from_arrays(levels) -> int:
     """A vfb_grid container holding the given levels (a list of dicts of named
