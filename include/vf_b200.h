@@ -290,7 +290,7 @@ int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t numberOfCells, co
  * (GEOMETRY)); [30..59] up to six side BCs as (side 0..5 = MX PX MY PY MZ PZ,
  * type 1 no-slip / 2 velocity / 3 pressure / 4 slip, three values) applied in
  * order (setNoSlip / setVelocity / setPressure / setSlipBoundaryCondition);
- * [60] enableThinWalls (not with a solid); [61] finest level of the box (0 =
+ * [60] enableThinWalls (with a solid: boundary nodes without a fluid neighbour become solid stoppers); [61] finest level of the box (0 =
  * 1; needs n >= 62).  Returns a handle, NULL on error.  Array names per level:
  * "geo", "neighborX/Y/Z", "neighborNeg", "coordX/Y/Z", "fluid", "dims",
  * "velocity.k/.q/.vx/.vy/.vz", "slip.k/.q/.nx/.ny/.nz", "geometry.k/.q",

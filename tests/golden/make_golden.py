@@ -9,6 +9,7 @@ machine without the reference tree.
     python tests/golden/make_golden.py                 (all fixtures)
     python tests/golden/make_golden.py --init-noneq    (the non-equilibrium init only)
     python tests/golden/make_golden.py --outflow       (the non-reflecting outflow only)
+    python tests/golden/make_golden.py --thin-walls    (the thin-wall grids only)
 """
 from __future__ import annotations
 
@@ -24,8 +25,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle.pyoracle import Reference  # noqa: E402
-from tests.golden.scenarios import (GRID_SCENARIOS, REFINED_SCENARIOS, grid_spec, lattice_sequence,  # noqa: E402
-                                    refined_spec)
+from tests.golden.scenarios import (GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS, grid_spec,  # noqa: E402
+                                    lattice_sequence, refined_spec)
 
 OUT = Path(__file__).resolve().parent
 
@@ -53,6 +54,15 @@ def k17_nodes(precision: str) -> None:
 def grids() -> None:
     R = Reference("f64")
     for name in GRID_SCENARIOS:
+        levels = R.grid(grid_spec(name))
+        arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
+        np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
+
+
+def thin_wall_grids() -> None:
+    """Solids built with thin walls, from the reference builder."""
+    R = Reference("f64")
+    for name in THIN_WALL_SCENARIOS:
         levels = R.grid(grid_spec(name))
         arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
         np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
@@ -131,6 +141,9 @@ if __name__ == "__main__":
             init_noneq(p)
         outflow(p)
         sys.exit(0)
+    if len(sys.argv) == 2 and sys.argv[1] == "--thin-walls":
+        thin_wall_grids()
+        sys.exit(0)
     if len(sys.argv) == 2 and sys.argv[1] == "--outflow":
         for p in ("f64", "f32"):
             outflow(p)
@@ -140,6 +153,7 @@ if __name__ == "__main__":
         lattice(p)
         init_noneq(p)
     grids()
+    thin_wall_grids()
     refined_grids()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

@@ -44,10 +44,26 @@ def grid_spec(name: str) -> np.ndarray:
         s[20:24] = [12, 7.3, 7.6, 3.2]
         s[26] = 1.0
         return s
+    if name in ("thin_wall_cube", "thin_wall_sphere"):
+        # a solid half a node above the no-slip floor of a 16^3 box, built
+        # with thin walls: the boundary nodes squeezed between the solid and
+        # the floor have no fluid neighbour and become solid stoppers
+        sides = [(MZ, NOSLIP, 0, 0, 0), (PZ, NOSLIP, 0, 0, 0)]
+        s = _spec([0, 0, 0, 15, 15, 15, 1.0], (1, 1, 0), sides=sides, thin_walls=True)
+        if name == "thin_wall_cube":
+            s[19] = 1.0
+            s[20:26] = [4, 4, 0.5, 10, 10, 6]
+        else:
+            s[19] = 2.0
+            s[20:24] = [7.3, 7.1, 3.5, 3.0]
+        s[26] = 1.0
+        return s
     raise KeyError(name)
 
 
 GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel", "sphere_channel"]
+# solids built with thin walls (MultipleGridBuilder::buildGrids(true))
+THIN_WALL_SCENARIOS = ["thin_wall_cube", "thin_wall_sphere"]
 
 # multi-level grids made by the reference's builder, which the repository's
 # builder reproduces: a channel 24 x 16 x 16 with a refined box and the

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from oracle.pyoracle import Reference, ref_available
-from tests.golden.scenarios import GRID_SCENARIOS, REFINED_SCENARIOS, grid_spec, refined_spec
+from tests.golden.scenarios import GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS, grid_spec, refined_spec
 from virtualfluids_b200 import grid as vgrid
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -47,6 +47,45 @@ def test_grid_matches_golden(name):
     levels = sorted({int(k.split(":")[0][1:]) for k in z.files})
     ref = [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith(f"L{lvl}:")} for lvl in levels]
     compare(build_mine(grid_spec(name)), ref)
+
+
+@pytest.mark.parametrize("name", THIN_WALL_SCENARIOS)
+def test_thin_wall_grid_matches_golden(name):
+    """buildGrids(enableThinWalls=true) with a solid: the boundary nodes
+    without a fluid neighbour become solid stoppers before the q computation
+    (GridImp::closeNeedleCellsThinWall); the whole grid, geometry list and q
+    values included, equals the reference builder's."""
+    z = np.load(GOLDEN / f"grid_{name}.npz")
+    ref = [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}]
+    mine = build_mine(grid_spec(name))
+    compare(mine, ref)
+    spec = grid_spec(name)
+    spec[60] = 0
+    plain = build_mine(spec)
+    # the thin-wall treatment removed boundary nodes from the geometry list
+    assert len(mine[0]["geometry.k"]) < len(plain[0]["geometry.k"])
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("kind", ["cube", "sphere"])
+@pytest.mark.parametrize("z0", [0.5, 1.0, 1.5])
+@pytest.mark.parametrize("periodic", [0, 1])
+def test_thin_walls_match_live_reference(kind, z0, periodic):
+    s = np.zeros(64)
+    s[0:7] = [0, 0, 0, 15, 15, 15, 1.0]
+    s[7:10] = [periodic, periodic, 0]
+    if kind == "cube":
+        s[19] = 1
+        s[20:26] = [4, 4, z0, 10, 10, 6]
+    else:
+        s[19] = 2
+        s[20:24] = [7.3, 7.1, z0 + 3.0, 3.0]
+    s[26] = 1
+    s[30:35] = [4, 1, 0, 0, 0]
+    s[35:40] = [5, 1, 0, 0, 0]
+    s[60] = 1
+    ref = Reference("f64").grid(s)
+    compare(build_mine(s), [ref[lvl] for lvl in sorted(ref)])
 
 
 def test_taylor_green_layout():
@@ -162,7 +201,6 @@ def _spec_with(**kv):
 
 
 @pytest.mark.parametrize("bad", [
-    {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s60": 1},          # thin walls with a solid: not supported
     {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s26": 2},          # velocity BC on the geometry: not supported
     {"s30": [7, 1, 0, 0, 0]},                                 # side id outside 0..5
     {"s30": [0, 9, 0, 0, 0]},                                 # unknown BC type

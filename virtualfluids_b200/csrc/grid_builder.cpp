@@ -399,8 +399,15 @@ void LevelGrid::findFluidNodes()
 // strictly inside the cuboid become INVALID_SOLID (GridImp::discretize
 // :251-268), needle cells are closed (:1362-1401), INVALID_SOLID nodes next to
 // fluid become STOPPER_SOLID (:449-453) and fluid nodes next to those BC_SOLID,
-// numbered in matrix order (:455-463).
-void LevelGrid::meshSolid(const Solid& solid)
+// numbered in matrix order (:455-463).  With thin walls
+// (MultipleGridBuilder.cpp:543-552) BC_SOLID nodes without a fluid neighbour
+// become STOPPER_SOLID before the q computation (GridImp::closeNeedleCellsThinWall,
+// GridImp.cpp:1403-1434); they keep their q slot, which stays unused.  The
+// reference's preceding search for further boundary nodes
+// (findQsPrimitive in the FindSolidBoundaryNodes stage, :1522-1555) only
+// visits nodes that already have a q slot, which are BC_SOLID, never FLUID,
+// so for a primitive it changes nothing and is not repeated here.
+void LevelGrid::meshSolid(const Solid& solid, bool thinWalls)
 {
     for (uint64_t idx = 0; idx < size; ++idx) {
         if (field[idx] == INVALID_SOLID)
@@ -440,6 +447,12 @@ void LevelGrid::meshSolid(const Solid& solid)
             field[idx] = BC_SOLID;
             solidBoundaryIndex[idx] = numberOfSolidBoundaryNodes++;
         }
+    }
+    if (thinWalls) {
+        // closing a node changes no FLUID node, so one pass reaches the fixed point
+        for (uint64_t idx = 0; idx < size; ++idx)
+            if (field[idx] == BC_SOLID && !hasNeighborOfType(idx, FLUID))
+                field[idx] = STOPPER_SOLID;
     }
     // GridImp::findQsPrimitive / calculateQs (GridImp.cpp:1522-1596): per
     // BC_SOLID node and link to a node of the grid, the distance to the
@@ -923,13 +936,11 @@ void GridBuilder::buildGrids(bool enableThinWalls)
 {
     if (grids.empty())
         throw std::runtime_error("buildGrids: no coarse grid");
-    if (enableThinWalls && hasSolid)
-        throw std::runtime_error("thin-wall treatment of solids is not supported");
     const int L = (int)grids.size();
     for (int level = L - 1; level >= 0; --level)
         grids[level]->initial(level + 1 < L ? grids[level + 1].get() : nullptr);
     if (hasSolid)
-        grids[L - 1]->meshSolid(solid);
+        grids[L - 1]->meshSolid(solid, enableThinWalls);
     for (int level = 0; level + 1 < L; ++level)
         grids[level]->findGridInterface(*grids[level + 1]);
     for (int level = 0; level + 1 < L; ++level)

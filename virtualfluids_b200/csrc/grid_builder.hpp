@@ -111,7 +111,7 @@ public:
     // solid primitive on this level (GridImp::mesh + findQsPrimitive for a
     // geometric primitive): inside nodes removed, one stopper layer inside the
     // solid, one BC_SOLID layer outside it, the links' q values
-    void meshSolid(const Solid& solid);
+    void meshSolid(const Solid& solid, bool thinWalls);
     // interface cells to the next finer level (GridImp::findGridInterface,
     // repairGridInterfaceOnMultiGPU) and their sparse renumbering
     void findGridInterface(LevelGrid& fine);
