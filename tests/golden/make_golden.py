@@ -10,6 +10,7 @@ machine without the reference tree.
     python tests/golden/make_golden.py --init-noneq    (the non-equilibrium init only)
     python tests/golden/make_golden.py --outflow       (the non-reflecting outflow only)
     python tests/golden/make_golden.py --thin-walls    (the thin-wall grids only)
+    python tests/golden/make_golden.py --extra-grids   (the cylinder grid only)
 """
 from __future__ import annotations
 
@@ -25,8 +26,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle.pyoracle import Reference  # noqa: E402
-from tests.golden.scenarios import (GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS, grid_spec,  # noqa: E402
-                                    lattice_sequence, refined_spec)
+from tests.golden.scenarios import (EXTRA_GRID_SCENARIOS, GRID_SCENARIOS, REFINED_SCENARIOS,  # noqa: E402
+                                    THIN_WALL_SCENARIOS, grid_spec, lattice_sequence, refined_spec)
 
 OUT = Path(__file__).resolve().parent
 
@@ -59,10 +60,11 @@ def grids() -> None:
         np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
 
 
-def thin_wall_grids() -> None:
-    """Solids built with thin walls, from the reference builder."""
+def thin_wall_grids(names=THIN_WALL_SCENARIOS) -> None:
+    """Solids built with thin walls (and the later solid scenarios), from the
+    reference builder."""
     R = Reference("f64")
-    for name in THIN_WALL_SCENARIOS:
+    for name in names:
         levels = R.grid(grid_spec(name))
         arrays = {f"L{lvl}:{k}": v for lvl, d in levels.items() for k, v in d.items()}
         np.savez_compressed(OUT / f"grid_{name}.npz", **arrays)
@@ -144,6 +146,9 @@ if __name__ == "__main__":
     if len(sys.argv) == 2 and sys.argv[1] == "--thin-walls":
         thin_wall_grids()
         sys.exit(0)
+    if len(sys.argv) == 2 and sys.argv[1] == "--extra-grids":
+        thin_wall_grids(EXTRA_GRID_SCENARIOS)
+        sys.exit(0)
     if len(sys.argv) == 2 and sys.argv[1] == "--outflow":
         for p in ("f64", "f32"):
             outflow(p)
@@ -154,6 +159,7 @@ if __name__ == "__main__":
         init_noneq(p)
     grids()
     thin_wall_grids()
+    thin_wall_grids(EXTRA_GRID_SCENARIOS)
     refined_grids()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

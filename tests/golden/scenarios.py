@@ -58,12 +58,22 @@ def grid_spec(name: str) -> np.ndarray:
             s[20:24] = [7.3, 7.1, 3.5, 3.0]
         s[26] = 1.0
         return s
+    if name == "cylinder_channel":
+        # a solid cylinder across a channel (axis y, the periodic direction)
+        sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 23, 11, 15, 1.0], (0, 1, 0), sides=sides)
+        s[19] = 3.0
+        s[20:26] = [8.4, 5.7, 7.3, 2.6, 6.0, 1]
+        s[26] = 1.0
+        return s
     raise KeyError(name)
 
 
 GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel", "sphere_channel"]
 # solids built with thin walls (MultipleGridBuilder::buildGrids(true))
 THIN_WALL_SCENARIOS = ["thin_wall_cube", "thin_wall_sphere"]
+# solids added after the first fixtures (generated with --extra-grids)
+EXTRA_GRID_SCENARIOS = ["cylinder_channel"]
 
 # multi-level grids made by the reference's builder, which the repository's
 # builder reproduces: a channel 24 x 16 x 16 with a refined box and the

@@ -11,7 +11,8 @@ import numpy as np
 import pytest
 
 from oracle.pyoracle import Reference, ref_available
-from tests.golden.scenarios import GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS, grid_spec, refined_spec
+from tests.golden.scenarios import (EXTRA_GRID_SCENARIOS, GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS,
+                                    grid_spec, refined_spec)
 from virtualfluids_b200 import grid as vgrid
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -64,6 +65,54 @@ def test_thin_wall_grid_matches_golden(name):
     plain = build_mine(spec)
     # the thin-wall treatment removed boundary nodes from the geometry list
     assert len(mine[0]["geometry.k"]) < len(plain[0]["geometry.k"])
+
+
+@pytest.mark.parametrize("name", EXTRA_GRID_SCENARIOS)
+def test_cylinder_grid_matches_golden(name):
+    """A solid cylinder (Cylinder::isPointInObject; no ray intersection, so
+    its links get q = 1/2 next to solid stoppers) across a channel."""
+    z = np.load(GOLDEN / f"grid_{name}.npz")
+    ref = [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}]
+    mine = build_mine(grid_spec(name))
+    compare(mine, ref)
+    assert len(mine[0]["geometry.k"]) > 100
+
+
+def test_cylinder_through_the_builder_api():
+    b = vgrid.MultipleGridBuilder()
+    s = grid_spec("cylinder_channel")
+    b.addCoarseGrid(*s[0:7])
+    b.addGeometry(vgrid.Cylinder(*s[20:25], vgrid.Axis.y))
+    b.setPeriodicBoundaryCondition(False, True, False)
+    b.buildGrids()
+    b.setVelocityBoundaryCondition(vgrid.SideType.MX, 0.04, 0.0, 0.0)
+    b.setPressureBoundaryCondition(vgrid.SideType.PX, 0.0)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.MZ)
+    b.setSlipBoundaryCondition(vgrid.SideType.PZ, 0.0, 0.0, 1.0)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.GEOMETRY)
+    z = np.load(GOLDEN / "grid_cylinder_channel.npz")
+    compare(b.arrays(), [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}])
+    with pytest.raises(ValueError):
+        vgrid.Cylinder(0, 0, 0, 1, 1, 3)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("thin", [0, 1])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_cylinders_match_live_reference(axis, thin, seed):
+    rng = np.random.default_rng(seed)
+    s = np.zeros(64)
+    s[0:7] = [0, 0, 0, 23, 19, 17, 1.0]
+    s[7:10] = [0, 1, 0]
+    c = [11.3 + rng.uniform(-1, 1), 9.6 + rng.uniform(-1, 1), 8.2 + rng.uniform(-1, 1)]
+    s[19] = 3
+    s[20:26] = [*c, rng.uniform(2.0, 4.0), rng.uniform(4.0, 8.0), axis]
+    s[26] = 1
+    s[30:50] = [0, 2, 0.04, 0, 0, 1, 3, 0, 0, 0, 4, 1, 0, 0, 0, 5, 4, 0, 0, 1]
+    s[60] = thin
+    ref = Reference("f64").grid(s)
+    compare(build_mine(s), [ref[lvl] for lvl in sorted(ref)])
 
 
 @pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")

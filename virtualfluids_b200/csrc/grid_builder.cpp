@@ -73,6 +73,17 @@ bool Solid::contains(double x, double y, double z) const
 {
     if (kind == Kind::Cuboid)
         return box.containsPoint(x, y, z);
+    if (kind == Kind::Cylinder) {
+        // Cylinder::isPointInObject with zero offsets (Cylinder.cpp:163-187):
+        // within half the height along the axis, strictly inside the circle
+        const double d[3] = { x - cx, y - cy, z - cz };
+        const double along = d[axis];
+        if (along > 0.5 * height || along < -0.5 * height)
+            return false;
+        const double a = d[(axis + 1) % 3], b = d[(axis + 2) % 3];
+        const double u = axis == 1 ? b : a, v = axis == 1 ? a : b; // the reference's (x, z) order for the y axis
+        return (u * u + v * v) < (r * r);
+    }
     // Sphere::isPointInObject with zero offsets (Sphere.cpp)
     const double dx = x - cx, dy = y - cy, dz = z - cz;
     return (dx * dx + dy * dy + dz * dz) < (r * r);
@@ -82,7 +93,7 @@ bool Solid::contains(double x, double y, double z) const
 // the smaller non-negative one
 bool Solid::intersect(double px, double py, double pz, double dx, double dy, double dz, double& t) const
 {
-    if (kind == Kind::Cuboid)
+    if (kind != Kind::Sphere) // Object::getIntersection (Object.cpp:42-45) reports no hit
         return false;
     const double rx = px - cx, ry = py - cy, rz = pz - cz;
     const double dd = dx * dx + dy * dy + dz * dz;

@@ -60,13 +60,15 @@ struct Box {
 // geometries/Sphere): which lattice points it holds and, for the sphere, where
 // a ray from a point along a lattice direction meets its surface.
 struct Solid {
-    enum class Kind { Cuboid, Sphere } kind = Kind::Cuboid;
+    enum class Kind { Cuboid, Sphere, Cylinder } kind = Kind::Cuboid;
     Box box {};                           // cuboid
-    double cx = 0, cy = 0, cz = 0, r = 0; // sphere
+    double cx = 0, cy = 0, cz = 0, r = 0; // sphere, cylinder (centre, radius)
+    double height = 0;                    // cylinder: length along its axis
+    int axis = 0;                         // cylinder: 0 x, 1 y, 2 z
     bool contains(double x, double y, double z) const;
     // Object::getIntersection: true with t (in units of the direction
     // vector) when the ray point + t * direction meets the surface at t >= 0;
-    // a cuboid reports no intersection, as the reference's primitive does
+    // a cuboid or cylinder reports no intersection, as the reference's primitives do
     bool intersect(double px, double py, double pz, double dx, double dy, double dz, double& t) const;
 };
 

@@ -74,6 +74,23 @@ class Sphere:
         self.centerX, self.centerY, self.centerZ, self.radius = centerX, centerY, centerZ, radius
 
 
+class Axis:
+    """Axis ids of a Cylinder (basics/geometry3d/Axis.h)."""
+    x, y, z = 0, 1, 2
+
+
+class Cylinder:
+    """Cylinder parallel to a coordinate axis: centre, radius, length along
+    the axis (geometries/Cylinder).  As a solid it has no ray intersection,
+    so, like a cuboid, its links get q = 1/2 next to solid stoppers."""
+
+    def __init__(self, centerX, centerY, centerZ, radius, height, rotationalAxis=Axis.z):
+        if int(rotationalAxis) not in (0, 1, 2):
+            raise ValueError("rotationalAxis must be Axis.x, Axis.y or Axis.z")
+        self.centerX, self.centerY, self.centerZ = centerX, centerY, centerZ
+        self.radius, self.height, self.rotationalAxis = radius, height, int(rotationalAxis)
+
+
 class MultipleGridBuilder:
     """Builder with the reference's call sequence: addCoarseGrid, (addGrid,
     addGeometry), setPeriodicBoundaryCondition, buildGrids, then the side
@@ -104,11 +121,15 @@ class MultipleGridBuilder:
         self.spec[17:19] = [fine, between]
 
     def addGeometry(self, solid):
-        """Solid primitive, meshed on the finest level: a Sphere, a Cuboid, or
-        a plain (minX, minY, minZ, maxX, maxY, maxZ) cuboid."""
+        """Solid primitive, meshed on the finest level: a Sphere, a Cylinder,
+        a Cuboid, or a plain (minX, minY, minZ, maxX, maxY, maxZ) cuboid."""
         if isinstance(solid, Sphere):
             self.spec[19] = 2
             self.spec[20:26] = [solid.centerX, solid.centerY, solid.centerZ, solid.radius, 0, 0]
+        elif isinstance(solid, Cylinder):
+            self.spec[19] = 3
+            self.spec[20:26] = [solid.centerX, solid.centerY, solid.centerZ, solid.radius, solid.height,
+                                solid.rotationalAxis]
         else:
             c = solid.box() if isinstance(solid, Cuboid) else tuple(solid)
             self.spec[19] = 1
