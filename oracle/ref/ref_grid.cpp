@@ -17,6 +17,7 @@
 #include "geometries/Cuboid/Cuboid.h"
 #include "geometries/Sphere/Sphere.h"
 #include "geometries/Cylinder/Cylinder.h"
+#include "geometries/VerticalCylinder/VerticalCylinder.h"
 #include "grid/BoundaryConditions/Side.h"
 #include "grid/GridBuilder/LevelGridBuilder.h"
 #include "grid/GridBuilder/MultipleGridBuilder.h"
@@ -93,7 +94,8 @@ extern "C" {
 //  [17..18] number of layers fine / between levels (used when [17] > 0)
 //  [19]     solid primitive: 1 Cuboid with [20..25] its extent, 2 Sphere with [20..23]
 //           centre and radius, 3 Cylinder with [20..25] centre, radius, height and
-//           axis (0 x, 1 y, 2 z)
+//           axis (0 x, 1 y, 2 z), 4 VerticalCylinder with [20..24] centre, radius and
+//           height
 //  [26..29] geometry BC type (1 no-slip, 2 velocity, 4 slip) and values
 //  [30..59] six side BCs in the order they are set: side id (0..5 = MX..PZ),
 //           type (0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip), 3 values
@@ -108,7 +110,9 @@ void* REF(vfref_grid_build)(const double* s)
     if (s[10] > 0)
         builder->addGrid(std::make_shared<Cuboid>(s[11], s[12], s[13], s[14], s[15], s[16]),
                          s[61] > 0 ? (uint)s[61] : 1u);
-    if (s[19] == 3)
+    if (s[19] == 4)
+        builder->addGeometry(std::make_shared<VerticalCylinder>(s[20], s[21], s[22], s[23], s[24]));
+    else if (s[19] == 3)
         builder->addGeometry(std::make_shared<Cylinder>(s[20], s[21], s[22], s[23], s[24], (Axis)(int)s[25]));
     else if (s[19] == 2)
         builder->addGeometry(std::make_shared<Sphere>(s[20], s[21], s[22], s[23]));

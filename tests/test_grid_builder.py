@@ -116,6 +116,31 @@ def test_cylinders_match_live_reference(axis, thin, seed):
 
 
 @pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("thin", [0, 1])
+def test_vertical_cylinder_matches_live_reference(thin):
+    """The reference's VerticalCylinder (spec kind 4) equals the cylinder
+    about the z axis, through the Python builder's VerticalCylinder too."""
+    s = np.zeros(64)
+    s[0:7] = [0, 0, 0, 19, 19, 15, 1.0]
+    s[19] = 4
+    s[20:25] = [9.4, 10.2, 7.1, 3.3, 6.5]
+    s[26] = 1
+    s[30:40] = [4, 1, 0, 0, 0, 5, 1, 0, 0, 0]
+    s[60] = thin
+    ref = Reference("f64").grid(s)
+    ref = [ref[lvl] for lvl in sorted(ref)]
+    compare(build_mine(s), ref)
+    b = vgrid.MultipleGridBuilder()
+    b.addCoarseGrid(*s[0:7])
+    b.addGeometry(vgrid.VerticalCylinder(*s[20:25]))
+    b.buildGrids(bool(thin))
+    b.setNoSlipBoundaryCondition(vgrid.SideType.MZ)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.PZ)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.GEOMETRY)
+    compare(b.arrays(), ref)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
 @pytest.mark.parametrize("kind", ["cube", "sphere"])
 @pytest.mark.parametrize("z0", [0.5, 1.0, 1.5])
 @pytest.mark.parametrize("periodic", [0, 1])

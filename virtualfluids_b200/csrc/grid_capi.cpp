@@ -166,7 +166,8 @@ extern "C" {
  * [10] refinement box present, [11..16] the box (min x,y,z, max x,y,z);
  * [17..18] layers fine / between levels (used when [17] > 0); [19] solid
  * primitive: 1 cuboid with [20..25] its extent, 2 sphere with [20..23]
- * centre and radius, 3 cylinder with [20..25] centre, radius, height, axis;
+ * centre and radius, 3 cylinder with [20..25] centre, radius, height, axis,
+ * 4 vertical cylinder with [20..24] centre, radius, height;
  * [26..29] geometry BC (type 1 =
  * no-slip); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
  * are set; [60] enableThinWalls; [61] finest level of the refinement box
@@ -191,14 +192,15 @@ void* vfb_grid_build(const double* s, int n)
         }
         if (s[19] > 0) {
             Solid solid;
-            if (s[19] == 3) {
+            if (s[19] == 3 || s[19] == 4) {
+                // 4: VerticalCylinder (VerticalCylinder.cpp:97-112), the same test about the z axis
                 solid.kind = Solid::Kind::Cylinder;
                 solid.cx = s[20];
                 solid.cy = s[21];
                 solid.cz = s[22];
                 solid.r = s[23];
                 solid.height = s[24];
-                solid.axis = (int)s[25];
+                solid.axis = s[19] == 4 ? 2 : (int)s[25];
                 if (solid.axis < 0 || solid.axis > 2)
                     throw std::invalid_argument("cylinder axis must be 0, 1 or 2");
             } else if (s[19] == 2) {

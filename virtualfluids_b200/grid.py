@@ -91,6 +91,11 @@ class Cylinder:
         self.radius, self.height, self.rotationalAxis = radius, height, int(rotationalAxis)
 
 
+def VerticalCylinder(centerX, centerY, centerZ, radius, height):
+    """geometries/VerticalCylinder: a cylinder about the z axis."""
+    return Cylinder(centerX, centerY, centerZ, radius, height, Axis.z)
+
+
 class MultipleGridBuilder:
     """Builder with the reference's call sequence: addCoarseGrid, (addGrid,
     addGeometry), setPeriodicBoundaryCondition, buildGrids, then the side
