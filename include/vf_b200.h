@@ -289,7 +289,10 @@ int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t numberOfCells, co
  * links' q values from the ray intersection, GridImp::calculateQs), 3 a
  * Cylinder with [20..25] centre, radius, height and axis (0 x, 1 y, 2 z;
  * no ray intersection, like the cuboid), 4 a VerticalCylinder with [20..24]
- * centre, radius and height; [26] geometry BC (1 = no-slip, setNoSlipBoundaryCondition
+ * centre, radius and height, 5 a Conglomerate (Conglomerate::add / subtract)
+ * of [62] added and [63] subtracted primitives, 7 values each (kind 1..4 and
+ * its parameters as above) from [64] on, n >= 64 + 7 parts (no ray
+ * intersection); [26] geometry BC (1 = no-slip, setNoSlipBoundaryCondition
  * (GEOMETRY)); [30..59] up to six side BCs as (side 0..5 = MX PX MY PY MZ PZ,
  * type 1 no-slip / 2 velocity / 3 pressure / 4 slip, three values) applied in
  * order (setNoSlip / setVelocity / setPressure / setSlipBoundaryCondition);

@@ -236,7 +236,7 @@ class Reference(_Lib):
 
     def grid(self, spec):
         """Build a grid with the reference builder; returns {level: {name: array}}."""
-        s = np.zeros(64)
+        s = np.zeros(max(64, len(spec)))
         s[:len(spec)] = spec
         h = self.fn("vfref_grid_build")(_ptr(s))
         try:

@@ -18,6 +18,7 @@
 #include "geometries/Sphere/Sphere.h"
 #include "geometries/Cylinder/Cylinder.h"
 #include "geometries/VerticalCylinder/VerticalCylinder.h"
+#include "geometries/Conglomerate/Conglomerate.h"
 #include "grid/BoundaryConditions/Side.h"
 #include "grid/GridBuilder/LevelGridBuilder.h"
 #include "grid/GridBuilder/MultipleGridBuilder.h"
@@ -95,12 +96,26 @@ extern "C" {
 //  [19]     solid primitive: 1 Cuboid with [20..25] its extent, 2 Sphere with [20..23]
 //           centre and radius, 3 Cylinder with [20..25] centre, radius, height and
 //           axis (0 x, 1 y, 2 z), 4 VerticalCylinder with [20..24] centre, radius and
-//           height
+//           height, 5 Conglomerate of [62] added and [63] subtracted primitives,
+//           7 values each (kind 1..4 and the parameters above) from [64] on
 //  [26..29] geometry BC type (1 no-slip, 2 velocity, 4 slip) and values
 //  [30..59] six side BCs in the order they are set: side id (0..5 = MX..PZ),
 //           type (0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip), 3 values
 //  [60]     enableThinWalls argument of buildGrids
 //  [61]     finest level of the refinement box (0 = level 1)
+// a primitive from 7 spec values: kind (1 Cuboid, 2 Sphere, 3 Cylinder,
+// 4 VerticalCylinder) and its parameters
+static std::shared_ptr<Object> primitive(const double* p)
+{
+    if (p[0] == 4)
+        return std::make_shared<VerticalCylinder>(p[1], p[2], p[3], p[4], p[5]);
+    if (p[0] == 3)
+        return std::make_shared<Cylinder>(p[1], p[2], p[3], p[4], p[5], (Axis)(int)p[6]);
+    if (p[0] == 2)
+        return std::make_shared<Sphere>(p[1], p[2], p[3], p[4]);
+    return std::make_shared<Cuboid>(p[1], p[2], p[3], p[4], p[5], p[6]);
+}
+
 void* REF(vfref_grid_build)(const double* s)
 {
     auto builder = std::make_shared<MultipleGridBuilder>();
@@ -110,14 +125,20 @@ void* REF(vfref_grid_build)(const double* s)
     if (s[10] > 0)
         builder->addGrid(std::make_shared<Cuboid>(s[11], s[12], s[13], s[14], s[15], s[16]),
                          s[61] > 0 ? (uint)s[61] : 1u);
-    if (s[19] == 4)
-        builder->addGeometry(std::make_shared<VerticalCylinder>(s[20], s[21], s[22], s[23], s[24]));
-    else if (s[19] == 3)
-        builder->addGeometry(std::make_shared<Cylinder>(s[20], s[21], s[22], s[23], s[24], (Axis)(int)s[25]));
-    else if (s[19] == 2)
-        builder->addGeometry(std::make_shared<Sphere>(s[20], s[21], s[22], s[23]));
-    else if (s[19] > 0)
-        builder->addGeometry(std::make_shared<Cuboid>(s[20], s[21], s[22], s[23], s[24], s[25]));
+    if (s[19] == 5) {
+        auto conglomerate = Conglomerate::makeShared();
+        const int nAdd = (int)s[62], nSub = (int)s[63];
+        for (int i = 0; i < nAdd + nSub; ++i) {
+            auto part = primitive(s + 64 + 7 * i);
+            if (i < nAdd)
+                conglomerate->add(part);
+            else
+                conglomerate->subtract(part);
+        }
+        builder->addGeometry(conglomerate);
+    } else if (s[19] > 0) {
+        builder->addGeometry(primitive(s + 19));
+    }
     builder->setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);
     builder->buildGrids(s[60] > 0);
 

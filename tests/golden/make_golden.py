@@ -10,7 +10,7 @@ machine without the reference tree.
     python tests/golden/make_golden.py --init-noneq    (the non-equilibrium init only)
     python tests/golden/make_golden.py --outflow       (the non-reflecting outflow only)
     python tests/golden/make_golden.py --thin-walls    (the thin-wall grids only)
-    python tests/golden/make_golden.py --extra-grids   (the cylinder grid only)
+    python tests/golden/make_golden.py --extra-grids   (the cylinder and conglomerate grids only)
 """
 from __future__ import annotations
 

@@ -66,6 +66,17 @@ def grid_spec(name: str) -> np.ndarray:
         s[20:26] = [8.4, 5.7, 7.3, 2.6, 6.0, 1]
         s[26] = 1.0
         return s
+    if name == "conglomerate_channel":
+        # three primitives united, a sphere removed from the cuboid
+        # (Conglomerate); parts as 7 values each from index 64 on
+        sides = [(MX, VELOCITY, 0.04, 0, 0), (PX, PRESSURE, 0.0, 0, 0), (MZ, NOSLIP, 0, 0, 0), (PZ, SLIP, 0, 0, 1)]
+        s = _spec([0, 0, 0, 27, 19, 17, 1.0], (0, 1, 0), sides=sides)
+        parts = [[1, 4, 5, 3, 9, 12, 9], [2, 15.2, 9.6, 8.1, 3.1, 0, 0], [3, 21.4, 9.8, 8.7, 2.2, 7.0, 1],
+                 [2, 6.5, 8.3, 7.0, 2.4, 0, 0]]
+        s[19] = 5.0
+        s[62:64] = [3, 1]
+        s[26] = 1.0
+        return np.concatenate([s, np.array(parts, float).ravel()])
     raise KeyError(name)
 
 
@@ -73,7 +84,7 @@ GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel", "sph
 # solids built with thin walls (MultipleGridBuilder::buildGrids(true))
 THIN_WALL_SCENARIOS = ["thin_wall_cube", "thin_wall_sphere"]
 # solids added after the first fixtures (generated with --extra-grids)
-EXTRA_GRID_SCENARIOS = ["cylinder_channel"]
+EXTRA_GRID_SCENARIOS = ["cylinder_channel", "conglomerate_channel"]
 
 # multi-level grids made by the reference's builder, which the repository's
 # builder reproduces: a channel 24 x 16 x 16 with a refined box and the

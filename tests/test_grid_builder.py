@@ -21,7 +21,8 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 def build_mine(spec):
     b = vgrid.MultipleGridBuilder()
     b.spec[:] = 0
-    b.spec[:len(spec)] = spec
+    b.spec[:min(64, len(spec))] = spec[:64]
+    b._extra = np.asarray(spec[64:], float)
     b._coarse = True
     b._built = True
     return b.arrays()
@@ -68,9 +69,10 @@ def test_thin_wall_grid_matches_golden(name):
 
 
 @pytest.mark.parametrize("name", EXTRA_GRID_SCENARIOS)
-def test_cylinder_grid_matches_golden(name):
-    """A solid cylinder (Cylinder::isPointInObject; no ray intersection, so
-    its links get q = 1/2 next to solid stoppers) across a channel."""
+def test_cylinder_and_conglomerate_grids_match_golden(name):
+    """A solid cylinder (Cylinder::isPointInObject) and a conglomerate of
+    primitives across a channel; neither has a ray intersection, so their
+    links get q = 1/2 next to solid stoppers."""
     z = np.load(GOLDEN / f"grid_{name}.npz")
     ref = [{k.split(":", 1)[1]: z[k] for k in z.files if k.startswith("L0:")}]
     mine = build_mine(grid_spec(name))
@@ -113,6 +115,55 @@ def test_cylinders_match_live_reference(axis, thin, seed):
     s[60] = thin
     ref = Reference("f64").grid(s)
     compare(build_mine(s), [ref[lvl] for lvl in sorted(ref)])
+
+
+def _conglomerate_spec(thin, with_subtract):
+    s = np.zeros(64 + 7 * 4)
+    s[0:7] = [0, 0, 0, 27, 19, 17, 1.0]
+    s[7:10] = [0, 1, 0]
+    s[19] = 5
+    parts = [[1, 4, 5, 3, 9, 12, 9],            # cuboid
+             [2, 15.2, 9.6, 8.1, 3.1, 0, 0],    # sphere (no q of its own inside a conglomerate)
+             [3, 21.4, 9.8, 8.7, 2.2, 7.0, 1]]  # cylinder along y
+    if with_subtract:
+        parts.append([2, 6.5, 8.3, 7.0, 2.4, 0, 0])  # a hole in the cuboid
+    s[62:64] = [3, len(parts) - 3]
+    for i, p in enumerate(parts):
+        s[64 + 7 * i: 71 + 7 * i] = p
+    s[26] = 1
+    s[30:50] = [0, 2, 0.04, 0, 0, 1, 3, 0, 0, 0, 4, 1, 0, 0, 0, 5, 4, 0, 0, 1]
+    s[60] = thin
+    return s[:64 + 7 * len(parts)]
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("thin", [0, 1])
+@pytest.mark.parametrize("with_subtract", [False, True])
+def test_conglomerate_matches_live_reference(thin, with_subtract):
+    """Several primitives as one solid (Conglomerate: union of the added,
+    minus the subtracted), through the spec and through the Python builder."""
+    s = _conglomerate_spec(thin, with_subtract)
+    ref = Reference("f64").grid(s)
+    ref = [ref[lvl] for lvl in sorted(ref)]
+    compare(build_mine(s), ref)
+    assert len(ref[0]["geometry.k"]) > 200
+    c = vgrid.Conglomerate()
+    c.add((4, 5, 3, 9, 12, 9))
+    c.add(vgrid.Sphere(15.2, 9.6, 8.1, 3.1))
+    c.add(vgrid.Cylinder(21.4, 9.8, 8.7, 2.2, 7.0, vgrid.Axis.y))
+    if with_subtract:
+        c.subtract(vgrid.Sphere(6.5, 8.3, 7.0, 2.4))
+    b = vgrid.MultipleGridBuilder()
+    b.addCoarseGrid(*s[0:7])
+    b.addGeometry(c)
+    b.setPeriodicBoundaryCondition(False, True, False)
+    b.buildGrids(bool(thin))
+    b.setVelocityBoundaryCondition(vgrid.SideType.MX, 0.04, 0.0, 0.0)
+    b.setPressureBoundaryCondition(vgrid.SideType.PX, 0.0)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.MZ)
+    b.setSlipBoundaryCondition(vgrid.SideType.PZ, 0.0, 0.0, 1.0)
+    b.setNoSlipBoundaryCondition(vgrid.SideType.GEOMETRY)
+    compare(b.arrays(), ref)
 
 
 @pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")

@@ -73,6 +73,16 @@ bool Solid::contains(double x, double y, double z) const
 {
     if (kind == Kind::Cuboid)
         return box.containsPoint(x, y, z);
+    if (kind == Kind::Conglomerate) {
+        // Conglomerate::isPointInObject (Conglomerate.cpp:153-164)
+        for (const Solid& part : subtract)
+            if (part.contains(x, y, z))
+                return false;
+        for (const Solid& part : add)
+            if (part.contains(x, y, z))
+                return true;
+        return false;
+    }
     if (kind == Kind::Cylinder) {
         // Cylinder::isPointInObject with zero offsets (Cylinder.cpp:163-187):
         // within half the height along the axis, strictly inside the circle

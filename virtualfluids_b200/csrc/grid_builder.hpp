@@ -60,15 +60,17 @@ struct Box {
 // geometries/Sphere): which lattice points it holds and, for the sphere, where
 // a ray from a point along a lattice direction meets its surface.
 struct Solid {
-    enum class Kind { Cuboid, Sphere, Cylinder } kind = Kind::Cuboid;
+    enum class Kind { Cuboid, Sphere, Cylinder, Conglomerate } kind = Kind::Cuboid;
     Box box {};                           // cuboid
     double cx = 0, cy = 0, cz = 0, r = 0; // sphere, cylinder (centre, radius)
     double height = 0;                    // cylinder: length along its axis
     int axis = 0;                         // cylinder: 0 x, 1 y, 2 z
+    std::vector<Solid> add, subtract;     // conglomerate: primitives united, then removed
     bool contains(double x, double y, double z) const;
     // Object::getIntersection: true with t (in units of the direction
     // vector) when the ray point + t * direction meets the surface at t >= 0;
-    // a cuboid or cylinder reports no intersection, as the reference's primitives do
+    // a cuboid, cylinder or conglomerate reports no intersection, as the
+    // reference's objects do
     bool intersect(double px, double py, double pz, double dx, double dy, double dz, double& t) const;
 };
 

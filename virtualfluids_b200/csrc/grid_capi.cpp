@@ -12,6 +12,36 @@
 
 namespace
 {
+// a primitive from 7 spec values: kind (1 cuboid, 2 sphere, 3 cylinder,
+// 4 vertical cylinder) and its parameters
+vfb::grid::Solid primitiveFrom(const double* p)
+{
+    using vfb::grid::Box;
+    using vfb::grid::Solid;
+    Solid solid;
+    if (p[0] == 3 || p[0] == 4) {
+        // 4: VerticalCylinder (VerticalCylinder.cpp:97-112), the same test about the z axis
+        solid.kind = Solid::Kind::Cylinder;
+        solid.cx = p[1];
+        solid.cy = p[2];
+        solid.cz = p[3];
+        solid.r = p[4];
+        solid.height = p[5];
+        solid.axis = p[0] == 4 ? 2 : (int)p[6];
+        if (solid.axis < 0 || solid.axis > 2)
+            throw std::invalid_argument("cylinder axis must be 0, 1 or 2");
+    } else if (p[0] == 2) {
+        solid.kind = Solid::Kind::Sphere;
+        solid.cx = p[1];
+        solid.cy = p[2];
+        solid.cz = p[3];
+        solid.r = p[4];
+    } else {
+        solid.box = Box { p[1], p[2], p[3], p[4], p[5], p[6] };
+    }
+    return solid;
+}
+
 using namespace vfb::grid;
 
 struct Exported {
@@ -167,7 +197,9 @@ extern "C" {
  * [17..18] layers fine / between levels (used when [17] > 0); [19] solid
  * primitive: 1 cuboid with [20..25] its extent, 2 sphere with [20..23]
  * centre and radius, 3 cylinder with [20..25] centre, radius, height, axis,
- * 4 vertical cylinder with [20..24] centre, radius, height;
+ * 4 vertical cylinder with [20..24] centre, radius, height, 5 conglomerate
+ * ([62] parts added, [63] parts subtracted, 7 values each from [64] on:
+ * kind 1..4 and its parameters);
  * [26..29] geometry BC (type 1 =
  * no-slip); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
  * are set; [60] enableThinWalls; [61] finest level of the refinement box
@@ -190,29 +222,25 @@ void* vfb_grid_build(const double* s, int n)
             const int levelFine = (n > 61 && s[61] > 0) ? (int)s[61] : 1;
             h->builder.addGrid(Box { s[11], s[12], s[13], s[14], s[15], s[16] }, levelFine);
         }
-        if (s[19] > 0) {
+        if (s[19] == 5) {
+            // Conglomerate (Conglomerate.cpp:153-164): [62] parts added, [63]
+            // parts subtracted, each 7 values from [64] on, added ones first
+            if (n < 64)
+                throw std::invalid_argument("a conglomerate needs the part counts at [62] and [63]");
+            const int nAdd = (int)s[62], nSub = (int)s[63];
+            if (nAdd < 1 || nSub < 0 || nAdd + nSub > 16 || n < 64 + 7 * (nAdd + nSub))
+                throw std::invalid_argument("conglomerate part counts do not fit the spec");
             Solid solid;
-            if (s[19] == 3 || s[19] == 4) {
-                // 4: VerticalCylinder (VerticalCylinder.cpp:97-112), the same test about the z axis
-                solid.kind = Solid::Kind::Cylinder;
-                solid.cx = s[20];
-                solid.cy = s[21];
-                solid.cz = s[22];
-                solid.r = s[23];
-                solid.height = s[24];
-                solid.axis = s[19] == 4 ? 2 : (int)s[25];
-                if (solid.axis < 0 || solid.axis > 2)
-                    throw std::invalid_argument("cylinder axis must be 0, 1 or 2");
-            } else if (s[19] == 2) {
-                solid.kind = Solid::Kind::Sphere;
-                solid.cx = s[20];
-                solid.cy = s[21];
-                solid.cz = s[22];
-                solid.r = s[23];
-            } else {
-                solid.box = Box { s[20], s[21], s[22], s[23], s[24], s[25] };
+            solid.kind = Solid::Kind::Conglomerate;
+            for (int i = 0; i < nAdd + nSub; ++i) {
+                const double* p = s + 64 + 7 * i;
+                if (p[0] < 1 || p[0] > 4)
+                    throw std::invalid_argument("a conglomerate part must be a primitive (kind 1..4)");
+                (i < nAdd ? solid.add : solid.subtract).push_back(primitiveFrom(p));
             }
             h->builder.addGeometry(solid);
+        } else if (s[19] > 0) {
+            h->builder.addGeometry(primitiveFrom(s + 19));
         }
         h->builder.setPeriodicBoundaryCondition(s[7] > 0, s[8] > 0, s[9] > 0);
         h->builder.buildGrids(s[60] > 0);

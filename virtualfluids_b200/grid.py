@@ -91,6 +91,30 @@ class Cylinder:
         self.radius, self.height, self.rotationalAxis = radius, height, int(rotationalAxis)
 
 
+class Conglomerate:
+    """geometries/Conglomerate: primitives united (add) minus primitives
+    removed (subtract); as a solid it has no ray intersection."""
+
+    def __init__(self):
+        self.added, self.subtracted = [], []
+
+    def add(self, obj):
+        self.added.append(obj)
+
+    def subtract(self, obj):
+        self.subtracted.append(obj)
+
+
+def _primitive_values(obj) -> list[float]:
+    """kind and the 6 parameters of a primitive, as the grid spec holds them."""
+    if isinstance(obj, Sphere):
+        return [2, obj.centerX, obj.centerY, obj.centerZ, obj.radius, 0, 0]
+    if isinstance(obj, Cylinder):
+        return [3, obj.centerX, obj.centerY, obj.centerZ, obj.radius, obj.height, obj.rotationalAxis]
+    c = obj.box() if isinstance(obj, Cuboid) else tuple(obj)
+    return [1, *c]
+
+
 def VerticalCylinder(centerX, centerY, centerZ, radius, height):
     """geometries/VerticalCylinder: a cylinder about the z axis."""
     return Cylinder(centerX, centerY, centerZ, radius, height, Axis.z)
@@ -103,6 +127,7 @@ class MultipleGridBuilder:
 
     def __init__(self):
         self.spec = np.zeros(64)
+        self._extra = np.zeros(0)   # conglomerate parts, from spec index 64 on
         self._coarse = False
         self._built = False
         self._bcs: list[tuple[int, int, float, float, float]] = []
@@ -128,17 +153,14 @@ class MultipleGridBuilder:
     def addGeometry(self, solid):
         """Solid primitive, meshed on the finest level: a Sphere, a Cylinder,
         a Cuboid, or a plain (minX, minY, minZ, maxX, maxY, maxZ) cuboid."""
-        if isinstance(solid, Sphere):
-            self.spec[19] = 2
-            self.spec[20:26] = [solid.centerX, solid.centerY, solid.centerZ, solid.radius, 0, 0]
-        elif isinstance(solid, Cylinder):
-            self.spec[19] = 3
-            self.spec[20:26] = [solid.centerX, solid.centerY, solid.centerZ, solid.radius, solid.height,
-                                solid.rotationalAxis]
+        if isinstance(solid, Conglomerate):
+            if not solid.added:
+                raise ValueError("a conglomerate needs at least one added object")
+            self.spec[19] = 5
+            self.spec[62:64] = [len(solid.added), len(solid.subtracted)]
+            self._extra = np.array([v for o in solid.added + solid.subtracted for v in _primitive_values(o)], float)
         else:
-            c = solid.box() if isinstance(solid, Cuboid) else tuple(solid)
-            self.spec[19] = 1
-            self.spec[20:26] = c
+            self.spec[19:26] = _primitive_values(solid)
 
     def setPeriodicBoundaryCondition(self, px: bool, py: bool, pz: bool):
         self.spec[7:10] = [float(px), float(py), float(pz)]
@@ -178,7 +200,7 @@ class MultipleGridBuilder:
         s = self.spec.copy()
         for i, b in enumerate(self._bcs):
             s[30 + 5 * i: 35 + 5 * i] = b
-        return s
+        return np.concatenate([s, self._extra])
 
     def arrays(self) -> list[dict[str, np.ndarray]]:
         """Run the native builder and return the arrays of every level."""
