@@ -343,7 +343,8 @@ typedef struct vfb_sim_params {
     int collisionKernel;       /* 0 "K17CompressibleNavierStokes", 1 "BGKCompSP27" (KernelTypes.h:36-38) */
     int velocityBC;            /* VFB_BC_VELOCITY_INTERPOLATED, VFB_BC_VELOCITY_BOUNCE_BACK or VFB_BC_VELOCITY_WITH_PRESSURE */
     int noSlipBC;              /* VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK, -1 NoSlipDelayBounceBack (no kernel) */
-    int geometryBC;            /* as noSlipBC, for the geometry list */
+    int geometryBC;            /* as noSlipBC, for the geometry list; or a velocity kind when the grid gives
+                                  the geometry a velocity (geometry.vx/vy/vz) */
     int slipBC;                /* VFB_BC_SLIP or -1 */
     int pressureBC;            /* 0 PressureNonEquilibriumCompressible, 1 OutflowNonReflective,
                                   2 OutflowNonReflectivePressureCorrection, -1 none */

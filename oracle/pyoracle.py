@@ -321,7 +321,8 @@ class ReferenceGpu(_Lib):
 
 _NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims", "fluid",
           "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k", "slip.nx", "slip.ny",
-          "slip.nz", "slip.q", "geometry.k", "geometry.q", "pressure.count", "cf.coarse", "cf.fine", "fc.coarse",
+          "slip.nz", "slip.q", "geometry.k", "geometry.q", "geometry.vx", "geometry.vy", "geometry.vz",
+          "pressure.count", "cf.coarse", "cf.fine", "fc.coarse",
           "fc.fine", "cf.offX", "cf.offY", "cf.offZ", "fc.offX", "fc.offY", "fc.offZ"]
 _INT_NAMES = {"velocity.k", "slip.k", "geometry.k", "pressure.count", "dims"}
 

@@ -208,6 +208,17 @@ void* REF(vfref_grid_build)(const double* s)
             builder->getGeometryIndices(gk.data(), level);
         A.put("geometry.k", gk.data(), ng);
         exportQs(A, "geometry.q", ng, &LevelGridBuilder::getGeometryQs, *builder, level);
+        // hasGeometryValues() is also true after a no-slip geometry BC
+        // (LevelGridBuilder.cpp:287-289), whose velocity lists stay empty, so
+        // reading them would run past their end: values only for a velocity
+        if (builder->hasGeometryValues() && (int)s[26] == 2) {
+            std::vector<real> gvx(ng), gvy(ng), gvz(ng);
+            if (ng)
+                builder->getGeometryValues(gvx.data(), gvy.data(), gvz.data(), level);
+            A.put("geometry.vx", gvx.data(), ng);
+            A.put("geometry.vy", gvy.data(), ng);
+            A.put("geometry.vz", gvz.data(), ng);
+        }
 
         const size_t npb = builder->getNumberOfPressureBoundaryConditions(level);
         int npbi = (int)npb;

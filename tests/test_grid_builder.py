@@ -137,6 +137,20 @@ def _conglomerate_spec(thin, with_subtract):
 
 
 @pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("name", ["sphere_channel", "cylinder_channel", "conglomerate_channel"])
+def test_velocity_on_the_geometry_matches_live_reference(name):
+    """setVelocityBoundaryCondition(GEOMETRY, vx, vy, vz): the same geometry
+    list, with the velocity of every node (LevelGridBuilder::getGeometryValues)."""
+    s = grid_spec(name).copy()
+    s[26:30] = [2, 0.01, -0.02, 0.005]
+    ref = Reference("f64").grid(s)
+    ref = [ref[lvl] for lvl in sorted(ref)]
+    mine = build_mine(s)
+    compare(mine, ref)
+    assert np.all(mine[0]["geometry.vy"] == -0.02) and len(mine[0]["geometry.vy"]) == len(mine[0]["geometry.k"])
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
 @pytest.mark.parametrize("thin", [0, 1])
 @pytest.mark.parametrize("with_subtract", [False, True])
 def test_conglomerate_matches_live_reference(thin, with_subtract):
@@ -326,7 +340,7 @@ def _spec_with(**kv):
 
 
 @pytest.mark.parametrize("bad", [
-    {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s26": 2},          # velocity BC on the geometry: not supported
+    {"s19": 1, "s20": [3, 3, 3, 6, 6, 6], "s26": 4},          # slip BC on the geometry: not supported
     {"s30": [7, 1, 0, 0, 0]},                                 # side id outside 0..5
     {"s30": [0, 9, 0, 0, 0]},                                 # unknown BC type
 ])

@@ -984,6 +984,15 @@ void GridBuilder::setNoSlipGeometryBoundaryCondition()
     geometryNoSlip = true;
 }
 
+// LevelGridBuilder::setVelocityGeometryBoundaryCondition (LevelGridBuilder.cpp:176-194):
+// the geometry list with one velocity for all its nodes
+void GridBuilder::setVelocityGeometryBoundaryCondition(double vx, double vy, double vz)
+{
+    setNoSlipGeometryBoundaryCondition();
+    geometryHasValues = true;
+    geometryValues = { vx, vy, vz };
+}
+
 static void addSide(std::vector<std::unique_ptr<LevelGrid>>& grids, std::vector<std::vector<BCList>>& lists,
                     SideType side, BCKind kind, double v0, double v1, double v2)
 {

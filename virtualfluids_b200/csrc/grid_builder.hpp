@@ -223,6 +223,7 @@ public:
     void setSlipBoundaryCondition(SideType side, double normalX, double normalY, double normalZ);
     // no-slip on the solid geometry's BC_SOLID nodes, every level
     void setNoSlipGeometryBoundaryCondition();
+    void setVelocityGeometryBoundaryCondition(double vx, double vy, double vz);
 
     int numberOfLevels() const { return (int)grids.size(); }
     LevelGrid& grid(int level) { return *grids.at(level); }
@@ -234,6 +235,9 @@ public:
     const std::vector<BCList>& slipBCs(int level) const { return slip.at(level); }
     const std::vector<BCList>& pressureBCs(int level) const { return pressure.at(level); }
     bool hasGeometryBC() const { return geometryNoSlip; }
+    // LevelGridBuilder::hasGeometryValues / getGeometryValues: a velocity on the geometry
+    bool hasGeometryValues() const { return geometryHasValues; }
+    const std::array<double, 3>& geometryVelocity() const { return geometryValues; }
 
 private:
     std::array<double, 6> staggeredCoordinates(const Box& shape, int level, int levelFine, bool odd[3]) const;
@@ -243,6 +247,8 @@ private:
     bool hasSolid = false;
     Solid solid {};
     bool geometryNoSlip = false;
+    bool geometryHasValues = false;
+    std::array<double, 3> geometryValues { 0.0, 0.0, 0.0 };
     bool built = false;
 };
 

@@ -152,6 +152,12 @@ void exportAll(GridHandle& h)
             g.geometryList(gk, gq);
         E.put("geometry.k", gk);
         E.put("geometry.q", gq);
+        if (b.hasGeometryValues()) {
+            const auto& v = b.geometryVelocity();
+            E.put("geometry.vx", std::vector<double>(gk.size(), v[0]));
+            E.put("geometry.vy", std::vector<double>(gk.size(), v[1]));
+            E.put("geometry.vz", std::vector<double>(gk.size(), v[2]));
+        }
         const auto& pres = b.pressureBCs(level);
         E.put("pressure.count", std::vector<int32_t> { (int32_t)pres.size() });
         for (size_t i = 0; i < pres.size(); ++i) {
@@ -200,8 +206,7 @@ extern "C" {
  * 4 vertical cylinder with [20..24] centre, radius, height, 5 conglomerate
  * ([62] parts added, [63] parts subtracted, 7 values each from [64] on:
  * kind 1..4 and its parameters);
- * [26..29] geometry BC (type 1 =
- * no-slip); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
+ * [26..29] geometry BC (type 1 = no-slip, 2 = velocity with [27..29]); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
  * are set; [60] enableThinWalls; [61] finest level of the refinement box
  * (0 = 1; n >= 62 values).  Same layout as the grid oracle.  Returns NULL on
  * error (see vfb_last_error).
@@ -249,9 +254,12 @@ void* vfb_grid_build(const double* s, int n)
             applyBC(h->builder, (int)b[0], (int)b[1], b[2], b[3], b[4]);
         }
         if (s[19] > 0 && (int)s[26] != 0) {
-            if ((int)s[26] != 1)
-                throw std::invalid_argument("only a no-slip boundary condition is supported on the geometry");
-            h->builder.setNoSlipGeometryBoundaryCondition();
+            if ((int)s[26] == 2)
+                h->builder.setVelocityGeometryBoundaryCondition(s[27], s[28], s[29]);
+            else if ((int)s[26] == 1)
+                h->builder.setNoSlipGeometryBoundaryCondition();
+            else
+                throw std::invalid_argument("only no-slip and velocity boundary conditions are supported on the geometry");
         }
         for (int level = 0; level < h->builder.numberOfLevels(); ++level)
             h->builder.grid(level).findFluidNodes();

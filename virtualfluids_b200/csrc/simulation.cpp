@@ -206,9 +206,15 @@ int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, st
     if (e == cudaSuccess)
         if (const int rc = list("slip", L.slip, false))
             return rc;
-    if (e == cudaSuccess)
-        if (const int rc = list("geometry", L.geometry, false))
+    if (e == cudaSuccess) {
+        // a velocity on the geometry (setVelocityBoundaryCondition(GEOMETRY, ...)) comes with the list
+        std::vector<char> probe;
+        long long pc = 0;
+        int pes = 0;
+        const bool geometryVelocity = gridArray(grid, level, "geometry.vx", probe, pc, pes);
+        if (const int rc = list("geometry", L.geometry, geometryVelocity))
             return rc;
+    }
     if (e == cudaSuccess && need("pressure.count", 4) && count == 1) {
         const int np = *reinterpret_cast<const int32_t*>(raw.data());
         for (int i = 0; i < np && e == cudaSuccess; ++i) {
@@ -472,7 +478,9 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         P.velocityBC != VFB_BC_VELOCITY_WITH_PRESSURE)
         return setError(VFB_ERR_INVALID_ARGUMENT, "velocityBC must be a velocity kind");
     if (!validKind(P.noSlipBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
-        !validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
+        !(validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
+          P.geometryBC == VFB_BC_VELOCITY_INTERPOLATED || P.geometryBC == VFB_BC_VELOCITY_BOUNCE_BACK ||
+          P.geometryBC == VFB_BC_VELOCITY_WITH_PRESSURE) ||
         !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC >= -1 && P.pressureBC <= 2))
         return setError(VFB_ERR_INVALID_ARGUMENT, "invalid boundary-condition selection");
     if (!(P.viscosity > 0.0))
@@ -489,6 +497,8 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         auto* L = new Level;
         S->levels.push_back(L);
         rc = uploadLevel(*L, grid, l, P.storage, s, keep);
+        if (rc == VFB_OK && P.geometryBC >= VFB_BC_VELOCITY_INTERPOLATED && L->geometry.n > 0 && !L->geometry.vx.ptr)
+            rc = setError(VFB_ERR_CONFIGURATION, "a velocity geometry BC needs the geometry velocities (level %d)", l);
         if (rc == VFB_OK) {
             // the inverse neighbour: required by useInitNeq, otherwise uploaded when the grid has it
             std::vector<char> nn;

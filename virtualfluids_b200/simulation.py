@@ -82,8 +82,13 @@ class BoundaryConditionFactory:
     def set_no_slip_boundary_condition(self, boundary_condition_type: NoSlipBC):
         self.no_slip = NoSlipBC(boundary_condition_type)
 
-    def set_geometry_boundary_condition(self, boundary_condition_type: NoSlipBC):
-        self.geometry = NoSlipBC(boundary_condition_type)
+    def set_geometry_boundary_condition(self, boundary_condition_type):
+        """A no-slip kind, or a velocity kind for a geometry given a velocity
+        (setVelocityBoundaryCondition(SideType.GEOMETRY, ...))."""
+        if isinstance(boundary_condition_type, VelocityBC):
+            self.geometry = boundary_condition_type
+        else:
+            self.geometry = NoSlipBC(boundary_condition_type)
 
     def set_slip_boundary_condition(self, boundary_condition_type: SlipBC):
         self.slip = SlipBC(boundary_condition_type)
