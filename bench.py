@@ -146,61 +146,88 @@ def whole_job_rate(units_per_rank: int, world: int, slowest_ms: float) -> float:
 # --------------------------------------------------------------------------- #
 # reference arm: the reference's CPU K17 path on the host cores
 # --------------------------------------------------------------------------- #
-def cpu_reference_mlups(n_block: int, steps: int):
+def host_cpu() -> dict:
+    """Thread count and CPU model of this host (the cores the CPU legs use)."""
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    model = None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"threads": threads, "model": model}
+
+
+def cpu_reference_block(n: int, u0: float):
+    """The reference CPU path's EsoSplit block holding the n^3 Taylor-Green
+    vortex, or None when oracle/_ref is absent."""
     from oracle.pyoracle import Reference, ref_available
     if not ref_available("f32"):
         return None
-    R = Reference("f32")
-    sec, mlups = R.cpu_block_mlups(n_block, steps)
-    return {"value": mlups, "seconds": sec, "cores": os.cpu_count(), "block": n_block, "steps": steps}
+    return Reference("f32").cpu_tgv_block(n, u0)
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU K17 loop (EsoSplit storage, FP32, OpenMP on every
+    host thread) on the same Taylor-Green n^3 workload: one block created
+    once, W untimed passes, then K passes each timed as one step."""
     if rank != 0:
         return 0
-    import platform
-    n_block = 96
-    rows = []
+    cpu = host_cpu()
+    omega = 1.0 / (3.0 * (args.u0 * (args.n / (2 * math.pi)) / 1600.0) + 0.5)
+    t0 = time.time()
+    block = cpu_reference_block(args.n, args.u0)
+    if block is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent)"}))
+        return 0
+    setup_s = time.time() - t0
     for _ in range(args.warmup):
-        cpu_reference_mlups(n_block, 1)
-    for _ in range(args.steps):
-        r = cpu_reference_mlups(n_block, 2)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent)"}))
-            return 0
-        rows.append(r)
-    value = statistics.median([r["value"] for r in rows])
-    sample = (f"{n_block}^3 block of the reference CPU K17 loop (EsoSplit storage, FP32), 2 passes per step, "
-              f"OpenMP over x3 on {os.cpu_count()} threads ({platform.processor() or platform.machine()})")
+        block.run(1, omega)
+    secs = [block.run(1, omega) for _ in range(args.steps)]
+    block.close()
+    nodes = args.n ** 3
+    value = nodes * len(secs) / sum(secs) / 1e6
+    sample = (f"the whole {args.n}^3 Taylor-Green block in the reference CPU K17 loop (EsoSplit storage, FP32), "
+              f"{args.steps} timed passes after {args.warmup} warm-up passes on the same block, OpenMP on "
+              f"{cpu['threads']} threads ({cpu['model']})")
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median([r["seconds"] for r in rows]),
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"taylor-green {args.n}^3 K17 (sampled on a {n_block}^3 block)",
-                       "storage": "fp32"},
-            "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+            "config": {"workload": f"taylor-green {args.n}^3 periodic, K17 cumulant, fp32 storage",
+                       "fluid_nodes": nodes, "same_config": True, "setup_s": round(setup_s, 1),
+                       "cpu_threads": cpu["threads"], "cpu_model": cpu["model"]},
+            "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cpu["threads"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
-def cpu_baseline(seconds_target: float = 12.0):
-    """The reference CPU K17 path timed on the host cores for about
-    `seconds_target` seconds (rank 0, one GPU only)."""
+def cpu_baseline(n: int, u0: float, omega: float, seconds_target: float = 12.0):
+    """The reference CPU K17 path on the host cores for about
+    `seconds_target` seconds (rank 0, one GPU only): the same n^3
+    Taylor-Green block as the reference arm, created once, one warm-up pass,
+    then whole passes until the target time is reached."""
+    cpu = host_cpu()
     try:
-        first = cpu_reference_mlups(96, 1)
+        block = cpu_reference_block(n, u0)
     except Exception as e:  # the baseline must not sink the GPU result
-        return {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+        return {"value": None, "unit": "MLUPS", "cores": cpu["threads"], "kind": "reference",
                 "sample": f"failed: {e}"}
-    if first is None:
-        return {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
+    if block is None:
+        return {"value": None, "unit": "MLUPS", "cores": cpu["threads"], "kind": "reference",
                 "sample": "oracle/_ref not built"}
-    steps = int(max(1, min(5000, seconds_target / max(first["seconds"], 1e-3))))
-    r = cpu_reference_mlups(96, steps)
-    return {"value": r["value"], "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"reference CPU K17 loop (EsoSplit, FP32) on a 96^3 block, {steps} passes, "
-                      f"{r['seconds']:.1f} s, OpenMP on {os.cpu_count()} threads"}
+    first = block.run(1, omega)
+    passes = int(max(1, min(1000, seconds_target / max(first, 1e-3))))
+    sec = block.run(passes, omega)
+    block.close()
+    return {"value": n ** 3 * passes / sec / 1e6, "unit": "MLUPS", "cores": cpu["threads"], "kind": "reference",
+            "sample": f"reference CPU K17 loop (EsoSplit, FP32) on the whole {n}^3 Taylor-Green block, {passes} "
+                      f"passes after one warm-up pass, {sec:.1f} s, OpenMP on {cpu['threads']} threads "
+                      f"({cpu['model']})"}
 
 
 def run_gpu(args, world, rank, local):
@@ -311,16 +338,20 @@ def run_gpu(args, world, rank, local):
     out_np = [t.numpy() for t in out_pinned]
     barrier(world)
     torch.cuda.synchronize(device)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    e0, ea, eb, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     e0.record(stream)
     sim.init_level(0, *fields_np)
+    ea.record(stream)
     sim.run(args.steps)
+    eb.record(stream)
     out_host = sim.macroscopic(0, out=out_np)
     e1.record(stream)
     torch.cuda.synchronize(device)
     barrier(world)
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    # where the end-to-end time goes (rank 0's events)
+    e2e_parts = {"h2d_and_init_ms": e0.elapsed_time(ea), "steps_ms": ea.elapsed_time(eb),
+                 "macroscopic_and_d2h_ms": eb.elapsed_time(e1)}
     h2d = sum(a.nbytes for a in fields_np)
     d2h = sum(a.nbytes for a in out_host)
     finite = bool(np.isfinite(out_host[1][g["fluid"][:1000]]).all())
@@ -356,11 +387,11 @@ def run_gpu(args, world, rank, local):
                      "avg_launch_ms": avg_launch_ms},
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
-                "d2h_bytes_per_step": d2h // args.steps},
+                "d2h_bytes_per_step": d2h // args.steps, "breakdown": e2e_parts},
         "gpu_launches": args.steps * (2 if lane_nodes else 1),
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(args.n, args.u0, omega)
     print(json.dumps(line), flush=True)
     return 0
 

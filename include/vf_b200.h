@@ -356,6 +356,10 @@ typedef struct vfb_sim_params {
     int useInitNeq;            /* 1: vfb_sim_init_level writes equilibrium plus the strain-rate part
                                   (Parameter::setUseInitNeq); the grid must carry neighborNeg */
     double outflowPressureCorrectionFactor; /* pressureBC 2 (Parameter::setOutflowPressureCorrectionFactor) */
+    double velocityRatio;      /* Parameter::getVelocityRatio (world to lattice units): the geometry list's
+                                  velocities are divided by it at upload, in the compute precision, as
+                                  GridGenerator.cpp:507-513 does (side velocity BCs are not scaled);
+                                  0 or 1: no scaling */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;
@@ -478,7 +482,9 @@ int vfb_mass_and_energy(int storage, const void* distributions, unsigned long lo
  * the array's device address; make that first call before any stream
  * capture.  All calls on a device share the array, so calls that overlap on
  * the GPU (other streams, other host threads) race; the call synchronises its
- * stream before it returns.
+ * stream before it returns.  The looked-up address belongs to the device's
+ * context: after a cudaDeviceReset of that device in the same process it is
+ * stale, so do not call this entry point on that device again after a reset.
  */
 int vfb_mass_and_energy_static(int storage, const void* distributions, unsigned long long numberOfLBnodes,
                                const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,

@@ -177,6 +177,8 @@ class Reference(_Lib):
         self.fn("vfref_grid_free").argtypes = [_vp]
         self.fn("vfref_cpu_block_create").restype = _vp
         self.fn("vfref_cpu_block_create").argtypes = [_c.c_int, _c.c_int, _c.c_int]
+        self.fn("vfref_cpu_block_create_tgv").restype = _vp
+        self.fn("vfref_cpu_block_create_tgv").argtypes = [_c.c_int, _c.c_double]
         self.fn("vfref_cpu_block_free").argtypes = [_vp]
         self.fn("vfref_cpu_block_run").restype = _c.c_double
         self.fn("vfref_cpu_block_run").argtypes = [_vp, _c.c_int, R]
@@ -247,6 +249,11 @@ class Reference(_Lib):
         finally:
             self.fn("vfref_grid_free")(h)
 
+    def cpu_tgv_block(self, n: int, u0: float = 0.05) -> "CpuBlock":
+        """The reference CPU path's EsoSplit block holding the n^3 Taylor-Green
+        vortex (created once; run passes on it with .run)."""
+        return CpuBlock(self, self.fn("vfref_cpu_block_create_tgv")(n, u0), n)
+
     def cpu_block_mlups(self, n: int, steps: int, omega: float = 1.9) -> tuple[float, float]:
         """Run the reference CPU K17 loop on an n^3 block; returns (seconds, MLUPS)."""
         h = self.fn("vfref_cpu_block_create")(n, n, n)
@@ -255,6 +262,27 @@ class Reference(_Lib):
         finally:
             self.fn("vfref_cpu_block_free")(h)
         return sec, steps * n ** 3 / sec / 1e6
+
+
+class CpuBlock:
+    """An EsoSplit block of the reference CPU path kept between timed passes."""
+
+    def __init__(self, ref: "Reference", handle, n: int):
+        self.ref, self.h, self.n = ref, handle, n
+        if not handle:
+            raise MemoryError(f"could not create the {n}^3 CPU block")
+
+    def run(self, steps: int, omega: float) -> float:
+        """`steps` collision passes of the reference CPU K17 loop; seconds."""
+        return self.ref.fn("vfref_cpu_block_run")(self.h, steps, omega)
+
+    def close(self):
+        if self.h:
+            self.ref.fn("vfref_cpu_block_free")(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def ref_gpu_available(precision: str = "f64") -> bool:

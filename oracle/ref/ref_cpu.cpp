@@ -10,6 +10,7 @@
 // (src/cpu/core/Simulation/Simulation.cpp:366-401), so this is the same work
 // per thread.  Used to time the reference CPU path on the host.
 #include <chrono>
+#include <cmath>
 #include <memory>
 
 #include <basics/DataTypes.h>
@@ -18,6 +19,7 @@
 #include <lbm/collision/TurbulentViscosity.h>
 
 #include "Data/EsoSplit.h"
+#include "LBM/D3Q27System.h"
 
 #ifdef VF_DOUBLE_ACCURACY
 #define REF(name) name##_f64
@@ -40,6 +42,34 @@ void* REF(vfref_cpu_block_create)(int nx1, int nx2, int nx3)
                     f[d] = (real)1e-4 * (real)(((x * 7 + y * 13 + z * 29 + (size_t)d * 3) % 17) - 8);
                 e->setPreCollisionDistribution(f, x, y, z);
             }
+    return e;
+}
+
+// A block holding the Taylor-Green vortex of the benchmark workload (n^3
+// interior nodes on [-pi, pi)^3, u0, the density of the workload's formula),
+// set to the reference CPU path's compressible equilibrium
+// (D3Q27System::calcCompFeq) in every node, ghost layer included.  The nodes
+// are written in parallel over x3.
+void* REF(vfref_cpu_block_create_tgv)(int n, double u0)
+{
+    const size_t m = (size_t)n + 2;
+    auto* e = new EsoSplit(m, m, m, (real)0);
+    const double h = 2.0 * M_PI / n;
+#pragma omp parallel for schedule(static)
+    for (long long z = 0; z < (long long)m; ++z) {
+        real f[27];
+        for (size_t y = 0; y < m; ++y)
+            for (size_t x = 0; x < m; ++x) {
+                const double X = -M_PI + h * ((double)x - 1.0), Y = -M_PI + h * ((double)y - 1.0),
+                             Z = -M_PI + h * ((double)z - 1.0);
+                const real vx = (real)(u0 * std::sin(X) * std::cos(Y) * std::cos(Z));
+                const real vy = (real)(-u0 * std::cos(X) * std::sin(Y) * std::cos(Z));
+                const real drho = (real)(3.0 * (u0 * u0 / 16.0) * (std::cos(2 * X) + std::cos(2 * Y)) *
+                                         (std::cos(2 * Z) + 2.0));
+                D3Q27System::calcCompFeq(f, drho, vx, vy, (real)0);
+                e->setPreCollisionDistribution(f, x, y, (size_t)z);
+            }
+    }
     return e;
 }
 

@@ -81,3 +81,26 @@ def test_reference_arm_runs_on_rank_zero_only():
     outs = _launch(REFERENCE_ARM)
     assert outs[0].strip().endswith("rank0")
     assert outs[1].strip() == ""
+
+
+def test_reference_arm_line_on_a_small_block(capsys):
+    """The reference arm's JSON line: one block created once, W untimed and K
+    timed passes, the same workload name as the GPU arm, the host's threads
+    and CPU model recorded."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from oracle.pyoracle import ref_available
+    if not ref_available("f32"):
+        pytest.skip("reference build oracle/_ref absent")
+
+    class A:
+        steps, warmup, n, gpus, u0 = 3, 1, 16, 1, 0.05
+
+    assert bench.run_reference(A, 1, 0) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "MLUPS" and line["value"] > 0
+    assert line["config"]["workload"] == "taylor-green 16^3 periodic, K17 cumulant, fp32 storage"
+    assert line["config"]["same_config"] is True and line["config"]["fluid_nodes"] == 16 ** 3
+    assert line["cpu_baseline"]["cores"] == line["config"]["cpu_threads"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}

@@ -150,3 +150,37 @@ def test_initial_condition_helpers():
     p.set_initial_condition_perturbed_log_law(0.3, 0.1, 100.0, 50.0, 20.0, 10.0)
     _, vx, vy, vz = p.initial_condition(x, x, x)
     assert np.all(np.isfinite(vx)) and np.all(np.isfinite(vz)) and np.abs(vy).max() > 0
+
+
+def test_geometry_bc_setter_accepts_plain_ints():
+    """set_geometry_boundary_condition takes either enum's members or their
+    plain values: no-slip kinds first, then the velocity kinds."""
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, NoSlipBC, Parameter, VelocityBC
+    bc = BoundaryConditionFactory()
+    for kind in NoSlipBC:
+        bc.set_geometry_boundary_condition(int(kind))
+        assert bc.geometry is kind
+    for kind in VelocityBC:
+        bc.set_geometry_boundary_condition(int(kind))
+        assert bc.geometry is kind
+        bc.set_geometry_boundary_condition(kind)
+        assert bc.geometry is kind
+    with pytest.raises(ValueError):
+        bc.set_geometry_boundary_condition(99)
+    p = Parameter()
+    assert p.velocity_ratio == 1.0
+    p.set_velocity_ratio(2.5)
+    assert p.velocity_ratio == 2.5
+    with pytest.raises(ValueError):
+        p.set_velocity_ratio(0.0)
+
+
+def test_sim_params_layout_matches_header():
+    """The ctypes mirror of vfb_sim_params lists the header's fields in order."""
+    import re
+    from pathlib import Path
+    from virtualfluids_b200.simulation import VfbSimParams
+    text = Path(__file__).resolve().parents[1].joinpath("include", "vf_b200.h").read_text()
+    body = text[text.index("typedef struct vfb_sim_params {"):text.index("} vfb_sim_params;")]
+    names = re.findall(r"^\s+(?:int|double)\s+(\w+)", body, re.M)
+    assert names == [f[0] for f in VfbSimParams._fields_]

@@ -44,7 +44,7 @@ def initial(g, seed):
 class HostSchedule:
     """UpdateGrid27::updateGrid for all levels on the host."""
 
-    def __init__(self, lv, inits, slip=False, geometry=False):
+    def __init__(self, lv, inits, slip=False, geometry=False, nu=NU):
         self.slip, self.geometry = slip, geometry
         self.O = Oracle("f64")
         self.lv = lv
@@ -56,7 +56,7 @@ class HostSchedule:
                 self.O.init_eq(d, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], *init, ev)
             self.d.append(d)
         self.even = [True] * len(lv)
-        self.omega = [1.0 / (3.0 * NU * 2 ** l + 0.5) for l in range(len(lv))]
+        self.omega = [1.0 / (3.0 * nu * 2 ** l + 0.5) for l in range(len(lv))]
 
     def update(self, level):
         O, g, d = self.O, self.lv[level], self.d[level]

@@ -123,7 +123,10 @@ __global__ void __launch_bounds__(kStaticThreads)
 }
 
 // Device address of the scratch on the current device, looked up once per
-// device; nullptr (and the error recorded) if the lookup fails.
+// device; nullptr (and the error recorded) if the lookup fails.  The address
+// is that of the device's context at the first call: a cudaDeviceReset
+// destroys that context, after which the cached address is stale (the header
+// tells callers not to use the entry point on a device after a reset).
 static StaticMassEnergyScratch* scratchOnCurrentDevice()
 {
     static std::mutex lock;

@@ -129,8 +129,11 @@ cudaError_t uploadRaw(DeviceBuffer& b, const void* host, size_t bytes, cudaStrea
 }
 
 // uploads a double array as the compute precision of the storage
+// Host doubles into a device array of the compute precision.  A divisor other
+// than 1 divides every value after the conversion, in the compute precision, as
+// the reference scales the geometry velocities (GridGenerator.cpp:507-513).
 cudaError_t uploadReal(DeviceBuffer& b, const std::vector<char>& raw, int storage, cudaStream_t s,
-                       std::vector<std::vector<char>>& keep)
+                       std::vector<std::vector<char>>& keep, double divisor = 1.0)
 {
     const size_t n = raw.size() / sizeof(double);
     const double* src = reinterpret_cast<const double*>(raw.data());
@@ -138,16 +141,23 @@ cudaError_t uploadReal(DeviceBuffer& b, const std::vector<char>& raw, int storag
     std::vector<char>& host = keep.back();
     if (computeIsDouble(storage)) {
         host = raw;
+        if (divisor != 1.0) {
+            double* dst = reinterpret_cast<double*>(host.data());
+            for (size_t i = 0; i < n; ++i)
+                dst[i] = dst[i] / divisor;
+        }
     } else {
         host.resize(n * sizeof(float));
         float* dst = reinterpret_cast<float*>(host.data());
+        const float d = (float)divisor;
         for (size_t i = 0; i < n; ++i)
-            dst[i] = (float)src[i];
+            dst[i] = divisor != 1.0 ? (float)src[i] / d : (float)src[i];
     }
     return uploadRaw(b, host.data(), host.size(), s);
 }
 
-int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, std::vector<std::vector<char>>& keep)
+int uploadLevel(Level& L, void* grid, int level, int storage, double geometryVelocityDivisor, cudaStream_t s,
+                std::vector<std::vector<char>>& keep)
 {
     std::vector<char> raw;
     long long count = 0;
@@ -178,7 +188,7 @@ int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, st
         e = uploadRaw(L.fluid, keep.back().data(), raw.size(), s);
     }
     // compacted BC lists: k (int32), q (27 * n doubles), velocities
-    auto list = [&](const std::string& prefix, BcListDevice& B, bool velocity) -> int {
+    auto list = [&](const std::string& prefix, BcListDevice& B, bool velocity, double divisor = 1.0) -> int {
         if (!need((prefix + ".k").c_str(), 4))
             return fail((prefix + ".k").c_str());
         B.n = (uint32_t)count;
@@ -195,7 +205,7 @@ int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, st
             for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
                 if (!need((prefix + v[i]).c_str(), 8) || (uint32_t)count != B.n)
                     return fail((prefix + v[i]).c_str());
-                e = uploadReal(*vb[i], raw, storage, s, keep);
+                e = uploadReal(*vb[i], raw, storage, s, keep, divisor);
             }
         }
         return VFB_OK;
@@ -212,7 +222,7 @@ int uploadLevel(Level& L, void* grid, int level, int storage, cudaStream_t s, st
         long long pc = 0;
         int pes = 0;
         const bool geometryVelocity = gridArray(grid, level, "geometry.vx", probe, pc, pes);
-        if (const int rc = list("geometry", L.geometry, geometryVelocity))
+        if (const int rc = list("geometry", L.geometry, geometryVelocity, geometryVelocityDivisor))
             return rc;
     }
     if (e == cudaSuccess && need("pressure.count", 4) && count == 1) {
@@ -496,7 +506,7 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
     for (int l = 0; l < nLevels && rc == VFB_OK; ++l) {
         auto* L = new Level;
         S->levels.push_back(L);
-        rc = uploadLevel(*L, grid, l, P.storage, s, keep);
+        rc = uploadLevel(*L, grid, l, P.storage, P.velocityRatio > 0.0 ? P.velocityRatio : 1.0, s, keep);
         if (rc == VFB_OK && P.geometryBC >= VFB_BC_VELOCITY_INTERPOLATED && L->geometry.n > 0 && !L->geometry.vx.ptr)
             rc = setError(VFB_ERR_CONFIGURATION, "a velocity geometry BC needs the geometry velocities (level %d)", l);
         if (rc == VFB_OK) {

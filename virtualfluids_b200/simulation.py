@@ -36,6 +36,7 @@ class VfbSimParams(ctypes.Structure):
         ("useGraphs", ctypes.c_int),
         ("useInitNeq", ctypes.c_int),
         ("outflowPressureCorrectionFactor", ctypes.c_double),
+        ("velocityRatio", ctypes.c_double),
     ]
 
 
@@ -84,11 +85,16 @@ class BoundaryConditionFactory:
 
     def set_geometry_boundary_condition(self, boundary_condition_type):
         """A no-slip kind, or a velocity kind for a geometry given a velocity
-        (setVelocityBoundaryCondition(SideType.GEOMETRY, ...))."""
-        if isinstance(boundary_condition_type, VelocityBC):
+        (setVelocityBoundaryCondition(SideType.GEOMETRY, ...)).  Plain ints are
+        looked up among the no-slip kinds first, then the velocity kinds, as
+        the reference's variant setter accepts either enum."""
+        if isinstance(boundary_condition_type, (VelocityBC, NoSlipBC)):
             self.geometry = boundary_condition_type
-        else:
+            return
+        try:
             self.geometry = NoSlipBC(boundary_condition_type)
+        except ValueError:
+            self.geometry = VelocityBC(boundary_condition_type)
 
     def set_slip_boundary_condition(self, boundary_condition_type: SlipBC):
         self.slip = SlipBC(boundary_condition_type)
@@ -112,6 +118,9 @@ class Parameter:
         # the reference leaves it unset; it matters only for
         # PressureBC.OutflowNonReflectivePressureCorrection
         self.outflow_pressure_correction_factor = 0.0
+        # world-to-lattice velocity ratio; only the geometry list's velocities
+        # are divided by it (GridGenerator.cpp:507-513)
+        self.velocity_ratio = 1.0
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -145,6 +154,14 @@ class Parameter:
         """Parameter::setOutflowPressureCorrectionFactor: the density
         correction of OutflowNonReflectivePressureCorrection."""
         self.outflow_pressure_correction_factor = float(correction_factor)
+
+    def set_velocity_ratio(self, velocity_ratio: float):
+        """Parameter::setVelocityRatio.  The grid generator divides the
+        geometry BC's velocities by it when it uploads them
+        (GridGenerator.cpp:507-513); side velocity BCs are not scaled."""
+        if not velocity_ratio > 0.0:
+            raise ValueError("velocity ratio must be positive")
+        self.velocity_ratio = float(velocity_ratio)
 
     def set_initial_condition(self, init_func):
         """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
@@ -227,6 +244,7 @@ class Simulation:
         p.useGraphs = int(bool(parameter.use_graphs))
         p.useInitNeq = int(bool(parameter.use_init_neq))
         p.outflowPressureCorrectionFactor = parameter.outflow_pressure_correction_factor
+        p.velocityRatio = parameter.velocity_ratio
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
