@@ -70,6 +70,23 @@ struct Level {
     InterfaceDevice coarseToFine, fineToCoarse;
     DeviceBuffer energyNodes; // the kinetic-energy analyzer's node set
     uint32_t nEnergy = 0;
+    // drho / vx / vy / vz in the compute precision: the initial fields on their
+    // way in and the macroscopic fields on their way out (allocated at first use
+    // and kept, so repeated transfers pay no allocation)
+    DeviceBuffer fields[4];
+    cudaError_t fieldBuffers(size_t bytes)
+    {
+        for (auto& f : fields)
+            if (!f.ptr || f.bytes != bytes) {
+                if (f.ptr) {
+                    cudaFree(f.ptr);
+                    f.ptr = nullptr;
+                }
+                if (const cudaError_t e = f.allocate(bytes))
+                    return e;
+            }
+        return cudaSuccess;
+    }
     double omega = 1.0;
     double forceFactor = 1.0;
     bool isEven = true;
@@ -630,10 +647,12 @@ extern "C" int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rh
         return setError(VFB_ERR_INVALID_ARGUMENT, "NULL field");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = L->N * (computeIsDouble(sim->params.storage) ? sizeof(double) : sizeof(float));
-    DeviceBuffer f[4];
+    if (L->fieldBuffers(bytes) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "field buffers: %s", cudaGetErrorString(cudaGetLastError()));
+    DeviceBuffer* f = L->fields;
     const void* host[4] = { rho, vx, vy, vz };
     for (int i = 0; i < 4; ++i)
-        if (uploadRaw(f[i], host[i], bytes, s) != cudaSuccess)
+        if (cudaMemcpyAsync(f[i].ptr, host[i], bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
             return setError(VFB_ERR_CUDA, "field upload failed");
     int rc = VFB_OK;
     const auto* geo = static_cast<const uint32_t*>(L->geo.ptr);
@@ -651,7 +670,7 @@ extern "C" int vfb_sim_init_level(vfb_simulation* sim, int level, const void* rh
                                       f[2].ptr, f[3].ptr, even, stream);
     }
     L->isEven = true;
-    // the temporary fields are freed on return: wait for the init kernels
+    // the caller may reuse its host arrays on return: wait for the copies and the init kernels
     if (cudaStreamSynchronize(s) != cudaSuccess && rc == VFB_OK)
         rc = setError(VFB_ERR_CUDA, "init failed: %s", cudaGetErrorString(cudaGetLastError()));
     return rc;
@@ -738,10 +757,9 @@ extern "C" int vfb_sim_macroscopic(vfb_simulation* sim, int level, void* rho, vo
         return setError(VFB_ERR_INVALID_ARGUMENT, "NULL output");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = L->N * (computeIsDouble(sim->params.storage) ? sizeof(double) : sizeof(float));
-    DeviceBuffer f[4];
-    for (int i = 0; i < 4; ++i)
-        if (f[i].allocate(bytes) != cudaSuccess)
-            return setError(VFB_ERR_CUDA, "allocation failed");
+    if (L->fieldBuffers(bytes) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "field buffers: %s", cudaGetErrorString(cudaGetLastError()));
+    DeviceBuffer* f = L->fields;
     int rc = vfb_macroscopic(sim->params.storage, L->dist.ptr, L->N, static_cast<const uint32_t*>(L->geo.ptr),
                              static_cast<const uint32_t*>(L->nX.ptr), static_cast<const uint32_t*>(L->nY.ptr),
                              static_cast<const uint32_t*>(L->nZ.ptr), L->isEven ? 1 : 0, f[0].ptr, f[1].ptr, f[2].ptr,
