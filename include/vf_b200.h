@@ -396,6 +396,44 @@ int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* s
  * number.  Computes the macroscopic fields into temporary device arrays
  * first; synchronises the stream. */
 int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream);
+/*
+ * Adjoint of the time step (no counterpart in the reference, which has no
+ * adjoint).  The differentiated step is the reference's single-level
+ * UpdateGrid27 step (UpdateGrid27.cpp:54-96): K17 collision with the global
+ * force (K17CompressibleNavierStokes.h:87-591, RunCollision.cuh:88-114), the
+ * velocity list (VelocityInterpolatedCompressible.cu:44-418), the no-slip and
+ * geometry lists (NoSlipInterpolatedCompressible.cu:44-378), the parity swap
+ * and the pressure lists (PressureNonEquilibriumCompressible.cu:45-311).
+ * Other configurations (several levels, BGK, 16-bit storage, bounce-back,
+ * slip or outflow lists) return VFB_ERR_UNSUPPORTED.
+ *
+ * vfb_sim_adjoint_forward runs `steps` time steps from the current state (the
+ * state advances, as with vfb_sim_run), keeping a copy of the state every
+ * checkpointInterval steps, and returns in *J the objective on the final state
+ *     J = sum_j wx[j] ux(k_j) + wy[j] uy(k_j) + wz[j] uz(k_j),
+ * u = (momentum) / (1 + drho) of node k_j = objectiveNodes[j] (host arrays).
+ * vfb_sim_adjoint_backward then computes, for L with dL/dJ = seed,
+ *     dVelocity[c * n + i] = dL / dU_c of entry i of the level's velocity list
+ *                            (c = 0, 1, 2 for x, y, z; n entries; host array),
+ *     dForces[c]           = dL / d(global force c)   (host array of 3),
+ * by recomputing each checkpoint segment with taped inputs and running the
+ * hand-written adjoint kernels backwards through it.  Either output may be
+ * NULL.  Both calls synchronise the stream.  Device memory: a state copy per
+ * checkpoint, and per segment 27 values per fluid node and per BC node and step.
+ */
+int vfb_sim_adjoint_forward(vfb_simulation* sim, unsigned int steps, unsigned int checkpointInterval,
+                            const uint32_t* objectiveNodes, const double* wx, const double* wy, const double* wz,
+                            uint32_t numberOfObjectiveNodes, double* J, void* stream);
+int vfb_sim_adjoint_backward(vfb_simulation* sim, double seed, double* dVelocity, double* dForces, void* stream);
+/* Parameter::setForcing (Parameter.cpp:463) on a running simulation (the next steps use
+ * the new global force); no reference counterpart as an in-run setter */
+int vfb_sim_set_forces(vfb_simulation* sim, const double* forces3);
+/* the velocity values of every entry of a level's velocity list (host arrays
+ * of the list's length), as the grid generator's getVelocityValues hands them
+ * over (GridGenerator.cpp:345-363); they take effect from the next step */
+int vfb_sim_set_velocity_bc(vfb_simulation* sim, int level, const double* vx, const double* vy, const double* vz,
+                            void* stream);
+
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,
                         int* isEvenTimestep, double* omega);
@@ -503,6 +541,16 @@ int vfb_debug_side_qs(int side, const int* alreadySet, int nSet, double* q27);
  */
 int vfb_debug_collide_node(int op, int precision, double* f27, double omega, const double* limiters,
                            const double* force, double* out4);
+/*
+ * The reverse sweep of one node's K17 collision on the host with the code the
+ * collision adjoint kernel runs: f27 = pre-collision populations, lam27 in =
+ * adjoint of the post-collision populations, out = adjoint of the
+ * pre-collision populations; gforce3 = adjoint of the half force (fx, fy, fz)
+ * that vfb_debug_collide_node takes.  precision: VFB_FP64 or VFB_FP32.
+ * No counterpart in the reference.
+ */
+int vfb_debug_k17_adjoint_node(int precision, const double* f27, double* lam27, double omega, const double* limiters,
+                               const double* force, double* gforce3);
 /*
  * One node of the non-equilibrium initialisation on the host with the code
  * the kernel runs: drhoVelocity4 = drho, vx, vy, vz; gradient9[3a + b] =

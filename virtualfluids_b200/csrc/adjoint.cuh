@@ -1,5 +1,5 @@
 // adjoint.cuh -- kernels of the adjoint (reverse-mode) time step, launched by
-// the simulation's adjoint driver (simulation.cpp, vfb_sim_adjoint_*).
+// the simulation's adjoint driver (sim_adjoint.cu, vfb_sim_adjoint_*).
 //
 // The forward step they differentiate is the single-level UpdateGrid27 step
 // (UpdateGrid27.cpp:54-96): K17 collision over the fluid list with in-place

@@ -1,0 +1,468 @@
+// sim_adjoint.cu -- the adjoint of the simulation's time step: gradients of
+// a flow objective with respect to the velocity-BC values and the global body
+// force, by a hand-written reverse pass with checkpointing.  No counterpart in
+// the reference (which has no adjoint); the step it differentiates is the
+// reference's single-level UpdateGrid27 step (UpdateGrid27.cpp:54-96): K17
+// collision with esoteric-twist streaming, the post-collision lists
+// (velocity, no-slip, geometry) and, after the parity swap, the pressure
+// lists.
+//
+// vfb_sim_adjoint_forward runs T steps with the adjoint's forward kernels
+// (adjoint.cu: the library's operator and BC arithmetic), keeps the state
+// every `interval` steps (checkpoints) and evaluates the objective
+//   J = sum_j (wx_j ux + wy_j uy + wz_j uz)(node_j)
+// on the final state.  vfb_sim_adjoint_backward seeds lam = dJ/df on the
+// final state, then walks the checkpoint segments backwards: it restores a
+// checkpoint into a work array, recomputes the segment's steps while taping
+// each step's collision inputs and BC inputs, and applies the adjoint steps
+// in reverse order (pressure, geometry, no-slip, velocity, collision).  The
+// BC adjoints accumulate dJ/dU per velocity-list entry; the collision adjoint
+// gives dJ/d(half force), which is dJ/dg times 1/2 * forceFactor.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "adjoint.cuh"
+#include "capi_common.cuh"
+#include "sim_state.hpp"
+
+namespace vfb
+{
+struct AdjointState {
+    int storage = -1;
+    unsigned steps = 0, interval = 0;
+    std::vector<DeviceBuffer*> checkpoints;
+    std::vector<char> checkpointEven;
+    DeviceBuffer finalState, work, lam;
+    bool finalEven = true;
+    bool ready = false;
+    // per segment: the collision tape and the BC records of every step
+    DeviceBuffer tape, recVelocity, recNoSlip, recGeometry, recPressure;
+    DeviceBuffer tmpVelocity, tmpNoSlip, tmpGeometry, tmpPressure;
+    std::vector<size_t> pressureOffset; // first entry of each pressure list in recPressure / tmpPressure
+    size_t pressureTotal = 0;
+    DeviceBuffer objNodes, objW[3], partials, accForce, gVelocity;
+    uint32_t nObj = 0;
+    int velocityKind = -1, noSlipKind = -1, geometryKind = -1;
+    bool pressure = false;
+    ~AdjointState()
+    {
+        for (auto* c : checkpoints)
+            delete c;
+    }
+};
+
+void destroyAdjoint(AdjointState* a) { delete a; }
+
+namespace
+{
+cudaError_t ensure(DeviceBuffer& b, size_t bytes)
+{
+    if (b.ptr && b.bytes >= bytes)
+        return cudaSuccess;
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        b.ptr = nullptr;
+    }
+    return b.allocate(bytes);
+}
+
+template <class T>
+T* as(DeviceBuffer& b)
+{
+    return static_cast<T*>(b.ptr);
+}
+
+// the supported configuration: one level, K17, FP32 or FP64, interpolated
+// velocity / no-slip lists, non-equilibrium pressure lists, no slip list
+int checkSupported(const vfb_simulation& S)
+{
+    const vfb_sim_params& P = S.params;
+    if (S.levels.size() != 1)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers single-level simulations (this one has %zu levels)",
+                        S.levels.size());
+    if (P.collisionKernel != 0)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers the K17 collision");
+    if (P.storage != VFB_FP32 && P.storage != VFB_FP64)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint needs FP32 or FP64 storage");
+    const Level& L = *S.levels[0];
+    if (L.velocity.n && P.velocityBC != VFB_BC_VELOCITY_INTERPOLATED)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers VelocityInterpolatedCompressible on the velocity list");
+    if (L.noSlip.n && P.noSlipBC >= 0 && P.noSlipBC != VFB_BC_NOSLIP_INTERPOLATED)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers NoSlipInterpolatedCompressible on the no-slip list");
+    if (L.geometry.n && P.geometryBC >= 0 && P.geometryBC != VFB_BC_NOSLIP_INTERPOLATED)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers NoSlipInterpolatedCompressible on the geometry list");
+    if (L.slip.n && P.slipBC >= 0)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint does not cover the slip list");
+    size_t np = 0;
+    for (const auto* p : L.pressure)
+        np += p->n;
+    if (np && P.pressureBC > 0)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers PressureNonEquilibriumCompressible pressure lists");
+    return VFB_OK;
+}
+
+template <class R>
+struct Stepper {
+    vfb_simulation& S;
+    Level& L;
+    AdjointState& A;
+    cudaStream_t s;
+    K17Rates<R> rates;
+    R fx, fy, fz;
+    BcLattice<R> lat;
+
+    Stepper(vfb_simulation& sim, AdjointState& a, cudaStream_t stream)
+        : S(sim), L(*sim.levels[0]), A(a), s(stream)
+    {
+        const vfb_sim_params& P = S.params;
+        // the forward collision's per-launch constants (collision.cu)
+        rates = makeK17Rates<R>((R)L.omega, (R)P.quadricLimiters[0], (R)P.quadricLimiters[1], (R)P.quadricLimiters[2]);
+        const R factor = (R)L.forceFactor;
+        fx = (R)P.forces[0] * R(0.5) * factor;
+        fy = (R)P.forces[1] * R(0.5) * factor;
+        fz = (R)P.forces[2] * R(0.5) * factor;
+        lat = BcLattice<R>{ L.N, as<const uint32_t>(L.nX), as<const uint32_t>(L.nY), as<const uint32_t>(L.nZ),
+                            (R)L.omega };
+    }
+
+    const uint32_t* nX() { return as<const uint32_t>(L.nX); }
+    const uint32_t* nY() { return as<const uint32_t>(L.nY); }
+    const uint32_t* nZ() { return as<const uint32_t>(L.nZ); }
+
+    R* slotOf(DeviceBuffer& b, int slot, size_t n) { return slot < 0 ? nullptr : as<R>(b) + (size_t)slot * 27 * n; }
+
+    // one step of the forward schedule on `dist` (parity `even` flips); with
+    // slot >= 0 the step's inputs are recorded in that slot of the tapes
+    int forward(R* dist, bool& even, int slot)
+    {
+        if (const int rc = adjoint::collision<R>(dist, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid), L.nFluid,
+                                                 rates, fx, fy, fz, even, slotOf(A.tape, slot, L.nFluid), s))
+            return rc;
+        BcLattice<R> t = lat;
+        struct Item {
+            BcListDevice* list;
+            int kind;
+            DeviceBuffer* rec;
+        } items[3] = { { &L.velocity, A.velocityKind, &A.recVelocity },
+                       { &L.noSlip, A.noSlipKind, &A.recNoSlip },
+                       { &L.geometry, A.geometryKind, &A.recGeometry } };
+        for (Item& it : items) {
+            if (it.list->n == 0 || it.kind < 0)
+                continue;
+            if (const int rc = adjoint::postBC<R>(it.kind, dist, t, as<const int32_t>(it.list->k),
+                                                  as<const R>(it.list->q), it.list->n, as<const R>(it.list->vx),
+                                                  as<const R>(it.list->vy), as<const R>(it.list->vz), even,
+                                                  slotOf(*it.rec, slot, it.list->n), s))
+                return rc;
+        }
+        even = !even;
+        if (A.pressure)
+            for (size_t p = 0; p < L.pressure.size(); ++p) {
+                PressureListDevice& P = *L.pressure[p];
+                if (P.n == 0)
+                    continue;
+                R* rec = slot < 0 ? nullptr : as<R>(A.recPressure) + (size_t)slot * 27 * A.pressureTotal +
+                                                  27 * A.pressureOffset[p];
+                if (const int rc = adjoint::pressureBC<R>(dist, t, as<const int32_t>(P.k), as<const int32_t>(P.kN),
+                                                          as<const R>(P.rho), P.n, P.direction, even, rec, s))
+                    return rc;
+            }
+        return VFB_OK;
+    }
+
+    // the adjoint of the step recorded in `slot`, whose collision ran with parity `even`
+    int reverse(bool even, int slot)
+    {
+        R* lam = as<R>(A.lam);
+        if (A.pressure)
+            for (size_t p = L.pressure.size(); p-- > 0;) {
+                PressureListDevice& P = *L.pressure[p];
+                if (P.n == 0)
+                    continue;
+                const size_t off = 27 * A.pressureOffset[p];
+                const R* rec = as<R>(A.recPressure) + (size_t)slot * 27 * A.pressureTotal + off;
+                if (const int rc = adjoint::pressureBCAdjoint<R>(lam, lat, as<const int32_t>(P.k),
+                                                                 as<const int32_t>(P.kN), as<const R>(P.rho), P.n,
+                                                                 P.direction, !even, rec, as<R>(A.tmpPressure) + off,
+                                                                 s))
+                    return rc;
+            }
+        struct Item {
+            BcListDevice* list;
+            int kind;
+            DeviceBuffer* rec;
+            DeviceBuffer* tmp;
+            double* gV;
+        } items[3] = { { &L.geometry, A.geometryKind, &A.recGeometry, &A.tmpGeometry, nullptr },
+                       { &L.noSlip, A.noSlipKind, &A.recNoSlip, &A.tmpNoSlip, nullptr },
+                       { &L.velocity, A.velocityKind, &A.recVelocity, &A.tmpVelocity, as<double>(A.gVelocity) } };
+        for (Item& it : items) {
+            if (it.list->n == 0 || it.kind < 0)
+                continue;
+            if (const int rc = adjoint::postBCAdjoint<R>(
+                    it.kind, lam, lat, as<const int32_t>(it.list->k), as<const R>(it.list->q), it.list->n,
+                    as<const R>(it.list->vx), as<const R>(it.list->vy), as<const R>(it.list->vz), even,
+                    slotOf(*it.rec, slot, it.list->n), as<R>(*it.tmp), it.gV, s))
+                return rc;
+        }
+        if (const int rc = adjoint::collisionAdjoint<R>(lam, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
+                                                        L.nFluid, rates, fx, fy, fz, even,
+                                                        slotOf(A.tape, slot, L.nFluid), as<double>(A.partials), s))
+            return rc;
+        return adjoint::reducePartials(as<double>(A.partials), adjoint::collisionBlocks(L.nFluid), 3,
+                                       as<double>(A.accForce), 0.5 * L.forceFactor, s);
+    }
+};
+
+int cudaFail(const char* what)
+{
+    return setError(VFB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(cudaGetLastError()));
+}
+
+template <class R>
+int objectiveValue(vfb_simulation& S, AdjointState& A, const R* dist, bool even, double* J, R* lam, double seed,
+                   cudaStream_t s)
+{
+    Level& L = *S.levels[0];
+    const unsigned blocks = adjoint::objectiveBlocks(A.nObj);
+    if (cudaMemsetAsync(A.accForce.ptr, 0, 4 * sizeof(double), s) != cudaSuccess)
+        return cudaFail("objective accumulator");
+    if (const int rc = adjoint::objective<R>(dist, L.N, as<const uint32_t>(L.nX), as<const uint32_t>(L.nY),
+                                             as<const uint32_t>(L.nZ), as<const uint32_t>(A.objNodes),
+                                             as<const double>(A.objW[0]), as<const double>(A.objW[1]),
+                                             as<const double>(A.objW[2]), A.nObj, even, as<double>(A.partials), lam,
+                                             seed, s))
+        return rc;
+    if (const int rc = adjoint::reducePartials(as<double>(A.partials), blocks, 1, as<double>(A.accForce) + 3, 1.0, s))
+        return rc;
+    if (J) {
+        if (cudaMemcpyAsync(J, as<double>(A.accForce) + 3, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return cudaFail("objective copy");
+    }
+    return VFB_OK;
+}
+
+template <class R>
+int adjointForward(vfb_simulation& S, AdjointState& A, unsigned steps, double* J, cudaStream_t s)
+{
+    Level& L = *S.levels[0];
+    const size_t stateBytes = 27ull * L.N * sizeof(R);
+    const unsigned segments = (steps + A.interval - 1) / A.interval;
+    while (A.checkpoints.size() < segments)
+        A.checkpoints.push_back(new DeviceBuffer);
+    A.checkpointEven.assign(segments, 1);
+    for (unsigned c = 0; c < segments; ++c)
+        if (ensure(*A.checkpoints[c], stateBytes) != cudaSuccess)
+            return cudaFail("checkpoint allocation");
+    Stepper<R> st(S, A, s);
+    R* dist = as<R>(L.dist);
+    bool even = L.isEven;
+    for (unsigned t = 0; t < steps; ++t) {
+        if (t % A.interval == 0) {
+            const unsigned c = t / A.interval;
+            if (cudaMemcpyAsync(A.checkpoints[c]->ptr, dist, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                return cudaFail("checkpoint copy");
+            A.checkpointEven[c] = even ? 1 : 0;
+        }
+        if (const int rc = st.forward(dist, even, -1))
+            return rc;
+    }
+    L.isEven = even;
+    S.stepsRun += steps;
+    if (ensure(A.finalState, stateBytes) != cudaSuccess ||
+        cudaMemcpyAsync(A.finalState.ptr, dist, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return cudaFail("final state copy");
+    A.finalEven = even;
+    return objectiveValue<R>(S, A, dist, even, J, nullptr, 0.0, s);
+}
+
+template <class R>
+int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVelocity, double* dForces,
+                    cudaStream_t s)
+{
+    Level& L = *S.levels[0];
+    const size_t stateBytes = 27ull * L.N * sizeof(R);
+    const unsigned I = A.interval;
+    auto perStep = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, (size_t)I * 27 * n * sizeof(R))); };
+    auto once = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, 27 * n * sizeof(R))); };
+    if (ensure(A.work, stateBytes) || ensure(A.lam, stateBytes) || perStep(A.tape, L.nFluid) ||
+        perStep(A.recVelocity, L.velocity.n) || perStep(A.recNoSlip, L.noSlip.n) ||
+        perStep(A.recGeometry, L.geometry.n) || perStep(A.recPressure, A.pressureTotal) ||
+        once(A.tmpVelocity, L.velocity.n) || once(A.tmpNoSlip, L.noSlip.n) || once(A.tmpGeometry, L.geometry.n) ||
+        once(A.tmpPressure, A.pressureTotal) ||
+        ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))))
+        return cudaFail("adjoint buffers");
+    if (cudaMemsetAsync(A.lam.ptr, 0, stateBytes, s) != cudaSuccess ||
+        cudaMemsetAsync(A.gVelocity.ptr, 0, A.gVelocity.bytes, s) != cudaSuccess)
+        return cudaFail("adjoint clear");
+    // seed: lam = seed * dJ/df on the final state
+    if (const int rc = objectiveValue<R>(S, A, as<const R>(A.finalState), A.finalEven, nullptr, as<R>(A.lam), seed, s))
+        return rc;
+    if (cudaMemsetAsync(A.accForce.ptr, 0, 3 * sizeof(double), s) != cudaSuccess)
+        return cudaFail("force accumulator");
+    Stepper<R> st(S, A, s);
+    const unsigned segments = (A.steps + I - 1) / I;
+    std::vector<char> evenAt(I);
+    for (unsigned c = segments; c-- > 0;) {
+        const unsigned t0 = c * I;
+        const unsigned len = std::min(I, A.steps - t0);
+        if (cudaMemcpyAsync(A.work.ptr, A.checkpoints[c]->ptr, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return cudaFail("checkpoint restore");
+        bool even = A.checkpointEven[c] != 0;
+        for (unsigned j = 0; j < len; ++j) {
+            evenAt[j] = even ? 1 : 0;
+            if (const int rc = st.forward(as<R>(A.work), even, (int)j))
+                return rc;
+        }
+        for (unsigned j = len; j-- > 0;)
+            if (const int rc = st.reverse(evenAt[j] != 0, (int)j))
+                return rc;
+    }
+    if (dVelocity && L.velocity.n &&
+        cudaMemcpyAsync(dVelocity, A.gVelocity.ptr, 3ull * L.velocity.n * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess)
+        return cudaFail("velocity gradient copy");
+    double g[3] = { 0, 0, 0 };
+    if (cudaMemcpyAsync(g, A.accForce.ptr, sizeof(g), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return cudaFail("backward pass");
+    if (dForces)
+        for (int c = 0; c < 3; ++c)
+            dForces[c] = g[c];
+    return VFB_OK;
+}
+} // namespace
+} // namespace vfb
+
+using namespace vfb;
+
+extern "C" int vfb_sim_set_forces(vfb_simulation* sim, const double* forces)
+{
+    clearError();
+    if (!sim || !forces)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int c = 0; c < 3; ++c)
+        sim->params.forces[c] = forces[c];
+    // captured graphs hold the old force in their kernel arguments
+    for (auto& g : sim->graphs)
+        cudaGraphExecDestroy(g.second);
+    sim->graphs.clear();
+    if (sim->adjoint)
+        sim->adjoint->ready = false;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_set_velocity_bc(vfb_simulation* sim, int level, const double* vx, const double* vy,
+                                       const double* vz, void* stream)
+{
+    clearError();
+    if (!sim || level < 0 || level >= (int)sim->levels.size())
+        return setError(VFB_ERR_INVALID_ARGUMENT, "no level %d", level);
+    if (!vx || !vy || !vz)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL velocity array");
+    BcListDevice& B = sim->levels[level]->velocity;
+    if (B.n == 0)
+        return VFB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool dbl = sim->params.storage == VFB_FP64;
+    const double* src[3] = { vx, vy, vz };
+    DeviceBuffer* dst[3] = { &B.vx, &B.vy, &B.vz };
+    std::vector<float> f(B.n);
+    for (int c = 0; c < 3; ++c) {
+        if (!dst[c]->ptr)
+            return setError(VFB_ERR_CONFIGURATION, "the velocity list has no velocity arrays");
+        cudaError_t e;
+        if (dbl) {
+            e = cudaMemcpyAsync(dst[c]->ptr, src[c], B.n * sizeof(double), cudaMemcpyHostToDevice, s);
+        } else {
+            for (uint32_t i = 0; i < B.n; ++i)
+                f[i] = (float)src[c][i];
+            e = cudaMemcpyAsync(dst[c]->ptr, f.data(), B.n * sizeof(float), cudaMemcpyHostToDevice, s);
+        }
+        if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+            return cudaFail("velocity upload");
+    }
+    if (sim->adjoint)
+        sim->adjoint->ready = false;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_adjoint_forward(vfb_simulation* sim, unsigned int steps, unsigned int checkpointInterval,
+                                       const uint32_t* objectiveNodes, const double* wx, const double* wy,
+                                       const double* wz, uint32_t numberOfObjectiveNodes, double* J, void* stream)
+{
+    clearError();
+    if (!sim || !J)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (checkpointInterval == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "checkpoint interval must be positive");
+    if (numberOfObjectiveNodes && (!objectiveNodes || !wx || !wy || !wz))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL objective array");
+    if (const int rc = checkSupported(*sim))
+        return rc;
+    Level& L = *sim->levels[0];
+    for (uint32_t j = 0; j < numberOfObjectiveNodes; ++j)
+        if (objectiveNodes[j] == 0 || objectiveNodes[j] >= L.N)
+            return setError(VFB_ERR_OUT_OF_RANGE, "objective node %u outside 1..%llu", objectiveNodes[j], L.N - 1);
+    if (!sim->adjoint)
+        sim->adjoint = new AdjointState;
+    AdjointState& A = *sim->adjoint;
+    A.storage = sim->params.storage;
+    A.steps = steps;
+    A.interval = checkpointInterval;
+    A.ready = false;
+    const vfb_sim_params& P = sim->params;
+    A.velocityKind = L.velocity.n ? VFB_BC_VELOCITY_INTERPOLATED : -1;
+    A.noSlipKind = L.noSlip.n && P.noSlipBC >= 0 ? VFB_BC_NOSLIP_INTERPOLATED : -1;
+    A.geometryKind = L.geometry.n && P.geometryBC >= 0 ? VFB_BC_NOSLIP_INTERPOLATED : -1;
+    A.pressure = P.pressureBC == 0;
+    A.pressureOffset.clear();
+    A.pressureTotal = 0;
+    for (const auto* p : L.pressure) {
+        A.pressureOffset.push_back(A.pressureTotal);
+        A.pressureTotal += p->n;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    A.nObj = numberOfObjectiveNodes;
+    const size_t n = std::max<uint32_t>(1, numberOfObjectiveNodes);
+    const unsigned partials = std::max(adjoint::collisionBlocks(L.nFluid), adjoint::objectiveBlocks(A.nObj));
+    if (ensure(A.objNodes, n * sizeof(uint32_t)) || ensure(A.objW[0], n * sizeof(double)) ||
+        ensure(A.objW[1], n * sizeof(double)) || ensure(A.objW[2], n * sizeof(double)) ||
+        ensure(A.partials, 3ull * std::max(1u, partials) * sizeof(double)) || ensure(A.accForce, 4 * sizeof(double)))
+        return cudaFail("objective buffers");
+    if (numberOfObjectiveNodes) {
+        const double* w[3] = { wx, wy, wz };
+        if (cudaMemcpyAsync(A.objNodes.ptr, objectiveNodes, numberOfObjectiveNodes * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return cudaFail("objective upload");
+        for (int c = 0; c < 3; ++c)
+            if (cudaMemcpyAsync(A.objW[c].ptr, w[c], numberOfObjectiveNodes * sizeof(double), cudaMemcpyHostToDevice,
+                                s) != cudaSuccess)
+                return cudaFail("objective upload");
+    }
+    const int rc = sim->params.storage == VFB_FP64 ? adjointForward<double>(*sim, A, steps, J, s)
+                                                   : adjointForward<float>(*sim, A, steps, J, s);
+    if (rc == VFB_OK && numberOfObjectiveNodes == 0)
+        *J = 0.0;
+    A.ready = rc == VFB_OK;
+    return rc;
+}
+
+extern "C" int vfb_sim_adjoint_backward(vfb_simulation* sim, double seed, double* dVelocity, double* dForces,
+                                        void* stream)
+{
+    clearError();
+    if (!sim)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "sim is NULL");
+    if (!sim->adjoint || !sim->adjoint->ready)
+        return setError(VFB_ERR_CONFIGURATION, "no adjoint forward pass to differentiate (run vfb_sim_adjoint_forward "
+                                               "after the last change of forces or BC velocities)");
+    AdjointState& A = *sim->adjoint;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return A.storage == VFB_FP64 ? adjointBackward<double>(*sim, A, seed, dVelocity, dForces, s)
+                                 : adjointBackward<float>(*sim, A, seed, dVelocity, dForces, s);
+}

@@ -1,0 +1,117 @@
+// sim_state.hpp -- the device-side state of a simulation (per-level arrays,
+// BC lists, interface cells) shared by the schedule (simulation.cpp) and the
+// adjoint driver (sim_adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "../../include/vf_b200.h"
+
+namespace vfb
+{
+struct AdjointState;
+void destroyAdjoint(AdjointState* a);
+
+// a device array owned by the simulation
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t allocate(size_t n)
+    {
+        bytes = n;
+        return cudaMalloc(&ptr, n ? n : 1);
+    }
+    ~DeviceBuffer()
+    {
+        if (ptr)
+            cudaFree(ptr);
+    }
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+};
+
+struct BcListDevice {
+    DeviceBuffer k, q, vx, vy, vz;
+    uint32_t n = 0;
+};
+
+// interface cells between this level and the next finer one (InterpolationCells
+// + ICellNeigh, Calculation.h:72-89)
+struct InterfaceDevice {
+    DeviceBuffer coarse, fine, offX, offY, offZ, mask;
+    uint32_t n = 0;
+};
+
+struct PressureListDevice {
+    DeviceBuffer k, kN, rho;
+    uint32_t n = 0;
+    int direction = 0;
+};
+
+struct Level {
+    unsigned long long N = 0;
+    uint32_t nFluid = 0;
+    DeviceBuffer dist, nX, nY, nZ, geo, fluid;
+    DeviceBuffer nNeg; // the -x-y-z neighbour (non-equilibrium init, enstrophy)
+    BcListDevice velocity, noSlip, slip, geometry;
+    std::vector<PressureListDevice*> pressure;
+    InterfaceDevice coarseToFine, fineToCoarse;
+    DeviceBuffer energyNodes; // the kinetic-energy analyzer's node set
+    uint32_t nEnergy = 0;
+    // drho / vx / vy / vz in the compute precision: the initial fields on their
+    // way in and the macroscopic fields on their way out (allocated at first use
+    // and kept, so repeated transfers pay no allocation)
+    DeviceBuffer fields[4];
+    cudaError_t fieldBuffers(size_t bytes)
+    {
+        for (auto& f : fields)
+            if (!f.ptr || f.bytes != bytes) {
+                if (f.ptr) {
+                    cudaFree(f.ptr);
+                    f.ptr = nullptr;
+                }
+                if (const cudaError_t e = f.allocate(bytes))
+                    return e;
+            }
+        return cudaSuccess;
+    }
+    double omega = 1.0;
+    double forceFactor = 1.0;
+    bool isEven = true;
+    vfb_collision_plan* plan = nullptr;
+    ~Level()
+    {
+        for (auto* p : pressure)
+            delete p;
+        if (plan)
+            vfb_collision_plan_destroy(plan);
+    }
+};
+
+} // namespace vfb
+
+struct vfb_simulation {
+    vfb_sim_params params;
+    std::vector<vfb::Level*> levels;
+    // captured two-coarse-step graphs, keyed by the parity pattern they start from
+    cudaStream_t captureStream = nullptr;
+    std::map<unsigned long long, cudaGraphExec_t> graphs;
+    unsigned long long stepsRun = 0;
+    // the adjoint's checkpoints, tapes and gradients (vfb_sim_adjoint_*)
+    vfb::AdjointState* adjoint = nullptr;
+    ~vfb_simulation()
+    {
+        vfb::destroyAdjoint(adjoint);
+        for (auto& g : graphs)
+            cudaGraphExecDestroy(g.second);
+        if (captureStream)
+            cudaStreamDestroy(captureStream);
+        for (auto* l : levels)
+            delete l;
+    }
+};

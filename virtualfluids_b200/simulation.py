@@ -314,6 +314,44 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_enstrophy(self._h, level, out, self.stream))
         return out[0], int(out[1])
 
+    def set_forces(self, fx: float, fy: float, fz: float):
+        """The global force of the following steps (Parameter::setForcing)."""
+        g = (ctypes.c_double * 3)(float(fx), float(fy), float(fz))
+        _lib.check(_lib.lib().vfb_sim_set_forces(self._h, g))
+
+    def set_velocity_bc(self, vx, vy, vz, level: int = 0):
+        """The velocities of every entry of a level's velocity list (in the
+        list's order, levels[level]["velocity.k"]), from the next step on."""
+        n = len(self.levels[level]["velocity.k"])
+        a = [np.ascontiguousarray(np.broadcast_to(np.asarray(v, np.float64), (n,))) for v in (vx, vy, vz)]
+        _lib.check(_lib.lib().vfb_sim_set_velocity_bc(self._h, level, *[x.ctypes.data for x in a], self.stream))
+        for c, x in zip(("vx", "vy", "vz"), a):
+            self.levels[level][f"velocity.{c}"] = x.copy()
+
+    def adjoint_forward(self, steps: int, checkpoint_interval: int, nodes, wx, wy=None, wz=None) -> float:
+        """Run `steps` steps (the state advances) keeping a checkpoint every
+        `checkpoint_interval` steps, and return the objective
+        J = sum_j wx[j] ux + wy[j] uy + wz[j] uz at the nodes `nodes` of the
+        final state (single-level simulations; see vfb_sim_adjoint_forward)."""
+        nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+        n = len(nodes)
+        w = [np.ascontiguousarray(np.broadcast_to(np.asarray(0.0 if v is None else v, np.float64), (n,)))
+             for v in (wx, wy, wz)]
+        J = ctypes.c_double()
+        _lib.check(_lib.lib().vfb_sim_adjoint_forward(self._h, int(steps), int(checkpoint_interval), nodes.ctypes.data,
+                                                      *[x.ctypes.data for x in w], n, ctypes.byref(J), self.stream))
+        return J.value
+
+    def adjoint_backward(self, seed: float = 1.0):
+        """Gradients of seed * J from the last adjoint_forward: (dJ/dU of the
+        velocity list as an array of shape (3, n), dJ/d(global force) of shape (3,))."""
+        n = len(self.levels[0]["velocity.k"])
+        dv = np.zeros((3, n), np.float64)
+        df = np.zeros(3, np.float64)
+        _lib.check(_lib.lib().vfb_sim_adjoint_backward(self._h, float(seed), dv.ctypes.data, df.ctypes.data,
+                                                       self.stream))
+        return dv, df
+
     def level_state(self, level: int = 0):
         """(device pointer of the populations, N, isEvenTimestep, omega)."""
         ptr = ctypes.c_void_p()
