@@ -31,7 +31,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "D3Q27 cumulant MLUPS & % HBM roofline; FP16-store vs FP32 at stated L2 err"
-STORAGE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}
+STORAGE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2, "fx16": 2}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -237,7 +237,8 @@ def run_gpu(args, world, rank, local):
     from virtualfluids_b200 import kernels as K
     from virtualfluids_b200.workloads import taylor_green
 
-    dtype = {"fp32": torch.float32, "fp64": torch.float64, "fp16": torch.float16, "bf16": torch.bfloat16}[
+    dtype = {"fp32": torch.float32, "fp64": torch.float64, "fp16": torch.float16, "bf16": torch.bfloat16,
+             "fx16": torch.int16}[
         args.storage]
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
@@ -374,7 +375,8 @@ def run_gpu(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f16-store/f32", "bf16": "bf16-store/f32"}[
+        "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f16-store/f32", "bf16": "bf16-store/f32",
+                                         "fx16": "fx16-store/f32"}[
             args.storage],
         "data": "synthetic",
         "config": {"workload": f"taylor-green {args.n}^3 periodic, K17 cumulant, {args.storage} storage",
@@ -392,8 +394,81 @@ def run_gpu(args, world, rank, local):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, args.u0, omega)
+    if world == 1 and args.precision_steps > 0 and args.storage == "fp32":
+        line["precision_form"] = precision_form_record(args, value, device)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def precision_form_record(args, fp32_value, device):
+    """The precision form beside the FP32 bench value: the FX16 storage's
+    throughput on the same K planned steps of the same workload, its ratio to
+    the FP32 value of this run, and its L2 velocity error against FP64 storage
+    after --precision-steps steps (both run through the Simulation API from
+    the same initial field; the FP64 path matches the FP64 oracle to 1e-12 in
+    the GPU tests)."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200 import kernels as K
+    from virtualfluids_b200.grid import MultipleGridBuilder
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, Simulation
+    from virtualfluids_b200.workloads import taylor_green
+
+    w = taylor_green(args.n)
+    g = w.grid
+    lat = K.DeviceLattice.from_arrays(g, device)
+    dist = K.new_distributions(lat, torch.int16, device)
+    fields = [torch.from_numpy(a).to(device, torch.float32) for a in (w.rho, w.vx, w.vy, w.vz)]
+    for ev in (False, True):
+        K.init_equilibrium(dist, lat, *fields, ev)
+    del fields
+    stream = torch.cuda.current_stream(device)
+    plan = K.CollisionPlan(torch.int16, lat, stream=stream)
+    even = True
+    for _ in range(args.warmup):
+        K.collision("K17", dist, lat, w.omega, even, stream=stream, plan=plan)
+        even = not even
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        K.collision("K17", dist, lat, w.omega, even, stream=stream, plan=plan)
+        even = not even
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    plan.check(stream)
+    plan.close()
+    ms = e0.elapsed_time(e1)
+    value = lat.numberOfFluidNodes * args.steps / (ms * 1e-3) / 1e6
+    bpn = algorithmic_bytes_per_node("fx16")
+    del dist, plan, lat
+    torch.cuda.empty_cache()
+
+    fl = g["fluid"]
+    b = MultipleGridBuilder()
+    d = 2.0 * math.pi / args.n
+    b.addCoarseGrid(-math.pi, -math.pi, -math.pi, math.pi, math.pi, math.pi, d)
+    b.setPeriodicBoundaryCondition(True, True, True)
+    b.buildGrids(True)
+    nu = args.u0 * (args.n / (2 * math.pi)) / 1600.0
+    u = {}
+    for storage in ("fp64", "fx16"):
+        p = Parameter()
+        p.set_storage(storage)
+        p.set_viscosity_LB(nu)
+        sim = Simulation(p, b, BoundaryConditionFactory())
+        sim.init_level(0, w.rho, w.vx, w.vy, w.vz)
+        sim.run(args.precision_steps)
+        _, vx, vy, vz = sim.macroscopic(0)
+        u[storage] = [a[fl].astype(np.float64) for a in (vx, vy, vz)]
+        sim.close()
+    num = math.sqrt(sum(float(np.sum((a - r) ** 2)) for a, r in zip(u["fx16"], u["fp64"])))
+    den = math.sqrt(sum(float(np.sum(r ** 2)) for r in u["fp64"]))
+    return {"storage": "fx16", "value": value, "unit": "MLUPS", "ratio_vs_fp32": value / fp32_value,
+            "bytes_per_node": bpn, "ms_per_step": ms / args.steps,
+            "l2_velocity_err_vs_fp64": num / den, "l2_steps": args.precision_steps,
+            "format": "int16 q, f_d - w_d = q w_d 2^-17 (FP32 arithmetic)"}
 
 
 def precision_report(args):
@@ -418,7 +493,7 @@ def precision_report(args):
     b.setPeriodicBoundaryCondition(True, True, True)
     b.buildGrids(True)
     rows, ref = {}, None
-    for storage in ("fp64", "fp32", "fp16", "bf16"):
+    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16"):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(nu)
@@ -450,6 +525,7 @@ def precision_report(args):
         rows[storage] = row
     rows["fp16_over_fp32_mlups"] = rows["fp16"]["mlups"] / rows["fp32"]["mlups"]
     rows["bf16_over_fp32_mlups"] = rows["bf16"]["mlups"] / rows["fp32"]["mlups"]
+    rows["fx16_over_fp32_mlups"] = rows["fx16"]["mlups"] / rows["fp32"]["mlups"]
     print(json.dumps({"report": "precision form", "workload": f"taylor-green {args.n}^3 periodic, K17",
                       "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
@@ -710,6 +786,75 @@ def kernel_report(args):
     return 0
 
 
+def adjoint_report(args):
+    """The adjoint form: the channel of 128 x 64 x 64 nodes (12^3 cube at x =
+    40, parabolic inlet profile with +-2% noise, pressure outlet, no-slip
+    walls, g = (1e-6, 0, 0), nu = 0.02), K17, T = --steps (default 1000) time
+    steps with a checkpoint every 32, objective J = mean u_x over the 16^3 box
+    x in [80, 96).  Per storage (FP32, FP64): the plain forward step through
+    the Simulation API (graph replay), the adjoint's forward pass (with
+    checkpoints) and its backward pass (recompute with tapes, then the adjoint
+    kernels), all event-timed per step, and the backward / forward ratio.
+    One JSON line."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200.adjoint import FlowProblem
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, NoSlipBC, Parameter, PressureBC, Simulation
+    from virtualfluids_b200.workloads import adjoint_channel, inlet_entries, inlet_profile, initial_fields, objective_box
+
+    steps = args.steps if args.steps != 50 else 1000
+    rows = {}
+    for storage in ("fp32", "fp64"):
+        p = Parameter()
+        p.set_storage(storage)
+        p.set_viscosity_LB(0.02)
+        p.set_forcing(1e-6, 0.0, 0.0)
+        bc = BoundaryConditionFactory()
+        bc.set_geometry_boundary_condition(NoSlipBC.NoSlipInterpolatedCompressible)
+        bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
+        sim = Simulation(p, adjoint_channel(), bc)
+        g = sim.levels[0]
+        nodes, w = objective_box(g, 80, 96, 24, 40, 24, 40)
+        pb = FlowProblem(sim, inlet_entries(g), initial_fields(g), steps, 32, nodes, (w, None, None))
+        prof = inlet_profile(g)
+        pb.evaluate(prof, (1e-6, 0.0, 0.0))  # warm-up: allocations, first launches
+        pb.gradient(1.0)
+        stream = torch.cuda.current_stream()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        sim.init_level(0, *initial_fields(g))
+        sim.run(4)
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        sim.run(steps)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        sim.init_level(0, *initial_fields(g))
+        torch.cuda.synchronize()
+        ev[2].record(stream)
+        J = sim.adjoint_forward(steps, 32, nodes, w)
+        ev[3].record(stream)
+        ev[4].record(stream)
+        dv, df = sim.adjoint_backward(1.0)
+        ev[5].record(stream)
+        torch.cuda.synchronize()
+        fwd = ev[0].elapsed_time(ev[1]) / steps
+        afwd = ev[2].elapsed_time(ev[3]) / steps
+        bwd = ev[4].elapsed_time(ev[5]) / steps
+        rows[storage] = {"forward_ms_per_step": fwd, "adjoint_forward_ms_per_step": afwd,
+                         "adjoint_backward_ms_per_step": bwd, "backward_over_forward": bwd / fwd,
+                         "gradient_over_forward": (afwd + bwd) / fwd, "J": J,
+                         "dJ_dg": [float(x) for x in df],
+                         "dJ_dinlet_norm": float(np.linalg.norm(dv[0][inlet_entries(g)])),
+                         "fluid_nodes": len(g["fluid"])}
+        sim.close()
+    print(json.dumps({"report": "adjoint form", "workload": "channel 128x64x64, 12^3 cube at x=40, parabolic inlet "
+                      "(peak 0.04, +-2% noise), pressure outlet, no-slip walls, g=(1e-6,0,0), nu=0.02, K17",
+                      "steps": steps, "checkpoint_interval": 32, "objective": "mean u_x over x in [80,96), 16^3 box",
+                      "results": rows}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -721,6 +866,8 @@ def main(argv=None):
     ap.add_argument("--path", default="planned", choices=["planned", "generic"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-steps", type=int, default=2000,
+                    help="steps of the FX16-vs-FP64 error in the bench line's precision_form record (0: skip it)")
     ap.add_argument("--kernel-report", action="store_true",
                     help="bandwidth of the BGK, BC and interface kernels (not a bench line)")
     ap.add_argument("--cavity-report", action="store_true",
@@ -729,6 +876,8 @@ def main(argv=None):
                     help="wall-mounted cube on two levels: NUPS per storage and errors against FP64 (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",
                     help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
+    ap.add_argument("--adjoint-report", action="store_true",
+                    help="adjoint channel 128x64x64: forward, adjoint forward and backward step times (not a bench line)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -740,6 +889,8 @@ def main(argv=None):
         return cube_report(args)
     if args.kernel_report:
         return kernel_report(args)
+    if args.adjoint_report:
+        return adjoint_report(args)
     world, rank, local = init_distributed()
     try:
         if args.impl == "reference":

@@ -16,8 +16,11 @@
  *   fluid node list uint32 sparse indices (GridImp.cpp:965-986).
  *
  * The storage argument selects the element type of the distributions:
- * VFB_FP32 (float), VFB_FP64 (double), VFB_FP16 and VFB_BF16 (the precision
- * form: 16-bit storage, FP32 arithmetic).  Arrays documented as "compute
+ * VFB_FP32 (float), VFB_FP64 (double), and the precision form (16-bit storage,
+ * FP32 arithmetic): VFB_FP16 (IEEE half of the deviation times 2^12),
+ * VFB_BF16 (bfloat16) and VFB_FX16 (int16 q with f_d - w_d = q * w_d * 2^-17:
+ * deviations below a quarter of the weight at a uniform step, saturating
+ * beyond; no counterpart in the reference).  Arrays documented as "compute
  * precision" are double for VFB_FP64 and float otherwise.
  */
 #ifndef VF_B200_H
@@ -44,6 +47,7 @@ extern "C" {
 #define VFB_FP64 1
 #define VFB_FP16 2
 #define VFB_BF16 3
+#define VFB_FX16 4
 
 /* CollisionTemplate (src/gpu/core/Calculation/Calculation.h:55-68) */
 #define VFB_TEMPLATE_DEFAULT 0

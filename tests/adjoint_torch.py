@@ -344,19 +344,21 @@ class Step:
             active = (q[d] >= 0) & (q[d] <= 1)
             if not bool(active.any()):
                 continue
+            # the formula on the active entries only (inactive q = -1 would
+            # divide by zero, and a zero gradient times inf is NaN)
+            sel = torch.nonzero(active).flatten()
             e = INV[d]
             w = weight(d)
-            qd = q[d]
-            feq = w * (drho + 4.5 * cdot(d, vx1, vx2, vx3) ** 2 * (1.0 + drho) - cu_sq)
-            base = (1.0 - qd) / (1.0 + qd) * (gd[d] - gd[e] + (gd[d] + gd[e] - 2.0 * feq * self.omega) /
-                                              (1.0 - self.omega)) * 0.5
+            qd = q[d][sel]
+            fd, fe, dr = gd[d][sel], gd[e][sel], drho[sel]
+            feq = w * (dr + 4.5 * cdot(d, vx1[sel], vx2[sel], vx3[sel]) ** 2 * (1.0 + dr) - cu_sq[sel])
+            base = (1.0 - qd) / (1.0 + qd) * (fd - fe + (fd + fe - 2.0 * feq * self.omega) / (1.0 - self.omega)) * 0.5
             if kind == 2:
-                v = base + (qd * (gd[d] + gd[e]) - 6.0 * w * cdot(d, U[0], U[1], U[2])) / (1.0 + qd)
+                v = base + (qd * (fd + fe) - 6.0 * w * cdot(d, U[0][sel], U[1][sel], U[2][sel])) / (1.0 + qd)
             else:
-                v = base + (qd * (gd[d] + gd[e])) / (1.0 + qd)
-            sel = torch.nonzero(active).flatten()
+                v = base + (qd * (fd + fe)) / (1.0 + qd)
             targets.append(self.cells(L, e, not even)[sel])
-            values.append(v[sel])
+            values.append(v)
         return D.index_put((torch.cat(targets),), torch.cat(values))
 
     def pressure_bc(self, D, even):

@@ -10,7 +10,7 @@ torch = pytest.importorskip("torch")
 
 from oracle.pyoracle import Oracle  # noqa: E402
 from tests import adjoint_torch as AT  # noqa: E402
-from tests.adjoint_cases import inlet_entries, inlet_profile, initial_fields, small_channel  # noqa: E402
+from virtualfluids_b200.workloads import adjoint_channel_small, inlet_entries, inlet_profile, initial_fields  # noqa: E402,E501
 from tests.test_adjoint_host import state  # noqa: E402
 
 
@@ -29,7 +29,7 @@ def test_torch_k17_equals_oracle(seed):
 
 
 def test_torch_step_equals_oracle_schedule():
-    g = small_channel().arrays()[0]
+    g = adjoint_channel_small().arrays()[0]
     vx = g["velocity.vx"].copy()
     vx[inlet_entries(g)] = inlet_profile(g)
     g["velocity.vx"] = vx

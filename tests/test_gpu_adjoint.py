@@ -16,8 +16,8 @@ kernels) behind virtualfluids_b200.adjoint.FlowObjective.
 import numpy as np
 import pytest
 
-from tests.adjoint_cases import (full_channel, inlet_entries, inlet_profile, initial_fields, objective_box,
-                                 small_channel)
+from virtualfluids_b200.workloads import (adjoint_channel, adjoint_channel_small, inlet_entries, inlet_profile,
+                                         initial_fields, objective_box)
 from virtualfluids_b200 import _lib
 from virtualfluids_b200.simulation import BoundaryConditionFactory, NoSlipBC, Parameter, PressureBC, Simulation
 
@@ -75,11 +75,11 @@ def torch_reference(g, steps, profile, force):
     # the gradient of every velocity-list value: x component with the inlet entries from p
     gx = U[0].grad.clone()
     gx[torch.from_numpy(entries)] = p.grad
-    return float(J), np.stack([gx.numpy(), U[1].grad.numpy(), U[2].grad.numpy()]), gforce.grad.numpy()
+    return float(J.detach()), np.stack([gx.numpy(), U[1].grad.numpy(), U[2].grad.numpy()]), gforce.grad.numpy()
 
 
 def test_small_channel_fp64_matches_torch_autograd(cuda):
-    sim = make_sim(small_channel())
+    sim = make_sim(adjoint_channel_small())
     g = sim.levels[0]
     profile = inlet_profile(g)
     pb = problem(sim, 24, 5, SMALL_BOX)
@@ -102,7 +102,7 @@ def test_flow_objective_autograd_function(cuda):
     profile and the force; the gradient equals the direct adjoint call, also
     after another evaluation ran in between."""
     from virtualfluids_b200.adjoint import FlowObjective
-    sim = make_sim(small_channel())
+    sim = make_sim(adjoint_channel_small())
     g = sim.levels[0]
     pb = problem(sim, 12, 4, SMALL_BOX)
     prof = torch.tensor(inlet_profile(g), dtype=torch.float64, requires_grad=True)
@@ -121,7 +121,7 @@ def test_flow_objective_autograd_function(cuda):
 def test_small_channel_fp32_adjoint_close_to_fp64(cuda):
     out = []
     for storage in ("fp64", "fp32"):
-        sim = make_sim(small_channel(), storage)
+        sim = make_sim(adjoint_channel_small(), storage)
         pb = problem(sim, 24, 5, SMALL_BOX)
         pb.evaluate(inlet_profile(sim.levels[0]), G)
         out.append(pb.gradient(1.0))
@@ -135,12 +135,12 @@ def test_adjoint_errors(cuda):
     p = Parameter()
     p.set_viscosity_LB(NU)
     p.configure_main_kernel("BGKCompSP27")
-    sim = Simulation(p, small_channel(), BoundaryConditionFactory())
+    sim = Simulation(p, adjoint_channel_small(), BoundaryConditionFactory())
     with pytest.raises(_lib.VfbError) as e:
         sim.adjoint_forward(4, 2, [1], [1.0])
     assert e.value.code == _lib.VFB_ERR_UNSUPPORTED
     sim.close()
-    sim = make_sim(small_channel())
+    sim = make_sim(adjoint_channel_small())
     with pytest.raises(_lib.VfbError) as e:
         sim.adjoint_backward()
     assert e.value.code == _lib.VFB_ERR_CONFIGURATION
@@ -156,7 +156,7 @@ def test_adjoint_errors(cuda):
 def full_problem():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    sim = make_sim(full_channel())
+    sim = make_sim(adjoint_channel())
     g = sim.levels[0]
     pb = problem(sim, 1000, 32, (80, 96, 24, 40, 24, 40))
     yield sim, g, pb

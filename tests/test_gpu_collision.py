@@ -43,7 +43,7 @@ def test_fp32_matches_oracle(cuda, kernel):
     assert rel_max(got[0][fluid], ref[0][fluid]) < 1e-4
 
 
-@pytest.mark.parametrize("dtype,tol", [("float16", 5e-3), ("bfloat16", 3e-2)])
+@pytest.mark.parametrize("dtype,tol", [("float16", 5e-3), ("bfloat16", 3e-2), ("int16", 1e-3)])
 def test_low_precision_storage_against_fp64(cuda, dtype, tol):
     w = tgv_state(16)
     steps = 40

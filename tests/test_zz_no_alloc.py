@@ -36,7 +36,7 @@ def _close(a, b):
 
 
 @pytest.mark.parametrize("n", [8, 64])
-@pytest.mark.parametrize("dtype", ["float32", "float64", "float16", "bfloat16"])
+@pytest.mark.parametrize("dtype", ["float32", "float64", "float16", "bfloat16", "int16"])
 def test_static_sums_match_allocating_entry_point(cuda, n, dtype):
     dtype = getattr(torch, dtype)
     w = tgv_state(n)

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
     R g[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        g[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(inv(d)) * N + L.k[loc(inv(d))]);
+        g[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(inv(d)) * N + L.k[loc(inv(d))], d);
 
     R drho = R(0), vx1 = R(0), vx2 = R(0), vx3 = R(0), cuSq = R(0);
     if (KIND == VFB_BC_NOSLIP_INTERPOLATED || KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_SLIP ||
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
             const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
             value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, sx, sy, sz), w);
         }
-        Storage<S>::store(target, value);
+        Storage<S>::store(target, value, d);
     }
 }
 
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)]);
+        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)], d);
     R drho1 = pyramidDensity(f);
     const R oneOverRho = R(1) / (drho1 + R(1));
     const R vx1 = pyramidJx(f) * oneOverRho;
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
         const int c = axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d);
         if (c == sgn)
             continue;
-        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d]);
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d], d);
     }
 }
 
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(128) bcOutflowKernel(S* __restrict__ dist, con
         R f[27];
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+            f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], d);
         rhoCorrection = factor * pyramidDensity(f);
     }
 #pragma unroll
@@ -216,12 +216,12 @@ __global__ void __launch_bounds__(128) bcOutflowKernel(S* __restrict__ dist, con
         const int c = axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d);
         if (c != -sgn)
             continue;
-        const R fNode = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
-        const R fNeighbour = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)]);
+        const R fNode = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], d);
+        const R fNeighbour = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + LN.k[loc(d)], d);
         R v = fNeighbour * cs + (R(1) - cs) * fNode;
         if (CORRECTION)
             v = v - weight<R>(d) * rhoCorrection;
-        Storage<S>::store(dist + (unsigned long long)slot<!EVEN>(d) * N + L.k[loc(d)], v);
+        Storage<S>::store(dist + (unsigned long long)slot<!EVEN>(d) * N + L.k[loc(d)], v, d);
     }
 }
 
@@ -345,6 +345,7 @@ extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice,
     case VFB_FP32: return launchPost<float>(kind, lattice, list, s);
     case VFB_FP64: return launchPost<double>(kind, lattice, list, s);
     case VFB_FP16: return launchPost<__half>(kind, lattice, list, s);
+    case VFB_FX16: return launchPost<int16_t>(kind, lattice, list, s);
     default: return launchPost<__nv_bfloat16>(kind, lattice, list, s);
     }
 }
@@ -370,6 +371,7 @@ extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice,
     case VFB_FP32: return launchPressure<float>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     case VFB_FP64: return launchPressure<double>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     case VFB_FP16: return launchPressure<__half>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    case VFB_FX16: return launchPressure<int16_t>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     }
 }
@@ -399,6 +401,7 @@ extern "C" int vfb_bc_outflow_nonreflecting(int storage, const vfb_bc_lattice* l
     case VFB_FP32: return launchOutflow<float>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     case VFB_FP64: return launchOutflow<double>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     case VFB_FP16: return launchOutflow<__half>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
+    case VFB_FX16: return launchOutflow<int16_t>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     default:
         return launchOutflow<__nv_bfloat16>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     }

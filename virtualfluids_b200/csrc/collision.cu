@@ -51,7 +51,7 @@ __device__ __forceinline__ void gatherPre(typename Storage<S>::R* f, const S* __
 {
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], d);
 }
 
 template <class S, bool EVEN>
@@ -60,7 +60,7 @@ __device__ __forceinline__ void scatterPost(const typename Storage<S>::R* f, S* 
 {
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[inv(d)]);
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[inv(d)], d);
 }
 
 template <class S, bool EVEN>
@@ -69,7 +69,7 @@ __device__ __forceinline__ void scatterPre(const typename Storage<S>::R* f, S* _
 {
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d]);
+        Storage<S>::store(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], f[d], d);
 }
 
 constexpr int kCollisionThreads = 128;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)]);
+        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)], d);
     R drho, ux, uy, uz;
     k17Collide<R>(f, a.rates, fx, fy, fz, drho, ux, uy, uz);
     if (WRITE_MACRO) {
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
     }
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)]);
+        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)], d);
 }
 
 template <class S, bool EVEN>
@@ -123,11 +123,11 @@ __global__ void __launch_bounds__(kCollisionThreads) bgkKernel(const CollisionKe
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)]);
+        f[d] = Storage<S>::load(a.base[d] + L.k[loc(d)], d);
     bgkCollide<R>(f, a.rates.omega);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)]);
+        Storage<S>::store(a.base[d] + L.k[loc(d)], f[inv(d)], d);
 }
 
 // InitNavierStokesCompressible_Device.cu:173-200
@@ -219,15 +219,15 @@ __host__ __device__ inline void noneqNode(R drho, R vx1, R vx2, R vx3, const R g
 }
 
 // The reference sets the rest population of a solid or void node to 96
-// (:490-499).  Scaled FP16 cannot hold 96 (its range ends near 16), so it
-// stores the largest finite value instead.
+// (:490-499).  The scaled 16-bit formats cannot hold 96 (their ranges end near
+// 16 and at 0.07), so they store their largest code instead.
 template <class S>
 __device__ __forceinline__ void storeSolidMarker(S* p)
 {
     if constexpr (Storage<S>::scaled)
-        Storage<S>::storeRaw(p, 65504.0f);
+        Storage<S>::storeRaw(p, Storage<S>::marker);
     else
-        Storage<S>::store(p, typename Storage<S>::R(96));
+        Storage<S>::store(p, typename Storage<S>::R(96), d000);
 }
 
 template <class S, bool EVEN>
@@ -524,6 +524,7 @@ extern "C" int vfb_k17_collision(int storage, const vfb_collision_args* args, vo
     case VFB_FP32: return launchCollision<float>(false, args, s);
     case VFB_FP64: return launchCollision<double>(false, args, s);
     case VFB_FP16: return launchCollision<__half>(false, args, s);
+    case VFB_FX16: return launchCollision<int16_t>(false, args, s);
     case VFB_BF16: return launchCollision<__nv_bfloat16>(false, args, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -540,6 +541,7 @@ extern "C" int vfb_bgk_collision(int storage, const vfb_collision_args* args, vo
     case VFB_FP32: return launchCollision<float>(true, args, s);
     case VFB_FP64: return launchCollision<double>(true, args, s);
     case VFB_FP16: return launchCollision<__half>(true, args, s);
+    case VFB_FX16: return launchCollision<int16_t>(true, args, s);
     case VFB_BF16: return launchCollision<__nv_bfloat16>(true, args, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -559,6 +561,7 @@ extern "C" int vfb_init_equilibrium(int storage, void* distributions, unsigned l
     case VFB_FP32: return launchInit<float>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_FP64: return launchInit<double>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_FP16: return launchInit<__half>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    case VFB_FX16: return launchInit<int16_t>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_BF16: return launchInit<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -582,6 +585,7 @@ extern "C" int vfb_init_nonequilibrium(int storage, void* distributions, unsigne
     case VFB_FP32: return launchInitNoneq<float>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_FP64: return launchInitNoneq<double>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_FP16: return launchInitNoneq<__half>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
+    case VFB_FX16: return launchInitNoneq<int16_t>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_BF16:
         return launchInitNoneq<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
@@ -602,6 +606,7 @@ extern "C" int vfb_macroscopic(int storage, const void* distributions, unsigned 
     case VFB_FP32: return launchMacro<float>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_FP64: return launchMacro<double>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_FP16: return launchMacro<__half>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    case VFB_FX16: return launchMacro<int16_t>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_BF16: return launchMacro<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -637,6 +642,7 @@ extern "C" int vfb_mass_and_energy(int storage, const void* distributions, unsig
     case VFB_FP32: rc = launchMassEnergy<float>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     case VFB_FP64: rc = launchMassEnergy<double>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     case VFB_FP16: rc = launchMassEnergy<__half>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    case VFB_FX16: rc = launchMassEnergy<int16_t>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     default: rc = launchMassEnergy<__nv_bfloat16>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     }
     if (rc == VFB_OK) {

@@ -286,14 +286,14 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
             if (!wrapWarp) {
 #pragma unroll
                 for (int d = 0; d < 27; ++d)
-                    f[d] = Storage<S>::load(st + a.smemOff[d]);
+                    f[d] = Storage<S>::load(st + a.smemOff[d], d);
             } else {
                 const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
                 for (int d = 0; d < 27; ++d) {
                     const int l = loc(d);
-                    f[d] = (l & wb) ? Storage<S>::load(a.sbase[d] + locIndex(k, o, l))
-                                    : Storage<S>::load(st + a.smemOff[d]);
+                    f[d] = (l & wb) ? Storage<S>::load(a.sbase[d] + locIndex(k, o, l), d)
+                                    : Storage<S>::load(st + a.smemOff[d], d);
                 }
             }
         }
@@ -308,12 +308,12 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
             if (!wrapWarp) {
 #pragma unroll
                 for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+                    Storage<S>::store(a.gbase[d] + k, f[inv(d)], d);
             } else {
                 const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
                 for (int d = 0; d < 27; ++d)
-                    Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
+                    Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
             }
         }
     }
@@ -341,11 +341,11 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
     if (!wrapWarp) {
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = Storage<S>::load(a.gbase[d] + k);
+            f[d] = Storage<S>::load(a.gbase[d] + k, d);
         collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            Storage<S>::store(a.gbase[d] + k, f[inv(d)]);
+            Storage<S>::store(a.gbase[d] + k, f[inv(d)], d);
     } else {
         const int wb = (int)((__ldg(meta + 4 + WARPS + warp) >> lane) & 1u) |
                        (int)(((__ldg(meta + 4 + 2 * WARPS + warp) >> lane) & 1u) << 1) |
@@ -353,11 +353,11 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
         const LaneOffsets o = laneOffsets(a, wb);
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, loc(d)));
+            f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, loc(d)), d);
         collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
+            Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
     }
 }
 
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
         oA = laneOffsets(a, bitsOf(warp));
         oB = laneOffsets(a, bitsOf(W2 + warp));
     }
-    // FP16's storage scale is applied to both nodes in one paired multiply
+    // a 16-bit format's storage scale is applied to both nodes in one paired multiply
     using St = Storage<S>;
     F2 f[27];
     if (full) {
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
     if (St::scaled) {
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = f[d] * F2(kHalfInvScale);
+            f[d] = f[d] * F2(St::invScale(d));
     }
     F2 fx = a.fx2, fy = a.fy2, fz = a.fz2;
     if (BF) {
@@ -452,9 +452,10 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
         }
     }
     if (St::scaled) {
+        // f[inv(d)] is stored into the slot of d; both directions have the same weight
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = f[d] * F2(kHalfScale);
+            f[d] = f[d] * F2(St::scale(d));
     }
     if (full) {
 #pragma unroll
@@ -543,14 +544,14 @@ __global__ void __launch_bounds__(C::T, C::MINB) asyncKernel(const TiledArgs<S> 
             for (int d = 0; d < 27; ++d) {
                 const int l = loc(d);
                 if (l & wb)
-                    f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, l));
+                    f[d] = Storage<S>::load(a.sbase[d] + locIndex(k, o, l), d);
                 else
-                    f[d] = Storage<S>::load(src + d * C::T);
+                    f[d] = Storage<S>::load(src + d * C::T, d);
             }
             collideNode<S, EVEN, OP, WM, BF>(a, f, k);
 #pragma unroll
             for (int d = 0; d < 27; ++d)
-                Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)]);
+                Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
         }
         k0 = nk0;
         act = nact;
@@ -1070,6 +1071,7 @@ static int runPlanned(Op op, const vfb_collision_plan* plan, const vfb_collision
     case VFB_FP32: return launchTiled<float>(op, p, c, s);
     case VFB_FP64: return launchTiled<double>(op, p, c, s);
     case VFB_FP16: return launchTiled<__half>(op, p, c, s);
+    case VFB_FX16: return launchTiled<int16_t>(op, p, c, s);
     default: return launchTiled<__nv_bfloat16>(op, p, c, s);
     }
 }

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kStaticThreads)
         R f[27];
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)]);
+            f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + L.k[loc(d)], d);
         const R drho = pyramidDensity(f);
         const R oneOverRho = R(1) / (drho + R(1));
         const double ux = (double)(pyramidJx(f) * oneOverRho);
@@ -208,6 +208,7 @@ extern "C" int vfb_mass_and_energy_static(int storage, const void* distributions
     case VFB_FP32: rc = launchStatic<float>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     case VFB_FP64: rc = launchStatic<double>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     case VFB_FP16: rc = launchStatic<__half>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
+    case VFB_FX16: rc = launchStatic<int16_t>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     default: rc = launchStatic<__nv_bfloat16>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     }
     if (rc != VFB_OK)

@@ -91,14 +91,14 @@ __host__ __device__ __forceinline__ uint32_t cornerLocation(const uint32_t* B, i
 template <class S>
 struct DeviceAccess {
     using R = typename Storage<S>::R;
-    __device__ __forceinline__ static R load(const S* p) { return Storage<S>::load(p); }
-    __device__ __forceinline__ static void store(S* p, R v) { Storage<S>::store(p, v); }
+    __device__ __forceinline__ static R load(const S* p, int d) { return Storage<S>::load(p, d); }
+    __device__ __forceinline__ static void store(S* p, R v, int d) { Storage<S>::store(p, v, d); }
 };
 template <class S>
 struct HostAccess {
     using R = S;
-    static R load(const S* p) { return *p; }
-    static void store(S* p, R v) { *p = v; }
+    static R load(const S* p, int) { return *p; }
+    static void store(S* p, R v, int) { *p = v; }
 };
 
 template <class S, class R>
@@ -134,7 +134,7 @@ __host__ __device__ __forceinline__ void cellSourceMoments(const S* dist, unsign
         R f[27];
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            f[d] = A::load(dist + (unsigned long long)slot<EVEN>(d) * N + cornerLocation(B, c, loc(d)));
+            f[d] = A::load(dist + (unsigned long long)slot<EVEN>(d) * N + cornerLocation(B, c, loc(d)), d);
         src[c] = sourceMoments(f, omega);
     }
 }
@@ -160,7 +160,7 @@ __host__ __device__ __forceinline__ void coarseToFineCell(const ScalingView<S, R
 #pragma unroll
         for (int d = 0; d < 27; ++d)
             if (!writes || ((writes[d] >> c) & 1))
-                A::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + cornerLocation(B, c, loc(d)), f[d]);
+                A::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + cornerLocation(B, c, loc(d)), f[d], d);
     }
 }
 
@@ -187,7 +187,7 @@ __host__ __device__ __forceinline__ void fineToCoarseCell(const ScalingView<S, R
     L[7] = v.nZc[L[3]];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        A::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d]);
+        A::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d], d);
 }
 
 template <class S, bool EVEN_C>
@@ -281,6 +281,7 @@ static int runScaling(bool cf, int storage, const vfb_scaling_args* a, void* str
     case VFB_FP32: return launchScaling<float>(cf, a, s);
     case VFB_FP64: return launchScaling<double>(cf, a, s);
     case VFB_FP16: return launchScaling<__half>(cf, a, s);
+    case VFB_FX16: return launchScaling<int16_t>(cf, a, s);
     default: return launchScaling<__nv_bfloat16>(cf, a, s);
     }
 }

@@ -22,17 +22,42 @@ except ImportError:  # pragma: no cover - torch is part of the environment
 STORAGE_OF_DTYPE = {}
 if torch is not None:
     STORAGE_OF_DTYPE = {torch.float32: _lib.FP32, torch.float64: _lib.FP64, torch.float16: _lib.FP16,
-                        torch.bfloat16: _lib.BF16}
+                        torch.bfloat16: _lib.BF16, torch.int16: _lib.FX16}
 
 
 # FP16 storage holds the shifted populations times this power of two (so that
 # deviations of order 1e-6 stay normal numbers); the kernels undo it on load
 HALF_STORAGE_SCALE = 4096.0
+# FX16 storage holds q = round((f_d - w_d) * 2^17 / w_d) as int16
+WEIGHTS = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+FX16_SCALE = 2.0 ** 17 / WEIGHTS
 
 
-def storage_scale(storage_dtype) -> float:
-    """Factor between a stored population and its value (1 except FP16)."""
+def storage_scale(storage_dtype):
+    """Factor between a population and its stored number: a scalar (1 except
+    FP16), or for FX16 an array of 27 per-slot factors (2^17 / w_d)."""
+    if storage_dtype == torch.int16:
+        return FX16_SCALE
     return HALF_STORAGE_SCALE if storage_dtype == torch.float16 else 1.0
+
+
+def decode(dist) -> np.ndarray:
+    """The populations f_d - w_d (FP64 host array, 27 * N) of a stored array."""
+    a = dist.detach().cpu().to(torch.float64).numpy()
+    s = storage_scale(dist.dtype)
+    if np.ndim(s):
+        return (a.reshape(27, -1) / s[:, None]).ravel()
+    return a / s
+
+
+def encode(values, storage_dtype, device="cuda"):
+    """A stored array (27 * N) of the given populations f_d - w_d."""
+    v = np.asarray(values, dtype=np.float64)
+    s = storage_scale(storage_dtype)
+    if np.ndim(s):
+        q = np.clip(np.rint(v.reshape(27, -1) * s[:, None]), -32768, 32767).ravel()
+        return torch.from_numpy(q.astype(np.int16)).to(device)
+    return torch.from_numpy(v * s).to(device, storage_dtype)
 
 
 def compute_dtype(storage_dtype):

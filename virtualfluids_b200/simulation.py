@@ -138,7 +138,8 @@ class Parameter:
         self.main_kernel = kernel
 
     def set_storage(self, storage: str):
-        """Population storage: "fp64", "fp32", or the 16-bit forms "fp16" / "bf16"."""
+        """Population storage: "fp64", "fp32", or the 16-bit forms "fp16" /
+        "bf16" / "fx16" (fixed point relative to the weight, see vf_b200.h)."""
         if storage not in _lib.STORAGE_NAMES:
             raise ValueError(f"unknown storage {storage!r}")
         self.storage = storage
