@@ -144,12 +144,13 @@ def test_planned_bgk_matches_generic(cuda, dtype):
 # every compiled tile configuration (VFB_TILE_CONFIG, read at plan creation):
 # index -> storages it serves
 _CONFIGS_FP64 = [1, 6, 10, 11, 17, 18]
-_CONFIGS_FP32 = [0, 2, 3, 4, 5, 7, 8, 9, 12, 13, 14, 15, 16, 19]
-_CONFIGS_HALF = [9, 12, 19]
+_CONFIGS_FP32 = [0, 2, 3, 4, 5, 7, 8, 9, 12, 13, 14, 15, 16, 19, 20]
+_CONFIGS_HALF = [9, 12, 19, 20]
 
 
 @pytest.mark.parametrize("config,dtype", [(c, "float64") for c in _CONFIGS_FP64] +
-                         [(c, "float32") for c in _CONFIGS_FP32] + [(c, "float16") for c in _CONFIGS_HALF])
+                         [(c, "float32") for c in _CONFIGS_FP32] + [(c, "float16") for c in _CONFIGS_HALF] +
+                         [(c, "int16") for c in _CONFIGS_HALF])
 def test_every_tile_configuration_matches_oracle(cuda, monkeypatch, config, dtype):
     """Each tuning configuration on a box whose rows and tiles do not line up
     (13^3: wrap lanes and partial warps), 6 steps against the FP64 oracle."""
@@ -162,4 +163,4 @@ def test_every_tile_configuration_matches_oracle(cuda, monkeypatch, config, dtyp
         if dtype == "float64":
             assert rel_max(a[fl], b[fl]) < 1e-12
         else:
-            assert rel_l2(a[fl], b[fl]) < (1e-5 if dtype == "float32" else 5e-3)
+            assert rel_l2(a[fl], b[fl]) < {"float32": 1e-5, "float16": 5e-3, "int16": 1e-3}[dtype]

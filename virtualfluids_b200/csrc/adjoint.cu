@@ -161,10 +161,15 @@ __global__ void __launch_bounds__(kThreads)
         UY = __ldg(Vy + i);
         UZ = __ldg(Vz + i);
     }
+    // all q values first: loads issued together, not one per loop iteration
+    R qv[26];
+#pragma unroll
+    for (int j = 0; j < 26; ++j)
+        qv[j] = __ldg(q + (unsigned long long)qOrder(j) * n + i);
 #pragma unroll
     for (int j = 0; j < 26; ++j) {
         const int d = qOrder(j);
-        const R qd = __ldg(q + (unsigned long long)d * n + i);
+        const R qd = qv[j];
         if (!(qd >= R(0) && qd <= R(1)))
             continue;
         const int e = inv(d);
@@ -186,10 +191,15 @@ __global__ void __launch_bounds__(kThreads)
     if (i >= n)
         return;
     const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    // all q values first: loads issued together, not one per loop iteration
+    R qv[26];
+#pragma unroll
+    for (int j = 0; j < 26; ++j)
+        qv[j] = __ldg(q + (unsigned long long)qOrder(j) * n + i);
 #pragma unroll
     for (int j = 0; j < 26; ++j) {
         const int d = qOrder(j);
-        const R qd = __ldg(q + (unsigned long long)d * n + i);
+        const R qd = qv[j];
         if (!(qd >= R(0) && qd <= R(1)))
             continue;
         const int e = inv(d);
@@ -223,10 +233,15 @@ __global__ void __launch_bounds__(kThreads)
     const R c1 = R(1) / (R(1) - omega);
     R gdrho = R(0), gux = R(0), guy = R(0), guz = R(0), gcuSq = R(0);
     R gUx = R(0), gUy = R(0), gUz = R(0);
+    // all q values first: loads issued together, not one per loop iteration
+    R qv[26];
+#pragma unroll
+    for (int j = 0; j < 26; ++j)
+        qv[j] = __ldg(q + (unsigned long long)qOrder(j) * n + i);
 #pragma unroll
     for (int j = 0; j < 26; ++j) {
         const int d = qOrder(j);
-        const R qd = __ldg(q + (unsigned long long)d * n + i);
+        const R qd = qv[j];
         if (!(qd >= R(0) && qd <= R(1)))
             continue;
         const int e = inv(d);
@@ -260,7 +275,10 @@ __global__ void __launch_bounds__(kThreads)
     for (int k = 0; k < 27; ++k) {
         const R v = gg[k] + gdrho +
                     (gux * (R(cx(k)) - vx1) + guy * (R(cy(k)) - vx2) + guz * (R(cz(k)) - vx3)) * oneOverRho;
-        lam[cell<R>(slot<EVEN>(inv(k)), lat.N, L.k[loc(inv(k))])] += v;
+        // atomic: a node can appear in a list more than once (an edge node of
+        // two walls, with the directions of each wall), and all its entries
+        // add into the same cells
+        atomicAdd(lam + cell<R>(slot<EVEN>(inv(k)), lat.N, L.k[loc(inv(k))]), v);
     }
     if (KIND == VFB_BC_VELOCITY_INTERPOLATED && gV) {
         gV[i] += (double)gUx;
@@ -427,16 +445,26 @@ __global__ void __launch_bounds__(kThreads)
         partials[blockIdx.x] = val;
 }
 
-__global__ void reduceKernel(const double* __restrict__ partials, unsigned blocks, int width, double* acc,
-                             double scale)
+// one block per component: each thread sums a fixed strided subset, then a
+// fixed-shape tree (the same order every call)
+constexpr int kReduceThreads = 256;
+__global__ void __launch_bounds__(kReduceThreads)
+    reduceKernel(const double* __restrict__ partials, unsigned blocks, int width, double* acc, double scale)
 {
-    const int c = threadIdx.x;
-    if (c >= width)
-        return;
+    __shared__ double part[kReduceThreads];
+    const int c = blockIdx.x;
     double s = 0.0;
-    for (unsigned b = 0; b < blocks; ++b)
+    for (unsigned b = threadIdx.x; b < blocks; b += kReduceThreads)
         s += partials[(unsigned long long)width * b + c];
-    acc[c] += scale * s;
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kReduceThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            part[threadIdx.x] += part[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        acc[c] += scale * part[0];
 }
 
 int axisOf(int direction, int& axis, int& sgn)
@@ -609,7 +637,7 @@ int objective(const R* dist, unsigned long long N, const uint32_t* nX, const uin
 
 int reducePartials(const double* partials, unsigned blocks, int width, double* acc, double scale, cudaStream_t s)
 {
-    reduceKernel<<<1, 32, 0, s>>>(partials, blocks, width, acc, scale);
+    reduceKernel<<<width, kReduceThreads, 0, s>>>(partials, blocks, width, acc, scale);
     return checkLaunch("partial-sum reduction");
 }
 

@@ -21,9 +21,11 @@
 // Overwritten cells: a BC writes some cells without reading them, so its
 // adjoint runs in two launches: "gather" moves lam at every written cell into
 // tmp[d * n + i] and clears the cell; "scatter" adds the contributions of the
-// node's formula to the cells it read.  Each BC node writes only its own
-// cells, so neither launch races; the pressure scatter adds into the
-// neighbour's cells with atomics, since two BC nodes may share a neighbour.
+// node's formula to the cells it read.  The entries of a list write disjoint
+// cells, so the gather does not race; the scatters add with atomics, since a
+// node may appear in a list more than once (edge nodes of two walls, each
+// entry with the directions of its wall) and two pressure nodes may share a
+// neighbour.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -77,10 +77,16 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
     }
     // slip: normal components are removed for each axis with an active axis direction
     bool flagX = false, flagY = false, flagZ = false;
+    // all q values first, so that their loads are in flight together instead
+    // of one per direction behind the branch on the previous one
+    R qv[26];
+#pragma unroll
+    for (int j = 0; j < 26; ++j)
+        qv[j] = __ldg(q + (unsigned long long)qOrder(j) * nBC + i);
 #pragma unroll
     for (int j = 0; j < 26; ++j) {
         const int d = qOrder(j);
-        const R qd = __ldg(q + (unsigned long long)d * nBC + i);
+        const R qd = qv[j];
         if (!(qd >= R(0) && qd <= R(1)))
             continue;
         const int e = inv(d);

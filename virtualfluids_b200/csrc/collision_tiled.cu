@@ -655,6 +655,8 @@ static const TileConfigInfo kTileConfigs[] = {
     { 256, 2, 3, false }, { 128, 2, 6, false }, { 128, 2, 3, true }, { 128, 2, 2, true },
     // paired, five resident blocks (96 registers, small spills)
     { 256, 1, 5, false },
+    // paired, six resident blocks (80 registers)
+    { 256, 1, 6, false },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
@@ -1023,6 +1025,7 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 13: return dispatchTiled<S, TileCfg<S, 256, 1, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 14: return dispatchTiled<S, TileCfg<S, 256, 1, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 19: return dispatchTiled<S, TileCfg<S, 256, 1, 5>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
+        case 20: return dispatchTiled<S, TileCfg<S, 256, 1, 6>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 9:
             // direct loads, six resident blocks (16-bit storage: all templates)

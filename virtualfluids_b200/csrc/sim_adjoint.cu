@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "adjoint.cuh"
@@ -47,8 +49,21 @@ struct AdjointState {
     uint32_t nObj = 0;
     int velocityKind = -1, noSlipKind = -1, geometryKind = -1;
     bool pressure = false;
+    // captured backward segments (recompute with tapes, then the reverse
+    // steps), keyed by the segment length and the parity it starts from
+    cudaStream_t captureStream = nullptr;
+    std::map<std::pair<unsigned, int>, cudaGraphExec_t> segments;
+    void dropGraphs()
+    {
+        for (auto& g : segments)
+            cudaGraphExecDestroy(g.second);
+        segments.clear();
+    }
     ~AdjointState()
     {
+        dropGraphs();
+        if (captureStream)
+            cudaStreamDestroy(captureStream);
         for (auto* c : checkpoints)
             delete c;
     }
@@ -289,6 +304,13 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
     const unsigned I = A.interval;
     auto perStep = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, (size_t)I * 27 * n * sizeof(R))); };
     auto once = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, 27 * n * sizeof(R))); };
+    // the segment graphs hold these buffers' addresses: a reallocation drops them
+    DeviceBuffer* held[] = { &A.work, &A.lam, &A.tape, &A.recVelocity, &A.recNoSlip, &A.recGeometry, &A.recPressure,
+                             &A.tmpVelocity, &A.tmpNoSlip, &A.tmpGeometry, &A.tmpPressure, &A.gVelocity,
+                             &A.partials, &A.accForce };
+    std::vector<void*> before;
+    for (DeviceBuffer* b : held)
+        before.push_back(b->ptr);
     if (ensure(A.work, stateBytes) || ensure(A.lam, stateBytes) || perStep(A.tape, L.nFluid) ||
         perStep(A.recVelocity, L.velocity.n) || perStep(A.recNoSlip, L.noSlip.n) ||
         perStep(A.recGeometry, L.geometry.n) || perStep(A.recPressure, A.pressureTotal) ||
@@ -296,6 +318,11 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         once(A.tmpPressure, A.pressureTotal) ||
         ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))))
         return cudaFail("adjoint buffers");
+    for (size_t i = 0; i < before.size(); ++i)
+        if (held[i]->ptr != before[i]) {
+            A.dropGraphs();
+            break;
+        }
     if (cudaMemsetAsync(A.lam.ptr, 0, stateBytes, s) != cudaSuccess ||
         cudaMemsetAsync(A.gVelocity.ptr, 0, A.gVelocity.bytes, s) != cudaSuccess)
         return cudaFail("adjoint clear");
@@ -304,15 +331,12 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         return rc;
     if (cudaMemsetAsync(A.accForce.ptr, 0, 3 * sizeof(double), s) != cudaSuccess)
         return cudaFail("force accumulator");
-    Stepper<R> st(S, A, s);
-    const unsigned segments = (A.steps + I - 1) / I;
-    std::vector<char> evenAt(I);
-    for (unsigned c = segments; c-- > 0;) {
-        const unsigned t0 = c * I;
-        const unsigned len = std::min(I, A.steps - t0);
-        if (cudaMemcpyAsync(A.work.ptr, A.checkpoints[c]->ptr, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-            return cudaFail("checkpoint restore");
-        bool even = A.checkpointEven[c] != 0;
+    if (!A.captureStream && cudaStreamCreateWithFlags(&A.captureStream, cudaStreamNonBlocking) != cudaSuccess)
+        return cudaFail("capture stream");
+    // one segment: recompute its steps from the work array with tapes, then
+    // the adjoint steps in reverse order
+    auto segment = [&](Stepper<R>& st, unsigned len, bool even) -> int {
+        std::vector<char> evenAt(len);
         for (unsigned j = 0; j < len; ++j) {
             evenAt[j] = even ? 1 : 0;
             if (const int rc = st.forward(as<R>(A.work), even, (int)j))
@@ -321,6 +345,41 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         for (unsigned j = len; j-- > 0;)
             if (const int rc = st.reverse(evenAt[j] != 0, (int)j))
                 return rc;
+        return VFB_OK;
+    };
+    const unsigned segments = (A.steps + I - 1) / I;
+    for (unsigned c = segments; c-- > 0;) {
+        const unsigned t0 = c * I;
+        const unsigned len = std::min(I, A.steps - t0);
+        if (cudaMemcpyAsync(A.work.ptr, A.checkpoints[c]->ptr, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return cudaFail("checkpoint restore");
+        const bool even = A.checkpointEven[c] != 0;
+        const auto key = std::make_pair(len, even ? 1 : 0);
+        auto it = A.segments.find(key);
+        if (it == A.segments.end()) {
+            // capture the segment's launches once; every segment of this length
+            // and starting parity replays the same graph (same buffers)
+            Stepper<R> cst(S, A, A.captureStream);
+            if (cudaStreamBeginCapture(A.captureStream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                return cudaFail("begin capture");
+            const int rc = segment(cst, len, even);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(A.captureStream, &graph);
+            if (rc != VFB_OK) {
+                if (graph)
+                    cudaGraphDestroy(graph);
+                return rc;
+            }
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = e == cudaSuccess && graph ? cudaGraphInstantiate(&exec, graph, 0) : e;
+            if (graph)
+                cudaGraphDestroy(graph);
+            if (ie != cudaSuccess)
+                return setError(VFB_ERR_CUDA, "segment graph: %s", cudaGetErrorString(ie));
+            it = A.segments.emplace(key, exec).first;
+        }
+        if (cudaGraphLaunch(it->second, s) != cudaSuccess)
+            return cudaFail("segment graph launch");
     }
     if (dVelocity && L.velocity.n &&
         cudaMemcpyAsync(dVelocity, A.gVelocity.ptr, 3ull * L.velocity.n * sizeof(double), cudaMemcpyDeviceToHost, s) !=
@@ -351,8 +410,10 @@ extern "C" int vfb_sim_set_forces(vfb_simulation* sim, const double* forces)
     for (auto& g : sim->graphs)
         cudaGraphExecDestroy(g.second);
     sim->graphs.clear();
-    if (sim->adjoint)
+    if (sim->adjoint) {
         sim->adjoint->ready = false;
+        sim->adjoint->dropGraphs();
+    }
     return VFB_OK;
 }
 
@@ -411,6 +472,8 @@ extern "C" int vfb_sim_adjoint_forward(vfb_simulation* sim, unsigned int steps, 
     if (!sim->adjoint)
         sim->adjoint = new AdjointState;
     AdjointState& A = *sim->adjoint;
+    if (A.interval != checkpointInterval)
+        A.dropGraphs(); // the segment graphs are sized by the interval
     A.storage = sim->params.storage;
     A.steps = steps;
     A.interval = checkpointInterval;
