@@ -438,6 +438,21 @@ int vfb_sim_set_forces(vfb_simulation* sim, const double* forces3);
 int vfb_sim_set_velocity_bc(vfb_simulation* sim, int level, const double* vx, const double* vy, const double* vz,
                             void* stream);
 
+/*
+ * The output of a level in one read of its populations (the work of
+ * Simulation::readAndWriteFiles, Simulation.cpp:595-739, with the analyzers
+ * KineticEnergyAnalyzer.cu:66-154 and EnstrophyAnalyzer.cu:63-98): out8 =
+ * {sum of drho over the fluid list, sum of (1 + drho)|u|^2/2 over it,
+ * non-finite nodes, the kinetic-energy analyzer's mean, its node count, the
+ * enstrophy analyzer's mean, its node count (0 without an inverse neighbour
+ * array), the fluid-list length}, sums in FP64; the same values as
+ * vfb_sim_mass_and_energy, vfb_sim_kinetic_energy and vfb_sim_enstrophy.  The
+ * fields drho, vx, vy, vz (compute precision, numberOfLBnodes) are copied into
+ * the host arrays given (NULL: not copied).  Synchronises the stream.
+ */
+int vfb_sim_output(vfb_simulation* sim, int level, double* out8, void* rho, void* vx, void* vy, void* vz,
+                   void* stream);
+
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,
                         int* isEvenTimestep, double* omega);
@@ -487,6 +502,21 @@ int vfb_enstrophy(int precision, const void* rho, const void* vx, const void* vy
                   unsigned long long numberOfLBnodes, const uint32_t* geo, const uint32_t* neighborX,
                   const uint32_t* neighborY, const uint32_t* neighborZ, const uint32_t* neighborInverse,
                   double* out2, void* stream);
+
+/*
+ * One pass over all nodes: the fields of vfb_macroscopic (into rho/vx/vy/vz,
+ * device arrays of the compute precision) and FP64 sums into the host array
+ * out5 = {sum of drho, sum of (1 + drho)|u|^2/2 and the non-finite count over
+ * the nodes with bit 0 of nodeMask set (the fluid list), the energy sum and
+ * the count over the nodes with bit 1 set (the kinetic-energy analyzer's
+ * set)}.  nodeMask: uint8 per node.  Synchronises the stream.  No reference
+ * counterpart as one pass (MacroscopicQuantities.cu and
+ * KineticEnergyAnalyzer.cu:66-154 in separate ones).
+ */
+int vfb_output_pass(int storage, const void* distributions, unsigned long long numberOfLBnodes, const uint32_t* geo,
+                    const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
+                    const uint8_t* nodeMask, int isEvenTimestep, void* rho, void* vx, void* vy, void* vz,
+                    double* out5, void* stream);
 
 /*
  * drho and velocity of every node from the populations of the given parity

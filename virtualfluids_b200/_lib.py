@@ -187,6 +187,13 @@ _SIGNATURES = [
     ("vfb_sim_adjoint_backward", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_sim_set_forces", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("vfb_sim_output", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("vfb_output_pass", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_sim_set_velocity_bc", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_debug_init_nonequilibrium_node", ctypes.c_int,

@@ -512,11 +512,14 @@ __host__ __device__ __forceinline__ void bgkCollide(R* f, R omega)
                            (f[d00P] - f[d00M]));
     const R cusq = R(1.5) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
     const R keep = R(1) + (-omega);
-    f[d000] = f[d000] * keep - (-omega) * weight<R>(d000) * (drho - rho * cusq);
+    // the weights as compile-time scalars (for a paired type R this avoids a
+    // runtime division per direction; for float / double it is weight<R>)
+    using S = typename ScalarOf<R>::type;
+    f[d000] = f[d000] * keep - (-omega) * R(weight<S>(d000)) * (drho - rho * cusq);
 #pragma unroll
     for (int d = 1; d < 27; ++d) {
         const R cu = cdot<R>(d, vx1, vx2, vx3);
-        f[d] = f[d] * keep - (-omega) * weight<R>(d) * (drho + rho * (R(3) * cu + R(4.5) * cu * cu - cusq));
+        f[d] = f[d] * keep - (-omega) * R(weight<S>(d)) * (drho + rho * (R(3) * cu + R(4.5) * cu * cu - cusq));
     }
 }
 

@@ -1,0 +1,11 @@
+// collision_tiled_fp64.cu -- the planned collision's kernels and launchers for
+// FP64 storage (one translation unit per format, compiled in parallel).
+#include "collision_tiled.cuh"
+
+namespace vfb
+{
+int launchTiledFP64(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s)
+{
+    return launchTiled<double>(op, p, c, s);
+}
+} // namespace vfb

@@ -67,6 +67,7 @@ struct Level {
     // way in and the macroscopic fields on their way out (allocated at first use
     // and kept, so repeated transfers pay no allocation)
     DeviceBuffer fields[4];
+    DeviceBuffer outMask; // the output pass's node mask (built at its first call)
     cudaError_t fieldBuffers(size_t bytes)
     {
         for (auto& f : fields)

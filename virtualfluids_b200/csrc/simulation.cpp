@@ -719,6 +719,77 @@ extern "C" int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, v
     return rc;
 }
 
+// Simulation::readAndWriteFiles (Simulation.cpp:595-739) with the analyzers of
+// the level in two kernels: the output pass (fields, mass / energy sums, the
+// kinetic-energy analyzer's sum) and the enstrophy on the fields it wrote.
+extern "C" int vfb_sim_output(vfb_simulation* sim, int level, double* out8, void* rho, void* vx, void* vy, void* vz,
+                              void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!out8)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out8 is NULL");
+    for (int i = 0; i < 8; ++i)
+        out8[i] = 0.0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!L->outMask.ptr) {
+        // bit 0: in the fluid list; bit 1: in the kinetic-energy analyzer's set
+        std::vector<uint8_t> mask(L->N, 0);
+        std::vector<uint32_t> fl(L->nFluid), en(L->nEnergy);
+        if ((L->nFluid && cudaMemcpyAsync(fl.data(), L->fluid.ptr, fl.size() * 4, cudaMemcpyDeviceToHost, s)) ||
+            (L->nEnergy && cudaMemcpyAsync(en.data(), L->energyNodes.ptr, en.size() * 4, cudaMemcpyDeviceToHost, s)) ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "node lists: %s", cudaGetErrorString(cudaGetLastError()));
+        for (uint32_t k : fl)
+            if (k < L->N)
+                mask[k] |= 1u;
+        for (uint32_t k : en)
+            if (k < L->N)
+                mask[k] |= 2u;
+        if (uploadRaw(L->outMask, mask.data(), mask.size(), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "node mask upload: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    const bool dbl = computeIsDouble(sim->params.storage);
+    const size_t bytes = L->N * (dbl ? sizeof(double) : sizeof(float));
+    if (L->fieldBuffers(bytes) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "field buffers: %s", cudaGetErrorString(cudaGetLastError()));
+    DeviceBuffer* f = L->fields;
+    const auto* geo = static_cast<const uint32_t*>(L->geo.ptr);
+    const auto* nX = static_cast<const uint32_t*>(L->nX.ptr);
+    const auto* nY = static_cast<const uint32_t*>(L->nY.ptr);
+    const auto* nZ = static_cast<const uint32_t*>(L->nZ.ptr);
+    double sums[5];
+    int rc = vfb_output_pass(sim->params.storage, L->dist.ptr, L->N, geo, nX, nY, nZ,
+                             static_cast<const uint8_t*>(L->outMask.ptr), L->isEven ? 1 : 0, f[0].ptr, f[1].ptr,
+                             f[2].ptr, f[3].ptr, sums, stream);
+    if (rc)
+        return rc;
+    out8[0] = sums[0];
+    out8[1] = sums[1];
+    out8[2] = sums[2];
+    out8[3] = L->nEnergy ? sums[3] / (double)L->nEnergy : 0.0;
+    out8[4] = (double)L->nEnergy;
+    out8[7] = (double)L->nFluid;
+    if (L->nNeg.ptr) {
+        double e[2];
+        rc = vfb_enstrophy(dbl ? VFB_FP64 : VFB_FP32, f[0].ptr, f[1].ptr, f[2].ptr, f[3].ptr, L->N, geo, nX, nY, nZ,
+                           static_cast<const uint32_t*>(L->nNeg.ptr), e, stream);
+        if (rc)
+            return rc;
+        out8[5] = e[0];
+        out8[6] = e[1];
+    }
+    void* out[4] = { rho, vx, vy, vz };
+    for (int i = 0; i < 4; ++i)
+        if (out[i] && cudaMemcpyAsync(out[i], f[i].ptr, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "field copy failed");
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "output: %s", cudaGetErrorString(cudaGetLastError()));
+    return VFB_OK;
+}
+
 extern "C" int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* stream)
 {
     clearError();

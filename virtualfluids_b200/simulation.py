@@ -315,6 +315,23 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_enstrophy(self._h, level, out, self.stream))
         return out[0], int(out[1])
 
+    def output(self, level: int = 0, fields: bool = True):
+        """The level's output in one pass over its populations: a dict of the
+        FP64 sums (mass, energy, non-finite count over the fluid list), the
+        kinetic-energy and enstrophy analyzers' means and node counts, and,
+        with fields=True, the host arrays drho, vx, vy, vz."""
+        out = (ctypes.c_double * 8)()
+        N = len(self.levels[level]["geo"])
+        arrays = [np.zeros(N, self.real) for _ in range(4)] if fields else [None] * 4
+        ptrs = [None if a is None else a.ctypes.data for a in arrays]
+        _lib.check(_lib.lib().vfb_sim_output(self._h, level, out, *ptrs, self.stream))
+        r = {"mass": out[0], "energy": out[1], "nonfinite": int(out[2]), "kinetic_energy": out[3],
+             "kinetic_energy_nodes": int(out[4]), "enstrophy": out[5], "enstrophy_nodes": int(out[6]),
+             "fluid_nodes": int(out[7])}
+        if fields:
+            r["fields"] = arrays
+        return r
+
     def set_forces(self, fx: float, fy: float, fz: float):
         """The global force of the following steps (Parameter::setForcing)."""
         g = (ctypes.c_double * 3)(float(fx), float(fy), float(fz))
