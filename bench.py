@@ -471,6 +471,94 @@ def precision_form_record(args, fp32_value, device):
             "format": "int16 q, f_d - w_d = q w_d 2^-17 (FP32 arithmetic)"}
 
 
+def format_study(args):
+    """Which 16-bit storage format reaches the precision target: the
+    Taylor-Green case (n^3, --steps steps, default 2000) run by the FP32
+    planned kernel with the stored populations rounded to a candidate format
+    after every step (what storing in that format does to FP32 arithmetic),
+    against FP64 storage.  Formats: IEEE FP16 (x 2^12), fixed point of
+    (f - w)/w over +-R (R = 1, 0.5, 0.25: the last is FX16), and floating
+    formats of (f - w)/w with p significant bits (FP16C-like 1/4/11 and
+    1/3/12).  The real FX16 kernel is run beside its emulation.  One JSON line."""
+    import numpy as np
+    import torch
+
+    from virtualfluids_b200 import kernels as K
+    from virtualfluids_b200.workloads import taylor_green
+
+    steps = args.steps if args.steps != 50 else 2000
+    dev = torch.device("cuda", 0)
+    w = taylor_green(args.n)
+    g = w.grid
+    lat = K.DeviceLattice.from_arrays(g, dev)
+    N = lat.N
+    fl = torch.from_numpy(g["fluid"].astype(np.int64)).to(dev)
+    W = torch.tensor(K.WEIGHTS, dtype=torch.float32, device=dev)
+    fields = [torch.from_numpy(a).to(dev) for a in (w.rho, w.vx, w.vy, w.vz)]
+
+    def rounder(kind, **kw):
+        def rnd(dist):
+            d = dist.view(27, N)
+            for r in range(27):
+                x = d[r]
+                if kind == "fp16":
+                    x.copy_((x * 4096.0).half().float() / 4096.0)
+                    continue
+                v = x / W[r]
+                if kind == "fixed":
+                    R = kw["R"]
+                    q = torch.clamp(torch.round(v / R * 32768.0), -32768, 32767)
+                    x.copy_(q * (R / 32768.0) * W[r])
+                else:
+                    p, emin, emax = kw["p"], kw["emin"], kw["emax"]
+                    _, e = torch.frexp(v)
+                    e = torch.clamp(e - 1, min=emin)
+                    step = torch.ldexp(torch.ones_like(v), e - (p - 1))
+                    top = (2.0 - 2.0 ** (1 - p)) * 2.0 ** emax
+                    x.copy_(torch.clamp(torch.round(v / step) * step, -top, top) * W[r])
+        return rnd
+
+    def run(dtype, rnd=None):
+        dist = K.new_distributions(lat, dtype, dev)
+        cd = K.compute_dtype(dtype)
+        f = [a.to(cd) for a in fields]
+        for ev in (False, True):
+            K.init_equilibrium(dist, lat, *f, ev)
+        plan = K.CollisionPlan(dtype, lat)
+        if rnd:
+            rnd(dist)
+        even = True
+        for _ in range(steps):
+            K.collision("K17", dist, lat, w.omega, even, plan=plan)
+            if rnd:
+                rnd(dist)
+            even = not even
+        plan.check()
+        plan.close()
+        _, vx, vy, vz = K.macroscopic(dist, lat, even)
+        u = torch.stack([vx[fl], vy[fl], vz[fl]]).double()
+        del dist
+        torch.cuda.empty_cache()
+        return u
+
+    ref = run(torch.float64)
+    nref = float(torch.linalg.norm(ref))
+    rows = {}
+    cases = [("fp32", torch.float32, None), ("fp16_ieee_x4096", torch.float32, rounder("fp16")),
+             ("fixed_R1", torch.float32, rounder("fixed", R=1.0)), ("fixed_R0.5", torch.float32, rounder("fixed", R=0.5)),
+             ("fixed_R0.25_emulated", torch.float32, rounder("fixed", R=0.25)),
+             ("float_p12_e4", torch.float32, rounder("float", p=12, emin=-14, emax=0)),
+             ("float_p13_e3", torch.float32, rounder("float", p=13, emin=-6, emax=0)),
+             ("fx16_kernel", torch.int16, None), ("fp16_kernel", torch.float16, None)]
+    for name, dt, rnd in cases:
+        u = run(dt, rnd)
+        rows[name] = float(torch.linalg.norm(u - ref)) / nref
+        print(json.dumps({name: rows[name]}), file=sys.stderr, flush=True)
+    print(json.dumps({"report": "16-bit format study", "workload": f"taylor-green {args.n}^3, K17, FP32 arithmetic",
+                      "steps": steps, "l2_velocity_error_vs_fp64": rows}), flush=True)
+    return 0
+
+
 def precision_report(args):
     """The precision form: the Taylor-Green case run for --steps steps with
     every storage format through the same public API; L2 velocity error and
@@ -730,6 +818,12 @@ def kernel_report(args):
     n_bc = len(g["velocity.k"])
     ms = timed(lambda: K.bc_post(_lib.BC_VELOCITY_INTERPOLATED, dist, lat, k, q, 1.9, True, *v))
     record(f"velocity_bc_cavity{nb}", n_bc, (27 * 4 + 27 * 4 + 4 + 12) + active * 4 / n_bc, ms, "bc_nodes")
+    # the same with the list's location table (as the simulation runs it): 32 B of
+    # locations per node in place of the neighbour chain
+    locs = K.bc_locations(lat, k)
+    ms = timed(lambda: K.bc_post(_lib.BC_VELOCITY_INTERPOLATED, dist, lat, k, q, 1.9, True, *v, locations=locs))
+    record(f"velocity_bc_cavity{nb}_location_table", n_bc, (27 * 4 + 27 * 4 + 32 + 12) + active * 4 / n_bc, ms,
+           "bc_nodes")
     del dist, lat
     torch.cuda.empty_cache()
     b = MultipleGridBuilder()
@@ -876,6 +970,8 @@ def main(argv=None):
                     help="wall-mounted cube on two levels: NUPS per storage and errors against FP64 (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",
                     help="run every storage format --steps steps and report errors against FP64 (not a bench line)")
+    ap.add_argument("--format-study", action="store_true",
+                    help="L2 error of candidate 16-bit storage formats at TGV n^3 (not a bench line)")
     ap.add_argument("--adjoint-report", action="store_true",
                     help="adjoint channel 128x64x64: forward, adjoint forward and backward step times (not a bench line)")
     args = ap.parse_args(argv)
@@ -891,6 +987,8 @@ def main(argv=None):
         return kernel_report(args)
     if args.adjoint_report:
         return adjoint_report(args)
+    if args.format_study:
+        return format_study(args)
     world, rank, local = init_distributed()
     try:
         if args.impl == "reference":

@@ -163,7 +163,20 @@ typedef struct vfb_bc_list {
     const void* Vy;
     const void* Vz;
     uint32_t numberOfBCnodes;
+    /* optional (NULL: the kernels walk the neighbour arrays as the reference
+     * does): the eight locations of every entry's node, locations[l * n + i]
+     * for location l of entry i (vfb_bc_locations); no reference counterpart */
+    const uint32_t* locations;
 } vfb_bc_list;
+
+/* The location table of a BC list (vfb_bc_list.locations): for each entry i
+ * the eight locations k, nX[k], nY[k], nY[nX[k]], nZ[k], nZ[nX[k]], nZ[nY[k]],
+ * nZ[nY[nX[k]]] of its node k (KernelUtilities.h:221-245) into the device
+ * array out (8 * numberOfBCnodes uint32).  Computed once per list, it spares
+ * every BC launch the chain of dependent neighbour loads.  No reference
+ * counterpart. */
+int vfb_bc_locations(const int32_t* k, uint32_t numberOfBCnodes, const uint32_t* neighborX,
+                     const uint32_t* neighborY, const uint32_t* neighborZ, uint32_t* out, void* stream);
 
 /* post-collision BC kinds (BoundaryConditionFactory.h:75-94) */
 #define VFB_BC_NOSLIP_INTERPOLATED 0   /* NoSlipInterpolatedCompressible_Device, NoSlip/NoSlipInterpolatedCompressible.cu:44-378 */

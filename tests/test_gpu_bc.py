@@ -212,3 +212,24 @@ def test_geometry_bc_with_fractional_q_matches_oracle(cuda, kind, is_even):
         want[changed] = one[changed]
         written |= changed
     assert rel_max(got, want) < 1e-12
+
+
+@pytest.mark.parametrize("kind,lst", CASES)
+@pytest.mark.parametrize("is_even", [True, False])
+def test_location_table_equals_neighbour_chain(cuda, kind, lst, is_even):
+    """A BC list with its location table (vfb_bc_locations) writes exactly what
+    the walk through the neighbour arrays writes."""
+    g = _grid("cavity8" if lst == "velocity" else "channel")
+    _, d = _random_state(g, "f64")
+    k, q = g[f"{lst}.k"], g[f"{lst}.q"]
+    vel = [g[f"velocity.{c}"] for c in ("vx", "vy", "vz")] if lst == "velocity" else [None] * 3
+    out = []
+    for with_table in (False, True):
+        imp = GpuImpl(g, torch.float64)
+        imp.load(d)
+        kk = imp._i(k)
+        locs = K.bc_locations(imp.lat, kk) if with_table else None
+        v = [None if a is None else imp._t(a) for a in vel]
+        K.bc_post(kind, imp.dist, imp.lat, kk, imp._t(q), 1.7, is_even, *v, locations=locs)
+        out.append(imp.dist.cpu().numpy())
+    assert np.array_equal(out[0], out[1])

@@ -79,6 +79,7 @@ class BcList(ctypes.Structure):
         ("Vy", ctypes.c_void_p),
         ("Vz", ctypes.c_void_p),
         ("numberOfBCnodes", ctypes.c_uint32),
+        ("locations", ctypes.c_void_p),
     ]
 
 
@@ -139,6 +140,9 @@ _SIGNATURES = [
       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_bc_post", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.POINTER(BcList), ctypes.c_void_p]),
+    ("vfb_bc_locations", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
     ("vfb_bc_pressure_noneq", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
       ctypes.c_int, ctypes.c_void_p]),

@@ -42,20 +42,50 @@
 namespace vfb
 {
 
+// the eight locations of entry i: from the list's location table when it has
+// one (eight independent loads), else through the neighbour arrays
+__device__ __forceinline__ Locs bcLocations(const uint32_t* __restrict__ table, uint32_t i, uint32_t n,
+                                            const int32_t* __restrict__ bcK, const uint32_t* __restrict__ nX,
+                                            const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ)
+{
+    if (table) {
+        Locs L;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+            L.k[l] = __ldg(table + (unsigned long long)l * n + i);
+        return L;
+    }
+    return listIndices((uint32_t)__ldg(bcK + i), nX, nY, nZ);
+}
+
+__global__ void bcLocationsKernel(const int32_t* __restrict__ bcK, uint32_t n, const uint32_t* __restrict__ nX,
+                                  const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ,
+                                  uint32_t* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const Locs L = listIndices((uint32_t)__ldg(bcK + i), nX, nY, nZ);
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+        out[(unsigned long long)l * n + i] = L.k[l];
+}
+
 template <class S, int KIND, bool EVEN>
 __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
                                                      const int32_t* __restrict__ bcK,
                                                      const typename Storage<S>::R* __restrict__ q, uint32_t nBC,
                                                      const typename Storage<S>::R* __restrict__ Vx,
                                                      const typename Storage<S>::R* __restrict__ Vy,
-                                                     const typename Storage<S>::R* __restrict__ Vz)
+                                                     const typename Storage<S>::R* __restrict__ Vz,
+                                                     const uint32_t* __restrict__ locations)
 {
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nBC)
         return;
     const unsigned long long N = lat.N;
-    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    const Locs L = bcLocations(locations, i, nBC, bcK, lat.nX, lat.nY, lat.nZ);
     // post-collision population moving in direction d: slot of inv(d), location of inv(d)
     R g[27];
 #pragma unroll
@@ -241,9 +271,11 @@ static void launchPostKind(bool even, unsigned blocks, cudaStream_t stream, S* d
     const R* vy = static_cast<const R*>(l->Vy);
     const R* vz = static_cast<const R*>(l->Vz);
     if (even)
-        bcPostKernel<S, KIND, true><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz);
+        bcPostKernel<S, KIND, true><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz,
+                                                                l->locations);
     else
-        bcPostKernel<S, KIND, false><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz);
+        bcPostKernel<S, KIND, false><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz,
+                                                                 l->locations);
 }
 
 template <class S>
@@ -354,6 +386,19 @@ extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice,
     case VFB_FX16: return launchPost<int16_t>(kind, lattice, list, s);
     default: return launchPost<__nv_bfloat16>(kind, lattice, list, s);
     }
+}
+
+extern "C" int vfb_bc_locations(const int32_t* k, uint32_t numberOfBCnodes, const uint32_t* neighborX,
+                                const uint32_t* neighborY, const uint32_t* neighborZ, uint32_t* out, void* stream)
+{
+    clearError();
+    if (numberOfBCnodes == 0)
+        return VFB_OK;
+    if (!k || !neighborX || !neighborY || !neighborZ || !out)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    bcLocationsKernel<<<(numberOfBCnodes + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        k, numberOfBCnodes, neighborX, neighborY, neighborZ, out);
+    return checkLaunch("BC location table");
 }
 
 extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,

@@ -37,6 +37,7 @@ struct DeviceBuffer {
 
 struct BcListDevice {
     DeviceBuffer k, q, vx, vy, vz;
+    DeviceBuffer locations; // 8 * n: the entries' node locations (vfb_bc_locations)
     uint32_t n = 0;
 };
 

@@ -120,6 +120,18 @@ int uploadLevel(Level& L, void* grid, int level, int storage, double geometryVel
         e = uploadRaw(B.k, keep.back().data(), raw.size(), s);
         if (e != cudaSuccess)
             return VFB_OK;
+        // the entries' node locations, once (the BC launches read them instead of the neighbour chain)
+        if (B.n) {
+            e = B.locations.allocate(8ull * B.n * sizeof(uint32_t));
+            if (e != cudaSuccess)
+                return VFB_OK;
+            if (const int rc = vfb_bc_locations(static_cast<const int32_t*>(B.k.ptr), B.n,
+                                                static_cast<const uint32_t*>(L.nX.ptr),
+                                                static_cast<const uint32_t*>(L.nY.ptr),
+                                                static_cast<const uint32_t*>(L.nZ.ptr),
+                                                static_cast<uint32_t*>(B.locations.ptr), s))
+                return rc;
+        }
         if (!need((prefix + ".q").c_str(), 8) || (unsigned long long)count != 27ull * B.n)
             return fail((prefix + ".q").c_str());
         e = uploadReal(B.q, raw, storage, s, keep);
@@ -268,6 +280,7 @@ vfb_bc_list bcList(const BcListDevice& B)
     l.Vy = B.vy.ptr;
     l.Vz = B.vz.ptr;
     l.numberOfBCnodes = B.n;
+    l.locations = static_cast<const uint32_t*>(B.locations.ptr);
     return l;
 }
 

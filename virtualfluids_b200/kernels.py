@@ -254,16 +254,27 @@ def _bc_lattice(dist, lat: DeviceLattice, omega: float, is_even: bool) -> _lib.B
     return t
 
 
+def bc_locations(lat: DeviceLattice, k, stream=None):
+    """The location table of a BC list (8 * len(k) uint32 on the device)."""
+    out = torch.empty(8 * int(k.numel()), dtype=torch.int32, device=k.device)
+    _lib.check(_lib.lib().vfb_bc_locations(k.data_ptr(), int(k.numel()), lat.neighborX.data_ptr(),
+                                           lat.neighborY.data_ptr(), lat.neighborZ.data_ptr(), out.data_ptr(),
+                                           _stream(stream)))
+    return out
+
+
 def bc_post(kind: int, dist, lat: DeviceLattice, k, q, omega: float, is_even: bool, vx=None, vy=None, vz=None,
-            stream=None) -> None:
+            stream=None, locations=None) -> None:
     """One post-collision BC kernel (``kind`` one of _lib.BC_*) over a list:
     ``k`` int32 node indices, ``q`` compute-precision array of 27 * len(k)
-    (direction-major), ``vx``/``vy``/``vz`` per-node wall velocity."""
+    (direction-major), ``vx``/``vy``/``vz`` per-node wall velocity,
+    ``locations`` the list's location table (bc_locations) or None."""
     lst = _lib.BcList()
     lst.k = k.data_ptr()
     lst.q = q.data_ptr()
     lst.Vx, lst.Vy, lst.Vz = _p(vx), _p(vy), _p(vz)
     lst.numberOfBCnodes = int(k.numel())
+    lst.locations = _p(locations)
     t = _bc_lattice(dist, lat, omega, is_even)
     _lib.check(_lib.lib().vfb_bc_post(int(kind), STORAGE_OF_DTYPE[dist.dtype], ctypes.byref(t), ctypes.byref(lst),
                                       _stream(stream)))
