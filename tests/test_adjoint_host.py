@@ -93,3 +93,11 @@ def test_k17_adjoint_is_linear_in_lam():
     g2, _ = adjoint(a, l2, 1.786, (0.01,) * 3, (0, 0, 0))
     g12, _ = adjoint(a, 2.0 * l1 - 3.0 * l2, 1.786, (0.01,) * 3, (0, 0, 0))
     assert np.allclose(g12, 2.0 * g1 - 3.0 * g2, rtol=0, atol=1e-13 * np.abs(g12).max())
+
+
+def test_generated_header_is_current(tmp_path):
+    """The committed reverse sweep (csrc/adjoint_ops.gen.cuh) is what the
+    generator makes from the current operator source."""
+    from virtualfluids_b200 import build
+    out = build.generate_adjoint(tmp_path / "adjoint_ops.gen.cuh")
+    assert out.read_bytes() == build.GEN_OUT.read_bytes()

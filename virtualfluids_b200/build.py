@@ -64,7 +64,42 @@ def compile_one(src: Path, force: bool, verbose: bool) -> Path:
     return obj
 
 
+GEN = PKG / "gen" / "adjoint_gen.cpp"
+GEN_OUT = CSRC / "adjoint_ops.gen.cuh"
+
+
+def cuda_include() -> str:
+    return str(Path(nvcc()).resolve().parent.parent / "include")
+
+
+def generate_adjoint(out: Path = GEN_OUT, verbose: bool = False) -> Path:
+    """Compile and run the adjoint generator (host C++), writing the reverse
+    sweep of the K17 operator to `out` (the header is rewritten only when its
+    content changes, so an unchanged operator does not trigger a rebuild)."""
+    exe = ROOT / "_build" / "gen" / "adjoint_gen"
+    exe.parent.mkdir(parents=True, exist_ok=True)
+    gxx = shutil.which("g++", path="/usr/bin") or shutil.which("g++") or "g++"
+    cmd = [gxx, "-std=c++17", "-O1", "-I", cuda_include(), str(GEN), "-o", str(exe)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"adjoint generator failed to compile:\n{r.stdout}\n{r.stderr}")
+    tmp = exe.parent / "adjoint_ops.gen.cuh.new"
+    r = subprocess.run([str(exe), str(tmp)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"adjoint generator failed:\n{r.stdout}\n{r.stderr}")
+    if not out.exists() or out.read_bytes() != tmp.read_bytes():
+        shutil.copyfile(tmp, out)
+    tmp.unlink()
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
+    # the generated reverse sweep follows the operator it is traced from
+    op = CSRC / "collision_math.cuh"
+    if force or not GEN_OUT.exists() or GEN_OUT.stat().st_mtime < max(GEN.stat().st_mtime, op.stat().st_mtime):
+        generate_adjoint(verbose=verbose)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: compile_one(s, force, verbose), srcs))
