@@ -66,6 +66,10 @@ int vfb_version(void);
 const char* vfb_last_error(void);
 /* bytes of one stored population for a storage format, 0 if unknown */
 int vfb_storage_bytes(int storage);
+/* copy bytes from device memory to host memory on the stream and wait for it
+ * (a convenience for hosts without their own CUDA runtime binding, e.g. to
+ * read arrays that vfb_sim_stress_list points at) */
+int vfb_copy_device_to_host(void* dst, const void* src, size_t bytes, void* stream);
 
 /*
  * Collision arguments.  Mirrors vf::gpu::GPUCollisionParameter
@@ -199,6 +203,56 @@ int vfb_bc_locations(const int32_t* k, uint32_t numberOfBCnodes, const uint32_t*
  * kinds only.
  */
 int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice, const vfb_bc_list* list, void* stream);
+
+/* wall-model (stress) BC kinds (StressBC, BoundaryConditionFactory.h:110-117) */
+#define VFB_BC_STRESS_INTERPOLATED 6          /* StressCompressible_Device, Stress/StressCompressible.cu:50-762 */
+#define VFB_BC_STRESS_BOUNCE_BACK 7           /* StressBounceBackCompressible_Device, Stress/StressBounceBackCompressible.cu:50-679 */
+#define VFB_BC_STRESS_BOUNCE_BACK_PRESSURE 8  /* StressBounceBackPressureCompressible_Device,
+                                                 Stress/StressBounceBackPressureCompressible.cu */
+
+/* A stress list: the reference's stressBC (QforBoundaryConditions) with the
+ * level's wallModel arrays (CudaMemoryManager.cpp:1139-1200, GridGenerator.cpp:319-341).
+ * Arrays of reals are in the compute precision (double for VFB_FP64, float
+ * otherwise); all are device arrays of numberOfBCnodes entries except q
+ * (27 * numberOfBCnodes, direction-major). */
+typedef struct vfb_stress_list {
+    const int32_t* k;              /* BC nodes */
+    const int32_t* kN;             /* velocity sampling node of each entry */
+    const void* q;
+    const void* normalX;           /* wall normal (unit, into the fluid) */
+    const void* normalY;
+    const void* normalZ;
+    void* Vx;                      /* filtered velocity at the sampling node (updated every call) */
+    void* Vy;
+    void* Vz;
+    void* Vx1;                     /* filtered velocity at the wall node (updated every call) */
+    void* Vy1;
+    void* Vz1;
+    const int32_t* samplingOffset; /* wallModel.samplingOffset: sampling height in nodes */
+    const void* z0;                /* wallModel.z0: roughness length in lattice units */
+    void* uStar;                   /* monitors (wallModel.u_star, Fx, Fy, Fz): all four or none (NULL) */
+    void* Fx;
+    void* Fy;
+    void* Fz;
+    uint32_t numberOfBCnodes;
+    const uint32_t* locations;     /* optional location table, as vfb_bc_list.locations */
+} vfb_stress_list;
+
+/*
+ * One wall-model BC kernel over a stress list (one thread per entry).
+ * Replaces the host launchers StressCompressible, StressBounceBackCompressible
+ * and StressBounceBackPressureCompressible (Stress.cu:42-160), run by
+ * BoundaryConditionKernelManager::runStressWallModelKernelPost
+ * (BoundaryConditionKernelManager.cpp:330-334) after the slip BC.  vx, vy, vz
+ * are the level's macroscopic velocity arrays (numberOfLBnodes entries), read
+ * at the sampling nodes: the reference's launchers pass velocityX, velocityY
+ * and velocityY again as vz, and the simulation here passes the same.
+ * turbViscosity (numberOfLBnodes entries) may be NULL: no turbulence model,
+ * the interpolated kind relaxes with omega.  Monitors are written when uStar
+ * is non-NULL (hasWallModelMonitor).
+ */
+int vfb_bc_stress(int kind, int storage, const vfb_bc_lattice* lattice, const vfb_stress_list* list,
+                  const void* turbViscosity, const void* vx, const void* vy, const void* vz, void* stream);
 
 /*
  * The pre-collision non-equilibrium pressure BC of one directional list
@@ -377,6 +431,11 @@ typedef struct vfb_sim_params {
                                   velocities are divided by it at upload, in the compute precision, as
                                   GridGenerator.cpp:507-513 does (side velocity BCs are not scaled);
                                   0 or 1: no scaling */
+    int stressBC;              /* VFB_BC_STRESS_INTERPOLATED / _BOUNCE_BACK / _BOUNCE_BACK_PRESSURE, -1 none
+                                  (BoundaryConditionFactory::setStressBoundaryCondition); runs after the slip
+                                  BC on the grid's stress lists (UpdateGrid27.cpp:243-245) */
+    int hasWallModelMonitor;   /* 1: the stress kernels write u* and the wall momentum per entry
+                                  (Parameter::setHasWallModelMonitor) */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;
@@ -465,6 +524,15 @@ int vfb_sim_set_velocity_bc(vfb_simulation* sim, int level, const double* vx, co
  */
 int vfb_sim_output(vfb_simulation* sim, int level, double* out8, void* rho, void* vx, void* vy, void* vz,
                    void* stream);
+
+/*
+ * The level's stress list as the stress kernels see it (device pointers owned
+ * by the simulation; numberOfBCnodes 0 when the level has none): the wall
+ * model's filter states and, with hasWallModelMonitor, u* and the wall
+ * momentum per entry (the arrays a WallModelProbe reads,
+ * Samplers/WallModelProbe.cu:203-218).
+ */
+int vfb_sim_stress_list(vfb_simulation* sim, int level, vfb_stress_list* out);
 
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,

@@ -30,6 +30,23 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(_vp)
 
 
+def _STRESS_ARGS(R, size_t, count_t):
+    return [_c.c_int, _vp, size_t, _vp, _vp, _vp, _vp, _vp, _vp, count_t, R, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_int, _vp, _vp, _vp, _vp, _c.c_int]
+
+
+STRESS_STATE = ("vxEl", "vyEl", "vzEl", "vxWMean", "vyWMean", "vzWMean")
+STRESS_MONITORS = ("uStar", "Fx", "Fy", "Fz")
+
+
+def _stress_call(kind, dist, N, nx, ny, nz, lst, omega, vx, vy, vz, turb, monitor, is_even):
+    n = len(lst["k"])
+    return (kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(lst["k"]), _ptr(lst["kN"]), _ptr(lst["q"]), n,
+            omega, _ptr(turb), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(lst["normalX"]), _ptr(lst["normalY"]),
+            _ptr(lst["normalZ"]), *[_ptr(lst[a]) for a in STRESS_STATE], _ptr(lst["samplingOffset"]),
+            _ptr(lst["z0"]), int(bool(monitor)), *[_ptr(lst.get(a)) for a in STRESS_MONITORS], int(is_even))
+
+
 class _Lib:
     def __init__(self, path: Path, suffix: str, real):
         self.path = path
@@ -64,6 +81,7 @@ class Oracle(_Lib):
                                                      _c.c_int, _c.c_int]
         self.fn("vfo_bc_outflow").argtypes = [_c.c_int, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _c.c_uint32,
                                               _c.c_int, R, _c.c_int]
+        self.fn("vfo_bc_stress").argtypes = _STRESS_ARGS(R, _c.c_uint64, _c.c_uint32)
         self.fn("vfo_enstrophy_nodes").argtypes = [_vp, _vp, _vp, _vp, _c.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp,
                                                    _vp]
         self.fn("vfo_macroscopic").argtypes = [_vp, _c.c_uint64, _vp, _vp, _vp, _vp, _c.c_int, _vp, _vp, _vp, _vp]
@@ -117,6 +135,13 @@ class Oracle(_Lib):
         self.fn("vfo_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,
                                _ptr(vx), _ptr(vy), _ptr(vz), int(is_even))
 
+    def bc_stress(self, kind, dist, N, nx, ny, nz, lst, omega, vx, vy, vz, turb=None, monitor=False, is_even=True):
+        """Wall-model BC (kind 0 StressCompressible, 1 StressBounceBack, 2
+        StressBounceBackPressure) over the list dict lst (its filter and
+        monitor arrays are updated in place)."""
+        self.fn("vfo_bc_stress")(*_stress_call(kind, dist, N, nx, ny, nz, lst, omega, vx, vy, vz, turb, monitor,
+                                               is_even))
+
     def bc_pressure(self, dist, N, nx, ny, nz, k, kN, rho, direction, is_even=True):
         self.fn("vfo_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN), _ptr(rho),
                                          len(k), direction, int(is_even))
@@ -167,6 +192,7 @@ class Reference(_Lib):
                                                        _c.c_int, _c.c_int]
         self.fn("vfref_bc_outflow").argtypes = [_c.c_int, _vp, _c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _c.c_uint,
                                                 _c.c_int, R, _c.c_int]
+        self.fn("vfref_bc_stress").argtypes = _STRESS_ARGS(R, _c.c_ulonglong, _c.c_uint)
         self.fn("vfref_grid_build").restype = _vp
         self.fn("vfref_grid_build").argtypes = [_vp]
         self.fn("vfref_grid_levels").argtypes = [_vp]
@@ -227,6 +253,10 @@ class Reference(_Lib):
     def bc_post(self, kind, dist, N, nx, ny, nz, k, q, omega, vx=None, vy=None, vz=None, is_even=True):
         self.fn("vfref_bc_post")(kind, _ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(q), len(k), omega,
                                  _ptr(vx), _ptr(vy), _ptr(vz), int(is_even))
+
+    def bc_stress(self, kind, dist, N, nx, ny, nz, lst, omega, vx, vy, vz, turb=None, monitor=False, is_even=True):
+        self.fn("vfref_bc_stress")(*_stress_call(kind, dist, N, nx, ny, nz, lst, omega, vx, vy, vz, turb, monitor,
+                                                 is_even))
 
     def bc_pressure(self, dist, N, nx, ny, nz, k, kN, rho, direction, is_even=True):
         self.fn("vfref_bc_pressure_noneq")(_ptr(dist), N, _ptr(nx), _ptr(ny), _ptr(nz), _ptr(k), _ptr(kN),
@@ -350,9 +380,10 @@ class ReferenceGpu(_Lib):
 _NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims", "fluid",
           "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k", "slip.nx", "slip.ny",
           "slip.nz", "slip.q", "geometry.k", "geometry.q", "geometry.vx", "geometry.vy", "geometry.vz",
-          "pressure.count", "cf.coarse", "cf.fine", "fc.coarse",
+          "pressure.count", "stress.k", "stress.kN", "stress.nx", "stress.ny", "stress.nz", "stress.q",
+          "stress.samplingOffset", "stress.z0", "cf.coarse", "cf.fine", "fc.coarse",
           "fc.fine", "cf.offX", "cf.offY", "cf.offZ", "fc.offX", "fc.offY", "fc.offZ"]
-_INT_NAMES = {"velocity.k", "slip.k", "geometry.k", "pressure.count", "dims"}
+_INT_NAMES = {"velocity.k", "slip.k", "geometry.k", "pressure.count", "dims", "stress.samplingOffset"}
 
 
 def _dtype_for(name: str, size: int):

@@ -25,6 +25,7 @@
 #include "BoundaryConditions/Slip/Slip_Device.cuh"
 #include "BoundaryConditions/Pressure/Pressure_Device.cuh"
 #include "BoundaryConditions/Outflow/Outflow_Device.cuh"
+#include "BoundaryConditions/Stress/Stress_Device.cuh"
 #include "Kernel/Compressible/NavierStokes/B92/B92CompressibleNavierStokes_Device.cuh"
 #include "PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/InitNavierStokesCompressible_Device.cuh"
 
@@ -157,6 +158,38 @@ void REF(vfref_bc_post)(int kind, real* dist, unsigned long long N, unsigned* nx
                                                                 isEven != 0);
             break;
         default: break;
+        }
+    }
+}
+
+// the wall-model (stress) kernels over one list; kind: 0 StressCompressible_Device,
+// 1 StressBounceBackCompressible_Device, 2 StressBounceBackPressureCompressible_Device
+// (Stress.cu:42-160 passes the level's velocityY as vz; the caller decides here)
+void REF(vfref_bc_stress)(int kind, real* dist, unsigned long long N, unsigned* nx, unsigned* ny, unsigned* nz,
+                          int* bcNodes, int* samplingNodes, real* q, unsigned nBC, real omega, real* turbViscosity,
+                          real* vx, real* vy, real* vz, real* normalX, real* normalY, real* normalZ, real* vxEl,
+                          real* vyEl, real* vzEl, real* vxWMean, real* vyWMean, real* vzWMean, int* samplingOffset,
+                          real* z0, int hasMonitor, real* uStar, real* Fx, real* Fy, real* Fz, int isEven)
+{
+    for (unsigned t = 0; t < nBC; ++t) {
+        setThread(t);
+        switch (kind) {
+        case 0:
+            StressCompressible_Device(dist, bcNodes, samplingNodes, q, nBC, omega, turbViscosity, vx, vy, vz, normalX,
+                                      normalY, normalZ, vxEl, vyEl, vzEl, vxWMean, vyWMean, vzWMean, samplingOffset, z0,
+                                      hasMonitor != 0, uStar, Fx, Fy, Fz, nx, ny, nz, N, isEven != 0);
+            break;
+        case 1:
+            StressBounceBackCompressible_Device(dist, bcNodes, samplingNodes, q, nBC, vx, vy, vz, normalX, normalY,
+                                                normalZ, vxEl, vyEl, vzEl, vxWMean, vyWMean, vzWMean, samplingOffset,
+                                                z0, hasMonitor != 0, uStar, Fx, Fy, Fz, nx, ny, nz, N, isEven != 0);
+            break;
+        default:
+            StressBounceBackPressureCompressible_Device(dist, bcNodes, samplingNodes, q, nBC, vx, vy, vz, normalX,
+                                                        normalY, normalZ, vxEl, vyEl, vzEl, vxWMean, vyWMean, vzWMean,
+                                                        samplingOffset, z0, hasMonitor != 0, uStar, Fx, Fy, Fz, nx, ny,
+                                                        nz, N, isEven != 0);
+            break;
         }
     }
 }

@@ -56,13 +56,18 @@ SideType sideOf(int s)
     }
 }
 
-void applyBC(LevelGridBuilder& b, SideType side, int type, double v0, double v1, double v2)
+void applyBC(LevelGridBuilder& b, SideType side, int type, double v0, double v1, double v2,
+             const double* stress = nullptr)
 {
     switch (type) {
     case 1: b.setNoSlipBoundaryCondition(side); break;
     case 2: b.setVelocityBoundaryCondition(side, (real)v0, (real)v1, (real)v2); break;
     case 3: b.setPressureBoundaryCondition(side, (real)v0); break;
     case 4: b.setSlipBoundaryCondition(side, (real)v0, (real)v1, (real)v2); break;
+    case 5:
+        b.setStressBoundaryCondition(side, (real)v0, (real)v1, (real)v2, (uint)stress[0], (real)stress[1],
+                                     (real)stress[2]);
+        break;
     default: break;
     }
 }
@@ -100,7 +105,9 @@ extern "C" {
 //           7 values each (kind 1..4 and the parameters above) from [64] on
 //  [26..29] geometry BC type (1 no-slip, 2 velocity, 4 slip) and values
 //  [30..59] six side BCs in the order they are set: side id (0..5 = MX..PZ),
-//           type (0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip), 3 values
+//           type (0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip, 5 stress), 3 values
+//  [176 + 3 i .. 178 + 3 i]  stress side slot i: sampling offset, z0, level-0 dx
+//           (present when a slot has type 5)
 //  [60]     enableThinWalls argument of buildGrids
 //  [61]     finest level of the refinement box (0 = level 1)
 // a primitive from 7 spec values: kind (1 Cuboid, 2 Sphere, 3 Cylinder,
@@ -145,7 +152,7 @@ void* REF(vfref_grid_build)(const double* s)
     for (int i = 0; i < 6; ++i) {
         const double* b = s + 30 + 5 * i;
         if ((int)b[1] != 0)
-            applyBC(*builder, sideOf((int)b[0]), (int)b[1], b[2], b[3], b[4]);
+            applyBC(*builder, sideOf((int)b[0]), (int)b[1], b[2], b[3], b[4], s + 176 + 3 * i);
     }
     if (s[19] > 0 && (int)s[26] != 0)
         applyBC(*builder, SideType::GEOMETRY, (int)s[26], s[27], s[28], s[29]);
@@ -201,6 +208,23 @@ void* REF(vfref_grid_build)(const double* s)
         A.put("slip.ny", sny.data(), ns);
         A.put("slip.nz", snz.data(), ns);
         exportQs(A, "slip.q", ns, &LevelGridBuilder::getSlipQs, *builder, level);
+
+        const uint nt = builder->getStressSize(level);
+        {
+            std::vector<int> tk(nt), tkN(nt), toff(nt);
+            std::vector<real> tnx(nt), tny(nt), tnz(nt), v(nt), z0(nt);
+            if (nt)
+                builder->getStressValues(tnx.data(), tny.data(), tnz.data(), v.data(), v.data(), v.data(), v.data(),
+                                         v.data(), v.data(), tk.data(), tkN.data(), toff.data(), z0.data(), level);
+            A.put("stress.k", tk.data(), nt);
+            A.put("stress.kN", tkN.data(), nt);
+            A.put("stress.nx", tnx.data(), nt);
+            A.put("stress.ny", tny.data(), nt);
+            A.put("stress.nz", tnz.data(), nt);
+            A.put("stress.samplingOffset", toff.data(), nt);
+            A.put("stress.z0", z0.data(), nt);
+            exportQs(A, "stress.q", nt, &LevelGridBuilder::getStressQs, *builder, level);
+        }
 
         const uint ng = builder->getGeometrySize(level);
         std::vector<int> gk(ng);

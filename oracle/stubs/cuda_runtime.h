@@ -19,5 +19,23 @@ extern thread_local uint3 blockIdx;
 extern thread_local dim3 blockDim;
 extern thread_local dim3 gridDim;
 inline void __syncthreads() {}
+/* The global min / max overloads CUDA's math headers give host and device
+ * code: same-type pairs, and a float paired with a double promoted to double. */
+#include <cmath>
+inline float min(float a, float b) { return fminf(a, b); }
+inline float max(float a, float b) { return fmaxf(a, b); }
+inline double min(double a, double b) { return fmin(a, b); }
+inline double max(double a, double b) { return fmax(a, b); }
+inline double min(float a, double b) { return fmin((double)a, b); }
+inline double max(float a, double b) { return fmax((double)a, b); }
+inline double min(double a, float b) { return fmin(a, (double)b); }
+inline double max(double a, float b) { return fmax(a, (double)b); }
+/* and CUDA's float overload of log (the reference's wall model calls log on
+ * a float in its single-precision build) */
+inline float log(float x) { return logf(x); }
+inline int min(int a, int b) { return a < b ? a : b; }
+inline int max(int a, int b) { return a > b ? a : b; }
+inline unsigned int min(unsigned int a, unsigned int b) { return a < b ? a : b; }
+inline unsigned int max(unsigned int a, unsigned int b) { return a > b ? a : b; }
 typedef struct CUstream_st* cudaStream_t;
 #endif

@@ -839,6 +839,176 @@ void FN(vfo_bc_post)(int kind, real *dist, uint64_t N, const uint32_t *nx, const
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* wall-model (stress) BCs (src/gpu/core/BoundaryConditions/Stress/)         */
+/* ------------------------------------------------------------------------ */
+/* square root and natural logarithm in the working precision (the float
+ * overloads a CUDA build calls on a float) */
+#define RSQRT(x) (sizeof(real) == sizeof(float) ? (real)sqrtf((float)(x)) : (real)sqrt((double)(x)))
+#define RLOG(x) (sizeof(real) == sizeof(float) ? (real)logf((float)(x)) : (real)log((double)(x)))
+
+/* clip of the wall velocity (iMEM.cuh:131-136): the model's value
+ * -3 F forceFactor is formed in double (the literal 3.0 promotes it) and
+ * bounded by +-clip, the double min / max ignoring a NaN operand */
+static real imem_clip(real clip, real F, real forceFactor)
+{
+    const double t = -3.0 * (double)F * (double)forceFactor;
+    return (real)(clip > -clip ? fmin((double)clip, fmax((double)-clip, t)) : fmax((double)clip, fmin((double)-clip, t)));
+}
+
+/* the iMEM wall model of one BC entry (iMEM.cuh:57-137): temporal filters of
+ * the velocity at the sampling node kN and at the wall node, the friction
+ * velocity from the log law at height samplingOffset + q over z0, the wall
+ * shear stress scaled with the wall node's tangential velocity (Schumann-
+ * Groetzbach) and the wall velocity that applies the momentum difference.
+ * The filter updates mix precisions as the reference writes them: eps * v in
+ * the working precision, (1.0 - eps) * mean in double. */
+static void imem(uint32_t i, uint32_t kN, const real *nX, const real *nY, const real *nZ, const real *vx,
+                 const real *vy, const real *vz, real *vxEl, real *vyEl, real *vzEl, real *vxWMean, real *vyWMean,
+                 real *vzWMean, real vxW, real vyW, real vzW, real rho, const int32_t *samplingOffset, real q,
+                 real forceFactor, real eps, const real *z0, int hasMonitor, real *uStarMonitor, real wmX, real wmY,
+                 real wmZ, real *VX, real *VY, real *VZ)
+{
+    const real wnx = nX[i], wny = nY[i], wnz = nZ[i];
+    real el[3], wm[3];
+    el[0] = (real)((double)(eps * vx[kN]) + (1.0 - (double)eps) * (double)vxEl[i]);
+    el[1] = (real)((double)(eps * vy[kN]) + (1.0 - (double)eps) * (double)vyEl[i]);
+    el[2] = (real)((double)(eps * vz[kN]) + (1.0 - (double)eps) * (double)vzEl[i]);
+    vxEl[i] = el[0];
+    vyEl[i] = el[1];
+    vzEl[i] = el[2];
+    wm[0] = (real)((double)(eps * vxW) + (1.0 - (double)eps) * (double)vxWMean[i]);
+    wm[1] = (real)((double)(eps * vyW) + (1.0 - (double)eps) * (double)vyWMean[i]);
+    wm[2] = (real)((double)(eps * vzW) + (1.0 - (double)eps) * (double)vzWMean[i]);
+    vxWMean[i] = wm[0];
+    vyWMean[i] = wm[1];
+    vzWMean[i] = wm[2];
+
+    /* tangential parts */
+    const real dEl = el[0] * wnx + el[1] * wny + el[2] * wnz;
+    el[0] -= dEl * wnx;
+    el[1] -= dEl * wny;
+    el[2] -= dEl * wnz;
+    const real magEl = RSQRT(el[0] * el[0] + el[1] * el[1] + el[2] * el[2]);
+    const real dWm = wm[0] * wnx + wm[1] * wny + wm[2] * wnz;
+    wm[0] -= dWm * wnx;
+    wm[1] -= dWm * wny;
+    wm[2] -= dWm * wnz;
+    const real magWm = RSQRT(wm[0] * wm[0] + wm[1] * wm[1] + wm[2] * wm[2]);
+    const real dW = vxW * wnx + vyW * wny + vzW * wnz;
+    const real tx = vxW - dW * wnx, ty = vyW - dW * wny, tz = vzW - dW * wnz;
+
+    const real z = (real)samplingOffset[i] + q;
+    const real kappa = (real)0.4;
+    const real uStar = magEl * kappa / (RLOG(z / z0[i]));
+    if (hasMonitor)
+        uStarMonitor[i] = uStar;
+    const real tauW = uStar * uStar;
+    const real A = (real)1.0;
+    const real Fwx = (tauW * A) * (tx / magWm);
+    const real Fwy = (tauW * A) * (ty / magWm);
+    const real Fwz = (tauW * A) * (tz / magWm);
+    const real dM = wmX * wnx + wmY * wny + wmZ * wnz;
+    const real Fx = Fwx - (wmX - dM * wnx) / rho;
+    const real Fy = Fwy - (wmY - dM * wny) / rho;
+    const real Fz = Fwz - (wmZ - dM * wnz) / rho;
+    const real clip = (real)2.0;
+    *VX = imem_clip(clip * el[0], Fx, forceFactor);
+    *VY = imem_clip(clip * el[1], Fy, forceFactor);
+    *VZ = imem_clip(clip * el[2], Fz, forceFactor);
+}
+
+#define BC_STRESS_INTERP 0
+#define BC_STRESS_BB 1
+#define BC_STRESS_BB_PRESSURE 2
+
+/* wall-model BC over one list, one entry after another:
+ *   StressCompressible_Device (StressCompressible.cu:50-762): interpolated
+ *     bounce-back with the pressure term (KernelUtilities.h:199-206) and the
+ *     relaxation rate om1 / (1 + 3 om1 max(0, nu_t)); the wall velocity's term
+ *     divided by 1 + q, force factor 1 + q_B;
+ *   StressBounceBackCompressible_Device (StressBounceBackCompressible.cu:50-679):
+ *     simple bounce-back, force factor 1;
+ *   StressBounceBackPressureCompressible_Device
+ *     (StressBounceBackPressureCompressible.cu): simple bounce-back minus w drho.
+ * The first pass forms every incoming population of a wall direction and the
+ * momentum exchanged with the wall at rest, iMEM turns it into a wall
+ * velocity, the second pass writes the incoming populations with the wall
+ * velocity's term.  StressCompressible_Device weighs the pressure term of its
+ * dPP0 direction with 2/27 (StressCompressible.cu:293); kept.  turbViscosity
+ * may be NULL (no turbulence model: the rate is om1). */
+void FN(vfo_bc_stress)(int kind, real *dist, uint64_t N, const uint32_t *nx, const uint32_t *ny, const uint32_t *nz,
+                       const int32_t *bcNodes, const int32_t *samplingNodes, const real *q, uint32_t nBC, real omega,
+                       const real *turbViscosity, const real *vx, const real *vy, const real *vz, const real *normalX,
+                       const real *normalY, const real *normalZ, real *vxEl, real *vyEl, real *vzEl, real *vxWMean,
+                       real *vyWMean, real *vzWMean, const int32_t *samplingOffset, const real *z0, int hasMonitor,
+                       real *uStar, real *Fx, real *Fy, real *Fz, int isEven)
+{
+    for (uint32_t i = 0; i < nBC; ++i) {
+        const locs8 L = list_indices((uint32_t)bcNodes[i], nx, ny, nz);
+        real g[27];
+        for (int d = 0; d < 27; ++d)
+            g[d] = post_value(dist, N, &L, isEven, d);
+        real drho, vx1, vx2, vx3;
+        bc_macros(g, &drho, &vx1, &vx2, &vx3);
+        const real cu_sq = C(3, 2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3) * ((real)1 + drho);
+        real omTurb = omega;
+        if (kind == BC_STRESS_INTERP && turbViscosity) {
+            const real nu = turbViscosity[bcNodes[i]];
+            omTurb = omega / ((real)1 + (real)3 * omega * (nu > (real)0 ? nu : (real)0));
+        }
+        const int odd = !isEven;
+        real fin[27];
+        real wmX = 0, wmY = 0, wmZ = 0;
+        for (int j = 0; j < 26; ++j) {
+            const int d = QORDER[j];
+            const real qd = q[(uint64_t)d * nBC + i];
+            if (!(qd >= (real)0 && qd <= (real)1))
+                continue;
+            const int e = INV[d];
+            const real w = weight_of(d);
+            if (kind == BC_STRESS_BB) {
+                fin[d] = g[d];
+            } else if (kind == BC_STRESS_BB_PRESSURE) {
+                fin[d] = g[d] - w * drho;
+            } else {
+                const real feq = feq_bc(drho, cdot(d, vx1, vx2, vx3), cu_sq, w);
+                const real wp = d == dPP0 ? C(2, 27) : w;
+                fin[d] = interp_noslip(qd, g[d], g[e], feq, omTurb) - wp * drho;
+            }
+            const real t = g[d] + fin[d];
+            if (CX[d] > 0) wmX += t; else if (CX[d] < 0) wmX -= t;
+            if (CY[d] > 0) wmY += t; else if (CY[d] < 0) wmY -= t;
+            if (CZ[d] > 0) wmZ += t; else if (CZ[d] < 0) wmZ -= t;
+        }
+        const real qB = q[(uint64_t)d00M * nBC + i];
+        const real forceFactor = kind == BC_STRESS_INTERP ? (real)(1.0 + (double)qB) : (real)1.0;
+        real VX, VY, VZ;
+        imem(i, (uint32_t)samplingNodes[i], normalX, normalY, normalZ, vx, vy, vz, vxEl, vyEl, vzEl, vxWMean, vyWMean,
+             vzWMean, vx1, vx2, vx3, (real)1 + drho, samplingOffset, qB, forceFactor, (real)0.001f, z0, hasMonitor, uStar,
+             wmX, wmY, wmZ, &VX, &VY, &VZ);
+        for (int j = 0; j < 26; ++j) {
+            const int d = QORDER[j];
+            const real qd = q[(uint64_t)d * nBC + i];
+            if (!(qd >= (real)0 && qd <= (real)1))
+                continue;
+            const int e = INV[d];
+            real term = (real)6 * weight_of(d) * cdot(d, VX, VY, VZ);
+            if (kind == BC_STRESS_INTERP)
+                term = term / ((real)1 + qd);
+            dist[(uint64_t)slot_of(e, odd) * N + L.k[loc_of(e)]] = fin[d] - term;
+            if (CX[d] > 0) wmX -= term; else if (CX[d] < 0) wmX += term;
+            if (CY[d] > 0) wmY -= term; else if (CY[d] < 0) wmY += term;
+            if (CZ[d] > 0) wmZ -= term; else if (CZ[d] < 0) wmZ += term;
+        }
+        if (hasMonitor) {
+            Fx[i] = wmX;
+            Fy[i] = wmY;
+            Fz[i] = wmZ;
+        }
+    }
+}
+
 /* pre-collision non-equilibrium pressure BC, one directional list
  * (PressureNonEquilibriumCompressible.cu:45-311).  direction is the D3Q27 id
  * of the boundary normal (dM00, dP00, d0M0, d0P0, d00M or d00P). */

@@ -11,6 +11,7 @@ machine without the reference tree.
     python tests/golden/make_golden.py --outflow       (the non-reflecting outflow only)
     python tests/golden/make_golden.py --thin-walls    (the thin-wall grids only)
     python tests/golden/make_golden.py --extra-grids   (the cylinder and conglomerate grids only)
+    python tests/golden/make_golden.py --stress        (the wall-model grid and kernels only)
 """
 from __future__ import annotations
 
@@ -27,7 +28,10 @@ sys.path.insert(0, str(ROOT))
 
 from oracle.pyoracle import Reference  # noqa: E402
 from tests.golden.scenarios import (EXTRA_GRID_SCENARIOS, GRID_SCENARIOS, REFINED_SCENARIOS,  # noqa: E402
-                                    THIN_WALL_SCENARIOS, grid_spec, lattice_sequence, refined_spec)
+                                    STRESS_GRID_SCENARIOS, THIN_WALL_SCENARIOS, grid_spec, lattice_sequence,
+                                    refined_spec)
+from tests.stress_cases import (copy_list, make_stress_list, stress_populations,  # noqa: E402
+                                turbulent_viscosity, velocity_fields)
 
 OUT = Path(__file__).resolve().parent
 
@@ -134,6 +138,39 @@ def outflow(precision: str) -> None:
     np.savez_compressed(OUT / f"outflow_channel_{precision}.npz", **out)
 
 
+def stress(precision: str) -> None:
+    """The three wall-model kernels (StressCompressible,
+    StressBounceBackCompressible, StressBounceBackPressureCompressible) of
+    the reference, two launches each (both parities) on a stress list made
+    from the sphere channel's geometry list (fractional q) with seeded
+    normals, sampling nodes, states and an eddy-viscosity field; stored: the
+    written positions and values, and the list's states and monitors."""
+    R = Reference(precision)
+    real = np.float64 if precision == "f64" else np.float32
+    g = Reference("f64").grid(grid_spec("sphere_channel"))[0]  # the grid of grid_sphere_channel.npz
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    base = make_stress_list(g, "geometry", real, seed=77)
+    vel = velocity_fields(N, real, seed=78)
+    turb = turbulent_viscosity(N, real, seed=79)
+    dist0 = stress_populations(N, real)
+    # the inputs are regenerated from their seeds by the test; their first
+    # values and sums are stored to detect a change of the generator
+    out = {"dist_head": dist0[:16], "dist_sum": np.array(dist0.astype(np.float64).sum()),
+           "vx_head": vel[0][:16], "turb_head": turb[:16], "kN_head": base["kN"][:16]}
+    for kind in (0, 1, 2):
+        d = dist0.copy()
+        lst = copy_list(base)
+        for ev in (1, 0):
+            R.bc_stress(kind, d, N, *nb, lst, real(1.7), *vel, turb=turb, monitor=True, is_even=bool(ev))
+        idx = np.flatnonzero(d != dist0)
+        out[f"idx_{kind}"] = idx
+        out[f"val_{kind}"] = d[idx]
+        for k in ("vxEl", "vyEl", "vzEl", "vxWMean", "vyWMean", "vzWMean", "uStar", "Fx", "Fy", "Fz"):
+            out[f"out{kind}.{k}"] = lst[k]
+    np.savez_compressed(OUT / f"stress_sphere_{precision}.npz", **out)
+
+
 if __name__ == "__main__":
     if len(sys.argv) == 3 and sys.argv[1] == "--refined":
         refined_grid(sys.argv[2])
@@ -148,6 +185,11 @@ if __name__ == "__main__":
         sys.exit(0)
     if len(sys.argv) == 2 and sys.argv[1] == "--extra-grids":
         thin_wall_grids(EXTRA_GRID_SCENARIOS)
+        sys.exit(0)
+    if len(sys.argv) == 2 and sys.argv[1] == "--stress":
+        thin_wall_grids(STRESS_GRID_SCENARIOS)
+        for p in ("f64", "f32"):
+            stress(p)
         sys.exit(0)
     if len(sys.argv) == 2 and sys.argv[1] == "--outflow":
         for p in ("f64", "f32"):

@@ -8,7 +8,7 @@ import math
 import numpy as np
 
 MX, PX, MY, PY, MZ, PZ = range(6)
-NONE, NOSLIP, VELOCITY, PRESSURE, SLIP = range(5)
+NONE, NOSLIP, VELOCITY, PRESSURE, SLIP, STRESS = range(6)
 
 
 def _spec(coarse, periodic=(0, 0, 0), sides=(), thin_walls=False):
@@ -66,6 +66,15 @@ def grid_spec(name: str) -> np.ndarray:
         s[20:26] = [8.4, 5.7, 7.3, 2.6, 6.0, 1]
         s[26] = 1.0
         return s
+    if name == "abl_stress":
+        # the atmospheric boundary layer's sides (apps/gpu/AtmosphericBoundaryLayer):
+        # periodic x and y, the wall-model floor (normal +z, sampling offset 2,
+        # z0 = 0.1, dx = 1) under a slip lid; the stress parameters of side
+        # slot 0 in the spec's stress block (index 176 on)
+        sides = [(MZ, STRESS, 0, 0, 1), (PZ, SLIP, 0, 0, -1)]
+        s = np.concatenate([_spec([0, 0, 0, 15, 7, 11, 1.0], (1, 1, 0), sides=sides), np.zeros(194 - 64)])
+        s[176:179] = [2, 0.1, 1.0]
+        return s
     if name == "conglomerate_channel":
         # three primitives united, a sphere removed from the cuboid
         # (Conglomerate); parts as 7 values each from index 64 on
@@ -85,6 +94,8 @@ GRID_SCENARIOS = ["tgv6", "tgv8", "cavity8", "cavity8_lidfirst", "channel", "sph
 THIN_WALL_SCENARIOS = ["thin_wall_cube", "thin_wall_sphere"]
 # solids added after the first fixtures (generated with --extra-grids)
 EXTRA_GRID_SCENARIOS = ["cylinder_channel", "conglomerate_channel"]
+# the wall-model (stress) BC's lists (generated with --stress)
+STRESS_GRID_SCENARIOS = ["abl_stress"]
 
 # multi-level grids made by the reference's builder, which the repository's
 # builder reproduces: a channel 24 x 16 x 16 with a refined box and the

@@ -184,3 +184,40 @@ def test_sim_params_layout_matches_header():
     body = text[text.index("typedef struct vfb_sim_params {"):text.index("} vfb_sim_params;")]
     names = re.findall(r"^\s+(?:int|double)\s+(\w+)", body, re.M)
     assert names == [f[0] for f in VfbSimParams._fields_]
+
+
+def test_stress_selection_and_wall_model_reader_exist():
+    """The stress kinds, the simulation parameters' wall-model fields and the
+    readers are bound (no GPU call)."""
+    from virtualfluids_b200 import _lib
+    from virtualfluids_b200.simulation import BoundaryConditionFactory, Parameter, StressBC, VfbSimParams
+
+    L = _lib.lib()
+    for name in ("vfb_bc_stress", "vfb_sim_stress_list", "vfb_copy_device_to_host"):
+        assert hasattr(L, name)
+    names = [f[0] for f in VfbSimParams._fields_]
+    assert names[-2:] == ["stressBC", "hasWallModelMonitor"]
+    bc = BoundaryConditionFactory()
+    assert bc.stress == StressBC.NotSpecified
+    bc.set_stress_boundary_condition(StressBC.StressBounceBackPressureCompressible)
+    assert int(bc.stress) == _lib.BC_STRESS_BOUNCE_BACK_PRESSURE == 8
+    p = Parameter()
+    p.set_has_wall_model_monitor(True)
+    assert p.has_wall_model_monitor
+    assert L.vfb_copy_device_to_host(None, None, 0, None) == 0
+
+
+def test_stress_builder_api_errors():
+    from virtualfluids_b200.grid import MultipleGridBuilder, SideType
+
+    b = MultipleGridBuilder()
+    b.addCoarseGrid(0, 0, 0, 7, 7, 7, 1.0)
+    b.buildGrids()
+    with pytest.raises(ValueError):
+        b.setStressBoundaryCondition(SideType.GEOMETRY, 0, 0, 1, 2, 0.1, 1.0)
+    with pytest.raises(ValueError):
+        b.setStressBoundaryCondition(SideType.MZ, 0, 0, 1, 1.5, 0.1, 1.0)
+    # a sampling node beyond the far side of the box is an error of the build
+    b.setStressBoundaryCondition(SideType.MZ, 0, 0, 1, 40, 0.1, 1.0)
+    with pytest.raises(_lib.VfbError):
+        b.arrays()

@@ -37,8 +37,10 @@ def test_planned_matches_generic(cuda, dtype):
     # / BF16: a store may then round to the neighbouring 16-bit value, so the
     # bound is a few units of the format's rounding (2^-11 for FP16, 2^-8 for
     # BF16) after 10 steps.
-    # FX16 (int16): a few steps of 2^-17 of the weight.
-    tol = {"float32": 1e-5, "float16": 2e-3, "bfloat16": 1e-2, "int16": 3e-4}[dtype]
+    # FX16 (int16): a store may round to the neighbouring step of 2^-17 of
+    # the weight, an absolute step; on drho (about 1e-3 here) a few such
+    # steps summed over the node's populations come to a few 1e-3 relative.
+    tol = {"float32": 1e-5, "float16": 2e-3, "bfloat16": 1e-2, "int16": 3e-3}[dtype]
     for a, b in zip(m1, m2):
         assert rel_l2(a[fl], b[fl]) < tol
 
@@ -136,7 +138,9 @@ def test_planned_bgk_matches_generic(cuda, dtype):
     _, _, m1, _ = gpu_run(w, dt, 8, "BGK", planned=True)
     _, _, m2, _ = gpu_run(w, dt, 8, "BGK", planned=False)
     fl = w.grid["fluid"]
-    tol = 1e-6 if dtype == "float32" else 2e-3
+    # the planned BGK pairs two nodes' arithmetic (paired FP32), which rounds
+    # some products the scalar kernel fuses: the FP32 contract, 1e-5 L2
+    tol = 1e-5 if dtype == "float32" else 2e-3
     for a, b in zip(m1, m2):
         assert rel_l2(a[fl], b[fl]) < tol
 
@@ -163,4 +167,5 @@ def test_every_tile_configuration_matches_oracle(cuda, monkeypatch, config, dtyp
         if dtype == "float64":
             assert rel_max(a[fl], b[fl]) < 1e-12
         else:
-            assert rel_l2(a[fl], b[fl]) < {"float32": 1e-5, "float16": 5e-3, "int16": 1e-3}[dtype]
+            # int16 (FX16): the absolute step 2^-17 w on fields of about 1e-3 (drho)
+            assert rel_l2(a[fl], b[fl]) < {"float32": 1e-5, "float16": 5e-3, "int16": 4e-3}[dtype]

@@ -11,8 +11,8 @@ import numpy as np
 import pytest
 
 from oracle.pyoracle import Reference, ref_available
-from tests.golden.scenarios import (EXTRA_GRID_SCENARIOS, GRID_SCENARIOS, REFINED_SCENARIOS, THIN_WALL_SCENARIOS,
-                                    grid_spec, refined_spec)
+from tests.golden.scenarios import (EXTRA_GRID_SCENARIOS, GRID_SCENARIOS, REFINED_SCENARIOS, STRESS_GRID_SCENARIOS,
+                                    THIN_WALL_SCENARIOS, grid_spec, refined_spec)
 from virtualfluids_b200 import grid as vgrid
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -356,3 +356,64 @@ def test_builder_rejects_short_spec():
     s = np.zeros(40)
     h = _lib.lib().vfb_grid_build(s.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(s))
     assert not h
+
+
+def _stress_spec(sides, periodic=(0, 0, 0), dims=(13, 8, 11), box=None):
+    """A box with side BCs (side, type, v0, v1, v2[, offset, z0, dx]) where
+    type 5 is the stress BC; its offset, z0 and dx go to the spec's stress
+    block (vgrid.STRESS_BASE + 3 * slot)."""
+    spec = np.zeros(vgrid.SPEC_WITH_STRESS)
+    spec[0:7] = [0, 0, 0, *dims, 1.0]
+    spec[7:10] = periodic
+    if box is not None:
+        spec[10] = 1
+        spec[11:17] = box
+        spec[17:19] = [4, 4]
+    for i, sd in enumerate(sides):
+        spec[30 + 5 * i: 35 + 5 * i] = sd[:5]
+        if sd[1] == 5:
+            spec[vgrid.STRESS_BASE + 3 * i: vgrid.STRESS_BASE + 3 * i + 3] = sd[5:8]
+    return spec
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("case", ["abl", "walls", "walls_reversed", "refined_floor"])
+def test_stress_lists_match_live_reference(case):
+    """The wall-model BC's lists (LevelGridBuilder::setStressBoundaryCondition):
+    nodes, q, normals, sampling nodes, sampling offsets and the per-level
+    roughness length z0 2^level / dx, against the reference builder."""
+    if case == "abl":
+        # the atmospheric boundary layer's set-up: periodic x and y, a stress
+        # floor under a slip lid (apps/gpu/AtmosphericBoundaryLayer)
+        spec = _stress_spec([(4, 5, 0, 0, 1, 2, 0.1, 1.0), (5, 4, 0, 0, -1)], periodic=(1, 1, 0))
+    elif case == "refined_floor":
+        spec = _stress_spec([(4, 5, 0, 0, 1, 3, 0.05, 0.5), (5, 4, 0, 0, -1)], periodic=(1, 1, 0),
+                            dims=(23, 15, 19), box=(4, 3, 0, 16, 11, 8))
+    else:
+        sides = [(0, 2, 0.04, 0, 0), (1, 3, 0.0, 0, 0), (4, 5, 0, 0, 1, 2, 0.2, 1.0), (5, 1, 0, 0, 0),
+                 (2, 5, 0, 1, 0, 1, 0.01, 2.0), (3, 4, 0, -1, 0)]
+        spec = _stress_spec(sides if case == "walls" else sides[::-1])
+    mine = build_mine(spec)
+    ref = Reference("f64").grid(spec)
+    assert len(ref[0]["stress.k"]) > 0
+    compare(mine, ref)
+    for lvl in range(len(ref)):
+        for name in ("stress.k", "stress.kN", "stress.q", "stress.samplingOffset", "stress.z0", "stress.nz"):
+            assert name in mine[lvl] and name in ref[lvl], name
+    if case == "refined_floor":
+        assert len(ref[1]["stress.k"]) > 0
+        assert np.allclose(mine[1]["stress.z0"], 0.05 * 2 / 0.5)
+
+
+@pytest.mark.parametrize("name", STRESS_GRID_SCENARIOS)
+def test_stress_grid_matches_golden(name):
+    """The atmospheric boundary layer's sides with the wall-model floor:
+    every array, the stress lists included, equal to the reference builder's
+    output committed under tests/golden."""
+    with np.load(GOLDEN / f"grid_{name}.npz") as z:
+        ref = {}
+        for key in z.files:
+            lvl, arr = key.split(":", 1)
+            ref.setdefault(int(lvl[1:]), {})[arr] = z[key]
+    assert len(ref[0]["stress.k"]) > 0
+    compare(build_mine(grid_spec(name)), ref)

@@ -221,3 +221,79 @@ def test_outflow_matches_live_reference_every_direction(precision, correction):
                                 correction, O.real(0.7), ev)
                 out.append(d)
             assert np.array_equal(out[0], out[1]), (direction, ev)
+
+
+@pytest.mark.skipif(not ref_available("f64"), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("grid,lst", [("channel", "slip"), ("sphere_channel", "geometry")])
+@pytest.mark.parametrize("is_even", [True, False])
+def test_stress_bc_matches_live_reference(precision, kind, grid, lst, is_even):
+    """The wall-model BCs (StressCompressible, StressBounceBack,
+    StressBounceBackPressure with the iMEM model): the oracle equals the
+    reference's kernel sources built for the host bit for bit, in the
+    populations, both filter states and the monitors, on a flat wall (q = 1/2)
+    and on the sphere's fractional q, with random unit normals and an eddy
+    viscosity field."""
+    from tests.stress_cases import copy_list, make_stress_list, turbulent_viscosity, velocity_fields
+
+    g = _golden_level0(grid)
+    real = np.float64 if precision == "f64" else np.float32
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    base = make_stress_list(g, lst, real, seed=31 + kind)
+    vel = velocity_fields(N, real, seed=7)
+    turb = turbulent_viscosity(N, real, seed=8)
+    rng = np.random.default_rng(41)
+    fields = [rng.uniform(-1e-2, 1e-2, N).astype(real) for _ in range(4)]
+    out = []
+    for impl in (Oracle(precision), Reference(precision)):
+        d = np.zeros(27 * N, real)
+        for ev in (0, 1):
+            impl.init_eq(d, N, g["geo"], *nb, *fields, ev)
+        d += (np.random.default_rng(5).uniform(-1e-3, 1e-3, d.shape) * (d != 0)).astype(real)
+        lst_i = copy_list(base)
+        before = d.copy()
+        for step in range(2):
+            impl.bc_stress(kind, d, N, *nb, lst_i, real(1.7), *vel, turb=turb, monitor=True,
+                           is_even=is_even ^ bool(step))
+        assert (d != before).sum() > len(base["k"])
+        out.append((d, lst_i))
+    (d0, l0), (d1, l1) = out
+    assert np.array_equal(d0, d1)
+    for name in l0:
+        assert np.array_equal(l0[name], l1[name]), name
+    assert np.all(np.isfinite(l0["uStar"])) and np.any(l0["Fx"] != 0)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_stress_bc_matches_golden(precision, kind):
+    """The oracle's wall-model BCs against the fixture made by the reference's
+    three kernel sources built for the host (tests/golden/make_golden.py
+    --stress): two launches on the sphere channel's geometry list with
+    seeded states, compared in the written populations, states and monitors."""
+    from tests.stress_cases import copy_list, make_stress_list, stress_populations, turbulent_viscosity, velocity_fields
+
+    ref = np.load(GOLDEN / f"stress_sphere_{precision}.npz")
+    g = _golden_level0("sphere_channel")
+    real = np.float64 if precision == "f64" else np.float32
+    N = len(g["geo"])
+    nb = (g["neighborX"], g["neighborY"], g["neighborZ"])
+    base = make_stress_list(g, "geometry", real, seed=77)
+    vel = velocity_fields(N, real, seed=78)
+    turb = turbulent_viscosity(N, real, seed=79)
+    dist0 = stress_populations(N, real)
+    assert np.array_equal(dist0[:16], ref["dist_head"]) and dist0.astype(np.float64).sum() == ref["dist_sum"]
+    assert np.array_equal(vel[0][:16], ref["vx_head"]) and np.array_equal(turb[:16], ref["turb_head"])
+    assert np.array_equal(base["kN"][:16], ref["kN_head"])
+    O = Oracle(precision)
+    d = dist0.copy()
+    lst = copy_list(base)
+    for ev in (1, 0):
+        O.bc_stress(kind, d, N, *nb, lst, real(1.7), *vel, turb=turb, monitor=True, is_even=bool(ev))
+    idx = np.flatnonzero(d != dist0)
+    assert np.array_equal(idx, ref[f"idx_{kind}"])
+    assert np.array_equal(d[idx], ref[f"val_{kind}"])
+    for k in ("vxEl", "vyEl", "vzEl", "vxWMean", "vyWMean", "vzWMean", "uStar", "Fx", "Fy", "Fz"):
+        assert np.array_equal(lst[k], ref[f"out{kind}.{k}"]), k

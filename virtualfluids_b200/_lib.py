@@ -83,6 +83,14 @@ class BcList(ctypes.Structure):
     ]
 
 
+class StressList(ctypes.Structure):
+    """vfb_stress_list (include/vf_b200.h)."""
+
+    _fields_ = [(name, ctypes.c_void_p) for name in (
+        "k", "kN", "q", "normalX", "normalY", "normalZ", "Vx", "Vy", "Vz", "Vx1", "Vy1", "Vz1", "samplingOffset",
+        "z0", "uStar", "Fx", "Fy", "Fz")] + [("numberOfBCnodes", ctypes.c_uint32), ("locations", ctypes.c_void_p)]
+
+
 class ScalingArgs(ctypes.Structure):
     """vfb_scaling_args (include/vf_b200.h)."""
 
@@ -111,7 +119,7 @@ class ScalingArgs(ctypes.Structure):
 
 
 (BC_NOSLIP_INTERPOLATED, BC_NOSLIP_BOUNCE_BACK, BC_VELOCITY_INTERPOLATED, BC_VELOCITY_BOUNCE_BACK, BC_SLIP,
- BC_VELOCITY_WITH_PRESSURE) = range(6)
+ BC_VELOCITY_WITH_PRESSURE, BC_STRESS_INTERPOLATED, BC_STRESS_BOUNCE_BACK, BC_STRESS_BOUNCE_BACK_PRESSURE) = range(9)
 
 # (name, restype, argtypes) of every exported entry point
 _SIGNATURES = [
@@ -140,6 +148,9 @@ _SIGNATURES = [
       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_bc_post", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.POINTER(BcList), ctypes.c_void_p]),
+    ("vfb_bc_stress", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BcLattice), ctypes.POINTER(StressList), ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_bc_locations", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p]),
@@ -163,6 +174,8 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_sim_kinetic_energy", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ("vfb_sim_stress_list", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StressList)]),
+    ("vfb_copy_device_to_host", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("vfb_sim_level_state", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong),
       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),

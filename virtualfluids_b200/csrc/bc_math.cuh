@@ -101,4 +101,64 @@ __device__ __forceinline__ R interpVelocity(R q, R f, R finv, R feq, R omega, R 
            (q * (f + finv) - R(6) * w * vel) / (R(1) + q);
 }
 
+// KernelUtilities.h:199-206 (the interpolated no-slip value minus w drho)
+template <class R>
+__device__ __forceinline__ R interpNoSlipPressure(R q, R f, R finv, R feq, R omega, R drho, R w)
+{
+    return interpNoSlip(q, f, finv, feq, omega) - w * drho;
+}
+
+// The wall model's clip (iMEM.cuh:131-136): -3 F forceFactor formed in
+// double (the reference's literal 3.0 promotes it), bounded by +-clip with
+// the NaN-ignoring double min / max.
+template <class R>
+__device__ __forceinline__ R imemClip(R clip, R F, R forceFactor)
+{
+    const double t = -3.0 * (double)F * (double)forceFactor;
+    return (R)(clip > -clip ? fmin((double)clip, fmax((double)-clip, t)) : fmax((double)clip, fmin((double)-clip, t)));
+}
+
+// one step of a temporal filter, eps v + (1 - eps) mean with the second
+// product in double as the reference writes it (iMEM.cuh:78-90)
+template <class R>
+__device__ __forceinline__ R imemFilter(R eps, R v, R mean)
+{
+    return (R)((double)(eps * v) + (1.0 - (double)eps) * (double)mean);
+}
+
+// The iMEM wall model of one BC entry (iMEM.cuh:57-137, Asmuth et al. 2021):
+// the filtered velocities at the sampling node (el, in/out) and at the wall
+// node (wm, in/out), the friction velocity u* = kappa |u_el,t| / ln(z / z0)
+// at z = samplingOffset + q, the wall shear stress u*^2 along the wall node's
+// tangential velocity over the filtered one's magnitude, minus the tangential
+// momentum the bounce-back exchanged with the wall at rest (mom), and the wall
+// velocity -3 F forceFactor clipped to twice the filtered tangential velocity.
+template <class R>
+__device__ __forceinline__ void imemWallVelocity(const R n[3], R el[3], R wm[3], const R vw[3], R rho, R z, R z0,
+                                                 R forceFactor, const R mom[3], R& uStar, R V[3])
+{
+    const R dEl = el[0] * n[0] + el[1] * n[1] + el[2] * n[2];
+    R t[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        t[a] = el[a] - dEl * n[a];
+    const R magEl = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    const R dWm = wm[0] * n[0] + wm[1] * n[1] + wm[2] * n[2];
+    R tm[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        tm[a] = wm[a] - dWm * n[a];
+    const R magWm = sqrt(tm[0] * tm[0] + tm[1] * tm[1] + tm[2] * tm[2]);
+    const R dW = vw[0] * n[0] + vw[1] * n[1] + vw[2] * n[2];
+    uStar = magEl * R(0.4) / log(z / z0);
+    const R tauW = uStar * uStar;
+    const R dM = mom[0] * n[0] + mom[1] * n[1] + mom[2] * n[2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const R Fw = (tauW * R(1)) * ((vw[a] - dW * n[a]) / magWm);
+        const R F = Fw - (mom[a] - dM * n[a]) / rho;
+        V[a] = imemClip(R(2) * t[a], F, forceFactor);
+    }
+}
+
 } // namespace vfb

@@ -43,3 +43,17 @@ extern "C" int vfb_storage_bytes(int storage)
     default: return 0;
     }
 }
+
+extern "C" int vfb_copy_device_to_host(void* dst, const void* src, size_t bytes, void* stream)
+{
+    vfb::clearError();
+    if (bytes == 0)
+        return VFB_OK;
+    if (!dst || !src)
+        return vfb::setError(VFB_ERR_INVALID_ARGUMENT, "NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        return vfb::setError(VFB_ERR_CUDA, "device to host copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return VFB_OK;
+}

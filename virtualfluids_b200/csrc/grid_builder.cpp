@@ -837,6 +837,7 @@ void GridBuilder::addCoarseGrid(double sx, double sy, double sz, double ex, doub
     grids.emplace_back(new LevelGrid(sx, sy, sz, ex, ey, ez, delta, 0));
     velocity.emplace_back();
     slip.emplace_back();
+    stress.emplace_back();
     pressure.emplace_back();
 }
 
@@ -928,6 +929,7 @@ void GridBuilder::addGrid(const Box& box, int levelFine)
         grids.emplace_back(g);
         velocity.emplace_back();
         slip.emplace_back();
+        stress.emplace_back();
         pressure.emplace_back();
     }
 }
@@ -993,8 +995,14 @@ void GridBuilder::setVelocityGeometryBoundaryCondition(double vx, double vy, dou
     geometryValues = { vx, vy, vz };
 }
 
+// stress sides: the sampling offset (nodes) and the level-0 roughness length and spacing
+struct StressParams {
+    uint32_t samplingOffset = 0;
+    double z0 = 0, dx = 1;
+};
+
 static void addSide(std::vector<std::unique_ptr<LevelGrid>>& grids, std::vector<std::vector<BCList>>& lists,
-                    SideType side, BCKind kind, double v0, double v1, double v2)
+                    SideType side, BCKind kind, double v0, double v1, double v2, const StressParams& sp = {})
 {
     for (size_t level = 0; level < grids.size(); ++level) {
         LevelGrid& g = *grids[level];
@@ -1022,7 +1030,12 @@ static void addSide(std::vector<std::unique_ptr<LevelGrid>>& grids, std::vector<
         const int a2 = axis == 2 ? 1 : 2;      // outer loop axis
         const int64_t n1 = a1 == 0 ? g.nx : g.ny;
         const int64_t n2 = a2 == 1 ? g.ny : g.nz;
-        const uint8_t type = kind == BCKind::Pressure ? BC_PRESSURE : kind == BCKind::Slip ? BC_SLIP : BC_VELOCITY;
+        const uint8_t type = kind == BCKind::Pressure ? BC_PRESSURE
+                             : kind == BCKind::Slip   ? BC_SLIP
+                             : kind == BCKind::Stress ? BC_STRESS
+                                                      : BC_VELOCITY;
+        // StressBoundaryCondition::make(..., z0 * pow(2.0f, level) / dx) (LevelGridBuilder.cpp:135)
+        const double z0Level = sp.z0 * std::ldexp(1.0, (int)level) / sp.dx;
         for (int64_t j2 = 0; j2 < n2; ++j2) {
             for (int64_t j1 = 0; j1 < n1; ++j1) {
                 int64_t c[3];
@@ -1055,10 +1068,22 @@ static void addSide(std::vector<std::unique_ptr<LevelGrid>>& grids, std::vector<
                     bc.vy.push_back(kind == BCKind::NoSlip ? 0.0 : v1);
                     bc.vz.push_back(kind == BCKind::NoSlip ? 0.0 : v2);
                 }
-                if (kind == BCKind::Slip) {
+                if (kind == BCKind::Slip || kind == BCKind::Stress) {
                     bc.normalX.push_back(v0);
                     bc.normalY.push_back(v1);
                     bc.normalZ.push_back(v2);
+                }
+                if (kind == BCKind::Stress) {
+                    // Side::setStressSamplingIndices (Side.cpp:125-145): samplingOffset
+                    // nodes from the BC node against the side's outward direction
+                    int64_t m[3] = { c[0], c[1], c[2] };
+                    m[axis] -= (int64_t)sgn * (int64_t)sp.samplingOffset;
+                    const int64_t at = g.index(m[0], m[1], m[2]);
+                    if (at < 0 || g.sparseIndex[(uint64_t)at] < 0)
+                        throw std::invalid_argument("the stress BC's sampling node lies outside the grid");
+                    bc.kN.push_back((int32_t)(g.sparseIndex[(uint64_t)at] + 1));
+                    bc.samplingOffset.push_back((int32_t)sp.samplingOffset);
+                    bc.z0.push_back(z0Level);
                 }
             }
         }
@@ -1089,6 +1114,13 @@ void GridBuilder::setPressureBoundaryCondition(SideType side, double rho)
 void GridBuilder::setSlipBoundaryCondition(SideType side, double nx, double ny, double nz)
 {
     addSide(grids, slip, side, BCKind::Slip, nx, ny, nz);
+}
+void GridBuilder::setStressBoundaryCondition(SideType side, double nx, double ny, double nz, uint32_t samplingOffset,
+                                             double z0, double dx)
+{
+    if (!(dx > 0) || !(z0 > 0))
+        throw std::invalid_argument("the stress BC needs z0 > 0 and dx > 0");
+    addSide(grids, stress, side, BCKind::Stress, nx, ny, nz, StressParams { samplingOffset, z0, dx });
 }
 
 } // namespace vfb::grid

@@ -47,7 +47,7 @@ enum NodeType : uint8_t {
 
 enum class SideType { MX = 0, PX = 1, MY = 2, PY = 3, MZ = 4, PZ = 5, GEOMETRY = 6 };
 
-enum class BCKind { NoSlip = 1, Velocity = 2, Pressure = 3, Slip = 4 };
+enum class BCKind { NoSlip = 1, Velocity = 2, Pressure = 3, Slip = 4, Stress = 5 };
 
 struct Box {
     double minX, minY, minZ, maxX, maxY, maxZ;
@@ -95,7 +95,9 @@ struct BCList {
     std::vector<double> q;              // 27 * size, -1 = no link
     std::vector<double> vx, vy, vz;     // velocity per node
     std::vector<double> rho;            // pressure per node
-    std::vector<double> normalX, normalY, normalZ; // slip normals per node
+    std::vector<double> normalX, normalY, normalZ; // slip and stress normals per node
+    std::vector<int32_t> samplingOffset; // stress: sampling height in nodes (kN holds the sampling node)
+    std::vector<double> z0;              // stress: roughness length in this level's lattice units
     size_t size() const { return k.size(); }
 };
 
@@ -221,6 +223,12 @@ public:
     void setVelocityBoundaryCondition(SideType side, double vx, double vy, double vz);
     void setPressureBoundaryCondition(SideType side, double rho);
     void setSlipBoundaryCondition(SideType side, double normalX, double normalY, double normalZ);
+    // wall-model BC (LevelGridBuilder::setStressBoundaryCondition, LevelGridBuilder.cpp:129-150):
+    // the side's nodes with their normal, the node samplingOffset layers
+    // further inside as the velocity sampling node, and z0 * 2^level / dx as
+    // the level's roughness length
+    void setStressBoundaryCondition(SideType side, double normalX, double normalY, double normalZ,
+                                    uint32_t samplingOffset, double z0, double dx);
     // no-slip on the solid geometry's BC_SOLID nodes, every level
     void setNoSlipGeometryBoundaryCondition();
     void setVelocityGeometryBoundaryCondition(double vx, double vy, double vz);
@@ -234,6 +242,7 @@ public:
     const std::vector<BCList>& velocityBCs(int level) const { return velocity.at(level); }
     const std::vector<BCList>& slipBCs(int level) const { return slip.at(level); }
     const std::vector<BCList>& pressureBCs(int level) const { return pressure.at(level); }
+    const std::vector<BCList>& stressBCs(int level) const { return stress.at(level); }
     bool hasGeometryBC() const { return geometryNoSlip; }
     // LevelGridBuilder::hasGeometryValues / getGeometryValues: a velocity on the geometry
     bool hasGeometryValues() const { return geometryHasValues; }
@@ -242,7 +251,7 @@ public:
 private:
     std::array<double, 6> staggeredCoordinates(const Box& shape, int level, int levelFine, bool odd[3]) const;
     std::vector<std::unique_ptr<LevelGrid>> grids;
-    std::vector<std::vector<BCList>> velocity, slip, pressure;
+    std::vector<std::vector<BCList>> velocity, slip, pressure, stress;
     uint32_t layersFine = 12, layersBetweenLevels = 8; // MultipleGridBuilder.cpp:53
     bool hasSolid = false;
     Solid solid {};

@@ -1,5 +1,6 @@
 // grid_capi.cpp -- C ABI of the grid builder: build a multi-level sparse grid
 // from a flat description and export the arrays the GPU solver consumes.
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <stdexcept>
@@ -70,7 +71,11 @@ SideType sideOf(int s)
     return (SideType)s;
 }
 
-void applyBC(GridBuilder& b, int side, int type, double v0, double v1, double v2)
+// the stress parameters of side slot i: spec[176 + 3 i .. 178 + 3 i]
+constexpr int kStressBase = 176;
+constexpr int kSpecWithStress = kStressBase + 18;
+
+void applyBC(GridBuilder& b, int side, int type, double v0, double v1, double v2, const double* stress)
 {
     switch (type) {
     case 0: break;
@@ -78,6 +83,13 @@ void applyBC(GridBuilder& b, int side, int type, double v0, double v1, double v2
     case 2: b.setVelocityBoundaryCondition(sideOf(side), v0, v1, v2); break;
     case 3: b.setPressureBoundaryCondition(sideOf(side), v0); break;
     case 4: b.setSlipBoundaryCondition(sideOf(side), v0, v1, v2); break;
+    case 5:
+        if (!stress)
+            throw std::invalid_argument("a stress BC needs the spec's stress block (194 values)");
+        if (!(stress[0] >= 0) || stress[0] != std::floor(stress[0]))
+            throw std::invalid_argument("the stress BC's sampling offset must be a whole number >= 0");
+        b.setStressBoundaryCondition(sideOf(side), v0, v1, v2, (uint32_t)stress[0], stress[1], stress[2]);
+        break;
     default: throw std::invalid_argument("unknown boundary-condition type");
     }
 }
@@ -146,6 +158,20 @@ void exportAll(GridHandle& h)
         E.put("fluid", g.fluidNodes);
         concatenate(b.velocityBCs(level), E, "velocity", true, false);
         concatenate(b.slipBCs(level), E, "slip", false, true);
+        // LevelGridBuilder::getStressValues / getStressQs (LevelGridBuilder.cpp:549-598)
+        concatenate(b.stressBCs(level), E, "stress", false, true);
+        {
+            std::vector<int32_t> kN, off;
+            std::vector<double> z0;
+            for (const auto& l : b.stressBCs(level)) {
+                kN.insert(kN.end(), l.kN.begin(), l.kN.end());
+                off.insert(off.end(), l.samplingOffset.begin(), l.samplingOffset.end());
+                z0.insert(z0.end(), l.z0.begin(), l.z0.end());
+            }
+            E.put("stress.kN", kN);
+            E.put("stress.samplingOffset", off);
+            E.put("stress.z0", z0);
+        }
         std::vector<int32_t> gk;
         std::vector<double> gq;
         if (b.hasGeometryBC())
@@ -207,9 +233,11 @@ extern "C" {
  * ([62] parts added, [63] parts subtracted, 7 values each from [64] on:
  * kind 1..4 and its parameters);
  * [26..29] geometry BC (type 1 = no-slip, 2 = velocity with [27..29]); [30..59] six side BCs (side, type, v0, v1, v2) in the order they
- * are set; [60] enableThinWalls; [61] finest level of the refinement box
- * (0 = 1; n >= 62 values).  Same layout as the grid oracle.  Returns NULL on
- * error (see vfb_last_error).
+ * are set, type 0 none, 1 no-slip, 2 velocity, 3 pressure, 4 slip (v = normal),
+ * 5 stress (v = normal, with [176 + 3 i .. 178 + 3 i] the sampling offset,
+ * z0 and the level-0 dx of side slot i; n >= 194); [60] enableThinWalls; [61]
+ * finest level of the refinement box (0 = 1; n >= 62 values).  Same layout as
+ * the grid oracle.  Returns NULL on error (see vfb_last_error).
  */
 void* vfb_grid_build(const double* s, int n)
 {
@@ -251,7 +279,8 @@ void* vfb_grid_build(const double* s, int n)
         h->builder.buildGrids(s[60] > 0);
         for (int i = 0; i < 6; ++i) {
             const double* b = s + 30 + 5 * i;
-            applyBC(h->builder, (int)b[0], (int)b[1], b[2], b[3], b[4]);
+            applyBC(h->builder, (int)b[0], (int)b[1], b[2], b[3], b[4],
+                    n >= kSpecWithStress ? s + kStressBase + 3 * i : nullptr);
         }
         if (s[19] > 0 && (int)s[26] != 0) {
             if ((int)s[26] == 2)

@@ -111,6 +111,8 @@ int checkSupported(const vfb_simulation& S)
         return setError(VFB_ERR_UNSUPPORTED, "the adjoint covers NoSlipInterpolatedCompressible on the geometry list");
     if (L.slip.n && P.slipBC >= 0)
         return setError(VFB_ERR_UNSUPPORTED, "the adjoint does not cover the slip list");
+    if (L.stress.n && P.stressBC >= 0)
+        return setError(VFB_ERR_UNSUPPORTED, "the adjoint does not cover the stress (wall-model) list");
     size_t np = 0;
     for (const auto* p : L.pressure)
         np += p->n;

@@ -54,12 +54,23 @@ struct PressureListDevice {
     int direction = 0;
 };
 
+// the level's stress list with the wall model's arrays (stressBC and
+// wallModel of the reference's level parameters, CudaMemoryManager.cpp:1139-1200)
+struct StressListDevice {
+    DeviceBuffer k, kN, q, nx, ny, nz, samplingOffset, z0;
+    DeviceBuffer el[3], wm[3];    // filter states Vx/Vy/Vz and Vx1/Vy1/Vz1 (zero at start)
+    DeviceBuffer uStar, F[3];     // monitors (hasWallModelMonitor)
+    DeviceBuffer locations;
+    uint32_t n = 0;
+};
+
 struct Level {
     unsigned long long N = 0;
     uint32_t nFluid = 0;
     DeviceBuffer dist, nX, nY, nZ, geo, fluid;
     DeviceBuffer nNeg; // the -x-y-z neighbour (non-equilibrium init, enstrophy)
     BcListDevice velocity, noSlip, slip, geometry;
+    StressListDevice stress;
     std::vector<PressureListDevice*> pressure;
     InterfaceDevice coarseToFine, fineToCoarse;
     DeviceBuffer energyNodes; // the kinetic-energy analyzer's node set

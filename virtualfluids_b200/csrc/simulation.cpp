@@ -161,6 +161,57 @@ int uploadLevel(Level& L, void* grid, int level, int storage, double geometryVel
         if (const int rc = list("geometry", L.geometry, geometryVelocity, geometryVelocityDivisor))
             return rc;
     }
+    // the stress lists (GridGenerator.cpp:319-341, which keeps a list only
+    // when it has more than one entry) with the wall model's state, zero at start
+    if (e == cudaSuccess && need("stress.k", 4) && count > 1) {
+        StressListDevice& T = L.stress;
+        T.n = (uint32_t)count;
+        keep.push_back(raw);
+        e = uploadRaw(T.k, keep.back().data(), raw.size(), s);
+        if (e == cudaSuccess) {
+            if (!need("stress.kN", 4) || (uint32_t)count != T.n)
+                return fail("stress.kN");
+            keep.push_back(raw);
+            e = uploadRaw(T.kN, keep.back().data(), raw.size(), s);
+        }
+        if (e == cudaSuccess) {
+            if (!need("stress.samplingOffset", 4) || (uint32_t)count != T.n)
+                return fail("stress.samplingOffset");
+            keep.push_back(raw);
+            e = uploadRaw(T.samplingOffset, keep.back().data(), raw.size(), s);
+        }
+        if (e == cudaSuccess) {
+            if (!need("stress.q", 8) || (unsigned long long)count != 27ull * T.n)
+                return fail("stress.q");
+            e = uploadReal(T.q, raw, storage, s, keep);
+        }
+        const char* reals[4] = { "stress.nx", "stress.ny", "stress.nz", "stress.z0" };
+        DeviceBuffer* rb[4] = { &T.nx, &T.ny, &T.nz, &T.z0 };
+        for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+            if (!need(reals[i], 8) || (uint32_t)count != T.n)
+                return fail(reals[i]);
+            e = uploadReal(*rb[i], raw, storage, s, keep);
+        }
+        const size_t rbytes = (size_t)T.n * (computeIsDouble(storage) ? sizeof(double) : sizeof(float));
+        for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+            e = T.el[c].allocate(rbytes);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(T.el[c].ptr, 0, rbytes, s);
+            if (e == cudaSuccess)
+                e = T.wm[c].allocate(rbytes);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(T.wm[c].ptr, 0, rbytes, s);
+        }
+        if (e == cudaSuccess)
+            e = T.locations.allocate(8ull * T.n * sizeof(uint32_t));
+        if (e == cudaSuccess)
+            if (const int rc = vfb_bc_locations(static_cast<const int32_t*>(T.k.ptr), T.n,
+                                                static_cast<const uint32_t*>(L.nX.ptr),
+                                                static_cast<const uint32_t*>(L.nY.ptr),
+                                                static_cast<const uint32_t*>(L.nZ.ptr),
+                                                static_cast<uint32_t*>(T.locations.ptr), s))
+                return rc;
+    }
     if (e == cudaSuccess && need("pressure.count", 4) && count == 1) {
         const int np = *reinterpret_cast<const int32_t*>(raw.data());
         for (int i = 0; i < np && e == cudaSuccess; ++i) {
@@ -294,8 +345,37 @@ int collision(vfb_simulation& S, Level& L, void* stream)
     return k17 ? vfb_k17_collision(S.params.storage, &a, stream) : vfb_bgk_collision(S.params.storage, &a, stream);
 }
 
+vfb_stress_list stressList(StressListDevice& T, bool monitor)
+{
+    vfb_stress_list l;
+    std::memset(&l, 0, sizeof(l));
+    l.k = static_cast<const int32_t*>(T.k.ptr);
+    l.kN = static_cast<const int32_t*>(T.kN.ptr);
+    l.q = T.q.ptr;
+    l.normalX = T.nx.ptr;
+    l.normalY = T.ny.ptr;
+    l.normalZ = T.nz.ptr;
+    l.Vx = T.el[0].ptr;
+    l.Vy = T.el[1].ptr;
+    l.Vz = T.el[2].ptr;
+    l.Vx1 = T.wm[0].ptr;
+    l.Vy1 = T.wm[1].ptr;
+    l.Vz1 = T.wm[2].ptr;
+    l.samplingOffset = static_cast<const int32_t*>(T.samplingOffset.ptr);
+    l.z0 = T.z0.ptr;
+    if (monitor) {
+        l.uStar = T.uStar.ptr;
+        l.Fx = T.F[0].ptr;
+        l.Fy = T.F[1].ptr;
+        l.Fz = T.F[2].ptr;
+    }
+    l.numberOfBCnodes = T.n;
+    l.locations = static_cast<const uint32_t*>(T.locations.ptr);
+    return l;
+}
+
 // UpdateGrid27::postCollisionBC (UpdateGrid27.cpp:228-263): velocity, no-slip,
-// slip, (stress: not built), geometry; every kernel only when its list is not empty
+// slip, stress, geometry; every kernel only when its list is not empty
 int postCollisionBC(vfb_simulation& S, Level& L, void* stream)
 {
     const vfb_bc_lattice t = bcLattice(L);
@@ -307,7 +387,19 @@ int postCollisionBC(vfb_simulation& S, Level& L, void* stream)
                    { &L.noSlip, S.params.noSlipBC },
                    { &L.slip, S.params.slipBC },
                    { &L.geometry, S.params.geometryBC } };
-    for (const Item& it : items) {
+    for (int i = 0; i < 4; ++i) {
+        const Item& it = items[i];
+        if (i == 3 && L.stress.n > 0 && S.params.stressBC >= 0) {
+            // runStressWallModelKernelPost (BoundaryConditionKernelManager.cpp:330-334);
+            // the launchers of Stress.cu:42-160 pass the level's velocityY as vz too
+            if (!L.fields[1].ptr || !L.fields[2].ptr)
+                return setError(VFB_ERR_CONFIGURATION,
+                                "the stress BC reads the level's macroscopic velocity: initialise the level first");
+            const vfb_stress_list l = stressList(L.stress, S.params.hasWallModelMonitor != 0);
+            if (const int rc = vfb_bc_stress(S.params.stressBC, storage, &t, &l, nullptr, L.fields[1].ptr,
+                                             L.fields[2].ptr, L.fields[2].ptr, stream))
+                return rc;
+        }
         if (it.list->n == 0 || it.kind < 0)
             continue;
         const vfb_bc_list l = bcList(*it.list);
@@ -428,7 +520,8 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         !(validKind(P.geometryBC, VFB_BC_NOSLIP_INTERPOLATED, VFB_BC_NOSLIP_BOUNCE_BACK) ||
           P.geometryBC == VFB_BC_VELOCITY_INTERPOLATED || P.geometryBC == VFB_BC_VELOCITY_BOUNCE_BACK ||
           P.geometryBC == VFB_BC_VELOCITY_WITH_PRESSURE) ||
-        !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC >= -1 && P.pressureBC <= 2))
+        !(P.slipBC < 0 || P.slipBC == VFB_BC_SLIP) || !(P.pressureBC >= -1 && P.pressureBC <= 2) ||
+        !validKind(P.stressBC, VFB_BC_STRESS_INTERPOLATED, VFB_BC_STRESS_BOUNCE_BACK_PRESSURE))
         return setError(VFB_ERR_INVALID_ARGUMENT, "invalid boundary-condition selection");
     if (!(P.viscosity > 0.0))
         return setError(VFB_ERR_INVALID_ARGUMENT, "viscosity %g must be positive", P.viscosity);
@@ -444,6 +537,15 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         auto* L = new Level;
         S->levels.push_back(L);
         rc = uploadLevel(*L, grid, l, P.storage, P.velocityRatio > 0.0 ? P.velocityRatio : 1.0, s, keep);
+        if (rc == VFB_OK && P.hasWallModelMonitor && L->stress.n > 0) {
+            // CudaMemoryManager::cudaAllocWallModel with the monitor
+            const size_t rbytes = (size_t)L->stress.n * (computeIsDouble(P.storage) ? sizeof(double) : sizeof(float));
+            DeviceBuffer* mon[4] = { &L->stress.uStar, &L->stress.F[0], &L->stress.F[1], &L->stress.F[2] };
+            for (DeviceBuffer* b : mon)
+                if (rc == VFB_OK &&
+                    (b->allocate(rbytes) != cudaSuccess || cudaMemsetAsync(b->ptr, 0, rbytes, s) != cudaSuccess))
+                    rc = setError(VFB_ERR_CUDA, "wall-model monitor allocation failed");
+        }
         if (rc == VFB_OK && P.geometryBC >= VFB_BC_VELOCITY_INTERPOLATED && L->geometry.n > 0 && !L->geometry.vx.ptr)
             rc = setError(VFB_ERR_CONFIGURATION, "a velocity geometry BC needs the geometry velocities (level %d)", l);
         if (rc == VFB_OK) {
@@ -823,6 +925,18 @@ extern "C" int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* ou
         return rc;
     out2[0] = sums[1] / (double)L->nEnergy;
     out2[1] = (double)L->nEnergy;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_stress_list(vfb_simulation* sim, int level, vfb_stress_list* out)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!out)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = stressList(L->stress, sim->params.hasWallModelMonitor != 0);
     return VFB_OK;
 }
 

@@ -34,14 +34,18 @@ class SideType(enum.IntEnum):
     GEOMETRY = 6
 
 
-_BC_NONE, _BC_NOSLIP, _BC_VELOCITY, _BC_PRESSURE, _BC_SLIP = 0, 1, 2, 3, 4
+_BC_NONE, _BC_NOSLIP, _BC_VELOCITY, _BC_PRESSURE, _BC_SLIP, _BC_STRESS = 0, 1, 2, 3, 4, 5
+# the grid spec's stress block: side slot i holds its sampling offset, z0 and
+# level-0 dx at STRESS_BASE + 3 i
+STRESS_BASE = 176
+SPEC_WITH_STRESS = STRESS_BASE + 18
 
 _REAL_NAMES_PREFIX = ("coord",)
 
 
 def _dtype(name: str, esize: int):
     base = name.split(".")[-1]
-    if name in ("dims", "pressure.count") or base in ("k", "kN", "dir"):
+    if name in ("dims", "pressure.count") or base in ("k", "kN", "dir", "samplingOffset"):
         return np.int32
     if name in ("neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "fluid", "cf.coarse", "cf.fine",
                 "fc.coarse", "fc.fine"):
@@ -52,7 +56,8 @@ def _dtype(name: str, esize: int):
 GRID_ARRAY_NAMES = ["coordX", "coordY", "coordZ", "neighborX", "neighborY", "neighborZ", "neighborNeg", "geo", "dims",
                     "fluid", "velocity.k", "velocity.vx", "velocity.vy", "velocity.vz", "velocity.q", "slip.k",
                     "slip.nx", "slip.ny", "slip.nz", "slip.q", "geometry.k", "geometry.q", "geometry.vx",
-                    "geometry.vy", "geometry.vz", "pressure.count",
+                    "geometry.vy", "geometry.vz", "pressure.count", "stress.k", "stress.kN", "stress.nx",
+                    "stress.ny", "stress.nz", "stress.q", "stress.samplingOffset", "stress.z0",
                     "cf.coarse", "cf.fine", "fc.coarse", "fc.fine", "cf.offX", "cf.offY", "cf.offZ", "fc.offX",
                     "fc.offY", "fc.offZ"]
 
@@ -132,6 +137,7 @@ class MultipleGridBuilder:
         self._coarse = False
         self._built = False
         self._bcs: list[tuple[int, int, float, float, float]] = []
+        self._stress: dict[int, tuple[float, float, float]] = {}  # side slot -> (offset, z0, dx)
 
     # --- grid ---------------------------------------------------------------
     def addCoarseGrid(self, startX, startY, startZ, endX, endY, endZ, delta):
@@ -196,12 +202,29 @@ class MultipleGridBuilder:
     def setSlipBoundaryCondition(self, side, normalX, normalY, normalZ):
         self._add(side, _BC_SLIP, normalX, normalY, normalZ)
 
+    def setStressBoundaryCondition(self, side, normalX, normalY, normalZ, samplingOffset: int, z0, dx):
+        """Wall-model BC on a side (LevelGridBuilder::setStressBoundaryCondition,
+        LevelGridBuilder.cpp:129-150): the wall normal, the velocity sampling
+        node samplingOffset nodes inside, the roughness length z0 and the
+        level-0 spacing dx in the units of z0."""
+        if SideType(side) == SideType.GEOMETRY:
+            raise ValueError("the stress BC is set on a domain side")
+        if int(samplingOffset) != samplingOffset or samplingOffset < 0:
+            raise ValueError("samplingOffset must be a whole number >= 0")
+        self._add(side, _BC_STRESS, normalX, normalY, normalZ)
+        self._stress[len(self._bcs) - 1] = (float(samplingOffset), float(z0), float(dx))
+
     # --- result ---------------------------------------------------------------
     def full_spec(self) -> np.ndarray:
         s = self.spec.copy()
         for i, b in enumerate(self._bcs):
             s[30 + 5 * i: 35 + 5 * i] = b
-        return np.concatenate([s, self._extra])
+        s = np.concatenate([s, self._extra])
+        if self._stress:
+            s = np.concatenate([s, np.zeros(max(0, SPEC_WITH_STRESS - len(s)))])
+            for i, v in self._stress.items():
+                s[STRESS_BASE + 3 * i: STRESS_BASE + 3 * i + 3] = v
+        return s
 
     def arrays(self) -> list[dict[str, np.ndarray]]:
         """Run the native builder and return the arrays of every level."""

@@ -280,6 +280,31 @@ def bc_post(kind: int, dist, lat: DeviceLattice, k, q, omega: float, is_even: bo
                                       _stream(stream)))
 
 
+STRESS_ARRAYS = ("k", "kN", "q", "normalX", "normalY", "normalZ", "Vx", "Vy", "Vz", "Vx1", "Vy1", "Vz1",
+                 "samplingOffset", "z0")
+STRESS_MONITORS = ("uStar", "Fx", "Fy", "Fz")
+
+
+def bc_stress(kind: int, dist, lat: DeviceLattice, lst: dict, omega: float, is_even: bool, vx, vy, vz,
+              turbulent_viscosity=None, stream=None) -> None:
+    """One wall-model (stress) BC kernel (``kind`` one of _lib.BC_STRESS_*)
+    over a stress list: ``lst`` maps the vfb_stress_list names (k, kN, q,
+    normalX.., Vx.. / Vx1.. the two filter states, samplingOffset, z0 and,
+    for the monitor, uStar, Fx, Fy, Fz; optionally locations) to device
+    tensors; ``vx``/``vy``/``vz`` are the level's macroscopic velocity."""
+    s = _lib.StressList()
+    for name in STRESS_ARRAYS:
+        setattr(s, name, lst[name].data_ptr())
+    for name in STRESS_MONITORS:
+        setattr(s, name, _p(lst.get(name)))
+    s.locations = _p(lst.get("locations"))
+    s.numberOfBCnodes = int(lst["k"].numel())
+    t = _bc_lattice(dist, lat, omega, is_even)
+    _lib.check(_lib.lib().vfb_bc_stress(int(kind), STORAGE_OF_DTYPE[dist.dtype], ctypes.byref(t), ctypes.byref(s),
+                                        _p(turbulent_viscosity), vx.data_ptr(), vy.data_ptr(), vz.data_ptr(),
+                                        _stream(stream)))
+
+
 def bc_outflow(dist, lat: DeviceLattice, k, kN, direction: int, is_even: bool, pressure_correction: bool = False,
                correction_factor: float = 0.0, stream=None) -> None:
     """The non-reflecting outflow (OutflowNonReflecting, or with

@@ -37,6 +37,8 @@ class VfbSimParams(ctypes.Structure):
         ("useInitNeq", ctypes.c_int),
         ("outflowPressureCorrectionFactor", ctypes.c_double),
         ("velocityRatio", ctypes.c_double),
+        ("stressBC", ctypes.c_int),
+        ("hasWallModelMonitor", ctypes.c_int),
     ]
 
 
@@ -57,6 +59,13 @@ class SlipBC(enum.IntEnum):
     SlipCompressible = _lib.BC_SLIP
 
 
+class StressBC(enum.IntEnum):
+    NotSpecified = -1
+    StressCompressible = _lib.BC_STRESS_INTERPOLATED
+    StressBounceBackCompressible = _lib.BC_STRESS_BOUNCE_BACK
+    StressBounceBackPressureCompressible = _lib.BC_STRESS_BOUNCE_BACK_PRESSURE
+
+
 class PressureBC(enum.IntEnum):
     NotSpecified = -1
     PressureNonEquilibriumCompressible = 0
@@ -75,6 +84,7 @@ class BoundaryConditionFactory:
         self.no_slip = NoSlipBC.NoSlipDelayBounceBack
         self.geometry = NoSlipBC.NoSlipDelayBounceBack
         self.slip = SlipBC.NotSpecified
+        self.stress = StressBC.NotSpecified
         self.pressure = PressureBC.NotSpecified
 
     def set_velocity_boundary_condition(self, boundary_condition_type: VelocityBC):
@@ -99,6 +109,9 @@ class BoundaryConditionFactory:
     def set_slip_boundary_condition(self, boundary_condition_type: SlipBC):
         self.slip = SlipBC(boundary_condition_type)
 
+    def set_stress_boundary_condition(self, boundary_condition_type: StressBC):
+        self.stress = StressBC(boundary_condition_type)
+
     def set_pressure_boundary_condition(self, boundary_condition_type: PressureBC):
         self.pressure = PressureBC(boundary_condition_type)
 
@@ -121,6 +134,7 @@ class Parameter:
         # world-to-lattice velocity ratio; only the geometry list's velocities
         # are divided by it (GridGenerator.cpp:507-513)
         self.velocity_ratio = 1.0
+        self.has_wall_model_monitor = False
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -163,6 +177,12 @@ class Parameter:
         if not velocity_ratio > 0.0:
             raise ValueError("velocity ratio must be positive")
         self.velocity_ratio = float(velocity_ratio)
+
+    def set_has_wall_model_monitor(self, has_wall_model_monitor: bool):
+        """The stress kernels write u* and the wall momentum per entry
+        (Parameter::setHasWallModelMonitor); read them with
+        Simulation.wall_model()."""
+        self.has_wall_model_monitor = bool(has_wall_model_monitor)
 
     def set_initial_condition(self, init_func):
         """init_func(x, y, z) -> (drho, vx, vy, vz), evaluated on numpy arrays of coordinates."""
@@ -246,6 +266,8 @@ class Simulation:
         p.useInitNeq = int(bool(parameter.use_init_neq))
         p.outflowPressureCorrectionFactor = parameter.outflow_pressure_correction_factor
         p.velocityRatio = parameter.velocity_ratio
+        p.stressBC = int(bcFactory.stress)
+        p.hasWallModelMonitor = int(bool(parameter.has_wall_model_monitor))
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
@@ -369,6 +391,28 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_adjoint_backward(self._h, float(seed), dv.ctypes.data, df.ctypes.data,
                                                        self.stream))
         return dv, df
+
+    def wall_model(self, level: int = 0) -> dict[str, np.ndarray]:
+        """The level's stress list and wall-model arrays as host copies: the
+        filter states Vx, Vy, Vz (sampling node) and Vx1, Vy1, Vz1 (wall
+        node) and, with the monitor, uStar, Fx, Fy, Fz; empty when the level
+        has no stress list."""
+        L = _lib.lib()
+        lst = _lib.StressList()
+        _lib.check(L.vfb_sim_stress_list(self._h, level, ctypes.byref(lst)))
+        n = int(lst.numberOfBCnodes)
+        out = {}
+        if n == 0:
+            return out
+        names = ["Vx", "Vy", "Vz", "Vx1", "Vy1", "Vz1", "uStar", "Fx", "Fy", "Fz"]
+        for name in names:
+            ptr = getattr(lst, name)
+            if not ptr:
+                continue
+            a = np.zeros(n, self.real)
+            _lib.check(L.vfb_copy_device_to_host(a.ctypes.data, ptr, a.nbytes, self.stream))
+            out[name] = a
+        return out
 
     def level_state(self, level: int = 0):
         """(device pointer of the populations, N, isEvenTimestep, omega)."""
