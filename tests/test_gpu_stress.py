@@ -32,7 +32,8 @@ def _grid(name):
 
 
 def _state(g, seed=3):
-    """FP64 populations near equilibrium with a non-equilibrium part."""
+    """FP64 populations near equilibrium with a non-equilibrium part of up to
+    5% of each weight (inside FX16's range of a quarter of the weight)."""
     O = Oracle("f64")
     N = len(g["geo"])
     rng = np.random.default_rng(seed)
@@ -41,7 +42,8 @@ def _state(g, seed=3):
     u = [rng.uniform(-2e-2, 2e-2, N) for _ in range(3)]
     for ev in (0, 1):
         O.init_eq(d, N, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"], rho, *u, ev)
-    d += rng.uniform(-1e-3, 1e-3, d.shape) * (d != 0)
+    w = np.repeat(np.asarray(K.WEIGHTS, float), N)
+    d += rng.uniform(-0.05, 0.05, d.shape) * w * (d != 0)
     return d
 
 
@@ -256,7 +258,10 @@ def test_abl_schedule_with_stress_matches_oracle(cuda, kind, storage):
                     is_even=even)
         even = not even
     want = O.macroscopic(d, N, geo, nx, ny, nz, even)
-    tol = 1e-11 if storage == "fp64" else 1e-5
+    # FP32: drho is of order 1e-4 here, and the GPU's FP32 arithmetic
+    # (contracted multiply-adds, logf) rounds along other paths than the
+    # oracle's; 1e-4 L2 on every field
+    tol = 1e-11 if storage == "fp64" else 1e-4
     for a, w in zip(got, want):
         assert (rel_max if storage == "fp64" else rel_l2)(a[fl], w[fl]) < tol
     for abi, name in [("Vx", "vxEl"), ("Vy", "vyEl"), ("Vz", "vzEl"), ("Vx1", "vxWMean"), ("Vy1", "vyWMean"),

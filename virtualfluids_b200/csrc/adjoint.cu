@@ -26,6 +26,8 @@
 //   out_d = fN_d + w_d (rho_BC - drho_N) (1 + 3 c_d.u + 9/2 (c_d.u)^2 - 3/2 |u|^2).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "adjoint.cuh"
 #include "adjoint_ops.gen.cuh"
 #include "capi_common.cuh"
@@ -38,6 +40,9 @@ namespace adjoint
 namespace
 {
 constexpr int kThreads = 128;
+// resident blocks per SM of the collision adjoint (see collisionAdjointKernel)
+constexpr int kAdjointBlocksFP32 = 3;
+constexpr int kAdjointBlocksFP64 = 2;
 
 unsigned blocksFor(uint32_t n) { return (n + kThreads - 1) / kThreads; }
 
@@ -66,18 +71,34 @@ __device__ __forceinline__ double blockSum(double v)
     return s;
 }
 
+// the eight locations of fluid-list entry i: from the list's location table
+// (eight independent loads) when there is one, else through the neighbour arrays
+__device__ __forceinline__ Locs fluidLocations(const uint32_t* __restrict__ table, uint32_t i, uint32_t n,
+                                               const uint32_t* __restrict__ fluid, const uint32_t* __restrict__ nX,
+                                               const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ)
+{
+    if (table) {
+        Locs L;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+            L.k[l] = __ldg(table + (unsigned long long)l * n + i);
+        return L;
+    }
+    return listIndices(__ldg(fluid + i), nX, nY, nZ);
+}
+
 // ------------------------------------------------------------- collision --
 template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
     tapeCollisionKernel(R* __restrict__ dist, unsigned long long N, const uint32_t* __restrict__ nX,
                         const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ,
-                        const uint32_t* __restrict__ fluid, uint32_t n, const K17Rates<R> r, R fx, R fy, R fz,
-                        R* __restrict__ tape)
+                        const uint32_t* __restrict__ fluid, const uint32_t* __restrict__ table, uint32_t n,
+                        const K17Rates<R> r, R fx, R fy, R fz, R* __restrict__ tape)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const Locs L = listIndices(__ldg(fluid + i), nX, nY, nZ);
+    const Locs L = fluidLocations(table, i, n, fluid, nX, nY, nZ);
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -94,17 +115,21 @@ __global__ void __launch_bounds__(kThreads)
         dist[cell<R>(slot<EVEN>(d), N, L.k[loc(d)])] = f[inv(d)];
 }
 
-template <class R, bool EVEN>
-__global__ void __launch_bounds__(kThreads)
+// MINB: resident blocks per SM the register allocation aims at (the reverse
+// sweep wants more than 128 registers a thread; fewer registers spill to
+// local memory but hide more latency)
+template <class R, bool EVEN, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     collisionAdjointKernel(R* __restrict__ lam, unsigned long long N, const uint32_t* __restrict__ nX,
                            const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ,
-                           const uint32_t* __restrict__ fluid, uint32_t n, const K17Rates<R> r, R fx, R fy, R fz,
-                           const R* __restrict__ tape, double* __restrict__ partials)
+                           const uint32_t* __restrict__ fluid, const uint32_t* __restrict__ table, uint32_t n,
+                           const K17Rates<R> r, R fx, R fy, R fz, const R* __restrict__ tape,
+                           double* __restrict__ partials)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double gx = 0.0, gy = 0.0, gz = 0.0;
     if (i < n) {
-        const Locs L = listIndices(__ldg(fluid + i), nX, nY, nZ);
+        const Locs L = fluidLocations(table, i, n, fluid, nX, nY, nZ);
         R a[27], l[27];
 #pragma unroll
         for (int d = 0; d < 27; ++d)
@@ -482,35 +507,65 @@ unsigned objectiveBlocks(uint32_t n) { return blocksFor(n); }
 
 template <class R>
 int collision(R* dist, unsigned long long N, const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
-              const uint32_t* fluid, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz, bool even, R* tape,
-              cudaStream_t s)
+              const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz,
+              bool even, R* tape, cudaStream_t s)
 {
     if (nFluid == 0)
         return VFB_OK;
     const unsigned b = blocksFor(nFluid);
     if (even)
-        tapeCollisionKernel<R, true><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, nFluid, rates, fx, fy, fz,
-                                                            tape);
+        tapeCollisionKernel<R, true><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy,
+                                                            fz, tape);
     else
-        tapeCollisionKernel<R, false><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, nFluid, rates, fx, fy, fz,
-                                                             tape);
+        tapeCollisionKernel<R, false><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy,
+                                                             fz, tape);
     return checkLaunch("adjoint forward collision");
+}
+
+template <class R, int MINB>
+void launchCollisionAdjoint(bool even, unsigned b, cudaStream_t s, R* lam, unsigned long long N, const uint32_t* nX,
+                            const uint32_t* nY, const uint32_t* nZ, const uint32_t* fluid, const uint32_t* loc,
+                            uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz, const R* tape,
+                            double* partials)
+{
+    if (even)
+        collisionAdjointKernel<R, true, MINB><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, loc, nFluid, rates,
+                                                                     fx, fy, fz, tape, partials);
+    else
+        collisionAdjointKernel<R, false, MINB><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, loc, nFluid, rates,
+                                                                      fx, fy, fz, tape, partials);
+}
+
+static int collisionAdjointOccupancy(bool dbl)
+{
+    // measured defaults (FP32: 3 blocks of 128 threads per SM; FP64: 2); the
+    // environment variable VFB_ADJOINT_BLOCKS (2, 3 or 4) overrides them for tuning
+    static const int env = [] {
+        const char* e = std::getenv("VFB_ADJOINT_BLOCKS");
+        const int v = e ? std::atoi(e) : 0;
+        return v >= 2 && v <= 4 ? v : 0;
+    }();
+    if (env)
+        return env;
+    return dbl ? kAdjointBlocksFP64 : kAdjointBlocksFP32;
 }
 
 template <class R>
 int collisionAdjoint(R* lam, unsigned long long N, const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
-                     const uint32_t* fluid, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz, bool even,
-                     const R* tape, double* partials, cudaStream_t s)
+                     const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx,
+                     R fy, R fz, bool even, const R* tape, double* partials, cudaStream_t s)
 {
     if (nFluid == 0)
         return VFB_OK;
     const unsigned b = blocksFor(nFluid);
-    if (even)
-        collisionAdjointKernel<R, true><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, nFluid, rates, fx, fy, fz,
-                                                               tape, partials);
-    else
-        collisionAdjointKernel<R, false><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, nFluid, rates, fx, fy, fz,
-                                                                tape, partials);
+    switch (collisionAdjointOccupancy(sizeof(R) == 8)) {
+    case 2: launchCollisionAdjoint<R, 2>(even, b, s, lam, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy, fz, tape,
+                                         partials); break;
+    case 3: launchCollisionAdjoint<R, 3>(even, b, s, lam, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy, fz, tape,
+                                         partials); break;
+    default: launchCollisionAdjoint<R, 4>(even, b, s, lam, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy, fz, tape,
+                                          partials); break;
+    }
     return checkLaunch("collision adjoint");
 }
 
@@ -643,10 +698,11 @@ int reducePartials(const double* partials, unsigned blocks, int width, double* a
 
 #define VFB_ADJOINT_INSTANTIATE(R)                                                                                    \
     template int collision<R>(R*, unsigned long long, const uint32_t*, const uint32_t*, const uint32_t*,             \
-                              const uint32_t*, uint32_t, const K17Rates<R>&, R, R, R, bool, R*, cudaStream_t);        \
+                              const uint32_t*, const uint32_t*, uint32_t, const K17Rates<R>&, R, R, R, bool, R*,     \
+                              cudaStream_t);                                                                           \
     template int collisionAdjoint<R>(R*, unsigned long long, const uint32_t*, const uint32_t*, const uint32_t*,      \
-                                     const uint32_t*, uint32_t, const K17Rates<R>&, R, R, R, bool, const R*, double*, \
-                                     cudaStream_t);                                                                    \
+                                     const uint32_t*, const uint32_t*, uint32_t, const K17Rates<R>&, R, R, R, bool,   \
+                                     const R*, double*, cudaStream_t);                                                 \
     template int postBC<R>(int, R*, const BcLattice<R>&, const int32_t*, const R*, uint32_t, const R*, const R*,      \
                            const R*, bool, R*, cudaStream_t);                                                          \
     template int postBCAdjoint<R>(int, R*, const BcLattice<R>&, const int32_t*, const R*, uint32_t, const R*,         \

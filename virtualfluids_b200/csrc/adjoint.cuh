@@ -42,18 +42,19 @@ namespace adjoint
 // blocks of the collision adjoint (its block partial sums of the force adjoint)
 unsigned collisionBlocks(uint32_t nFluid);
 
-// forward K17 collision over the fluid list; tape may be null
+// forward K17 collision over the fluid list; tape may be null; loc is the
+// fluid list's location table (8 * nFluid, vfb_bc_locations layout) or null
 template <class R>
 int collision(R* dist, unsigned long long N, const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
-              const uint32_t* fluid, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz, bool even, R* tape,
-              cudaStream_t s);
+              const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz,
+              bool even, R* tape, cudaStream_t s);
 
 // adjoint of the collision: lam in place; partials[3 * b + c] receive the
 // block sums of the adjoint of the half force (fx, fy, fz)
 template <class R>
 int collisionAdjoint(R* lam, unsigned long long N, const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
-                     const uint32_t* fluid, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz, bool even,
-                     const R* tape, double* partials, cudaStream_t s);
+                     const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx,
+                     R fy, R fz, bool even, const R* tape, double* partials, cudaStream_t s);
 
 // forward post-collision BC (kind VFB_BC_VELOCITY_INTERPOLATED or
 // VFB_BC_NOSLIP_INTERPOLATED); rec may be null

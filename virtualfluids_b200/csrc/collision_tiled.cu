@@ -68,8 +68,10 @@ cudaError_t upload(T** dst, const std::vector<T>& v, cudaStream_t stream)
 
 // Tile configurations (tile width, stages, resident blocks) the library is
 // compiled for; 0 stages selects the direct-load kernel, 1 stage the paired
-// direct-load kernel.  Entry 12 (paired) is the default for FP32, FP16 and
-// BF16, entry 1 for FP64 (the fastest at Taylor-Green 512^3 on B200);
+// direct-load kernel.  Entry 12 (paired, four blocks per SM) is the default
+// for FP32, entry 19 (paired, five blocks) for the 16-bit storages and entry 1
+// for FP64 (the fastest at Taylor-Green 512^3 on B200: FP16 / FX16 33.5 G node
+// updates per second with entry 19 against 32.5 / 31.8 with entry 12);
 // VFB_TILE_CONFIG=<index> selects another one at plan creation (used to tune
 // the shape on new hardware).
 struct TileConfigInfo {
@@ -95,7 +97,7 @@ static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTile
 static int chooseTileConfig(int storage)
 {
     const bool fp64 = storage == VFB_FP64;
-    int def = fp64 ? 1 : 12;
+    int def = fp64 ? 1 : storage == VFB_FP32 ? 12 : 19;
     if (const char* env = std::getenv("VFB_TILE_CONFIG")) {
         const int c = std::atoi(env);
         if (c >= 0 && c < kNumTileConfigs && kTileConfigs[c].fp64 == fp64)

@@ -46,6 +46,7 @@ struct AdjointState {
     std::vector<size_t> pressureOffset; // first entry of each pressure list in recPressure / tmpPressure
     size_t pressureTotal = 0;
     DeviceBuffer objNodes, objW[3], partials, accForce, gVelocity;
+    DeviceBuffer fluidLocations; // 8 * nFluid: the fluid list's node locations (vfb_bc_locations)
     uint32_t nObj = 0;
     int velocityKind = -1, noSlipKind = -1, geometryKind = -1;
     bool pressure = false;
@@ -155,8 +156,9 @@ struct Stepper {
     // slot >= 0 the step's inputs are recorded in that slot of the tapes
     int forward(R* dist, bool& even, int slot)
     {
-        if (const int rc = adjoint::collision<R>(dist, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid), L.nFluid,
-                                                 rates, fx, fy, fz, even, slotOf(A.tape, slot, L.nFluid), s))
+        if (const int rc = adjoint::collision<R>(dist, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
+                                                 as<const uint32_t>(A.fluidLocations), L.nFluid, rates, fx, fy, fz,
+                                                 even, slotOf(A.tape, slot, L.nFluid), s))
             return rc;
         BcLattice<R> t = lat;
         struct Item {
@@ -226,7 +228,8 @@ struct Stepper {
                 return rc;
         }
         if (const int rc = adjoint::collisionAdjoint<R>(lam, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
-                                                        L.nFluid, rates, fx, fy, fz, even,
+                                                        as<const uint32_t>(A.fluidLocations), L.nFluid, rates, fx,
+                                                        fy, fz, even,
                                                         slotOf(A.tape, slot, L.nFluid), as<double>(A.partials), s))
             return rc;
         return adjoint::reducePartials(as<double>(A.partials), adjoint::collisionBlocks(L.nFluid), 3,
@@ -275,6 +278,16 @@ int adjointForward(vfb_simulation& S, AdjointState& A, unsigned steps, double* J
     for (unsigned c = 0; c < segments; ++c)
         if (ensure(*A.checkpoints[c], stateBytes) != cudaSuccess)
             return cudaFail("checkpoint allocation");
+    // the fluid list's location table, once (the collision kernels of both
+    // passes read it instead of walking the neighbour arrays)
+    if (!A.fluidLocations.ptr && L.nFluid) {
+        if (ensure(A.fluidLocations, 8ull * L.nFluid * sizeof(uint32_t)) != cudaSuccess)
+            return cudaFail("fluid location table");
+        if (const int rc = vfb_bc_locations(as<const int32_t>(L.fluid), L.nFluid, as<const uint32_t>(L.nX),
+                                            as<const uint32_t>(L.nY), as<const uint32_t>(L.nZ),
+                                            as<uint32_t>(A.fluidLocations), s))
+            return rc;
+    }
     Stepper<R> st(S, A, s);
     R* dist = as<R>(L.dist);
     bool even = L.isEven;

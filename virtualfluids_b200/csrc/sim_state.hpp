@@ -115,6 +115,10 @@ struct vfb_simulation {
     cudaStream_t captureStream = nullptr;
     std::map<unsigned long long, cudaGraphExec_t> graphs;
     unsigned long long stepsRun = 0;
+    // level l > 0 runs its two substeps on side[l - 1] beside level l - 1's own
+    // step (fork / join events per level; see updateGrid in simulation.cpp)
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> fork, join;
     // the adjoint's checkpoints, tapes and gradients (vfb_sim_adjoint_*)
     vfb::AdjointState* adjoint = nullptr;
     ~vfb_simulation()
@@ -124,6 +128,12 @@ struct vfb_simulation {
             cudaGraphExecDestroy(g.second);
         if (captureStream)
             cudaStreamDestroy(captureStream);
+        for (cudaStream_t s : side)
+            cudaStreamDestroy(s);
+        for (cudaEvent_t e : fork)
+            cudaEventDestroy(e);
+        for (cudaEvent_t e : join)
+            cudaEventDestroy(e);
         for (auto* l : levels)
             delete l;
     }

@@ -472,27 +472,47 @@ int refinement(vfb_simulation& S, Level& C, Level& F, void* stream)
     return VFB_OK;
 }
 
-// UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-96)
+// UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-96).  The reference runs the
+// finer level's two substeps, then this level's collision, BCs and parity
+// swap, then fine-to-coarse and coarse-to-fine.  The finer level's substeps
+// touch only the finer level's arrays and this level's step only this
+// level's, and both read what the previous refinement wrote, so they run
+// side by side here: the substeps on this level's side stream, forked from
+// and joined back into the level's stream before the refinement.  Every
+// array sees the reference's sequence of writes, so the result is the same;
+// the short BC and interface launches of one level overlap the other's work.
 int updateGrid(vfb_simulation& S, int level, void* stream)
 {
     const int finest = (int)S.levels.size() - 1;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = VFB_OK;
     if (level != finest) {
-        if (const int rc = updateGrid(S, level + 1, stream))
-            return rc;
-        if (const int rc = updateGrid(S, level + 1, stream))
-            return rc;
+        cudaStream_t side = S.side[level];
+        if (cudaEventRecord(S.fork[level], s) != cudaSuccess || cudaStreamWaitEvent(side, S.fork[level], 0) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "level fork: %s", cudaGetErrorString(cudaGetLastError()));
+        rc = updateGrid(S, level + 1, side);
+        if (rc == VFB_OK)
+            rc = updateGrid(S, level + 1, side);
+        // joined below in every case, so that no side stream is left forked
+        if (cudaEventRecord(S.join[level], side) != cudaSuccess && rc == VFB_OK)
+            rc = setError(VFB_ERR_CUDA, "level join: %s", cudaGetErrorString(cudaGetLastError()));
     }
     Level& L = *S.levels[level];
-    if (const int rc = collision(S, L, stream))
+    if (rc == VFB_OK)
+        rc = collision(S, L, stream);
+    if (rc == VFB_OK)
+        rc = postCollisionBC(S, L, stream);
+    if (rc == VFB_OK) {
+        L.isEven = !L.isEven; // swapBetweenEvenAndOddTimestep (:265-269)
+        rc = preCollisionBC(S, L, stream);
+    }
+    if (level == finest)
         return rc;
-    if (const int rc = postCollisionBC(S, L, stream))
+    if (cudaStreamWaitEvent(s, S.join[level], 0) != cudaSuccess && rc == VFB_OK)
+        rc = setError(VFB_ERR_CUDA, "level join: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rc != VFB_OK)
         return rc;
-    L.isEven = !L.isEven; // swapBetweenEvenAndOddTimestep (:265-269)
-    if (const int rc = preCollisionBC(S, L, stream))
-        return rc;
-    if (level != finest)
-        return refinement(S, L, *S.levels[level + 1], stream);
-    return VFB_OK;
+    return refinement(S, L, *S.levels[level + 1], stream);
 }
 
 bool validKind(int k, int lo, int hi) { return k < 0 || (k >= lo && k <= hi); }
@@ -566,6 +586,21 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         const double nu = P.viscosity * std::pow(2.0, l);
         L->omega = 1.0 / (3.0 * nu + 0.5);
         L->forceFactor = 1.0 / std::pow(2.0, l);
+    }
+    // a side stream and fork / join events per level with a finer level
+    for (int l = 0; l + 1 < nLevels && rc == VFB_OK; ++l) {
+        cudaStream_t side = nullptr;
+        cudaEvent_t f = nullptr, j = nullptr;
+        if (cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess)
+            rc = setError(VFB_ERR_CUDA, "level streams: %s", cudaGetErrorString(cudaGetLastError()));
+        if (side)
+            S->side.push_back(side);
+        if (f)
+            S->fork.push_back(f);
+        if (j)
+            S->join.push_back(j);
     }
     // the kinetic-energy analyzer's node set of every level (KineticEnergyAnalyzer.cu:137-154)
     for (int l = 0; l < nLevels && rc == VFB_OK; ++l) {
