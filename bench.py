@@ -679,7 +679,7 @@ def cube_report(args):
     the library's builder, stepped by the C++ schedule with graph replay.
     Per storage: NUPS as the reference counts them (steps x sum over levels
     of nodes x 2^level / s, PerformanceMeasurement.cpp:43,63) and fluid-node
-    updates per second; for FP32 / FP16 / BF16 the L2 velocity error and the
+    updates per second; for FP32 / FP16 / BF16 / FX16 the L2 velocity error and the
     kinetic-energy error against the FP64 run after --steps coarse steps
     (both levels).  One JSON line."""
     import numpy as np
@@ -698,7 +698,7 @@ def cube_report(args):
     per_step_nodes = sum(n * 2 ** lvl for lvl, n in enumerate(nodes))
     per_step_fluid = sum(n * 2 ** lvl for lvl, n in enumerate(fluid))
     rows, ref = {}, None
-    for storage in ("fp64", "fp32", "fp16", "bf16"):
+    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16"):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(nu)
@@ -739,7 +739,7 @@ def cube_report(args):
             row["kinetic_energy_error_vs_fp64"] = [abs(f[3] - r[3]) / abs(r[3]) if r[3] != 0 else None
                                                    for f, r in zip(fields, ref)]
         rows[storage] = row
-    for s16 in ("fp16", "bf16"):
+    for s16 in ("fp16", "bf16", "fx16"):
         rows[f"{s16}_over_fp32_nups"] = rows[s16]["nups"] / rows["fp32"]["nups"]
     print(json.dumps({"report": "wall-mounted cube, two levels", "workload":
                       "cube channel 256x96x96 + refined box 48..128 x 24..72 x 0..40, cube 16 at x=64, K17",

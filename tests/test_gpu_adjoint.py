@@ -112,8 +112,10 @@ def test_flow_objective_autograd_function(cuda):
     (2.0 * J).backward()
     pb.evaluate(inlet_profile(g), G)
     dv, df = pb.gradient(2.0)
-    assert np.allclose(prof.grad.numpy(), dv, rtol=1e-12, atol=0)
-    assert np.allclose(force.grad.numpy(), df, rtol=1e-12, atol=0)
+    # equal to 1e-12 of each gradient's largest entry: the BC scatters add with
+    # atomics, whose order may change the last bits of entries that cancel
+    assert np.allclose(prof.grad.numpy(), dv, rtol=0, atol=1e-12 * np.abs(dv).max())
+    assert np.allclose(force.grad.numpy(), df, rtol=0, atol=1e-12 * np.abs(df).max())
     assert float(J2) != float(J)
     sim.close()
 
