@@ -87,6 +87,22 @@ __device__ __forceinline__ Locs fluidLocations(const uint32_t* __restrict__ tabl
     return listIndices(__ldg(fluid + i), nX, nY, nZ);
 }
 
+// the eight locations of BC entry i: from the list's location table when it
+// has one, else through the neighbour arrays
+__device__ __forceinline__ Locs bcEntryLocations(const uint32_t* __restrict__ table, uint32_t i, uint32_t n,
+                                                 const int32_t* __restrict__ bcK, const uint32_t* __restrict__ nX,
+                                                 const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ)
+{
+    if (table) {
+        Locs L;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+            L.k[l] = __ldg(table + (unsigned long long)l * n + i);
+        return L;
+    }
+    return listIndices((uint32_t)__ldg(bcK + i), nX, nY, nZ);
+}
+
 // ------------------------------------------------------------- collision --
 template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
@@ -149,10 +165,11 @@ __global__ void __launch_bounds__(kThreads, MINB)
     gx = blockSum(gx);
     gy = blockSum(gy);
     gz = blockSum(gz);
+    // accumulated over the steps of a backward pass, each block in step order
     if (threadIdx.x == 0) {
-        partials[3 * blockIdx.x + 0] = gx;
-        partials[3 * blockIdx.x + 1] = gy;
-        partials[3 * blockIdx.x + 2] = gz;
+        partials[3 * blockIdx.x + 0] += gx;
+        partials[3 * blockIdx.x + 1] += gy;
+        partials[3 * blockIdx.x + 2] += gz;
     }
 }
 
@@ -160,6 +177,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 template <class R, int KIND, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
     postBCKernel(R* __restrict__ dist, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+                 const uint32_t* __restrict__ table,
                  const R* __restrict__ q, uint32_t n, const R* __restrict__ Vx, const R* __restrict__ Vy,
                  const R* __restrict__ Vz, R* __restrict__ rec)
 {
@@ -167,7 +185,7 @@ __global__ void __launch_bounds__(kThreads)
     if (i >= n)
         return;
     const unsigned long long N = lat.N;
-    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     R g[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -210,12 +228,13 @@ __global__ void __launch_bounds__(kThreads)
 template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
     postGatherKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+                 const uint32_t* __restrict__ table,
                      const R* __restrict__ q, uint32_t n, R* __restrict__ tmp)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     // all q values first: loads issued together, not one per loop iteration
     R qv[26];
 #pragma unroll
@@ -237,13 +256,14 @@ __global__ void __launch_bounds__(kThreads)
 template <class R, int KIND, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
     postScatterKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+                 const uint32_t* __restrict__ table,
                       const R* __restrict__ q, uint32_t n, const R* __restrict__ rec, const R* __restrict__ tmp,
                       double* __restrict__ gV)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+    const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     R g[27], gg[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
@@ -569,36 +589,41 @@ int collisionAdjoint(R* lam, unsigned long long N, const uint32_t* nX, const uin
     return checkLaunch("collision adjoint");
 }
 
+template <class R, int KIND, bool EVEN>
+void launchPostBC(unsigned b, cudaStream_t s, R* dist, const BcLattice<R>& lat, const int32_t* k,
+                  const uint32_t* table, const R* q, uint32_t n, const R* Vx, const R* Vy, const R* Vz, R* rec)
+{
+    postBCKernel<R, KIND, EVEN><<<b, kThreads, 0, s>>>(dist, lat, k, table, q, n, Vx, Vy, Vz, rec);
+}
+
 template <class R>
-int postBC(int kind, R* dist, const BcLattice<R>& lat, const int32_t* k, const R* q, uint32_t n, const R* Vx,
-           const R* Vy, const R* Vz, bool even, R* rec, cudaStream_t s)
+int postBC(int kind, R* dist, const BcLattice<R>& lat, const int32_t* k, const uint32_t* table, const R* q, uint32_t n,
+           const R* Vx, const R* Vy, const R* Vz, bool even, R* rec, cudaStream_t s)
 {
     if (n == 0)
         return VFB_OK;
     const unsigned b = blocksFor(n);
-    if (kind == VFB_BC_VELOCITY_INTERPOLATED) {
-        if (even)
-            postBCKernel<R, VFB_BC_VELOCITY_INTERPOLATED, true><<<b, kThreads, 0, s>>>(dist, lat, k, q, n, Vx, Vy, Vz,
-                                                                                       rec);
-        else
-            postBCKernel<R, VFB_BC_VELOCITY_INTERPOLATED, false><<<b, kThreads, 0, s>>>(dist, lat, k, q, n, Vx, Vy,
-                                                                                        Vz, rec);
-    } else if (kind == VFB_BC_NOSLIP_INTERPOLATED) {
-        if (even)
-            postBCKernel<R, VFB_BC_NOSLIP_INTERPOLATED, true><<<b, kThreads, 0, s>>>(dist, lat, k, q, n, Vx, Vy, Vz,
-                                                                                     rec);
-        else
-            postBCKernel<R, VFB_BC_NOSLIP_INTERPOLATED, false><<<b, kThreads, 0, s>>>(dist, lat, k, q, n, Vx, Vy, Vz,
-                                                                                      rec);
-    } else {
+    constexpr int V = VFB_BC_VELOCITY_INTERPOLATED, NS = VFB_BC_NOSLIP_INTERPOLATED;
+    if (kind == V)
+        (even ? launchPostBC<R, V, true> : launchPostBC<R, V, false>)(b, s, dist, lat, k, table, q, n, Vx, Vy, Vz, rec);
+    else if (kind == NS)
+        (even ? launchPostBC<R, NS, true> : launchPostBC<R, NS, false>)(b, s, dist, lat, k, table, q, n, Vx, Vy, Vz,
+                                                                       rec);
+    else
         return setError(VFB_ERR_INVALID_ARGUMENT, "BC kind %d has no adjoint", kind);
-    }
     return checkLaunch("adjoint forward BC");
 }
 
+template <class R, int KIND, bool EVEN>
+void launchPostScatter(unsigned b, cudaStream_t s, R* lam, const BcLattice<R>& lat, const int32_t* k,
+                       const uint32_t* table, const R* q, uint32_t n, const R* rec, const R* tmp, double* gV)
+{
+    postScatterKernel<R, KIND, EVEN><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, rec, tmp, gV);
+}
+
 template <class R>
-int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, const R* q, uint32_t n,
-                  const R* Vx, const R* Vy, const R* Vz, bool even, const R* rec, R* tmp, double* gV,
+int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, const uint32_t* table, const R* q,
+                  uint32_t n, const R* Vx, const R* Vy, const R* Vz, bool even, const R* rec, R* tmp, double* gV,
                   cudaStream_t s)
 {
     (void)Vx;
@@ -610,26 +635,18 @@ int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, c
         return setError(VFB_ERR_INVALID_ARGUMENT, "BC kind %d has no adjoint", kind);
     const unsigned b = blocksFor(n);
     if (even)
-        postGatherKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, tmp);
+        postGatherKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, tmp);
     else
-        postGatherKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, tmp);
+        postGatherKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, tmp);
     if (const int rc = checkLaunch("BC adjoint gather"))
         return rc;
-    if (kind == VFB_BC_VELOCITY_INTERPOLATED) {
-        if (even)
-            postScatterKernel<R, VFB_BC_VELOCITY_INTERPOLATED, true><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, rec,
-                                                                                            tmp, gV);
-        else
-            postScatterKernel<R, VFB_BC_VELOCITY_INTERPOLATED, false><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, rec,
-                                                                                             tmp, gV);
-    } else {
-        if (even)
-            postScatterKernel<R, VFB_BC_NOSLIP_INTERPOLATED, true><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, rec, tmp,
-                                                                                          nullptr);
-        else
-            postScatterKernel<R, VFB_BC_NOSLIP_INTERPOLATED, false><<<b, kThreads, 0, s>>>(lam, lat, k, q, n, rec,
-                                                                                           tmp, nullptr);
-    }
+    constexpr int V = VFB_BC_VELOCITY_INTERPOLATED, NS = VFB_BC_NOSLIP_INTERPOLATED;
+    if (kind == V)
+        (even ? launchPostScatter<R, V, true> : launchPostScatter<R, V, false>)(b, s, lam, lat, k, table, q, n, rec,
+                                                                               tmp, gV);
+    else
+        (even ? launchPostScatter<R, NS, true> : launchPostScatter<R, NS, false>)(b, s, lam, lat, k, table, q, n, rec,
+                                                                                 tmp, nullptr);
     return checkLaunch("BC adjoint scatter");
 }
 
@@ -703,10 +720,10 @@ int reducePartials(const double* partials, unsigned blocks, int width, double* a
     template int collisionAdjoint<R>(R*, unsigned long long, const uint32_t*, const uint32_t*, const uint32_t*,      \
                                      const uint32_t*, const uint32_t*, uint32_t, const K17Rates<R>&, R, R, R, bool,   \
                                      const R*, double*, cudaStream_t);                                                 \
-    template int postBC<R>(int, R*, const BcLattice<R>&, const int32_t*, const R*, uint32_t, const R*, const R*,      \
-                           const R*, bool, R*, cudaStream_t);                                                          \
-    template int postBCAdjoint<R>(int, R*, const BcLattice<R>&, const int32_t*, const R*, uint32_t, const R*,         \
-                                  const R*, const R*, bool, const R*, R*, double*, cudaStream_t);                      \
+    template int postBC<R>(int, R*, const BcLattice<R>&, const int32_t*, const uint32_t*, const R*, uint32_t,         \
+                           const R*, const R*, const R*, bool, R*, cudaStream_t);                                      \
+    template int postBCAdjoint<R>(int, R*, const BcLattice<R>&, const int32_t*, const uint32_t*, const R*, uint32_t,  \
+                                  const R*, const R*, const R*, bool, const R*, R*, double*, cudaStream_t);            \
     template int pressureBC<R>(R*, const BcLattice<R>&, const int32_t*, const int32_t*, const R*, uint32_t, int,     \
                                bool, R*, cudaStream_t);                                                                \
     template int pressureBCAdjoint<R>(R*, const BcLattice<R>&, const int32_t*, const int32_t*, const R*, uint32_t,   \

@@ -49,24 +49,26 @@ int collision(R* dist, unsigned long long N, const uint32_t* nX, const uint32_t*
               const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx, R fy, R fz,
               bool even, R* tape, cudaStream_t s);
 
-// adjoint of the collision: lam in place; partials[3 * b + c] receive the
-// block sums of the adjoint of the half force (fx, fy, fz)
+// adjoint of the collision: lam in place; partials[3 * b + c] accumulate the
+// block sums of the adjoint of the half force (fx, fy, fz) (the caller
+// clears them before the first step and reduces them after the last)
 template <class R>
 int collisionAdjoint(R* lam, unsigned long long N, const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
                      const uint32_t* fluid, const uint32_t* loc, uint32_t nFluid, const K17Rates<R>& rates, R fx,
                      R fy, R fz, bool even, const R* tape, double* partials, cudaStream_t s);
 
 // forward post-collision BC (kind VFB_BC_VELOCITY_INTERPOLATED or
-// VFB_BC_NOSLIP_INTERPOLATED); rec may be null
+// VFB_BC_NOSLIP_INTERPOLATED); rec may be null; table is the list's location
+// table (vfb_bc_locations) or null
 template <class R>
-int postBC(int kind, R* dist, const BcLattice<R>& lat, const int32_t* k, const R* q, uint32_t n, const R* Vx,
-           const R* Vy, const R* Vz, bool even, R* rec, cudaStream_t s);
+int postBC(int kind, R* dist, const BcLattice<R>& lat, const int32_t* k, const uint32_t* table, const R* q, uint32_t n,
+           const R* Vx, const R* Vy, const R* Vz, bool even, R* rec, cudaStream_t s);
 
 // adjoint of postBC: gather then scatter; gV (3 n doubles: x block, y block,
 // z block) accumulates the adjoint of the BC velocities (velocity kind)
 template <class R>
-int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, const R* q, uint32_t n,
-                  const R* Vx, const R* Vy, const R* Vz, bool even, const R* rec, R* tmp, double* gV,
+int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, const uint32_t* table, const R* q,
+                  uint32_t n, const R* Vx, const R* Vy, const R* Vz, bool even, const R* rec, R* tmp, double* gV,
                   cudaStream_t s);
 
 // forward non-equilibrium pressure BC (after the swap); rec may be null

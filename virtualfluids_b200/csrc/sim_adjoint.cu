@@ -46,6 +46,7 @@ struct AdjointState {
     std::vector<size_t> pressureOffset; // first entry of each pressure list in recPressure / tmpPressure
     size_t pressureTotal = 0;
     DeviceBuffer objNodes, objW[3], partials, accForce, gVelocity;
+    DeviceBuffer forcePartials; // 3 per collision block, accumulated over a backward pass
     DeviceBuffer fluidLocations; // 8 * nFluid: the fluid list's node locations (vfb_bc_locations)
     uint32_t nObj = 0;
     int velocityKind = -1, noSlipKind = -1, geometryKind = -1;
@@ -172,7 +173,8 @@ struct Stepper {
             if (it.list->n == 0 || it.kind < 0)
                 continue;
             if (const int rc = adjoint::postBC<R>(it.kind, dist, t, as<const int32_t>(it.list->k),
-                                                  as<const R>(it.list->q), it.list->n, as<const R>(it.list->vx),
+                                                  as<const uint32_t>(it.list->locations), as<const R>(it.list->q),
+                                                  it.list->n, as<const R>(it.list->vx),
                                                   as<const R>(it.list->vy), as<const R>(it.list->vz), even,
                                                   slotOf(*it.rec, slot, it.list->n), s))
                 return rc;
@@ -222,7 +224,8 @@ struct Stepper {
             if (it.list->n == 0 || it.kind < 0)
                 continue;
             if (const int rc = adjoint::postBCAdjoint<R>(
-                    it.kind, lam, lat, as<const int32_t>(it.list->k), as<const R>(it.list->q), it.list->n,
+                    it.kind, lam, lat, as<const int32_t>(it.list->k), as<const uint32_t>(it.list->locations),
+                    as<const R>(it.list->q), it.list->n,
                     as<const R>(it.list->vx), as<const R>(it.list->vy), as<const R>(it.list->vz), even,
                     slotOf(*it.rec, slot, it.list->n), as<R>(*it.tmp), it.gV, s))
                 return rc;
@@ -230,10 +233,10 @@ struct Stepper {
         if (const int rc = adjoint::collisionAdjoint<R>(lam, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
                                                         as<const uint32_t>(A.fluidLocations), L.nFluid, rates, fx,
                                                         fy, fz, even,
-                                                        slotOf(A.tape, slot, L.nFluid), as<double>(A.partials), s))
+                                                        slotOf(A.tape, slot, L.nFluid),
+                                                        as<double>(A.forcePartials), s))
             return rc;
-        return adjoint::reducePartials(as<double>(A.partials), adjoint::collisionBlocks(L.nFluid), 3,
-                                       as<double>(A.accForce), 0.5 * L.forceFactor, s);
+        return VFB_OK;
     }
 };
 
@@ -322,7 +325,7 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
     // the segment graphs hold these buffers' addresses: a reallocation drops them
     DeviceBuffer* held[] = { &A.work, &A.lam, &A.tape, &A.recVelocity, &A.recNoSlip, &A.recGeometry, &A.recPressure,
                              &A.tmpVelocity, &A.tmpNoSlip, &A.tmpGeometry, &A.tmpPressure, &A.gVelocity,
-                             &A.partials, &A.accForce };
+                             &A.partials, &A.accForce, &A.forcePartials };
     std::vector<void*> before;
     for (DeviceBuffer* b : held)
         before.push_back(b->ptr);
@@ -331,7 +334,8 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         perStep(A.recGeometry, L.geometry.n) || perStep(A.recPressure, A.pressureTotal) ||
         once(A.tmpVelocity, L.velocity.n) || once(A.tmpNoSlip, L.noSlip.n) || once(A.tmpGeometry, L.geometry.n) ||
         once(A.tmpPressure, A.pressureTotal) ||
-        ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))))
+        ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))) ||
+        ensure(A.forcePartials, 3ull * std::max(1u, adjoint::collisionBlocks(L.nFluid)) * sizeof(double)))
         return cudaFail("adjoint buffers");
     for (size_t i = 0; i < before.size(); ++i)
         if (held[i]->ptr != before[i]) {
@@ -344,7 +348,8 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
     // seed: lam = seed * dJ/df on the final state
     if (const int rc = objectiveValue<R>(S, A, as<const R>(A.finalState), A.finalEven, nullptr, as<R>(A.lam), seed, s))
         return rc;
-    if (cudaMemsetAsync(A.accForce.ptr, 0, 3 * sizeof(double), s) != cudaSuccess)
+    if (cudaMemsetAsync(A.accForce.ptr, 0, 3 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(A.forcePartials.ptr, 0, A.forcePartials.bytes, s) != cudaSuccess)
         return cudaFail("force accumulator");
     if (!A.captureStream && cudaStreamCreateWithFlags(&A.captureStream, cudaStreamNonBlocking) != cudaSuccess)
         return cudaFail("capture stream");
@@ -396,6 +401,10 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         if (cudaGraphLaunch(it->second, s) != cudaSuccess)
             return cudaFail("segment graph launch");
     }
+    // the force adjoint: every block's sum over all steps, reduced once in block order
+    if (const int rc = adjoint::reducePartials(as<double>(A.forcePartials), adjoint::collisionBlocks(L.nFluid), 3,
+                                               as<double>(A.accForce), 0.5 * L.forceFactor, s))
+        return rc;
     if (dVelocity && L.velocity.n &&
         cudaMemcpyAsync(dVelocity, A.gVelocity.ptr, 3ull * L.velocity.n * sizeof(double), cudaMemcpyDeviceToHost, s) !=
             cudaSuccess)
