@@ -615,7 +615,8 @@ def precision_report(args):
     rows["bf16_over_fp32_mlups"] = rows["bf16"]["mlups"] / rows["fp32"]["mlups"]
     rows["fx16_over_fp32_mlups"] = rows["fx16"]["mlups"] / rows["fp32"]["mlups"]
     print(json.dumps({"report": "precision form", "workload": f"taylor-green {args.n}^3 periodic, K17",
-                      "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
+                      "steps": args.steps, "bc_epilogue": bool(args.bc_epilogue),
+                      "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
 
 
@@ -648,6 +649,7 @@ def cavity_report(args):
         p.set_storage("fp64")
         p.set_viscosity_LB(nu)
         p.use_graphs = graphs
+        p.use_bc_epilogue = bool(args.bc_epilogue)
         sim = Simulation(p, builder(), BoundaryConditionFactory())
         g = sim.levels[0]
         zero = np.zeros(len(g["geo"]))
@@ -702,6 +704,7 @@ def cube_report(args):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(nu)
+        p.use_bc_epilogue = bool(args.bc_epilogue)
         bc = BoundaryConditionFactory()
         bc.set_slip_boundary_condition(SlipBC.SlipCompressible)
         bc.set_geometry_boundary_condition(NoSlipBC.NoSlipInterpolatedCompressible)
@@ -966,6 +969,9 @@ def main(argv=None):
                     help="bandwidth of the BGK, BC and interface kernels (not a bench line)")
     ap.add_argument("--cavity-report", action="store_true",
                     help="lid-driven cavity 64^3 FP64: graph replay vs direct launches (not a bench line)")
+    ap.add_argument("--bc-epilogue", type=int, default=1, choices=[0, 1],
+                    help="reports: 1 lets the planned collision apply the wall nodes' post-collision BCs (default), "
+                         "0 runs every BC entry in its own launch")
     ap.add_argument("--cube-report", action="store_true",
                     help="wall-mounted cube on two levels: NUPS per storage and errors against FP64 (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",

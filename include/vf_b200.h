@@ -138,6 +138,39 @@ int vfb_collision_plan_stats(const vfb_collision_plan* plan, unsigned long long*
 /* VFB_OK, or VFB_ERR_CUDA if a bounded wait of a planned kernel ran out
  * (synchronises the stream) */
 int vfb_collision_plan_check(const vfb_collision_plan* plan, void* stream);
+/*
+ * BC epilogue of a plan: the post-collision BC lists of the plan's level, in
+ * the order the schedule runs them.  Every list entry whose node the plan's
+ * tiles collide, and whose active links all write cells that no collision
+ * and no other entry reads in the same step (the cell's reader, the node
+ * across the link, is a boundary stopper or a solid node, not a fluid node),
+ * is applied by the planned collision kernel right after that node's own
+ * collision, from the values the kernel has just stored, instead of by a
+ * separate BC launch after the whole collision; the result is the same.
+ * Nodes listed in excludedNodes (device array, e.g. a stress list whose kernel
+ * runs between the post-collision lists) are never taken.  fused (device,
+ * one byte per entry) receives 1 for the entries the epilogue applies; the
+ * caller runs the remaining entries with vfb_bc_post after the collision as
+ * before.  The lists' arrays must stay valid while the plan is used; nLists 0
+ * removes the epilogue.  VFB_ERR_UNSUPPORTED for the direct-load and
+ * per-thread pipelined tile configurations.  No reference counterpart.
+ */
+typedef struct vfb_bc_epilogue_list {
+    int kind;                   /* a post-collision VFB_BC_* kind */
+    const int32_t* k;
+    const void* q;              /* 27 * numberOfBCnodes, direction-major, compute precision */
+    const void* Vx;             /* velocity kinds */
+    const void* Vy;
+    const void* Vz;
+    const uint32_t* locations;  /* the list's location table (vfb_bc_locations), required */
+    uint32_t numberOfBCnodes;
+    uint8_t* fused;             /* output */
+} vfb_bc_epilogue_list;
+int vfb_collision_plan_set_bc_epilogue(vfb_collision_plan* plan, const vfb_bc_epilogue_list* lists, int nLists,
+                                       double omega, const int32_t* excludedNodes, uint32_t nExcluded, void* stream);
+/* out2: nodes and entries the plan's BC epilogue applies */
+int vfb_collision_plan_epilogue_stats(const vfb_collision_plan* plan, unsigned long long* out2);
+
 /* planned K17CompressibleNavierStokes::runOnIndices / B92 run */
 int vfb_k17_collision_planned(const vfb_collision_plan* plan, const vfb_collision_args* args, void* stream);
 int vfb_bgk_collision_planned(const vfb_collision_plan* plan, const vfb_collision_args* args, void* stream);
@@ -436,6 +469,9 @@ typedef struct vfb_sim_params {
                                   BC on the grid's stress lists (UpdateGrid27.cpp:243-245) */
     int hasWallModelMonitor;   /* 1: the stress kernels write u* and the wall momentum per entry
                                   (Parameter::setHasWallModelMonitor) */
+    int bcEpilogue;            /* 1: with usePlan, the planned collision applies the post-collision BCs of
+                                  its wall nodes itself (vfb_collision_plan_set_bc_epilogue; the same
+                                  result); 0: separate BC launches for every entry */
 } vfb_sim_params;
 
 typedef struct vfb_simulation vfb_simulation;
@@ -533,6 +569,11 @@ int vfb_sim_output(vfb_simulation* sim, int level, double* out8, void* rho, void
  * Samplers/WallModelProbe.cu:203-218).
  */
 int vfb_sim_stress_list(vfb_simulation* sim, int level, vfb_stress_list* out);
+
+/* out3: nodes and BC entries the level's collision applies in its BC
+ * epilogue, and the entries left to separate BC launches (all of them
+ * without the epilogue) */
+int vfb_sim_bc_epilogue_stats(vfb_simulation* sim, int level, unsigned long long* out3);
 
 /* the level's device population array and its parity, for inspection */
 int vfb_sim_level_state(vfb_simulation* sim, int level, void** distributions, unsigned long long* numberOfLBnodes,

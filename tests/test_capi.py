@@ -196,7 +196,7 @@ def test_stress_selection_and_wall_model_reader_exist():
     for name in ("vfb_bc_stress", "vfb_sim_stress_list", "vfb_copy_device_to_host"):
         assert hasattr(L, name)
     names = [f[0] for f in VfbSimParams._fields_]
-    assert names[-2:] == ["stressBC", "hasWallModelMonitor"]
+    assert names[-3:] == ["stressBC", "hasWallModelMonitor", "bcEpilogue"]
     bc = BoundaryConditionFactory()
     assert bc.stress == StressBC.NotSpecified
     bc.set_stress_boundary_condition(StressBC.StressBounceBackPressureCompressible)

@@ -175,6 +175,11 @@ _SIGNATURES = [
     ("vfb_sim_kinetic_energy", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_sim_stress_list", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StressList)]),
+    ("vfb_sim_bc_epilogue_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("vfb_collision_plan_set_bc_epilogue", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_uint32,
+      ctypes.c_void_p]),
+    ("vfb_collision_plan_epilogue_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_copy_device_to_host", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("vfb_sim_level_state", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong),

@@ -33,6 +33,7 @@
 
 #include <cmath>
 
+#include "bc_entry.cuh"
 #include "bc_math.cuh"
 #include "capi_common.cuh"
 #include "collision_math.cuh"
@@ -80,79 +81,11 @@ __global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const 
                                                      const typename Storage<S>::R* __restrict__ Vz,
                                                      const uint32_t* __restrict__ locations)
 {
-    using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nBC)
         return;
-    const unsigned long long N = lat.N;
     const Locs L = bcLocations(locations, i, nBC, bcK, lat.nX, lat.nY, lat.nZ);
-    // post-collision population moving in direction d: slot of inv(d), location of inv(d)
-    R g[27];
-#pragma unroll
-    for (int d = 0; d < 27; ++d)
-        g[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(inv(d)) * N + L.k[loc(inv(d))], d);
-
-    R drho = R(0), vx1 = R(0), vx2 = R(0), vx3 = R(0), cuSq = R(0);
-    if (KIND == VFB_BC_NOSLIP_INTERPOLATED || KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_SLIP ||
-        KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
-        bcMacros(g, drho, vx1, vx2, vx3);
-        cuSq = R(3) / R(2) * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3) * (R(1) + drho);
-    }
-    R UX = R(0), UY = R(0), UZ = R(0);
-    if (KIND == VFB_BC_VELOCITY_INTERPOLATED || KIND == VFB_BC_VELOCITY_BOUNCE_BACK ||
-        KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
-        UX = __ldg(Vx + i);
-        UY = __ldg(Vy + i);
-        UZ = __ldg(Vz + i);
-    }
-    // slip: normal components are removed for each axis with an active axis direction
-    bool flagX = false, flagY = false, flagZ = false;
-    // all q values first, so that their loads are in flight together instead
-    // of one per direction behind the branch on the previous one
-    R qv[26];
-#pragma unroll
-    for (int j = 0; j < 26; ++j)
-        qv[j] = __ldg(q + (unsigned long long)qOrder(j) * nBC + i);
-#pragma unroll
-    for (int j = 0; j < 26; ++j) {
-        const int d = qOrder(j);
-        const R qd = qv[j];
-        if (!(qd >= R(0) && qd <= R(1)))
-            continue;
-        const int e = inv(d);
-        S* target = dist + (unsigned long long)slot<!EVEN>(e) * N + L.k[loc(e)];
-        const R w = weight<R>(d);
-        R value;
-        if (KIND == VFB_BC_NOSLIP_BOUNCE_BACK) {
-            value = g[d];
-        } else if (KIND == VFB_BC_VELOCITY_BOUNCE_BACK) {
-            // 6 w (-c_d . U) with 6 w = 4/9, 1/9, 1/36 for face, edge, corner directions
-            const R k6 = order(d) == 1 ? R(4) / R(9) : order(d) == 2 ? R(1) / R(9) : R(1) / R(36);
-            value = g[d] + k6 * cdot<R>(e, UX, UY, UZ);
-        } else if (KIND == VFB_BC_NOSLIP_INTERPOLATED) {
-            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
-            value = interpNoSlip(qd, g[d], g[e], feq, lat.omega);
-        } else if (KIND == VFB_BC_VELOCITY_INTERPOLATED) {
-            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
-            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, UX, UY, UZ), w);
-        } else if (KIND == VFB_BC_VELOCITY_WITH_PRESSURE) {
-            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
-            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, UX, UY, UZ), w) - w * drho;
-        } else {
-            if (order(d) == 1) {
-                if (cx(d) != 0)
-                    flagX = true;
-                else if (cy(d) != 0)
-                    flagY = true;
-                else
-                    flagZ = true;
-            }
-            const R sx = flagX ? R(0) : vx1, sy = flagY ? R(0) : vx2, sz = flagZ ? R(0) : vx3;
-            const R feq = feqBC(drho, cdot<R>(d, vx1, vx2, vx3), cuSq, w);
-            value = interpVelocity(qd, g[d], g[e], feq, lat.omega, cdot<R>(d, sx, sy, sz), w);
-        }
-        Storage<S>::store(target, value, d);
-    }
+    bcPostEntry<S, KIND, EVEN>(dist, lat.N, lat.omega, L, q, nBC, i, Vx, Vy, Vz);
 }
 
 // PressureNonEquilibriumCompressible.cu:75-309: the neighbour's

@@ -344,6 +344,18 @@ extern "C" int vfb_collision_plan_create(int storage, const vfb_collision_args* 
     return VFB_OK;
 }
 
+static void freeEpilogue(vfb_collision_plan_impl& p)
+{
+    cudaFree(p.epi);
+    cudaFree(p.epiNodes);
+    cudaFree(p.epiRecords);
+    cudaFree(p.epiTiles);
+    p.epi = nullptr;
+    p.epiNodes = nullptr;
+    p.epiRecords = nullptr;
+    p.epiTiles = nullptr;
+}
+
 extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
 {
     clearError();
@@ -353,7 +365,215 @@ extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
     cudaFree(p->meta);
     cudaFree(p->laneList);
     cudaFree(p->error);
+    freeEpilogue(*p);
     delete p;
+    return VFB_OK;
+}
+
+namespace
+{
+template <class T>
+cudaError_t download(std::vector<T>& v, const void* src, size_t n, cudaStream_t s)
+{
+    v.resize(n);
+    return n ? cudaMemcpyAsync(v.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, s) : cudaSuccess;
+}
+
+// the tile configurations whose kernels run the BC epilogue: the paired
+// kernels (one stage) and the staged kernels (entries 0-6)
+bool epilogueConfig(int c)
+{
+    return (c >= 0 && c <= 6) || c == 12 || c == 13 || c == 14 || c == 19 || c == 20;
+}
+} // namespace
+
+extern "C" int vfb_collision_plan_set_bc_epilogue(vfb_collision_plan* plan, const vfb_bc_epilogue_list* lists,
+                                                  int nLists, double omega, const int32_t* excludedNodes,
+                                                  uint32_t nExcluded, void* stream)
+{
+    clearError();
+    if (!plan)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "plan is NULL");
+    auto& p = *reinterpret_cast<vfb_collision_plan_impl*>(plan);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "BC epilogue: %s", cudaGetErrorString(cudaGetLastError()));
+    freeEpilogue(p);
+    if (nLists == 0)
+        return VFB_OK;
+    if (nLists < 0 || nLists > kMaxFusedLists || !lists)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "the BC epilogue takes 1 to %d lists", kMaxFusedLists);
+    if (!epilogueConfig(p.config))
+        return setError(VFB_ERR_UNSUPPORTED, "tile configuration %d has no BC epilogue", p.config);
+    if (!(omega > 0.0 && omega < 2.0 && omega != 1.0))
+        return setError(VFB_ERR_INVALID_ARGUMENT, "omega %g outside (0, 2) or equal to 1", omega);
+    if (nExcluded && !excludedNodes)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "excludedNodes is NULL");
+    for (int l = 0; l < nLists; ++l) {
+        const vfb_bc_epilogue_list& L = lists[l];
+        if (L.kind < VFB_BC_NOSLIP_INTERPOLATED || L.kind > VFB_BC_VELOCITY_WITH_PRESSURE)
+            return setError(VFB_ERR_INVALID_ARGUMENT, "list %d: kind %d is not a post-collision kind", l, L.kind);
+        if (L.numberOfBCnodes && (!L.k || !L.q || !L.locations || !L.fused))
+            return setError(VFB_ERR_INVALID_ARGUMENT, "list %d: NULL k, q, locations or fused", l);
+        const bool velocity = L.kind == VFB_BC_VELOCITY_INTERPOLATED || L.kind == VFB_BC_VELOCITY_BOUNCE_BACK ||
+                              L.kind == VFB_BC_VELOCITY_WITH_PRESSURE;
+        if (velocity && L.numberOfBCnodes && (!L.Vx || !L.Vy || !L.Vz))
+            return setError(VFB_ERR_INVALID_ARGUMENT, "list %d: a velocity kind needs Vx, Vy, Vz", l);
+        if (L.numberOfBCnodes > kFusedEntryMask)
+            return setError(VFB_ERR_OUT_OF_RANGE, "list %d: too many entries", l);
+    }
+    const uint64_t N = p.N;
+    const bool dbl = p.storage == VFB_FP64;
+    std::vector<uint32_t> nx, ny, nz, fl, meta;
+    std::vector<int32_t> excl;
+    cudaError_t e = download(nx, p.nX, N, s);
+    if (e == cudaSuccess) e = download(ny, p.nY, N, s);
+    if (e == cudaSuccess) e = download(nz, p.nZ, N, s);
+    if (e == cudaSuccess) e = download(fl, p.fluid, p.nFluid, s);
+    if (e == cudaSuccess) e = download(meta, p.meta, (size_t)p.nTiles * p.metaWords, s);
+    if (e == cudaSuccess) e = download(excl, excludedNodes, nExcluded, s);
+    std::vector<std::vector<int32_t>> ks(nLists);
+    std::vector<std::vector<uint32_t>> locs(nLists);
+    std::vector<std::vector<double>> qs(nLists);
+    std::vector<float> qf;
+    for (int l = 0; l < nLists && e == cudaSuccess; ++l) {
+        const uint32_t n = lists[l].numberOfBCnodes;
+        e = download(ks[l], lists[l].k, n, s);
+        if (e == cudaSuccess)
+            e = download(locs[l], lists[l].locations, 8ull * n, s);
+        if (e == cudaSuccess && dbl)
+            e = download(qs[l], lists[l].q, 27ull * n, s);
+        if (e == cudaSuccess && !dbl) {
+            e = download(qf, lists[l].q, 27ull * n, s);
+            if (e == cudaSuccess)
+                e = cudaStreamSynchronize(s);
+            qs[l].assign(qf.begin(), qf.end());
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "BC epilogue: copying the lists failed: %s", cudaGetErrorString(e));
+
+    // the bulk tile of every node the tiles collide, and the fluid nodes
+    const uint32_t T = p.tileWidth;
+    std::vector<int64_t> tileOf(N, -1);
+    for (uint32_t t = 0; t < p.nTiles; ++t) {
+        const uint32_t* m = meta.data() + (size_t)t * p.metaWords;
+        for (uint32_t off = 0; off < T; ++off)
+            if ((m[4 + off / 32] >> (off % 32)) & 1u)
+                tileOf[(uint64_t)m[0] + off] = t;
+    }
+    std::vector<uint8_t> isFluid(N, 0), ok(N, 1);
+    for (uint32_t k : fl)
+        isFluid[k] = 1;
+    for (int32_t k : excl)
+        if (k >= 0 && (uint64_t)k < N)
+            ok[(uint64_t)k] = 0;
+    // inverse neighbours: the node whose +axis neighbour is k
+    const uint32_t none = 0xffffffffu;
+    std::vector<uint32_t> invNb[3] = { std::vector<uint32_t>(N, none), std::vector<uint32_t>(N, none),
+                                       std::vector<uint32_t>(N, none) };
+    const std::vector<uint32_t>* nb[3] = { &nx, &ny, &nz };
+    for (uint64_t k = 0; k < N; ++k)
+        for (int ax = 0; ax < 3; ++ax) {
+            const uint32_t j = (*nb[ax])[k];
+            if (j < N && j != k)
+                invNb[ax][j] = (uint32_t)k;
+        }
+    // a node qualifies when it is a bulk-tile node, not excluded, and every
+    // active link of every entry of it writes a cell whose reader (the node C
+    // whose location loc(d) is that cell in slot d) is not a fluid node
+    for (int l = 0; l < nLists; ++l) {
+        const uint32_t n = lists[l].numberOfBCnodes;
+        for (uint32_t i = 0; i < n; ++i) {
+            const int64_t A = ks[l][i];
+            if (A < 0 || (uint64_t)A >= N)
+                return setError(VFB_ERR_OUT_OF_RANGE, "list %d entry %u: node %lld outside the lattice", l, i,
+                                (long long)A);
+            if (tileOf[(uint64_t)A] < 0) {
+                ok[(uint64_t)A] = 0;
+                continue;
+            }
+            for (int d = 1; d < 27 && ok[(uint64_t)A]; ++d) {
+                const double qd = qs[l][(size_t)d * n + i];
+                if (!(qd >= 0.0 && qd <= 1.0))
+                    continue;
+                uint32_t c = locs[l][(size_t)loc(inv(d)) * n + i]; // the written cell's location index
+                const int bits = loc(d);
+                for (int ax = 2; ax >= 0 && c != none; --ax)
+                    if (bits & (1 << ax))
+                        c = invNb[ax][c];
+                if (c != none && isFluid[c])
+                    ok[(uint64_t)A] = 0;
+            }
+        }
+    }
+    // records of the qualifying nodes: per node, in list order, then entry order
+    std::vector<std::vector<uint32_t>> byNode; // per qualifying node, in order of first appearance
+    std::vector<uint32_t> slotOf(N, none);
+    std::vector<uint64_t> nodes;
+    for (int l = 0; l < nLists; ++l) {
+        const uint32_t n = lists[l].numberOfBCnodes;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t A = (uint64_t)ks[l][i];
+            if (!ok[A])
+                continue;
+            if (slotOf[A] == none) {
+                slotOf[A] = (uint32_t)byNode.size();
+                byNode.emplace_back();
+                nodes.push_back(A);
+            }
+            byNode[slotOf[A]].push_back(((uint32_t)l << 28) | i);
+        }
+    }
+    std::vector<uint32_t> nodeRecord(N, 0u), records;
+    std::vector<uint8_t> tiles(p.nTiles, 0);
+    for (size_t j = 0; j < nodes.size(); ++j) {
+        nodeRecord[nodes[j]] = (uint32_t)records.size() + 1u;
+        for (size_t r = 0; r < byNode[j].size(); ++r)
+            records.push_back(byNode[j][r] | (r + 1 == byNode[j].size() ? kFusedLast : 0u));
+        tiles[(size_t)tileOf[nodes[j]]] = 1;
+    }
+    std::vector<std::vector<uint8_t>> fused(nLists);
+    for (int l = 0; l < nLists; ++l) {
+        fused[l].resize(lists[l].numberOfBCnodes);
+        for (uint32_t i = 0; i < lists[l].numberOfBCnodes; ++i)
+            fused[l][i] = ok[(uint64_t)ks[l][i]];
+    }
+    BcEpilogue h {};
+    for (int l = 0; l < nLists; ++l) {
+        h.kind[l] = lists[l].kind;
+        h.n[l] = lists[l].numberOfBCnodes;
+        h.q[l] = lists[l].q;
+        h.V[l][0] = lists[l].Vx;
+        h.V[l][1] = lists[l].Vy;
+        h.V[l][2] = lists[l].Vz;
+        h.locations[l] = lists[l].locations;
+    }
+    h.omega = omega;
+    e = upload(&p.epiNodes, nodeRecord, s);
+    if (e == cudaSuccess)
+        e = upload(&p.epiRecords, records, s);
+    if (e == cudaSuccess)
+        e = upload(&p.epiTiles, tiles, s);
+    h.nodeRecord = p.epiNodes;
+    h.records = p.epiRecords;
+    if (e == cudaSuccess)
+        e = cudaMalloc(&p.epi, sizeof(BcEpilogue));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p.epi, &h, sizeof(BcEpilogue), cudaMemcpyHostToDevice, s);
+    for (int l = 0; l < nLists && e == cudaSuccess; ++l)
+        if (lists[l].numberOfBCnodes)
+            e = cudaMemcpyAsync(lists[l].fused, fused[l].data(), fused[l].size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        freeEpilogue(p);
+        return setError(VFB_ERR_CUDA, "BC epilogue upload failed: %s", cudaGetErrorString(e));
+    }
+    p.epiCount[0] = nodes.size();
+    p.epiCount[1] = records.size();
     return VFB_OK;
 }
 
@@ -365,6 +585,17 @@ extern "C" int vfb_collision_plan_stats(const vfb_collision_plan* plan, unsigned
     const auto* p = reinterpret_cast<const vfb_collision_plan_impl*>(plan);
     for (int i = 0; i < 6; ++i)
         out6[i] = p->stats[i];
+    return VFB_OK;
+}
+
+extern "C" int vfb_collision_plan_epilogue_stats(const vfb_collision_plan* plan, unsigned long long* out2)
+{
+    clearError();
+    if (!plan || !out2)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    const auto* p = reinterpret_cast<const vfb_collision_plan_impl*>(plan);
+    out2[0] = p->epi ? p->epiCount[0] : 0;
+    out2[1] = p->epi ? p->epiCount[1] : 0;
     return VFB_OK;
 }
 

@@ -41,6 +41,7 @@
 #include <map>
 #include <vector>
 
+#include "bc_entry.cuh"
 #include "capi_common.cuh"
 #include "collision_math.cuh"
 #include "d3q27.cuh"
@@ -132,6 +133,10 @@ struct TiledArgs {
     R* bfy;
     R* bfz;
     int* errorFlag;
+    // the BC epilogue (bc_entry.cuh) or null; epiTiles[t] != 0 when tile t
+    // holds a node with BC records
+    const BcEpilogue* epi;
+    const uint8_t* epiTiles;
 };
 
 // offset of location loc (bit 0 x, bit 1 y, bit 2 z) from the node for the
@@ -320,6 +325,9 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                 for (int d = 0; d < 27; ++d)
                     Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
             }
+            // the node's post-collision BCs, from the values this thread just stored
+            if (a.epi && __ldg(a.epiTiles + t0 + j * stride))
+                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, k);
         }
     }
 }
@@ -484,6 +492,13 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
                 St::storeRaw(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
         }
     }
+    // the nodes' post-collision BCs, from the values this thread just stored
+    if (a.epi && __ldg(a.epiTiles + blockIdx.x)) {
+        if (actA)
+            bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kA);
+        if (actB)
+            bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kB);
+    }
 }
 
 // Per-thread pipelined form (KIND 1, 4- and 8-byte storage): a persistent
@@ -589,6 +604,13 @@ struct vfb_collision_plan_impl {
     // tiles, bulk tiles, lane blocks, bulk-fed nodes, wrap nodes served in bulk tiles, nodes collided lane by lane
     unsigned long long stats[6] = { 0, 0, 0, 0, 0, 0 };
     int* error = nullptr;
+    // the BC epilogue (vfb_collision_plan_set_bc_epilogue): descriptor, per-node
+    // first record, records and per-tile flags, all device memory
+    BcEpilogue* epi = nullptr;
+    uint32_t* epiNodes = nullptr;
+    uint32_t* epiRecords = nullptr;
+    uint8_t* epiTiles = nullptr;
+    unsigned long long epiCount[2] = { 0, 0 }; // nodes, records
 };
 
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
@@ -743,6 +765,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.bfy = static_cast<R*>(c->bodyForceY);
     a.bfz = static_cast<R*>(c->bodyForceZ);
     a.errorFlag = p.error;
+    a.epi = p.epi;
+    a.epiTiles = p.epiTiles;
     if (p.nTiles == 0)
         return VFB_OK;
     const bool even = c->isEvenTimestep != 0;

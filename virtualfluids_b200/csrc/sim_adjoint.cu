@@ -471,6 +471,26 @@ extern "C" int vfb_sim_set_velocity_bc(vfb_simulation* sim, int level, const dou
         if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
             return cudaFail("velocity upload");
     }
+    // the entries of the velocity list the BC epilogue leaves to the separate launch
+    Level& L = *sim->levels[level];
+    if (L.epilogue && L.residual[0].list.n) {
+        ResidualList& R = L.residual[0];
+        DeviceBuffer* rdst[3] = { &R.list.vx, &R.list.vy, &R.list.vz };
+        std::vector<double> g(R.index.size());
+        std::vector<float> gf(R.index.size());
+        for (int c = 0; c < 3; ++c) {
+            for (size_t j = 0; j < R.index.size(); ++j) {
+                g[j] = src[c][R.index[j]];
+                gf[j] = (float)g[j];
+            }
+            const cudaError_t e = dbl ? cudaMemcpyAsync(rdst[c]->ptr, g.data(), g.size() * sizeof(double),
+                                                        cudaMemcpyHostToDevice, s)
+                                      : cudaMemcpyAsync(rdst[c]->ptr, gf.data(), gf.size() * sizeof(float),
+                                                        cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+                return cudaFail("velocity upload");
+        }
+    }
     if (sim->adjoint)
         sim->adjoint->ready = false;
     return VFB_OK;

@@ -41,6 +41,14 @@ struct BcListDevice {
     uint32_t n = 0;
 };
 
+// a post-collision list under the plan's BC epilogue: the entries the
+// collision kernel does not apply itself, run by the separate BC launch, and
+// their indices in the full list (to refresh the velocities)
+struct ResidualList {
+    BcListDevice list;
+    std::vector<uint32_t> index;
+};
+
 // interface cells between this level and the next finer one (InterpolationCells
 // + ICellNeigh, Calculation.h:72-89)
 struct InterfaceDevice {
@@ -71,6 +79,10 @@ struct Level {
     DeviceBuffer nNeg; // the -x-y-z neighbour (non-equilibrium init, enstrophy)
     BcListDevice velocity, noSlip, slip, geometry;
     StressListDevice stress;
+    // with the plan's BC epilogue: the remaining entries of velocity, no-slip,
+    // slip and geometry (in that order), launched after the collision
+    bool epilogue = false;
+    ResidualList residual[4];
     std::vector<PressureListDevice*> pressure;
     InterfaceDevice coarseToFine, fineToCoarse;
     DeviceBuffer energyNodes; // the kinetic-energy analyzer's node set

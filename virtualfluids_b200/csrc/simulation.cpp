@@ -345,6 +345,134 @@ int collision(vfb_simulation& S, Level& L, void* stream)
     return k17 ? vfb_k17_collision(S.params.storage, &a, stream) : vfb_bgk_collision(S.params.storage, &a, stream);
 }
 
+// the entries `index` of a list, gathered on the host into a new device list
+// (element sizes: k and locations 4 bytes, q and velocities `real` bytes)
+int gatherList(const BcListDevice& B, const std::vector<uint32_t>& index, size_t real, BcListDevice& out,
+               cudaStream_t s)
+{
+    const uint32_t n = B.n, m = (uint32_t)index.size();
+    out.n = m;
+    std::vector<char> k(4ull * n), loc(32ull * n), q(27ull * n * real), v[3];
+    cudaError_t e = cudaMemcpyAsync(k.data(), B.k.ptr, k.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(loc.data(), B.locations.ptr, loc.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(q.data(), B.q.ptr, q.size(), cudaMemcpyDeviceToHost, s);
+    const DeviceBuffer* vb[3] = { &B.vx, &B.vy, &B.vz };
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+        if (vb[c]->ptr) {
+            v[c].resize(real * n);
+            e = cudaMemcpyAsync(v[c].data(), vb[c]->ptr, v[c].size(), cudaMemcpyDeviceToHost, s);
+        }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "residual BC list: %s", cudaGetErrorString(e));
+    std::vector<char> k2(4ull * m), loc2(32ull * m), q2(27ull * m * real), v2[3];
+    for (uint32_t j = 0; j < m; ++j) {
+        const uint32_t i = index[j];
+        std::memcpy(&k2[4ull * j], &k[4ull * i], 4);
+        for (int l = 0; l < 8; ++l)
+            std::memcpy(&loc2[4ull * ((size_t)l * m + j)], &loc[4ull * ((size_t)l * n + i)], 4);
+        for (int d = 0; d < 27; ++d)
+            std::memcpy(&q2[real * ((size_t)d * m + j)], &q[real * ((size_t)d * n + i)], real);
+    }
+    DeviceBuffer* ob[3] = { &out.vx, &out.vy, &out.vz };
+    for (int c = 0; c < 3; ++c)
+        if (!v[c].empty()) {
+            v2[c].resize(real * m);
+            for (uint32_t j = 0; j < m; ++j)
+                std::memcpy(&v2[c][real * j], &v[c][real * index[j]], real);
+        }
+    e = uploadRaw(out.k, k2.data(), k2.size(), s);
+    if (e == cudaSuccess)
+        e = uploadRaw(out.locations, loc2.data(), loc2.size(), s);
+    if (e == cudaSuccess)
+        e = uploadRaw(out.q, q2.data(), q2.size(), s);
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+        if (!v2[c].empty())
+            e = uploadRaw(*ob[c], v2[c].data(), v2[c].size(), s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "residual BC list upload: %s", cudaGetErrorString(e));
+    return VFB_OK;
+}
+
+// the plan's BC epilogue for a level: the post-collision lists in schedule
+// order (a stress list's nodes excluded, since its kernel runs between them),
+// then the residual lists of the entries the epilogue does not take
+int setupEpilogue(vfb_simulation& S, Level& L, cudaStream_t s)
+{
+    const vfb_sim_params& P = S.params;
+    BcListDevice* full[4] = { &L.velocity, &L.noSlip, &L.slip, &L.geometry };
+    const int kinds[4] = { P.velocityBC, P.noSlipBC, P.slipBC, P.geometryBC };
+    vfb_bc_epilogue_list lists[4];
+    int which[4];
+    int n = 0;
+    DeviceBuffer fused[4];
+    for (int i = 0; i < 4; ++i) {
+        if (full[i]->n == 0 || kinds[i] < 0)
+            continue;
+        if (fused[n].allocate(full[i]->n) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "epilogue flags");
+        vfb_bc_epilogue_list& e = lists[n];
+        e.kind = kinds[i];
+        e.k = static_cast<const int32_t*>(full[i]->k.ptr);
+        e.q = full[i]->q.ptr;
+        e.Vx = full[i]->vx.ptr;
+        e.Vy = full[i]->vy.ptr;
+        e.Vz = full[i]->vz.ptr;
+        e.locations = static_cast<const uint32_t*>(full[i]->locations.ptr);
+        e.numberOfBCnodes = full[i]->n;
+        e.fused = static_cast<uint8_t*>(fused[n].ptr);
+        which[n++] = i;
+    }
+    if (n == 0)
+        return VFB_OK;
+    const bool stress = L.stress.n > 0 && P.stressBC >= 0;
+    const int rc = vfb_collision_plan_set_bc_epilogue(L.plan, lists, n, L.omega,
+                                                      stress ? static_cast<const int32_t*>(L.stress.k.ptr) : nullptr,
+                                                      stress ? L.stress.n : 0u, s);
+    if (rc == VFB_ERR_UNSUPPORTED) { // a tuning configuration without the epilogue: separate launches
+        clearError();
+        return VFB_OK;
+    }
+    if (rc)
+        return rc;
+    const size_t real = computeIsDouble(P.storage) ? sizeof(double) : sizeof(float);
+    for (int j = 0; j < n; ++j) {
+        const int i = which[j];
+        std::vector<uint8_t> f(full[i]->n);
+        if (cudaMemcpyAsync(f.data(), fused[j].ptr, f.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return setError(VFB_ERR_CUDA, "epilogue flags: %s", cudaGetErrorString(cudaGetLastError()));
+        ResidualList& R = L.residual[i];
+        R.index.clear();
+        for (uint32_t e = 0; e < full[i]->n; ++e)
+            if (!f[e])
+                R.index.push_back(e);
+        if (const int g = gatherList(*full[i], R.index, real, R.list, s))
+            return g;
+    }
+    // lists the epilogue was not given keep all their entries
+    for (int i = 0; i < 4; ++i) {
+        bool given = false;
+        for (int j = 0; j < n; ++j)
+            given = given || which[j] == i;
+        if (!given && full[i]->n) {
+            ResidualList& R = L.residual[i];
+            R.index.resize(full[i]->n);
+            for (uint32_t e = 0; e < full[i]->n; ++e)
+                R.index[e] = e;
+            if (const int g = gatherList(*full[i], R.index, real, R.list, s))
+                return g;
+        }
+    }
+    L.epilogue = true;
+    return VFB_OK;
+}
+
 vfb_stress_list stressList(StressListDevice& T, bool monitor)
 {
     vfb_stress_list l;
@@ -383,10 +511,10 @@ int postCollisionBC(vfb_simulation& S, Level& L, void* stream)
     struct Item {
         const BcListDevice* list;
         int kind;
-    } items[4] = { { &L.velocity, S.params.velocityBC },
-                   { &L.noSlip, S.params.noSlipBC },
-                   { &L.slip, S.params.slipBC },
-                   { &L.geometry, S.params.geometryBC } };
+    } items[4] = { { L.epilogue ? &L.residual[0].list : &L.velocity, S.params.velocityBC },
+                   { L.epilogue ? &L.residual[1].list : &L.noSlip, S.params.noSlipBC },
+                   { L.epilogue ? &L.residual[2].list : &L.slip, S.params.slipBC },
+                   { L.epilogue ? &L.residual[3].list : &L.geometry, S.params.geometryBC } };
     for (int i = 0; i < 4; ++i) {
         const Item& it = items[i];
         if (i == 3 && L.stress.n > 0 && S.params.stressBC >= 0) {
@@ -666,6 +794,8 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
         Level& L = *S->levels[l];
         vfb_collision_args a = collisionArgs(*S, L);
         rc = vfb_collision_plan_create(P.storage, &a, &L.plan, stream);
+        if (rc == VFB_OK && P.bcEpilogue)
+            rc = setupEpilogue(*S, L, s);
     }
     if (rc != VFB_OK) {
         delete S;
@@ -960,6 +1090,26 @@ extern "C" int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* ou
         return rc;
     out2[0] = sums[1] / (double)L->nEnergy;
     out2[1] = (double)L->nEnergy;
+    return VFB_OK;
+}
+
+extern "C" int vfb_sim_bc_epilogue_stats(vfb_simulation* sim, int level, unsigned long long* out3)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    if (!out3)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "out3 is NULL");
+    out3[0] = out3[1] = 0;
+    if (L->epilogue && L->plan)
+        if (const int rc = vfb_collision_plan_epilogue_stats(L->plan, out3))
+            return rc;
+    unsigned long long rest = 0;
+    const BcListDevice* full[4] = { &L->velocity, &L->noSlip, &L->slip, &L->geometry };
+    for (int i = 0; i < 4; ++i)
+        rest += L->epilogue ? L->residual[i].list.n : full[i]->n;
+    out3[2] = rest;
     return VFB_OK;
 }
 

@@ -39,6 +39,7 @@ class VfbSimParams(ctypes.Structure):
         ("velocityRatio", ctypes.c_double),
         ("stressBC", ctypes.c_int),
         ("hasWallModelMonitor", ctypes.c_int),
+        ("bcEpilogue", ctypes.c_int),
     ]
 
 
@@ -135,6 +136,9 @@ class Parameter:
         # are divided by it (GridGenerator.cpp:507-513)
         self.velocity_ratio = 1.0
         self.has_wall_model_monitor = False
+        # the planned collision applies the post-collision BCs of its wall
+        # nodes itself (same result, no separate pass over those entries)
+        self.use_bc_epilogue = True
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
@@ -268,6 +272,7 @@ class Simulation:
         p.velocityRatio = parameter.velocity_ratio
         p.stressBC = int(bcFactory.stress)
         p.hasWallModelMonitor = int(bool(parameter.has_wall_model_monitor))
+        p.bcEpilogue = int(bool(parameter.use_bc_epilogue))
         self._double = p.storage == _lib.FP64
         if isinstance(gridBuilder, MultipleGridBuilder):
             spec = gridBuilder.full_spec()
@@ -391,6 +396,13 @@ class Simulation:
         _lib.check(_lib.lib().vfb_sim_adjoint_backward(self._h, float(seed), dv.ctypes.data, df.ctypes.data,
                                                        self.stream))
         return dv, df
+
+    def bc_epilogue_stats(self, level: int = 0) -> tuple[int, int, int]:
+        """(nodes, BC entries) the level's collision applies in its BC
+        epilogue, and the entries left to the separate BC launches."""
+        out = (ctypes.c_ulonglong * 3)()
+        _lib.check(_lib.lib().vfb_sim_bc_epilogue_stats(self._h, level, out))
+        return int(out[0]), int(out[1]), int(out[2])
 
     def wall_model(self, level: int = 0) -> dict[str, np.ndarray]:
         """The level's stress list and wall-model arrays as host copies: the
