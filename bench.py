@@ -615,8 +615,7 @@ def precision_report(args):
     rows["bf16_over_fp32_mlups"] = rows["bf16"]["mlups"] / rows["fp32"]["mlups"]
     rows["fx16_over_fp32_mlups"] = rows["fx16"]["mlups"] / rows["fp32"]["mlups"]
     print(json.dumps({"report": "precision form", "workload": f"taylor-green {args.n}^3 periodic, K17",
-                      "steps": args.steps, "bc_epilogue": bool(args.bc_epilogue),
-                      "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
+                      "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
 
 
@@ -747,7 +746,8 @@ def cube_report(args):
     print(json.dumps({"report": "wall-mounted cube, two levels", "workload":
                       "cube channel 256x96x96 + refined box 48..128 x 24..72 x 0..40, cube 16 at x=64, K17",
                       "nodes_per_level": nodes, "fluid_nodes_per_level": fluid, "grid_build_s": build_s,
-                      "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
+                      "steps": args.steps, "bc_epilogue": bool(args.bc_epilogue),
+                      "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
 
 
@@ -827,6 +827,24 @@ def kernel_report(args):
     ms = timed(lambda: K.bc_post(_lib.BC_VELOCITY_INTERPOLATED, dist, lat, k, q, 1.9, True, *v, locations=locs))
     record(f"velocity_bc_cavity{nb}_location_table", n_bc, (27 * 4 + 27 * 4 + 32 + 12) + active * 4 / n_bc, ms,
            "bc_nodes")
+    # the same list split by wall: x faces (consecutive entries a row apart in
+    # memory) against y and z faces (consecutive entries adjacent)
+    kk = g["velocity.k"]
+    qq = g["velocity.q"].reshape(27, n_bc)
+    cx, cy = g["coordX"][kk], g["coordY"][kk]
+    on_x = (cx == cx.min()) | (cx == cx.max())
+    on_y = ((cy == cy.min()) | (cy == cy.max())) & ~on_x
+    for face, sel in (("x", on_x), ("y", on_y), ("z", ~on_x & ~on_y)):
+        idx = np.flatnonzero(sel)
+        fk = torch.from_numpy(kk[idx].astype(np.int32)).cuda()
+        fq = torch.from_numpy(np.ascontiguousarray(qq[:, idx]).astype(np.float32).ravel()).cuda()
+        fv = [torch.from_numpy(g[f"velocity.{c}"][idx].astype(np.float32)).cuda() for c in ("vx", "vy", "vz")]
+        floc = K.bc_locations(lat, fk)
+        fa = int((qq[:, idx] >= 0).sum())
+        ms = timed(lambda: K.bc_post(_lib.BC_VELOCITY_INTERPOLATED, dist, lat, fk, fq, 1.9, True, *fv,
+                                     locations=floc))
+        record(f"velocity_bc_cavity{nb}_{face}_faces", len(idx), (27 * 4 + 27 * 4 + 32 + 12) + fa * 4 / len(idx), ms,
+               "bc_nodes")
     del dist, lat
     torch.cuda.empty_cache()
     b = MultipleGridBuilder()
@@ -969,9 +987,9 @@ def main(argv=None):
                     help="bandwidth of the BGK, BC and interface kernels (not a bench line)")
     ap.add_argument("--cavity-report", action="store_true",
                     help="lid-driven cavity 64^3 FP64: graph replay vs direct launches (not a bench line)")
-    ap.add_argument("--bc-epilogue", type=int, default=1, choices=[0, 1],
-                    help="reports: 1 lets the planned collision apply the wall nodes' post-collision BCs (default), "
-                         "0 runs every BC entry in its own launch")
+    ap.add_argument("--bc-epilogue", type=int, default=0, choices=[0, 1],
+                    help="reports: 1 lets the planned collision apply the wall nodes' post-collision BCs, "
+                         "0 (default) runs every BC entry in the separate BC launches")
     ap.add_argument("--cube-report", action="store_true",
                     help="wall-mounted cube on two levels: NUPS per storage and errors against FP64 (not a bench line)")
     ap.add_argument("--precision-report", action="store_true",

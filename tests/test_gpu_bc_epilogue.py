@@ -1,4 +1,5 @@
-"""The BC epilogue of the planned collision (vfb_collision_plan_set_bc_epilogue):
+"""The BC epilogue of the planned collision (vfb_collision_plan_set_bc_epilogue,
+an option of the simulation, off by default):
 a simulation whose collision applies the post-collision BCs of its wall nodes
 itself equals, bit for bit, the same simulation with separate BC launches for
 every entry -- the entries read the same post-collision values and write

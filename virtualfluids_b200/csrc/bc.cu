@@ -72,8 +72,11 @@ __global__ void bcLocationsKernel(const int32_t* __restrict__ bcK, uint32_t n, c
         out[(unsigned long long)l * n + i] = L.k[l];
 }
 
+// six resident blocks of 128 threads: the gathers of a wall entry are DRAM
+// bursts, so more of them in flight matter more than the few registers the
+// 80-register bound spills
 template <class S, int KIND, bool EVEN>
-__global__ void __launch_bounds__(128) bcPostKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
+__global__ void __launch_bounds__(128, 6) bcPostKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
                                                      const int32_t* __restrict__ bcK,
                                                      const typename Storage<S>::R* __restrict__ q, uint32_t nBC,
                                                      const typename Storage<S>::R* __restrict__ Vx,

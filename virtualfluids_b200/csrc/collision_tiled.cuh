@@ -219,7 +219,7 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
 // consumers.  Every warp waits on "full", moves its 32 nodes' values into
 // registers, arrives on "empty", then collides and stores.  Warps never wait
 // for each other otherwise.
-template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> a)
 {
     using R = typename Storage<S>::R;
@@ -326,8 +326,9 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                     Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
             }
             // the node's post-collision BCs, from the values this thread just stored
-            if (a.epi && __ldg(a.epiTiles + t0 + j * stride))
-                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, k);
+            if constexpr (EPI)
+                if (__ldg(a.epiTiles + t0 + j * stride))
+                    bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, k);
         }
     }
 }
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
 // loads and stores without predicates, the second node's address an
 // immediate offset from the first's.  Other warps take the general path:
 // per-lane predicates and the lanes' location offsets.
-template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<S> a)
 {
     constexpr int HALF = C::T / 2;
@@ -493,11 +494,13 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
         }
     }
     // the nodes' post-collision BCs, from the values this thread just stored
-    if (a.epi && __ldg(a.epiTiles + blockIdx.x)) {
-        if (actA)
-            bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kA);
-        if (actB)
-            bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kB);
+    if constexpr (EPI) {
+        if (__ldg(a.epiTiles + blockIdx.x)) {
+            if (actA)
+                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kA);
+            if (actB)
+                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kB);
+        }
     }
 }
 
@@ -613,7 +616,7 @@ struct vfb_collision_plan_impl {
     unsigned long long epiCount[2] = { 0, 0 }; // nodes, records
 };
 
-template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
+template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
     if constexpr (C::KIND == 1) {
@@ -634,32 +637,50 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
         asyncKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, smem, stream>>>(a);
         return checkLaunch("pipelined planned collision");
     } else if constexpr (C::STAGES == 1 && sizeof(S) <= 4) {
-        pairKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T / 2, 0, stream>>>(a);
+        pairKernel<S, C, EVEN, OP, WM, BF, EPI><<<a.nTiles, C::T / 2, 0, stream>>>(a);
         return checkLaunch("paired planned collision");
     } else if constexpr (C::STAGES == 1) {
         // the paired form computes in FP32: FP64 storage uses the staged kernel
         // of the same tile width (same metadata layout and copy geometry)
-        return launchTiledT<S, TileCfg<S, C::T, 2, 3>, EVEN, OP, WM, BF>(a, stream);
+        return launchTiledT<S, TileCfg<S, C::T, 2, 3>, EVEN, OP, WM, BF, EPI>(a, stream);
     } else if constexpr (C::STAGES == 0) {
         directKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T, 0, stream>>>(a);
         return checkLaunch("direct planned collision");
     } else {
     static int blocks = 0;
     if (blocks == 0) {
-        cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, C, EVEN, OP, WM, BF>,
+        cudaError_t e = cudaFuncSetAttribute(tiledKernel<S, C, EVEN, OP, WM, BF, EPI>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES);
         if (e != cudaSuccess)
             return setError(VFB_ERR_CUDA, "tiled kernel shared memory attribute: %s", cudaGetErrorString(e));
         int perSM = 0, device = 0, sms = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, C, EVEN, OP, WM, BF>, C::T,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, tiledKernel<S, C, EVEN, OP, WM, BF, EPI>, C::T,
                                                       C::SMEM_BYTES);
         blocks = std::max(1, perSM) * sms;
     }
     const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
-    tiledKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, C::SMEM_BYTES, stream>>>(a);
+    tiledKernel<S, C, EVEN, OP, WM, BF, EPI><<<std::max(1u, grid), C::T, C::SMEM_BYTES, stream>>>(a);
     return checkLaunch("tiled collision");
+    }
+}
+
+// the kernels with the BC epilogue, compiled for the default K17 template and
+// BGK (the schedule's passes); the epilogue exists for the paired and staged kernels
+template <class S, class C>
+static int launchEpilogue(Op op, bool even, int tmpl, const TiledArgs<S>& a, cudaStream_t stream)
+{
+    if constexpr (C::KIND == 1 || C::STAGES == 0) {
+        return setError(VFB_ERR_UNSUPPORTED, "this tile configuration has no BC epilogue");
+    } else {
+        if (op == Op::BGK)
+            return even ? launchTiledT<S, C, true, Op::BGK, false, false, true>(a, stream)
+                        : launchTiledT<S, C, false, Op::BGK, false, false, true>(a, stream);
+        if (tmpl != VFB_TEMPLATE_DEFAULT)
+            return setError(VFB_ERR_UNSUPPORTED, "the BC epilogue runs with the default collision template");
+        return even ? launchTiledT<S, C, true, Op::K17, false, false, true>(a, stream)
+                    : launchTiledT<S, C, false, Op::K17, false, false, true>(a, stream);
     }
 }
 
@@ -680,6 +701,8 @@ static int dispatchTiled(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t s
         a.lastSrc[d] = a.dist + ((27ull * a.N - a.bytes[d] / sizeof(S)) / C::E) * C::E;
         a.totalBytes += a.bytes[d];
     }
+    if (a.epi)
+        return launchEpilogue<S, C>(op, even, tmpl, a, stream);
     if (op == Op::BGK)
         return even ? launchTiledT<S, C, true, Op::BGK, false, false>(a, stream)
                     : launchTiledT<S, C, false, Op::BGK, false, false>(a, stream);
@@ -721,6 +744,8 @@ static int dispatchTuning(Op op, bool even, int tmpl, TiledArgs<S>& a, uint32_t 
         a.lastSrc[d] = a.dist + ((27ull * a.N - a.bytes[d] / sizeof(S)) / C::E) * C::E;
         a.totalBytes += a.bytes[d];
     }
+    if (a.epi)
+        return launchEpilogue<S, C>(op, even, tmpl, a, stream);
     if (op == Op::BGK)
         return even ? launchTiledT<S, C, true, Op::BGK, false, false>(a, stream)
                     : launchTiledT<S, C, false, Op::BGK, false, false>(a, stream);

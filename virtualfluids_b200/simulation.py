@@ -136,9 +136,11 @@ class Parameter:
         # are divided by it (GridGenerator.cpp:507-513)
         self.velocity_ratio = 1.0
         self.has_wall_model_monitor = False
-        # the planned collision applies the post-collision BCs of its wall
-        # nodes itself (same result, no separate pass over those entries)
-        self.use_bc_epilogue = True
+        # True: the planned collision applies the post-collision BCs of its
+        # wall nodes itself (the same result).  Off by default: measured slower
+        # on B200 (an x-face wall puts one BC node in every row, so the
+        # epilogue runs in one lane of most warps)
+        self.use_bc_epilogue = False
         self.initial_condition = None
 
     def set_viscosity_LB(self, viscosity: float):
