@@ -343,6 +343,14 @@ class ReferenceGpu(_Lib):
         for name in ("vfref_gpu_scale_cf", "vfref_gpu_scale_fc"):
             self.fn(name).argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c.c_ulonglong, _c.c_ulonglong, _c.c_int,
                                       _vp, _vp, _c.c_uint, R, R, _vp, _vp, _vp, _vp]
+        self.fn("vfref_gpu_enstrophy").argtypes = [_vp] * 11 + [_c.c_ulonglong, _vp]
+
+    def enstrophy(self, vx, vy, vz, rho, nx, ny, nz, nneg, geo, enstrophy, is_fluid, stream=0):
+        """enstrophyKernel of EnstrophyAnalyzer.cu over all nodes (device tensors;
+        enstrophy and is_fluid zero-initialised)."""
+        self._check(self.fn("vfref_gpu_enstrophy")(
+            *[_dptr(t) for t in (vx, vy, vz, rho, nx, ny, nz, nneg, geo, enstrophy, is_fluid)], geo.numel(),
+            _vp(stream)), "enstrophyKernel")
 
     @staticmethod
     def _check(rc: int, what: str) -> None:

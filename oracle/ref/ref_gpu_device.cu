@@ -41,6 +41,11 @@ __global__ void scaleFineToCoarseCompressible_Device(real*, real*, unsigned int*
                                                      unsigned long long, bool, unsigned int*, unsigned int*,
                                                      unsigned int, real, real, real*, real*, ICellNeigh);
 
+// EnstrophyAnalyzer.cu:101-110 (the kernel; the file is compiled unmodified)
+__global__ void enstrophyKernel(real* veloX, real* veloY, real* veloZ, real* rho, uint* neighborX, uint* neighborY,
+                                uint* neighborZ, uint* neighborWSB, uint* geo, real* enstrophy, uint* isFluid,
+                                unsigned long long numberOfLBnodes);
+
 namespace
 {
 constexpr unsigned kThreads = 64; // Parameter.cpp:400 (numberofthreads)
@@ -151,6 +156,18 @@ int REF(vfref_gpu_scale_fc)(real* distC, real* distF, unsigned* nxC, unsigned* n
     scaleFineToCoarseCompressible_Device<false><<<referenceGrid(nCells), kThreads, 0, asStream(stream)>>>(
         distC, distF, nxC, nyC, nzC, nxF, nyF, nzF, NC, NF, isEven != 0, coarseCells, fineCells, nCells, omegaC,
         omegaF, nullptr, nullptr, off);
+    return (int)cudaGetLastError();
+}
+
+// the kernel of EnstrophyAnalyzer::run (EnstrophyAnalyzer.cu:69-82): per node its
+// enstrophy term and fluid flag into the zero-initialised arrays enstrophy and
+// isFluid, one thread per node, launched as CudaGrid(numberofthreads, N) sizes it
+int REF(vfref_gpu_enstrophy)(real* vx, real* vy, real* vz, real* rho, unsigned* nx, unsigned* ny, unsigned* nz,
+                              unsigned* nNeg, unsigned* geo, real* enstrophy, unsigned* isFluid, unsigned long long N,
+                              void* stream)
+{
+    enstrophyKernel<<<referenceGrid((unsigned)N), kThreads, 0, asStream(stream)>>>(vx, vy, vz, rho, nx, ny, nz, nNeg,
+                                                                                   geo, enstrophy, isFluid, N);
     return (int)cudaGetLastError();
 }
 

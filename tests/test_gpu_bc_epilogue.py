@@ -1,9 +1,12 @@
 """The BC epilogue of the planned collision (vfb_collision_plan_set_bc_epilogue,
 an option of the simulation, off by default):
 a simulation whose collision applies the post-collision BCs of its wall nodes
-itself equals, bit for bit, the same simulation with separate BC launches for
-every entry -- the entries read the same post-collision values and write
-cells nobody else touches in the step.  Cavity (all six walls), channel
+itself equals the same simulation with separate BC launches for every entry
+-- the entries read the same post-collision values and write cells nobody
+else touches in the step.  The collision kernel with the epilogue is a
+separate compilation of the same source, which may round a few FP32
+operations differently: FP64 is compared bit for bit, FP32 and the 16-bit
+storages to a bound far below the size of a wrong boundary value.  Cavity (all six walls), channel
 (inlet, outlet, no-slip floor, slip lid), the sphere channel (geometry list
 with fractional q, whose clipping links keep some nodes out of the
 epilogue), the two-level cube channel, every storage."""
@@ -92,9 +95,11 @@ def test_epilogue_equals_separate_launches(cuda, storage, case):
     b, sb = _run(grid, storage, False, steps)
     assert sum(s[0] for s in sa) > 0, sa       # the epilogue took nodes
     assert all(s[0] == 0 for s in sb)
+    tol = {"fp64": 0.0, "fp32": 1e-5, "fp16": 2e-3, "fx16": 3e-3}[storage]
     for lvl in range(len(a)):
         for x, y in zip(a[lvl], b[lvl]):
-            assert np.array_equal(x, y), (case, storage, lvl)
+            scale = max(np.abs(y).max(), 1e-300)
+            assert np.abs(x.astype(np.float64) - y).max() <= tol * scale, (case, storage, lvl)
     if case == "sphere_channel":
         # the clipping links of the sphere keep some geometry entries out
         assert sa[0][2] > 0
@@ -107,4 +112,4 @@ def test_epilogue_with_bounce_back_kinds(cuda):
     b, _ = _run(grid, "fp32", False, 7, **kw)
     assert sa[0][0] > 0
     for x, y in zip(a[0], b[0]):
-        assert np.array_equal(x, y)
+        assert np.abs(x.astype(np.float64) - y).max() <= 1e-5 * np.abs(y).max()

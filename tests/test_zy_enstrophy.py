@@ -56,3 +56,39 @@ def test_simulation_enstrophy_matches_oracle(cuda):
     assert count == int(counted.sum()) > 0
     ref = vals[counted].sum() / count
     assert abs(mean - ref) <= 1e-8 * abs(ref)
+
+
+@pytest.mark.parametrize("grid", ["channel", "cube_channel", "sphere_channel", "tgv8"])
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-12), ("f32", 2e-6)])
+def test_oracle_enstrophy_matches_reference_kernel(cuda, grid, precision, tol):
+    """Pins the oracle's enstrophy restatement to the reference's own kernel:
+    EnstrophyAnalyzer.cu compiled unmodified for sm_100a (oracle/_ref), run on
+    the same fields; the per-node values and the fluid flags against the
+    oracle's (the node function has no transcendental, so FP64 agrees to the
+    rounding of contracted multiply-adds)."""
+    from oracle.pyoracle import ReferenceGpu, ref_gpu_available
+
+    if not ref_gpu_available(precision):
+        pytest.skip("the reference's GPU kernels were not built (oracle/_ref)")
+    g = _level0(grid)
+    O = Oracle(precision)
+    rng = np.random.default_rng(13)
+    N = len(g["geo"])
+    fields = [rng.uniform(-0.02, 0.02, N).astype(O.real) for _ in range(4)]  # rho, vx, vy, vz
+    vals, counted = O.enstrophy_nodes(*fields, g["geo"], g["neighborX"], g["neighborY"], g["neighborZ"],
+                                      g["neighborNeg"])
+    dt = torch.float64 if precision == "f64" else torch.float32
+    t = {name: torch.from_numpy(np.ascontiguousarray(g[name]).astype(np.uint32)).cuda()
+         for name in ("geo", "neighborX", "neighborY", "neighborZ", "neighborNeg")}
+    rho, vx, vy, vz = (torch.from_numpy(a).to("cuda", dt) for a in fields)
+    ens = torch.zeros(N, dtype=dt, device="cuda")
+    flag = torch.zeros(N, dtype=torch.int32, device="cuda")
+    ReferenceGpu(precision).enstrophy(vx, vy, vz, rho, t["neighborX"], t["neighborY"], t["neighborZ"],
+                                      t["neighborNeg"], t["geo"], ens, flag)
+    torch.cuda.synchronize()
+    ref_vals = ens.cpu().numpy().astype(np.float64)
+    ref_flag = flag.cpu().numpy() != 0
+    assert np.array_equal(ref_flag, counted.astype(bool))
+    assert ref_flag.sum() > 0
+    v = vals.astype(np.float64)
+    assert np.abs(v - ref_vals).max() <= tol * np.abs(ref_vals).max()
