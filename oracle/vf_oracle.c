@@ -28,10 +28,12 @@
  * bit for bit against the reference's own sources compiled on the host
  * (oracle/Makefile, target ref), and tests/golden/ holds fixtures generated
  * from that build so the pin also runs where the reference tree is absent.
- * One exception, parity unpinned: vfo_enstrophy_nodes restates
+ * One function is pinned on the GPU instead: vfo_enstrophy_nodes restates
  * EnstrophyAnalyzer.cu by reading, because that file (a kernel launch and
  * thrust device vectors beside the node function) does not build for the
- * host; tests/test_enstrophy_host.py checks it against analytic curls.
+ * host; tests/test_zy_enstrophy.py compares it with the reference's
+ * enstrophyKernel compiled unmodified for sm_100a (oracle/Makefile, target
+ * refgpu), and tests/test_enstrophy_host.py against analytic curls.
  *
  * Compiled twice by oracle/Makefile: -DVFO_REAL=double (suffix _f64) and
  * -DVFO_REAL=float (suffix _f32), always with -ffp-contract=off so that no
