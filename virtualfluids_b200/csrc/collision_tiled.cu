@@ -91,11 +91,6 @@ static const TileConfigInfo kTileConfigs[] = {
     { 256, 1, 5, false },
     // paired, six resident blocks (80 registers)
     { 256, 1, 6, false },
-    // staged FP64, four resident blocks (128 registers; four 56 KB stage pairs fill the SM's shared memory)
-    { 128, 2, 4, true },
-    // staged paired (bulk-copy stages feeding the paired arithmetic): 2 stages 4 blocks, 3 stages 4 blocks,
-    // 2 stages 5 blocks
-    { 256, 2, 4, false }, { 256, 3, 4, false }, { 256, 2, 5, false },
 };
 static constexpr int kNumTileConfigs = (int)(sizeof(kTileConfigs) / sizeof(kTileConfigs[0]));
 
@@ -385,10 +380,10 @@ cudaError_t download(std::vector<T>& v, const void* src, size_t n, cudaStream_t 
 }
 
 // the tile configurations whose kernels run the BC epilogue: the paired
-// kernels (one stage) and the staged kernels (entries 0-6 and 21)
+// kernels (one stage) and the staged kernels (entries 0-6)
 bool epilogueConfig(int c)
 {
-    return (c >= 0 && c <= 6) || c == 12 || c == 13 || c == 14 || c == 19 || c == 20 || c == 21;
+    return (c >= 0 && c <= 6) || c == 12 || c == 13 || c == 14 || c == 19 || c == 20;
 }
 } // namespace
 

@@ -504,154 +504,6 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
     }
 }
 
-// Staged paired form (KIND 2, 4- and 2-byte storage): the staged kernel's
-// pipeline -- thread 0 of a persistent block issues a tile's 27 bulk copies
-// into a shared-memory stage STAGES - 1 tiles ahead -- feeding the paired
-// kernel's arithmetic: C::T / 2 threads per T-node tile, thread t collides
-// the tile's nodes t and T / 2 + t as one register pair.  A warp reads its
-// 64 nodes' values from the stage (wrap lanes read their wrapped locations in
-// global memory), releases the stage and then collides, so the load latency
-// of the next tile is hidden behind the arithmetic without more registers.
-template <class S, class C, bool EVEN, Op OP>
-__global__ void __launch_bounds__(C::T / 2, C::MINB) stagedPairKernel(const TiledArgs<S> a)
-{
-    constexpr int HALF = C::T / 2;
-    constexpr int W2 = HALF / 32; // warps of a block = mask words of one half
-    constexpr int WARPS = C::T / 32;
-    constexpr int ST = C::STAGES;
-    using St = Storage<S>;
-    extern __shared__ __align__(128) unsigned char smemRaw[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smemRaw + ST * C::STAGE_BYTES);
-    uint64_t* empty = full + ST;
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        for (int i = 0; i < ST; ++i) {
-            tma::mbarInit(&full[i], 1);
-            tma::mbarInit(&empty[i], W2);
-        }
-        tma::fenceBarrierInit();
-    }
-    __syncthreads();
-
-    const uint32_t t0 = blockIdx.x, stride = gridDim.x;
-    if (t0 >= a.nTiles)
-        return;
-    const uint32_t mine = (a.nTiles - t0 + stride - 1) / stride;
-    auto k0Of = [&](uint32_t j) { return tma::ldgOrdered(a.meta + (size_t)(t0 + j * stride) * C::META_WORDS); };
-    uint32_t pk0 = 0;
-    if (tid == 0) {
-        const uint32_t pre = mine < (uint32_t)(ST - 1) ? mine : (uint32_t)(ST - 1);
-        for (uint32_t q = 0; q < pre; ++q)
-            issueTile<S, C>(a, t0 + q * stride, k0Of(q), smemRaw, (int)q, full);
-        if ((uint32_t)(ST - 1) < mine)
-            pk0 = k0Of(ST - 1);
-    }
-    bool failed = false;
-
-    for (uint32_t j = 0; j < mine; ++j) {
-        const int s = (int)(j % ST);
-        if (tid == 0) {
-            const uint32_t q = j + ST - 1;
-            if (q < mine) {
-                const int sq = (int)(q % ST);
-                if (q >= (uint32_t)ST && !tma::mbarWait(&empty[sq], ((q - ST) / ST) & 1u, kWaitLimit))
-                    failed = true;
-                if (!failed) {
-                    tma::fenceProxyAsync();
-                    issueTile<S, C>(a, t0 + q * stride, pk0, smemRaw, sq, full);
-                }
-                if (q + 1 < mine)
-                    pk0 = k0Of(q + 1);
-            }
-        }
-        const bool ok = tma::mbarWait(&full[s], (j / ST) & 1u, kWaitLimit);
-        if (!__all_sync(0xffffffffu, ok) || __any_sync(0xffffffffu, failed)) {
-            if (lane == 0)
-                atomicExch(a.errorFlag, 1);
-            return;
-        }
-        const unsigned char* stage = smemRaw + s * C::STAGE_BYTES;
-        const uint32_t* meta = reinterpret_cast<const uint32_t*>(stage + C::DATA_BYTES);
-        const uint32_t maskA = meta[4 + warp], maskB = meta[4 + W2 + warp];
-        const bool actA = (maskA >> lane) & 1u, actB = (maskB >> lane) & 1u;
-        const uint32_t k0 = meta[0];
-        const uint32_t kA = k0 + tid, kB = k0 + HALF + tid;
-        const uint32_t wf = meta[1];
-        const bool wrap = (((wf >> warp) | (wf >> (W2 + warp))) & 1u) != 0;
-        int wbA = 0, wbB = 0;
-        if (wrap) {
-            auto bitsOf = [&](int word) {
-                return (int)((meta[4 + WARPS + word] >> lane) & 1u) |
-                       (int)(((meta[4 + 2 * WARPS + word] >> lane) & 1u) << 1) |
-                       (int)(((meta[4 + 3 * WARPS + word] >> lane) & 1u) << 2);
-            };
-            wbA = bitsOf(warp);
-            wbB = bitsOf(W2 + warp);
-        }
-        const S* st = reinterpret_cast<const S*>(stage) + tid;
-        F2 f[27];
-        if (!wrap) {
-#pragma unroll
-            for (int d = 0; d < 27; ++d)
-                f[d] = F2(actA ? St::loadRaw(st + a.smemOff[d]) : 0.0f, actB ? St::loadRaw(st + a.smemOff[d] + HALF) : 0.0f);
-        } else {
-            const LaneOffsets oA = laneOffsets(a, wbA), oB = laneOffsets(a, wbB);
-#pragma unroll
-            for (int d = 0; d < 27; ++d) {
-                const int l = loc(d);
-                const float x = !actA ? 0.0f
-                                      : (l & wbA) ? St::loadRaw(a.sbase[d] + locIndex(kA, oA, l))
-                                                  : St::loadRaw(st + a.smemOff[d]);
-                const float y = !actB ? 0.0f
-                                      : (l & wbB) ? St::loadRaw(a.sbase[d] + locIndex(kB, oB, l))
-                                                  : St::loadRaw(st + a.smemOff[d] + HALF);
-                f[d] = F2(x, y);
-            }
-        }
-        __syncwarp();
-        if (lane == 0)
-            tma::mbarArrive(&empty[s]);
-        if (!(actA || actB))
-            continue;
-        if (St::scaled) {
-#pragma unroll
-            for (int d = 0; d < 27; ++d)
-                f[d] = f[d] * F2(St::invScale(d));
-        }
-        F2 drho, ux, uy, uz;
-        if constexpr (OP == Op::K17)
-            k17Collide<F2>(f, a.rates2, a.fx2, a.fy2, a.fz2, drho, ux, uy, uz);
-        else
-            bgkCollide<F2>(f, a.rates2.omega);
-        if (St::scaled) {
-#pragma unroll
-            for (int d = 0; d < 27; ++d)
-                f[d] = f[d] * F2(St::scale(d));
-        }
-        if (!wrap && (maskA & maskB) == 0xffffffffu) {
-#pragma unroll
-            for (int d = 0; d < 27; ++d) {
-                S* p = a.gbase[d] + kA;
-                const F2 v = f[inv(d)];
-                St::storeRaw(p, v.v.x);
-                St::storeRaw(p + HALF, v.v.y);
-            }
-        } else {
-            const LaneOffsets oA = laneOffsets(a, wbA), oB = laneOffsets(a, wbB);
-#pragma unroll
-            for (int d = 0; d < 27; ++d) {
-                const int l = loc(d);
-                const F2 v = f[inv(d)];
-                if (actA)
-                    St::storeRaw(a.sbase[d] + locIndex(kA, oA, l), v.v.x);
-                if (actB)
-                    St::storeRaw(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
-            }
-        }
-    }
-}
-
 // Per-thread pipelined form (KIND 1, 4- and 8-byte storage): a persistent
 // grid; every thread owns one lane of every tile its block visits and
 // prefetches the 27 values of its node of the next tile with cp.async into
@@ -767,25 +619,7 @@ struct vfb_collision_plan_impl {
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 {
-    if constexpr (C::KIND == 2) {
-        static int blocks = 0;
-        if (blocks == 0) {
-            cudaError_t e = cudaFuncSetAttribute(stagedPairKernel<S, C, EVEN, OP>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES);
-            if (e != cudaSuccess)
-                return setError(VFB_ERR_CUDA, "staged paired kernel shared memory attribute: %s",
-                                cudaGetErrorString(e));
-            int perSM = 0, device = 0, sms = 0;
-            cudaGetDevice(&device);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, stagedPairKernel<S, C, EVEN, OP>, C::T / 2,
-                                                          C::SMEM_BYTES);
-            blocks = std::max(1, perSM) * sms;
-        }
-        const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
-        stagedPairKernel<S, C, EVEN, OP><<<std::max(1u, grid), C::T / 2, C::SMEM_BYTES, stream>>>(a);
-        return checkLaunch("staged paired collision");
-    } else if constexpr (C::KIND == 1) {
+    if constexpr (C::KIND == 1) {
         static int blocks = 0;
         constexpr int smem = 2 * 27 * C::T * (int)sizeof(S);
         if (blocks == 0) {
@@ -837,7 +671,7 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
 template <class S, class C>
 static int launchEpilogue(Op op, bool even, int tmpl, const TiledArgs<S>& a, cudaStream_t stream)
 {
-    if constexpr (C::KIND != 0 || C::STAGES == 0) {
+    if constexpr (C::KIND == 1 || C::STAGES == 0) {
         return setError(VFB_ERR_UNSUPPORTED, "this tile configuration has no BC epilogue");
     } else {
         if (op == Op::BGK)
@@ -969,7 +803,6 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 11: return dispatchTuning<S, TileCfg<S, 128, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 17: return dispatchTuning<S, TileCfg<S, 128, 2, 3, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 18: return dispatchTuning<S, TileCfg<S, 128, 2, 2, 1>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
-        case 21: return dispatchTuning<S, TileCfg<S, 128, 2, 4>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         default: return dispatchTiled<S, TileCfg<S, 128, 2, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         }
     } else {
@@ -993,9 +826,6 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
         case 13: return dispatchTiled<S, TileCfg<S, 256, 1, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 14: return dispatchTiled<S, TileCfg<S, 256, 1, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 19: return dispatchTiled<S, TileCfg<S, 256, 1, 5>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
-        case 22: return dispatchTuning<S, TileCfg<S, 256, 2, 4, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
-        case 23: return dispatchTuning<S, TileCfg<S, 256, 3, 4, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
-        case 24: return dispatchTuning<S, TileCfg<S, 256, 2, 5, 2>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 20: return dispatchTiled<S, TileCfg<S, 256, 1, 6>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 8: return dispatchTuning<S, TileCfg<S, 256, 0, 3>>(op, even, t, a, p.sy, p.sz, p.metaWords, stream);
         case 9:
