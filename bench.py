@@ -905,12 +905,14 @@ def adjoint_report(args):
     """The adjoint form: the channel of 128 x 64 x 64 nodes (12^3 cube at x =
     40, parabolic inlet profile with +-2% noise, pressure outlet, no-slip
     walls, g = (1e-6, 0, 0), nu = 0.02), K17, T = --steps (default 1000) time
-    steps with a checkpoint every 32, objective J = mean u_x over the 16^3 box
-    x in [80, 96).  Per storage (FP32, FP64): the plain forward step through
-    the Simulation API (graph replay), the adjoint's forward pass (with
-    checkpoints) and its backward pass (recompute with tapes, then the adjoint
-    kernels), all event-timed per step, and the backward / forward ratio.
-    One JSON line."""
+    steps, objective J = mean u_x over the 16^3 box x in [80, 96).  Per
+    storage (FP32, FP64): the plain forward step through the Simulation API
+    (graph replay), then for two schedules the adjoint's forward pass and its
+    backward pass, all event-timed per step, with the backward / forward
+    ratio: "checkpointed" keeps a state every 32 steps and recomputes each
+    segment with tapes backwards; "taped" (checkpoint interval = T, when its
+    tapes fit in device memory) records the tapes in the forward pass and
+    recomputes nothing.  One JSON line."""
     import numpy as np
     import torch
 
@@ -919,22 +921,20 @@ def adjoint_report(args):
     from virtualfluids_b200.workloads import adjoint_channel, inlet_entries, inlet_profile, initial_fields, objective_box
 
     steps = args.steps if args.steps != 50 else 1000
+    force = (1e-6, 0.0, 0.0)
     rows = {}
     for storage in ("fp32", "fp64"):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(0.02)
-        p.set_forcing(1e-6, 0.0, 0.0)
+        p.set_forcing(*force)
         bc = BoundaryConditionFactory()
         bc.set_geometry_boundary_condition(NoSlipBC.NoSlipInterpolatedCompressible)
         bc.set_pressure_boundary_condition(PressureBC.PressureNonEquilibriumCompressible)
         sim = Simulation(p, adjoint_channel(), bc)
         g = sim.levels[0]
         nodes, w = objective_box(g, 80, 96, 24, 40, 24, 40)
-        pb = FlowProblem(sim, inlet_entries(g), initial_fields(g), steps, 32, nodes, (w, None, None))
         prof = inlet_profile(g)
-        pb.evaluate(prof, (1e-6, 0.0, 0.0))  # warm-up: allocations, first launches
-        pb.gradient(1.0)
         stream = torch.cuda.current_stream()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         sim.init_level(0, *initial_fields(g))
@@ -944,28 +944,48 @@ def adjoint_report(args):
         sim.run(steps)
         ev[1].record(stream)
         torch.cuda.synchronize()
-        sim.init_level(0, *initial_fields(g))
-        torch.cuda.synchronize()
-        ev[2].record(stream)
-        J = sim.adjoint_forward(steps, 32, nodes, w)
-        ev[3].record(stream)
-        ev[4].record(stream)
-        dv, df = sim.adjoint_backward(1.0)
-        ev[5].record(stream)
-        torch.cuda.synchronize()
         fwd = ev[0].elapsed_time(ev[1]) / steps
-        afwd = ev[2].elapsed_time(ev[3]) / steps
-        bwd = ev[4].elapsed_time(ev[5]) / steps
-        rows[storage] = {"forward_ms_per_step": fwd, "adjoint_forward_ms_per_step": afwd,
-                         "adjoint_backward_ms_per_step": bwd, "backward_over_forward": bwd / fwd,
-                         "gradient_over_forward": (afwd + bwd) / fwd, "J": J,
-                         "dJ_dg": [float(x) for x in df],
-                         "dJ_dinlet_norm": float(np.linalg.norm(dv[0][inlet_entries(g)])),
-                         "fluid_nodes": len(g["fluid"])}
+        row = {"forward_ms_per_step": fwd, "fluid_nodes": len(g["fluid"])}
+        # tape and BC records of one segment of T steps (27 values per fluid node, BC node and step)
+        real = 8 if storage == "fp64" else 4
+        bc_nodes = len(g["velocity.k"]) + len(g["geometry.k"]) + int(np.sum(g["pressure.count"]))
+        tape_bytes = 27 * real * steps * (len(g["fluid"]) + bc_nodes)
+        free = torch.cuda.mem_get_info()[0]
+        schedules = [("checkpointed", 32)]
+        if tape_bytes < 0.85 * free:
+            schedules.append(("taped", steps))
+        else:
+            row["taped"] = {"skipped": f"tapes of {tape_bytes / 1e9:.1f} GB exceed 85% of the free "
+                                       f"{free / 1e9:.1f} GB"}
+        for name, interval in schedules:
+            pb = FlowProblem(sim, inlet_entries(g), initial_fields(g), steps, interval, nodes, (w, None, None))
+            pb.evaluate(prof, force)  # warm-up: allocations, first launches, segment graphs
+            pb.gradient(1.0)
+            sim.init_level(0, *initial_fields(g))
+            torch.cuda.synchronize()
+            ev[2].record(stream)
+            J = sim.adjoint_forward(steps, interval, nodes, w)
+            ev[3].record(stream)
+            ev[4].record(stream)
+            dv, df = sim.adjoint_backward(1.0)
+            ev[5].record(stream)
+            torch.cuda.synchronize()
+            afwd = ev[2].elapsed_time(ev[3]) / steps
+            bwd = ev[4].elapsed_time(ev[5]) / steps
+            row[name] = {"checkpoint_interval": interval, "schedule": sim.adjoint_schedule(),
+                         "adjoint_forward_ms_per_step": afwd, "adjoint_backward_ms_per_step": bwd,
+                         "backward_over_forward": bwd / fwd, "gradient_over_forward": (afwd + bwd) / fwd,
+                         "J": J, "dJ_dg": [float(x) for x in df],
+                         "dJ_dinlet_norm": float(np.linalg.norm(dv[0][inlet_entries(g)]))}
+            if name == "taped":
+                row[name]["tape_gb"] = tape_bytes / 1e9
+        rows[storage] = row
         sim.close()
+        del sim
+        torch.cuda.empty_cache()
     print(json.dumps({"report": "adjoint form", "workload": "channel 128x64x64, 12^3 cube at x=40, parabolic inlet "
                       "(peak 0.04, +-2% noise), pressure outlet, no-slip walls, g=(1e-6,0,0), nu=0.02, K17",
-                      "steps": steps, "checkpoint_interval": 32, "objective": "mean u_x over x in [80,96), 16^3 box",
+                      "steps": steps, "objective": "mean u_x over x in [80,96), 16^3 box",
                       "results": rows}), flush=True)
     return 0
 

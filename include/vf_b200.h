@@ -529,14 +529,22 @@ int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream
  *                            (c = 0, 1, 2 for x, y, z; n entries; host array),
  *     dForces[c]           = dL / d(global force c)   (host array of 3),
  * by recomputing each checkpoint segment with taped inputs and running the
- * hand-written adjoint kernels backwards through it.  Either output may be
- * NULL.  Both calls synchronise the stream.  Device memory: a state copy per
- * checkpoint, and per segment 27 values per fluid node and per BC node and step.
+ * hand-written adjoint kernels backwards through it.  With checkpointInterval
+ * >= steps the run is one segment and the forward pass records the tapes
+ * itself, so the backward pass recomputes nothing (the same tape memory).
+ * Either output may be NULL.  Both calls synchronise the stream.  Device
+ * memory: a state copy per checkpoint, and per segment 27 values per fluid
+ * node and per BC node and step.
  */
 int vfb_sim_adjoint_forward(vfb_simulation* sim, unsigned int steps, unsigned int checkpointInterval,
                             const uint32_t* objectiveNodes, const double* wx, const double* wy, const double* wz,
                             uint32_t numberOfObjectiveNodes, double* J, void* stream);
 int vfb_sim_adjoint_backward(vfb_simulation* sim, double seed, double* dVelocity, double* dForces, void* stream);
+/* the schedule of the last vfb_sim_adjoint_forward: out2[0] = 1 when the
+ * velocity, no-slip and geometry lists run in one launch per step (no list
+ * writes a cell another list reads or writes), out2[1] = 1 when the forward
+ * pass taped its only segment (the backward pass recomputes nothing) */
+int vfb_sim_adjoint_schedule(const vfb_simulation* sim, int* out2);
 /* Parameter::setForcing (Parameter.cpp:463) on a running simulation (the next steps use
  * the new global force); no reference counterpart as an in-run setter */
 int vfb_sim_set_forces(vfb_simulation* sim, const double* forces3);

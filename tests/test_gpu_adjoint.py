@@ -120,6 +120,33 @@ def test_flow_objective_autograd_function(cuda):
     sim.close()
 
 
+def test_schedules_give_the_same_gradient(cuda, monkeypatch):
+    """The checkpointed schedule (each segment recomputed with tapes), the
+    taped one (interval >= steps: the forward pass records the tapes) and one
+    launch per BC list instead of the lists together give the same J (bit for
+    bit: the same forward arithmetic) and the same gradients (to the order of
+    the scatters' atomic additions)."""
+    out = []
+    for separate, interval in ((True, 5), (False, 5), (False, 24), (False, 100), (True, 24)):
+        if separate:
+            monkeypatch.setenv("VFB_ADJOINT_SEPARATE_LISTS", "1")
+        else:
+            monkeypatch.delenv("VFB_ADJOINT_SEPARATE_LISTS", raising=False)
+        sim = make_sim(adjoint_channel_small())
+        pb = problem(sim, 24, interval, SMALL_BOX)
+        J = pb.evaluate(inlet_profile(sim.levels[0]), G)
+        dv, df = pb.gradient(1.0)
+        sched = sim.adjoint_schedule()
+        assert sched == {"lists_together": not separate, "taped_forward": interval >= 24}, sched
+        out.append((J, dv, df))
+        sim.close()
+    J0, dv0, df0 = out[0]
+    for J, dv, df in out[1:]:
+        assert J == J0
+        assert np.abs(dv - dv0).max() <= 1e-12 * np.abs(dv0).max()
+        assert np.abs(df - df0).max() <= 1e-12 * np.abs(df0).max()
+
+
 def test_small_channel_fp32_adjoint_close_to_fp64(cuda):
     out = []
     for storage in ("fp64", "fp32"):

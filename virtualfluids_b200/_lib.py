@@ -208,6 +208,7 @@ _SIGNATURES = [
       ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ("vfb_sim_adjoint_backward", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("vfb_sim_adjoint_schedule", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("vfb_sim_set_forces", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("vfb_sim_output", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,

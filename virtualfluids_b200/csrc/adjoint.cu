@@ -174,16 +174,14 @@ __global__ void __launch_bounds__(kThreads, MINB)
 }
 
 // --------------------------------------------------- post-collision BCs --
+// one entry of a forward post-collision list
 template <class R, int KIND, bool EVEN>
-__global__ void __launch_bounds__(kThreads)
-    postBCKernel(R* __restrict__ dist, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
-                 const uint32_t* __restrict__ table,
-                 const R* __restrict__ q, uint32_t n, const R* __restrict__ Vx, const R* __restrict__ Vy,
-                 const R* __restrict__ Vz, R* __restrict__ rec)
+__device__ __forceinline__ void postBCEntry(R* __restrict__ dist, const BcLattice<R>& lat,
+                                            const int32_t* __restrict__ bcK, const uint32_t* __restrict__ table,
+                                            const R* __restrict__ q, uint32_t n, const R* __restrict__ Vx,
+                                            const R* __restrict__ Vy, const R* __restrict__ Vz, R* __restrict__ rec,
+                                            uint32_t i)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
     const unsigned long long N = lat.N;
     const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     R g[27];
@@ -225,15 +223,23 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-template <class R, bool EVEN>
+template <class R, int KIND, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
-    postGatherKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+    postBCKernel(R* __restrict__ dist, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
                  const uint32_t* __restrict__ table,
-                     const R* __restrict__ q, uint32_t n, R* __restrict__ tmp)
+                 const R* __restrict__ q, uint32_t n, const R* __restrict__ Vx, const R* __restrict__ Vy,
+                 const R* __restrict__ Vz, R* __restrict__ rec)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
+    if (i < n)
+        postBCEntry<R, KIND, EVEN>(dist, lat, bcK, table, q, n, Vx, Vy, Vz, rec, i);
+}
+
+template <class R, bool EVEN>
+__device__ __forceinline__ void postGatherEntry(R* __restrict__ lam, const BcLattice<R>& lat,
+                                                const int32_t* __restrict__ bcK, const uint32_t* __restrict__ table,
+                                                const R* __restrict__ q, uint32_t n, R* __restrict__ tmp, uint32_t i)
+{
     const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     // all q values first: loads issued together, not one per loop iteration
     R qv[26];
@@ -253,16 +259,22 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-template <class R, int KIND, bool EVEN>
+template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads)
-    postScatterKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
-                 const uint32_t* __restrict__ table,
-                      const R* __restrict__ q, uint32_t n, const R* __restrict__ rec, const R* __restrict__ tmp,
-                      double* __restrict__ gV)
+    postGatherKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+                     const uint32_t* __restrict__ table, const R* __restrict__ q, uint32_t n, R* __restrict__ tmp)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
+    if (i < n)
+        postGatherEntry<R, EVEN>(lam, lat, bcK, table, q, n, tmp, i);
+}
+
+template <class R, int KIND, bool EVEN>
+__device__ __forceinline__ void postScatterEntry(R* __restrict__ lam, const BcLattice<R>& lat,
+                                                 const int32_t* __restrict__ bcK, const uint32_t* __restrict__ table,
+                                                 const R* __restrict__ q, uint32_t n, const R* __restrict__ rec,
+                                                 const R* __restrict__ tmp, double* __restrict__ gV, uint32_t i)
+{
     const Locs L = bcEntryLocations(table, i, n, bcK, lat.nX, lat.nY, lat.nZ);
     R g[27], gg[27];
 #pragma unroll
@@ -330,6 +342,76 @@ __global__ void __launch_bounds__(kThreads)
         gV[(unsigned long long)n + i] += (double)gUy;
         gV[2ull * n + i] += (double)gUz;
     }
+}
+
+template <class R, int KIND, bool EVEN>
+__global__ void __launch_bounds__(kThreads)
+    postScatterKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
+                      const uint32_t* __restrict__ table, const R* __restrict__ q, uint32_t n,
+                      const R* __restrict__ rec, const R* __restrict__ tmp, double* __restrict__ gV)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        postScatterEntry<R, KIND, EVEN>(lam, lat, bcK, table, q, n, rec, tmp, gV, i);
+}
+
+// ------------------------------------------ post-collision lists together --
+// One launch over several lists: block b serves the last list whose first
+// block is <= b.  Valid when no list writes a cell another list reads or
+// writes (the caller checks this once, sim_adjoint.cu), so the lists' order
+// within a step does not matter.
+template <class R>
+__device__ __forceinline__ const PostList<R>& listOf(const PostLists<R>& P, uint32_t& i)
+{
+    int l = 0;
+#pragma unroll
+    for (int j = 1; j < kMaxPostLists; ++j)
+        if (j < P.count && blockIdx.x >= P.firstBlock[j])
+            l = j;
+    i = (blockIdx.x - P.firstBlock[l]) * kThreads + threadIdx.x;
+    return P.list[l];
+}
+
+template <class R, bool EVEN>
+__global__ void __launch_bounds__(kThreads) postBCListsKernel(R* __restrict__ dist, const BcLattice<R> lat,
+                                                              const PostLists<R> P)
+{
+    uint32_t i;
+    const PostList<R>& L = listOf(P, i);
+    if (i >= L.n)
+        return;
+    if (L.kind == VFB_BC_VELOCITY_INTERPOLATED)
+        postBCEntry<R, VFB_BC_VELOCITY_INTERPOLATED, EVEN>(dist, lat, L.k, L.table, L.q, L.n, L.Vx, L.Vy, L.Vz,
+                                                           L.rec, i);
+    else
+        postBCEntry<R, VFB_BC_NOSLIP_INTERPOLATED, EVEN>(dist, lat, L.k, L.table, L.q, L.n, L.Vx, L.Vy, L.Vz, L.rec,
+                                                         i);
+}
+
+template <class R, bool EVEN>
+__global__ void __launch_bounds__(kThreads) postGatherListsKernel(R* __restrict__ lam, const BcLattice<R> lat,
+                                                                  const PostLists<R> P)
+{
+    uint32_t i;
+    const PostList<R>& L = listOf(P, i);
+    if (i < L.n)
+        postGatherEntry<R, EVEN>(lam, lat, L.k, L.table, L.q, L.n, L.tmp, i);
+}
+
+template <class R, bool EVEN>
+__global__ void __launch_bounds__(kThreads) postScatterListsKernel(R* __restrict__ lam, const BcLattice<R> lat,
+                                                                   const PostLists<R> P)
+{
+    uint32_t i;
+    const PostList<R>& L = listOf(P, i);
+    if (i >= L.n)
+        return;
+    if (L.kind == VFB_BC_VELOCITY_INTERPOLATED)
+        postScatterEntry<R, VFB_BC_VELOCITY_INTERPOLATED, EVEN>(lam, lat, L.k, L.table, L.q, L.n, L.rec, L.tmp,
+                                                                L.gV, i);
+    else
+        postScatterEntry<R, VFB_BC_NOSLIP_INTERPOLATED, EVEN>(lam, lat, L.k, L.table, L.q, L.n, L.rec, L.tmp,
+                                                              nullptr, i);
 }
 
 // --------------------------------------------------------------- pressure --
@@ -650,6 +732,59 @@ int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, c
     return checkLaunch("BC adjoint scatter");
 }
 
+// first blocks of the lists of a multi-list launch; the total block count
+template <class R>
+int listBlocks(PostLists<R>& P, unsigned& blocks)
+{
+    if (P.count < 1 || P.count > kMaxPostLists)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "%d post-collision lists in one launch", P.count);
+    blocks = 0;
+    for (int l = 0; l < P.count; ++l) {
+        const int kind = P.list[l].kind;
+        if (kind != VFB_BC_VELOCITY_INTERPOLATED && kind != VFB_BC_NOSLIP_INTERPOLATED)
+            return setError(VFB_ERR_INVALID_ARGUMENT, "BC kind %d has no adjoint", kind);
+        P.firstBlock[l] = blocks;
+        blocks += blocksFor(P.list[l].n);
+    }
+    return VFB_OK;
+}
+
+template <class R>
+int postBCLists(R* dist, const BcLattice<R>& lat, PostLists<R> P, bool even, cudaStream_t s)
+{
+    unsigned b = 0;
+    if (const int rc = listBlocks(P, b))
+        return rc;
+    if (b == 0)
+        return VFB_OK;
+    if (even)
+        postBCListsKernel<R, true><<<b, kThreads, 0, s>>>(dist, lat, P);
+    else
+        postBCListsKernel<R, false><<<b, kThreads, 0, s>>>(dist, lat, P);
+    return checkLaunch("adjoint forward BC lists");
+}
+
+template <class R>
+int postBCAdjointLists(R* lam, const BcLattice<R>& lat, PostLists<R> P, bool even, cudaStream_t s)
+{
+    unsigned b = 0;
+    if (const int rc = listBlocks(P, b))
+        return rc;
+    if (b == 0)
+        return VFB_OK;
+    if (even)
+        postGatherListsKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, P);
+    else
+        postGatherListsKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, P);
+    if (const int rc = checkLaunch("BC lists adjoint gather"))
+        return rc;
+    if (even)
+        postScatterListsKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, P);
+    else
+        postScatterListsKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, P);
+    return checkLaunch("BC lists adjoint scatter");
+}
+
 template <class R>
 int pressureBC(R* dist, const BcLattice<R>& lat, const int32_t* k, const int32_t* kN, const R* rhoBC, uint32_t n,
                int direction, bool even, R* rec, cudaStream_t s)
@@ -724,6 +859,8 @@ int reducePartials(const double* partials, unsigned blocks, int width, double* a
                            const R*, const R*, const R*, bool, R*, cudaStream_t);                                      \
     template int postBCAdjoint<R>(int, R*, const BcLattice<R>&, const int32_t*, const uint32_t*, const R*, uint32_t,  \
                                   const R*, const R*, const R*, bool, const R*, R*, double*, cudaStream_t);            \
+    template int postBCLists<R>(R*, const BcLattice<R>&, PostLists<R>, bool, cudaStream_t);                          \
+    template int postBCAdjointLists<R>(R*, const BcLattice<R>&, PostLists<R>, bool, cudaStream_t);                   \
     template int pressureBC<R>(R*, const BcLattice<R>&, const int32_t*, const int32_t*, const R*, uint32_t, int,     \
                                bool, R*, cudaStream_t);                                                                \
     template int pressureBCAdjoint<R>(R*, const BcLattice<R>&, const int32_t*, const int32_t*, const R*, uint32_t,   \

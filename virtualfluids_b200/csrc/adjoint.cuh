@@ -71,6 +71,35 @@ int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, c
                   uint32_t n, const R* Vx, const R* Vy, const R* Vz, bool even, const R* rec, R* tmp, double* gV,
                   cudaStream_t s);
 
+// Several post-collision lists of one step in one launch (the caller has
+// checked that no list writes a cell another list reads or writes).  rec is
+// the list's record slot of the step (forward: written, may be null;
+// adjoint: read), tmp and gV as for postBCAdjoint.
+constexpr int kMaxPostLists = 3;
+template <class R>
+struct PostList {
+    int kind;
+    const int32_t* k;
+    const uint32_t* table;
+    const R* q;
+    uint32_t n;
+    const R* Vx;
+    const R* Vy;
+    const R* Vz;
+    R* rec;
+    R* tmp;
+    double* gV;
+};
+template <class R>
+struct PostLists {
+    int count = 0;
+    unsigned firstBlock[kMaxPostLists] = { 0, 0, 0 }; // filled by the launchers
+    PostList<R> list[kMaxPostLists];
+};
+template <class R>
+int postBCLists(R* dist, const BcLattice<R>& lat, PostLists<R> lists, bool even, cudaStream_t s);
+template <class R>
+int postBCAdjointLists(R* lam, const BcLattice<R>& lat, PostLists<R> lists, bool even, cudaStream_t s);
 // forward non-equilibrium pressure BC (after the swap); rec may be null
 template <class R>
 int pressureBC(R* dist, const BcLattice<R>& lat, const int32_t* k, const int32_t* kN, const R* rhoBC, uint32_t n,

@@ -349,11 +349,13 @@ static void freeEpilogue(vfb_collision_plan_impl& p)
     cudaFree(p.epi);
     cudaFree(p.epiNodes);
     cudaFree(p.epiRecords);
-    cudaFree(p.epiTiles);
+    cudaFree(p.epiTileStart);
+    cudaFree(p.epiTileNodes);
     p.epi = nullptr;
     p.epiNodes = nullptr;
     p.epiRecords = nullptr;
-    p.epiTiles = nullptr;
+    p.epiTileStart = nullptr;
+    p.epiTileNodes = nullptr;
 }
 
 extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
@@ -528,12 +530,22 @@ extern "C" int vfb_collision_plan_set_bc_epilogue(vfb_collision_plan* plan, cons
         }
     }
     std::vector<uint32_t> nodeRecord(N, 0u), records;
-    std::vector<uint8_t> tiles(p.nTiles, 0);
+    std::vector<uint32_t> tileStart(p.nTiles + 1, 0u), tileNodes(nodes.size());
     for (size_t j = 0; j < nodes.size(); ++j) {
         nodeRecord[nodes[j]] = (uint32_t)records.size() + 1u;
         for (size_t r = 0; r < byNode[j].size(); ++r)
             records.push_back(byNode[j][r] | (r + 1 == byNode[j].size() ? kFusedLast : 0u));
-        tiles[(size_t)tileOf[nodes[j]]] = 1;
+        ++tileStart[(size_t)tileOf[nodes[j]] + 1];
+    }
+    // the BC nodes grouped by tile, in node order within a tile
+    for (uint32_t t = 0; t < p.nTiles; ++t)
+        tileStart[t + 1] += tileStart[t];
+    {
+        std::vector<uint64_t> sorted(nodes);
+        std::sort(sorted.begin(), sorted.end());
+        std::vector<uint32_t> fill(tileStart.begin(), tileStart.end() - 1);
+        for (uint64_t A : sorted)
+            tileNodes[fill[(size_t)tileOf[A]]++] = (uint32_t)A;
     }
     std::vector<std::vector<uint8_t>> fused(nLists);
     for (int l = 0; l < nLists; ++l) {
@@ -556,7 +568,9 @@ extern "C" int vfb_collision_plan_set_bc_epilogue(vfb_collision_plan* plan, cons
     if (e == cudaSuccess)
         e = upload(&p.epiRecords, records, s);
     if (e == cudaSuccess)
-        e = upload(&p.epiTiles, tiles, s);
+        e = upload(&p.epiTileStart, tileStart, s);
+    if (e == cudaSuccess)
+        e = upload(&p.epiTileNodes, tileNodes, s);
     h.nodeRecord = p.epiNodes;
     h.records = p.epiRecords;
     if (e == cudaSuccess)

@@ -133,10 +133,11 @@ struct TiledArgs {
     R* bfy;
     R* bfz;
     int* errorFlag;
-    // the BC epilogue (bc_entry.cuh) or null; epiTiles[t] != 0 when tile t
-    // holds a node with BC records
+    // the BC epilogue (bc_entry.cuh) or null; the nodes with BC records of
+    // tile t are epiTileNodes[epiTileStart[t] .. epiTileStart[t + 1])
     const BcEpilogue* epi;
-    const uint8_t* epiTiles;
+    const uint32_t* epiTileStart;
+    const uint32_t* epiTileNodes;
 };
 
 // offset of location loc (bit 0 x, bit 1 y, bit 2 z) from the node for the
@@ -326,9 +327,11 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
                     Storage<S>::store(a.sbase[d] + locIndex(k, o, loc(d)), f[inv(d)], d);
             }
             // the node's post-collision BCs, from the values this thread just stored
-            if constexpr (EPI)
-                if (__ldg(a.epiTiles + t0 + j * stride))
+            if constexpr (EPI) {
+                const uint32_t t = t0 + j * stride;
+                if (__ldg(a.epiTileStart + t) != __ldg(a.epiTileStart + t + 1))
                     bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, k);
+            }
         }
     }
 }
@@ -397,7 +400,9 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
     const uint32_t maskA = __ldg(meta + 4 + warp), maskB = __ldg(meta + 4 + W2 + warp);
     const bool actA = (maskA >> lane) & 1u;
     const bool actB = (maskB >> lane) & 1u;
-    if (!(actA || actB))
+    // with the BC epilogue every thread reaches the block barrier before it; an
+    // inactive lane runs the general path below with all its accesses predicated off
+    if (!EPI && !(actA || actB))
         return;
     const uint32_t k0 = __ldg(meta);
     const uint32_t kA = k0 + tid, kB = k0 + HALF + tid;
@@ -493,13 +498,16 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
                 St::storeRaw(a.sbase[d] + locIndex(kB, oB, l), v.v.y);
         }
     }
-    // the nodes' post-collision BCs, from the values this thread just stored
+    // the post-collision BCs of the tile's nodes, shared out over the block
+    // once every node of the tile is stored (the barrier makes the block's
+    // global stores visible to all its threads).  The values are re-read from
+    // L1 / L2, and no lane waits on another lane's BC node of the same warp.
     if constexpr (EPI) {
-        if (__ldg(a.epiTiles + blockIdx.x)) {
-            if (actA)
-                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kA);
-            if (actB)
-                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, kB);
+        const uint32_t b = __ldg(a.epiTileStart + blockIdx.x), e = __ldg(a.epiTileStart + blockIdx.x + 1);
+        if (b != e) {
+            __syncthreads();
+            for (uint32_t j = b + tid; j < e; j += HALF)
+                bcEpilogueNode<S, EVEN>(a.dist, a.N, a.epi, __ldg(a.epiTileNodes + j));
         }
     }
 }
@@ -608,11 +616,13 @@ struct vfb_collision_plan_impl {
     unsigned long long stats[6] = { 0, 0, 0, 0, 0, 0 };
     int* error = nullptr;
     // the BC epilogue (vfb_collision_plan_set_bc_epilogue): descriptor, per-node
-    // first record, records and per-tile flags, all device memory
+    // first record, records, per-tile start of the BC nodes and the BC nodes
+    // grouped by tile, all device memory
     BcEpilogue* epi = nullptr;
     uint32_t* epiNodes = nullptr;
     uint32_t* epiRecords = nullptr;
-    uint8_t* epiTiles = nullptr;
+    uint32_t* epiTileStart = nullptr;
+    uint32_t* epiTileNodes = nullptr;
     unsigned long long epiCount[2] = { 0, 0 }; // nodes, records
 };
 
@@ -791,7 +801,8 @@ static int launchTiled(Op op, const vfb_collision_plan_impl& p, const vfb_collis
     a.bfz = static_cast<R*>(c->bodyForceZ);
     a.errorFlag = p.error;
     a.epi = p.epi;
-    a.epiTiles = p.epiTiles;
+    a.epiTileStart = p.epiTileStart;
+    a.epiTileNodes = p.epiTileNodes;
     if (p.nTiles == 0)
         return VFB_OK;
     const bool even = c->isEvenTimestep != 0;

@@ -21,8 +21,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -51,6 +53,12 @@ struct AdjointState {
     uint32_t nObj = 0;
     int velocityKind = -1, noSlipKind = -1, geometryKind = -1;
     bool pressure = false;
+    // the post-collision lists write cells no other list reads or writes, so
+    // each step launches them together (-1: not checked yet)
+    int listsCommute = -1;
+    // the forward pass recorded the tapes and BC records of its only segment:
+    // the backward pass reverses them without recomputing the steps
+    bool taped = false;
     // captured backward segments (recompute with tapes, then the reverse
     // steps), keyed by the segment length and the parity it starts from
     cudaStream_t captureStream = nullptr;
@@ -123,6 +131,11 @@ int checkSupported(const vfb_simulation& S)
     return VFB_OK;
 }
 
+int cudaFail(const char* what)
+{
+    return setError(VFB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(cudaGetLastError()));
+}
+
 template <class R>
 struct Stepper {
     vfb_simulation& S;
@@ -153,6 +166,12 @@ struct Stepper {
 
     R* slotOf(DeviceBuffer& b, int slot, size_t n) { return slot < 0 ? nullptr : as<R>(b) + (size_t)slot * 27 * n; }
 
+    adjoint::PostList<R> postList(BcListDevice& B, int kind, R* rec, R* tmp, double* gV)
+    {
+        return adjoint::PostList<R>{ kind, as<const int32_t>(B.k), as<const uint32_t>(B.locations), as<const R>(B.q),
+                                     B.n, as<const R>(B.vx), as<const R>(B.vy), as<const R>(B.vz), rec, tmp, gV };
+    }
+
     // one step of the forward schedule on `dist` (parity `even` flips); with
     // slot >= 0 the step's inputs are recorded in that slot of the tapes
     int forward(R* dist, bool& even, int slot)
@@ -169,8 +188,17 @@ struct Stepper {
         } items[3] = { { &L.velocity, A.velocityKind, &A.recVelocity },
                        { &L.noSlip, A.noSlipKind, &A.recNoSlip },
                        { &L.geometry, A.geometryKind, &A.recGeometry } };
+        if (A.listsCommute == 1) {
+            adjoint::PostLists<R> P;
+            for (Item& it : items)
+                if (it.list->n && it.kind >= 0)
+                    P.list[P.count++] = postList(*it.list, it.kind, slotOf(*it.rec, slot, it.list->n), nullptr,
+                                                 nullptr);
+            if (const int rc = adjoint::postBCLists<R>(dist, t, P, even, s))
+                return rc;
+        }
         for (Item& it : items) {
-            if (it.list->n == 0 || it.kind < 0)
+            if (A.listsCommute == 1 || it.list->n == 0 || it.kind < 0)
                 continue;
             if (const int rc = adjoint::postBC<R>(it.kind, dist, t, as<const int32_t>(it.list->k),
                                                   as<const uint32_t>(it.list->locations), as<const R>(it.list->q),
@@ -220,8 +248,17 @@ struct Stepper {
         } items[3] = { { &L.geometry, A.geometryKind, &A.recGeometry, &A.tmpGeometry, nullptr },
                        { &L.noSlip, A.noSlipKind, &A.recNoSlip, &A.tmpNoSlip, nullptr },
                        { &L.velocity, A.velocityKind, &A.recVelocity, &A.tmpVelocity, as<double>(A.gVelocity) } };
+        if (A.listsCommute == 1) {
+            adjoint::PostLists<R> P;
+            for (Item& it : items)
+                if (it.list->n && it.kind >= 0)
+                    P.list[P.count++] = postList(*it.list, it.kind, slotOf(*it.rec, slot, it.list->n), as<R>(*it.tmp),
+                                                 it.gV);
+            if (const int rc = adjoint::postBCAdjointLists<R>(lam, lat, P, even, s))
+                return rc;
+        }
         for (Item& it : items) {
-            if (it.list->n == 0 || it.kind < 0)
+            if (A.listsCommute == 1 || it.list->n == 0 || it.kind < 0)
                 continue;
             if (const int rc = adjoint::postBCAdjoint<R>(
                     it.kind, lam, lat, as<const int32_t>(it.list->k), as<const uint32_t>(it.list->locations),
@@ -230,20 +267,11 @@ struct Stepper {
                     slotOf(*it.rec, slot, it.list->n), as<R>(*it.tmp), it.gV, s))
                 return rc;
         }
-        if (const int rc = adjoint::collisionAdjoint<R>(lam, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
-                                                        as<const uint32_t>(A.fluidLocations), L.nFluid, rates, fx,
-                                                        fy, fz, even,
-                                                        slotOf(A.tape, slot, L.nFluid),
-                                                        as<double>(A.forcePartials), s))
-            return rc;
-        return VFB_OK;
+        return adjoint::collisionAdjoint<R>(lam, L.N, nX(), nY(), nZ(), as<const uint32_t>(L.fluid),
+                                            as<const uint32_t>(A.fluidLocations), L.nFluid, rates, fx, fy, fz, even,
+                                            slotOf(A.tape, slot, L.nFluid), as<double>(A.forcePartials), s);
     }
 };
-
-int cudaFail(const char* what)
-{
-    return setError(VFB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(cudaGetLastError()));
-}
 
 template <class R>
 int objectiveValue(vfb_simulation& S, AdjointState& A, const R* dist, bool even, double* J, R* lam, double seed,
@@ -269,6 +297,111 @@ int objectiveValue(vfb_simulation& S, AdjointState& A, const R* dist, bool even,
     return VFB_OK;
 }
 
+// Whether the post-collision lists of the adjoint (velocity, no-slip,
+// geometry) can run in one launch per step: in both parities, no cell a list
+// writes (the cell of inv(d) in the other view, for each link d with
+// 0 <= q_d <= 1) is written by another list or is one of the 27 cells
+// another list's nodes read.  Then the lists commute, forward and adjoint.
+// VFB_ADJOINT_SEPARATE_LISTS=1 keeps one launch per list (for comparisons).
+template <class R>
+int listsCommute(vfb_simulation& S, AdjointState& A, cudaStream_t s, bool& result)
+{
+    result = false;
+    if (const char* env = std::getenv("VFB_ADJOINT_SEPARATE_LISTS"))
+        if (env[0] == '1')
+            return VFB_OK;
+    Level& L = *S.levels[0];
+    struct Item {
+        BcListDevice* list;
+        int kind;
+    } items[3] = { { &L.velocity, A.velocityKind }, { &L.noSlip, A.noSlipKind }, { &L.geometry, A.geometryKind } };
+    std::vector<std::vector<uint32_t>> locs;
+    std::vector<std::vector<R>> qs;
+    for (Item& it : items) {
+        if (it.list->n == 0 || it.kind < 0)
+            continue;
+        const uint32_t n = it.list->n;
+        locs.emplace_back(8ull * n);
+        qs.emplace_back(27ull * n);
+        if (!it.list->locations.ptr ||
+            cudaMemcpyAsync(locs.back().data(), it.list->locations.ptr, 8ull * n * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(qs.back().data(), it.list->q.ptr, 27ull * n * sizeof(R), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess)
+            return cudaFail("BC list download");
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+        return cudaFail("BC list download");
+    if (locs.size() < 2)
+        return VFB_OK; // nothing to launch together
+    const unsigned long long N = L.N;
+    for (int parity = 0; parity < 2; ++parity) {
+        const bool even = parity == 0;
+        std::unordered_map<unsigned long long, int> written; // cell -> list
+        for (size_t l = 0; l < locs.size(); ++l) {
+            const size_t n = locs[l].size() / 8;
+            for (size_t i = 0; i < n; ++i)
+                for (int d = 1; d < 27; ++d) {
+                    const R q = qs[l][(size_t)d * n + i];
+                    if (!(q >= R(0) && q <= R(1)))
+                        continue;
+                    const int e = inv(d);
+                    const unsigned long long c =
+                        (unsigned long long)(even ? slot<false>(e) : slot<true>(e)) * N + locs[l][(size_t)loc(e) * n + i];
+                    const auto ins = written.emplace(c, (int)l);
+                    if (!ins.second && ins.first->second != (int)l)
+                        return VFB_OK; // two lists write one cell
+                }
+        }
+        for (size_t l = 0; l < locs.size(); ++l) {
+            const size_t n = locs[l].size() / 8;
+            for (size_t i = 0; i < n; ++i)
+                for (int d = 0; d < 27; ++d) {
+                    const int r = inv(d);
+                    const unsigned long long c =
+                        (unsigned long long)(even ? slot<true>(r) : slot<false>(r)) * N + locs[l][(size_t)loc(r) * n + i];
+                    const auto it = written.find(c);
+                    if (it != written.end() && it->second != (int)l)
+                        return VFB_OK; // a list reads a cell another list writes
+                }
+        }
+    }
+    result = true;
+    return VFB_OK;
+}
+
+// the buffers of one backward segment (tapes, records, scratch); a
+// reallocation drops the captured segment graphs, which hold their addresses
+template <class R>
+int ensureSegmentBuffers(vfb_simulation& S, AdjointState& A)
+{
+    Level& L = *S.levels[0];
+    const size_t stateBytes = 27ull * L.N * sizeof(R);
+    const unsigned I = A.interval;
+    auto perStep = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, (size_t)I * 27 * n * sizeof(R))); };
+    auto once = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, 27 * n * sizeof(R))); };
+    DeviceBuffer* held[] = { &A.work, &A.lam, &A.tape, &A.recVelocity, &A.recNoSlip, &A.recGeometry, &A.recPressure,
+                             &A.tmpVelocity, &A.tmpNoSlip, &A.tmpGeometry, &A.tmpPressure, &A.gVelocity,
+                             &A.partials, &A.accForce, &A.forcePartials };
+    std::vector<void*> before;
+    for (DeviceBuffer* b : held)
+        before.push_back(b->ptr);
+    if (ensure(A.work, stateBytes) || ensure(A.lam, stateBytes) || perStep(A.tape, L.nFluid) ||
+        perStep(A.recVelocity, L.velocity.n) || perStep(A.recNoSlip, L.noSlip.n) ||
+        perStep(A.recGeometry, L.geometry.n) || perStep(A.recPressure, A.pressureTotal) ||
+        once(A.tmpVelocity, L.velocity.n) || once(A.tmpNoSlip, L.noSlip.n) || once(A.tmpGeometry, L.geometry.n) ||
+        once(A.tmpPressure, A.pressureTotal) ||
+        ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))) ||
+        ensure(A.forcePartials, 3ull * std::max(1u, adjoint::collisionBlocks(L.nFluid)) * sizeof(double)))
+        return cudaFail("adjoint buffers");
+    for (size_t i = 0; i < before.size(); ++i)
+        if (held[i]->ptr != before[i]) {
+            A.dropGraphs();
+            break;
+        }
+    return VFB_OK;
+}
+
 template <class R>
 int adjointForward(vfb_simulation& S, AdjointState& A, unsigned steps, double* J, cudaStream_t s)
 {
@@ -291,6 +424,18 @@ int adjointForward(vfb_simulation& S, AdjointState& A, unsigned steps, double* J
                                             as<uint32_t>(A.fluidLocations), s))
             return rc;
     }
+    if (A.listsCommute < 0) {
+        bool ok = false;
+        if (const int rc = listsCommute<R>(S, A, s, ok))
+            return rc;
+        A.listsCommute = ok ? 1 : 0;
+    }
+    // one segment: the forward pass records its tapes itself (the memory the
+    // backward pass would take for them anyway), and nothing is recomputed
+    A.taped = segments == 1;
+    if (A.taped)
+        if (const int rc = ensureSegmentBuffers<R>(S, A))
+            return rc;
     Stepper<R> st(S, A, s);
     R* dist = as<R>(L.dist);
     bool even = L.isEven;
@@ -301,7 +446,7 @@ int adjointForward(vfb_simulation& S, AdjointState& A, unsigned steps, double* J
                 return cudaFail("checkpoint copy");
             A.checkpointEven[c] = even ? 1 : 0;
         }
-        if (const int rc = st.forward(dist, even, -1))
+        if (const int rc = st.forward(dist, even, A.taped ? (int)t : -1))
             return rc;
     }
     L.isEven = even;
@@ -320,28 +465,8 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
     Level& L = *S.levels[0];
     const size_t stateBytes = 27ull * L.N * sizeof(R);
     const unsigned I = A.interval;
-    auto perStep = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, (size_t)I * 27 * n * sizeof(R))); };
-    auto once = [&](DeviceBuffer& b, size_t n) { return ensure(b, std::max<size_t>(1, 27 * n * sizeof(R))); };
-    // the segment graphs hold these buffers' addresses: a reallocation drops them
-    DeviceBuffer* held[] = { &A.work, &A.lam, &A.tape, &A.recVelocity, &A.recNoSlip, &A.recGeometry, &A.recPressure,
-                             &A.tmpVelocity, &A.tmpNoSlip, &A.tmpGeometry, &A.tmpPressure, &A.gVelocity,
-                             &A.partials, &A.accForce, &A.forcePartials };
-    std::vector<void*> before;
-    for (DeviceBuffer* b : held)
-        before.push_back(b->ptr);
-    if (ensure(A.work, stateBytes) || ensure(A.lam, stateBytes) || perStep(A.tape, L.nFluid) ||
-        perStep(A.recVelocity, L.velocity.n) || perStep(A.recNoSlip, L.noSlip.n) ||
-        perStep(A.recGeometry, L.geometry.n) || perStep(A.recPressure, A.pressureTotal) ||
-        once(A.tmpVelocity, L.velocity.n) || once(A.tmpNoSlip, L.noSlip.n) || once(A.tmpGeometry, L.geometry.n) ||
-        once(A.tmpPressure, A.pressureTotal) ||
-        ensure(A.gVelocity, std::max<size_t>(1, 3ull * L.velocity.n * sizeof(double))) ||
-        ensure(A.forcePartials, 3ull * std::max(1u, adjoint::collisionBlocks(L.nFluid)) * sizeof(double)))
-        return cudaFail("adjoint buffers");
-    for (size_t i = 0; i < before.size(); ++i)
-        if (held[i]->ptr != before[i]) {
-            A.dropGraphs();
-            break;
-        }
+    if (const int rc = ensureSegmentBuffers<R>(S, A))
+        return rc;
     if (cudaMemsetAsync(A.lam.ptr, 0, stateBytes, s) != cudaSuccess ||
         cudaMemsetAsync(A.gVelocity.ptr, 0, A.gVelocity.bytes, s) != cudaSuccess)
         return cudaFail("adjoint clear");
@@ -353,13 +478,15 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
         return cudaFail("force accumulator");
     if (!A.captureStream && cudaStreamCreateWithFlags(&A.captureStream, cudaStreamNonBlocking) != cudaSuccess)
         return cudaFail("capture stream");
-    // one segment: recompute its steps from the work array with tapes, then
-    // the adjoint steps in reverse order
+    // one segment: recompute its steps from the work array with tapes (unless
+    // the forward pass taped them), then the adjoint steps in reverse order
     auto segment = [&](Stepper<R>& st, unsigned len, bool even) -> int {
         std::vector<char> evenAt(len);
         for (unsigned j = 0; j < len; ++j) {
             evenAt[j] = even ? 1 : 0;
-            if (const int rc = st.forward(as<R>(A.work), even, (int)j))
+            if (A.taped)
+                even = !even; // the parity flips once per step
+            else if (const int rc = st.forward(as<R>(A.work), even, (int)j))
                 return rc;
         }
         for (unsigned j = len; j-- > 0;)
@@ -371,10 +498,11 @@ int adjointBackward(vfb_simulation& S, AdjointState& A, double seed, double* dVe
     for (unsigned c = segments; c-- > 0;) {
         const unsigned t0 = c * I;
         const unsigned len = std::min(I, A.steps - t0);
-        if (cudaMemcpyAsync(A.work.ptr, A.checkpoints[c]->ptr, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        if (!A.taped &&
+            cudaMemcpyAsync(A.work.ptr, A.checkpoints[c]->ptr, stateBytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             return cudaFail("checkpoint restore");
         const bool even = A.checkpointEven[c] != 0;
-        const auto key = std::make_pair(len, even ? 1 : 0);
+        const auto key = std::make_pair(len, (even ? 1 : 0) | (A.taped ? 2 : 0));
         auto it = A.segments.find(key);
         if (it == A.segments.end()) {
             // capture the segment's launches once; every segment of this length
@@ -572,4 +700,16 @@ extern "C" int vfb_sim_adjoint_backward(vfb_simulation* sim, double seed, double
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     return A.storage == VFB_FP64 ? adjointBackward<double>(*sim, A, seed, dVelocity, dForces, s)
                                  : adjointBackward<float>(*sim, A, seed, dVelocity, dForces, s);
+}
+
+extern "C" int vfb_sim_adjoint_schedule(const vfb_simulation* sim, int* out2)
+{
+    clearError();
+    if (!sim || !out2)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!sim->adjoint || !sim->adjoint->ready)
+        return setError(VFB_ERR_CONFIGURATION, "no adjoint forward pass");
+    out2[0] = sim->adjoint->listsCommute == 1 ? 1 : 0;
+    out2[1] = sim->adjoint->taped ? 1 : 0;
+    return VFB_OK;
 }

@@ -399,6 +399,14 @@ class Simulation:
                                                        self.stream))
         return dv, df
 
+    def adjoint_schedule(self) -> dict:
+        """The schedule of the last adjoint_forward: whether the BC lists run in
+        one launch per step, and whether the forward pass taped its only
+        segment (checkpoint_interval >= steps: no recomputation backwards)."""
+        out = (ctypes.c_int * 2)()
+        _lib.check(_lib.lib().vfb_sim_adjoint_schedule(self._h, out))
+        return {"lists_together": bool(out[0]), "taped_forward": bool(out[1])}
+
     def bc_epilogue_stats(self, level: int = 0) -> tuple[int, int, int]:
         """(nodes, BC entries) the level's collision applies in its BC
         epilogue, and the entries left to the separate BC launches."""
