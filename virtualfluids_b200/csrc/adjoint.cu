@@ -32,6 +32,7 @@
 #include "adjoint_ops.gen.cuh"
 #include "capi_common.cuh"
 #include "d3q27.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -111,6 +112,7 @@ __global__ void __launch_bounds__(kThreads)
                         const uint32_t* __restrict__ fluid, const uint32_t* __restrict__ table, uint32_t n,
                         const K17Rates<R> r, R fx, R fy, R fz, R* __restrict__ tape)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -142,6 +144,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
                            const K17Rates<R> r, R fx, R fy, R fz, const R* __restrict__ tape,
                            double* __restrict__ partials)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double gx = 0.0, gy = 0.0, gz = 0.0;
     if (i < n) {
@@ -230,6 +233,7 @@ __global__ void __launch_bounds__(kThreads)
                  const R* __restrict__ q, uint32_t n, const R* __restrict__ Vx, const R* __restrict__ Vy,
                  const R* __restrict__ Vz, R* __restrict__ rec)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         postBCEntry<R, KIND, EVEN>(dist, lat, bcK, table, q, n, Vx, Vy, Vz, rec, i);
@@ -264,6 +268,7 @@ __global__ void __launch_bounds__(kThreads)
     postGatherKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK,
                      const uint32_t* __restrict__ table, const R* __restrict__ q, uint32_t n, R* __restrict__ tmp)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         postGatherEntry<R, EVEN>(lam, lat, bcK, table, q, n, tmp, i);
@@ -350,6 +355,7 @@ __global__ void __launch_bounds__(kThreads)
                       const uint32_t* __restrict__ table, const R* __restrict__ q, uint32_t n,
                       const R* __restrict__ rec, const R* __restrict__ tmp, double* __restrict__ gV)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         postScatterEntry<R, KIND, EVEN>(lam, lat, bcK, table, q, n, rec, tmp, gV, i);
@@ -376,6 +382,7 @@ template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads) postBCListsKernel(R* __restrict__ dist, const BcLattice<R> lat,
                                                               const PostLists<R> P)
 {
+    gridDependencyWait();
     uint32_t i;
     const PostList<R>& L = listOf(P, i);
     if (i >= L.n)
@@ -392,6 +399,7 @@ template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads) postGatherListsKernel(R* __restrict__ lam, const BcLattice<R> lat,
                                                                   const PostLists<R> P)
 {
+    gridDependencyWait();
     uint32_t i;
     const PostList<R>& L = listOf(P, i);
     if (i < L.n)
@@ -402,6 +410,7 @@ template <class R, bool EVEN>
 __global__ void __launch_bounds__(kThreads) postScatterListsKernel(R* __restrict__ lam, const BcLattice<R> lat,
                                                                    const PostLists<R> P)
 {
+    gridDependencyWait();
     uint32_t i;
     const PostList<R>& L = listOf(P, i);
     if (i >= L.n)
@@ -421,6 +430,7 @@ __global__ void __launch_bounds__(kThreads)
                    const int32_t* __restrict__ bcKN, const R* __restrict__ rhoBC, uint32_t n, int axis, int sgn,
                    R* __restrict__ rec)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -476,6 +486,7 @@ __global__ void __launch_bounds__(kThreads)
     pressureGatherKernel(R* __restrict__ lam, const BcLattice<R> lat, const int32_t* __restrict__ bcK, uint32_t n,
                          int axis, int sgn, R* __restrict__ tmp)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -497,6 +508,7 @@ __global__ void __launch_bounds__(kThreads)
                           const R* __restrict__ rhoBC, uint32_t n, int axis, int sgn, const R* __restrict__ rec,
                           const R* __restrict__ tmp)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -616,11 +628,11 @@ int collision(R* dist, unsigned long long N, const uint32_t* nX, const uint32_t*
         return VFB_OK;
     const unsigned b = blocksFor(nFluid);
     if (even)
-        tapeCollisionKernel<R, true><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy,
-                                                            fz, tape);
+        launchDependent(tapeCollisionKernel<R, true>, b, kThreads, 0, s, dist, N, nX, nY, nZ, fluid, loc, nFluid,
+                        rates, fx, fy, fz, tape);
     else
-        tapeCollisionKernel<R, false><<<b, kThreads, 0, s>>>(dist, N, nX, nY, nZ, fluid, loc, nFluid, rates, fx, fy,
-                                                             fz, tape);
+        launchDependent(tapeCollisionKernel<R, false>, b, kThreads, 0, s, dist, N, nX, nY, nZ, fluid, loc, nFluid,
+                        rates, fx, fy, fz, tape);
     return checkLaunch("adjoint forward collision");
 }
 
@@ -631,11 +643,11 @@ void launchCollisionAdjoint(bool even, unsigned b, cudaStream_t s, R* lam, unsig
                             double* partials)
 {
     if (even)
-        collisionAdjointKernel<R, true, MINB><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, loc, nFluid, rates,
-                                                                     fx, fy, fz, tape, partials);
+        launchDependent(collisionAdjointKernel<R, true, MINB>, b, kThreads, 0, s, lam, N, nX, nY, nZ, fluid, loc,
+                        nFluid, rates, fx, fy, fz, tape, partials);
     else
-        collisionAdjointKernel<R, false, MINB><<<b, kThreads, 0, s>>>(lam, N, nX, nY, nZ, fluid, loc, nFluid, rates,
-                                                                      fx, fy, fz, tape, partials);
+        launchDependent(collisionAdjointKernel<R, false, MINB>, b, kThreads, 0, s, lam, N, nX, nY, nZ, fluid, loc,
+                        nFluid, rates, fx, fy, fz, tape, partials);
 }
 
 static int collisionAdjointOccupancy(bool dbl)
@@ -675,7 +687,7 @@ template <class R, int KIND, bool EVEN>
 void launchPostBC(unsigned b, cudaStream_t s, R* dist, const BcLattice<R>& lat, const int32_t* k,
                   const uint32_t* table, const R* q, uint32_t n, const R* Vx, const R* Vy, const R* Vz, R* rec)
 {
-    postBCKernel<R, KIND, EVEN><<<b, kThreads, 0, s>>>(dist, lat, k, table, q, n, Vx, Vy, Vz, rec);
+    launchDependent(postBCKernel<R, KIND, EVEN>, b, kThreads, 0, s, dist, lat, k, table, q, n, Vx, Vy, Vz, rec);
 }
 
 template <class R>
@@ -700,7 +712,7 @@ template <class R, int KIND, bool EVEN>
 void launchPostScatter(unsigned b, cudaStream_t s, R* lam, const BcLattice<R>& lat, const int32_t* k,
                        const uint32_t* table, const R* q, uint32_t n, const R* rec, const R* tmp, double* gV)
 {
-    postScatterKernel<R, KIND, EVEN><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, rec, tmp, gV);
+    launchDependent(postScatterKernel<R, KIND, EVEN>, b, kThreads, 0, s, lam, lat, k, table, q, n, rec, tmp, gV);
 }
 
 template <class R>
@@ -717,9 +729,9 @@ int postBCAdjoint(int kind, R* lam, const BcLattice<R>& lat, const int32_t* k, c
         return setError(VFB_ERR_INVALID_ARGUMENT, "BC kind %d has no adjoint", kind);
     const unsigned b = blocksFor(n);
     if (even)
-        postGatherKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, tmp);
+        launchDependent(postGatherKernel<R, true>, b, kThreads, 0, s, lam, lat, k, table, q, n, tmp);
     else
-        postGatherKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, k, table, q, n, tmp);
+        launchDependent(postGatherKernel<R, false>, b, kThreads, 0, s, lam, lat, k, table, q, n, tmp);
     if (const int rc = checkLaunch("BC adjoint gather"))
         return rc;
     constexpr int V = VFB_BC_VELOCITY_INTERPOLATED, NS = VFB_BC_NOSLIP_INTERPOLATED;
@@ -758,9 +770,9 @@ int postBCLists(R* dist, const BcLattice<R>& lat, PostLists<R> P, bool even, cud
     if (b == 0)
         return VFB_OK;
     if (even)
-        postBCListsKernel<R, true><<<b, kThreads, 0, s>>>(dist, lat, P);
+        launchDependent(postBCListsKernel<R, true>, b, kThreads, 0, s, dist, lat, P);
     else
-        postBCListsKernel<R, false><<<b, kThreads, 0, s>>>(dist, lat, P);
+        launchDependent(postBCListsKernel<R, false>, b, kThreads, 0, s, dist, lat, P);
     return checkLaunch("adjoint forward BC lists");
 }
 
@@ -773,15 +785,15 @@ int postBCAdjointLists(R* lam, const BcLattice<R>& lat, PostLists<R> P, bool eve
     if (b == 0)
         return VFB_OK;
     if (even)
-        postGatherListsKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, P);
+        launchDependent(postGatherListsKernel<R, true>, b, kThreads, 0, s, lam, lat, P);
     else
-        postGatherListsKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, P);
+        launchDependent(postGatherListsKernel<R, false>, b, kThreads, 0, s, lam, lat, P);
     if (const int rc = checkLaunch("BC lists adjoint gather"))
         return rc;
     if (even)
-        postScatterListsKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, P);
+        launchDependent(postScatterListsKernel<R, true>, b, kThreads, 0, s, lam, lat, P);
     else
-        postScatterListsKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, P);
+        launchDependent(postScatterListsKernel<R, false>, b, kThreads, 0, s, lam, lat, P);
     return checkLaunch("BC lists adjoint scatter");
 }
 
@@ -796,9 +808,9 @@ int pressureBC(R* dist, const BcLattice<R>& lat, const int32_t* k, const int32_t
         return rc;
     const unsigned b = blocksFor(n);
     if (even)
-        pressureKernel<R, true><<<b, kThreads, 0, s>>>(dist, lat, k, kN, rhoBC, n, axis, sgn, rec);
+        launchDependent(pressureKernel<R, true>, b, kThreads, 0, s, dist, lat, k, kN, rhoBC, n, axis, sgn, rec);
     else
-        pressureKernel<R, false><<<b, kThreads, 0, s>>>(dist, lat, k, kN, rhoBC, n, axis, sgn, rec);
+        launchDependent(pressureKernel<R, false>, b, kThreads, 0, s, dist, lat, k, kN, rhoBC, n, axis, sgn, rec);
     return checkLaunch("adjoint forward pressure BC");
 }
 
@@ -813,15 +825,16 @@ int pressureBCAdjoint(R* lam, const BcLattice<R>& lat, const int32_t* k, const i
         return rc;
     const unsigned b = blocksFor(n);
     if (even)
-        pressureGatherKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, k, n, axis, sgn, tmp);
+        launchDependent(pressureGatherKernel<R, true>, b, kThreads, 0, s, lam, lat, k, n, axis, sgn, tmp);
     else
-        pressureGatherKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, k, n, axis, sgn, tmp);
+        launchDependent(pressureGatherKernel<R, false>, b, kThreads, 0, s, lam, lat, k, n, axis, sgn, tmp);
     if (const int rc = checkLaunch("pressure adjoint gather"))
         return rc;
     if (even)
-        pressureScatterKernel<R, true><<<b, kThreads, 0, s>>>(lam, lat, kN, rhoBC, n, axis, sgn, rec, tmp);
+        launchDependent(pressureScatterKernel<R, true>, b, kThreads, 0, s, lam, lat, kN, rhoBC, n, axis, sgn, rec,
+                        tmp);
     else
-        pressureScatterKernel<R, false><<<b, kThreads, 0, s>>>(lam, lat, kN, rhoBC, n, axis, sgn, rec, tmp);
+        launchDependent(pressureScatterKernel<R, false>, b, kThreads, 0, s, lam, lat, kN, rhoBC, n, axis, sgn, rec, tmp);
     return checkLaunch("pressure adjoint scatter");
 }
 

@@ -39,6 +39,7 @@
 #include "collision_math.cuh"
 #include "d3q27.cuh"
 #include "storage.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -84,6 +85,7 @@ __global__ void __launch_bounds__(128, 6) bcPostKernel(S* __restrict__ dist, con
                                                      const typename Storage<S>::R* __restrict__ Vz,
                                                      const uint32_t* __restrict__ locations)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nBC)
         return;
@@ -102,6 +104,7 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
                                                          const typename Storage<S>::R* __restrict__ rhoBC, uint32_t nBC,
                                                          int axis, int sgn)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nBC)
@@ -164,6 +167,7 @@ __global__ void __launch_bounds__(128) bcOutflowKernel(S* __restrict__ dist, con
                                                         int sgn, typename Storage<S>::R cs,
                                                         typename Storage<S>::R factor)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nBC)
@@ -207,11 +211,11 @@ static void launchPostKind(bool even, unsigned blocks, cudaStream_t stream, S* d
     const R* vy = static_cast<const R*>(l->Vy);
     const R* vz = static_cast<const R*>(l->Vz);
     if (even)
-        bcPostKernel<S, KIND, true><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz,
-                                                                l->locations);
+        launchDependent(bcPostKernel<S, KIND, true>, blocks, 128, 0, stream, dist, lat,
+                        l->k, q, l->numberOfBCnodes, vx, vy, vz, l->locations);
     else
-        bcPostKernel<S, KIND, false><<<blocks, 128, 0, stream>>>(dist, lat, l->k, q, l->numberOfBCnodes, vx, vy, vz,
-                                                                 l->locations);
+        launchDependent(bcPostKernel<S, KIND, false>, blocks, 128, 0, stream, dist, lat,
+                        l->k, q, l->numberOfBCnodes, vx, vy, vz, l->locations);
 }
 
 template <class S>
@@ -245,9 +249,9 @@ static int launchPressure(const vfb_bc_lattice* t, const int32_t* k, const int32
     const unsigned blocks = (n + 127) / 128;
     const R* rho = static_cast<const R*>(rhoBC);
     if (t->isEvenTimestep)
-        bcPressureKernel<S, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, rho, n, axis, sgn);
+        launchDependent(bcPressureKernel<S, true>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn);
     else
-        bcPressureKernel<S, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, rho, n, axis, sgn);
+        launchDependent(bcPressureKernel<S, false>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn);
     return checkLaunch("pressure boundary condition");
 }
 
@@ -265,14 +269,18 @@ static int launchOutflow(const vfb_bc_lattice* t, const int32_t* k, const int32_
     const bool even = t->isEvenTimestep != 0;
     if (correction) {
         if (even)
-            bcOutflowKernel<S, true, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+            launchDependent(bcOutflowKernel<S, true, true>, blocks, 128, 0, stream, dist, lat, k, kN, n, axis, sgn, cs,
+                            fac);
         else
-            bcOutflowKernel<S, false, true><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+            launchDependent(bcOutflowKernel<S, false, true>, blocks, 128, 0, stream, dist, lat, k, kN, n, axis, sgn, cs,
+                            fac);
     } else {
         if (even)
-            bcOutflowKernel<S, true, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+            launchDependent(bcOutflowKernel<S, true, false>, blocks, 128, 0, stream, dist, lat, k, kN, n, axis, sgn, cs,
+                            fac);
         else
-            bcOutflowKernel<S, false, false><<<blocks, 128, 0, stream>>>(dist, lat, k, kN, n, axis, sgn, cs, fac);
+            launchDependent(bcOutflowKernel<S, false, false>, blocks, 128, 0, stream, dist, lat, k, kN, n, axis, sgn,
+                            cs, fac);
     }
     return checkLaunch("outflow boundary condition");
 }

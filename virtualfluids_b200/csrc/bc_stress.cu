@@ -32,6 +32,7 @@
 #include "collision_math.cuh"
 #include "d3q27.cuh"
 #include "storage.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -61,6 +62,7 @@ template <class S, int KIND, bool EVEN>
 __global__ void __launch_bounds__(128) bcStressKernel(S* __restrict__ dist, const BcLattice<typename Storage<S>::R> lat,
                                                        const StressArgs<typename Storage<S>::R> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n)
@@ -164,9 +166,9 @@ void launchKind(bool even, unsigned blocks, cudaStream_t s, S* dist, const BcLat
                 const StressArgs<typename Storage<S>::R>& a)
 {
     if (even)
-        bcStressKernel<S, KIND, true><<<blocks, 128, 0, s>>>(dist, lat, a);
+        launchDependent(bcStressKernel<S, KIND, true>, blocks, 128, 0, s, dist, lat, a);
     else
-        bcStressKernel<S, KIND, false><<<blocks, 128, 0, s>>>(dist, lat, a);
+        launchDependent(bcStressKernel<S, KIND, false>, blocks, 128, 0, s, dist, lat, a);
 }
 
 template <class S>

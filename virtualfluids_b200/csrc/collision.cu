@@ -17,6 +17,7 @@
 #include "collision_math.cuh"
 #include "d3q27.cuh"
 #include "storage.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -77,6 +78,7 @@ constexpr int kCollisionThreads = 128;
 template <class S, bool EVEN, bool WRITE_MACRO, bool BODY_FORCE>
 __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKernelArgs<S> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nFluid)
@@ -114,6 +116,7 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
 template <class S, bool EVEN>
 __global__ void __launch_bounds__(kCollisionThreads) bgkKernel(const CollisionKernelArgs<S> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nFluid)
@@ -396,13 +399,13 @@ static int launchCollision(bool bgk, const vfb_collision_args* a, cudaStream_t s
         k.base[d] = k.dist + (unsigned long long)(even ? d : inv(d)) * k.N;
     if (bgk) {
         if (even)
-            bgkKernel<S, true><<<blocks, kCollisionThreads, 0, stream>>>(k);
+            launchDependent(bgkKernel<S, true>, blocks, kCollisionThreads, 0, stream, k);
         else
-            bgkKernel<S, false><<<blocks, kCollisionThreads, 0, stream>>>(k);
+            launchDependent(bgkKernel<S, false>, blocks, kCollisionThreads, 0, stream, k);
         return checkLaunch("bgk collision");
     }
     const int t = a->collisionTemplate;
-#define VFB_K17(E, W, B) k17Kernel<S, E, W, B><<<blocks, kCollisionThreads, 0, stream>>>(k)
+#define VFB_K17(E, W, B) launchDependent(k17Kernel<S, E, W, B>, blocks, kCollisionThreads, 0, stream, k)
     switch (t) {
     case VFB_TEMPLATE_DEFAULT: even ? VFB_K17(true, false, false) : VFB_K17(false, false, false); break;
     case VFB_TEMPLATE_WRITE_MACRO_VARS: even ? VFB_K17(true, true, false) : VFB_K17(false, true, false); break;

@@ -48,6 +48,7 @@
 #include "storage.cuh"
 #include "pair32.cuh"
 #include "tma.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -223,6 +224,7 @@ __device__ __forceinline__ void collideNode(const TiledArgs<S>& a, typename Stor
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     constexpr int WARPS = C::T / 32;
     constexpr int ST = C::STAGES;
@@ -344,6 +346,7 @@ __global__ void __launch_bounds__(C::T, C::MINB) tiledKernel(const TiledArgs<S> 
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     constexpr int WARPS = C::T / 32;
     const int tid = threadIdx.x;
@@ -391,6 +394,7 @@ __global__ void __launch_bounds__(C::T, C::MINB) directKernel(const TiledArgs<S>
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF, bool EPI = false>
 __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<S> a)
 {
+    gridDependencyWait();
     constexpr int HALF = C::T / 2;
     constexpr int W2 = HALF / 32; // warps of a block = mask words of one half
     constexpr int WARPS = C::T / 32;
@@ -521,6 +525,7 @@ __global__ void __launch_bounds__(C::T / 2, C::MINB) pairKernel(const TiledArgs<
 template <class S, class C, bool EVEN, Op OP, bool WM, bool BF>
 __global__ void __launch_bounds__(C::T, C::MINB) asyncKernel(const TiledArgs<S> a)
 {
+    gridDependencyWait();
     using R = typename Storage<S>::R;
     constexpr int WARPS = C::T / 32;
     extern __shared__ __align__(16) unsigned char smemAsync[];
@@ -644,17 +649,17 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
             blocks = std::max(1, perSM) * sms;
         }
         const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
-        asyncKernel<S, C, EVEN, OP, WM, BF><<<std::max(1u, grid), C::T, smem, stream>>>(a);
+        launchDependent(asyncKernel<S, C, EVEN, OP, WM, BF>, std::max(1u, grid), C::T, smem, stream, a);
         return checkLaunch("pipelined planned collision");
     } else if constexpr (C::STAGES == 1 && sizeof(S) <= 4) {
-        pairKernel<S, C, EVEN, OP, WM, BF, EPI><<<a.nTiles, C::T / 2, 0, stream>>>(a);
+        launchDependent(pairKernel<S, C, EVEN, OP, WM, BF, EPI>, a.nTiles, C::T / 2, 0, stream, a);
         return checkLaunch("paired planned collision");
     } else if constexpr (C::STAGES == 1) {
         // the paired form computes in FP32: FP64 storage uses the staged kernel
         // of the same tile width (same metadata layout and copy geometry)
         return launchTiledT<S, TileCfg<S, C::T, 2, 3>, EVEN, OP, WM, BF, EPI>(a, stream);
     } else if constexpr (C::STAGES == 0) {
-        directKernel<S, C, EVEN, OP, WM, BF><<<a.nTiles, C::T, 0, stream>>>(a);
+        launchDependent(directKernel<S, C, EVEN, OP, WM, BF>, a.nTiles, C::T, 0, stream, a);
         return checkLaunch("direct planned collision");
     } else {
     static int blocks = 0;
@@ -671,7 +676,7 @@ static int launchTiledT(const TiledArgs<S>& a, cudaStream_t stream)
         blocks = std::max(1, perSM) * sms;
     }
     const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)blocks, a.nTiles);
-    tiledKernel<S, C, EVEN, OP, WM, BF, EPI><<<std::max(1u, grid), C::T, C::SMEM_BYTES, stream>>>(a);
+    launchDependent(tiledKernel<S, C, EVEN, OP, WM, BF, EPI>, std::max(1u, grid), C::T, C::SMEM_BYTES, stream, a);
     return checkLaunch("tiled collision");
     }
 }

@@ -32,6 +32,7 @@
 #include "d3q27.cuh"
 #include "interpolation.cuh"
 #include "storage.cuh"
+#include "pdl.cuh"
 
 namespace vfb
 {
@@ -193,6 +194,7 @@ __host__ __device__ __forceinline__ void fineToCoarseCell(const ScalingView<S, R
 template <class S, bool EVEN_C>
 __global__ void __launch_bounds__(64) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < v.nCells)
         coarseToFineCell<DeviceAccess<S>, EVEN_C>(v, i);
@@ -201,6 +203,7 @@ __global__ void __launch_bounds__(64) coarseToFineKernel(const ScalingView<S, ty
 template <class S, bool EVEN_C>
 __global__ void __launch_bounds__(64) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
 {
+    gridDependencyWait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < v.nCells)
         fineToCoarseCell<DeviceAccess<S>, EVEN_C>(v, i);
@@ -240,14 +243,14 @@ static int launchScaling(bool cf, const vfb_scaling_args* a, cudaStream_t s)
     const unsigned blocks = (a->numberOfCells + 63) / 64;
     if (cf) {
         if (a->isEvenTimestep)
-            coarseToFineKernel<S, true><<<blocks, 64, 0, s>>>(v);
+            launchDependent(coarseToFineKernel<S, true>, blocks, 64, 0, s, v);
         else
-            coarseToFineKernel<S, false><<<blocks, 64, 0, s>>>(v);
+            launchDependent(coarseToFineKernel<S, false>, blocks, 64, 0, s, v);
     } else {
         if (a->isEvenTimestep)
-            fineToCoarseKernel<S, true><<<blocks, 64, 0, s>>>(v);
+            launchDependent(fineToCoarseKernel<S, true>, blocks, 64, 0, s, v);
         else
-            fineToCoarseKernel<S, false><<<blocks, 64, 0, s>>>(v);
+            launchDependent(fineToCoarseKernel<S, false>, blocks, 64, 0, s, v);
     }
     return checkLaunch(cf ? "coarse-to-fine interpolation" : "fine-to-coarse interpolation");
 }
