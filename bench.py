@@ -728,10 +728,14 @@ def cube_report(args):
             fl = g["fluid"]
             _, vx, vy, vz = [a[fl].astype(np.float64) for a in sim.macroscopic(lvl)]
             fields.append((vx, vy, vz, sim.kinetic_energy(lvl)[0], int(sim.mass_and_energy(lvl)[2])))
+        saturated = [sim.saturated_populations(lvl) for lvl in range(len(levels))]
         sim.close()
         row = {"nups": per_step_nodes * args.steps / (ms * 1e-3), "fluid_updates_per_s": per_step_fluid * args.steps /
                (ms * 1e-3), "ms_per_coarse_step": ms / args.steps, "nonfinite": sum(f[4] for f in fields),
                "kinetic_energy": [f[3] for f in fields]}
+        if storage == "fx16":
+            # stored deviations clipped at a quarter of their weight, per level
+            row["saturated_populations"] = saturated
         if ref is None:
             ref = fields
         else:

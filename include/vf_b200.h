@@ -508,6 +508,8 @@ int vfb_sim_kinetic_energy(vfb_simulation* sim, int level, double* out2, void* s
  * number.  Computes the macroscopic fields into temporary device arrays
  * first; synchronises the stream. */
 int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream);
+/* vfb_saturated_populations on a level's populations */
+int vfb_sim_saturated_populations(vfb_simulation* sim, int level, unsigned long long* count, void* stream);
 /*
  * Adjoint of the time step (no counterpart in the reference, which has no
  * adjoint).  The differentiated step is the reference's single-level
@@ -671,6 +673,17 @@ int vfb_mass_and_energy(int storage, const void* distributions, unsigned long lo
                         const uint32_t* neighborX, const uint32_t* neighborY, const uint32_t* neighborZ,
                         const uint32_t* nodeIndices, uint32_t numberOfIndices, int isEvenTimestep, double* out,
                         void* stream);
+
+/*
+ * The number of stored populations at either end of the FX16 range (int16
+ * codes 32767 and -32768) in slots 1..26 of an FX16 population array, i.e.
+ * deviations |f - w| that reached a quarter of their weight and were clipped
+ * on store.  0 for every other storage (their ranges are not reached by
+ * lattice flows).  A read-only pass over the array; synchronises the stream.
+ * No counterpart in the reference, which has no 16-bit storage.
+ */
+int vfb_saturated_populations(int storage, const void* distributions, unsigned long long numberOfLBnodes,
+                              unsigned long long* count, void* stream);
 
 /*
  * vfb_mass_and_energy without any allocation: same arguments, same sums in

@@ -209,6 +209,10 @@ _SIGNATURES = [
     ("vfb_sim_adjoint_backward", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vfb_sim_adjoint_schedule", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("vfb_saturated_populations", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_void_p]),
+    ("vfb_sim_saturated_populations", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_void_p]),
     ("vfb_sim_set_forces", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("vfb_sim_output", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,

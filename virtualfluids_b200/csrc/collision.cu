@@ -615,6 +615,71 @@ extern "C" int vfb_macroscopic(int storage, const void* distributions, unsigned 
     }
 }
 
+// stored FX16 codes at either end of the int16 range in slots 1..26 (slot 0,
+// the rest population, also holds the solid-node marker); one 64-bit count
+// per block, added with one atomic per block
+__global__ void __launch_bounds__(kReduceThreads)
+    saturationKernel(const int16_t* __restrict__ dist, unsigned long long begin, unsigned long long end,
+                     unsigned long long* __restrict__ count)
+{
+    __shared__ unsigned long long part[kReduceThreads / 32];
+    unsigned long long c = 0;
+    for (unsigned long long i = begin + blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < end;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const int16_t q = __ldg(dist + i);
+        c += (q == 32767 || q == -32768) ? 1u : 0u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0)
+        part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kReduceThreads / 32; ++w)
+            t += part[w];
+        if (t)
+            atomicAdd(count, t);
+    }
+}
+
+extern "C" int vfb_saturated_populations(int storage, const void* distributions, unsigned long long N,
+                                         unsigned long long* count, void* stream)
+{
+    clearError();
+    if (!count)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "count is NULL");
+    *count = 0;
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (storage != VFB_FX16 || N == 0)
+        return VFB_OK;
+    if (!distributions)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "distributions is NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    unsigned long long* d = nullptr;
+    if (cudaMallocAsync(&d, sizeof(unsigned long long), s) != cudaSuccess)
+        return setError(VFB_ERR_CUDA, "cudaMallocAsync of the counter failed");
+    int rc = VFB_OK;
+    if (cudaMemsetAsync(d, 0, sizeof(unsigned long long), s) != cudaSuccess)
+        rc = setError(VFB_ERR_CUDA, "counter clear failed");
+    if (rc == VFB_OK) {
+        saturationKernel<<<(unsigned)sms * 4u, kReduceThreads, 0, s>>>(static_cast<const int16_t*>(distributions), N,
+                                                                       27ull * N, d);
+        rc = checkLaunch("saturation count");
+    }
+    if (rc == VFB_OK && (cudaMemcpyAsync(count, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) !=
+                             cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess))
+        rc = setError(VFB_ERR_CUDA, "saturation count: %s", cudaGetErrorString(cudaGetLastError()));
+    cudaFreeAsync(d, s);
+    return rc;
+}
+
 extern "C" int vfb_mass_and_energy(int storage, const void* distributions, unsigned long long N, const uint32_t* nX,
                                    const uint32_t* nY, const uint32_t* nZ, const uint32_t* idx, uint32_t n,
                                    int isEven, double* out, void* stream)

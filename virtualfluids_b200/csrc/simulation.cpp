@@ -971,6 +971,15 @@ extern "C" int vfb_sim_mass_and_energy(vfb_simulation* sim, int level, double* o
                                static_cast<const uint32_t*>(L->fluid.ptr), L->nFluid, L->isEven ? 1 : 0, out3, stream);
 }
 
+extern "C" int vfb_sim_saturated_populations(vfb_simulation* sim, int level, unsigned long long* count, void* stream)
+{
+    clearError();
+    Level* L = levelOf(sim, level);
+    if (!L)
+        return VFB_ERR_INVALID_ARGUMENT;
+    return vfb_saturated_populations(sim->params.storage, L->dist.ptr, L->N, count, stream);
+}
+
 extern "C" int vfb_sim_enstrophy(vfb_simulation* sim, int level, double* out2, void* stream)
 {
     clearError();

@@ -399,6 +399,14 @@ class Simulation:
                                                        self.stream))
         return dv, df
 
+    def saturated_populations(self, level: int = 0) -> int:
+        """How many stored populations of the level sit at the ends of the FX16
+        range (deviations clipped at a quarter of their weight); 0 for the other
+        storages."""
+        n = ctypes.c_ulonglong()
+        _lib.check(_lib.lib().vfb_sim_saturated_populations(self._h, level, ctypes.byref(n), self.stream))
+        return n.value
+
     def adjoint_schedule(self) -> dict:
         """The schedule of the last adjoint_forward: whether the BC lists run in
         one launch per step, and whether the forward pass taped its only
