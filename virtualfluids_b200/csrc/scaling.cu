@@ -88,13 +88,7 @@ __host__ __device__ __forceinline__ uint32_t cornerLocation(const uint32_t* B, i
     return B[x + 3 * y + 9 * z];
 }
 
-// memory access of the cell functions: device storage (any format) or host FP32 / FP64
-template <class S>
-struct DeviceAccess {
-    using R = typename Storage<S>::R;
-    __device__ __forceinline__ static R load(const S* p, int d) { return Storage<S>::load(p, d); }
-    __device__ __forceinline__ static void store(S* p, R v, int d) { Storage<S>::store(p, v, d); }
-};
+// memory access of the one-thread cell functions (the host form: FP32 / FP64)
 template <class S>
 struct HostAccess {
     using R = S;
@@ -191,22 +185,137 @@ __host__ __device__ __forceinline__ void fineToCoarseCell(const ScalingView<S, R
         A::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d], d);
 }
 
-template <class S, bool EVEN_C>
-__global__ void __launch_bounds__(64) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
+// The device kernels give each cell eight threads (lanes 8g .. 8g + 7 of a
+// warp, corner c = lane % 8): each thread walks the cell's block, loads the
+// 27 populations of its own source corner and forms that corner's moments;
+// the group gathers the eight moment sets with shuffles, every thread forms
+// the same coefficients (interpolationCoefficients on the same eight sets, so
+// the same values as the one-thread cell functions above), and the writes
+// are shared out: fine corner c (coarse to fine) or the coarse node's
+// directions d with d % 8 == c (fine to coarse).  Eight times the threads of
+// a cell per cell keep eight times the loads in flight.
+constexpr int kScalingThreads = 128; // 16 cells per block
+
+// the eight corners' moments of the group of this lane, from each lane's own
+template <class R>
+__device__ __forceinline__ void gatherMoments(const SourceMoments<R>& mine, SourceMoments<R>* src)
 {
-    gridDependencyWait();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < v.nCells)
-        coarseToFineCell<DeviceAccess<S>, EVEN_C>(v, i);
+    const int base = (int)(threadIdx.x & 31u) & ~7;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        src[c].drho = __shfl_sync(0xffffffffu, mine.drho, base + c);
+        src[c].vx = __shfl_sync(0xffffffffu, mine.vx, base + c);
+        src[c].vy = __shfl_sync(0xffffffffu, mine.vy, base + c);
+        src[c].vz = __shfl_sync(0xffffffffu, mine.vz, base + c);
+        src[c].kxy = __shfl_sync(0xffffffffu, mine.kxy, base + c);
+        src[c].kyz = __shfl_sync(0xffffffffu, mine.kyz, base + c);
+        src[c].kxz = __shfl_sync(0xffffffffu, mine.kxz, base + c);
+        src[c].kxxMyy = __shfl_sync(0xffffffffu, mine.kxxMyy, base + c);
+        src[c].kxxMzz = __shfl_sync(0xffffffffu, mine.kxxMzz, base + c);
+    }
+}
+
+// the eight locations of corner c of a block (a switch over the lane's corner
+// keeps every index into B a constant, so B stays in registers)
+template <int C>
+__device__ __forceinline__ void cornerLocationsOf(const uint32_t* B, uint32_t* Lc)
+{
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+        Lc[l] = cornerLocation(B, C, l);
+}
+
+__device__ __forceinline__ void cornerLocations(const uint32_t* B, int c, uint32_t* Lc)
+{
+    switch (c) {
+    case 0: cornerLocationsOf<0>(B, Lc); break;
+    case 1: cornerLocationsOf<1>(B, Lc); break;
+    case 2: cornerLocationsOf<2>(B, Lc); break;
+    case 3: cornerLocationsOf<3>(B, Lc); break;
+    case 4: cornerLocationsOf<4>(B, Lc); break;
+    case 5: cornerLocationsOf<5>(B, Lc); break;
+    case 6: cornerLocationsOf<6>(B, Lc); break;
+    default: cornerLocationsOf<7>(B, Lc); break;
+    }
+}
+
+// the moments of the corner whose locations are Lc (pre-collision view of parity EVEN)
+template <bool EVEN, class S, class R>
+__device__ __forceinline__ SourceMoments<R> cornerMoments(const S* dist, unsigned long long N, const uint32_t* Lc, R omega)
+{
+    R f[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Storage<S>::load(dist + (unsigned long long)slot<EVEN>(d) * N + Lc[loc(d)], d);
+    return sourceMoments(f, omega);
 }
 
 template <class S, bool EVEN_C>
-__global__ void __launch_bounds__(64) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
+__global__ void __launch_bounds__(kScalingThreads) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
 {
     gridDependencyWait();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < v.nCells)
-        fineToCoarseCell<DeviceAccess<S>, EVEN_C>(v, i);
+    using R = typename Storage<S>::R;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int c = (int)(threadIdx.x & 7u);
+    const bool active = i < v.nCells;
+    // every lane takes part in the shuffles: a group past the end works on the last cell
+    const uint32_t ic = active ? i : v.nCells - 1;
+    uint32_t B[27], Lc[8];
+    blockWalk(v.coarseCells[ic], v.nXc, v.nYc, v.nZc, B);
+    cornerLocations(B, c, Lc);
+    SourceMoments<R> src[8];
+    gatherMoments(cornerMoments<EVEN_C>(v.distC, v.NC, Lc, v.omegaC), src);
+    const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[ic], v.offY[ic], v.offZ[ic]);
+    if (!active)
+        return;
+    blockWalk(v.fineCells[ic], v.nXf, v.nYf, v.nZf, B);
+    cornerLocations(B, c, Lc);
+    const R x = (c & 1) ? R(1) / R(4) : -R(1) / R(4);
+    const R y = (c & 2) ? R(1) / R(4) : -R(1) / R(4);
+    const R z = (c & 4) ? R(1) / R(4) : -R(1) / R(4);
+    R f[27];
+    interpolateCoarseToFine(f, k, v.omegaF, x, y, z);
+    const uint8_t* writes = v.mask ? v.mask + 27 * (size_t)ic : nullptr;
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        if (!writes || ((writes[d] >> c) & 1))
+            Storage<S>::store(v.distF + (unsigned long long)slot<true>(d) * v.NF + Lc[loc(d)], f[d], d);
+}
+
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(kScalingThreads) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
+{
+    gridDependencyWait();
+    using R = typename Storage<S>::R;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int c = (int)(threadIdx.x & 7u);
+    const bool active = i < v.nCells;
+    const uint32_t ic = active ? i : v.nCells - 1;
+    uint32_t B[27], Lc[8];
+    blockWalk(v.fineCells[ic], v.nXf, v.nYf, v.nZf, B);
+    cornerLocations(B, c, Lc);
+    SourceMoments<R> src[8];
+    gatherMoments(cornerMoments<true>(v.distF, v.NF, Lc, v.omegaF), src);
+    const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[ic], v.offY[ic], v.offZ[ic]);
+    if (!active)
+        return;
+    R f[27];
+    interpolateFineToCoarse(f, k, v.omegaC);
+    // the coarse node's own eight locations
+    const uint32_t kc = v.coarseCells[ic];
+    uint32_t L[8];
+    L[0] = kc;
+    L[1] = v.nXc[kc];
+    L[2] = v.nYc[kc];
+    L[4] = v.nZc[kc];
+    L[3] = v.nYc[L[1]];
+    L[5] = v.nZc[L[1]];
+    L[6] = v.nZc[L[2]];
+    L[7] = v.nZc[L[3]];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        if ((d & 7) == c)
+            Storage<S>::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d], d);
 }
 
 template <class S, class R>
@@ -240,17 +349,20 @@ static int launchScaling(bool cf, const vfb_scaling_args* a, cudaStream_t s)
 {
     using R = typename Storage<S>::R;
     const ScalingView<S, R> v = viewOf<S, R>(a);
-    const unsigned blocks = (a->numberOfCells + 63) / 64;
+    if (a->numberOfCells == 0)
+        return VFB_OK;
+    constexpr unsigned cellsPerBlock = kScalingThreads / 8;
+    const unsigned blocks = (a->numberOfCells + cellsPerBlock - 1) / cellsPerBlock;
     if (cf) {
         if (a->isEvenTimestep)
-            launchDependent(coarseToFineKernel<S, true>, blocks, 64, 0, s, v);
+            launchDependent(coarseToFineKernel<S, true>, blocks, kScalingThreads, 0, s, v);
         else
-            launchDependent(coarseToFineKernel<S, false>, blocks, 64, 0, s, v);
+            launchDependent(coarseToFineKernel<S, false>, blocks, kScalingThreads, 0, s, v);
     } else {
         if (a->isEvenTimestep)
-            launchDependent(fineToCoarseKernel<S, true>, blocks, 64, 0, s, v);
+            launchDependent(fineToCoarseKernel<S, true>, blocks, kScalingThreads, 0, s, v);
         else
-            launchDependent(fineToCoarseKernel<S, false>, blocks, 64, 0, s, v);
+            launchDependent(fineToCoarseKernel<S, false>, blocks, kScalingThreads, 0, s, v);
     }
     return checkLaunch(cf ? "coarse-to-fine interpolation" : "fine-to-coarse interpolation");
 }
