@@ -31,7 +31,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "D3Q27 cumulant MLUPS & % HBM roofline; FP16-store vs FP32 at stated L2 err"
-STORAGE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2, "fx16": 2}
+STORAGE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2, "fx16": 2, "fx16w": 2}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -581,7 +581,7 @@ def precision_report(args):
     b.setPeriodicBoundaryCondition(True, True, True)
     b.buildGrids(True)
     rows, ref = {}, None
-    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16"):
+    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16", "fx16w"):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(nu)
@@ -614,6 +614,7 @@ def precision_report(args):
     rows["fp16_over_fp32_mlups"] = rows["fp16"]["mlups"] / rows["fp32"]["mlups"]
     rows["bf16_over_fp32_mlups"] = rows["bf16"]["mlups"] / rows["fp32"]["mlups"]
     rows["fx16_over_fp32_mlups"] = rows["fx16"]["mlups"] / rows["fp32"]["mlups"]
+    rows["fx16w_over_fp32_mlups"] = rows["fx16w"]["mlups"] / rows["fp32"]["mlups"]
     print(json.dumps({"report": "precision form", "workload": f"taylor-green {args.n}^3 periodic, K17",
                       "steps": args.steps, "reference": "fp64 storage on the GPU", "results": rows}), flush=True)
     return 0
@@ -699,7 +700,7 @@ def cube_report(args):
     per_step_nodes = sum(n * 2 ** lvl for lvl, n in enumerate(nodes))
     per_step_fluid = sum(n * 2 ** lvl for lvl, n in enumerate(fluid))
     rows, ref = {}, None
-    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16"):
+    for storage in ("fp64", "fp32", "fp16", "bf16", "fx16", "fx16w"):
         p = Parameter()
         p.set_storage(storage)
         p.set_viscosity_LB(nu)
@@ -733,8 +734,8 @@ def cube_report(args):
         row = {"nups": per_step_nodes * args.steps / (ms * 1e-3), "fluid_updates_per_s": per_step_fluid * args.steps /
                (ms * 1e-3), "ms_per_coarse_step": ms / args.steps, "nonfinite": sum(f[4] for f in fields),
                "kinetic_energy": [f[3] for f in fields]}
-        if storage == "fx16":
-            # stored deviations clipped at a quarter of their weight, per level
+        if storage in ("fx16", "fx16w"):
+            # stored deviations clipped at the end of the format's range, per level
             row["saturated_populations"] = saturated
         if ref is None:
             ref = fields
@@ -745,7 +746,7 @@ def cube_report(args):
             row["kinetic_energy_error_vs_fp64"] = [abs(f[3] - r[3]) / abs(r[3]) if r[3] != 0 else None
                                                    for f, r in zip(fields, ref)]
         rows[storage] = row
-    for s16 in ("fp16", "bf16", "fx16"):
+    for s16 in ("fp16", "bf16", "fx16", "fx16w"):
         rows[f"{s16}_over_fp32_nups"] = rows[s16]["nups"] / rows["fp32"]["nups"]
     print(json.dumps({"report": "wall-mounted cube, two levels", "workload":
                       "cube channel 256x96x96 + refined box 48..128 x 24..72 x 0..40, cube 16 at x=64, K17",

@@ -18,9 +18,12 @@
  * The storage argument selects the element type of the distributions:
  * VFB_FP32 (float), VFB_FP64 (double), and the precision form (16-bit storage,
  * FP32 arithmetic): VFB_FP16 (IEEE half of the deviation times 2^12),
- * VFB_BF16 (bfloat16) and VFB_FX16 (int16 q with f_d - w_d = q * w_d * 2^-17:
+ * VFB_BF16 (bfloat16), VFB_FX16 (int16 q with f_d - w_d = q * w_d * 2^-17:
  * deviations below a quarter of the weight at a uniform step, saturating
- * beyond; no counterpart in the reference).  Arrays documented as "compute
+ * beyond) and VFB_FX16W (int16 q with f_d - w_d = q * w_d * R_d * 2^-15,
+ * R_d = 1/4 for the rest population, 1/2 for the faces, 1 for the edges and
+ * corners: the range of flows whose deviations leave FX16's); no counterpart
+ * in the reference.  Arrays documented as "compute
  * precision" are double for VFB_FP64 and float otherwise.
  */
 #ifndef VF_B200_H
@@ -48,6 +51,7 @@ extern "C" {
 #define VFB_FP16 2
 #define VFB_BF16 3
 #define VFB_FX16 4
+#define VFB_FX16W 5
 
 /* CollisionTemplate (src/gpu/core/Calculation/Calculation.h:55-68) */
 #define VFB_TEMPLATE_DEFAULT 0
@@ -675,11 +679,11 @@ int vfb_mass_and_energy(int storage, const void* distributions, unsigned long lo
                         void* stream);
 
 /*
- * The number of stored populations at either end of the FX16 range (int16
- * codes 32767 and -32768) in slots 1..26 of an FX16 population array, i.e.
- * deviations |f - w| that reached a quarter of their weight and were clipped
- * on store.  0 for every other storage (their ranges are not reached by
- * lattice flows).  A read-only pass over the array; synchronises the stream.
+ * The number of stored populations at either end of the FX16 / FX16W range
+ * (int16 codes 32767 and -32768) in slots 1..26 of such a population array,
+ * i.e. deviations |f - w| that reached the end of the format's range (a
+ * quarter of the weight for FX16) and were clipped on store.  0 for every
+ * other storage (their ranges are not reached by lattice flows).  A read-only pass over the array; synchronises the stream.
  * No counterpart in the reference, which has no 16-bit storage.
  */
 int vfb_saturated_populations(int storage, const void* distributions, unsigned long long numberOfLBnodes,

@@ -86,7 +86,7 @@ def _run(grid, storage, epilogue, steps, velocity=VelocityBC.VelocityInterpolate
     return out, stats
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp64", "fp16", "fx16"])
+@pytest.mark.parametrize("storage", ["fp32", "fp64", "fp16", "fx16", "fx16w"])
 @pytest.mark.parametrize("case", ["cavity", "channel", "sphere_channel", "cube_channel"])
 def test_epilogue_equals_separate_launches(cuda, storage, case):
     grid = {"cavity": _cavity, "channel": _channel}.get(case, lambda: _golden(case))()
@@ -95,7 +95,7 @@ def test_epilogue_equals_separate_launches(cuda, storage, case):
     b, sb = _run(grid, storage, False, steps)
     assert sum(s[0] for s in sa) > 0, sa       # the epilogue took nodes
     assert all(s[0] == 0 for s in sb)
-    tol = {"fp64": 0.0, "fp32": 1e-5, "fp16": 2e-3, "fx16": 3e-3}[storage]
+    tol = {"fp64": 0.0, "fp32": 1e-5, "fp16": 2e-3, "fx16": 3e-3, "fx16w": 1e-2}[storage]
     for lvl in range(len(a)):
         for x, y in zip(a[lvl], b[lvl]):
             scale = max(np.abs(y).max(), 1e-300)

@@ -1,9 +1,13 @@
-"""The FX16 range check (vfb_saturated_populations): FX16 stores
-f - w = q w 2^-17 with q an int16, so deviations beyond a quarter of the
-weight are clipped on store.  The count of clipped codes equals a count over
-the downloaded array; it is zero for a flow inside the range (Taylor-Green,
-u0 = 0.05) and positive for one outside it (a cavity whose lid moves at 0.3,
-where the diagonal populations leave the range), and zero for FP32 storage."""
+"""The FX16 range check (vfb_saturated_populations) and the wide format FX16W.
+
+FX16 stores f - w = q w 2^-17 with q an int16, so deviations beyond a quarter
+of the weight are clipped on store.  The count of clipped codes equals a
+count over the downloaded array; it is zero for a flow inside the range
+(Taylor-Green, u0 = 0.05) and positive for one outside it (a cavity whose lid
+moves at 0.3, where the diagonal populations leave the range), and zero for
+FP32 storage.  FX16W (f - w = q w R 2^-15, R = 1/4, 1/2, 1, 1 by the number
+of non-zero components) holds a cavity with a 0.1 lid that FX16 clips, and
+its velocities stay close to FP32's there while FX16's do not."""
 import ctypes
 
 import numpy as np
@@ -84,3 +88,41 @@ def test_fast_lid_clips_and_the_count_matches_the_array(cuda):
     sim.run(60)
     assert sim.saturated_populations(0) == 0
     sim.close()
+
+
+def _velocity(sim):
+    fl = sim.levels[0]["fluid"]
+    return np.stack([a[fl].astype(np.float64) for a in sim.macroscopic(0)[1:]])
+
+
+def test_wide_format_holds_what_fx16_clips(cuda):
+    out = {}
+    for storage in ("fp32", "fx16", "fx16w"):
+        sim = _sim(_cavity(24, 0.1), storage)
+        sim.run(200)
+        out[storage] = (sim.saturated_populations(0), _velocity(sim))
+        sim.close()
+    assert out["fx16"][0] > 0
+    assert out["fx16w"][0] == 0
+    ref = out["fp32"][1]
+    scale = np.abs(ref).max()
+    err_w = np.abs(out["fx16w"][1] - ref).max() / scale
+    err_n = np.abs(out["fx16"][1] - ref).max() / scale
+    assert err_w < 1e-2, err_w
+    assert err_w < err_n, (err_w, err_n)
+
+
+def test_wide_format_inside_the_range(cuda):
+    """On Taylor-Green both fixed-point formats stay inside their ranges and
+    close to FP32 (FX16W at about twice FX16's step on the faces)."""
+    out = {}
+    for storage in ("fp32", "fx16", "fx16w"):
+        sim = _sim(_periodic(32), storage, _taylor_green(32))
+        sim.run(100)
+        out[storage] = (sim.saturated_populations(0), _velocity(sim))
+        sim.close()
+    assert out["fx16"][0] == 0 == out["fx16w"][0]
+    ref = out["fp32"][1]
+    scale = np.abs(ref).max()
+    for storage in ("fx16", "fx16w"):
+        assert np.abs(out[storage][1] - ref).max() <= 2e-3 * scale, storage

@@ -20,8 +20,8 @@ VFB_ERR_NOT_FINITE = -4
 VFB_ERR_OUT_OF_RANGE = -5
 VFB_ERR_CONFIGURATION = -6
 
-FP32, FP64, FP16, BF16, FX16 = 0, 1, 2, 3, 4
-STORAGE_NAMES = {"fp32": FP32, "fp64": FP64, "fp16": FP16, "bf16": BF16, "fx16": FX16}
+FP32, FP64, FP16, BF16, FX16, FX16W = 0, 1, 2, 3, 4, 5
+STORAGE_NAMES = {"fp32": FP32, "fp64": FP64, "fp16": FP16, "bf16": BF16, "fx16": FX16, "fx16w": FX16W}
 
 TEMPLATE_DEFAULT, TEMPLATE_WRITE_MACRO_VARS, TEMPLATE_APPLY_BODY_FORCE, TEMPLATE_ALL_FEATURES = 0, 1, 2, 3
 

@@ -328,6 +328,7 @@ extern "C" int vfb_bc_post(int kind, int storage, const vfb_bc_lattice* lattice,
     case VFB_FP64: return launchPost<double>(kind, lattice, list, s);
     case VFB_FP16: return launchPost<__half>(kind, lattice, list, s);
     case VFB_FX16: return launchPost<int16_t>(kind, lattice, list, s);
+    case VFB_FX16W: return launchPost<fx16w_t>(kind, lattice, list, s);
     default: return launchPost<__nv_bfloat16>(kind, lattice, list, s);
     }
 }
@@ -367,6 +368,7 @@ extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice,
     case VFB_FP64: return launchPressure<double>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     case VFB_FP16: return launchPressure<__half>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     case VFB_FX16: return launchPressure<int16_t>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
+    case VFB_FX16W: return launchPressure<fx16w_t>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     }
 }
@@ -397,6 +399,7 @@ extern "C" int vfb_bc_outflow_nonreflecting(int storage, const vfb_bc_lattice* l
     case VFB_FP64: return launchOutflow<double>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     case VFB_FP16: return launchOutflow<__half>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     case VFB_FX16: return launchOutflow<int16_t>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
+    case VFB_FX16W: return launchOutflow<fx16w_t>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     default:
         return launchOutflow<__nv_bfloat16>(lattice, k, kN, numberOfBCnodes, axis, sgn, corr, correctionFactor, s);
     }

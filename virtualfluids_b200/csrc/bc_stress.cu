@@ -253,6 +253,7 @@ extern "C" int vfb_bc_stress(int kind, int storage, const vfb_bc_lattice* lattic
     case VFB_FP64: return launchStress<double>(kind, lattice, list, turbViscosity, vx, vy, vz, s);
     case VFB_FP16: return launchStress<__half>(kind, lattice, list, turbViscosity, vx, vy, vz, s);
     case VFB_FX16: return launchStress<int16_t>(kind, lattice, list, turbViscosity, vx, vy, vz, s);
+    case VFB_FX16W: return launchStress<fx16w_t>(kind, lattice, list, turbViscosity, vx, vy, vz, s);
     default: return launchStress<__nv_bfloat16>(kind, lattice, list, turbViscosity, vx, vy, vz, s);
     }
 }

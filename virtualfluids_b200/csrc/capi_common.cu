@@ -39,6 +39,7 @@ extern "C" int vfb_storage_bytes(int storage)
     case VFB_FP64: return 8;
     case VFB_FP16: return 2;
     case VFB_FX16: return 2;
+    case VFB_FX16W: return 2;
     case VFB_BF16: return 2;
     default: return 0;
     }

@@ -528,6 +528,7 @@ extern "C" int vfb_k17_collision(int storage, const vfb_collision_args* args, vo
     case VFB_FP64: return launchCollision<double>(false, args, s);
     case VFB_FP16: return launchCollision<__half>(false, args, s);
     case VFB_FX16: return launchCollision<int16_t>(false, args, s);
+    case VFB_FX16W: return launchCollision<fx16w_t>(false, args, s);
     case VFB_BF16: return launchCollision<__nv_bfloat16>(false, args, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -545,6 +546,7 @@ extern "C" int vfb_bgk_collision(int storage, const vfb_collision_args* args, vo
     case VFB_FP64: return launchCollision<double>(true, args, s);
     case VFB_FP16: return launchCollision<__half>(true, args, s);
     case VFB_FX16: return launchCollision<int16_t>(true, args, s);
+    case VFB_FX16W: return launchCollision<fx16w_t>(true, args, s);
     case VFB_BF16: return launchCollision<__nv_bfloat16>(true, args, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -565,6 +567,7 @@ extern "C" int vfb_init_equilibrium(int storage, void* distributions, unsigned l
     case VFB_FP64: return launchInit<double>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_FP16: return launchInit<__half>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_FX16: return launchInit<int16_t>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
+    case VFB_FX16W: return launchInit<fx16w_t>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     case VFB_BF16: return launchInit<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, rho, vx, vy, vz, isEven, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
@@ -589,6 +592,7 @@ extern "C" int vfb_init_nonequilibrium(int storage, void* distributions, unsigne
     case VFB_FP64: return launchInitNoneq<double>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_FP16: return launchInitNoneq<__half>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_FX16: return launchInitNoneq<int16_t>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
+    case VFB_FX16W: return launchInitNoneq<fx16w_t>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     case VFB_BF16:
         return launchInitNoneq<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, w, rho, vx, vy, vz, omega, isEven, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
@@ -610,12 +614,13 @@ extern "C" int vfb_macroscopic(int storage, const void* distributions, unsigned 
     case VFB_FP64: return launchMacro<double>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_FP16: return launchMacro<__half>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_FX16: return launchMacro<int16_t>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
+    case VFB_FX16W: return launchMacro<fx16w_t>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     case VFB_BF16: return launchMacro<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, isEven, rho, vx, vy, vz, s);
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
 }
 
-// stored FX16 codes at either end of the int16 range in slots 1..26 (slot 0,
+// stored FX16 / FX16W codes at either end of the int16 range in slots 1..26 (slot 0,
 // the rest population, also holds the solid-node marker); one 64-bit count
 // per block, added with one atomic per block
 __global__ void __launch_bounds__(kReduceThreads)
@@ -653,7 +658,7 @@ extern "C" int vfb_saturated_populations(int storage, const void* distributions,
     *count = 0;
     if (vfb_storage_bytes(storage) == 0)
         return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
-    if (storage != VFB_FX16 || N == 0)
+    if ((storage != VFB_FX16 && storage != VFB_FX16W) || N == 0)
         return VFB_OK;
     if (!distributions)
         return setError(VFB_ERR_INVALID_ARGUMENT, "distributions is NULL");
@@ -711,6 +716,7 @@ extern "C" int vfb_mass_and_energy(int storage, const void* distributions, unsig
     case VFB_FP64: rc = launchMassEnergy<double>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     case VFB_FP16: rc = launchMassEnergy<__half>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     case VFB_FX16: rc = launchMassEnergy<int16_t>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
+    case VFB_FX16W: rc = launchMassEnergy<fx16w_t>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     default: rc = launchMassEnergy<__nv_bfloat16>(distributions, N, nX, nY, nZ, idx, n, isEven, partial, blocks, s); break;
     }
     if (rc == VFB_OK) {

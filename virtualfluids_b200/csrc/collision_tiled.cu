@@ -310,6 +310,7 @@ static int runPlanned(Op op, const vfb_collision_plan* plan, const vfb_collision
     case VFB_FP64: return launchTiledFP64(op, p, c, s);
     case VFB_FP16: return launchTiledFP16(op, p, c, s);
     case VFB_FX16: return launchTiledFX16(op, p, c, s);
+    case VFB_FX16W: return launchTiledFX16W(op, p, c, s);
     default: return launchTiledBF16(op, p, c, s);
     }
 }

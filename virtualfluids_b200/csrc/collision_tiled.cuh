@@ -862,4 +862,5 @@ int launchTiledFP64(Op op, const vfb_collision_plan_impl& p, const vfb_collision
 int launchTiledFP16(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
 int launchTiledBF16(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
 int launchTiledFX16(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
+int launchTiledFX16W(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
 } // namespace vfb

@@ -209,6 +209,7 @@ extern "C" int vfb_mass_and_energy_static(int storage, const void* distributions
     case VFB_FP64: rc = launchStatic<double>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     case VFB_FP16: rc = launchStatic<__half>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     case VFB_FX16: rc = launchStatic<int16_t>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
+    case VFB_FX16W: rc = launchStatic<fx16w_t>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     default: rc = launchStatic<__nv_bfloat16>(distributions, N, nX, nY, nZ, idx, n, isEven, blocks, scratch, s); break;
     }
     if (rc != VFB_OK)

@@ -148,6 +148,7 @@ extern "C" int vfb_output_pass(int storage, const void* distributions, unsigned 
     case VFB_FP64: rc = launchOutput<double>(distributions, N, geo, nX, nY, nZ, nodeMask, isEven, rho, vx, vy, vz, partial, blocks, s); break;
     case VFB_FP16: rc = launchOutput<__half>(distributions, N, geo, nX, nY, nZ, nodeMask, isEven, rho, vx, vy, vz, partial, blocks, s); break;
     case VFB_FX16: rc = launchOutput<int16_t>(distributions, N, geo, nX, nY, nZ, nodeMask, isEven, rho, vx, vy, vz, partial, blocks, s); break;
+    case VFB_FX16W: rc = launchOutput<fx16w_t>(distributions, N, geo, nX, nY, nZ, nodeMask, isEven, rho, vx, vy, vz, partial, blocks, s); break;
     default: rc = launchOutput<__nv_bfloat16>(distributions, N, geo, nX, nY, nZ, nodeMask, isEven, rho, vx, vy, vz, partial, blocks, s); break;
     }
     if (rc == VFB_OK) {

@@ -397,6 +397,7 @@ static int runScaling(bool cf, int storage, const vfb_scaling_args* a, void* str
     case VFB_FP64: return launchScaling<double>(cf, a, s);
     case VFB_FP16: return launchScaling<__half>(cf, a, s);
     case VFB_FX16: return launchScaling<int16_t>(cf, a, s);
+    case VFB_FX16W: return launchScaling<fx16w_t>(cf, a, s);
     default: return launchScaling<__nv_bfloat16>(cf, a, s);
     }
 }

@@ -13,6 +13,12 @@
 //         is held with a uniform step of w_i * 2^-17 (values beyond saturate).
 //         At the flows of the benchmarks (|f_i - w_i| / w_i up to 0.16 at
 //         u0 = 0.05) this keeps 4 to 6 more significant bits than FP16.
+//   FX16W the same int16 code over a range that widens with the number of
+//         non-zero components of the direction: f_i - w_i = q * w_i * R * 2^-15
+//         with R = 1/4 (rest), 1/2 (faces), 1 (edges and corners), for flows
+//         whose deviations leave FX16's quarter of the weight (a bluff body's
+//         refined wake reaches 0.39 / 0.55 / 0.72 of the weight on faces /
+//         edges / corners); the step of the face populations doubles.
 // Every access names the direction d whose slot it touches (the slots of d
 // and of its inverse hold populations of equal weight), so a format may scale
 // per direction.
@@ -117,5 +123,41 @@ struct Storage<int16_t> {
     }
     __device__ __forceinline__ static R load(const int16_t* p, int d) { return loadRaw(p) * invScale(d); }
     __device__ __forceinline__ static void store(int16_t* p, R v, int d) { storeRaw(p, v * scale(d)); }
+};
+
+// FX16W: an int16 code whose scale is 2^15 / (R_d w_d) (storage.cuh header)
+struct fx16w_t {
+    int16_t q;
+};
+
+// 2^15 / (R_d w_d) for the four weight classes: 27/2, 27, 54 and 216 times
+// 2^15, all exact in FP32
+__host__ __device__ constexpr float fx16wScale(int d)
+{
+    return order(d) == 0 ? 442368.0f : order(d) == 1 ? 884736.0f : order(d) == 2 ? 1769472.0f : 7077888.0f;
+}
+
+template <>
+struct Storage<fx16w_t> {
+    using R = float;
+    static constexpr int id = 5;
+    static constexpr bool scaled = true;
+    static constexpr float marker = 32767.0f;
+    static constexpr float invScale(int d) { return 1.0f / fx16wScale(d); }
+    static constexpr float scale(int d) { return fx16wScale(d); }
+    __device__ __forceinline__ static R loadRaw(const fx16w_t* p)
+    {
+        float r;
+        asm("cvt.rn.f32.s16 %0, %1;" : "=f"(r) : "h"(p->q));
+        return r;
+    }
+    __device__ __forceinline__ static void storeRaw(fx16w_t* p, R v)
+    {
+        int16_t q;
+        asm("cvt.rni.sat.s16.f32 %0, %1;" : "=h"(q) : "f"(v));
+        p->q = q;
+    }
+    __device__ __forceinline__ static R load(const fx16w_t* p, int d) { return loadRaw(p) * invScale(d); }
+    __device__ __forceinline__ static void store(fx16w_t* p, R v, int d) { storeRaw(p, v * scale(d)); }
 };
 } // namespace vfb

@@ -159,7 +159,9 @@ class Parameter:
 
     def set_storage(self, storage: str):
         """Population storage: "fp64", "fp32", or the 16-bit forms "fp16" /
-        "bf16" / "fx16" (fixed point relative to the weight, see vf_b200.h)."""
+        "bf16" / "fx16" / "fx16w" (fixed point relative to the weight over a
+        quarter of it, or over a range that widens with the direction's
+        non-zero components; see vf_b200.h)."""
         if storage not in _lib.STORAGE_NAMES:
             raise ValueError(f"unknown storage {storage!r}")
         self.storage = storage
@@ -401,7 +403,7 @@ class Simulation:
 
     def saturated_populations(self, level: int = 0) -> int:
         """How many stored populations of the level sit at the ends of the FX16
-        range (deviations clipped at a quarter of their weight); 0 for the other
+        or FX16W range (deviations clipped on store); 0 for the other
         storages."""
         n = ctypes.c_ulonglong()
         _lib.check(_lib.lib().vfb_sim_saturated_populations(self._h, level, ctypes.byref(n), self.stream))
