@@ -369,6 +369,25 @@ typedef struct vfb_scaling_args {
 
 int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream);
 int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* stream);
+/* vfb_scale_fine_to_coarse then vfb_scale_coarse_to_fine, in one launch (the
+ * two lists' cells in one grid).  Valid only when neither list reads a cell
+ * the other writes (vfb_scaling_independent), so that the reference's order
+ * (fine to coarse first, UpdateGrid27.cpp:89-93) does not matter.  No
+ * counterpart in the reference. */
+int vfb_scale_interface(int storage, const vfb_scaling_args* fineToCoarse, const vfb_scaling_args* coarseToFine,
+                        void* stream);
+/* Host arrays: *independent = 1 when, in both parities, no fine cell the
+ * coarse-to-fine cells write (under cfMask, NULL = all) is read by the
+ * fine-to-coarse cells and no coarse cell the fine-to-coarse cells write is
+ * read by the coarse-to-fine cells; else 0.  No counterpart in the reference. */
+int vfb_scaling_independent(const uint32_t* fineToCoarseCoarseCells, const uint32_t* fineToCoarseFineCells,
+                            uint32_t numberOfFineToCoarseCells, const uint32_t* coarseToFineCoarseCells,
+                            const uint32_t* coarseToFineFineCells, uint32_t numberOfCoarseToFineCells,
+                            const uint8_t* coarseToFineWriteMask, const uint32_t* neighborXcoarse,
+                            const uint32_t* neighborYcoarse, const uint32_t* neighborZcoarse,
+                            unsigned long long numberOfLBnodesCoarse, const uint32_t* neighborXfine,
+                            const uint32_t* neighborYfine, const uint32_t* neighborZfine,
+                            unsigned long long numberOfLBnodesFine, int* independent);
 /* the same interpolation on the host (host arrays, VFB_FP32 or VFB_FP64),
  * with the library's own arithmetic; for checks without a GPU.  No
  * counterpart in the reference. */

@@ -2,6 +2,9 @@
 through vfb_debug_scale_host) against the reference's own
 scaleCoarseToFineCompressible / scaleFineToCoarseCompressible kernels
 compiled on the host (oracle/_ref)."""
+import ctypes
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -100,3 +103,46 @@ def test_sequential_result_matches_reference_on_refined_grid():
     Reference("f64").scale(True, rC, rF, c["gc"], c["gf"], True, c["coarse_cf"], c["fine_cf"], c["omegaC"],
                            c["omegaF"], c["offX"], c["offY"], c["offZ"])
     assert rel_max(dF, rF) < 1e-13
+
+
+def _golden_levels(name):
+    with np.load(Path(__file__).resolve().parent / "golden" / f"grid_{name}.npz") as z:
+        levels = {}
+        for key in z.files:
+            lvl, arr = key.split(":", 1)
+            levels.setdefault(int(lvl[1:]), {})[arr] = z[key]
+    return [levels[i] for i in sorted(levels)]
+
+
+def _independent(g, gf, cf_mask=None, fc_fine=None):
+    u = lambda a: np.ascontiguousarray(a, dtype=np.uint32)
+    fcc, fcf = u(g["fc.coarse"]), u(g["fc.fine"] if fc_fine is None else fc_fine)
+    cfc, cff = u(g["cf.coarse"]), u(g["cf.fine"])
+    nc = [u(g[f"neighbor{a}"]) for a in "XYZ"]
+    nf = [u(gf[f"neighbor{a}"]) for a in "XYZ"]
+    mask = None
+    if cf_mask:
+        mask = np.zeros(27 * len(cff), np.uint8)
+        _lib.check(_lib.lib().vfb_scaling_write_mask(cff.ctypes.data, len(cff), nf[0].ctypes.data, nf[1].ctypes.data,
+                                                     nf[2].ctypes.data, len(nf[0]), mask.ctypes.data))
+    out = ctypes.c_int(-1)
+    _lib.check(_lib.lib().vfb_scaling_independent(
+        fcc.ctypes.data, fcf.ctypes.data, len(fcc), cfc.ctypes.data, cff.ctypes.data, len(cfc),
+        None if mask is None else mask.ctypes.data, *[a.ctypes.data for a in nc], len(nc[0]),
+        *[a.ctypes.data for a in nf], len(nf[0]), ctypes.byref(out)))
+    return out.value
+
+
+@pytest.mark.parametrize("name", ["cube_channel", "two_level_box", "refined_channel"])
+def test_interface_lists_independence(name):
+    """vfb_scaling_independent: on the refinement grids the builder makes, the
+    fine-to-coarse cells read no fine cell the coarse-to-fine cells write and
+    the coarse-to-fine cells read no coarse cell the fine-to-coarse cells
+    write, so one launch may serve both lists (vfb_scale_interface); with the
+    fine-to-coarse cells moved onto the coarse-to-fine cells' fine nodes the
+    check reports the dependence (grids with both lists)."""
+    lv = _golden_levels(name)
+    g, gf = lv[0], lv[1]
+    assert _independent(g, gf, cf_mask=True) == 1
+    if len(g["fc.fine"]):
+        assert _independent(g, gf, cf_mask=True, fc_fine=np.asarray(g["cf.fine"])[: len(g["fc.fine"])]) == 0

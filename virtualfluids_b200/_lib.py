@@ -186,6 +186,12 @@ _SIGNATURES = [
       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     ("vfb_scale_coarse_to_fine", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
     ("vfb_scale_fine_to_coarse", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
+    ("vfb_scale_interface", ctypes.c_int,
+     [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
+    ("vfb_scaling_independent", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_int)]),
     ("vfb_debug_scale_host", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ScalingArgs)]),
     ("vfb_scaling_write_mask", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong,

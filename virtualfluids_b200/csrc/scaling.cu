@@ -25,6 +25,8 @@
 // writer.  The fine-to-coarse cells of a grid write distinct coarse nodes.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <unordered_map>
 #include <vector>
 
@@ -250,12 +252,12 @@ __device__ __forceinline__ SourceMoments<R> cornerMoments(const S* dist, unsigne
     return sourceMoments(f, omega);
 }
 
+// the cells of block `block` (16 cells, eight threads each)
 template <class S, bool EVEN_C>
-__global__ void __launch_bounds__(kScalingThreads) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
+__device__ __forceinline__ void coarseToFineBlock(const ScalingView<S, typename Storage<S>::R>& v, uint32_t block)
 {
-    gridDependencyWait();
     using R = typename Storage<S>::R;
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const uint32_t i = (block * blockDim.x + threadIdx.x) >> 3;
     const int c = (int)(threadIdx.x & 7u);
     const bool active = i < v.nCells;
     // every lane takes part in the shuffles: a group past the end works on the last cell
@@ -283,11 +285,10 @@ __global__ void __launch_bounds__(kScalingThreads) coarseToFineKernel(const Scal
 }
 
 template <class S, bool EVEN_C>
-__global__ void __launch_bounds__(kScalingThreads) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
+__device__ __forceinline__ void fineToCoarseBlock(const ScalingView<S, typename Storage<S>::R>& v, uint32_t block)
 {
-    gridDependencyWait();
     using R = typename Storage<S>::R;
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const uint32_t i = (block * blockDim.x + threadIdx.x) >> 3;
     const int c = (int)(threadIdx.x & 7u);
     const bool active = i < v.nCells;
     const uint32_t ic = active ? i : v.nCells - 1;
@@ -316,6 +317,35 @@ __global__ void __launch_bounds__(kScalingThreads) fineToCoarseKernel(const Scal
     for (int d = 0; d < 27; ++d)
         if ((d & 7) == c)
             Storage<S>::store(v.distC + (unsigned long long)slot<EVEN_C>(d) * v.NC + L[loc(d)], f[d], d);
+}
+
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(kScalingThreads) coarseToFineKernel(const ScalingView<S, typename Storage<S>::R> v)
+{
+    gridDependencyWait();
+    coarseToFineBlock<S, EVEN_C>(v, blockIdx.x);
+}
+
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(kScalingThreads) fineToCoarseKernel(const ScalingView<S, typename Storage<S>::R> v)
+{
+    gridDependencyWait();
+    fineToCoarseBlock<S, EVEN_C>(v, blockIdx.x);
+}
+
+// both lists of a level pair in one launch: the first fcBlocks blocks take
+// the fine-to-coarse cells, the rest the coarse-to-fine cells (valid when
+// neither list reads what the other writes, vfb_scaling_independent)
+template <class S, bool EVEN_C>
+__global__ void __launch_bounds__(kScalingThreads)
+    interfaceKernel(const ScalingView<S, typename Storage<S>::R> fc, const ScalingView<S, typename Storage<S>::R> cf,
+                    uint32_t fcBlocks)
+{
+    gridDependencyWait();
+    if (blockIdx.x < fcBlocks)
+        fineToCoarseBlock<S, EVEN_C>(fc, blockIdx.x);
+    else
+        coarseToFineBlock<S, EVEN_C>(cf, blockIdx.x - fcBlocks);
 }
 
 template <class S, class R>
@@ -403,6 +433,21 @@ static int runScaling(bool cf, int storage, const vfb_scaling_args* a, void* str
 }
 
 template <class S>
+static int launchInterface(const vfb_scaling_args* fc, const vfb_scaling_args* cf, cudaStream_t s)
+{
+    using R = typename Storage<S>::R;
+    constexpr unsigned cellsPerBlock = kScalingThreads / 8;
+    const unsigned fcBlocks = (fc->numberOfCells + cellsPerBlock - 1) / cellsPerBlock;
+    const unsigned cfBlocks = (cf->numberOfCells + cellsPerBlock - 1) / cellsPerBlock;
+    const ScalingView<S, R> vf = viewOf<S, R>(fc), vc = viewOf<S, R>(cf);
+    if (fc->isEvenTimestep)
+        launchDependent(interfaceKernel<S, true>, fcBlocks + cfBlocks, kScalingThreads, 0, s, vf, vc, fcBlocks);
+    else
+        launchDependent(interfaceKernel<S, false>, fcBlocks + cfBlocks, kScalingThreads, 0, s, vf, vc, fcBlocks);
+    return checkLaunch("fine-to-coarse and coarse-to-fine interpolation");
+}
+
+template <class S>
 static void hostScaling(bool cf, const vfb_scaling_args* a)
 {
     const ScalingView<S, S> v = viewOf<S, S>(a);
@@ -465,6 +510,104 @@ extern "C" int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t n, con
 extern "C" int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream)
 {
     return runScaling(true, storage, args, stream);
+}
+
+extern "C" int vfb_scale_interface(int storage, const vfb_scaling_args* fineToCoarse,
+                                   const vfb_scaling_args* coarseToFine, void* stream)
+{
+    clearError();
+    if (const int rc = checkScalingArgs(storage, fineToCoarse))
+        return rc;
+    if (const int rc = checkScalingArgs(storage, coarseToFine))
+        return rc;
+    if (fineToCoarse->isEvenTimestep != coarseToFine->isEvenTimestep)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "the two lists' parities differ");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (fineToCoarse->numberOfCells == 0 || coarseToFine->numberOfCells == 0) {
+        if (const int rc = runScaling(false, storage, fineToCoarse, stream))
+            return rc;
+        return runScaling(true, storage, coarseToFine, stream);
+    }
+    switch (storage) {
+    case VFB_FP32: return launchInterface<float>(fineToCoarse, coarseToFine, s);
+    case VFB_FP64: return launchInterface<double>(fineToCoarse, coarseToFine, s);
+    case VFB_FP16: return launchInterface<__half>(fineToCoarse, coarseToFine, s);
+    case VFB_FX16: return launchInterface<int16_t>(fineToCoarse, coarseToFine, s);
+    case VFB_FX16W: return launchInterface<fx16w_t>(fineToCoarse, coarseToFine, s);
+    default: return launchInterface<__nv_bfloat16>(fineToCoarse, coarseToFine, s);
+    }
+}
+
+extern "C" int vfb_scaling_independent(const uint32_t* fcCoarse, const uint32_t* fcFine, uint32_t nFC,
+                                       const uint32_t* cfCoarse, const uint32_t* cfFine, uint32_t nCF,
+                                       const uint8_t* cfMask, const uint32_t* nXc, const uint32_t* nYc,
+                                       const uint32_t* nZc, unsigned long long NC, const uint32_t* nXf,
+                                       const uint32_t* nYf, const uint32_t* nZf, unsigned long long NF,
+                                       int* independent)
+{
+    clearError();
+    if (!independent)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "independent is NULL");
+    *independent = 0;
+    if ((nFC && (!fcCoarse || !fcFine)) || (nCF && (!cfCoarse || !cfFine)) || !nXc || !nYc || !nZc || !nXf ||
+        !nYf || !nZf || NC == 0 || NF == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    auto inRange = [](uint32_t k, unsigned long long n) { return (unsigned long long)k < n; };
+    uint32_t B[27];
+    // fine side: the cells the coarse-to-fine list writes, against those the fine-to-coarse list reads
+    std::vector<uint8_t> written(27ull * NF, 0);
+    for (uint32_t i = 0; i < nCF; ++i) {
+        if (!inRange(cfFine[i], NF))
+            return setError(VFB_ERR_OUT_OF_RANGE, "coarse-to-fine cell %u: fine node outside the level", i);
+        blockWalk(cfFine[i], nXf, nYf, nZf, B);
+        for (int c = 0; c < 8; ++c)
+            for (int d = 0; d < 27; ++d)
+                if (!cfMask || ((cfMask[27ull * i + d] >> c) & 1))
+                    written[(unsigned long long)slot<true>(d) * NF + cornerLocation(B, c, loc(d))] = 1;
+    }
+    for (uint32_t i = 0; i < nFC; ++i) {
+        if (!inRange(fcFine[i], NF))
+            return setError(VFB_ERR_OUT_OF_RANGE, "fine-to-coarse cell %u: fine node outside the level", i);
+        blockWalk(fcFine[i], nXf, nYf, nZf, B);
+        for (int c = 0; c < 8; ++c)
+            for (int d = 0; d < 27; ++d)
+                if (written[(unsigned long long)slot<true>(d) * NF + cornerLocation(B, c, loc(d))])
+                    return VFB_OK;
+    }
+    // coarse side, both parities: the cells the fine-to-coarse list writes,
+    // against those the coarse-to-fine list reads
+    std::vector<uint8_t> wc(27ull * NC);
+    for (int parity = 0; parity < 2; ++parity) {
+        std::fill(wc.begin(), wc.end(), 0);
+        for (uint32_t i = 0; i < nFC; ++i) {
+            const uint32_t kc = fcCoarse[i];
+            if (!inRange(kc, NC))
+                return setError(VFB_ERR_OUT_OF_RANGE, "fine-to-coarse cell %u: coarse node outside the level", i);
+            uint32_t L[8];
+            L[0] = kc;
+            L[1] = nXc[kc];
+            L[2] = nYc[kc];
+            L[4] = nZc[kc];
+            L[3] = nYc[L[1]];
+            L[5] = nZc[L[1]];
+            L[6] = nZc[L[2]];
+            L[7] = nZc[L[3]];
+            for (int d = 0; d < 27; ++d)
+                wc[(unsigned long long)(parity ? slot<true>(d) : slot<false>(d)) * NC + L[loc(d)]] = 1;
+        }
+        for (uint32_t i = 0; i < nCF; ++i) {
+            if (!inRange(cfCoarse[i], NC))
+                return setError(VFB_ERR_OUT_OF_RANGE, "coarse-to-fine cell %u: coarse node outside the level", i);
+            blockWalk(cfCoarse[i], nXc, nYc, nZc, B);
+            for (int c = 0; c < 8; ++c)
+                for (int d = 0; d < 27; ++d)
+                    if (wc[(unsigned long long)(parity ? slot<true>(d) : slot<false>(d)) * NC +
+                           cornerLocation(B, c, loc(d))])
+                        return VFB_OK;
+        }
+    }
+    *independent = 1;
+    return VFB_OK;
 }
 
 extern "C" int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* stream)

@@ -78,6 +78,9 @@ struct Level {
     DeviceBuffer dist, nX, nY, nZ, geo, fluid;
     DeviceBuffer nNeg; // the -x-y-z neighbour (non-equilibrium init, enstrophy)
     BcListDevice velocity, noSlip, slip, geometry;
+    // the interface lists to the next finer level run in one launch (neither
+    // reads what the other writes)
+    bool interfaceTogether = false;
     StressListDevice stress;
     // with the plan's BC epilogue: the remaining entries of velocity, no-slip,
     // slip and geometry (in that order), launched after the collision

@@ -581,6 +581,20 @@ int refinement(vfb_simulation& S, Level& C, Level& F, void* stream)
     a.omegaCoarse = C.omega;
     a.omegaFine = F.omega;
     const InterfaceDevice* order[2] = { &C.fineToCoarse, &C.coarseToFine };
+    if (C.interfaceTogether && C.fineToCoarse.n && C.coarseToFine.n) {
+        vfb_scaling_args b[2] = { a, a };
+        for (int i = 0; i < 2; ++i) {
+            const InterfaceDevice& I = *order[i];
+            b[i].coarseCells = static_cast<const uint32_t*>(I.coarse.ptr);
+            b[i].fineCells = static_cast<const uint32_t*>(I.fine.ptr);
+            b[i].numberOfCells = I.n;
+            b[i].offsetX = I.offX.ptr;
+            b[i].offsetY = I.offY.ptr;
+            b[i].offsetZ = I.offZ.ptr;
+            b[i].fineWriteMask = static_cast<const uint8_t*>(I.mask.ptr);
+        }
+        return vfb_scale_interface(S.params.storage, &b[0], &b[1], stream);
+    }
     for (int i = 0; i < 2; ++i) {
         const InterfaceDevice& I = *order[i];
         if (I.n == 0)
@@ -787,6 +801,20 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
                                     reinterpret_cast<uint8_t*>(mask.data()));
         if (rc == VFB_OK && uploadRaw(C.coarseToFine.mask, mask.data(), mask.size(), s) != cudaSuccess)
             rc = setError(VFB_ERR_CUDA, "interface mask upload failed");
+        // whether fine-to-coarse and coarse-to-fine can share one launch
+        std::vector<char> cfc, fcc, fcf, cnx, cny, cnz;
+        if (rc == VFB_OK && C.fineToCoarse.n &&
+            gridArray(grid, l, "cf.coarse", cfc, count, es) && gridArray(grid, l, "fc.coarse", fcc, count, es) &&
+            gridArray(grid, l, "fc.fine", fcf, count, es) && gridArray(grid, l, "neighborX", cnx, count, es) &&
+            gridArray(grid, l, "neighborY", cny, count, es) && gridArray(grid, l, "neighborZ", cnz, count, es)) {
+            int together = 0;
+            auto u32 = [](const std::vector<char>& v) { return reinterpret_cast<const uint32_t*>(v.data()); };
+            rc = vfb_scaling_independent(u32(fcc), u32(fcf), C.fineToCoarse.n, u32(cfc), u32(cells),
+                                         C.coarseToFine.n, reinterpret_cast<const uint8_t*>(mask.data()), u32(cnx),
+                                         u32(cny), u32(cnz), C.N, u32(nx), u32(ny), u32(nz), S->levels[l + 1]->N,
+                                         &together);
+            C.interfaceTogether = together != 0;
+        }
     }
     if (rc == VFB_OK && cudaStreamSynchronize(s) != cudaSuccess)
         rc = setError(VFB_ERR_CUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError()));
