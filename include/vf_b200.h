@@ -365,8 +365,20 @@ typedef struct vfb_scaling_args {
      * races there.  vfb_scaling_write_mask gives the mask under which the
      * result is that of the cells applied one by one in list order. */
     const uint8_t* fineWriteMask;
+    /* optional (NULL: the kernels walk the neighbour arrays): the 3x3x3 block
+     * of node indices above each cell's coarse / fine base node,
+     * coarseBlocks[27 i + x + 3 y + 9 z] (vfb_scaling_blocks), so that a
+     * launch reads the cell's nodes in one round instead of a chain of
+     * dependent neighbour loads.  No counterpart in the reference. */
+    const uint32_t* coarseBlocks;
+    const uint32_t* fineBlocks;
 } vfb_scaling_args;
 
+/* the blocks of vfb_scaling_args.coarseBlocks / fineBlocks for numberOfCells
+ * base nodes (device arrays; out holds 27 * numberOfCells uint32), walked
+ * along the reference's neighbour paths */
+int vfb_scaling_blocks(const uint32_t* cells, uint32_t numberOfCells, const uint32_t* neighborX,
+                       const uint32_t* neighborY, const uint32_t* neighborZ, uint32_t* out, void* stream);
 int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream);
 int vfb_scale_fine_to_coarse(int storage, const vfb_scaling_args* args, void* stream);
 /* vfb_scale_fine_to_coarse then vfb_scale_coarse_to_fine, in one launch (the

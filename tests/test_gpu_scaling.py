@@ -80,3 +80,35 @@ def test_gpu_interpolation_reduced_storage(cuda, coarse_to_fine, dtype, tol):
     host = run_host(c, coarse_to_fine, True, _lib.FP64)
     for g, h in zip(got, host):
         assert rel_l2(g, h) < tol
+
+
+@pytest.mark.parametrize("coarse_to_fine", [True, False])
+def test_block_tables_equal_the_neighbour_walk(cuda, coarse_to_fine):
+    """With the cells' block tables (vfb_scaling_blocks) the interpolation
+    reads the same nodes as through the neighbour walk: FP64 results equal bit
+    for bit."""
+    c = case(3)
+    outs = []
+    for tables in (False, True):
+        dC = torch.from_numpy(c["distC"].astype(np.float64)).cuda()
+        dF = torch.from_numpy(c["distF"].astype(np.float64)).cuda()
+        arrays, keep = device_arrays(c, np.float64)
+        a = scaling_args(c, coarse_to_fine, True, dC.data_ptr(), dF.data_ptr(), arrays)
+        if tables:
+            tag = "cf" if coarse_to_fine else "fc"
+            n = len(c[f"coarse_{tag}"])
+            bc = torch.empty(27 * n, dtype=torch.int32, device="cuda")
+            bf = torch.empty(27 * n, dtype=torch.int32, device="cuda")
+            lib = _lib.lib()
+            _lib.check(lib.vfb_scaling_blocks(arrays[f"coarse_{tag}"], n, arrays["gc.neighborX"], arrays["gc.neighborY"],
+                                              arrays["gc.neighborZ"], bc.data_ptr(), None))
+            _lib.check(lib.vfb_scaling_blocks(arrays[f"fine_{tag}"], n, arrays["gf.neighborX"], arrays["gf.neighborY"],
+                                              arrays["gf.neighborZ"], bf.data_ptr(), None))
+            keep += [bc, bf]
+            a.coarseBlocks, a.fineBlocks = bc.data_ptr(), bf.data_ptr()
+        fn = _lib.lib().vfb_scale_coarse_to_fine if coarse_to_fine else _lib.lib().vfb_scale_fine_to_coarse
+        _lib.check(fn(_lib.FP64, a, None))
+        torch.cuda.synchronize()
+        outs.append([t.cpu().numpy() for t in (dC, dF)])
+    for x, y in zip(*outs):
+        assert np.array_equal(x, y)

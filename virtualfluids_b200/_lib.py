@@ -115,6 +115,8 @@ class ScalingArgs(ctypes.Structure):
         ("offsetY", ctypes.c_void_p),
         ("offsetZ", ctypes.c_void_p),
         ("fineWriteMask", ctypes.c_void_p),
+        ("coarseBlocks", ctypes.c_void_p),
+        ("fineBlocks", ctypes.c_void_p),
     ]
 
 
@@ -186,6 +188,9 @@ _SIGNATURES = [
       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     ("vfb_scale_coarse_to_fine", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
     ("vfb_scale_fine_to_coarse", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
+    ("vfb_scaling_blocks", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
     ("vfb_scale_interface", ctypes.c_int,
      [ctypes.c_int, ctypes.POINTER(ScalingArgs), ctypes.POINTER(ScalingArgs), ctypes.c_void_p]),
     ("vfb_scaling_independent", ctypes.c_int,

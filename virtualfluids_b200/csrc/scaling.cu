@@ -117,6 +117,8 @@ struct ScalingView {
     const R* offY;
     const R* offZ;
     const uint8_t* mask; // coarse to fine: mask[27 i + d] bit c = corner c writes direction d (NULL: all)
+    const uint32_t* blocksC; // the cells' coarse / fine blocks, 27 per cell (NULL: walk)
+    const uint32_t* blocksF;
 };
 
 // the moments of the 8 source nodes of a cell (pre-collision view of parity EVEN);
@@ -241,6 +243,26 @@ __device__ __forceinline__ void cornerLocations(const uint32_t* B, int c, uint32
     }
 }
 
+// the eight locations of corner c of cell i: from the cell's block table
+// (eight independent loads) or by walking the neighbour arrays
+__device__ __forceinline__ void cellCornerLocations(const uint32_t* __restrict__ blocks, const uint32_t* cells,
+                                                    const uint32_t* nX, const uint32_t* nY, const uint32_t* nZ,
+                                                    uint32_t i, int c, uint32_t* Lc)
+{
+    if (blocks) {
+        const uint32_t* row = blocks + 27ull * i;
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            const int x = (c & 1) + (l & 1), y = ((c >> 1) & 1) + ((l >> 1) & 1), z = ((c >> 2) & 1) + ((l >> 2) & 1);
+            Lc[l] = __ldg(row + x + 3 * y + 9 * z);
+        }
+        return;
+    }
+    uint32_t B[27];
+    blockWalk(cells[i], nX, nY, nZ, B);
+    cornerLocations(B, c, Lc);
+}
+
 // the moments of the corner whose locations are Lc (pre-collision view of parity EVEN)
 template <bool EVEN, class S, class R>
 __device__ __forceinline__ SourceMoments<R> cornerMoments(const S* dist, unsigned long long N, const uint32_t* Lc, R omega)
@@ -262,16 +284,14 @@ __device__ __forceinline__ void coarseToFineBlock(const ScalingView<S, typename 
     const bool active = i < v.nCells;
     // every lane takes part in the shuffles: a group past the end works on the last cell
     const uint32_t ic = active ? i : v.nCells - 1;
-    uint32_t B[27], Lc[8];
-    blockWalk(v.coarseCells[ic], v.nXc, v.nYc, v.nZc, B);
-    cornerLocations(B, c, Lc);
+    uint32_t Lc[8];
+    cellCornerLocations(v.blocksC, v.coarseCells, v.nXc, v.nYc, v.nZc, ic, c, Lc);
     SourceMoments<R> src[8];
     gatherMoments(cornerMoments<EVEN_C>(v.distC, v.NC, Lc, v.omegaC), src);
     const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[ic], v.offY[ic], v.offZ[ic]);
     if (!active)
         return;
-    blockWalk(v.fineCells[ic], v.nXf, v.nYf, v.nZf, B);
-    cornerLocations(B, c, Lc);
+    cellCornerLocations(v.blocksF, v.fineCells, v.nXf, v.nYf, v.nZf, ic, c, Lc);
     const R x = (c & 1) ? R(1) / R(4) : -R(1) / R(4);
     const R y = (c & 2) ? R(1) / R(4) : -R(1) / R(4);
     const R z = (c & 4) ? R(1) / R(4) : -R(1) / R(4);
@@ -292,9 +312,8 @@ __device__ __forceinline__ void fineToCoarseBlock(const ScalingView<S, typename 
     const int c = (int)(threadIdx.x & 7u);
     const bool active = i < v.nCells;
     const uint32_t ic = active ? i : v.nCells - 1;
-    uint32_t B[27], Lc[8];
-    blockWalk(v.fineCells[ic], v.nXf, v.nYf, v.nZf, B);
-    cornerLocations(B, c, Lc);
+    uint32_t Lc[8];
+    cellCornerLocations(v.blocksF, v.fineCells, v.nXf, v.nYf, v.nZf, ic, c, Lc);
     SourceMoments<R> src[8];
     gatherMoments(cornerMoments<true>(v.distF, v.NF, Lc, v.omegaF), src);
     const InterpCoeffs<R> k = interpolationCoefficients(src, v.offX[ic], v.offY[ic], v.offZ[ic]);
@@ -302,17 +321,9 @@ __device__ __forceinline__ void fineToCoarseBlock(const ScalingView<S, typename 
         return;
     R f[27];
     interpolateFineToCoarse(f, k, v.omegaC);
-    // the coarse node's own eight locations
-    const uint32_t kc = v.coarseCells[ic];
+    // the coarse node's own eight locations (corner 0 of its block)
     uint32_t L[8];
-    L[0] = kc;
-    L[1] = v.nXc[kc];
-    L[2] = v.nYc[kc];
-    L[4] = v.nZc[kc];
-    L[3] = v.nYc[L[1]];
-    L[5] = v.nZc[L[1]];
-    L[6] = v.nZc[L[2]];
-    L[7] = v.nZc[L[3]];
+    cellCornerLocations(v.blocksC, v.coarseCells, v.nXc, v.nYc, v.nZc, ic, 0, L);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
         if ((d & 7) == c)
@@ -371,6 +382,8 @@ static ScalingView<S, R> viewOf(const vfb_scaling_args* a)
     v.offY = static_cast<const R*>(a->offsetY);
     v.offZ = static_cast<const R*>(a->offsetZ);
     v.mask = a->fineWriteMask;
+    v.blocksC = a->coarseBlocks;
+    v.blocksF = a->fineBlocks;
     return v;
 }
 
@@ -510,6 +523,32 @@ extern "C" int vfb_scaling_write_mask(const uint32_t* fineCells, uint32_t n, con
 extern "C" int vfb_scale_coarse_to_fine(int storage, const vfb_scaling_args* args, void* stream)
 {
     return runScaling(true, storage, args, stream);
+}
+
+__global__ void scalingBlocksKernel(const uint32_t* __restrict__ cells, uint32_t n, const uint32_t* __restrict__ nX,
+                                    const uint32_t* __restrict__ nY, const uint32_t* __restrict__ nZ,
+                                    uint32_t* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    uint32_t B[27];
+    blockWalk(cells[i], nX, nY, nZ, B);
+#pragma unroll
+    for (int j = 0; j < 27; ++j)
+        out[27ull * i + j] = B[j];
+}
+
+extern "C" int vfb_scaling_blocks(const uint32_t* cells, uint32_t n, const uint32_t* nX, const uint32_t* nY,
+                                  const uint32_t* nZ, uint32_t* out, void* stream)
+{
+    clearError();
+    if (n == 0)
+        return VFB_OK;
+    if (!cells || !nX || !nY || !nZ || !out)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    scalingBlocksKernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(cells, n, nX, nY, nZ, out);
+    return checkLaunch("interface cell blocks");
 }
 
 extern "C" int vfb_scale_interface(int storage, const vfb_scaling_args* fineToCoarse,

@@ -53,6 +53,7 @@ struct ResidualList {
 // + ICellNeigh, Calculation.h:72-89)
 struct InterfaceDevice {
     DeviceBuffer coarse, fine, offX, offY, offZ, mask;
+    DeviceBuffer blocksC, blocksF; // 27 node indices per cell above its coarse / fine base node
     uint32_t n = 0;
 };
 

@@ -592,6 +592,8 @@ int refinement(vfb_simulation& S, Level& C, Level& F, void* stream)
             b[i].offsetY = I.offY.ptr;
             b[i].offsetZ = I.offZ.ptr;
             b[i].fineWriteMask = static_cast<const uint8_t*>(I.mask.ptr);
+            b[i].coarseBlocks = static_cast<const uint32_t*>(I.blocksC.ptr);
+            b[i].fineBlocks = static_cast<const uint32_t*>(I.blocksF.ptr);
         }
         return vfb_scale_interface(S.params.storage, &b[0], &b[1], stream);
     }
@@ -606,6 +608,8 @@ int refinement(vfb_simulation& S, Level& C, Level& F, void* stream)
         a.offsetY = I.offY.ptr;
         a.offsetZ = I.offZ.ptr;
         a.fineWriteMask = static_cast<const uint8_t*>(I.mask.ptr);
+        a.coarseBlocks = static_cast<const uint32_t*>(I.blocksC.ptr);
+        a.fineBlocks = static_cast<const uint32_t*>(I.blocksF.ptr);
         const int rc = i == 0 ? vfb_scale_fine_to_coarse(S.params.storage, &a, stream)
                               : vfb_scale_coarse_to_fine(S.params.storage, &a, stream);
         if (rc)
@@ -814,6 +818,30 @@ extern "C" int vfb_sim_create(const vfb_sim_params* params, void* grid, vfb_simu
                                          u32(cny), u32(cnz), C.N, u32(nx), u32(ny), u32(nz), S->levels[l + 1]->N,
                                          &together);
             C.interfaceTogether = together != 0;
+        }
+    }
+    // the interface cells' blocks of node indices, walked once on the device
+    for (int l = 0; l + 1 < nLevels && rc == VFB_OK; ++l) {
+        Level& C = *S->levels[l];
+        Level& F = *S->levels[l + 1];
+        for (InterfaceDevice* I : { &C.coarseToFine, &C.fineToCoarse }) {
+            if (I->n == 0)
+                continue;
+            if (I->blocksC.allocate(27ull * I->n * sizeof(uint32_t)) != cudaSuccess ||
+                I->blocksF.allocate(27ull * I->n * sizeof(uint32_t)) != cudaSuccess) {
+                rc = setError(VFB_ERR_CUDA, "interface block tables");
+                break;
+            }
+            rc = vfb_scaling_blocks(static_cast<const uint32_t*>(I->coarse.ptr), I->n,
+                                    static_cast<const uint32_t*>(C.nX.ptr), static_cast<const uint32_t*>(C.nY.ptr),
+                                    static_cast<const uint32_t*>(C.nZ.ptr), static_cast<uint32_t*>(I->blocksC.ptr), s);
+            if (rc == VFB_OK)
+                rc = vfb_scaling_blocks(static_cast<const uint32_t*>(I->fine.ptr), I->n,
+                                        static_cast<const uint32_t*>(F.nX.ptr), static_cast<const uint32_t*>(F.nY.ptr),
+                                        static_cast<const uint32_t*>(F.nZ.ptr), static_cast<uint32_t*>(I->blocksF.ptr),
+                                        s);
+            if (rc != VFB_OK)
+                break;
         }
     }
     if (rc == VFB_OK && cudaStreamSynchronize(s) != cudaSuccess)
