@@ -33,6 +33,8 @@ struct CollisionKernelArgs {
     const uint32_t* __restrict__ nZ;
     const uint32_t* __restrict__ fluid;
     uint32_t nFluid;
+    // the list's location table (8 * nFluid, vfb_bc_locations layout) or null
+    const uint32_t* __restrict__ table;
     K17Rates<R> rates;
     R fx, fy, fz;         // forces * 1/2 * forceFactor
     R gfx, gfy, gfz;      // raw global forces (body-force template)
@@ -75,6 +77,21 @@ __device__ __forceinline__ void scatterPre(const typename Storage<S>::R* f, S* _
 
 constexpr int kCollisionThreads = 128;
 
+// the eight locations of list entry i (node k): from the list's location
+// table in one round of independent loads, or through the neighbour chain
+template <class S>
+__device__ __forceinline__ Locs entryLocations(const CollisionKernelArgs<S>& a, uint32_t i, uint32_t k)
+{
+    if (a.table) {
+        Locs L;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+            L.k[l] = __ldg(a.table + (unsigned long long)l * a.nFluid + i);
+        return L;
+    }
+    return listIndices(k, a.nX, a.nY, a.nZ);
+}
+
 template <class S, bool EVEN, bool WRITE_MACRO, bool BODY_FORCE>
 __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKernelArgs<S> a)
 {
@@ -95,7 +112,7 @@ __global__ void __launch_bounds__(kCollisionThreads) k17Kernel(const CollisionKe
         a.bfz[k] = R(0);
     }
 
-    const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
+    const Locs L = entryLocations(a, i, k);
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -122,7 +139,7 @@ __global__ void __launch_bounds__(kCollisionThreads) bgkKernel(const CollisionKe
     if (i >= a.nFluid)
         return;
     const uint32_t k = __ldg(a.fluid + i);
-    const Locs L = listIndices(k, a.nX, a.nY, a.nZ);
+    const Locs L = entryLocations(a, i, k);
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -364,10 +381,11 @@ __global__ void __launch_bounds__(kReduceThreads) massEnergyKernel(const S* dist
 
 // ------------------------------------------------------------- launchers --
 template <class S>
-static int launchCollision(bool bgk, const vfb_collision_args* a, cudaStream_t stream)
+static int launchCollision(bool bgk, const vfb_collision_args* a, cudaStream_t stream, const uint32_t* table = nullptr)
 {
     using R = typename Storage<S>::R;
     CollisionKernelArgs<S> k;
+    k.table = table;
     k.dist = static_cast<S*>(a->distributions);
     k.N = a->numberOfLBnodes;
     k.nX = a->neighborX;
@@ -533,6 +551,26 @@ extern "C" int vfb_k17_collision(int storage, const vfb_collision_args* args, vo
     default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
     }
 }
+
+namespace vfb
+{
+int laneCollision(int storage, bool bgk, const vfb_collision_args* args, const uint32_t* table, void* stream)
+{
+    int rc = checkCollisionArgs(storage, args, bgk);
+    if (rc != VFB_OK || args->numberOfFluidNodes == 0)
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchCollision<float>(bgk, args, s, table);
+    case VFB_FP64: return launchCollision<double>(bgk, args, s, table);
+    case VFB_FP16: return launchCollision<__half>(bgk, args, s, table);
+    case VFB_FX16: return launchCollision<int16_t>(bgk, args, s, table);
+    case VFB_FX16W: return launchCollision<fx16w_t>(bgk, args, s, table);
+    case VFB_BF16: return launchCollision<__nv_bfloat16>(bgk, args, s, table);
+    default: return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    }
+}
+} // namespace vfb
 
 extern "C" int vfb_bgk_collision(int storage, const vfb_collision_args* args, void* stream)
 {

@@ -263,6 +263,12 @@ static int buildPlan(vfb_collision_plan_impl& p, int storage, const vfb_collisio
     if (e == cudaSuccess)
         e = upload(&p.laneList, lane, stream);
     if (e == cudaSuccess)
+        e = cudaMalloc(&p.laneLocations, sizeof(uint32_t) * std::max<size_t>(1, 8 * lane.size()));
+    if (e == cudaSuccess && !lane.empty())
+        if (const int rc = vfb_bc_locations(reinterpret_cast<const int32_t*>(p.laneList), p.nLane, p.nX, p.nY, p.nZ,
+                                            p.laneLocations, stream))
+            return rc;
+    if (e == cudaSuccess)
         e = cudaMalloc(&p.error, sizeof(int));
     if (e == cudaSuccess)
         e = cudaMemsetAsync(p.error, 0, sizeof(int), stream);
@@ -301,7 +307,7 @@ static int runPlanned(Op op, const vfb_collision_plan* plan, const vfb_collision
         vfb_collision_args lane = *c;
         lane.fluidNodeIndices = p.laneList;
         lane.numberOfFluidNodes = p.nLane;
-        const int rc = op == Op::K17 ? vfb_k17_collision(p.storage, &lane, stream) : vfb_bgk_collision(p.storage, &lane, stream);
+        const int rc = laneCollision(p.storage, op != Op::K17, &lane, p.laneLocations, stream);
         if (rc != VFB_OK)
             return rc;
     }
@@ -337,6 +343,7 @@ extern "C" int vfb_collision_plan_create(int storage, const vfb_collision_args* 
     if (rc != VFB_OK) {
         cudaFree(p->meta);
         cudaFree(p->laneList);
+        cudaFree(p->laneLocations);
         cudaFree(p->error);
         delete p;
         return rc;
@@ -367,6 +374,7 @@ extern "C" int vfb_collision_plan_destroy(vfb_collision_plan* plan)
     auto* p = reinterpret_cast<vfb_collision_plan_impl*>(plan);
     cudaFree(p->meta);
     cudaFree(p->laneList);
+    cudaFree(p->laneLocations);
     cudaFree(p->error);
     freeEpilogue(*p);
     delete p;

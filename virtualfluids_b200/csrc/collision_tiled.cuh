@@ -615,6 +615,7 @@ struct vfb_collision_plan_impl {
     long long wrapDelta[3] = { 0, 0, 0 };
     uint32_t* meta = nullptr;
     uint32_t* laneList = nullptr;
+    uint32_t* laneLocations = nullptr; // 8 * nLane: the lane list's location table
     uint32_t nTiles = 0;
     uint32_t nLane = 0;
     // tiles, bulk tiles, lane blocks, bulk-fed nodes, wrap nodes served in bulk tiles, nodes collided lane by lane
@@ -863,4 +864,7 @@ int launchTiledFP16(Op op, const vfb_collision_plan_impl& p, const vfb_collision
 int launchTiledBF16(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
 int launchTiledFX16(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
 int launchTiledFX16W(Op op, const vfb_collision_plan_impl& p, const vfb_collision_args* c, cudaStream_t s);
+// the generic collision over a node list with the list's location table
+// (collision.cu; table may be null: the neighbour chain)
+int laneCollision(int storage, bool bgk, const vfb_collision_args* args, const uint32_t* table, void* stream);
 } // namespace vfb
