@@ -900,8 +900,19 @@ def kernel_report(args):
         a.omegaCoarse, a.omegaFine = 1.9, 1.85
         a.offsetX = a.offsetY = a.offsetZ = dev(zeros)
         ms = timed(lambda: _lib.check(fn(_lib.FP32, a, None)))
-        record("coarse_to_fine_cells" if tag == "cf" else "fine_to_coarse_cells", n, 8 * 27 * 4 + write + 20, ms,
-               "cells")
+        name = "coarse_to_fine_cells" if tag == "cf" else "fine_to_coarse_cells"
+        record(name, n, 8 * 27 * 4 + write + 20, ms, "cells")
+        # the same cells with their node blocks read from tables (vfb_scaling_blocks, as the simulation builds
+        # them once at setup) instead of walked through the neighbour arrays: 2 x 27 indices more per cell
+        bc = torch.empty(27 * n, dtype=torch.int32, device="cuda")
+        bf = torch.empty(27 * n, dtype=torch.int32, device="cuda")
+        keep += [bc, bf]
+        for cells_ptr, lat_, out_ in ((a.coarseCells, latc, bc), (a.fineCells, latf, bf)):
+            _lib.check(_lib.lib().vfb_scaling_blocks(cells_ptr, n, lat_.neighborX.data_ptr(), lat_.neighborY.data_ptr(),
+                                                     lat_.neighborZ.data_ptr(), out_.data_ptr(), None))
+        a.coarseBlocks, a.fineBlocks = bc.data_ptr(), bf.data_ptr()
+        ms = timed(lambda: _lib.check(fn(_lib.FP32, a, None)))
+        record(name + "_block_tables", n, 8 * 27 * 4 + write + 20 + 2 * 27 * 4, ms, "cells")
     print(json.dumps(out), flush=True)
     return 0
 
