@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
                                                          const int32_t* __restrict__ bcK,
                                                          const int32_t* __restrict__ bcKN,
                                                          const typename Storage<S>::R* __restrict__ rhoBC, uint32_t nBC,
-                                                         int axis, int sgn)
+                                                         int axis, int sgn, const uint32_t* __restrict__ locations)
 {
     gridDependencyWait();
     using R = typename Storage<S>::R;
@@ -110,8 +110,19 @@ __global__ void __launch_bounds__(128) bcPressureKernel(S* __restrict__ dist, co
     if (i >= nBC)
         return;
     const unsigned long long N = lat.N;
-    const Locs L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
-    const Locs LN = listIndices((uint32_t)__ldg(bcKN + i), lat.nX, lat.nY, lat.nZ);
+    // the BC node's and its neighbour's locations: from the list's table
+    // (16 * nBC, the node's eight then the neighbour's) or through the chain
+    Locs L, LN;
+    if (locations) {
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            L.k[l] = __ldg(locations + (unsigned long long)l * nBC + i);
+            LN.k[l] = __ldg(locations + (unsigned long long)(8 + l) * nBC + i);
+        }
+    } else {
+        L = listIndices((uint32_t)__ldg(bcK + i), lat.nX, lat.nY, lat.nZ);
+        LN = listIndices((uint32_t)__ldg(bcKN + i), lat.nX, lat.nY, lat.nZ);
+    }
     R f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -241,7 +252,7 @@ static int launchPost(int kind, const vfb_bc_lattice* t, const vfb_bc_list* l, c
 
 template <class S>
 static int launchPressure(const vfb_bc_lattice* t, const int32_t* k, const int32_t* kN, const void* rhoBC, uint32_t n,
-                          int axis, int sgn, cudaStream_t stream)
+                          int axis, int sgn, cudaStream_t stream, const uint32_t* locations = nullptr)
 {
     using R = typename Storage<S>::R;
     BcLattice<R> lat { t->numberOfLBnodes, t->neighborX, t->neighborY, t->neighborZ, (R)t->omega };
@@ -249,9 +260,11 @@ static int launchPressure(const vfb_bc_lattice* t, const int32_t* k, const int32
     const unsigned blocks = (n + 127) / 128;
     const R* rho = static_cast<const R*>(rhoBC);
     if (t->isEvenTimestep)
-        launchDependent(bcPressureKernel<S, true>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn);
+        launchDependent(bcPressureKernel<S, true>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn,
+                        locations);
     else
-        launchDependent(bcPressureKernel<S, false>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn);
+        launchDependent(bcPressureKernel<S, false>, blocks, 128, 0, stream, dist, lat, k, kN, rho, n, axis, sgn,
+                        locations);
     return checkLaunch("pressure boundary condition");
 }
 
@@ -372,6 +385,40 @@ extern "C" int vfb_bc_pressure_noneq(int storage, const vfb_bc_lattice* lattice,
     default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s);
     }
 }
+
+namespace vfb
+{
+// vfb_bc_pressure_noneq with the list's location table (16 * numberOfBCnodes:
+// the eight locations of each node k, then of its neighbour kN; the
+// simulation builds it once per list)
+int pressureNoneqWithLocations(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,
+                               const void* rhoBC, uint32_t numberOfBCnodes, int direction, const uint32_t* locations,
+                               void* stream)
+{
+    clearError();
+    if (vfb_storage_bytes(storage) == 0)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+    if (numberOfBCnodes == 0)
+        return VFB_OK;
+    if (const int rc = checkLattice(lattice))
+        return rc;
+    if (!k || !kN || !rhoBC)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "NULL k, kN or rhoBC");
+    if (direction < dP00 || direction > d00M)
+        return setError(VFB_ERR_INVALID_ARGUMENT, "direction %d is not an axis direction (1..6)", direction);
+    const int axis = cx(direction) != 0 ? 0 : cy(direction) != 0 ? 1 : 2;
+    const int sgn = axis == 0 ? cx(direction) : axis == 1 ? cy(direction) : cz(direction);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (storage) {
+    case VFB_FP32: return launchPressure<float>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    case VFB_FP64: return launchPressure<double>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    case VFB_FP16: return launchPressure<__half>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    case VFB_FX16: return launchPressure<int16_t>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    case VFB_FX16W: return launchPressure<fx16w_t>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    default: return launchPressure<__nv_bfloat16>(lattice, k, kN, rhoBC, numberOfBCnodes, axis, sgn, s, locations);
+    }
+}
+} // namespace vfb
 
 extern "C" int vfb_bc_outflow_nonreflecting(int storage, const vfb_bc_lattice* lattice, const int32_t* k,
                                             const int32_t* kN, uint32_t numberOfBCnodes, int direction,

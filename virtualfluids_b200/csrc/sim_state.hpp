@@ -59,6 +59,7 @@ struct InterfaceDevice {
 
 struct PressureListDevice {
     DeviceBuffer k, kN, rho;
+    DeviceBuffer locations; // 16 * n: the eight locations of each node, then of its neighbour
     uint32_t n = 0;
     int direction = 0;
 };
@@ -122,6 +123,10 @@ struct Level {
     }
 };
 
+// vfb_bc_pressure_noneq reading the list's location table (bc.cu)
+int pressureNoneqWithLocations(int storage, const vfb_bc_lattice* lattice, const int32_t* k, const int32_t* kN,
+                               const void* rhoBC, uint32_t numberOfBCnodes, int direction, const uint32_t* locations,
+                               void* stream);
 } // namespace vfb
 
 struct vfb_simulation {

@@ -234,6 +234,17 @@ int uploadLevel(Level& L, void* grid, int level, int storage, double geometryVel
                     return fail((p + ".rho").c_str());
                 e = uploadReal(P->rho, raw, storage, s, keep);
             }
+            if (e == cudaSuccess && P->n) {
+                e = P->locations.allocate(16ull * P->n * sizeof(uint32_t));
+                for (int half = 0; half < 2 && e == cudaSuccess; ++half)
+                    if (const int rc = vfb_bc_locations(static_cast<const int32_t*>(half ? P->kN.ptr : P->k.ptr), P->n,
+                                                        static_cast<const uint32_t*>(L.nX.ptr),
+                                                        static_cast<const uint32_t*>(L.nY.ptr),
+                                                        static_cast<const uint32_t*>(L.nZ.ptr),
+                                                        static_cast<uint32_t*>(P->locations.ptr) + 8ull * P->n * half,
+                                                        s))
+                        return rc;
+            }
             if (e == cudaSuccess) {
                 if (!need((p + ".dir").c_str(), 4) || count != 1)
                     return fail((p + ".dir").c_str());
@@ -550,7 +561,8 @@ int preCollisionBC(vfb_simulation& S, Level& L, void* stream)
         const auto* kN = static_cast<const int32_t*>(P->kN.ptr);
         // BoundaryConditionFactory::getPressureBoundaryConditionPre (BoundaryConditionFactory.cpp:151-168)
         const int rc = S.params.pressureBC == 0
-                           ? vfb_bc_pressure_noneq(S.params.storage, &t, k, kN, P->rho.ptr, P->n, P->direction, stream)
+                           ? pressureNoneqWithLocations(S.params.storage, &t, k, kN, P->rho.ptr, P->n, P->direction,
+                                                        static_cast<const uint32_t*>(P->locations.ptr), stream)
                            : vfb_bc_outflow_nonreflecting(S.params.storage, &t, k, kN, P->n, P->direction,
                                                           S.params.pressureBC == 2,
                                                           S.params.outflowPressureCorrectionFactor, stream);
